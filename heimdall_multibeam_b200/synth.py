@@ -1,0 +1,204 @@
+"""Seeded synthetic filterbanks for the single-pulse search.
+
+The reference ships no test data; its only generator (Formats/giant_maker.C:
+183-445) is not built.  This module writes filterbanks to the workload
+definitions used for parity tests and the benchmark:
+
+* Gaussian noise of mean 128 and standard deviation 16, rounded and clipped
+  to uint8 [0, 255];
+* dispersed Gaussian pulses with arrival time t_c = t0 + 4148.808 * DM *
+  (f_c^-2 - f_top^-2) s (f in MHz) in channel c = 0 (top of the band) ... C-1;
+* optional RFI: persistent narrow-band channels and zero-DM broadband bursts.
+
+Pulse amplitude follows the optimal matched-filter definition of integrated
+S/N: S/N = sqrt(sum_c sum_t s_c(t)^2) / sigma over the pulse footprint, so a
+pulse of S/N 20 carries amplitude 20 * sigma / sqrt(sum g^2) per sample.
+(giant_maker.C:344-365 uses a width-adjusted convention instead.)
+
+Random numbers come from numpy's Philox4x32-10 counter-based generator keyed by
+(seed, beam), so every beam is reproducible on its own and on any machine.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+DISPERSION_K = 4148.808  # s MHz^2 pc^-1 cm^3
+
+
+@dataclasses.dataclass
+class Pulse:
+    t0: float          # arrival sample at the top of the band (channel 0)
+    dm: float
+    fwhm_s: float      # full width at half maximum, seconds
+    snr: float         # integrated S/N (optimal matched filter)
+
+
+@dataclasses.dataclass
+class Beam:
+    data: np.ndarray   # (nsamps, nchans) uint8, time-major
+    pulses: List[Pulse]
+    nchans: int
+    dt: float
+    f0: float
+    df: float
+    seed: int
+    beam: int
+
+
+def _rng(seed: int, beam: int) -> np.random.Generator:
+    key = (int(seed) & 0xFFFFFFFF) << 32 | (int(beam) & 0xFFFFFFFF)
+    return np.random.Generator(np.random.Philox(key=key))
+
+
+def dispersion_delay_s(dm: float, f_mhz: np.ndarray, f_top: float) -> np.ndarray:
+    return DISPERSION_K * dm * (f_mhz ** -2.0 - f_top ** -2.0)
+
+
+def inject_pulse(x: np.ndarray, p: Pulse, dt: float, f0: float, df: float,
+                 sigma: float = 16.0) -> None:
+    """Adds one dispersed Gaussian pulse to the float filterbank x (in place)."""
+    nsamps, nchans = x.shape
+    f = f0 + df * np.arange(nchans)
+    centres = p.t0 + dispersion_delay_s(p.dm, f, f0) / dt
+    s = max(p.fwhm_s / dt / (2.0 * math.sqrt(2.0 * math.log(2.0))), 0.3)
+    half = int(math.ceil(6.0 * s)) + 1
+    prof = []
+    energy = 0.0
+    for c in range(nchans):
+        lo = int(math.floor(centres[c])) - half
+        hi = int(math.floor(centres[c])) + half + 1
+        t = np.arange(lo, hi)
+        g = np.exp(-0.5 * ((t - centres[c]) / s) ** 2)
+        keep = (t >= 0) & (t < nsamps)
+        prof.append((c, t[keep], g[keep]))
+        energy += float(np.sum(g * g))
+    if energy <= 0.0:
+        return
+    amp = p.snr * sigma / math.sqrt(energy)
+    for c, t, g in prof:
+        x[t, c] += amp * g
+
+
+def make_beam(nsamps: int, nchans: int, dt: float, f0: float, df: float,
+              pulses: Sequence[Pulse] = (), seed: int = 1, beam: int = 0,
+              rfi_chan_frac: float = 0.0, n_bursts: int = 0,
+              rng: Optional[np.random.Generator] = None) -> Beam:
+    """One beam of noise + pulses (+ RFI), rounded and clipped to uint8."""
+    g = rng if rng is not None else _rng(seed, beam)
+    x = g.standard_normal((nsamps, nchans), dtype=np.float32)
+    x *= 16.0
+    x += 128.0
+    for p in pulses:
+        inject_pulse(x, p, dt, f0, df)
+    if rfi_chan_frac > 0.0:
+        nbad = int(round(rfi_chan_frac * nchans))
+        bad = g.choice(nchans, size=nbad, replace=False)
+        x[:, bad] += 40.0 * 16.0
+    for _ in range(n_bursts):
+        width = int(g.integers(1, 51))
+        start = int(g.integers(0, max(nsamps - width, 1)))
+        x[start:start + width, :] += 8.0 * 16.0
+    np.rint(x, out=x)
+    np.clip(x, 0, 255, out=x)
+    return Beam(x.astype(np.uint8), list(pulses), nchans, dt, f0, df, seed, beam)
+
+
+def random_pulses(g: np.random.Generator, n: int, t_lo: float, t_hi: float,
+                  dm_lo: float, dm_hi: float, fwhm_lo_s: float, fwhm_hi_s: float,
+                  snr_lo: float, snr_hi: float) -> List[Pulse]:
+    out = []
+    for _ in range(n):
+        dm = float(g.uniform(dm_lo, dm_hi))
+        fwhm = float(math.exp(g.uniform(math.log(fwhm_lo_s), math.log(fwhm_hi_s))))
+        snr = float(g.uniform(snr_lo, snr_hi))
+        t0 = float(g.uniform(t_lo, t_hi))
+        out.append(Pulse(t0, dm, fwhm, snr))
+    return out
+
+
+def max_delay_samples(dm: float, nchans: int, dt: float, f0: float, df: float) -> float:
+    f_low = f0 + df * (nchans - 1)
+    return float(dispersion_delay_s(dm, np.array([f_low]), f0)[0] / dt)
+
+
+# --------------------------------------------------------------------------
+# Workloads
+# --------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    nchans: int
+    dt: float
+    f0: float
+    df: float
+    nsamps: int          # per beam
+    nbeams: int
+    dm_min: float
+    dm_max: float
+    boxcar_max: int
+    clean: bool
+    description: str
+
+
+SEARCH_C0 = Workload("plain_c256_n65536", 256, 64e-6, 1500.0, -1.5625, 1 << 16, 1,
+                     0.0, 1000.0, 1 << 10, False,
+                     "plain single beam: 256 ch uint8, 1500 MHz top, -1.5625 MHz, 64 us, "
+                     "2^16 samples, DM 0-1000, boxcars 2^0..2^10")
+SEARCH_C1 = Workload("plain_c1024_n262144_rfi", 1024, 64e-6, 1520.0, -0.390625, 1 << 18, 1,
+                     0.0, 2000.0, 1 << 12, True,
+                     "plain single beam at survey size with RFI: 1024 ch uint8, 1520 MHz top, "
+                     "-0.390625 MHz, 64 us, 2^18 samples, DM 0-2000, boxcars 2^0..2^12, "
+                     "clean_filterbank_rfi on")
+SEARCH_C2 = Workload("multibeam_36x_c320_n32768", 320, 655.36e-6, 851.0, -0.09765625, 1 << 15, 36,
+                     0.0, 2000.0, 1 << 9, False,
+                     "36 uniform beams x 320 ch uint8, 851 MHz top, -0.09765625 MHz, "
+                     "655.36 us, 2^15 samples per beam, DM 0-2000, boxcars 2^0..2^9")
+
+
+def make_c0(seed: int = 2024) -> Beam:
+    w = SEARCH_C0
+    md = max_delay_samples(w.dm_max, w.nchans, w.dt, w.f0, w.df)
+    span = w.nsamps - md - w.boxcar_max
+    pulses = [Pulse(w.boxcar_max + span * (k + 1) / 4.0, dm, fw, 20.0)
+              for k, (dm, fw) in enumerate([(100.0, 0.5e-3), (500.0, 2e-3), (900.0, 8e-3)])]
+    return make_beam(w.nsamps, w.nchans, w.dt, w.f0, w.df, pulses, seed=seed, beam=0)
+
+
+def make_c1(seed: int = 2025, nsamps: Optional[int] = None, nchans: Optional[int] = None,
+            npulses: int = 20, rfi: bool = True) -> Beam:
+    w = SEARCH_C1
+    ns = nsamps or w.nsamps
+    nc = nchans or w.nchans
+    df = w.df * (w.nchans / nc)
+    g = _rng(seed, 0x5EED)
+    md = max_delay_samples(w.dm_max, nc, w.dt, w.f0, df)
+    hi = max(ns - md - 2 * w.boxcar_max, w.boxcar_max + 1)
+    pulses = random_pulses(g, npulses, w.boxcar_max, hi, 50.0, 2000.0, 0.1e-3, 30e-3, 6.0, 50.0)
+    return make_beam(ns, nc, w.dt, w.f0, df, pulses, seed=seed, beam=0,
+                     rfi_chan_frac=0.05 if rfi else 0.0, n_bursts=10 if rfi else 0)
+
+
+def make_multibeam(w: Workload, seed: int = 2026, pulses_per_beam: int = 2,
+                   fwhm_lo_s: float = 1e-3, fwhm_hi_s: float = 50e-3,
+                   snr_lo: float = 6.0, snr_hi: float = 30.0) -> List[Beam]:
+    beams = []
+    md = max_delay_samples(w.dm_max, w.nchans, w.dt, w.f0, w.df)
+    hi = max(w.nsamps - md - 2 * w.boxcar_max, w.boxcar_max + 1)
+    for b in range(w.nbeams):
+        g = _rng(seed, b)
+        pulses = random_pulses(g, pulses_per_beam, w.boxcar_max, hi, 50.0, w.dm_max,
+                               fwhm_lo_s, fwhm_hi_s, snr_lo, snr_hi)
+        beams.append(make_beam(w.nsamps, w.nchans, w.dt, w.f0, w.df, pulses, seed=seed,
+                               beam=b, rng=g))
+    return beams
+
+
+def stf(beams: Sequence[Beam]) -> np.ndarray:
+    """Concatenates beams in time (the reference's multibeam "STF" layout,
+    Formats/PSRDadaRingBuffer.C:194-198)."""
+    return np.ascontiguousarray(np.concatenate([b.data for b in beams], axis=0))

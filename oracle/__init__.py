@@ -1,0 +1,302 @@
+"""ctypes front end of the CPU checker (TEST INFRASTRUCTURE ONLY).
+
+Two libraries are wrapped:
+
+* ``_build/liboracle.so`` -- the C restatement in oracle.c of every stage of
+  Heimdall's per-gulp chain;
+* ``_ref/libhdref.so`` -- the reference's own ``Pipeline/*.cu`` rebuilt on
+  Thrust's OpenMP backend (``make -C oracle ref``), driven through its own
+  ``hd_create_pipeline`` / ``hd_execute`` (Pipeline/pipeline.cu:138-1087).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU baseline leg import
+this package.  The product (heimdall_multibeam_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import subprocess
+import tempfile
+from typing import Dict, List, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libhdref.so")            # CLEANING defined
+REF_NOCLEAN_PATH = os.path.join(HERE, "_ref", "libhdref_noclean.so")
+
+_szp = C.POINTER(C.c_size_t)
+_fp = C.POINTER(C.c_float)
+
+
+class OrParams(C.Structure):
+    _fields_ = [
+        ("nchans", C.c_size_t),
+        ("dt", C.c_float), ("f0", C.c_float), ("df", C.c_float),
+        ("dm_min", C.c_float), ("dm_max", C.c_float), ("dm_tol", C.c_float),
+        ("dm_pulse_width", C.c_float),
+        ("baseline_length", C.c_float),
+        ("rfi_tol", C.c_float),
+        ("boxcar_max", C.c_size_t),
+        ("detect_thresh", C.c_float),
+        ("cand_sep_time", C.c_size_t), ("cand_sep_filter", C.c_size_t),
+        ("cand_sep_dm", C.c_size_t),
+        ("max_giant_rate", C.c_float),
+        ("min_tscrunch_width", C.c_size_t),
+        ("clean", C.c_int),
+        ("num_channel_zaps", C.c_uint),
+        ("channel_zaps", _szp),
+        ("nthreads", C.c_int),
+    ]
+
+
+class OrGiants(C.Structure):
+    _fields_ = [("count", C.c_size_t), ("cap", C.c_size_t), ("peaks", _fp),
+                ("inds", _szp), ("begins", _szp), ("ends", _szp),
+                ("filter_inds", _szp), ("dm_inds", _szp), ("members", _szp)]
+
+
+class OrResult(C.Structure):
+    _fields_ = [("error", C.c_int), ("nsamps_processed", C.c_size_t),
+                ("dm_count", C.c_size_t), ("max_delay", C.c_size_t),
+                ("giants", OrGiants), ("labels", _szp), ("label_count", C.c_size_t),
+                ("groups", OrGiants), ("group_dms", _fp)]
+
+
+DEFAULTS = dict(  # Pipeline/default_params.C:10-66
+    nchans=1024, dt=64e-6, f0=1581.804688, df=-0.390625, dm_min=0.0, dm_max=1000.0,
+    dm_tol=1.25, dm_pulse_width=40.0, baseline_length=2.0, rfi_tol=5.0, boxcar_max=4096,
+    detect_thresh=6.0, cand_sep_time=3, cand_sep_filter=3, cand_sep_dm=200,
+    max_giant_rate=0.0, min_tscrunch_width=4096, clean=0, channel_zaps=(), nthreads=0,
+    beam=0)
+
+_lib = None
+_ref = {}
+
+
+def build(ref: bool = False) -> None:
+    """Compiles the checker (and, with ref=True, the reference build)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.or_generate_dm_list.restype = C.c_size_t
+        L.or_generate_dm_list.argtypes = [C.c_float, C.c_float, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_size_t, C.c_double,
+                                          _fp, C.c_size_t]
+        L.or_delay_table.argtypes = [C.c_size_t, C.c_float, C.c_float, C.c_float, _fp]
+        L.or_max_delay.restype = C.c_size_t
+        L.or_max_delay.argtypes = [_fp, C.c_size_t, _fp, C.c_size_t]
+        L.or_dedisperse.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                    C.c_void_p, _fp, C.c_size_t, _fp, _fp, C.c_size_t, C.c_int]
+        for n in ("or_median3", "or_median4", "or_median5"):
+            getattr(L, n).restype = C.c_float
+        L.or_median3.argtypes = [C.c_float] * 3
+        L.or_median4.argtypes = [C.c_float] * 4
+        L.or_median5.argtypes = [C.c_float] * 5
+        L.or_hd_execute.argtypes = [C.POINTER(OrParams), C.c_void_p, C.c_size_t, C.c_size_t,
+                                    C.c_size_t, C.c_size_t, C.POINTER(OrResult)]
+        L.or_result_free.argtypes = [C.POINTER(OrResult)]
+        L.or_clean_filterbank_rfi.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                              C.c_float, C.c_float, C.c_float, C.c_size_t,
+                                              C.c_size_t, C.c_void_p, C.c_void_p]
+        L.or_hash.restype = C.c_uint32
+        L.or_hash.argtypes = [C.c_uint32]
+        L.or_uniform_uint.restype = C.c_uint32
+        L.or_uniform_uint.argtypes = [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32]
+        L.or_rms_block.restype = C.c_float
+        L.or_rms_block.argtypes = [_fp, C.c_size_t, C.c_size_t, C.c_size_t]
+        L.or_rms_beams.argtypes = [_fp, _fp, C.c_size_t, C.c_size_t, C.c_size_t]
+        L.or_remove_baseline.argtypes = [_fp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                         C.c_size_t]
+        L.or_baseline_plan.argtypes = [C.c_size_t, C.c_size_t, _szp, _szp, _szp]
+        L.or_exclusive_scan.argtypes = [_fp, C.c_size_t, _fp]
+        L.or_linear_stretch.argtypes = [_fp, C.c_size_t, _fp, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH) and os.path.exists(REF_NOCLEAN_PATH)
+
+
+def ref_lib(clean: bool = True):
+    path = REF_PATH if clean else REF_NOCLEAN_PATH
+    if path not in _ref:
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                "reference build missing: run `make -C oracle ref` where the reference "
+                "sources are present")
+        R = C.CDLL(path)
+        R.ref_execute.restype = C.c_int
+        R.ref_execute.argtypes = [C.POINTER(OrParams), C.c_void_p, C.c_size_t, C.c_size_t,
+                                  C.c_size_t, C.c_size_t, C.c_char_p, _szp,
+                                  C.POINTER(C.c_double), C.c_int]
+        _ref[path] = R
+    return _ref[path]
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
+
+
+def make_params(**kw) -> OrParams:
+    d = dict(DEFAULTS)
+    d.update(kw)
+    p = OrParams()
+    for name, _ in OrParams._fields_:
+        if name in ("channel_zaps", "num_channel_zaps"):
+            continue
+        setattr(p, name, d[name])
+    zaps = np.asarray(d.get("channel_zaps") or [], dtype=np.uintp).reshape(-1)
+    p._zaps = np.ascontiguousarray(zaps, dtype=np.uint64)
+    p.num_channel_zaps = len(zaps) // 2
+    p.channel_zaps = p._zaps.ctypes.data_as(_szp) if len(zaps) else None
+    return p
+
+
+# ---------------------------------------------------------------- stages
+def dm_list(dm_start, dm_end, dt, ti, f0, df, nchans, tol) -> np.ndarray:
+    L = lib()
+    n = L.or_generate_dm_list(dm_start, dm_end, dt, ti, f0, df, nchans, tol, None, 0)
+    out = np.zeros(n, np.float32)
+    L.or_generate_dm_list(dm_start, dm_end, dt, ti, f0, df, nchans, tol, _fptr(out), n)
+    return out
+
+
+def delay_table(nchans, dt, f0, df) -> np.ndarray:
+    out = np.zeros(nchans, np.float32)
+    lib().or_delay_table(nchans, dt, f0, df, _fptr(out))
+    return out
+
+
+def delays(dms: np.ndarray, table: np.ndarray) -> np.ndarray:
+    """delay(d, c) = (size_t)(dm * table[c] + 0.5f), float arithmetic."""
+    v = np.float32(dms)[:, None] * np.float32(table)[None, :] + np.float32(0.5)
+    return np.where(v > 0, v, 0).astype(np.uint64)
+
+
+def dedisperse(fb: np.ndarray, dms: np.ndarray, table: np.ndarray,
+               killmask: Optional[np.ndarray] = None, nthreads: int = 0) -> np.ndarray:
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    dms = np.ascontiguousarray(dms, np.float32)
+    table = np.ascontiguousarray(table, np.float32)
+    km = np.ones(nchans, np.int32) if killmask is None else np.ascontiguousarray(killmask, np.int32)
+    md = lib().or_max_delay(_fptr(dms), len(dms), _fptr(table), nchans)
+    nout = nsamps - md
+    out = np.zeros((len(dms), nout), np.float32)
+    lib().or_dedisperse(fb.ctypes.data, nsamps, nchans, nchans, km.ctypes.data, _fptr(dms),
+                        len(dms), _fptr(table), _fptr(out), nout, nthreads)
+    return out
+
+
+def median(*v) -> float:
+    L = lib()
+    return {3: L.or_median3, 4: L.or_median4, 5: L.or_median5}[len(v)](*[float(x) for x in v])
+
+
+def clean_filterbank(fb: np.ndarray, dt: float, baseline_length=2.0, rfi_tol=5.0,
+                     nbeams: int = 1, boxcar_max: int = 64):
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    out = np.zeros_like(fb)
+    mask = np.zeros(nsamps, np.int32)
+    rc = lib().or_clean_filterbank_rfi(fb.ctypes.data, nsamps, 8, nchans, dt, baseline_length,
+                                       rfi_tol, boxcar_max, nbeams, out.ctypes.data,
+                                       mask.ctypes.data)
+    if rc != 0:
+        raise ValueError("resample radius not below nsamps")
+    return out, mask
+
+
+# ---------------------------------------------------------------- chain
+def _giants_to_dict(g: OrGiants) -> Dict[str, np.ndarray]:
+    n = g.count
+
+    def arr(p, dt):
+        if n == 0:
+            return np.zeros(0, dt)
+        return np.ctypeslib.as_array(p, shape=(n,)).astype(dt).copy()
+    return dict(peaks=arr(g.peaks, np.float32), inds=arr(g.inds, np.uint64),
+                begins=arr(g.begins, np.uint64), ends=arr(g.ends, np.uint64),
+                filter_inds=arr(g.filter_inds, np.uint64), dm_inds=arr(g.dm_inds, np.uint64),
+                members=arr(g.members, np.uint64))
+
+
+def execute(fb: np.ndarray, nbeams: int = 1, first_idx: int = 0, **kw) -> dict:
+    """Whole hd_execute chain on one gulp (STF layout for nbeams > 1)."""
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    p = make_params(nchans=nchans, **kw)
+    res = OrResult()
+    lib().or_hd_execute(C.byref(p), fb.ctypes.data, nsamps, 8, first_idx, nbeams, C.byref(res))
+    out = dict(error=res.error, nsamps_processed=res.nsamps_processed, dm_count=res.dm_count,
+               max_delay=res.max_delay, giants=_giants_to_dict(res.giants),
+               label_count=res.label_count)
+    G = res.giants.count
+    out["labels"] = (np.ctypeslib.as_array(res.labels, shape=(G,)).astype(np.uint64).copy()
+                     if res.labels and G else np.zeros(0, np.uint64))
+    grp = _giants_to_dict(res.groups) if res.labels else _giants_to_dict(OrGiants())
+    L = len(grp["peaks"])
+    grp["dms"] = (np.ctypeslib.as_array(res.group_dms, shape=(L,)).astype(np.float32).copy()
+                  if L else np.zeros(0, np.float32))
+    out["groups"] = grp
+    lib().or_result_free(C.byref(res))
+    return out
+
+
+def cand_lines(groups: dict, nsamps: int, nbeams: int, first_idx: int,
+               nsamps_processed: int, boxcar_max: int, dt: float, beam: int = 0) -> List[str]:
+    """The .cand lines Pipeline/pipeline.cu:1012-1039 writes for these groups."""
+    lines = []
+    nsamps_beam = np.uint32(nsamps // nbeams)
+    nsamps_valid = np.uint32(nsamps_processed // nbeams)
+    dtf = np.float32(dt)
+    for i in range(len(groups["peaks"])):
+        ind = int(groups["inds"][i])
+        beam_idx = int(np.floor(np.float32(ind) / np.float32(nsamps_beam)))
+        beam_start = beam_idx * int(nsamps_beam) + boxcar_max // 2
+        beam_end = beam_start + int(nsamps_valid)
+        if not (beam_start <= ind < beam_end):
+            continue
+        samp_idx = first_idx + (ind - int(nsamps_beam) * beam_idx)
+        peak = np.float32(groups["peaks"][i])
+        snr = 0.0 if np.isinf(peak) else float(peak)
+        t = float(dtf * np.float32(samp_idx))
+        lines.append("%g\t%d\t%g\t%d\t%d\t%g\t%d\t%d\t%d\t%d\t" % (
+            snr, samp_idx, t, int(groups["filter_inds"][i]), int(groups["dm_inds"][i]),
+            float(groups["dms"][i]), int(groups["members"][i]),
+            first_idx + int(groups["begins"][i]) % int(nsamps_beam),
+            first_idx + int(groups["ends"][i]) % int(nsamps_beam), beam + beam_idx + 1))
+    return lines
+
+
+def ref_execute(fb: np.ndarray, nbeams: int = 1, first_idx: int = 0, nthreads: int = 1,
+                **kw):
+    """Runs the reference's own pipeline (the CLEANING build when kw clean=1,
+    the shipped build otherwise); returns (error, nsamps_processed, .cand
+    lines, seconds).  nthreads=1 fixes the order of the reference's racy
+    clustering sweep (Pipeline/label_candidate_clusters.cu:179-195)."""
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    p = make_params(nchans=nchans, **kw)
+    with tempfile.TemporaryDirectory() as d:
+        proc = C.c_size_t(0)
+        secs = C.c_double(0)
+        err = ref_lib(bool(kw.get("clean", 0))).ref_execute(C.byref(p), fb.ctypes.data, nsamps, 8, first_idx, nbeams,
+                                    d.encode(), C.byref(proc), C.byref(secs), nthreads)
+        lines: List[str] = []
+        for f in sorted(glob.glob(os.path.join(d, "*.cand"))):
+            with open(f) as fh:
+                lines += [ln.rstrip("\n") for ln in fh if ln.strip()]
+    return err, proc.value, lines, secs.value
