@@ -1,0 +1,381 @@
+"""heimdall_multibeam_b200 -- Heimdall's per-gulp single-pulse search on B200.
+
+Python face of ``libhdb200.so``, the C library whose interface
+(``include/heimdall_b200.h``, ``include/dedisp.h``) replaces the reference's
+``hd_*`` pipeline API (Pipeline/hd/pipeline.h:10-28) and the ``dedisp_*`` calls
+it makes.  Everything here is a thin ctypes binding: the computation runs in
+the sm_100a kernels of ``csrc/``.  There is no CPU fallback: if the library is
+missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Dict, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhdb200.so")
+
+# ---- error codes (Pipeline/hd/error.h:19-39) ------------------------------
+HD_NO_ERROR = 0
+HD_MEM_ALLOC_FAILED = 1
+HD_MEM_COPY_FAILED = 2
+HD_INVALID_DEVICE_INDEX = 3
+HD_DEVICE_ALREADY_SET = 4
+HD_INVALID_PIPELINE = 5
+HD_INVALID_POINTER = 6
+HD_INVALID_STRIDE = 7
+HD_INVALID_NBITS = 8
+HD_PRIOR_GPU_ERROR = 9
+HD_INTERNAL_GPU_ERROR = 10
+HD_TOO_FEW_NSAMPS = 11
+HD_TOO_MANY_EVENTS = 12
+HD_UNKNOWN_ERROR = 13
+
+DEDISP_NO_ERROR = 0
+DEDISP_DEVICE_POINTERS = 1 << 2
+
+
+class HdError(RuntimeError):
+    def __init__(self, code: int, where: str = ""):
+        self.code = code
+        super().__init__(f"{where}: {error_string(code)} (hd_error {code})")
+
+
+class HdRange(C.Structure):
+    _fields_ = [("start", C.c_size_t), ("end", C.c_size_t)]
+
+
+class HdParams(C.Structure):
+    """struct hd_params (Pipeline/hd/params.h:19-78), built without HAVE_PSRDADA."""
+    _fields_ = [
+        ("verbosity", C.c_int),
+        ("sigproc_file", C.c_char_p),
+        ("yield_cpu", C.c_bool),
+        ("nsamps_gulp", C.c_size_t),
+        ("dm_gulp_size", C.c_size_t),
+        ("baseline_length", C.c_float),
+        ("beam", C.c_size_t),
+        ("nbeams", C.c_size_t),
+        ("override_beam", C.c_bool),
+        ("nchans", C.c_size_t),
+        ("dt", C.c_float),
+        ("f0", C.c_float),
+        ("df", C.c_float),
+        ("dm_min", C.c_float),
+        ("dm_max", C.c_float),
+        ("dm_tol", C.c_float),
+        ("dm_pulse_width", C.c_float),
+        ("dm_nbits", C.c_size_t),
+        ("use_scrunching", C.c_bool),
+        ("scrunch_tol", C.c_float),
+        ("rfi_tol", C.c_float),
+        ("rfi_min_beams", C.c_size_t),
+        ("boxcar_max", C.c_size_t),
+        ("detect_thresh", C.c_float),
+        ("cand_sep_time", C.c_size_t),
+        ("cand_sep_filter", C.c_size_t),
+        ("cand_sep_dm", C.c_size_t),
+        ("cand_rfi_dm_cut", C.c_size_t),
+        ("max_giant_rate", C.c_float),
+        ("min_tscrunch_width", C.c_size_t),
+        ("coincidencer_host", C.c_char_p),
+        ("coincidencer_port", C.c_int),
+        ("num_channel_zaps", C.c_uint),
+        ("channel_zaps", C.POINTER(HdRange)),
+        ("beam_count", C.c_size_t),
+        ("gpu_id", C.c_int),
+        ("utc_start", C.c_long),
+        ("spectra_per_second", C.c_size_t),
+        ("output_dir", C.c_char_p),
+    ]
+
+
+class HdCandidate(C.Structure):
+    _fields_ = [("snr", C.c_float), ("samp_idx", C.c_size_t), ("time", C.c_float),
+                ("filter", C.c_size_t), ("dm_trial", C.c_size_t), ("dm", C.c_float),
+                ("members", C.c_size_t), ("begin", C.c_size_t), ("end", C.c_size_t),
+                ("beam", C.c_size_t)]
+
+
+CANDIDATE_DTYPE = np.dtype([("snr", "<f4"), ("samp_idx", "<u8"), ("time", "<f4"),
+                            ("filter", "<u8"), ("dm_trial", "<u8"), ("dm", "<f4"),
+                            ("members", "<u8"), ("begin", "<u8"), ("end", "<u8"),
+                            ("beam", "<u8")], align=True)
+
+# symbol -> (restype, argtypes); every function include/*.h declares
+_P = C.c_void_p
+_SZ = C.c_size_t
+_SZP = C.POINTER(C.c_size_t)
+_FP = C.POINTER(C.c_float)
+SYMBOLS = {
+    "hd_get_error_string": (C.c_char_p, [C.c_int]),
+    "hd_set_default_params": (None, [C.POINTER(HdParams)]),
+    "hd_parse_command_line": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.POINTER(HdParams)]),
+    "hd_print_usage": (None, []),
+    "hd_create_pipeline": (C.c_int, [C.POINTER(_P), HdParams]),
+    "hd_preallocate": (C.c_int, [_P, _SZ, _SZ]),
+    "hd_get_max_overlap": (_SZ, [_P, _SZ]),
+    "hd_execute": (C.c_int, [_P, _P, _SZ, _SZ, _SZ, _SZ, _SZP]),
+    "hd_destroy_pipeline": (None, [_P]),
+    "hd_clean_filterbank_rfi": (C.c_int, [_P, _P, _SZ, _SZ, _P, _P, C.c_float, C.c_float,
+                                          C.c_float, _SZ, _SZ]),
+    "hd_set_cleaning": (C.c_int, [_P, C.c_int]),
+    "hd_get_candidates": (C.c_int, [_P, _P, _SZP]),
+    "hd_get_giants": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _SZP]),
+    "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
+    "dedisp_create_plan": (C.c_int, [C.POINTER(_P), _SZ, C.c_float, C.c_float, C.c_float]),
+    "dedisp_destroy_plan": (None, [_P]),
+    "dedisp_set_dm_list": (C.c_int, [_P, _FP, _SZ]),
+    "dedisp_generate_dm_list": (C.c_int, [_P, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "dedisp_generate_dm_list_guru": (_FP, [C.c_float, C.c_float, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, _SZ, C.c_double, _SZP]),
+    "dedisp_set_killmask": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "dedisp_enable_adaptive_dt": (C.c_int, [_P, C.c_float, C.c_float]),
+    "dedisp_disable_adaptive_dt": (C.c_int, [_P]),
+    "dedisp_get_dm_count": (_SZ, [_P]),
+    "dedisp_get_dm_list": (_FP, [_P]),
+    "dedisp_get_dt_factors": (_SZP, [_P]),
+    "dedisp_get_max_delay": (_SZ, [_P]),
+    "dedisp_get_dm_delay": (_SZ, [_P, C.c_int]),
+    "dedisp_get_channel_count": (_SZ, [_P]),
+    "dedisp_get_dt": (C.c_float, [_P]),
+    "dedisp_get_f0": (C.c_float, [_P]),
+    "dedisp_get_df": (C.c_float, [_P]),
+    "dedisp_execute_adv": (C.c_int, [_P, _SZ, _P, _SZ, _SZ, _P, _SZ, _SZ, C.c_uint]),
+    "dedisp_execute": (C.c_int, [_P, _SZ, _P, _SZ, _P, _SZ, C.c_uint]),
+    "dedisp_get_error_string": (C.c_char_p, [C.c_int]),
+}
+
+_lib = None
+
+
+def build() -> str:
+    """Compiles libhdb200.so (nvcc, sm_100a) in place."""
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    """Loads libhdb200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              "heimdall_multibeam_b200.build() (there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SYMBOLS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def error_string(code: int) -> str:
+    try:
+        return lib().hd_get_error_string(code).decode()
+    except ImportError:
+        return f"hd_error {code}"
+
+
+def default_params(**overrides) -> HdParams:
+    p = HdParams()
+    lib().hd_set_default_params(C.byref(p))
+    for k, v in overrides.items():
+        if k == "output_dir" or k == "sigproc_file":
+            v = None if v is None else v.encode()
+        setattr(p, k, v)
+    return p
+
+
+def _u8(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    if a.dtype != np.uint8:
+        raise TypeError("filterbank must be uint8")
+    return a
+
+
+class Pipeline:
+    """hd_create_pipeline / hd_execute / hd_destroy_pipeline."""
+
+    def __init__(self, params: Optional[HdParams] = None, cleaning: bool = True,
+                 channel_zaps: Sequence[Tuple[int, int]] = (), **overrides):
+        L = lib()
+        self._p = None
+        if params is None:
+            params = default_params(**overrides)
+        else:
+            for k, v in overrides.items():
+                setattr(params, k, v.encode() if isinstance(v, str) else v)
+        self._zaps = (HdRange * max(len(channel_zaps), 1))()
+        for i, (a, b) in enumerate(channel_zaps):
+            self._zaps[i].start, self._zaps[i].end = a, b
+        if channel_zaps:
+            params.num_channel_zaps = len(channel_zaps)
+            params.channel_zaps = C.cast(self._zaps, C.POINTER(HdRange))
+        self.params = params
+        h = C.c_void_p()
+        err = L.hd_create_pipeline(C.byref(h), params)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_create_pipeline")
+        self._p = h
+        L.hd_set_cleaning(self._p, 1 if cleaning else 0)
+
+    def close(self) -> None:
+        if self._p:
+            lib().hd_destroy_pipeline(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def max_overlap(self, nbeams: int = 1) -> int:
+        return lib().hd_get_max_overlap(self._p, nbeams)
+
+    def execute(self, filterbank: np.ndarray, nbeams: int = 1, first_idx: int = 0,
+                raise_on_error: bool = True) -> Tuple[int, int]:
+        """One gulp; filterbank is (nsamps, nchans) uint8 (STF for nbeams > 1).
+        Returns (hd_error, nsamps_processed); HD_TOO_MANY_EVENTS is soft."""
+        fb = _u8(filterbank)
+        proc = C.c_size_t(0)
+        err = lib().hd_execute(self._p, fb.ctypes.data, fb.shape[0], 8, first_idx, nbeams,
+                               C.byref(proc))
+        if raise_on_error and err not in (HD_NO_ERROR, HD_TOO_MANY_EVENTS):
+            raise HdError(err, "hd_execute")
+        return err, proc.value
+
+    def execute_ptr(self, host_ptr: int, nsamps: int, nbeams: int = 1,
+                    first_idx: int = 0) -> Tuple[int, int]:
+        proc = C.c_size_t(0)
+        err = lib().hd_execute(self._p, C.c_void_p(host_ptr), nsamps, 8, first_idx, nbeams,
+                               C.byref(proc))
+        return err, proc.value
+
+    def candidates(self) -> np.ndarray:
+        n = C.c_size_t(0)
+        lib().hd_get_candidates(self._p, None, C.byref(n))
+        out = np.zeros(n.value, CANDIDATE_DTYPE)
+        if n.value:
+            lib().hd_get_candidates(self._p, out.ctypes.data, C.byref(n))
+        return out
+
+    def giants(self) -> Dict[str, np.ndarray]:
+        n = C.c_size_t(0)
+        lib().hd_get_giants(self._p, None, None, None, None, None, None, None, C.byref(n))
+        g = dict(peaks=np.zeros(n.value, np.float32),
+                 **{k: np.zeros(n.value, np.uint64) for k in
+                    ("inds", "begins", "ends", "filter_inds", "dm_inds", "labels")})
+        if n.value:
+            lib().hd_get_giants(self._p, g["peaks"].ctypes.data, g["inds"].ctypes.data,
+                                g["begins"].ctypes.data, g["ends"].ctypes.data,
+                                g["filter_inds"].ctypes.data, g["dm_inds"].ctypes.data,
+                                g["labels"].ctypes.data, C.byref(n))
+        return g
+
+    def timing(self) -> Dict[str, float]:
+        t = (C.c_float * 8)()
+        lib().hd_get_timing(self._p, t, 8)
+        names = ("total", "clean", "dedisperse", "baseline_scan", "boxcar_threshold",
+                 "giants", "cluster_merge", "h2d")
+        return {n: float(v) for n, v in zip(names, t)}
+
+    def clean_filterbank_rfi(self, filterbank: np.ndarray, dt: float, baseline_length=2.0,
+                             rfi_tol=5.0, boxcar_max=64, nbeams=1):
+        fb = _u8(filterbank)
+        out = np.zeros_like(fb)
+        mask = np.zeros(fb.shape[0], np.int32)
+        err = lib().hd_clean_filterbank_rfi(self._p, fb.ctypes.data, fb.shape[0], 8,
+                                            out.ctypes.data, mask.ctypes.data, dt,
+                                            baseline_length, rfi_tol, boxcar_max, nbeams)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_clean_filterbank_rfi")
+        return out, mask
+
+
+def cand_lines(c: np.ndarray) -> list:
+    """.cand text lines of candidate rows (Pipeline/pipeline.cu:1028-1038)."""
+    return ["%g\t%d\t%g\t%d\t%d\t%g\t%d\t%d\t%d\t%d\t" % (
+        float(r["snr"]), int(r["samp_idx"]), float(r["time"]), int(r["filter"]),
+        int(r["dm_trial"]), float(r["dm"]), int(r["members"]), int(r["begin"]), int(r["end"]),
+        int(r["beam"])) for r in c]
+
+
+class DedispPlan:
+    """dedisp_create_plan / ... / dedisp_execute (include/dedisp.h)."""
+
+    def __init__(self, nchans: int, dt: float, f0: float, df: float):
+        h = C.c_void_p()
+        err = lib().dedisp_create_plan(C.byref(h), nchans, dt, f0, df)
+        if err != DEDISP_NO_ERROR:
+            raise RuntimeError(lib().dedisp_get_error_string(err).decode())
+        self._p = h
+        self.nchans = nchans
+
+    def close(self):
+        if self._p:
+            lib().dedisp_destroy_plan(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, err, what):
+        if err != DEDISP_NO_ERROR:
+            raise RuntimeError(f"{what}: {lib().dedisp_get_error_string(err).decode()}")
+
+    def generate_dm_list(self, dm_min, dm_max, pulse_width=40.0, tol=1.25):
+        self._check(lib().dedisp_generate_dm_list(self._p, dm_min, dm_max, pulse_width, tol),
+                    "dedisp_generate_dm_list")
+
+    def set_dm_list(self, dms):
+        a = np.ascontiguousarray(dms, np.float32)
+        self._check(lib().dedisp_set_dm_list(self._p, a.ctypes.data_as(_FP), len(a)),
+                    "dedisp_set_dm_list")
+
+    def set_killmask(self, km):
+        a = np.ascontiguousarray(km, np.int32)
+        self._check(lib().dedisp_set_killmask(self._p, a.ctypes.data_as(C.POINTER(C.c_int))),
+                    "dedisp_set_killmask")
+
+    @property
+    def dm_list(self) -> np.ndarray:
+        n = lib().dedisp_get_dm_count(self._p)
+        p = lib().dedisp_get_dm_list(self._p)
+        return np.ctypeslib.as_array(p, shape=(n,)).copy() if n else np.zeros(0, np.float32)
+
+    @property
+    def max_delay(self) -> int:
+        return lib().dedisp_get_max_delay(self._p)
+
+    def execute(self, filterbank: np.ndarray) -> np.ndarray:
+        fb = _u8(filterbank)
+        nsamps = fb.shape[0]
+        nout = nsamps - self.max_delay
+        D = lib().dedisp_get_dm_count(self._p)
+        out = np.zeros((D, nout), np.float32)
+        self._check(lib().dedisp_execute(self._p, nsamps, fb.ctypes.data, 8, out.ctypes.data, 32,
+                                         0), "dedisp_execute")
+        return out
+
+
+def dm_list_guru(dm_min, dm_max, dt, pulse_width, f0, df, nchans, tol) -> np.ndarray:
+    n = C.c_size_t(0)
+    p = lib().dedisp_generate_dm_list_guru(dm_min, dm_max, dt, pulse_width, f0, df, nchans, tol,
+                                           C.byref(n))
+    return np.ctypeslib.as_array(p, shape=(n.value,)).copy()

@@ -1,0 +1,177 @@
+// internal.h -- declarations shared by the host pipeline and the kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hdb {
+
+// ---- filterbank kernels (kernels_fb.cu) ------------------------------------
+struct DedispArgs {
+  const uint8_t* in;      // FT rows, channel c at in + c*in_pitch
+  size_t in_pitch;
+  const int* delays;      // [dm_count][nchans] delay in samples
+  const int* blk_min;     // [n_dm_blocks][nchans] min delay over the block's DMs
+  const int* chans;       // active (not killed) channel indices
+  int nact;
+  int nchans;
+  int dm_count;
+  size_t nout;            // output samples per DM
+  float* out;
+  size_t out_pitch;       // floats between DM rows (multiple of 4)
+  int rowb;               // shared-memory row bytes (multiple of 16)
+  unsigned* err;          // device error word (bit 0: staging wait timed out)
+};
+
+int dedisp_dm_block();
+int dedisp_time_block();
+size_t dedisp_smem_bytes(int rowb);
+cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s);
+cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
+                                   size_t pitch, cudaStream_t s);
+cudaError_t launch_dm0_sum(const uint8_t* in, size_t nsamps, int nchans, float* out,
+                           cudaStream_t s);
+cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* mask,
+                       unsigned max_resample_dist, uint8_t* out_ft, size_t pitch,
+                       uint8_t* out_tf, cudaStream_t s);
+
+// ---- series kernels (kernels_search.cu) ------------------------------------
+// A batch of `nser` time series of `len` valid floats each, `pitch` floats
+// apart, every series holding `nbeams` beams of `stride` samples (the last
+// beam truncated by the dispersion delay: beam_count valid samples).
+struct SeriesBatch {
+  float* data;
+  size_t pitch;
+  int nser;
+  size_t len;
+  size_t stride;      // beam stride
+  size_t beam_count;  // valid samples per beam
+  int nbeams;
+};
+
+// Workspace for the median-of-5 trees (two ping-pong arrays).
+struct TreeScratch {
+  float* a;
+  float* b;
+  size_t cap;  // floats in each
+};
+
+// Samples per beam of the scrunched baseline (remove_baseline.cu:38) and the
+// tree scratch (floats per buffer) remove_baseline needs for nseg beams.
+size_t baseline_samples(size_t stride, size_t smooth_radius);
+size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg);
+// RemoveBaselinePlan::exec for every series (Pipeline/remove_baseline.cu:21-160).
+cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
+                            TreeScratch& ws, cudaStream_t s);
+// GetRMSPlanMB::exec_multibeam, vector form (Pipeline/get_rms.cu:236-270):
+// rms[ser*nbeams + b].
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s);
+// normalise_multibeam (get_rms.cu:372-382) fused with the exclusive prefix sum
+// of MatchedFilterPlan::prep (matched_filter.cu:21-32), sequential association:
+// scan[ser][0..len] (len + 1 values, pitch scan_pitch).  norm_out (nullable,
+// same layout as the batch) receives the normalised series.
+cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
+                           size_t scan_pitch, float* norm_out, cudaStream_t s);
+
+// Per-width constants of the boxcar loop (Pipeline/pipeline.cu:657-776).
+struct WidthInfo {
+  int width;          // rel_filter_width
+  int ts;             // rel_tscrunch_width
+  int ahead, behind;  // matched_filter.cu:44-45
+  int filter_idx;
+  unsigned n;         // cur_nsamps_filtered
+  unsigned bn;        // cur_beam_nsamps for the block RMS / giant window
+  unsigned merge_dist;
+  unsigned rel_off;   // rel_cur_filtered_offset
+  int prev_cover;     // index of the latest earlier width whose n covers more
+};
+
+struct WidthCtx {
+  const float* scan;
+  size_t scan_pitch;
+  int nser;
+  size_t stride;
+  int nbeams;
+  int offset;         // rel_boxcar_max / 2
+  int nw;             // widths per series
+  const WidthInfo* winfo;  // device copy
+  float* norm;        // [nser][nw]  1 / block_rms
+  float thresh;
+};
+
+// Block RMS of width wi for every series (get_rms.cu:274-301 on the filtered
+// series) -> ctx.norm[ser][wi].  Widths in [w_begin, w_end) are handled
+// together; widths with ts > 1 must be passed one at a time after all earlier
+// widths (their RMS window reads the earlier widths' normalised output).
+cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* host_winfo, int w_begin, int w_end,
+                      TreeScratch& ws, cudaStream_t s);
+
+// Threshold + ordered compaction of every (series, width) into hit lists.
+struct HitBuffers {
+  unsigned* tile_cnt;   // [nser][nw][ntiles]
+  unsigned* sw_cnt;     // [nser*nw + 1]
+  unsigned* sw_off;     // [nser*nw + 1]
+  unsigned* tile_off;   // [nser][nw][ntiles]
+  unsigned* ind;        // hits
+  float* val;
+  unsigned* sw;
+  size_t cap;
+  unsigned ntiles;
+};
+cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cudaStream_t s);
+cudaError_t scan_hit_counts(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s);
+cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s);
+
+// Device-wide exclusive scan of n unsigned values (out may alias in); the
+// total is written to *total.  tmp needs scan_tmp_words(n) words.
+size_t scan_tmp_words(size_t n);
+cudaError_t scan_u32(const unsigned* in, unsigned* out, size_t n, unsigned* total, unsigned* tmp,
+                     cudaStream_t s);
+
+// Giant list (find_giants.cu + pipeline.cu:755-775).
+struct GiantBuffers {
+  unsigned* head;       // [hits]
+  unsigned* gid;        // [hits]
+  unsigned long long* key;  // [giants]
+  float* peak;
+  unsigned long long* ind;
+  unsigned long long* begin;
+  unsigned long long* end;
+  int* filter;
+  int* dm;
+  int* label;
+  size_t cap;
+};
+cudaError_t giant_heads(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,
+                        GiantBuffers& gb, cudaStream_t s);
+cudaError_t giant_fill(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,
+                       unsigned ngiants, GiantBuffers& gb, cudaStream_t s);
+
+// label_candidate_clusters (Pipeline/label_candidate_clusters.cu:203-394),
+// sequential-sweep semantics; iterates until stable.
+struct ClusterArgs {
+  int ngiants;
+  unsigned long long time_tol, filter_tol, dm_tol, nsamps_beam;
+};
+cudaError_t cluster_init(GiantBuffers& gb, int ngiants, cudaStream_t s);
+cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* changed,
+                          cudaStream_t s);
+
+// merge_candidates (Pipeline/merge_candidates.cu:74-134) + DM gather.
+struct GroupRow {
+  float peak;
+  float dm;
+  unsigned long long ind, begin, end, filter, dm_ind, members;
+};
+cudaError_t merge_groups(const GiantBuffers& gb, int ngiants, const float* dm_list,
+                         unsigned* root_flag, unsigned* root_off, unsigned* nroots,
+                         unsigned* scan_tmp, unsigned long long* gkey, GroupRow* rows,
+                         cudaStream_t s);
+
+// RFI mask of clean_filterbank_rfi (clean_filterbank_rfi.cu:447-506) from the
+// normalised zero-DM series and its prefix sum.
+cudaError_t rfi_mask(const float* x, const float* scan, size_t count, size_t boxcar_max,
+                     float rfi_tol, int* mask, int* fmask, cudaStream_t s);
+
+}  // namespace hdb

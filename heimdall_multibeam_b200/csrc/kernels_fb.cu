@@ -1,0 +1,335 @@
+// kernels_fb.cu -- filterbank-side kernels: layout change, zero-DM series,
+// RFI zapping and brute-force dedispersion.
+//
+// Filterbank layouts:
+//   TF  (input, as the reference receives it): spectrum t at in + t*nchans,
+//       one byte per channel (8-bit data).
+//   FT  (device working copy): channel c at ft + c*pitch, one byte per sample,
+//       pitch a multiple of 64 bytes with zero padding past nsamps so the
+//       dedispersion tiles can be fetched with 16-byte-aligned bulk copies.
+#include "common.cuh"
+#include "internal.h"
+
+namespace hdb {
+
+// ---------------------------------------------------------------------------
+// TF -> FT byte transpose, 128 x 128 tiles through shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_transpose_tf_ft(const uint8_t* __restrict__ in,
+                                                         size_t nsamps, int nchans,
+                                                         uint8_t* __restrict__ out,
+                                                         size_t pitch) {
+  __shared__ uint32_t tile[128][33];  // [t][channel word], +1 word against conflicts
+  const size_t t0 = (size_t)blockIdx.x * 128;
+  const int c0 = blockIdx.y * 128;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwords = nchans >> 2;
+  for (int r = warp; r < 128; r += 8) {
+    size_t t = t0 + r;
+    int w = (c0 >> 2) + lane;
+    uint32_t v = 0;
+    if (t < nsamps && w < nwords) v = reinterpret_cast<const uint32_t*>(in + t * nchans)[w];
+    tile[r][lane] = v;
+  }
+  __syncthreads();
+  // each warp writes 16 channel rows; lane l writes samples 4l..4l+3 as a word
+  for (int cr = warp; cr < 128; cr += 8) {
+    int c = c0 + cr;
+    if (c >= nchans) break;
+    int wsel = cr >> 2, bsel = cr & 3;
+    uint32_t o = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      uint32_t v = tile[4 * lane + j][wsel];
+      o |= ((v >> (8 * bsel)) & 0xFFu) << (8 * j);
+    }
+    size_t t = t0 + 4 * lane;
+    if (t < nsamps) reinterpret_cast<uint32_t*>(out + (size_t)c * pitch + t)[0] = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Zero-DM series: s[t] = (float) sum_c in[t][c]  (dedisp at DM 0, all channels;
+// Pipeline/clean_filterbank_rfi.cu:361-397).  One warp per spectrum.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_dm0_sum(const uint8_t* __restrict__ in, size_t nsamps,
+                                                 int nchans, float* __restrict__ s) {
+  size_t t = (size_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (t >= nsamps) return;
+  const uint32_t* row = reinterpret_cast<const uint32_t*>(in + t * nchans);
+  unsigned acc = 0;
+  for (int w = lane; w < (nchans >> 2); w += 32) acc = __dp4a(row[w], 0x01010101u, acc);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) s[t] = (float)(int)acc;
+}
+
+// ---------------------------------------------------------------------------
+// Broadband zapping (Pipeline/clean_filterbank_rfi.cu:33-113,197-234).
+// ---------------------------------------------------------------------------
+// Robert Jenkins' 32-bit integer mix.
+__device__ __forceinline__ uint32_t mix32(uint32_t a) {
+  a = (a + 0x7ed55d16u) + (a << 12);
+  a = (a ^ 0xc761c23cu) ^ (a >> 19);
+  a = (a + 0x165667b1u) + (a << 5);
+  a = (a + 0xd3a2646cu) ^ (a << 9);
+  a = (a + 0xfd7046c5u) + (a << 3);
+  a = (a ^ 0xb55a4f09u) ^ (a >> 16);
+  return a;
+}
+
+// Park-Miller minimal standard (a = 48271, m = 2^31 - 1) and Thrust's integer
+// distribution: a double in [lo, hi + 1) from (x - 1) / (2^31 - 2), truncated.
+__device__ __forceinline__ uint32_t minstd_next(uint32_t& s) {
+  s = (uint32_t)((48271ull * (unsigned long long)s) % 2147483647ull);
+  return s;
+}
+__device__ __forceinline__ uint32_t uniform_uint(uint32_t& s, uint32_t lo, uint32_t hi) {
+  double a = (double)lo;
+  double b = __dadd_rn((double)hi, 1.0);
+  double u = (double)(minstd_next(s) - 1u);
+  u = __ddiv_rn(u, 2147483646.0);
+  double r = __dadd_rn(__dmul_rn(u, __dsub_rn(b, a)), a);
+  return __double2uint_rz(r);
+}
+
+__device__ uint32_t zap_word(const uint32_t* __restrict__ win, const int* __restrict__ mask,
+                             unsigned i, unsigned t, unsigned c, unsigned stride, unsigned ns,
+                             unsigned r) {
+  uint32_t s = mix32(i) % 2147483647u;
+  if (s == 0) s = 1;
+  uint32_t result = 0;
+#pragma unroll 1
+  for (unsigned k = 0; k < 32; k += 8) {
+    unsigned min_t = t > r ? t - r : 0;
+    unsigned max_t = t < ns - 1 - r ? t + r : ns - 1;
+    unsigned nt = uniform_uint(s, min_t, max_t);
+    int attempts = 0;
+    while (mask[nt] && ++attempts < 11) nt = uniform_uint(s, min_t, max_t);
+    uint32_t v = (win[nt * stride + c] >> k) & 0xFFu;
+    result |= v << k;
+  }
+  return result;
+}
+
+// Zap masked spectra and write the result channel-major (FT), and optionally
+// time-major (TF) for callers that want the cleaned filterbank back.
+__global__ void __launch_bounds__(256) k_zap_to_ft(const uint8_t* __restrict__ in, size_t nsamps,
+                                                   int nchans, const int* __restrict__ mask,
+                                                   unsigned max_resample_dist,
+                                                   uint8_t* __restrict__ out_ft, size_t pitch,
+                                                   uint8_t* __restrict__ out_tf) {
+  __shared__ uint32_t tile[128][33];
+  const size_t t0 = (size_t)blockIdx.x * 128;
+  const int c0 = blockIdx.y * 128;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned stride = (unsigned)(nchans >> 2);
+  const uint32_t* win = reinterpret_cast<const uint32_t*>(in);
+  for (int r = warp; r < 128; r += 8) {
+    size_t t = t0 + r;
+    unsigned w = (unsigned)(c0 >> 2) + lane;
+    uint32_t v = 0;
+    if (t < nsamps && w < stride) {
+      if (mask[t]) {
+        unsigned i = (unsigned)t * stride + w;
+        v = zap_word(win, mask, i, (unsigned)t, w, stride, (unsigned)nsamps, max_resample_dist);
+      } else {
+        v = win[t * stride + w];
+      }
+      if (out_tf) reinterpret_cast<uint32_t*>(out_tf)[t * stride + w] = v;
+    }
+    tile[r][lane] = v;
+  }
+  if (!out_ft) return;
+  __syncthreads();
+  for (int cr = warp; cr < 128; cr += 8) {
+    int c = c0 + cr;
+    if (c >= nchans) break;
+    int wsel = cr >> 2, bsel = cr & 3;
+    uint32_t o = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      uint32_t v = tile[4 * lane + j][wsel];
+      o |= ((v >> (8 * bsel)) & 0xFFu) << (8 * j);
+    }
+    size_t t = t0 + 4 * lane;
+    if (t < nsamps) reinterpret_cast<uint32_t*>(out_ft + (size_t)c * pitch + t)[0] = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Brute-force dedispersion.
+//
+//   out[d][t] = (float) sum_{c active} in[c][t + delay[d][c]],  t < nout
+//
+// CTA = DB = 2*NW DMs x TB = 128*G samples.  For each stage of CH channels,
+// one thread issues 1-D bulk async copies (TMA, cp.async.bulk) of each channel
+// row segment [t0 + min_d delay - align, +rowb) into shared memory; the copy of
+// stage s+1 overlaps the sums of stage s (double buffer, mbarrier completion).
+// Warp w owns DMs 2w and 2w+1; lane l owns samples 4(l + 32g) .. +3.  Each
+// 4-byte window is realigned with a funnel shift and split into two 16-bit
+// lane pairs (even/odd samples) so one integer add accumulates two samples;
+// the 16-bit lanes are drained into 32-bit sums every 256 channels (255*256 <
+// 65536), so the sums are exact.
+// ---------------------------------------------------------------------------
+template <int NW, int G, int CH>
+__global__ void __launch_bounds__(NW * 32) k_dedisp(DedispArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  uint8_t* rows = smem + 128;
+  constexpr int DB = 2 * NW;
+  constexpr int TB = 128 * G;
+  const int dblk = blockIdx.x;
+  const size_t t0 = (size_t)blockIdx.y * TB;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int d_lo = dblk * DB;
+  int dm[2];
+  dm[0] = min(d_lo + 2 * warp, a.dm_count - 1);
+  dm[1] = min(d_lo + 2 * warp + 1, a.dm_count - 1);
+  const int* __restrict__ bmin = a.blk_min + (size_t)dblk * a.nchans;
+  const int nstage = (a.nact + CH - 1) / CH;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  auto issue = [&](int st) {
+    int buf = st & 1;
+    int k0 = st * CH;
+    int nk = min(CH, a.nact - k0);
+    mbar_expect_tx(&bar[buf], (uint32_t)(nk * a.rowb));
+    for (int k = 0; k < nk; k++) {
+      int c = a.chans[k0 + k];
+      size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
+      bulk_g2s(rows + (size_t)(buf * CH + k) * a.rowb, a.in + (size_t)c * a.in_pitch + lo,
+               (uint32_t)a.rowb, &bar[buf]);
+    }
+  };
+
+  uint32_t pk[2][G][2];
+  int acc[2][G][4];
+#pragma unroll
+  for (int d = 0; d < 2; d++)
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      pk[d][g][0] = pk[d][g][1] = 0;
+      acc[d][g][0] = acc[d][g][1] = acc[d][g][2] = acc[d][g][3] = 0;
+    }
+  auto drain = [&]() {
+#pragma unroll
+    for (int d = 0; d < 2; d++)
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        acc[d][g][0] += (int)(pk[d][g][0] & 0xFFFFu);
+        acc[d][g][2] += (int)(pk[d][g][0] >> 16);
+        acc[d][g][1] += (int)(pk[d][g][1] & 0xFFFFu);
+        acc[d][g][3] += (int)(pk[d][g][1] >> 16);
+        pk[d][g][0] = pk[d][g][1] = 0;
+      }
+  };
+
+  if (threadIdx.x == 0) issue(0);
+  int nsum = 0;
+  for (int st = 0; st < nstage; st++) {
+    if (threadIdx.x == 0 && st + 1 < nstage) issue(st + 1);
+    bool ok = mbar_wait(&bar[st & 1], (uint32_t)((st >> 1) & 1), 1u << 24);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(a.err, 1u);
+      return;
+    }
+    const int k0 = st * CH;
+    const int nk = min(CH, a.nact - k0);
+    for (int k = 0; k < nk; k++) {
+      const int c = a.chans[k0 + k];
+      const uint32_t* rw =
+          reinterpret_cast<const uint32_t*>(rows + (size_t)((st & 1) * CH + k) * a.rowb);
+      const size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
+#pragma unroll
+      for (int d = 0; d < 2; d++) {
+        const int off = (int)(t0 + (size_t)a.delays[(size_t)dm[d] * a.nchans + c] - lo);
+        const int sh = (off & 3) * 8;
+        const int wb = (off >> 2) + lane;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          uint32_t x = __funnelshift_r(rw[wb + 32 * g], rw[wb + 32 * g + 1], sh);
+          pk[d][g][0] += x & 0x00FF00FFu;
+          pk[d][g][1] += __byte_perm(x, 0u, 0x4341);
+        }
+      }
+      if (++nsum == 256) { drain(); nsum = 0; }
+    }
+    __syncthreads();
+  }
+  drain();
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    int dd = d_lo + 2 * warp + d;
+    if (dd >= a.dm_count) continue;
+    float* o = a.out + (size_t)dd * a.out_pitch;
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      size_t t = t0 + 4 * (lane + 32 * g);
+      float4 v = make_float4((float)acc[d][g][0], (float)acc[d][g][1], (float)acc[d][g][2],
+                             (float)acc[d][g][3]);
+      if (t + 3 < a.nout) {
+        *reinterpret_cast<float4*>(o + t) = v;
+      } else {
+        if (t < a.nout) o[t] = v.x;
+        if (t + 1 < a.nout) o[t + 1] = v.y;
+        if (t + 2 < a.nout) o[t + 2] = v.z;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
+                                   size_t pitch, cudaStream_t s) {
+  dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128));
+  k_transpose_tf_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, out, pitch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dm0_sum(const uint8_t* in, size_t nsamps, int nchans, float* out,
+                           cudaStream_t s) {
+  k_dm0_sum<<<(unsigned)((nsamps + 7) / 8), 256, 0, s>>>(in, nsamps, nchans, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* mask,
+                       unsigned max_resample_dist, uint8_t* out_ft, size_t pitch,
+                       uint8_t* out_tf, cudaStream_t s) {
+  dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128));
+  k_zap_to_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, mask, max_resample_dist, out_ft, pitch,
+                                   out_tf);
+  return cudaGetLastError();
+}
+
+namespace {
+constexpr int DD_NW = 8, DD_G = 4, DD_CH = 8;
+}
+
+int dedisp_dm_block() { return 2 * DD_NW; }
+int dedisp_time_block() { return 128 * DD_G; }
+
+size_t dedisp_smem_bytes(int rowb) { return 128 + (size_t)2 * DD_CH * rowb; }
+
+cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s) {
+  auto kern = k_dedisp<DD_NW, DD_G, DD_CH>;
+  size_t smem = dedisp_smem_bytes(a.rowb);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const int DB = 2 * DD_NW, TB = 128 * DD_G;
+  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB));
+  kern<<<grid, DD_NW * 32, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace hdb

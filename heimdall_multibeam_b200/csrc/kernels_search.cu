@@ -1,0 +1,989 @@
+// kernels_search.cu -- per-DM-series kernels of the single-pulse search:
+// baseline removal, robust RMS, normalisation + prefix sum, boxcar block RMS,
+// thresholding, giant segmentation, clustering and merging.
+//
+// Every float operation mirrors the cited reference expression (same types,
+// same order; the file is compiled with -fmad=false), so outputs are
+// bit-identical to the reference's stage code.  Where the reference iterates
+// a median-of-5 scrunch level by level through global memory
+// (Pipeline/median_filter.cu:288-395), these kernels evaluate several levels
+// per block in shared memory: level-k value j of a tree depends only on the
+// aligned input block [j*5^k, (j+1)*5^k), and the reference's per-level
+// truncation (size/5) keeps exactly the complete blocks.
+#include "common.cuh"
+#include "internal.h"
+
+namespace hdb {
+
+namespace {
+
+constexpr int TREE_THREADS = 128;
+
+__host__ __device__ inline size_t pow5(int m) {
+  size_t r = 1;
+  for (int i = 0; i < m; i++) r *= 5;
+  return r;
+}
+
+// Level-m median of the 5^m source values src(0 .. 5^m-1) (m >= 1).  Result
+// valid in every thread after the call.  sm needs 5^(m-1) + 5^(m-2) floats.
+template <class F>
+__device__ float block_tree(F src, int m, float* sm) {
+  const int tid = threadIdx.x;
+  int n = (int)pow5(m - 1);
+  float* cur = sm;
+  float* nxt = sm + n;
+  for (int k = tid; k < n; k += blockDim.x)
+    cur[k] = med5(src(5 * k), src(5 * k + 1), src(5 * k + 2), src(5 * k + 3), src(5 * k + 4));
+  __syncthreads();
+  for (int lev = 2; lev <= m; lev++) {
+    n /= 5;
+    for (int k = tid; k < n; k += blockDim.x)
+      nxt[k] = med5(cur[5 * k], cur[5 * k + 1], cur[5 * k + 2], cur[5 * k + 3], cur[5 * k + 4]);
+    __syncthreads();
+    float* t = cur; cur = nxt; nxt = t;
+  }
+  float r = cur[0];
+  __syncthreads();
+  return r;
+}
+
+// Number of median-of-5 levels the reference performs on `count` values
+// before the remainder is <= 4, and that remainder.
+inline void tree_levels(size_t count, int* levels, size_t* rem) {
+  int l = 0;
+  size_t s = count;
+  while (s > 4) { s /= 5; l++; }
+  *levels = l;
+  *rem = s;
+}
+
+// Final step of a tree: count (1..4) values -> one value, the reference's
+// special cases (median_filter.cu:217-235 and 295-311).
+__device__ __forceinline__ float tree_tail(const float* v, size_t count) {
+  if (count <= 1) return v[0];
+  if (count == 2) return __fmul_rn(0.5f, __fadd_rn(v[0], v[1]));
+  if (count == 3) return med3(v[0], v[1], v[2]);
+  return med4(v[0], v[1], v[2], v[3]);
+}
+
+// ---- generic level pass over an array: in[seg][n_in] -> out[seg][n_in/5^m]
+__global__ void k_tree_array(const float* __restrict__ in, size_t in_pitch, int m,
+                             float* __restrict__ out, size_t out_pitch) {
+  __shared__ float sm[625 + 125];
+  const size_t seg = blockIdx.y + (size_t)blockIdx.z * gridDim.y;
+  const size_t g = blockIdx.x;
+  const float* p = in + seg * in_pitch + g * pow5(m);
+  float r = block_tree([&](int i) { return p[i]; }, m, sm);
+  if (threadIdx.x == 0) out[seg * out_pitch + g] = r;
+}
+
+// Runs the remaining tree levels of `nseg` segments held in `cur` (pitch
+// cur_pitch, `count` values each) down to <= 4 values per segment, using the
+// scratch ping-pong buffers.  Returns the array holding the last level.
+cudaError_t tree_reduce_array(float* cur, size_t cur_pitch, size_t count, size_t nseg,
+                              TreeScratch& ws, cudaStream_t s, float** out, size_t* out_pitch,
+                              size_t* out_count) {
+  int levels;
+  size_t rem;
+  tree_levels(count, &levels, &rem);
+  float* bufs[2] = {ws.a, ws.b};
+  int which = (cur == ws.a) ? 1 : 0;
+  while (levels > 0) {
+    int m = levels < 5 ? levels : 5;
+    size_t ng = count / pow5(m);
+    float* dst = bufs[which];
+    if (ng * nseg > ws.cap) return cudaErrorMemoryAllocation;
+    dim3 grid((unsigned)ng, (unsigned)(nseg > 65535 ? 65535 : nseg),
+              (unsigned)((nseg + 65534) / 65535));
+    if (nseg > 65535) {
+      // segments are laid out contiguously: fold into y*z with exact division
+      size_t y = 1;
+      for (size_t c = 65535; c >= 1; c--) if (nseg % c == 0) { y = c; break; }
+      grid.y = (unsigned)y;
+      grid.z = (unsigned)(nseg / y);
+    }
+    k_tree_array<<<grid, TREE_THREADS, 0, s>>>(cur, cur_pitch, m, dst, ng);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    cur = dst;
+    cur_pitch = ng;
+    count = ng;
+    levels -= m;
+    which ^= 1;
+  }
+  *out = cur;
+  *out_pitch = cur_pitch;
+  *out_count = count;
+  return cudaSuccess;
+}
+
+inline dim3 seg_grid(size_t ng, size_t nseg_y, size_t nseg_z) {
+  return dim3((unsigned)ng, (unsigned)nseg_y, (unsigned)nseg_z);
+}
+
+}  // namespace
+
+// ===========================================================================
+// Baseline removal (Pipeline/remove_baseline.cu:21-102)
+// ===========================================================================
+struct BaselinePlan {
+  size_t sample_count, nscrunches, count_round;
+};
+
+static BaselinePlan baseline_plan(size_t beam_stride, size_t smooth_radius) {
+  // remove_baseline.cu:36-46, same float/double arithmetic
+  BaselinePlan p{0, 0, 0};
+  if (smooth_radius == 0) return p;
+  float oversample = 2;
+  float q = oversample * (float)beam_stride / (float)(2 * smooth_radius);
+  size_t sc = (size_t)((double)q + 0.5);
+  p.sample_count = sc;
+  if (sc == 0) return p;
+  p.nscrunches = (size_t)(log((double)(beam_stride / sc)) / log(5.));
+  p.count_round = (size_t)(pow(5., (double)p.nscrunches) * (double)sc);
+  return p;
+}
+
+// Stretch of every beam to count_round samples followed by m median levels.
+__global__ void k_baseline_down(const float* __restrict__ data, size_t pitch, int nbeams,
+                                size_t stride, size_t beam_count, size_t cr, int m,
+                                float step_b, float step_last, float* __restrict__ out,
+                                size_t out_pitch_beam) {
+  __shared__ float sm[625 + 125];
+  const int b = blockIdx.y;
+  const size_t ser = blockIdx.z;
+  const size_t g = blockIdx.x;
+  const float* d = data + ser * pitch;
+  const size_t base_i = g * pow5(m);
+  float r;
+  if (b < nbeams - 1) {
+    const unsigned gi0 = (unsigned)((size_t)b * cr + base_i);
+    r = block_tree([&](int i) { return stretch_beam_at(d, gi0 + (unsigned)i, step_b,
+                                                       (unsigned long long)b); }, m, sm);
+  } else {
+    const float* dl = d + (size_t)(nbeams - 1) * stride;
+    r = block_tree([&](int i) { return stretch_at(dl, (unsigned)(base_i + i), step_last); },
+                   m, sm);
+  }
+  if (threadIdx.x == 0) out[(ser * nbeams + b) * out_pitch_beam + g] = r;
+}
+
+__global__ void k_baseline_stretch0(const float* __restrict__ data, size_t pitch, int nbeams,
+                                    size_t stride, size_t cr, float step_b, float step_last,
+                                    float* __restrict__ out) {
+  const int b = blockIdx.y;
+  const size_t ser = blockIdx.z;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cr) return;
+  const float* d = data + ser * pitch;
+  float v = (b < nbeams - 1)
+                ? stretch_beam_at(d, (unsigned)((size_t)b * cr + i), step_b, (unsigned long long)b)
+                : stretch_at(d + (size_t)(nbeams - 1) * stride, (unsigned)i, step_last);
+  out[(ser * nbeams + b) * cr + i] = v;
+}
+
+// data[i] -= stretched baseline, i < nbeams*stride - dm_delay
+__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, int nbeams, size_t stride,
+                               size_t beam_count, size_t nsub, const float* __restrict__ base,
+                               size_t sc, float step2, float step3) {
+  const size_t ser = blockIdx.y;
+  float* d = data + ser * pitch;
+  const float* bs = base + ser * (size_t)nbeams * sc;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nsub;
+       i += (size_t)gridDim.x * blockDim.x) {
+    size_t b = i / stride;
+    float v;
+    if ((int)b < nbeams - 1) {
+      v = stretch_beam_at(bs, (unsigned)i, step2, (unsigned long long)b);
+    } else {
+      size_t t = i - (size_t)(nbeams - 1) * stride;
+      v = stretch_at(bs + (size_t)(nbeams - 1) * sc, (unsigned)t, step3);
+    }
+    d[i] = __fsub_rn(d[i], v);
+  }
+}
+
+size_t baseline_samples(size_t stride, size_t smooth_radius) {
+  return baseline_plan(stride, smooth_radius).sample_count;
+}
+
+size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg) {
+  BaselinePlan p = baseline_plan(stride, smooth_radius);
+  size_t m1 = p.nscrunches < 5 ? p.nscrunches : 5;
+  size_t ng1 = p.count_round / pow5((int)m1);
+  return nseg * (ng1 + 8) + 64;
+}
+
+cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
+                            TreeScratch& ws, cudaStream_t s) {
+  BaselinePlan p = baseline_plan(sb.stride, smooth_radius);
+  if (p.sample_count == 0) return cudaSuccess;
+  const size_t sc = p.sample_count, cr = p.count_round;
+  const int k = (int)p.nscrunches;
+  const float step_b = (float)(sb.stride - 1) / (float)cr;            // median_filter.cu:490
+  const float step_last = (float)(sb.beam_count - 1) / (float)(cr - 1);  // median_filter.cu:457
+  const size_t nseg = (size_t)sb.nser * sb.nbeams;
+  float* lev_out;
+  int m1 = k < 5 ? k : 5;
+  size_t ng1 = cr / pow5(m1);
+  if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
+  if (k == 0) {
+    // no scrunch levels: the baseline samples are the stretched values
+    k_baseline_stretch0<<<dim3((unsigned)((cr + 127) / 128), sb.nbeams, sb.nser), 128, 0, s>>>(
+        sb.data, sb.pitch, sb.nbeams, sb.stride, cr, step_b, step_last, ws.a);
+  } else {
+    k_baseline_down<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
+        sb.data, sb.pitch, sb.nbeams, sb.stride, sb.beam_count, cr, m1, step_b, step_last, ws.a,
+        ng1);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  float* cur = ws.a;
+  size_t cur_pitch = ng1, count = ng1;
+  int left = k - m1;
+  float* bufs[2] = {ws.b, ws.a};
+  int w = 0;
+  while (left > 0) {
+    int m = left < 5 ? left : 5;
+    size_t ng = count / pow5(m);
+    float* dst = bufs[w];
+    k_tree_array<<<seg_grid(ng, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(cur, cur_pitch, m,
+                                                                           dst, ng);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cur = dst; cur_pitch = ng; count = ng; left -= m; w ^= 1;
+  }
+  // cur[seg][sc] holds the scrunched baseline samples
+  lev_out = cur;
+  if (cur_pitch != sc) return cudaErrorInvalidValue;
+  e = cudaMemcpyAsync(base_out, lev_out, nseg * sc * sizeof(float), cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return e;
+  const float step2 = (float)(sc - 1) / (float)sb.stride;              // stretch back, beams 0..n-2
+  const float step3 = (float)(sc - 1) / (float)(sb.beam_count - 1);    // last beam
+  const size_t dm_delay = sb.stride - sb.beam_count;
+  const size_t nsub = sb.stride * sb.nbeams - dm_delay;
+  dim3 grid((unsigned)((nsub + 255) / 256 < 4096 ? (nsub + 255) / 256 : 4096), sb.nser);
+  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, sb.nbeams, sb.stride, sb.beam_count,
+                                      nsub, base_out, sc, step2, step3);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Robust RMS per beam (Pipeline/get_rms.cu:236-270, reblock_abs_beam 384-418)
+// ===========================================================================
+__device__ __forceinline__ size_t reblock_index(size_t beam, float delta, unsigned o) {
+  return (size_t)__fadd_rn(__fmul_rn(__ull2float_rn(beam), delta), __uint2float_rn(o));
+}
+
+__global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, int nbeams,
+                                  size_t beam_count, float delta, int m,
+                                  float* __restrict__ out, size_t out_pitch_beam) {
+  __shared__ float sm[625 + 125];
+  const int b = blockIdx.y;
+  const size_t ser = blockIdx.z;
+  const size_t g = blockIdx.x;
+  const float* d = data + ser * pitch;
+  const size_t o0 = (size_t)b * beam_count + g * pow5(m);
+  float r = block_tree([&](int i) {
+    unsigned o = (unsigned)(o0 + i);
+    return fabsf(d[reblock_index((size_t)b, delta, o)]);
+  }, m, sm);
+  if (threadIdx.x == 0) out[(ser * nbeams + b) * out_pitch_beam + g] = r;
+}
+
+__global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitch, size_t count,
+                                  int nseg, const float* __restrict__ data, size_t pitch,
+                                  int nbeams, size_t beam_count, float delta, int from_data,
+                                  float* __restrict__ rms) {
+  int seg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (seg >= nseg) return;
+  float v[4];
+  if (from_data) {
+    int ser = seg / nbeams, b = seg % nbeams;
+    const float* d = data + (size_t)ser * pitch;
+    for (size_t i = 0; i < count && i < 4; i++)
+      v[i] = fabsf(d[reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i))]);
+  } else {
+    for (size_t i = 0; i < count && i < 4; i++) v[i] = lev[(size_t)seg * lev_pitch + i];
+  }
+  float m = tree_tail(v, count);
+  rms[seg] = __fmul_rn(m, (float)1.4862);  // multiplies<hd_float>(x, 1.4862)
+}
+
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s) {
+  int levels;
+  size_t rem;
+  tree_levels(sb.beam_count, &levels, &rem);
+  const float delta = (float)(sb.stride - sb.beam_count);
+  const size_t nseg = (size_t)sb.nser * sb.nbeams;
+  cudaError_t e;
+  if (levels == 0) {
+    k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
+        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms);
+    return cudaGetLastError();
+  }
+  int m1 = levels < 5 ? levels : 5;
+  size_t ng1 = sb.beam_count / pow5(m1);
+  if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
+  k_rms_beams_pass1<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
+      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  float* fin;
+  size_t fin_pitch, fin_count;
+  e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
+  if (e != cudaSuccess) return e;
+  k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
+      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Normalise + exclusive prefix sum with the sequential association of the
+// reference's scan (Thrust's sequential exclusive_scan: out[0] = 0,
+// out[k+1] = out[k] + in[k]).  One warp per series; every lane runs the same
+// serial chain on broadcast values and keeps the partial sum of its slot, so
+// each output is the exact left-to-right float sum.
+// ===========================================================================
+__global__ void __launch_bounds__(128) k_normalise_scan(const float* __restrict__ data,
+                                                        size_t pitch, int nser, size_t len,
+                                                        size_t stride, int nbeams,
+                                                        const float* __restrict__ rms,
+                                                        float* __restrict__ scan,
+                                                        size_t scan_pitch, float* norm_out) {
+  const int ser = blockIdx.x * 4 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (ser >= nser) return;
+  const float* d = data + (size_t)ser * pitch;
+  const float* r = rms + (size_t)ser * nbeams;
+  float* o = scan + (size_t)ser * scan_pitch;
+  float sum = 0.0f;
+  const size_t n_out = len + 1;
+  float nxt = 0.f;
+  {
+    size_t i = lane;
+    if (i < len) nxt = __fdiv_rn(d[i], r[i / stride]);
+  }
+  for (size_t base = 0; base < n_out; base += 32) {
+    float v = nxt;
+    size_t in2 = base + 32 + lane;
+    nxt = (in2 < len) ? __fdiv_rn(d[in2], r[in2 / stride]) : 0.f;
+    float mine = 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      float vj = __shfl_sync(0xffffffffu, v, j);
+      if (lane == j) mine = sum;
+      sum = __fadd_rn(sum, vj);
+    }
+    size_t i = base + lane;
+    if (i < n_out) o[i] = mine;
+    if (norm_out && i < len) norm_out[(size_t)ser * pitch + i] = v;
+  }
+}
+
+cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
+                           size_t scan_pitch, float* norm_out, cudaStream_t s) {
+  k_normalise_scan<<<(unsigned)((sb.nser + 3) / 4), 128, 0, s>>>(
+      sb.data, sb.pitch, sb.nser, sb.len, sb.stride, sb.nbeams, rms, scan, scan_pitch, norm_out);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Boxcar filter helpers (Pipeline/matched_filter.cu:37-67)
+// ===========================================================================
+__device__ __forceinline__ float boxcar(const float* sc, int offset, const WidthInfo& w,
+                                        size_t i) {
+  size_t p = (size_t)i * (size_t)w.ts;
+  return __fsub_rn(sc[offset + w.ahead + p], sc[offset - w.behind + p]);
+}
+
+// Value the reference's block-RMS window reads at filtered index i for width
+// wi: fresh (unnormalised) output of wi if i < n, otherwise the normalised
+// output of the latest earlier width that wrote index i.
+__device__ __forceinline__ float rms_window_value(const float* sc, int offset,
+                                                  const WidthInfo* winfo, const float* norm,
+                                                  int wi, size_t i) {
+  const WidthInfo& w = winfo[wi];
+  if (i < w.n) return boxcar(sc, offset, w, i);
+  int pw = w.prev_cover;
+  while (pw >= 0 && i >= winfo[pw].n) pw = winfo[pw].prev_cover;
+  if (pw < 0) return 0.f;
+  return __fmul_rn(boxcar(sc, offset, winfo[pw], i), norm[pw]);
+}
+
+// Pass 1 of the block RMS: level-m medians of |window| over aligned groups of
+// the reblocked index q (get_rms.cu:274-301; reblock_abs_beam with a float
+// delta).  Widths [w0, w0 + gridDim.y) of every series.
+__global__ void k_block_rms_pass1(WidthCtx ctx, int w0, int m, float* __restrict__ out,
+                                  size_t out_pitch) {
+  __shared__ float sm[625 + 125];
+  const int wi = w0 + blockIdx.y;
+  const size_t ser = blockIdx.z;
+  const size_t g = blockIdx.x;
+  const WidthInfo& w = ctx.winfo[wi];
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const float* norm = ctx.norm + ser * ctx.nw;
+  const float delta = (float)(ctx.stride - w.bn);
+  const size_t q0 = g * pow5(m);
+  float r = block_tree([&](int k) {
+    unsigned q = (unsigned)(q0 + k);
+    size_t beam = q / w.bn;
+    size_t i = reblock_index(beam, delta, q);
+    return fabsf(rms_window_value(sc, ctx.offset, ctx.winfo, norm, wi, i));
+  }, m, sm);
+  if (threadIdx.x == 0) out[(ser * gridDim.y + blockIdx.y) * out_pitch + g] = r;
+}
+
+__global__ void k_block_rms_final(WidthCtx ctx, int w0, int nwb, const float* __restrict__ lev,
+                                  size_t lev_pitch, size_t count, int from_window) {
+  int seg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (seg >= ctx.nser * nwb) return;
+  int ser = seg / nwb, wl = seg % nwb, wi = w0 + wl;
+  float v[4];
+  if (from_window) {
+    const WidthInfo& w = ctx.winfo[wi];
+    const float* sc = ctx.scan + (size_t)ser * ctx.scan_pitch;
+    const float* norm = ctx.norm + (size_t)ser * ctx.nw;
+    const float delta = (float)(ctx.stride - w.bn);
+    for (size_t k = 0; k < count && k < 4; k++) {
+      size_t beam = (unsigned)k / w.bn;
+      v[k] = fabsf(rms_window_value(sc, ctx.offset, ctx.winfo, norm, wi,
+                                    reblock_index(beam, delta, (unsigned)k)));
+    }
+  } else {
+    for (size_t k = 0; k < count && k < 4; k++) v[k] = lev[(size_t)seg * lev_pitch + k];
+  }
+  float m = tree_tail(v, count);
+  float rms = (float)((double)m * 1.4862);          // get_rms.cu:298
+  ctx.norm[(size_t)ser * ctx.nw + wi] = __fdiv_rn(1.0f, rms);  // get_rms.cu:365
+}
+
+cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end,
+                      TreeScratch& ws, cudaStream_t s) {
+  const int nwb = w_end - w_begin;
+  const size_t cnt = (size_t)ctx.nbeams * hw[w_begin].bn;
+  for (int wi = w_begin; wi < w_end; wi++)
+    if ((size_t)ctx.nbeams * hw[wi].bn != cnt) return cudaErrorInvalidValue;
+  int levels;
+  size_t rem;
+  tree_levels(cnt, &levels, &rem);
+  const size_t nseg = (size_t)ctx.nser * nwb;
+  cudaError_t e;
+  if (levels == 0) {
+    k_block_rms_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(ctx, w_begin, nwb, nullptr,
+                                                                     0, rem, 1);
+    return cudaGetLastError();
+  }
+  int m1 = levels < 5 ? levels : 5;
+  size_t ng1 = cnt / pow5(m1);
+  if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
+  k_block_rms_pass1<<<seg_grid(ng1, nwb, ctx.nser), TREE_THREADS, 0, s>>>(ctx, w_begin, m1,
+                                                                         ws.a, ng1);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  float* fin;
+  size_t fin_pitch, fin_count;
+  e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
+  if (e != cudaSuccess) return e;
+  k_block_rms_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(ctx, w_begin, nwb, fin,
+                                                                   fin_pitch, fin_count, 0);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Thresholding (find_giants.cu:47-60,137-183): hits are filtered indices i
+// with (i % beam_stride) < bn and normalised value > thresh.
+// ===========================================================================
+constexpr int HIT_TILE = 2048;
+constexpr int HIT_THREADS = 256;
+constexpr int HIT_PER_THREAD = HIT_TILE / HIT_THREADS;
+
+__device__ __forceinline__ bool hit_at(const WidthCtx& ctx, const float* sc, float norm,
+                                       const WidthInfo& w, size_t i, float* val) {
+  if (i >= w.n) return false;
+  if ((i % ctx.stride) >= w.bn) return false;
+  float v = __fmul_rn(boxcar(sc, ctx.offset, w, i), norm);
+  *val = v;
+  return v > ctx.thresh;
+}
+
+__global__ void __launch_bounds__(HIT_THREADS) k_count_hits(WidthCtx ctx, HitBuffers hb) {
+  const int wi = blockIdx.y;
+  const size_t ser = blockIdx.z;
+  const unsigned tile = blockIdx.x;
+  const WidthInfo& w = ctx.winfo[wi];
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const float norm = ctx.norm[ser * ctx.nw + wi];
+  const size_t i0 = (size_t)tile * HIT_TILE + (size_t)threadIdx.x * HIT_PER_THREAD;
+  unsigned c = 0;
+  float v;
+  if (i0 < w.n) {
+#pragma unroll
+    for (int k = 0; k < HIT_PER_THREAD; k++) c += hit_at(ctx, sc, norm, w, i0 + k, &v);
+  }
+  __shared__ unsigned red[HIT_THREADS / 32];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = 0;
+    for (int k = 0; k < HIT_THREADS / 32; k++) t += red[k];
+    size_t sw = ser * ctx.nw + wi;
+    hb.tile_cnt[sw * hb.ntiles + tile] = t;
+    if (t) atomicAdd(&hb.sw_cnt[sw], t);
+  }
+}
+
+// exclusive scan of each (series, width)'s tile counts, one warp per row
+__global__ void k_scan_tiles(const unsigned* __restrict__ cnt, unsigned* __restrict__ off,
+                             unsigned ntiles, size_t nrows) {
+  size_t row = (size_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  const unsigned* c = cnt + row * ntiles;
+  unsigned* o = off + row * ntiles;
+  unsigned carry = 0;
+  for (unsigned b = 0; b < ntiles; b += 32) {
+    unsigned v = (b + lane < ntiles) ? c[b + lane] : 0u;
+    unsigned x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      unsigned y = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= d) x += y;
+    }
+    if (b + lane < ntiles) o[b + lane] = carry + x - v;
+    carry += __shfl_sync(0xffffffffu, x, 31);
+  }
+}
+
+__global__ void __launch_bounds__(HIT_THREADS) k_write_hits(WidthCtx ctx, HitBuffers hb) {
+  const int wi = blockIdx.y;
+  const size_t ser = blockIdx.z;
+  const unsigned tile = blockIdx.x;
+  const size_t sw = ser * ctx.nw + wi;
+  if (hb.tile_cnt[sw * hb.ntiles + tile] == 0) return;
+  const WidthInfo& w = ctx.winfo[wi];
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const float norm = ctx.norm[sw];
+  const size_t i0 = (size_t)tile * HIT_TILE + (size_t)threadIdx.x * HIT_PER_THREAD;
+  unsigned flags = 0;
+  float vals[HIT_PER_THREAD];
+#pragma unroll
+  for (int k = 0; k < HIT_PER_THREAD; k++) {
+    vals[k] = 0.f;
+    if (hit_at(ctx, sc, norm, w, i0 + k, &vals[k])) flags |= 1u << k;
+  }
+  unsigned c = __popc(flags);
+  // block exclusive scan of c
+  __shared__ unsigned wsum[HIT_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned x = c;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    unsigned y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  unsigned wpre = 0;
+  for (int k = 0; k < warp; k++) wpre += wsum[k];
+  unsigned pos = hb.sw_off[sw] + hb.tile_off[sw * hb.ntiles + tile] + wpre + x - c;
+#pragma unroll
+  for (int k = 0; k < HIT_PER_THREAD; k++) {
+    if (flags & (1u << k)) {
+      if (pos < hb.cap) {
+        hb.ind[pos] = (unsigned)(i0 + k);
+        hb.val[pos] = vals[k];
+        hb.sw[pos] = (unsigned)sw;
+      }
+      pos++;
+    }
+  }
+}
+
+cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cudaStream_t s) {
+  hb.ntiles = ntiles;
+  cudaError_t e = cudaMemsetAsync(hb.sw_cnt, 0, ((size_t)ctx.nser * ctx.nw + 1) * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  k_count_hits<<<dim3(ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb);
+  return cudaGetLastError();
+}
+
+cudaError_t scan_hit_counts(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
+  size_t rows = (size_t)ctx.nser * ctx.nw;
+  k_scan_tiles<<<(unsigned)((rows + 3) / 4), 128, 0, s>>>(hb.tile_cnt, hb.tile_off, hb.ntiles,
+                                                          rows);
+  return cudaGetLastError();
+}
+
+cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
+  k_write_hits<<<dim3(hb.ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Device-wide exclusive scan of unsigned values (3 phases).
+// ===========================================================================
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ unsigned block_exclusive_scan(unsigned v, unsigned* total) {
+  __shared__ unsigned ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    unsigned y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned w = (lane < (int)(blockDim.x >> 5)) ? ws[lane] : 0u;
+    unsigned z = w;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      unsigned y = __shfl_up_sync(0xffffffffu, z, d);
+      if (lane >= d) z += y;
+    }
+    ws[lane] = z - w;
+    if (lane == 31 && total) *total = z;
+  }
+  __syncthreads();
+  unsigned r = ws[warp] + x - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles_u32(const unsigned* __restrict__ in,
+                                                                 unsigned* __restrict__ out,
+                                                                 size_t n,
+                                                                 unsigned* __restrict__ sums) {
+  const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
+  unsigned v[SCAN_ITEMS];
+  unsigned t = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = (base + k < n) ? in[base + k] : 0u;
+    t += v[k];
+  }
+  __shared__ unsigned tot;
+  unsigned pre = block_exclusive_scan(t, &tot);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < n) out[base + k] = pre;
+    pre += v[k];
+  }
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(unsigned* __restrict__ out, size_t n,
+                                                           const unsigned* __restrict__ sums_off) {
+  const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_ITEMS;
+  unsigned a = sums_off[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++)
+    if (base + k < n) out[base + k] += a;
+}
+
+size_t scan_tmp_words(size_t n) {
+  size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  size_t nb2 = (nb + SCAN_TILE - 1) / SCAN_TILE;
+  return 2 * nb + 2 * nb2 + 8;
+}
+
+cudaError_t scan_u32(const unsigned* in, unsigned* out, size_t n, unsigned* total, unsigned* tmp,
+                     cudaStream_t s) {
+  if (n == 0) return cudaMemsetAsync(total, 0, sizeof(unsigned), s);
+  size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  unsigned* sums = tmp;
+  unsigned* sums_off = tmp + nb;
+  k_scan_tiles_u32<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, sums);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (nb == 1) {
+    cudaMemsetAsync(sums_off, 0, sizeof(unsigned), s);
+    return cudaMemcpyAsync(total, sums, sizeof(unsigned), cudaMemcpyDeviceToDevice, s);
+  }
+  // recursive scan of the block sums
+  e = scan_u32(sums, sums_off, nb, total, tmp + 2 * nb, s);
+  if (e != cudaSuccess) return e;
+  k_scan_add<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(out, n, sums_off);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Giants (find_giants.cu:194-316, pipeline.cu:755-775)
+// ===========================================================================
+__global__ void k_giant_heads(WidthCtx ctx, HitBuffers hb, unsigned nhits, unsigned* head) {
+  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nhits) return;
+  unsigned sw = hb.sw[k];
+  unsigned h = 1;
+  if (k > 0 && hb.sw[k - 1] == sw) {
+    const WidthInfo& w = ctx.winfo[sw % ctx.nw];
+    // not_nearby: b > a + max_dist  (find_giants.cu:79-87)
+    h = ((unsigned long long)hb.ind[k] > (unsigned long long)hb.ind[k - 1] + w.merge_dist) ? 1u : 0u;
+  }
+  head[k] = h;
+}
+
+__global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, GiantBuffers gb) {
+  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nhits) return;
+  unsigned g = gb.gid[k] + gb.head[k] - 1u;  // inclusive count of heads - 1
+  // first maximum: larger value wins, ties to the smaller hit position
+  unsigned long long key = ((unsigned long long)float_key(hb.val[k]) << 32) |
+                           (unsigned long long)(0xFFFFFFFFu - (unsigned)k);
+  atomicMax(&gb.key[g], key);
+  unsigned sw = hb.sw[k];
+  const WidthInfo& w = ctx.winfo[sw % ctx.nw];
+  bool is_head = gb.head[k] != 0;
+  bool is_last = (k + 1 == nhits) || gb.head[k + 1] != 0;
+  unsigned long long scr = (unsigned long long)w.ts;
+  if (is_head) gb.begin[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * scr;
+  if (is_last) gb.end[g] = ((unsigned long long)hb.ind[k] + 1ull + w.rel_off) * scr;
+  if (is_head) {
+    gb.filter[g] = w.filter_idx;
+    gb.dm[g] = (int)(sw / ctx.nw);
+  }
+}
+
+__global__ void k_giant_finish(HitBuffers hb, unsigned ngiants, GiantBuffers gb,
+                               const WidthInfo* winfo, int nw) {
+  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngiants) return;
+  unsigned long long key = gb.key[g];
+  unsigned k = 0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull);
+  const WidthInfo& w = winfo[hb.sw[k] % nw];
+  gb.peak[g] = hb.val[k];
+  gb.ind[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * (unsigned long long)w.ts;
+}
+
+cudaError_t giant_heads(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,
+                        GiantBuffers& gb, cudaStream_t s) {
+  if (nhits == 0) return cudaSuccess;
+  k_giant_heads<<<(nhits + 255) / 256, 256, 0, s>>>(ctx, hb, nhits, gb.head);
+  return cudaGetLastError();
+}
+
+cudaError_t giant_fill(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,
+                       unsigned ngiants, GiantBuffers& gb, cudaStream_t s) {
+  if (nhits == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(gb.key, 0, (size_t)ngiants * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  k_giant_reduce<<<(nhits + 255) / 256, 256, 0, s>>>(ctx, hb, nhits, gb);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_giant_finish<<<(ngiants + 255) / 256, 256, 0, s>>>(hb, ngiants, gb, ctx.winfo, ctx.nw);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Clustering (label_candidate_clusters.cu:141-197,203-394)
+//
+// The reference's neighbour sweep labels[i] = min(labels[i], labels[j]) over
+// coincident j, run sequentially, gives every giant the smallest index
+// reachable from it through a chain of coincident giants with decreasing
+// indices (a coincident j > i still holds its own, larger, label when i is
+// swept).  That value is the unique fixed point of
+//   lab[i] = min(i, min_{j < i coincident} lab[j]),
+// which these sweeps reach from lab[i] = i with atomicMin updates in any
+// order; the final chain trace of the reference is then the identity.
+// ===========================================================================
+constexpr int CL_TILE = 128;
+
+__global__ void k_cluster_init(int* label, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) label[i] = i;
+}
+
+__global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantBuffers gb,
+                                                           unsigned* changed) {
+  __shared__ unsigned long long s_samp[CL_TILE];
+  __shared__ int s_f[CL_TILE], s_dm[CL_TILE], s_lab[CL_TILE];
+  const int i = blockIdx.x * CL_TILE + threadIdx.x;
+  const int i_first = blockIdx.x * CL_TILE;
+  const int i_last = min(i_first + CL_TILE, a.ngiants) - 1;
+  unsigned long long si = 0, bi = 0;
+  int fi = 0, di = 0, best = 0x7FFFFFFF;
+  if (i < a.ngiants) {
+    si = gb.ind[i];
+    bi = si / a.nsamps_beam;
+    fi = gb.filter[i];
+    di = gb.dm[i];
+    best = gb.label[i];
+  }
+  // giants are in ascending DM order: find the first giant within dm_tol of
+  // the tile's smallest DM
+  const int dm_first = gb.dm[i_first];
+  int lo = 0, hi = i_first;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if ((long long)gb.dm[mid] + (long long)a.dm_tol < (long long)dm_first) lo = mid + 1;
+    else hi = mid;
+  }
+  for (int j0 = lo; j0 <= i_last; j0 += CL_TILE) {
+    int j = j0 + threadIdx.x;
+    __syncthreads();
+    if (j <= i_last) {
+      s_samp[threadIdx.x] = gb.ind[j];
+      s_f[threadIdx.x] = gb.filter[j];
+      s_dm[threadIdx.x] = gb.dm[j];
+      s_lab[threadIdx.x] = *((volatile int*)&gb.label[j]);
+    }
+    __syncthreads();
+    if (i < a.ngiants) {
+      int jn = min(CL_TILE, i - j0);  // only j < i
+      for (int jj = 0; jj < jn; jj++) {
+        int fj = s_f[jj];
+        int wmax = max(1 << fi, 1 << fj);
+        unsigned long long tt = a.time_tol * (unsigned long long)wmax;
+        unsigned long long sj = s_samp[jj];
+        bool coinc = (sj / a.nsamps_beam) == bi &&
+                     (unsigned long long)abs((int)sj - (int)si) <= tt &&
+                     (unsigned long long)abs(fj - fi) <= a.filter_tol &&
+                     (unsigned long long)abs(s_dm[jj] - di) <= a.dm_tol;
+        if (coinc && s_lab[jj] < best) best = s_lab[jj];
+      }
+    }
+  }
+  if (i < a.ngiants && best < gb.label[i]) {
+    atomicMin(&gb.label[i], best);
+    *changed = 1u;
+  }
+}
+
+cudaError_t cluster_init(GiantBuffers& gb, int n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_cluster_init<<<(n + 255) / 256, 256, 0, s>>>(gb.label, n);
+  return cudaGetLastError();
+}
+
+cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* changed,
+                          cudaStream_t s) {
+  if (a.ngiants == 0) return cudaSuccess;
+  k_cluster_sweep<<<(a.ngiants + CL_TILE - 1) / CL_TILE, CL_TILE, 0, s>>>(a, gb, changed);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Merge (merge_candidates.cu:74-134): groups in ascending label order; per
+// group the first member with the largest peak, members summed; DM gathered.
+// ===========================================================================
+__global__ void k_root_flags(const int* label, int n, unsigned* flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = (label[i] == i) ? 1u : 0u;
+}
+
+__global__ void k_merge_reduce(GiantBuffers gb, int n, const unsigned* root_off,
+                               unsigned long long* gkey, unsigned long long* members) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned g = root_off[gb.label[i]];
+  unsigned long long key = ((unsigned long long)float_key(gb.peak[i]) << 32) |
+                           (unsigned long long)(0xFFFFFFFFu - (unsigned)i);
+  atomicMax(&gkey[g], key);
+  atomicAdd(&members[g], 1ull);
+}
+
+__global__ void k_merge_emit(GiantBuffers gb, const unsigned* ngroups,
+                             const unsigned long long* gkey, const unsigned long long* members,
+                             const float* dm_list, GroupRow* rows) {
+  unsigned g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= *ngroups) return;
+  unsigned i = 0xFFFFFFFFu - (unsigned)(gkey[g] & 0xFFFFFFFFull);
+  GroupRow r;
+  r.peak = gb.peak[i];
+  r.ind = gb.ind[i];
+  r.begin = gb.begin[i];
+  r.end = gb.end[i];
+  r.filter = (unsigned long long)gb.filter[i];
+  r.dm_ind = (unsigned long long)gb.dm[i];
+  r.members = members[g];
+  r.dm = dm_list[gb.dm[i]];
+  rows[g] = r;
+}
+
+cudaError_t merge_groups(const GiantBuffers& gb, int n, const float* dm_list, unsigned* root_flag,
+                         unsigned* root_off, unsigned* nroots, unsigned* scan_tmp,
+                         unsigned long long* gkey, GroupRow* rows, cudaStream_t s) {
+  if (n == 0) return cudaMemsetAsync(nroots, 0, sizeof(unsigned), s);
+  k_root_flags<<<(n + 255) / 256, 256, 0, s>>>(gb.label, n, root_flag);
+  cudaError_t e = scan_u32(root_flag, root_off, (size_t)n, nroots, scan_tmp, s);
+  if (e != cudaSuccess) return e;
+  // gkey: [n] keys followed by [n] member counts
+  unsigned long long* members = gkey + n;
+  if ((e = cudaMemsetAsync(gkey, 0, 2 * (size_t)n * sizeof(unsigned long long), s)) != cudaSuccess)
+    return e;
+  k_merge_reduce<<<(n + 255) / 256, 256, 0, s>>>(gb, n, root_off, gkey, members);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // emit for every possible group index; rows beyond nroots are never read
+  k_merge_emit<<<(n + 255) / 256, 256, 0, s>>>(gb, nroots, gkey, members, dm_list, rows);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// RFI mask (clean_filterbank_rfi.cu:447-506)
+//   mask[t] = |x[t]| > tol  OR, for some width w in 1,2,..,boxcar_max with
+//   t in [off, count+1-boxcar_max+off): a flagged j in [t-behind, t+ahead),
+//   where j in [off, count+1-boxcar_max+off) is flagged when
+//   |boxcar_w(j-off) * (1/sqrt(w))| > tol  (off = boxcar_max/2).
+// ===========================================================================
+__global__ void k_rfi_flags(const float* __restrict__ scan, size_t count, int bmax, int nwid,
+                            const float* __restrict__ wnorm, float tol,
+                            unsigned char* __restrict__ flags) {
+  size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  const int off = bmax / 2;
+  const size_t nf = count + 1 - (size_t)bmax;
+  unsigned char f = 0;
+  if (j >= (size_t)off && j < (size_t)off + nf) {
+    size_t k = j - off;
+    for (int wi = 0; wi < nwid; wi++) {
+      int w = 1 << wi;
+      int ahead = (w - 1) / 2 + 1, behind = w / 2;
+      float v = __fsub_rn(scan[off + ahead + k], scan[off - behind + k]);
+      v = __fmul_rn(v, wnorm[wi]);
+      if (fabsf(v) > tol) f |= (unsigned char)(1u << wi);
+    }
+  }
+  flags[j] = f;
+}
+
+__global__ void k_rfi_mask(const float* __restrict__ x, size_t count, int bmax, int nwid,
+                           float tol, const unsigned char* __restrict__ flags, int* __restrict__ mask) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const int off = bmax / 2;
+  const size_t nf = count + 1 - (size_t)bmax;
+  int m = fabsf(x[t]) > tol;
+  if (!m && t >= (size_t)off && t < (size_t)off + nf) {
+    for (int wi = 0; wi < nwid && !m; wi++) {
+      int w = 1 << wi;
+      int ahead = (w - 1) / 2 + 1, behind = w / 2;
+      for (size_t j = t - behind; j < t + ahead; j++) {
+        if (flags[j] & (1u << wi)) { m = 1; break; }
+      }
+    }
+  }
+  mask[t] = m;
+}
+
+cudaError_t rfi_mask(const float* x, const float* scan, size_t count, size_t boxcar_max,
+                     float rfi_tol, int* mask, int* fmask, cudaStream_t s) {
+  int nwid = 0;
+  float wn[32];
+  for (size_t w = 1; w <= boxcar_max && nwid < 32; w *= 2, nwid++)
+    wn[nwid] = (float)(1.0 / (double)sqrtf((float)w));  // clean_filterbank_rfi.cu:476-477
+  float* dwn = reinterpret_cast<float*>(fmask);
+  unsigned char* flags = reinterpret_cast<unsigned char*>(fmask + 32);
+  cudaError_t e = cudaMemcpyAsync(dwn, wn, nwid * sizeof(float), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  unsigned nb = (unsigned)((count + 255) / 256);
+  k_rfi_flags<<<nb, 256, 0, s>>>(scan, count, (int)boxcar_max, nwid, dwn, rfi_tol, flags);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_rfi_mask<<<nb, 256, 0, s>>>(x, count, (int)boxcar_max, nwid, rfi_tol, flags, mask);
+  return cudaGetLastError();
+}
+
+}  // namespace hdb

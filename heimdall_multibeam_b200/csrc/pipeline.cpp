@@ -1,0 +1,633 @@
+// pipeline.cpp -- the hd_* pipeline (Pipeline/pipeline.cu:138-1100) on the
+// sm_100a kernels.
+//
+// One gulp runs as a fixed sequence of kernels on the pipeline's own stream:
+//   H2D (TF filterbank)
+//   clean_filterbank_rfi: zero-DM sums -> baseline -> RMS -> normalise+scan ->
+//       RFI mask -> zap (writes the channel-major working copy)   [optional]
+//   dedispersion of all DM trials (TMA-staged, exact int32 sums)
+//   per-DM baseline, robust RMS, normalise + prefix sum        (all DMs at once)
+//   per-width block RMS, threshold + ordered hit compaction    (all DMs x widths)
+//   giant segmentation, clustering, merge, DM gather
+//   D2H of the merged candidate rows; .cand file on the host.
+// Host synchronisations: the hit and giant totals (to size buffers), the
+// clustering convergence flag and the final candidate rows.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "heimdall_b200.h"
+#include "internal.h"
+#include "plan.h"
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  template <class T>
+  T* as() { return reinterpret_cast<T*>(p); }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t b = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) cap = b;
+    return e;
+  }
+};
+
+}  // namespace
+
+struct hd_pipeline_t {
+  hd_params params;
+  std::string output_dir;
+  bool has_output_dir = true;
+  std::vector<hd_range_t> zaps;
+  dedisp_plan plan = nullptr;
+  bool cleaning = true;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[10] = {};
+  float timing[8] = {};
+
+  DevBuf fb_tf, fb_ft, fb_tf_clean;
+  DevBuf dm0, dm0_scan, base, rms, mask, fmask, rms0;
+  DevBuf dd, scan;
+  DevBuf ws_a, ws_b;
+  DevBuf winfo, norm;
+  DevBuf tile_cnt, tile_off, sw_cnt, sw_off, hit_ind, hit_val, hit_sw;
+  DevBuf head, gid, gkey, g_peak, g_ind, g_begin, g_end, g_filter, g_dm, g_label;
+  DevBuf scan_tmp, small;  // small: totals / flags
+  DevBuf root_flag, root_off, mkey, rows;
+  DevBuf h_small_dev;
+
+  unsigned* h_small = nullptr;  // pinned host words
+
+  std::vector<hd_candidate> cands;
+  std::vector<float> g_peaks;
+  std::vector<hd_size> g_inds, g_begins, g_ends, g_filters, g_dms, g_labels;
+
+  ~hd_pipeline_t() {
+    if (plan) dedisp_destroy_plan(plan);
+    for (auto& e : ev) if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+    if (h_small) cudaFreeHost(h_small);
+  }
+};
+
+namespace {
+
+hd_error cuda_err(cudaError_t e) {
+  if (e == cudaSuccess) return HD_NO_ERROR;
+  if (e == cudaErrorMemoryAllocation) return HD_MEM_ALLOC_FAILED;
+  if (e == cudaErrorInvalidDevice) return HD_INVALID_DEVICE_INDEX;
+  return HD_INTERNAL_GPU_ERROR;
+}
+
+hd_error dedisp_err(dedisp_error e) {
+  switch (e) {
+    case DEDISP_NO_ERROR: return HD_NO_ERROR;
+    case DEDISP_MEM_ALLOC_FAILED: return HD_MEM_ALLOC_FAILED;
+    case DEDISP_MEM_COPY_FAILED: return HD_MEM_COPY_FAILED;
+    case DEDISP_INVALID_DEVICE_INDEX: return HD_INVALID_DEVICE_INDEX;
+    case DEDISP_DEVICE_ALREADY_SET: return HD_DEVICE_ALREADY_SET;
+    case DEDISP_INVALID_POINTER: return HD_INVALID_POINTER;
+    case DEDISP_INVALID_STRIDE: return HD_INVALID_STRIDE;
+    case DEDISP_TOO_FEW_NSAMPS: return HD_TOO_FEW_NSAMPS;
+    case DEDISP_PRIOR_GPU_ERROR: return HD_PRIOR_GPU_ERROR;
+    case DEDISP_INTERNAL_GPU_ERROR: return HD_INTERNAL_GPU_ERROR;
+    default: return HD_UNKNOWN_ERROR;
+  }
+}
+
+#define HD_TRY(x)                                   \
+  do {                                              \
+    cudaError_t e_ = (x);                           \
+    if (e_ != cudaSuccess) return cuda_err(e_);     \
+  } while (0)
+
+unsigned log2u(size_t v) {
+  unsigned r = 0;
+  while ((v >> r) > 1) r++;
+  return r;
+}
+
+size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Scratch needed by the median trees of `nseg` segments of `count` values.
+size_t tree_cap(size_t nseg, size_t count) { return nseg * (count / 3125 + 8) + 64; }
+
+// Device clean_filterbank_rfi on the TF filterbank in pl->fb_tf; writes the
+// zapped filterbank channel-major into fb_ft (pitch) and, if out_tf, also
+// time-major.  Pipeline/clean_filterbank_rfi.cu:256-528.
+hd_error clean_device(hd_pipeline pl, size_t nsamps, size_t nchans, float dt,
+                      float baseline_length, float rfi_tol, size_t boxcar_max, size_t nbeams,
+                      uint8_t* fb_ft, size_t pitch, uint8_t* out_tf) {
+  cudaStream_t s = pl->stream;
+  const size_t nsmooth = (size_t)(baseline_length / (2 * dt));
+  if (nsamps < boxcar_max + 1 || nsmooth / 4 >= nsamps) return HD_TOO_FEW_NSAMPS;
+  const size_t spitch = round_up(nsamps + 8, 64);
+  HD_TRY(pl->dm0.ensure(spitch * sizeof(float)));
+  HD_TRY(pl->dm0_scan.ensure(spitch * sizeof(float)));
+  HD_TRY(pl->mask.ensure((nsamps + 64) * sizeof(int)));
+  HD_TRY(pl->fmask.ensure((nsamps + 256) * sizeof(int)));
+  HD_TRY(pl->rms0.ensure(nbeams * sizeof(float) + 64));
+  HD_TRY(pl->base.ensure((nbeams * hdb::baseline_samples(nsamps / nbeams, nsmooth) + 64) *
+                         sizeof(float)));
+  size_t cap = std::max(tree_cap(nbeams, nsamps),
+                        hdb::baseline_scratch(nsamps / nbeams, nsmooth, nbeams));
+  HD_TRY(pl->ws_a.ensure(cap * sizeof(float)));
+  HD_TRY(pl->ws_b.ensure(cap * sizeof(float)));
+  float* x = pl->dm0.as<float>();
+  HD_TRY(cudaMemsetAsync(x, 0, spitch * sizeof(float), s));
+  HD_TRY(hdb::launch_dm0_sum(pl->fb_tf.as<uint8_t>(), nsamps, (int)nchans, x, s));
+  hdb::SeriesBatch sb{x, spitch, 1, nsamps, nsamps / nbeams, nsamps / nbeams, (int)nbeams};
+  hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
+  HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
+  HD_TRY(hdb::rms_beams(sb, pl->rms0.as<float>(), ws, s));
+  HD_TRY(hdb::normalise_scan(sb, pl->rms0.as<float>(), pl->dm0_scan.as<float>(), spitch, x, s));
+  HD_TRY(hdb::rfi_mask(x, pl->dm0_scan.as<float>(), nsamps, boxcar_max, rfi_tol,
+                       pl->mask.as<int>(), pl->fmask.as<int>(), s));
+  HD_TRY(hdb::launch_zap(pl->fb_tf.as<uint8_t>(), nsamps, (int)nchans, pl->mask.as<int>(),
+                         (unsigned)(nsmooth / 4), fb_ft, pitch, out_tf, s));
+  return HD_NO_ERROR;
+}
+
+void write_cand_file(hd_pipeline pl, size_t first_idx) {
+  if (!pl->has_output_dir) return;
+  char buffer[64];
+  time_t off = pl->params.spectra_per_second
+                   ? (time_t)(first_idx / pl->params.spectra_per_second)
+                   : (time_t)0;
+  time_t now = pl->params.utc_start + off;
+  struct tm tmv;
+  gmtime_r(&now, &tmv);
+  strftime(buffer, sizeof(buffer), "%Y-%m-%d-%H:%M:%S", &tmv);
+  char beam[32];
+  snprintf(beam, sizeof(beam), "%02zu", (size_t)(pl->params.beam + 1));
+  std::string fn = pl->output_dir + "/" + buffer + "_" + beam + ".cand";
+  FILE* f = fopen(fn.c_str(), "w");
+  if (!f) {
+    fprintf(stdout, "Skipping dump due to bad file open on %s\n", fn.c_str());
+    return;
+  }
+  for (const hd_candidate& c : pl->cands)
+    fprintf(f, "%g\t%zu\t%g\t%zu\t%zu\t%g\t%zu\t%zu\t%zu\t%zu\t\n", (double)c.snr, c.samp_idx,
+            (double)c.time, c.filter, c.dm_trial, (double)c.dm, c.members, c.begin, c.end,
+            c.beam);
+  fclose(f);
+}
+
+}  // namespace
+
+extern "C" {
+
+hd_error hd_create_pipeline(hd_pipeline* pipeline_, hd_params params) {
+  if (!pipeline_) return HD_INVALID_POINTER;
+  *pipeline_ = nullptr;
+  hd_pipeline pl = new (std::nothrow) hd_pipeline_t();
+  if (!pl) return HD_MEM_ALLOC_FAILED;
+  pl->params = params;
+  if (params.output_dir) pl->output_dir = params.output_dir;
+  else pl->has_output_dir = false;
+  pl->params.output_dir = pl->has_output_dir ? pl->output_dir.c_str() : nullptr;
+  for (unsigned z = 0; z < params.num_channel_zaps && params.channel_zaps; z++)
+    pl->zaps.push_back(params.channel_zaps[z]);
+  pl->params.channel_zaps = pl->zaps.empty() ? nullptr : pl->zaps.data();
+  pl->params.coincidencer_host = nullptr;
+  pl->params.sigproc_file = nullptr;
+  // allocate_gpu (pipeline.cu:80-124)
+  cudaError_t ce = cudaSetDevice(params.gpu_id);
+  if (ce != cudaSuccess) { delete pl; return cuda_err(ce); }
+  pl->device = params.gpu_id;
+  if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete pl;
+    return HD_PRIOR_GPU_ERROR;
+  }
+  for (auto& e : pl->ev) cudaEventCreate(&e);
+  if (cudaMallocHost(&pl->h_small, 64 * sizeof(unsigned)) != cudaSuccess) {
+    delete pl;
+    return HD_MEM_ALLOC_FAILED;
+  }
+  if (params.use_scrunching) {
+    // adaptive dt is not provided (dedisp_enable_adaptive_dt reports it)
+    delete pl;
+    return HD_UNKNOWN_ERROR;
+  }
+  dedisp_error de = dedisp_create_plan(&pl->plan, params.nchans, params.dt, params.f0, params.df);
+  if (de == DEDISP_NO_ERROR)
+    de = dedisp_generate_dm_list(pl->plan, params.dm_min, params.dm_max, params.dm_pulse_width,
+                                 params.dm_tol);
+  if (de != DEDISP_NO_ERROR) {
+    delete pl;
+    return dedisp_err(de);
+  }
+  *pipeline_ = pl;
+  return HD_NO_ERROR;
+}
+
+hd_size hd_get_max_overlap(hd_pipeline pl, hd_size nbeams) {
+  if (!pl) return 0;
+  return (pl->params.boxcar_max + dedisp_get_max_delay(pl->plan)) * nbeams;
+}
+
+hd_error hd_preallocate(hd_pipeline pl, hd_size nsamps, hd_size nbeams) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  (void)nsamps;
+  (void)nbeams;
+  return HD_NO_ERROR;
+}
+
+hd_error hd_set_cleaning(hd_pipeline pl, int enable) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  pl->cleaning = enable != 0;
+  return HD_NO_ERROR;
+}
+
+hd_error hd_execute(hd_pipeline pl, const hd_byte* h_filterbank, hd_size nsamps, hd_size nbits,
+                    hd_size first_idx, hd_size nbeams, hd_size* nsamps_processed) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!h_filterbank || !nsamps_processed) return HD_INVALID_POINTER;
+  if (nbits != 8) return HD_INVALID_NBITS;
+  const hd_params& P = pl->params;
+  const size_t C = P.nchans;
+  if (C % 4 != 0 || nbeams == 0) return HD_INVALID_STRIDE;
+  if (P.min_tscrunch_width < 2) return HD_INVALID_STRIDE;
+  if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  cudaStream_t s = pl->stream;
+  pl->cands.clear();
+  pl->g_peaks.clear();
+  std::memset(pl->timing, 0, sizeof(pl->timing));
+
+  // killmask: manual channel zaps (clean_filterbank_rfi.cu:530-545)
+  std::vector<int> km(C, 1);
+  for (const hd_range_t& z : pl->zaps)
+    for (size_t j = z.start; j < z.end; j++)
+      if (j < C) km[j] = 0;
+  dedisp_set_killmask(pl->plan, km.data());
+  dedisp_error de = hdb::plan_prepare(pl->plan);
+  if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+  const size_t max_delay = pl->plan->max_delay;
+  const size_t D = pl->plan->dm_list.size();
+  if (nsamps <= max_delay) {
+    *nsamps_processed = 0;
+    return HD_TOO_FEW_NSAMPS;
+  }
+  const size_t nc = nsamps - max_delay;  // nsamps_computed
+  *nsamps_processed = nsamps - nbeams * (P.boxcar_max + max_delay);
+  if (nsamps < nbeams * (P.boxcar_max + max_delay)) *nsamps_processed = 0;
+
+  cudaEventRecord(pl->ev[0], s);
+  // ---- H2D ----------------------------------------------------------------
+  HD_TRY(pl->fb_tf.ensure(nsamps * C));
+  HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_filterbank, nsamps * C, cudaMemcpyHostToDevice, s));
+  cudaEventRecord(pl->ev[1], s);
+
+  // ---- clean + channel-major working copy ------------------------------------
+  const size_t pitch = hdb::ft_pitch(pl->plan, nsamps);
+  HD_TRY(pl->fb_ft.ensure(pitch * C));
+  if (pl->cleaning) {
+    hd_error he = clean_device(pl, nsamps, C, P.dt, P.baseline_length, P.rfi_tol, 64, nbeams,
+                               pl->fb_ft.as<uint8_t>(), pitch, nullptr);
+    if (he != HD_NO_ERROR) return he;
+  } else {
+    HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>(), nsamps, (int)C,
+                                       pl->fb_ft.as<uint8_t>(), pitch, s));
+  }
+  cudaEventRecord(pl->ev[2], s);
+
+  // ---- dedispersion ----------------------------------------------------------
+  const size_t dd_pitch = round_up(nc + 1, 4);
+  HD_TRY(pl->dd.ensure(D * dd_pitch * sizeof(float)));
+  float* dd = pl->dd.as<float>();
+  de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>(), pitch, nsamps, dd, dd_pitch, s);
+  if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+  // the element after each series is read (never used) by the baseline stretch
+  HD_TRY(cudaMemset2DAsync(dd + nc, dd_pitch * sizeof(float), 0, sizeof(float), D, s));
+  cudaEventRecord(pl->ev[3], s);
+
+  const size_t stride = nsamps / nbeams;
+  const size_t Bmax = P.boxcar_max;
+  bool search = !(max_delay >= stride) && !(max_delay + Bmax > stride);
+  unsigned nhits = 0, ngiants = 0;
+  std::vector<hdb::WidthInfo> wi;
+  hdb::WidthCtx wctx{};
+  hdb::HitBuffers hb{};
+  hdb::GiantBuffers gb{};
+  if (search) {
+    // ---- per-DM baseline, RMS, normalise + scan ------------------------------
+    const size_t bcount = stride - max_delay;
+    hdb::SeriesBatch sb{dd, dd_pitch, (int)D, nc, stride, bcount, (int)nbeams};
+    const float cur_dt = P.dt * 1.0f;
+    const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
+    size_t cap = std::max({tree_cap(D * nbeams, stride),
+                           tree_cap(D * (log2u(Bmax) + 1), nbeams * stride),
+                           hdb::baseline_scratch(stride, nsmooth, D * nbeams)});
+    HD_TRY(pl->ws_a.ensure(cap * sizeof(float)));
+    HD_TRY(pl->ws_b.ensure(cap * sizeof(float)));
+    hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
+    HD_TRY(pl->base.ensure((D * nbeams * hdb::baseline_samples(stride, nsmooth) + 64) *
+                           sizeof(float)));
+    HD_TRY(pl->rms.ensure(D * nbeams * sizeof(float) + 64));
+    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
+    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
+    const size_t scan_pitch = round_up(nc + 1, 4);
+    HD_TRY(pl->scan.ensure(D * scan_pitch * sizeof(float)));
+    HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), pl->scan.as<float>(), scan_pitch,
+                               nullptr, s));
+    cudaEventRecord(pl->ev[4], s);
+
+    // ---- widths --------------------------------------------------------------
+    const size_t rel_bmax = Bmax;
+    const size_t max_nf = nc + 1 - rel_bmax;
+    const size_t cur_off = rel_bmax / 2;
+    for (size_t fw = 1; fw <= Bmax; fw *= 2) {
+      hdb::WidthInfo w{};
+      size_t rel_min_ts = std::max<size_t>(P.min_tscrunch_width / 1, 1);
+      size_t ts = std::max<size_t>(2 * fw / rel_min_ts, 1);
+      w.width = (int)fw;
+      w.ts = (int)ts;
+      w.ahead = (int)((fw - 1) / 2 + 1);
+      w.behind = (int)(fw / 2);
+      w.filter_idx = (int)log2u(fw);
+      w.n = (unsigned)((max_nf - 1) / ts + 1);
+      w.bn = (unsigned)(stride - (max_delay + rel_bmax));
+      w.merge_dist = (unsigned)(P.cand_sep_time * (fw / ts));
+      w.rel_off = (unsigned)(cur_off / ts);
+      w.prev_cover = (int)wi.size() - 1;
+      wi.push_back(w);
+    }
+    const int nw = (int)wi.size();
+    HD_TRY(pl->winfo.ensure(nw * sizeof(hdb::WidthInfo)));
+    HD_TRY(cudaMemcpyAsync(pl->winfo.p, wi.data(), nw * sizeof(hdb::WidthInfo),
+                           cudaMemcpyHostToDevice, s));
+    HD_TRY(pl->norm.ensure(D * nw * sizeof(float)));
+    wctx.scan = pl->scan.as<float>();
+    wctx.scan_pitch = scan_pitch;
+    wctx.nser = (int)D;
+    wctx.stride = stride;
+    wctx.nbeams = (int)nbeams;
+    wctx.offset = (int)cur_off;
+    wctx.nw = nw;
+    wctx.winfo = pl->winfo.as<hdb::WidthInfo>();
+    wctx.norm = pl->norm.as<float>();
+    wctx.thresh = P.detect_thresh;
+    int n_ts1 = 0;
+    while (n_ts1 < nw && wi[n_ts1].ts == 1) n_ts1++;
+    if (n_ts1 > 0) HD_TRY(hdb::block_rms(wctx, wi.data(), 0, n_ts1, ws, s));
+    for (int w = n_ts1; w < nw; w++) HD_TRY(hdb::block_rms(wctx, wi.data(), w, w + 1, ws, s));
+
+    // ---- threshold + ordered compaction -------------------------------------
+    const unsigned ntiles = (unsigned)((wi[0].n + 2047) / 2048);
+    const size_t nsw = D * nw;
+    HD_TRY(pl->tile_cnt.ensure(nsw * ntiles * sizeof(unsigned)));
+    HD_TRY(pl->tile_off.ensure(nsw * ntiles * sizeof(unsigned)));
+    HD_TRY(pl->sw_cnt.ensure((nsw + 1) * sizeof(unsigned)));
+    HD_TRY(pl->sw_off.ensure((nsw + 1) * sizeof(unsigned)));
+    HD_TRY(pl->small.ensure(64 * sizeof(unsigned)));
+    hb.tile_cnt = pl->tile_cnt.as<unsigned>();
+    hb.tile_off = pl->tile_off.as<unsigned>();
+    hb.sw_cnt = pl->sw_cnt.as<unsigned>();
+    hb.sw_off = pl->sw_off.as<unsigned>();
+    HD_TRY(hdb::count_hits(wctx, hb, ntiles, s));
+    HD_TRY(hdb::scan_hit_counts(wctx, hb, s));
+    HD_TRY(pl->scan_tmp.ensure(hdb::scan_tmp_words(nsw) * sizeof(unsigned)));
+    unsigned* totals = pl->small.as<unsigned>();
+    HD_TRY(hdb::scan_u32(hb.sw_cnt, hb.sw_off, nsw, totals, pl->scan_tmp.as<unsigned>(), s));
+    HD_TRY(cudaMemcpyAsync(pl->h_small, totals, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaStreamSynchronize(s));
+    nhits = pl->h_small[0];
+    HD_TRY(pl->hit_ind.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
+    HD_TRY(pl->hit_val.ensure((size_t)(nhits + 1) * sizeof(float)));
+    HD_TRY(pl->hit_sw.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
+    hb.ind = pl->hit_ind.as<unsigned>();
+    hb.val = pl->hit_val.as<float>();
+    hb.sw = pl->hit_sw.as<unsigned>();
+    hb.cap = nhits;
+    if (nhits) HD_TRY(hdb::write_hits(wctx, hb, s));
+    cudaEventRecord(pl->ev[5], s);
+
+    // ---- giants ------------------------------------------------------------
+    if (nhits) {
+      HD_TRY(pl->head.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
+      HD_TRY(pl->gid.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
+      gb.head = pl->head.as<unsigned>();
+      gb.gid = pl->gid.as<unsigned>();
+      HD_TRY(hdb::giant_heads(wctx, hb, nhits, gb, s));
+      HD_TRY(pl->scan_tmp.ensure(hdb::scan_tmp_words(nhits) * sizeof(unsigned)));
+      HD_TRY(hdb::scan_u32(gb.head, gb.gid, nhits, totals + 1, pl->scan_tmp.as<unsigned>(), s));
+      HD_TRY(cudaMemcpyAsync(pl->h_small + 1, totals + 1, sizeof(unsigned),
+                             cudaMemcpyDeviceToHost, s));
+      HD_TRY(cudaStreamSynchronize(s));
+      ngiants = pl->h_small[1];
+      size_t G = (size_t)ngiants + 1;
+      HD_TRY(pl->gkey.ensure(G * sizeof(unsigned long long)));
+      HD_TRY(pl->g_peak.ensure(G * sizeof(float)));
+      HD_TRY(pl->g_ind.ensure(G * sizeof(unsigned long long)));
+      HD_TRY(pl->g_begin.ensure(G * sizeof(unsigned long long)));
+      HD_TRY(pl->g_end.ensure(G * sizeof(unsigned long long)));
+      HD_TRY(pl->g_filter.ensure(G * sizeof(int)));
+      HD_TRY(pl->g_dm.ensure(G * sizeof(int)));
+      HD_TRY(pl->g_label.ensure(G * sizeof(int)));
+      gb.key = pl->gkey.as<unsigned long long>();
+      gb.peak = pl->g_peak.as<float>();
+      gb.ind = pl->g_ind.as<unsigned long long>();
+      gb.begin = pl->g_begin.as<unsigned long long>();
+      gb.end = pl->g_end.as<unsigned long long>();
+      gb.filter = pl->g_filter.as<int>();
+      gb.dm = pl->g_dm.as<int>();
+      gb.label = pl->g_label.as<int>();
+      gb.cap = ngiants;
+      HD_TRY(hdb::giant_fill(wctx, hb, nhits, ngiants, gb, s));
+    }
+  }
+  cudaEventRecord(pl->ev[6], s);
+
+  // giant-rate bail-out (pipeline.cu:779-787): the running count only grows,
+  // so it trips exactly when the final count does
+  bool too_many = false;
+  {
+    float mins = (float)((double)((float)nsamps * P.dt) / 60.0);
+    if (P.max_giant_rate != 0.0f && ((float)ngiants / mins > P.max_giant_rate)) too_many = true;
+  }
+
+  unsigned ngroups = 0;
+  std::vector<hdb::GroupRow> rows;
+  if (!too_many && ngiants > 0) {
+    // ---- clustering ----------------------------------------------------------
+    HD_TRY(hdb::cluster_init(gb, (int)ngiants, s));
+    hdb::ClusterArgs ca{(int)ngiants, P.cand_sep_time, P.cand_sep_filter, P.cand_sep_dm,
+                        (unsigned long long)(nsamps / nbeams)};
+    unsigned* changed = pl->small.as<unsigned>() + 8;
+    for (unsigned it = 0; it <= ngiants; it++) {
+      HD_TRY(cudaMemsetAsync(changed, 0, sizeof(unsigned), s));
+      HD_TRY(hdb::cluster_sweep(ca, gb, changed, s));
+      HD_TRY(cudaMemcpyAsync(pl->h_small + 8, changed, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      HD_TRY(cudaStreamSynchronize(s));
+      if (pl->h_small[8] == 0) break;
+    }
+    // ---- merge -----------------------------------------------------------------
+    size_t G = ngiants;
+    HD_TRY(pl->root_flag.ensure((G + 1) * sizeof(unsigned)));
+    HD_TRY(pl->root_off.ensure((G + 1) * sizeof(unsigned)));
+    HD_TRY(pl->mkey.ensure(2 * (G + 1) * sizeof(unsigned long long)));
+    HD_TRY(pl->rows.ensure((G + 1) * sizeof(hdb::GroupRow)));
+    HD_TRY(pl->scan_tmp.ensure(hdb::scan_tmp_words(G) * sizeof(unsigned)));
+    unsigned* nroots = pl->small.as<unsigned>() + 16;
+    HD_TRY(hdb::merge_groups(gb, (int)G, pl->plan->d_dm_list, pl->root_flag.as<unsigned>(),
+                             pl->root_off.as<unsigned>(), nroots, pl->scan_tmp.as<unsigned>(),
+                             pl->mkey.as<unsigned long long>(), pl->rows.as<hdb::GroupRow>(), s));
+    HD_TRY(cudaMemcpyAsync(pl->h_small + 16, nroots, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaStreamSynchronize(s));
+    ngroups = pl->h_small[16];
+    rows.resize(ngroups);
+    if (ngroups)
+      HD_TRY(cudaMemcpyAsync(rows.data(), pl->rows.p, ngroups * sizeof(hdb::GroupRow),
+                             cudaMemcpyDeviceToHost, s));
+    // giants for hd_get_giants
+    pl->g_peaks.resize(G);
+    std::vector<unsigned long long> ind(G), beg(G), end(G);
+    std::vector<int> fil(G), dmi(G), lab(G);
+    HD_TRY(cudaMemcpyAsync(pl->g_peaks.data(), gb.peak, G * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(ind.data(), gb.ind, G * 8, cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(beg.data(), gb.begin, G * 8, cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(end.data(), gb.end, G * 8, cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(fil.data(), gb.filter, G * 4, cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(dmi.data(), gb.dm, G * 4, cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(lab.data(), gb.label, G * 4, cudaMemcpyDeviceToHost, s));
+    cudaEventRecord(pl->ev[7], s);
+    HD_TRY(cudaStreamSynchronize(s));
+    pl->g_inds.assign(ind.begin(), ind.end());
+    pl->g_begins.assign(beg.begin(), beg.end());
+    pl->g_ends.assign(end.begin(), end.end());
+    pl->g_filters.assign(fil.begin(), fil.end());
+    pl->g_dms.assign(dmi.begin(), dmi.end());
+    pl->g_labels.assign(lab.begin(), lab.end());
+  } else {
+    cudaEventRecord(pl->ev[7], s);
+    HD_TRY(cudaStreamSynchronize(s));
+    pl->g_inds.clear(); pl->g_begins.clear(); pl->g_ends.clear();
+    pl->g_filters.clear(); pl->g_dms.clear(); pl->g_labels.clear();
+  }
+  unsigned derr = 0;
+  cudaMemcpy(&derr, pl->plan->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (derr) return HD_INTERNAL_GPU_ERROR;
+
+  // ---- candidate rows (pipeline.cu:1012-1039) ----------------------------------
+  const unsigned nsamps_beam = (unsigned)(nsamps / nbeams);
+  const unsigned nsamps_valid = (unsigned)(*nsamps_processed / nbeams);
+  for (unsigned i = 0; i < ngroups; i++) {
+    const hdb::GroupRow& r = rows[i];
+    size_t ind = (size_t)r.ind;
+    size_t beam_idx = (size_t)std::floor((float)ind / (float)nsamps_beam);
+    size_t beam_start = beam_idx * nsamps_beam + (P.boxcar_max / 2);
+    size_t beam_end = beam_start + nsamps_valid;
+    if (!(beam_start <= ind && ind < beam_end)) continue;
+    hd_candidate c;
+    size_t samp_off = ind - (size_t)nsamps_beam * beam_idx;
+    c.samp_idx = first_idx + samp_off;
+    c.snr = std::isinf(r.peak) ? 0.0f : r.peak;
+    c.time = P.dt * (float)c.samp_idx;
+    c.filter = (hd_size)r.filter;
+    c.dm_trial = (hd_size)r.dm_ind;
+    c.dm = r.dm;
+    c.members = (hd_size)r.members;
+    c.begin = first_idx + ((size_t)r.begin % nsamps_beam);
+    c.end = first_idx + ((size_t)r.end % nsamps_beam);
+    c.beam = P.beam + beam_idx + 1;
+    pl->cands.push_back(c);
+  }
+  write_cand_file(pl, first_idx);
+
+  // stage timings
+  auto el = [&](int a, int b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pl->ev[a], pl->ev[b]) != cudaSuccess) ms = 0.f;
+    return ms;
+  };
+  pl->timing[0] = el(0, 7);
+  pl->timing[7] = el(0, 1);
+  pl->timing[1] = el(1, 2);
+  pl->timing[2] = el(2, 3);
+  if (search) {
+    pl->timing[3] = el(3, 4);
+    pl->timing[4] = el(4, 5);
+    pl->timing[5] = el(5, 6);
+  }
+  pl->timing[6] = el(6, 7);
+  return too_many ? HD_TOO_MANY_EVENTS : HD_NO_ERROR;
+}
+
+void hd_destroy_pipeline(hd_pipeline pl) {
+  if (!pl) return;
+  cudaSetDevice(pl->device);
+  delete pl;
+}
+
+hd_error hd_clean_filterbank_rfi(hd_pipeline pl, const hd_byte* h_in, hd_size nsamps,
+                                 hd_size nbits, hd_byte* h_out, int* h_mask, hd_float dt,
+                                 hd_float baseline_length, hd_float rfi_tol, hd_size boxcar_max,
+                                 hd_size nbeams) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!h_in || !h_out) return HD_INVALID_POINTER;
+  if (nbits != 8) return HD_INVALID_NBITS;
+  const size_t C = pl->params.nchans;
+  if (C % 4 != 0 || nbeams == 0) return HD_INVALID_STRIDE;
+  cudaSetDevice(pl->device);
+  cudaStream_t s = pl->stream;
+  HD_TRY(pl->fb_tf.ensure(nsamps * C));
+  HD_TRY(pl->fb_tf_clean.ensure(nsamps * C));
+  HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_in, nsamps * C, cudaMemcpyHostToDevice, s));
+  hd_error he = clean_device(pl, nsamps, C, dt, baseline_length, rfi_tol, boxcar_max, nbeams,
+                             nullptr, 0, pl->fb_tf_clean.as<uint8_t>());
+  if (he != HD_NO_ERROR) return he;
+  HD_TRY(cudaMemcpyAsync(h_out, pl->fb_tf_clean.p, nsamps * C, cudaMemcpyDeviceToHost, s));
+  if (h_mask)
+    HD_TRY(cudaMemcpyAsync(h_mask, pl->mask.p, nsamps * sizeof(int), cudaMemcpyDeviceToHost, s));
+  HD_TRY(cudaStreamSynchronize(s));
+  return HD_NO_ERROR;
+}
+
+hd_error hd_get_candidates(hd_pipeline pl, hd_candidate* out, hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!count) return HD_INVALID_POINTER;
+  size_t n = std::min(*count, pl->cands.size());
+  if (out && n) std::memcpy(out, pl->cands.data(), n * sizeof(hd_candidate));
+  *count = pl->cands.size();
+  return HD_NO_ERROR;
+}
+
+hd_error hd_get_giants(hd_pipeline pl, hd_float* peaks, hd_size* inds, hd_size* begins,
+                       hd_size* ends, hd_size* filter_inds, hd_size* dm_inds, hd_size* labels,
+                       hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!count) return HD_INVALID_POINTER;
+  size_t n = std::min(*count, pl->g_peaks.size());
+  if (peaks) std::memcpy(peaks, pl->g_peaks.data(), n * sizeof(float));
+  if (inds) std::memcpy(inds, pl->g_inds.data(), n * sizeof(hd_size));
+  if (begins) std::memcpy(begins, pl->g_begins.data(), n * sizeof(hd_size));
+  if (ends) std::memcpy(ends, pl->g_ends.data(), n * sizeof(hd_size));
+  if (filter_inds) std::memcpy(filter_inds, pl->g_filters.data(), n * sizeof(hd_size));
+  if (dm_inds) std::memcpy(dm_inds, pl->g_dms.data(), n * sizeof(hd_size));
+  if (labels) std::memcpy(labels, pl->g_labels.data(), n * sizeof(hd_size));
+  *count = pl->g_peaks.size();
+  return HD_NO_ERROR;
+}
+
+hd_error hd_get_timing(hd_pipeline pl, float* ms, int n) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!ms) return HD_INVALID_POINTER;
+  for (int i = 0; i < n && i < 8; i++) ms[i] = pl->timing[i];
+  return HD_NO_ERROR;
+}
+
+}  // extern "C"

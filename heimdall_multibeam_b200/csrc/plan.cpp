@@ -1,0 +1,391 @@
+// plan.cpp -- the dedisp_* C interface (include/dedisp.h) on sm_100a kernels.
+//
+// Plan semantics follow the reference's call sites (Pipeline/pipeline.cu:
+// 171-196,335-365,453-462,493; clean_filterbank_rfi.cu:361-397) with the
+// documented restatement of the external dedisp library: float delay table
+// with K = 4148.808, delays rounded half up, exact integer channel sums
+// written as float.
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "internal.h"
+
+namespace hdb {
+
+void delay_table(size_t nchans, float dt, float f0, float df, float* table) {
+  const float K = 4148.808f;
+  float b = 1.0f / f0;
+  for (size_t c = 0; c < nchans; c++) {
+    float fc = f0 + (float)c * df;
+    float a = 1.0f / fc;
+    table[c] = K * (a * a - b * b) / dt;
+  }
+}
+
+size_t delay_of(float dm, float table_c) {
+  float v = dm * table_c + 0.5f;
+  if (!(v > 0.0f)) return 0;
+  return (size_t)v;
+}
+
+// DM trial spacing for a smearing tolerance (dedisp's generator, golden
+// vector Share/dm2000.list).  With times in microseconds, trial p has width
+//   W(p)^2 = dt^2 + ti^2 + (a p)^2,  a = 8.3 df / f^3 (df MHz, f GHz, band
+// centre); the next trial x satisfies
+//   dt^2 + ti^2 + (a x)^2 + b^2 (x - p)^2 = tol^2 W(p)^2,  b = a nchans / 4,
+// whose positive root is taken.  Trials are stored as float and the stored
+// value seeds the next step; generation stops at the first trial >= dm_end.
+std::vector<float> generate_dm_list(float dm_start, float dm_end, double dt, double ti,
+                                    double f0, double df, size_t nchans, double tol) {
+  double dt_us = dt * 1e6;
+  double f = (f0 + ((double)(nchans / 2) - 0.5) * df) * 1e-3;
+  double tol2 = tol * tol;
+  double a = 8.3 * df / (f * f * f);
+  double a2 = a * a;
+  double b2 = a2 * ((double)(nchans * nchans) / 16.0);
+  double c = (dt_us * dt_us + ti * ti) * (tol2 - 1.0);
+  std::vector<float> out;
+  out.push_back(dm_start);
+  while (out.back() < dm_end && out.size() < (1u << 20)) {
+    double p = (double)out.back();
+    double k = c + tol2 * a2 * p * p;
+    double x = (b2 * p + std::sqrt(-a2 * b2 * p * p + (a2 + b2) * k)) / (a2 + b2);
+    out.push_back((float)x);
+  }
+  return out;
+}
+
+static void free_dev(void* p) {
+  if (p) cudaFree(p);
+}
+
+dedisp_error plan_prepare(dedisp_plan p) {
+  if (!p->dirty) return DEDISP_NO_ERROR;
+  if (p->dm_list.empty()) return DEDISP_NO_DM_LIST_SET;
+  const size_t D = p->dm_list.size(), C = p->nchans;
+  const int DB = dedisp_dm_block();
+  const size_t nblk = (D + DB - 1) / DB;
+  p->delays.assign(D * C, 0);
+  p->max_delay = 0;
+  for (size_t d = 0; d < D; d++)
+    for (size_t c = 0; c < C; c++) {
+      size_t v = delay_of(p->dm_list[d], p->table[c]);
+      if (v > (size_t)0x3FFFFFFF) return DEDISP_TOO_FEW_NSAMPS;
+      p->delays[d * C + c] = (int)v;
+      p->max_delay = std::max(p->max_delay, v);
+    }
+  p->blk_min.assign(nblk * C, 0);
+  p->max_span = 0;
+  for (size_t b = 0; b < nblk; b++)
+    for (size_t c = 0; c < C; c++) {
+      int lo = 0x7FFFFFFF, hi = 0;
+      for (size_t d = b * DB; d < std::min(D, (b + 1) * DB); d++) {
+        lo = std::min(lo, p->delays[d * C + c]);
+        hi = std::max(hi, p->delays[d * C + c]);
+      }
+      p->blk_min[b * C + c] = lo;
+      p->max_span = std::max(p->max_span, (size_t)(hi - lo));
+    }
+  p->active.clear();
+  for (size_t c = 0; c < C; c++)
+    if (p->killmask[c]) p->active.push_back((int)c);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  free_dev(p->d_delays); free_dev(p->d_blk_min); free_dev(p->d_active); free_dev(p->d_dm_list);
+  p->d_delays = nullptr; p->d_blk_min = nullptr; p->d_active = nullptr; p->d_dm_list = nullptr;
+  if (cudaMalloc(&p->d_delays, p->delays.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&p->d_blk_min, p->blk_min.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&p->d_active, (p->active.size() + 1) * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&p->d_dm_list, D * sizeof(float)) != cudaSuccess)
+    return DEDISP_MEM_ALLOC_FAILED;
+  if (!p->d_err && cudaMalloc(&p->d_err, sizeof(unsigned)) != cudaSuccess)
+    return DEDISP_MEM_ALLOC_FAILED;
+  cudaMemset(p->d_err, 0, sizeof(unsigned));
+  if (cudaMemcpy(p->d_delays, p->delays.data(), p->delays.size() * sizeof(int),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p->d_blk_min, p->blk_min.data(), p->blk_min.size() * sizeof(int),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      (!p->active.empty() &&
+       cudaMemcpy(p->d_active, p->active.data(), p->active.size() * sizeof(int),
+                  cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(p->d_dm_list, p->dm_list.data(), D * sizeof(float), cudaMemcpyHostToDevice) !=
+          cudaSuccess)
+    return DEDISP_MEM_COPY_FAILED;
+  p->device = dev;
+  p->dirty = false;
+  return DEDISP_NO_ERROR;
+}
+
+static int rowb_of(const dedisp_plan p) {
+  size_t tb = (size_t)dedisp_time_block();
+  size_t r = p->max_span + 16 + tb + 8;
+  return (int)((r + 15) & ~(size_t)15);
+}
+
+size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
+  size_t tb = (size_t)dedisp_time_block();
+  size_t nout = nsamps > p->max_delay ? nsamps - p->max_delay : 0;
+  size_t ntb = (nout + tb - 1) / tb;
+  size_t need = std::max(nsamps + 4, ntb * tb + p->max_delay + (size_t)rowb_of(p)) + 64;
+  return (need + 63) & ~(size_t)63;
+}
+
+dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch, size_t nsamps,
+                                float* d_out, size_t out_pitch, cudaStream_t s) {
+  dedisp_error de = plan_prepare(p);
+  if (de != DEDISP_NO_ERROR) return de;
+  if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
+  size_t nout = nsamps - p->max_delay;
+  if (nout == 0) return DEDISP_NO_ERROR;
+  if (p->active.empty()) {
+    for (size_t d = 0; d < p->dm_list.size(); d++)
+      if (cudaMemsetAsync(d_out + d * out_pitch, 0, nout * sizeof(float), s) != cudaSuccess)
+        return DEDISP_INTERNAL_GPU_ERROR;
+    return DEDISP_NO_ERROR;
+  }
+  DedispArgs a;
+  a.in = d_ft;
+  a.in_pitch = pitch;
+  a.delays = p->d_delays;
+  a.blk_min = p->d_blk_min;
+  a.chans = p->d_active;
+  a.nact = (int)p->active.size();
+  a.nchans = (int)p->nchans;
+  a.dm_count = (int)p->dm_list.size();
+  a.nout = nout;
+  a.out = d_out;
+  a.out_pitch = out_pitch;
+  a.rowb = rowb_of(p);
+  a.err = p->d_err;
+  if (dedisp_smem_bytes(a.rowb) > 200 * 1024) return DEDISP_NCHANS_EXCEEDS_LIMIT;
+  if (launch_dedisp(a, s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
+  return DEDISP_NO_ERROR;
+}
+
+}  // namespace hdb
+
+dedisp_plan_struct::~dedisp_plan_struct() {
+  hdb::free_dev(d_delays);
+  hdb::free_dev(d_blk_min);
+  hdb::free_dev(d_active);
+  hdb::free_dev(d_dm_list);
+  hdb::free_dev(d_err);
+  hdb::free_dev(d_in_tf);
+  hdb::free_dev(d_in_ft);
+  hdb::free_dev(d_out);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// ===========================================================================
+// C interface
+// ===========================================================================
+extern "C" {
+
+dedisp_error dedisp_create_plan(dedisp_plan* plan, dedisp_size nchans, dedisp_float dt,
+                                dedisp_float f0, dedisp_float df) {
+  if (!plan) return DEDISP_INVALID_POINTER;
+  *plan = nullptr;
+  if (nchans == 0) return DEDISP_NCHANS_EXCEEDS_LIMIT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DEDISP_PRIOR_GPU_ERROR;
+  dedisp_plan p = new (std::nothrow) dedisp_plan_struct();
+  if (!p) return DEDISP_MEM_ALLOC_FAILED;
+  p->nchans = nchans;
+  p->dt = dt;
+  p->f0 = f0;
+  p->df = df;
+  p->table.resize(nchans);
+  hdb::delay_table(nchans, dt, f0, df, p->table.data());
+  p->killmask.assign(nchans, 1);
+  *plan = p;
+  return DEDISP_NO_ERROR;
+}
+
+void dedisp_destroy_plan(dedisp_plan plan) { delete plan; }
+
+dedisp_error dedisp_set_dm_list(dedisp_plan p, const dedisp_float* l, dedisp_size n) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  if (!l) return DEDISP_INVALID_POINTER;
+  p->dm_list.assign(l, l + n);
+  p->dt_factors.assign(n, 1);
+  p->dirty = true;
+  return DEDISP_NO_ERROR;
+}
+
+dedisp_error dedisp_generate_dm_list(dedisp_plan p, dedisp_float a, dedisp_float b,
+                                     dedisp_float ti, dedisp_float tol) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  p->dm_list = hdb::generate_dm_list(a, b, p->dt, ti, p->f0, p->df, p->nchans, tol);
+  p->dt_factors.assign(p->dm_list.size(), 1);
+  p->dirty = true;
+  return DEDISP_NO_ERROR;
+}
+
+static thread_local std::vector<float> g_guru;
+const dedisp_float* dedisp_generate_dm_list_guru(dedisp_float a, dedisp_float b, double dt,
+                                                 double ti, double f0, double df,
+                                                 dedisp_size nchans, double tol,
+                                                 dedisp_size* count) {
+  g_guru = hdb::generate_dm_list(a, b, dt, ti, f0, df, nchans, tol);
+  if (count) *count = g_guru.size();
+  return g_guru.data();
+}
+
+dedisp_error dedisp_set_killmask(dedisp_plan p, const dedisp_bool* km) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  for (size_t c = 0; c < p->nchans; c++) p->killmask[c] = km ? (km[c] != 0) : 1;
+  p->dirty = true;
+  return DEDISP_NO_ERROR;
+}
+
+// Adaptive time resolution is not provided: the search is run at the native
+// sampling time for every DM (the reference's use_scrunching = 0 path).
+dedisp_error dedisp_enable_adaptive_dt(dedisp_plan p, dedisp_float w, dedisp_float tol) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  (void)w; (void)tol;
+  return DEDISP_INVALID_FLAG_COMBINATION;
+}
+
+dedisp_error dedisp_disable_adaptive_dt(dedisp_plan p) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  p->adaptive = false;
+  return DEDISP_NO_ERROR;
+}
+
+dedisp_size dedisp_get_dm_count(const dedisp_plan p) { return p ? p->dm_list.size() : 0; }
+const dedisp_float* dedisp_get_dm_list(const dedisp_plan p) {
+  return (p && !p->dm_list.empty()) ? p->dm_list.data() : nullptr;
+}
+const dedisp_size* dedisp_get_dt_factors(const dedisp_plan p) {
+  return (p && !p->dt_factors.empty()) ? p->dt_factors.data() : nullptr;
+}
+dedisp_size dedisp_get_max_delay(const dedisp_plan p) {
+  if (!p || p->dm_list.empty()) return 0;
+  size_t m = 0;
+  for (float dm : p->dm_list)
+    for (size_t c = 0; c < p->nchans; c++) m = std::max(m, hdb::delay_of(dm, p->table[c]));
+  return m;
+}
+dedisp_size dedisp_get_dm_delay(const dedisp_plan p, int d) {
+  if (!p || d < 0 || (size_t)d >= p->dm_list.size()) return 0;
+  size_t m = 0;
+  for (size_t c = 0; c < p->nchans; c++) m = std::max(m, hdb::delay_of(p->dm_list[d], p->table[c]));
+  return m;
+}
+dedisp_size dedisp_get_channel_count(const dedisp_plan p) { return p ? p->nchans : 0; }
+dedisp_float dedisp_get_dt(const dedisp_plan p) { return p ? p->dt : 0.f; }
+dedisp_float dedisp_get_f0(const dedisp_plan p) { return p ? p->f0 : 0.f; }
+dedisp_float dedisp_get_df(const dedisp_plan p) { return p ? p->df : 0.f; }
+
+dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const dedisp_byte* in,
+                                dedisp_size in_nbits, dedisp_size in_stride, dedisp_byte* out,
+                                dedisp_size out_nbits, dedisp_size out_stride, unsigned flags) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  if (!in || !out) return DEDISP_INVALID_POINTER;
+  if (p->dm_list.empty()) return DEDISP_NO_DM_LIST_SET;
+  if (in_nbits != 8) return DEDISP_UNSUPPORTED_IN_NBITS;
+  if (out_nbits != 32) return DEDISP_UNSUPPORTED_OUT_NBITS;
+  if (in_stride != p->nchans || (p->nchans % 4) != 0) return DEDISP_INVALID_STRIDE;
+  if (out_stride % 4) return DEDISP_INVALID_STRIDE;
+  dedisp_error de = hdb::plan_prepare(p);
+  if (de != DEDISP_NO_ERROR) return de;
+  if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
+  const size_t nout = nsamps - p->max_delay;
+  const size_t D = p->dm_list.size();
+  if (out_stride / 4 < nout) return DEDISP_INVALID_STRIDE;
+  if (!p->stream && cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return DEDISP_PRIOR_GPU_ERROR;
+  cudaStream_t s = p->stream;
+  const size_t pitch = hdb::ft_pitch(p, nsamps);
+  const bool dev_ptrs = (flags & DEDISP_DEVICE_POINTERS) != 0;
+  const uint8_t* d_tf = in;
+  if (!dev_ptrs) {
+    size_t need = nsamps * p->nchans;
+    if (p->d_in_tf_cap < need) {
+      hdb::free_dev(p->d_in_tf);
+      p->d_in_tf = nullptr;
+      if (cudaMalloc(&p->d_in_tf, need) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
+      p->d_in_tf_cap = need;
+    }
+    if (cudaMemcpyAsync(p->d_in_tf, in, need, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return DEDISP_MEM_COPY_FAILED;
+    d_tf = p->d_in_tf;
+  }
+  size_t need_ft = pitch * p->nchans;
+  if (p->d_in_ft_cap < need_ft) {
+    hdb::free_dev(p->d_in_ft);
+    p->d_in_ft = nullptr;
+    if (cudaMalloc(&p->d_in_ft, need_ft) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
+    cudaMemsetAsync(p->d_in_ft, 0, need_ft, s);
+    p->d_in_ft_cap = need_ft;
+  }
+  if (hdb::launch_transpose_tf_ft(d_tf, nsamps, (int)p->nchans, p->d_in_ft, pitch, s) !=
+      cudaSuccess)
+    return DEDISP_INTERNAL_GPU_ERROR;
+  float* d_o = reinterpret_cast<float*>(out);
+  size_t opitch = out_stride / 4;
+  if (!dev_ptrs) {
+    opitch = (nout + 3) & ~(size_t)3;
+    size_t need = opitch * D;
+    if (p->d_out_cap < need) {
+      hdb::free_dev(p->d_out);
+      p->d_out = nullptr;
+      if (cudaMalloc(&p->d_out, need * sizeof(float)) != cudaSuccess)
+        return DEDISP_MEM_ALLOC_FAILED;
+      p->d_out_cap = need;
+    }
+    d_o = p->d_out;
+  } else if (opitch % 4) {
+    return DEDISP_INVALID_STRIDE;
+  }
+  de = hdb::plan_dedisperse_ft(p, p->d_in_ft, pitch, nsamps, d_o, opitch, s);
+  if (de != DEDISP_NO_ERROR) return de;
+  if (!dev_ptrs) {
+    if (cudaMemcpy2DAsync(out, out_stride, d_o, opitch * sizeof(float), nout * sizeof(float), D,
+                          cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return DEDISP_MEM_COPY_FAILED;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
+  unsigned err = 0;
+  cudaMemcpy(&err, p->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (err) return DEDISP_INTERNAL_GPU_ERROR;
+  return DEDISP_NO_ERROR;
+}
+
+dedisp_error dedisp_execute(const dedisp_plan p, dedisp_size nsamps, const dedisp_byte* in,
+                            dedisp_size in_nbits, dedisp_byte* out, dedisp_size out_nbits,
+                            unsigned flags) {
+  if (!p) return DEDISP_INVALID_PLAN;
+  dedisp_size md = dedisp_get_max_delay(p);
+  if (nsamps < md) return DEDISP_TOO_FEW_NSAMPS;
+  return dedisp_execute_adv(p, nsamps, in, in_nbits, p->nchans * in_nbits / 8, out, out_nbits,
+                            (nsamps - md) * out_nbits / 8, flags);
+}
+
+const char* dedisp_get_error_string(dedisp_error e) {
+  switch (e) {
+    case DEDISP_NO_ERROR: return "No error";
+    case DEDISP_MEM_ALLOC_FAILED: return "Memory allocation failed";
+    case DEDISP_MEM_COPY_FAILED: return "Memory copy failed";
+    case DEDISP_NCHANS_EXCEEDS_LIMIT: return "No. channels exceeds internal limit";
+    case DEDISP_INVALID_PLAN: return "Invalid plan";
+    case DEDISP_INVALID_POINTER: return "Invalid pointer";
+    case DEDISP_INVALID_STRIDE: return "Invalid stride";
+    case DEDISP_NO_DM_LIST_SET: return "No DM list has been set";
+    case DEDISP_TOO_FEW_NSAMPS: return "No. samples < maximum delay";
+    case DEDISP_INVALID_FLAG_COMBINATION: return "Invalid flag combination";
+    case DEDISP_UNSUPPORTED_IN_NBITS: return "Unsupported in_nbits value";
+    case DEDISP_UNSUPPORTED_OUT_NBITS: return "Unsupported out_nbits value";
+    case DEDISP_INVALID_DEVICE_INDEX: return "Invalid device index";
+    case DEDISP_DEVICE_ALREADY_SET: return "Device is already set and cannot be changed";
+    case DEDISP_PRIOR_GPU_ERROR: return "Prior GPU error.";
+    case DEDISP_INTERNAL_GPU_ERROR: return "Internal GPU error.";
+    default: return "Unknown error";
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// plan.h -- host-side dedispersion plan shared by the dedisp_* C interface and
+// the hd_* pipeline.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "dedisp.h"
+
+struct dedisp_plan_struct {
+  dedisp_size nchans = 0;
+  float dt = 0.f, f0 = 0.f, df = 0.f;
+  std::vector<float> table;       // delay per unit DM per channel (samples)
+  std::vector<float> dm_list;
+  std::vector<int> killmask;
+  std::vector<dedisp_size> dt_factors;
+  bool adaptive = false;
+  float adaptive_width = 0.f, adaptive_tol = 0.f;
+
+  // derived / device state (rebuilt lazily when the list or killmask change)
+  bool dirty = true;
+  std::vector<int> delays;         // [dm][chan]
+  std::vector<int> blk_min;        // [dm block][chan]
+  std::vector<int> active;         // channels with killmask != 0
+  size_t max_delay = 0;
+  size_t max_span = 0;             // max over blocks/chans of (max - min) delay
+  int* d_delays = nullptr;
+  int* d_blk_min = nullptr;
+  int* d_active = nullptr;
+  float* d_dm_list = nullptr;
+  unsigned* d_err = nullptr;
+  int device = -1;
+
+  // scratch for dedisp_execute* with host pointers
+  uint8_t* d_in_tf = nullptr;
+  size_t d_in_tf_cap = 0;
+  uint8_t* d_in_ft = nullptr;
+  size_t d_in_ft_cap = 0;
+  float* d_out = nullptr;
+  size_t d_out_cap = 0;
+  cudaStream_t stream = nullptr;
+
+  ~dedisp_plan_struct();
+};
+
+namespace hdb {
+
+// include/dedisp.h restatement (float arithmetic as documented there).
+void delay_table(size_t nchans, float dt, float f0, float df, float* table);
+size_t delay_of(float dm, float table_c);
+std::vector<float> generate_dm_list(float dm_start, float dm_end, double dt, double ti,
+                                    double f0, double df, size_t nchans, double tol);
+
+// Recomputes delays, block minima, active channels and uploads them.
+dedisp_error plan_prepare(dedisp_plan p);
+
+// Pitch (bytes) of the channel-major working copy for nsamps samples.
+size_t ft_pitch(const dedisp_plan p, size_t nsamps);
+
+// Dedisperses the FT copy already on the device into out (device floats).
+dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch, size_t nsamps,
+                                float* d_out, size_t out_pitch, cudaStream_t s);
+
+}  // namespace hdb

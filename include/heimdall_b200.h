@@ -1,0 +1,188 @@
+/*
+ * heimdall_b200.h -- C interface of the B200 single-pulse search library
+ * (libhdb200.so).
+ *
+ * Drop-in for Heimdall's pipeline API.  Each declaration below replaces the
+ * reference interface cited beside it with the same name, argument meaning,
+ * error codes and ownership rules:
+ *
+ *   Pipeline/hd/types.h:12-48           hd_byte/hd_size/hd_float, hd_pipeline,
+ *                                       hd_range_t
+ *   Pipeline/hd/params.h:19-78          struct hd_params (same fields, order)
+ *   Pipeline/hd/error.h:19-41           hd_error codes, hd_get_error_string
+ *   Pipeline/hd/pipeline.h:10-28        hd_create_pipeline, hd_preallocate,
+ *                                       hd_get_max_overlap, hd_execute,
+ *                                       hd_destroy_pipeline
+ *   Pipeline/hd/default_params.h:16     hd_set_default_params
+ *   Pipeline/hd/parse_command_line.h:16-17  hd_parse_command_line, hd_print_usage
+ *   Pipeline/hd/clean_filterbank_rfi.h  hd_clean_filterbank_rfi
+ *
+ * Additions (no reference counterpart; the reference only writes candidates to
+ * a .cand file or a socket): hd_set_cleaning, hd_get_candidates, hd_get_giants,
+ * hd_get_timing.
+ *
+ * Ownership and threading: the caller owns every host buffer it passes; the
+ * pipeline owns all device memory, its CUDA stream and events.  A pipeline
+ * object is used by one thread at a time; separate pipelines are independent
+ * (no global state), so one pipeline per thread or per GPU is safe.
+ *
+ * The struct layout of hd_params depends on HAVE_PSRDADA exactly as in the
+ * reference: build the library and the caller with the same setting.
+ */
+#ifndef HEIMDALL_B200_H
+#define HEIMDALL_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <time.h>
+#ifdef HAVE_PSRDADA
+#include <sys/types.h>
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef unsigned char          hd_byte;
+typedef size_t                 hd_size;
+typedef float                  hd_float;
+typedef struct hd_pipeline_t*  hd_pipeline;
+
+typedef struct hd_range {
+  hd_size start;
+  hd_size end;
+} hd_range_t;
+
+struct hd_params {
+  int          verbosity;
+#ifdef HAVE_PSRDADA
+  key_t        dada_id;
+#endif
+  const char*  sigproc_file;
+  bool         yield_cpu;
+  hd_size      nsamps_gulp;
+  hd_size      dm_gulp_size;
+  hd_float     baseline_length;     /* seconds */
+  hd_size      beam;                /* 0-based index of the first beam */
+  hd_size      nbeams;
+  bool         override_beam;
+  hd_size      nchans;
+  hd_float     dt;                  /* seconds */
+  hd_float     f0;                  /* MHz, channel 0 */
+  hd_float     df;                  /* MHz per channel */
+  hd_float     dm_min;
+  hd_float     dm_max;
+  hd_float     dm_tol;
+  hd_float     dm_pulse_width;      /* microseconds */
+  hd_size      dm_nbits;
+  bool         use_scrunching;
+  hd_float     scrunch_tol;
+  hd_float     rfi_tol;
+  hd_size      rfi_min_beams;
+  hd_size      boxcar_max;
+  hd_float     detect_thresh;
+  hd_size      cand_sep_time;
+  hd_size      cand_sep_filter;
+  hd_size      cand_sep_dm;
+  hd_size      cand_rfi_dm_cut;
+  hd_float     max_giant_rate;
+  hd_size      min_tscrunch_width;
+  const char*  coincidencer_host;
+  int          coincidencer_port;
+  unsigned int num_channel_zaps;
+  hd_range_t*  channel_zaps;
+  hd_size      beam_count;
+  int          gpu_id;
+  time_t       utc_start;
+  hd_size      spectra_per_second;
+  const char*  output_dir;
+};
+
+typedef int hd_error;
+enum {
+  HD_NO_ERROR = 0,
+  HD_MEM_ALLOC_FAILED,
+  HD_MEM_COPY_FAILED,
+  HD_INVALID_DEVICE_INDEX,
+  HD_DEVICE_ALREADY_SET,
+  HD_INVALID_PIPELINE,
+  HD_INVALID_POINTER,
+  HD_INVALID_STRIDE,
+  HD_INVALID_NBITS,
+  HD_PRIOR_GPU_ERROR,
+  HD_INTERNAL_GPU_ERROR,
+  HD_TOO_FEW_NSAMPS,
+  HD_TOO_MANY_EVENTS,
+  HD_UNKNOWN_ERROR
+};
+
+const char* hd_get_error_string(hd_error error);
+
+void hd_set_default_params(struct hd_params* params);
+int  hd_parse_command_line(int argc, char* argv[], struct hd_params* params);
+void hd_print_usage(void);
+
+hd_error hd_create_pipeline(hd_pipeline* pipeline, struct hd_params params);
+hd_error hd_preallocate(hd_pipeline pipeline, hd_size nsamps, hd_size nbeams);
+hd_size  hd_get_max_overlap(hd_pipeline pipeline, hd_size nbeams);
+/* One gulp: nsamps spectra (nbeams beams of nsamps/nbeams spectra each, time
+ * concatenated) of nchans*nbits/8 bytes.  Candidates go to
+ * <output_dir>/<UTC>_<beam+1>.cand as in Pipeline/pipeline.cu:1001-1044
+ * (output_dir == NULL: no file).  Returns HD_TOO_MANY_EVENTS (soft) when the
+ * giant rate exceeds max_giant_rate. */
+hd_error hd_execute(hd_pipeline pipeline, const hd_byte* h_filterbank, hd_size nsamps,
+                    hd_size nbits, hd_size first_idx, hd_size nbeams,
+                    hd_size* nsamps_processed);
+void     hd_destroy_pipeline(hd_pipeline pipeline);
+
+/* Zero-DM RFI excision of Pipeline/clean_filterbank_rfi.cu:256-528 on host
+ * buffers (8-bit data): h_out receives the cleaned filterbank, h_mask (may be
+ * NULL) the per-spectrum RFI mask. */
+hd_error hd_clean_filterbank_rfi(hd_pipeline pipeline, const hd_byte* h_in, hd_size nsamps,
+                                 hd_size nbits, hd_byte* h_out, int* h_mask,
+                                 hd_float dt, hd_float baseline_length, hd_float rfi_tol,
+                                 hd_size boxcar_max, hd_size nbeams);
+
+/* ---- additions ---------------------------------------------------------- */
+
+/* Switches the zero-DM RFI cleaning stage on (default) or off.  The reference
+ * selects it at compile time (Pipeline/pipeline.cu:72-74,255-299, #ifdef
+ * CLEANING); its shipped build leaves it off. */
+hd_error hd_set_cleaning(hd_pipeline pipeline, int enable);
+
+/* One row of the .cand file (Pipeline/pipeline.cu:1028-1038). */
+typedef struct hd_candidate {
+  hd_float snr;
+  hd_size  samp_idx;
+  hd_float time;
+  hd_size  filter;
+  hd_size  dm_trial;
+  hd_float dm;
+  hd_size  members;
+  hd_size  begin;
+  hd_size  end;
+  hd_size  beam;
+} hd_candidate;
+
+/* Candidates of the last hd_execute, in .cand order.  Copies
+ * min(*count, available) rows into out (out may be NULL to query) and sets
+ * *count to the number available. */
+hd_error hd_get_candidates(hd_pipeline pipeline, hd_candidate* out, hd_size* count);
+
+/* Every giant of the last hd_execute in detection order (DM, width, time),
+ * before clustering, with its cluster label (the index of the cluster's first
+ * giant).  Any pointer may be NULL. */
+hd_error hd_get_giants(hd_pipeline pipeline, hd_float* peaks, hd_size* inds, hd_size* begins,
+                       hd_size* ends, hd_size* filter_inds, hd_size* dm_inds,
+                       hd_size* labels, hd_size* count);
+
+/* Device time of the last hd_execute per stage, milliseconds (CUDA events):
+ * [0] total, [1] clean, [2] dedisperse, [3] baseline+normalise+scan,
+ * [4] boxcar+threshold, [5] giants, [6] cluster+merge, [7] host->device copy. */
+hd_error hd_get_timing(hd_pipeline pipeline, float* ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HEIMDALL_B200_H */

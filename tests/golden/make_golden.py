@@ -1,0 +1,17 @@
+"""Regenerates the golden fixtures in this folder from the reference tree.
+
+dm2000.list is the reference's only shipped golden vector (Share/dm2000.list):
+the DM trials of its dedisp generator for the default search setup.  It is
+copied verbatim; nothing else is derived here.  Run from the repository root
+where the reference tree is available:
+
+    python tests/golden/make_golden.py /root/reference
+"""
+import os
+import shutil
+import sys
+
+ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+here = os.path.dirname(os.path.abspath(__file__))
+shutil.copyfile(os.path.join(ref, "Share", "dm2000.list"), os.path.join(here, "dm2000.list"))
+print("wrote", os.path.join(here, "dm2000.list"))

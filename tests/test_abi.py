@@ -1,0 +1,101 @@
+"""The C-ABI boundary: the library loads, exports every function the headers
+declare, and the Python mirror's struct layouts match the C compiler's."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+import heimdall_multibeam_b200 as hdb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in ("heimdall_b200.h", "dedisp.h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b((?:hd|dedisp)_[a-z0-9_]+)\s*\(", src):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol(hdb):
+    L = hdb.lib()
+    declared = declared_functions()
+    assert len(declared) >= 30
+    missing = [n for n in sorted(declared) if not hasattr(L, n)]
+    assert not missing, missing
+    assert declared == set(hdb.SYMBOLS), declared ^ set(hdb.SYMBOLS)
+
+
+def _c_layout(struct, fields):
+    body = "\n".join(f'  printf("%zu %zu\\n", offsetof({struct}, {f}), sizeof(((({struct}*)0))->{f}));'
+                     for f in fields)
+    prog = f"""#include <stdio.h>
+#include <stddef.h>
+#include "heimdall_b200.h"
+int main(void) {{
+  printf("%zu\\n", sizeof({struct}));
+{body}
+  return 0;
+}}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "l.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "l")
+        subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe],
+                       check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    size = int(out[0])
+    lay = [tuple(int(x) for x in ln.split()) for ln in out[1:] if ln.strip()]
+    return size, lay
+
+
+@pytest.mark.parametrize("cls,cname", [(hdb.HdParams, "struct hd_params"),
+                                       (hdb.HdCandidate, "hd_candidate")])
+def test_struct_layout_matches_c(cls, cname):
+    fields = [f for f, _ in cls._fields_]
+    size, lay = _c_layout(cname, fields)
+    assert size == C.sizeof(cls)
+    for (f, t), (off, sz) in zip(cls._fields_, lay):
+        assert getattr(cls, f).offset == off, f
+        assert C.sizeof(t) == sz, f
+
+
+def test_candidate_dtype_matches_struct():
+    assert hdb.CANDIDATE_DTYPE.itemsize == C.sizeof(hdb.HdCandidate)
+    for f, _ in hdb.HdCandidate._fields_:
+        assert hdb.CANDIDATE_DTYPE.fields[f][1] == getattr(hdb.HdCandidate, f).offset
+
+
+def test_default_params_and_errors(hdb):
+    p = hdb.default_params()
+    assert p.nchans == 1024 and p.boxcar_max == 4096 and abs(p.detect_thresh - 6.0) < 1e-6
+    assert p.cand_sep_dm == 200 and p.min_tscrunch_width == 4096
+    assert hdb.error_string(hdb.HD_TOO_MANY_EVENTS) == "Too many events"
+    assert hdb.error_string(hdb.HD_TOO_FEW_NSAMPS) == "No. samples < maximum delay"
+
+
+def test_parse_command_line(hdb):
+    L = hdb.lib()
+    p = hdb.default_params()
+    args = [b"heimdall", b"-f", b"x.fil", b"-dm", b"10", b"500", b"-boxcar_max", b"1024",
+            b"-zap_chans", b"5", b"9", b"-V", b"-beam", b"3"]
+    argv = (C.c_char_p * len(args))(*args)
+    assert L.hd_parse_command_line(len(args), argv, C.byref(p)) == 0
+    assert p.dm_min == 10.0 and p.dm_max == 500.0 and p.boxcar_max == 1024
+    assert p.num_channel_zaps == 1 and p.channel_zaps[0].start == 5 and p.channel_zaps[0].end == 9
+    assert p.verbosity == 2 and p.beam == 2 and p.override_beam
+
+
+def test_dm_list_guru_matches_golden(hdb):
+    """The product's generator reproduces Share/dm2000.list (host code, no GPU)."""
+    golden = open(os.path.join(ROOT, "tests", "golden", "dm2000.list")).read().split()
+    dms = hdb.dm_list_guru(0.0, 2000.0, 64e-6, 40.0, 1581.804688, -0.390625, 1024, 1.25)
+    assert ["%g" % float(x) for x in dms[1:]] == golden

@@ -1,0 +1,154 @@
+"""GPU parity: the CUDA product (through its C-ABI) against the oracle.
+
+Integer work (dedispersed sums, zapped filterbank, masks, giant indices,
+widths, DM indices, labels, counts) must be bit-exact.  Float SNRs are
+compared bit-exactly too: every float expression of the chain is evaluated in
+the reference's order on both sides (the 1e-4 relative bound of the
+specification is asserted as well, for the record)."""
+import os
+
+import numpy as np
+import pytest
+
+import heimdall_multibeam_b200 as H
+import oracle
+from heimdall_multibeam_b200 import synth
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+SNR_RTOL = 1e-4
+
+
+def _params(w, **kw):
+    d = dict(nchans=w.nchans, dt=w.dt, f0=w.f0, df=w.df, dm_min=w.dm_min, dm_max=w.dm_max,
+             boxcar_max=w.boxcar_max)
+    d.update(kw)
+    return d
+
+
+def _run_gpu(fb, nbeams=1, clean=True, zaps=(), **kw):
+    p = H.default_params(output_dir=None, **kw)
+    with H.Pipeline(p, cleaning=clean, channel_zaps=zaps) as pl:
+        err, proc = pl.execute(fb, nbeams=nbeams)
+        return err, proc, pl.candidates(), pl.giants()
+
+
+def _compare(fb, nbeams, w, clean, zaps=(), **kw):
+    pk = _params(w, **kw)
+    okw = dict(pk)
+    okw.pop("nchans")
+    r = oracle.execute(fb, nbeams=nbeams, clean=int(clean), channel_zaps=list(zaps), **okw)
+    err, proc, cands, g = _run_gpu(fb, nbeams=nbeams, clean=clean, zaps=zaps, **pk)
+    assert err == r["error"]
+    assert proc == r["nsamps_processed"]
+    og = r["giants"]
+    assert len(g["peaks"]) == len(og["peaks"])
+    for k in ("inds", "begins", "ends", "filter_inds", "dm_inds"):
+        np.testing.assert_array_equal(g[k], og[k], err_msg=k)
+    np.testing.assert_allclose(g["peaks"], og["peaks"], rtol=SNR_RTOL)
+    np.testing.assert_array_equal(g["peaks"].view(np.uint32), og["peaks"].view(np.uint32))
+    np.testing.assert_array_equal(g["labels"], r["labels"])
+    lines = oracle.cand_lines(r["groups"], fb.shape[0], nbeams, 0, r["nsamps_processed"],
+                              w.boxcar_max, w.dt)
+    assert H.cand_lines(cands) == lines
+    return cands
+
+
+def test_dedisp_bit_exact(hdb, oracle_lib):
+    rng = np.random.default_rng(5)
+    nchans, nsamps = 128, 20000
+    fb = rng.integers(0, 256, size=(nsamps, nchans), dtype=np.uint8)
+    plan = H.DedispPlan(nchans, 64e-6, 1500.0, -1.5625)
+    plan.generate_dm_list(0.0, 300.0, 40.0, 1.25)
+    dms = plan.dm_list
+    table = oracle.delay_table(nchans, 64e-6, 1500.0, -1.5625)
+    np.testing.assert_array_equal(
+        dms, oracle.dm_list(0.0, 300.0, 64e-6, 40.0, 1500.0, -1.5625, nchans, 1.25))
+    out = plan.execute(fb)
+    ref = oracle.dedisperse(fb, dms, table)
+    assert out.shape == ref.shape
+    np.testing.assert_array_equal(out, ref)
+    km = np.ones(nchans, np.int32)
+    km[[3, 17, 64, 65, 127]] = 0
+    plan.set_killmask(km)
+    np.testing.assert_array_equal(plan.execute(fb), oracle.dedisperse(fb, dms, table, km))
+
+
+def test_dedisp_odd_sizes(hdb, oracle_lib):
+    """Ragged sizes: channel count not a multiple of the staging chunk, DM
+    count not a multiple of the DM block, output length not a multiple of the
+    time block."""
+    rng = np.random.default_rng(9)
+    nchans, nsamps = 36, 7001
+    fb = rng.integers(0, 256, size=(nsamps, nchans), dtype=np.uint8)
+    plan = H.DedispPlan(nchans, 128e-6, 1400.0, -4.0)
+    dms = np.array([0.0, 3.0, 77.7, 150.0, 151.0, 299.0, 300.0], np.float32)
+    plan.set_dm_list(dms)
+    table = oracle.delay_table(nchans, 128e-6, 1400.0, -4.0)
+    np.testing.assert_array_equal(plan.execute(fb), oracle.dedisperse(fb, dms, table))
+
+
+def test_clean_bit_exact(hdb, oracle_lib):
+    w = synth.SEARCH_C1
+    b = synth.make_beam(1 << 15, 64, w.dt, w.f0, w.df * 16,
+                        [synth.Pulse(4000.0, 0.0, 0.5e-3, 40.0)], seed=3, n_bursts=6,
+                        rfi_chan_frac=0.05)
+    ref_out, ref_mask = oracle.clean_filterbank(b.data, w.dt)
+    assert ref_mask.sum() > 0
+    with H.Pipeline(H.default_params(nchans=64, output_dir=None)) as pl:
+        out, mask = pl.clean_filterbank_rfi(b.data, w.dt)
+    np.testing.assert_array_equal(mask, ref_mask)
+    np.testing.assert_array_equal(out, ref_out)
+
+
+@pytest.mark.parametrize("clean", [False, True])
+def test_execute_c0(hdb, oracle_lib, clean):
+    b = synth.make_c0()
+    cands = _compare(b.data, 1, synth.SEARCH_C0, clean)
+    assert len(cands) >= 3
+
+
+def test_execute_multibeam(hdb, oracle_lib):
+    w = synth.Workload("mb_small", 64, 655.36e-6, 851.0, -0.390625, 8192, 4, 0.0, 600.0, 256,
+                       False, "")
+    beams = synth.make_multibeam(w, seed=7, snr_lo=15, snr_hi=30)
+    _compare(synth.stf(beams), w.nbeams, w, True, baseline_length=1.0)
+
+
+def test_execute_zaps_and_rate(hdb, oracle_lib):
+    w = synth.SEARCH_C1
+    df = w.df * 8
+    pulses = [synth.Pulse(3000.0, 120.0, 1e-3, 25.0), synth.Pulse(9000.0, 400.0, 4e-3, 15.0)]
+    b = synth.make_beam(1 << 15, 128, w.dt, w.f0, df, pulses, seed=11, n_bursts=3)
+    kw = dict(df=df, dm_max=500.0, boxcar_max=256)
+    wl = synth.Workload("z", 128, w.dt, w.f0, df, 1 << 15, 1, 0.0, 500.0, 256, True, "")
+    cands = _compare(b.data, 1, wl, True, zaps=((10, 20), (100, 128)), **kw)
+    assert len(cands) >= 2
+    _compare(b.data, 1, wl, True, zaps=((10, 20), (100, 128)), max_giant_rate=1.0, **kw)
+
+
+def test_too_few_samples(hdb):
+    b = synth.make_c0()
+    err, proc, c, g = _run_gpu(b.data[:20000], **_params(synth.SEARCH_C0))
+    assert err == H.HD_TOO_FEW_NSAMPS and len(c) == 0
+
+
+def test_cand_file_written(hdb, tmp_path):
+    b = synth.make_c0()
+    p = H.default_params(output_dir=str(tmp_path), spectra_per_second=15625,
+                         **_params(synth.SEARCH_C0))
+    with H.Pipeline(p, cleaning=True) as pl:
+        pl.execute(b.data)
+        c = pl.candidates()
+    files = list(tmp_path.glob("*.cand"))
+    assert len(files) == 1 and files[0].name == "1970-01-01-00:00:00_01.cand"
+    assert files[0].read_text().splitlines() == H.cand_lines(c)
+
+
+@pytest.mark.slow
+def test_execute_c1_full(hdb, oracle_lib):
+    """Full survey-size gulp with RFI: 1024 channels, 2^18 samples, DM 0-2000,
+    boxcars to 4096 (the widest boxcar is time-scrunched)."""
+    b = synth.make_c1()
+    cands = _compare(b.data, 1, synth.SEARCH_C1, True)
+    assert len(cands) >= 20
