@@ -29,7 +29,7 @@ def _params(w, **kw):
 def _run_gpu(fb, nbeams=1, clean=True, zaps=(), **kw):
     p = H.default_params(output_dir=None, **kw)
     with H.Pipeline(p, cleaning=clean, channel_zaps=zaps) as pl:
-        err, proc = pl.execute(fb, nbeams=nbeams)
+        err, proc = pl.execute(fb, nbeams=nbeams, raise_on_error=False)
         return err, proc, pl.candidates(), pl.giants()
 
 
@@ -41,6 +41,11 @@ def _compare(fb, nbeams, w, clean, zaps=(), **kw):
     err, proc, cands, g = _run_gpu(fb, nbeams=nbeams, clean=clean, zaps=zaps, **pk)
     assert err == r["error"]
     assert proc == r["nsamps_processed"]
+    if err == H.HD_TOO_MANY_EVENTS:
+        # the reference stops searching at the bail-out; only the (empty)
+        # candidate list is defined
+        assert len(cands) == 0
+        return cands
     og = r["giants"]
     assert len(g["peaks"]) == len(og["peaks"])
     for k in ("inds", "begins", "ends", "filter_inds", "dm_inds"):
