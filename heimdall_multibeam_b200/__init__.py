@@ -124,6 +124,8 @@ SYMBOLS = {
     "hd_clean_filterbank_rfi": (C.c_int, [_P, _P, _SZ, _SZ, _P, _P, C.c_float, C.c_float,
                                           C.c_float, _SZ, _SZ]),
     "hd_set_cleaning": (C.c_int, [_P, C.c_int]),
+    "hd_execute_device": (C.c_int, [_P, _P, _SZ, _SZ, _SZ, _SZ, _SZP]),
+    "hd_get_launch_count": (C.c_ulonglong, []),
     "hd_get_candidates": (C.c_int, [_P, _P, _SZP]),
     "hd_get_giants": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _SZP]),
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
@@ -264,6 +266,14 @@ class Pipeline:
                                C.byref(proc))
         return err, proc.value
 
+    def execute_device(self, dev_ptr: int, nsamps: int, nbeams: int = 1,
+                       first_idx: int = 0) -> Tuple[int, int]:
+        """hd_execute_device: the filterbank already sits in device memory."""
+        proc = C.c_size_t(0)
+        err = lib().hd_execute_device(self._p, C.c_void_p(dev_ptr), nsamps, 8, first_idx, nbeams,
+                                      C.byref(proc))
+        return err, proc.value
+
     def candidates(self) -> np.ndarray:
         n = C.c_size_t(0)
         lib().hd_get_candidates(self._p, None, C.byref(n))
@@ -303,6 +313,10 @@ class Pipeline:
         if err != HD_NO_ERROR:
             raise HdError(err, "hd_clean_filterbank_rfi")
         return out, mask
+
+
+def launch_count() -> int:
+    return int(lib().hd_get_launch_count())
 
 
 def cand_lines(c: np.ndarray) -> list:

@@ -7,6 +7,11 @@
 
 namespace hdb {
 
+// Kernel launches made by this library in this process (additive counter,
+// read through hd_get_launch_count).
+void note_launch();
+unsigned long long launch_count();
+
 // ---- filterbank kernels (kernels_fb.cu) ------------------------------------
 struct DedispArgs {
   const uint8_t* in;      // FT rows, channel c at in + c*in_pitch

@@ -12,6 +12,10 @@
 
 namespace hdb {
 
+static unsigned long long g_launches = 0;
+void note_launch() { __atomic_add_fetch(&g_launches, 1ull, __ATOMIC_RELAXED); }
+unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
 // ---------------------------------------------------------------------------
 // TF -> FT byte transpose, 128 x 128 tiles through shared memory.
 // ---------------------------------------------------------------------------
@@ -292,13 +296,13 @@ __global__ void __launch_bounds__(NW * 32) k_dedisp(DedispArgs a) {
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
                                    size_t pitch, cudaStream_t s) {
   dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128));
-  k_transpose_tf_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, out, pitch);
+  k_transpose_tf_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, out, pitch); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_dm0_sum(const uint8_t* in, size_t nsamps, int nchans, float* out,
                            cudaStream_t s) {
-  k_dm0_sum<<<(unsigned)((nsamps + 7) / 8), 256, 0, s>>>(in, nsamps, nchans, out);
+  k_dm0_sum<<<(unsigned)((nsamps + 7) / 8), 256, 0, s>>>(in, nsamps, nchans, out); note_launch();
   return cudaGetLastError();
 }
 
@@ -307,7 +311,7 @@ cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* 
                        uint8_t* out_tf, cudaStream_t s) {
   dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128));
   k_zap_to_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, mask, max_resample_dist, out_ft, pitch,
-                                   out_tf);
+                                   out_tf); note_launch();
   return cudaGetLastError();
 }
 
@@ -328,7 +332,7 @@ cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   const int DB = 2 * DD_NW, TB = 128 * DD_G;
   dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB));
-  kern<<<grid, DD_NW * 32, smem, s>>>(a);
+  kern<<<grid, DD_NW * 32, smem, s>>>(a); note_launch();
   return cudaGetLastError();
 }
 

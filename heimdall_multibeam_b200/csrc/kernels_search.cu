@@ -103,7 +103,7 @@ cudaError_t tree_reduce_array(float* cur, size_t cur_pitch, size_t count, size_t
       grid.y = (unsigned)y;
       grid.z = (unsigned)(nseg / y);
     }
-    k_tree_array<<<grid, TREE_THREADS, 0, s>>>(cur, cur_pitch, m, dst, ng);
+    k_tree_array<<<grid, TREE_THREADS, 0, s>>>(cur, cur_pitch, m, dst, ng); note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cur = dst;
@@ -231,11 +231,11 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   if (k == 0) {
     // no scrunch levels: the baseline samples are the stretched values
     k_baseline_stretch0<<<dim3((unsigned)((cr + 127) / 128), sb.nbeams, sb.nser), 128, 0, s>>>(
-        sb.data, sb.pitch, sb.nbeams, sb.stride, cr, step_b, step_last, ws.a);
+        sb.data, sb.pitch, sb.nbeams, sb.stride, cr, step_b, step_last, ws.a); note_launch();
   } else {
     k_baseline_down<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
         sb.data, sb.pitch, sb.nbeams, sb.stride, sb.beam_count, cr, m1, step_b, step_last, ws.a,
-        ng1);
+        ng1); note_launch();
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -249,7 +249,7 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
     size_t ng = count / pow5(m);
     float* dst = bufs[w];
     k_tree_array<<<seg_grid(ng, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(cur, cur_pitch, m,
-                                                                           dst, ng);
+                                                                           dst, ng); note_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     cur = dst; cur_pitch = ng; count = ng; left -= m; w ^= 1;
   }
@@ -264,7 +264,7 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   const size_t nsub = sb.stride * sb.nbeams - dm_delay;
   dim3 grid((unsigned)((nsub + 255) / 256 < 4096 ? (nsub + 255) / 256 : 4096), sb.nser);
   k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, sb.nbeams, sb.stride, sb.beam_count,
-                                      nsub, base_out, sc, step2, step3);
+                                      nsub, base_out, sc, step2, step3); note_launch();
   return cudaGetLastError();
 }
 
@@ -319,21 +319,21 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
   cudaError_t e;
   if (levels == 0) {
     k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms);
+        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms); note_launch();
     return cudaGetLastError();
   }
   int m1 = levels < 5 ? levels : 5;
   size_t ng1 = sb.beam_count / pow5(m1);
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
   k_rms_beams_pass1<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
-      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1);
+      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   float* fin;
   size_t fin_pitch, fin_count;
   e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
   if (e != cudaSuccess) return e;
   k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms);
+      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
   return cudaGetLastError();
 }
 
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(128) k_normalise_scan(const float* __restrict_
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
                            size_t scan_pitch, float* norm_out, cudaStream_t s) {
   k_normalise_scan<<<(unsigned)((sb.nser + 3) / 4), 128, 0, s>>>(
-      sb.data, sb.pitch, sb.nser, sb.len, sb.stride, sb.nbeams, rms, scan, scan_pitch, norm_out);
+      sb.data, sb.pitch, sb.nser, sb.len, sb.stride, sb.nbeams, rms, scan, scan_pitch, norm_out); note_launch();
   return cudaGetLastError();
 }
 
@@ -470,21 +470,21 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
   cudaError_t e;
   if (levels == 0) {
     k_block_rms_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(ctx, w_begin, nwb, nullptr,
-                                                                     0, rem, 1);
+                                                                     0, rem, 1); note_launch();
     return cudaGetLastError();
   }
   int m1 = levels < 5 ? levels : 5;
   size_t ng1 = cnt / pow5(m1);
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
   k_block_rms_pass1<<<seg_grid(ng1, nwb, ctx.nser), TREE_THREADS, 0, s>>>(ctx, w_begin, m1,
-                                                                         ws.a, ng1);
+                                                                         ws.a, ng1); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   float* fin;
   size_t fin_pitch, fin_count;
   e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
   if (e != cudaSuccess) return e;
   k_block_rms_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(ctx, w_begin, nwb, fin,
-                                                                   fin_pitch, fin_count, 0);
+                                                                   fin_pitch, fin_count, 0); note_launch();
   return cudaGetLastError();
 }
 
@@ -604,19 +604,19 @@ cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cud
   hb.ntiles = ntiles;
   cudaError_t e = cudaMemsetAsync(hb.sw_cnt, 0, ((size_t)ctx.nser * ctx.nw + 1) * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  k_count_hits<<<dim3(ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb);
+  k_count_hits<<<dim3(ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t scan_hit_counts(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
   size_t rows = (size_t)ctx.nser * ctx.nw;
   k_scan_tiles<<<(unsigned)((rows + 3) / 4), 128, 0, s>>>(hb.tile_cnt, hb.tile_off, hb.ntiles,
-                                                          rows);
+                                                          rows); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
-  k_write_hits<<<dim3(hb.ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb);
+  k_write_hits<<<dim3(hb.ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb); note_launch();
   return cudaGetLastError();
 }
 
@@ -698,7 +698,7 @@ cudaError_t scan_u32(const unsigned* in, unsigned* out, size_t n, unsigned* tota
   size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
   unsigned* sums = tmp;
   unsigned* sums_off = tmp + nb;
-  k_scan_tiles_u32<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, sums);
+  k_scan_tiles_u32<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, sums); note_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (nb == 1) {
@@ -708,7 +708,7 @@ cudaError_t scan_u32(const unsigned* in, unsigned* out, size_t n, unsigned* tota
   // recursive scan of the block sums
   e = scan_u32(sums, sums_off, nb, total, tmp + 2 * nb, s);
   if (e != cudaSuccess) return e;
-  k_scan_add<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(out, n, sums_off);
+  k_scan_add<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(out, n, sums_off); note_launch();
   return cudaGetLastError();
 }
 
@@ -763,7 +763,7 @@ __global__ void k_giant_finish(HitBuffers hb, unsigned ngiants, GiantBuffers gb,
 cudaError_t giant_heads(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,
                         GiantBuffers& gb, cudaStream_t s) {
   if (nhits == 0) return cudaSuccess;
-  k_giant_heads<<<(nhits + 255) / 256, 256, 0, s>>>(ctx, hb, nhits, gb.head);
+  k_giant_heads<<<(nhits + 255) / 256, 256, 0, s>>>(ctx, hb, nhits, gb.head); note_launch();
   return cudaGetLastError();
 }
 
@@ -772,9 +772,9 @@ cudaError_t giant_fill(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits
   if (nhits == 0) return cudaSuccess;
   cudaError_t e = cudaMemsetAsync(gb.key, 0, (size_t)ngiants * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
-  k_giant_reduce<<<(nhits + 255) / 256, 256, 0, s>>>(ctx, hb, nhits, gb);
+  k_giant_reduce<<<(nhits + 255) / 256, 256, 0, s>>>(ctx, hb, nhits, gb); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_giant_finish<<<(ngiants + 255) / 256, 256, 0, s>>>(hb, ngiants, gb, ctx.winfo, ctx.nw);
+  k_giant_finish<<<(ngiants + 255) / 256, 256, 0, s>>>(hb, ngiants, gb, ctx.winfo, ctx.nw); note_launch();
   return cudaGetLastError();
 }
 
@@ -855,14 +855,14 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
 
 cudaError_t cluster_init(GiantBuffers& gb, int n, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_cluster_init<<<(n + 255) / 256, 256, 0, s>>>(gb.label, n);
+  k_cluster_init<<<(n + 255) / 256, 256, 0, s>>>(gb.label, n); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* changed,
                           cudaStream_t s) {
   if (a.ngiants == 0) return cudaSuccess;
-  k_cluster_sweep<<<(a.ngiants + CL_TILE - 1) / CL_TILE, CL_TILE, 0, s>>>(a, gb, changed);
+  k_cluster_sweep<<<(a.ngiants + CL_TILE - 1) / CL_TILE, CL_TILE, 0, s>>>(a, gb, changed); note_launch();
   return cudaGetLastError();
 }
 
@@ -908,17 +908,17 @@ cudaError_t merge_groups(const GiantBuffers& gb, int n, const float* dm_list, un
                          unsigned* root_off, unsigned* nroots, unsigned* scan_tmp,
                          unsigned long long* gkey, GroupRow* rows, cudaStream_t s) {
   if (n == 0) return cudaMemsetAsync(nroots, 0, sizeof(unsigned), s);
-  k_root_flags<<<(n + 255) / 256, 256, 0, s>>>(gb.label, n, root_flag);
+  k_root_flags<<<(n + 255) / 256, 256, 0, s>>>(gb.label, n, root_flag); note_launch();
   cudaError_t e = scan_u32(root_flag, root_off, (size_t)n, nroots, scan_tmp, s);
   if (e != cudaSuccess) return e;
   // gkey: [n] keys followed by [n] member counts
   unsigned long long* members = gkey + n;
   if ((e = cudaMemsetAsync(gkey, 0, 2 * (size_t)n * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
-  k_merge_reduce<<<(n + 255) / 256, 256, 0, s>>>(gb, n, root_off, gkey, members);
+  k_merge_reduce<<<(n + 255) / 256, 256, 0, s>>>(gb, n, root_off, gkey, members); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // emit for every possible group index; rows beyond nroots are never read
-  k_merge_emit<<<(n + 255) / 256, 256, 0, s>>>(gb, nroots, gkey, members, dm_list, rows);
+  k_merge_emit<<<(n + 255) / 256, 256, 0, s>>>(gb, nroots, gkey, members, dm_list, rows); note_launch();
   return cudaGetLastError();
 }
 
@@ -980,9 +980,9 @@ cudaError_t rfi_mask(const float* x, const float* scan, size_t count, size_t box
   cudaError_t e = cudaMemcpyAsync(dwn, wn, nwid * sizeof(float), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   unsigned nb = (unsigned)((count + 255) / 256);
-  k_rfi_flags<<<nb, 256, 0, s>>>(scan, count, (int)boxcar_max, nwid, dwn, rfi_tol, flags);
+  k_rfi_flags<<<nb, 256, 0, s>>>(scan, count, (int)boxcar_max, nwid, dwn, rfi_tol, flags); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_rfi_mask<<<nb, 256, 0, s>>>(x, count, (int)boxcar_max, nwid, rfi_tol, flags, mask);
+  k_rfi_mask<<<nb, 256, 0, s>>>(x, count, (int)boxcar_max, nwid, rfi_tol, flags, mask); note_launch();
   return cudaGetLastError();
 }
 

@@ -253,8 +253,9 @@ hd_error hd_set_cleaning(hd_pipeline pl, int enable) {
   return HD_NO_ERROR;
 }
 
-hd_error hd_execute(hd_pipeline pl, const hd_byte* h_filterbank, hd_size nsamps, hd_size nbits,
-                    hd_size first_idx, hd_size nbeams, hd_size* nsamps_processed) {
+static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool on_device,
+                             hd_size nsamps, hd_size nbits, hd_size first_idx, hd_size nbeams,
+                             hd_size* nsamps_processed) {
   if (!pl) return HD_INVALID_PIPELINE;
   if (!h_filterbank || !nsamps_processed) return HD_INVALID_POINTER;
   if (nbits != 8) return HD_INVALID_NBITS;
@@ -289,7 +290,8 @@ hd_error hd_execute(hd_pipeline pl, const hd_byte* h_filterbank, hd_size nsamps,
   cudaEventRecord(pl->ev[0], s);
   // ---- H2D ----------------------------------------------------------------
   HD_TRY(pl->fb_tf.ensure(nsamps * C));
-  HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_filterbank, nsamps * C, cudaMemcpyHostToDevice, s));
+  HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_filterbank, nsamps * C,
+                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   cudaEventRecord(pl->ev[1], s);
 
   // ---- clean + channel-major working copy ------------------------------------
@@ -566,6 +568,21 @@ hd_error hd_execute(hd_pipeline pl, const hd_byte* h_filterbank, hd_size nsamps,
   pl->timing[6] = el(6, 7);
   return too_many ? HD_TOO_MANY_EVENTS : HD_NO_ERROR;
 }
+
+hd_error hd_execute(hd_pipeline pl, const hd_byte* h_filterbank, hd_size nsamps, hd_size nbits,
+                    hd_size first_idx, hd_size nbeams, hd_size* nsamps_processed) {
+  return execute_impl(pl, h_filterbank, false, nsamps, nbits, first_idx, nbeams,
+                      nsamps_processed);
+}
+
+hd_error hd_execute_device(hd_pipeline pl, const hd_byte* d_filterbank, hd_size nsamps,
+                           hd_size nbits, hd_size first_idx, hd_size nbeams,
+                           hd_size* nsamps_processed) {
+  return execute_impl(pl, d_filterbank, true, nsamps, nbits, first_idx, nbeams,
+                      nsamps_processed);
+}
+
+unsigned long long hd_get_launch_count(void) { return hdb::launch_count(); }
 
 void hd_destroy_pipeline(hd_pipeline pl) {
   if (!pl) return;

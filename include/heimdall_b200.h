@@ -18,8 +18,8 @@
  *   Pipeline/hd/clean_filterbank_rfi.h  hd_clean_filterbank_rfi
  *
  * Additions (no reference counterpart; the reference only writes candidates to
- * a .cand file or a socket): hd_set_cleaning, hd_get_candidates, hd_get_giants,
- * hd_get_timing.
+ * a .cand file or a socket): hd_set_cleaning, hd_execute_device,
+ * hd_get_candidates, hd_get_giants, hd_get_timing, hd_get_launch_count.
  *
  * Ownership and threading: the caller owns every host buffer it passes; the
  * pipeline owns all device memory, its CUDA stream and events.  A pipeline
@@ -149,6 +149,15 @@ hd_error hd_clean_filterbank_rfi(hd_pipeline pipeline, const hd_byte* h_in, hd_s
  * selects it at compile time (Pipeline/pipeline.cu:72-74,255-299, #ifdef
  * CLEANING); its shipped build leaves it off. */
 hd_error hd_set_cleaning(hd_pipeline pipeline, int enable);
+
+/* hd_execute on a filterbank already in device memory (same layout; a
+ * device-to-device copy replaces the host-to-device one). */
+hd_error hd_execute_device(hd_pipeline pipeline, const hd_byte* d_filterbank, hd_size nsamps,
+                           hd_size nbits, hd_size first_idx, hd_size nbeams,
+                           hd_size* nsamps_processed);
+
+/* Number of kernels this library has launched in this process. */
+unsigned long long hd_get_launch_count(void);
 
 /* One row of the .cand file (Pipeline/pipeline.cu:1028-1038). */
 typedef struct hd_candidate {
