@@ -35,6 +35,10 @@ HD_TOO_FEW_NSAMPS = 11
 HD_TOO_MANY_EVENTS = 12
 HD_UNKNOWN_ERROR = 13
 
+# fixed scratch limits of hd_clean_filterbank_rfi_noalloc (include/heimdall_b200.h)
+HD_NOALLOC_MAX_NSAMPS = 524288
+HD_NOALLOC_MAX_BEAMS = 64
+
 DEDISP_NO_ERROR = 0
 DEDISP_DEVICE_POINTERS = 1 << 2
 
@@ -126,6 +130,8 @@ SYMBOLS = {
     "hd_set_cleaning": (C.c_int, [_P, C.c_int]),
     "hd_execute_device": (C.c_int, [_P, _P, _SZ, _SZ, _SZ, _SZ, _SZP]),
     "hd_get_launch_count": (C.c_ulonglong, []),
+    "hd_clean_filterbank_rfi_noalloc": (C.c_int, [_P, _SZ, _SZ, _SZ, _P, _P, C.c_float,
+                                                  C.c_float, C.c_float, _SZ, _SZ, _P]),
     "hd_get_candidates": (C.c_int, [_P, _P, _SZP]),
     "hd_get_giants": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _SZP]),
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),

@@ -156,6 +156,34 @@ hd_error hd_execute_device(hd_pipeline pipeline, const hd_byte* d_filterbank, hd
                            hd_size nbits, hd_size first_idx, hd_size nbeams,
                            hd_size* nsamps_processed);
 
+/* Allocation-free zero-DM RFI cleaning.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory while they run -- a
+ * real-time ingest loop where a cudaMalloc/cudaFree would synchronise the
+ * device and stall other streams, or a process whose device memory is
+ * committed up front.  Same computation as hd_clean_filterbank_rfi, but on
+ * caller-owned device buffers (d_in: nsamps x nchans bytes, d_out: same size,
+ * d_mask: nsamps ints), queued on `stream` (a cudaStream_t, NULL = default
+ * stream) without waiting for it, and with every scratch buffer taken from one
+ * fixed array of HD_NOALLOC_SCRATCH_BYTES that this library reserves on each
+ * GPU where its device code is loaded, until the process exits.  It performs
+ * no cudaMalloc, cudaFree or other allocating call.
+ *
+ * Limits: nsamps <= HD_NOALLOC_MAX_NSAMPS and nbeams <= HD_NOALLOC_MAX_BEAMS;
+ * larger requests return HD_INVALID_STRIDE (with a message on stderr).
+ * The first call on each device looks up the scratch array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array: calls whose work overlaps on the GPU (e.g. on
+ * two streams at once) race and must be serialised by the caller. */
+#define HD_NOALLOC_MAX_NSAMPS    524288u
+#define HD_NOALLOC_MAX_BEAMS     64u
+#define HD_NOALLOC_SCRATCH_BYTES 11534336u
+hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size nsamps, hd_size nchans,
+                                         hd_size nbits, hd_byte* d_out, int* d_mask,
+                                         hd_float dt, hd_float baseline_length,
+                                         hd_float rfi_tol, hd_size boxcar_max, hd_size nbeams,
+                                         void* stream);
+
 /* Number of kernels this library has launched in this process. */
 unsigned long long hd_get_launch_count(void);
 
