@@ -109,10 +109,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload():
+def workload(nsamps=None):
     from heimdall_multibeam_b200 import synth
     w = synth.SEARCH_C1
-    b = synth.make_c1()
+    b = synth.make_c1(nsamps=nsamps)
+    if nsamps:
+        import dataclasses
+        w = dataclasses.replace(w, name=f"plain_c1024_n{nsamps}_rfi", nsamps=nsamps)
     return w, b
 
 
@@ -157,7 +160,7 @@ def run_product(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", local if world > 1 else 0)
 
-    w, b = workload()
+    w, b = workload(args.nsamps)
     nsamps, nchans = b.data.shape
     beam_s = nsamps * w.dt
     p = params_for(H, w)
@@ -310,7 +313,7 @@ def run_reference(args):
     if rank != 0:
         return
     import oracle
-    w, b = workload()
+    w, b = workload(args.nsamps)
     nsamps = b.data.shape[0]
     beam_s = nsamps * w.dt
     if not oracle.ref_available():
@@ -355,6 +358,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nsamps", type=int, default=None,
+                    help="gulp length (default 2^18); smaller gulps are for profiling")
     ap.add_argument("--ref-dm1", type=float, default=20.0)
     ap.add_argument("--ref-dm2", type=float, default=60.0)
     args = ap.parse_args()
