@@ -100,7 +100,9 @@ struct WidthCtx {
   int nbeams;
   int offset;         // rel_boxcar_max / 2
   int nw;             // widths per series
-  const WidthInfo* winfo;  // device copy
+  const WidthInfo* winfo;       // device copy
+  const WidthInfo* host_winfo;  // host copy (launch decisions)
+  size_t scan_len;              // valid prefix-sum entries per series (len + 1)
   float* norm;        // [nser][nw]  1 / block_rms
   float thresh;
 };

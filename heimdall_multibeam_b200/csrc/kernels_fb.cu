@@ -167,53 +167,91 @@ __global__ void __launch_bounds__(256) k_zap_to_ft(const uint8_t* __restrict__ i
 //
 //   out[d][t] = (float) sum_{c active} in[c][t + delay[d][c]],  t < nout
 //
-// CTA = DB = 2*NW DMs x TB = 128*G samples.  For each stage of CH channels,
-// one thread issues 1-D bulk async copies (TMA, cp.async.bulk) of each channel
-// row segment [t0 + min_d delay - align, +rowb) into shared memory; the copy of
-// stage s+1 overlaps the sums of stage s (double buffer, mbarrier completion).
+// CTA = DB = 2*NW DMs x TB = 128*G samples, NW consumer warps + 1 producer
+// warp.  The producer walks the active channels in stages of CH: for each
+// stage it tabulates the byte offset of every (DM, channel) pair in shared
+// memory and issues one 1-D bulk async copy (TMA, cp.async.bulk) per channel
+// row segment [t0 + min_d delay - align, +rowb) into a ring of NST stage
+// buffers, signalling a `full` mbarrier; consumer warps release a buffer
+// through an `empty` mbarrier (one arrival per warp).  There is no block-wide
+// barrier in the main loop, so warps drift freely within the ring.
 // Warp w owns DMs 2w and 2w+1; lane l owns samples 4(l + 32g) .. +3.  Each
 // 4-byte window is realigned with a funnel shift and split into two 16-bit
-// lane pairs (even/odd samples) so one integer add accumulates two samples;
-// the 16-bit lanes are drained into 32-bit sums every 256 channels (255*256 <
-// 65536), so the sums are exact.
+// lane pairs (even/odd samples); two channels are summed per 3-input add, so
+// one add accumulates four sample-channel terms.  The 16-bit lanes are drained
+// into 32-bit sums after at most 257 channels (255 * 257 = 65535), so the
+// sums are exact.  Every mbarrier wait is bounded; a wait that gives up sets
+// bit 0 of a.err and the warp leaves its loop.
 // ---------------------------------------------------------------------------
-template <int NW, int G, int CH>
-__global__ void __launch_bounds__(NW * 32) k_dedisp(DedispArgs a) {
+constexpr uint32_t DD_WAIT_LIMIT = 1u << 22;
+
+template <int NW, int G, int CH, int NST>
+__global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
-  uint8_t* rows = smem + 128;
   constexpr int DB = 2 * NW;
   constexpr int TB = 128 * G;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + NST;
+  int* s_off = reinterpret_cast<int*>(smem + 128);          // [NST][DB*CH]
+  uint8_t* rows = smem + 128 + NST * DB * CH * sizeof(int);  // [NST][CH][rowb]
   const int dblk = blockIdx.x;
   const size_t t0 = (size_t)blockIdx.y * TB;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int d_lo = dblk * DB;
-  int dm[2];
-  dm[0] = min(d_lo + 2 * warp, a.dm_count - 1);
-  dm[1] = min(d_lo + 2 * warp + 1, a.dm_count - 1);
   const int* __restrict__ bmin = a.blk_min + (size_t)dblk * a.nchans;
   const int nstage = (a.nact + CH - 1) / CH;
+  const size_t C = (size_t)a.nchans;
 
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int b = 0; b < NST; b++) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], NW);
+    }
     fence_mbar_init();
   }
   __syncthreads();
 
-  auto issue = [&](int st) {
-    int buf = st & 1;
-    int k0 = st * CH;
-    int nk = min(CH, a.nact - k0);
-    mbar_expect_tx(&bar[buf], (uint32_t)(nk * a.rowb));
-    for (int k = 0; k < nk; k++) {
-      int c = a.chans[k0 + k];
-      size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
-      bulk_g2s(rows + (size_t)(buf * CH + k) * a.rowb, a.in + (size_t)c * a.in_pitch + lo,
-               (uint32_t)a.rowb, &bar[buf]);
+  if (warp == NW) {
+    // ---------------- producer ----------------
+    int issued = 0;
+    for (int st = 0; st < nstage; st++) {
+      const int buf = st % NST;
+      if (st >= NST) {
+        if (!mbar_wait(&empty[buf], (uint32_t)(((st / NST) - 1) & 1), DD_WAIT_LIMIT)) {
+          if (lane == 0) atomicOr(a.err, 1u);
+          break;
+        }
+      }
+      const int k0 = st * CH;
+      const int nk = min(CH, a.nact - k0);
+      int* off = s_off + buf * DB * CH;
+      for (int e = lane; e < DB * CH; e += 32) {
+        const int k = e % CH;
+        if (k < nk) {
+          const int c = a.chans[k0 + k];
+          const int d = min(d_lo + e / CH, a.dm_count - 1);
+          const size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
+          off[e] = (int)(t0 + (size_t)a.delays[(size_t)d * C + c] - lo);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_expect_tx(&full[buf], (uint32_t)(nk * a.rowb));
+      __syncwarp();
+      if (lane < nk) {
+        const int c = a.chans[k0 + lane];
+        const size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
+        bulk_g2s(rows + (size_t)(buf * CH + lane) * a.rowb, a.in + (size_t)c * a.in_pitch + lo,
+                 (uint32_t)a.rowb, &full[buf]);
+      }
+      issued = st + 1;
     }
-  };
+    // let every copy this CTA issued land before the warp exits
+    for (int st = (issued > NST ? issued - NST : 0); st < issued; st++)
+      mbar_wait(&full[st % NST], (uint32_t)((st / NST) & 1), DD_WAIT_LIMIT);
+    return;
+  }
 
+  // ---------------- consumers ----------------
   uint32_t pk[2][G][2];
   int acc[2][G][4];
 #pragma unroll
@@ -236,38 +274,62 @@ __global__ void __launch_bounds__(NW * 32) k_dedisp(DedispArgs a) {
       }
   };
 
-  if (threadIdx.x == 0) issue(0);
   int nsum = 0;
+  bool failed = false;
   for (int st = 0; st < nstage; st++) {
-    if (threadIdx.x == 0 && st + 1 < nstage) issue(st + 1);
-    bool ok = mbar_wait(&bar[st & 1], (uint32_t)((st >> 1) & 1), 1u << 24);
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(a.err, 1u);
-      return;
+    const int buf = st % NST;
+    if (!mbar_wait(&full[buf], (uint32_t)((st / NST) & 1), DD_WAIT_LIMIT)) {
+      if (lane == 0) atomicOr(a.err, 1u);
+      failed = true;
+      break;
     }
     const int k0 = st * CH;
     const int nk = min(CH, a.nact - k0);
-    for (int k = 0; k < nk; k++) {
-      const int c = a.chans[k0 + k];
-      const uint32_t* rw =
-          reinterpret_cast<const uint32_t*>(rows + (size_t)((st & 1) * CH + k) * a.rowb);
-      const size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
+    const int* off = s_off + buf * DB * CH + (2 * warp) * CH;
+    const uint8_t* stage_rows = rows + (size_t)(buf * CH) * a.rowb;
+    int k = 0;
+    for (; k + 1 < nk; k += 2) {
+      const uint32_t* ra = reinterpret_cast<const uint32_t*>(stage_rows + (size_t)k * a.rowb);
+      const uint32_t* rb = reinterpret_cast<const uint32_t*>(stage_rows + (size_t)(k + 1) * a.rowb);
 #pragma unroll
       for (int d = 0; d < 2; d++) {
-        const int off = (int)(t0 + (size_t)a.delays[(size_t)dm[d] * a.nchans + c] - lo);
-        const int sh = (off & 3) * 8;
-        const int wb = (off >> 2) + lane;
+        const int oa = off[d * CH + k];
+        const int ob = off[d * CH + k + 1];
+        const int sa = (oa & 3) * 8, sb = (ob & 3) * 8;
+        const int wa = (oa >> 2) + lane, wb = (ob >> 2) + lane;
 #pragma unroll
         for (int g = 0; g < G; g++) {
-          uint32_t x = __funnelshift_r(rw[wb + 32 * g], rw[wb + 32 * g + 1], sh);
-          pk[d][g][0] += x & 0x00FF00FFu;
-          pk[d][g][1] += __byte_perm(x, 0u, 0x4341);
+          const uint32_t xa = __funnelshift_r(ra[wa + 32 * g], ra[wa + 32 * g + 1], sa);
+          const uint32_t xb = __funnelshift_r(rb[wb + 32 * g], rb[wb + 32 * g + 1], sb);
+          pk[d][g][0] += (xa & 0x00FF00FFu) + (xb & 0x00FF00FFu);
+          pk[d][g][1] += __byte_perm(xa, 0u, 0x4341) + __byte_perm(xb, 0u, 0x4341);
         }
       }
-      if (++nsum == 256) { drain(); nsum = 0; }
+      nsum += 2;
+      if (nsum >= 256) { drain(); nsum = 0; }
     }
-    __syncthreads();
+    if (k < nk) {
+      const uint32_t* ra = reinterpret_cast<const uint32_t*>(stage_rows + (size_t)k * a.rowb);
+#pragma unroll
+      for (int d = 0; d < 2; d++) {
+        const int oa = off[d * CH + k];
+        const int sa = (oa & 3) * 8;
+        const int wa = (oa >> 2) + lane;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          const uint32_t xa = __funnelshift_r(ra[wa + 32 * g], ra[wa + 32 * g + 1], sa);
+          pk[d][g][0] += xa & 0x00FF00FFu;
+          pk[d][g][1] += __byte_perm(xa, 0u, 0x4341);
+        }
+      }
+      nsum += 1;
+      if (nsum >= 256) { drain(); nsum = 0; }
+    }
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];"
+                                :: "r"(smem_addr(&empty[buf])) : "memory");
   }
+  if (failed) return;
   drain();
 #pragma unroll
   for (int d = 0; d < 2; d++) {
@@ -316,23 +378,25 @@ cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* 
 }
 
 namespace {
-constexpr int DD_NW = 8, DD_G = 4, DD_CH = 8;
+constexpr int DD_NW = 8, DD_G = 4, DD_CH = 8, DD_NST = 3;
 }
 
 int dedisp_dm_block() { return 2 * DD_NW; }
 int dedisp_time_block() { return 128 * DD_G; }
 
-size_t dedisp_smem_bytes(int rowb) { return 128 + (size_t)2 * DD_CH * rowb; }
+size_t dedisp_smem_bytes(int rowb) {
+  return 128 + (size_t)DD_NST * 2 * DD_NW * DD_CH * sizeof(int) + (size_t)DD_NST * DD_CH * rowb;
+}
 
 cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s) {
-  auto kern = k_dedisp<DD_NW, DD_G, DD_CH>;
+  auto kern = k_dedisp<DD_NW, DD_G, DD_CH, DD_NST>;
   size_t smem = dedisp_smem_bytes(a.rowb);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   const int DB = 2 * DD_NW, TB = 128 * DD_G;
   dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB));
-  kern<<<grid, DD_NW * 32, smem, s>>>(a); note_launch();
+  kern<<<grid, (DD_NW + 1) * 32, smem, s>>>(a); note_launch();
   return cudaGetLastError();
 }
 

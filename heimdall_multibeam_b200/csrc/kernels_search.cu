@@ -340,50 +340,122 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // ===========================================================================
 // Normalise + exclusive prefix sum with the sequential association of the
 // reference's scan (Thrust's sequential exclusive_scan: out[0] = 0,
-// out[k+1] = out[k] + in[k]).  One warp per series; every lane runs the same
-// serial chain on broadcast values and keeps the partial sum of its slot, so
-// each output is the exact left-to-right float sum.
+// out[k+1] = out[k] + in[k]).  A segment of SCAN_SEG lanes owns one series;
+// every lane of the segment runs the same serial chain on broadcast values and
+// keeps the partial sum of its slot, so each output is the exact left-to-right
+// float sum.  Loads run SCAN_AHEAD chunks ahead of the chain (the chain is
+// ~4 cycles per sample; a load round trip is hundreds of cycles).
 // ===========================================================================
-__global__ void __launch_bounds__(128) k_normalise_scan(const float* __restrict__ data,
-                                                        size_t pitch, int nser, size_t len,
-                                                        size_t stride, int nbeams,
-                                                        const float* __restrict__ rms,
-                                                        float* __restrict__ scan,
-                                                        size_t scan_pitch, float* norm_out) {
-  const int ser = blockIdx.x * 4 + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (ser >= nser) return;
-  const float* d = data + (size_t)ser * pitch;
-  const float* r = rms + (size_t)ser * nbeams;
-  float* o = scan + (size_t)ser * scan_pitch;
-  float sum = 0.0f;
-  const size_t n_out = len + 1;
-  float nxt = 0.f;
-  {
-    size_t i = lane;
-    if (i < len) nxt = __fdiv_rn(d[i], r[i / stride]);
-  }
-  for (size_t base = 0; base < n_out; base += 32) {
-    float v = nxt;
-    size_t in2 = base + 32 + lane;
-    nxt = (in2 < len) ? __fdiv_rn(d[in2], r[in2 / stride]) : 0.f;
-    float mine = 0.f;
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
-      float vj = __shfl_sync(0xffffffffu, v, j);
-      if (lane == j) mine = sum;
-      sum = __fadd_rn(sum, vj);
+constexpr int SQ_SER = 8;        // series per block (one chain lane each)
+constexpr int SQ_CH = 256;       // samples per series per stage
+constexpr int SQ_THREADS = 64;
+constexpr int SQ_PAD = SQ_CH + 4;  // 16-byte rows; lane s reads banks 4s..4s+3
+constexpr int SQ_MAXB = 64;      // beams whose RMS is kept in shared memory
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__global__ void __launch_bounds__(SQ_THREADS) k_normalise_scan(const float* __restrict__ data,
+                                                               size_t pitch, int nser,
+                                                               unsigned len, unsigned stride,
+                                                               int nbeams,
+                                                               const float* __restrict__ rms,
+                                                               float* __restrict__ scan,
+                                                               size_t scan_pitch,
+                                                               float* norm_out) {
+  extern __shared__ __align__(16) float sq_smem[];
+  float (*raw)[SQ_SER][SQ_CH] = reinterpret_cast<float (*)[SQ_SER][SQ_CH]>(sq_smem);
+  float (*val)[SQ_PAD] = reinterpret_cast<float (*)[SQ_PAD]>(sq_smem + 2 * SQ_SER * SQ_CH);
+  float* srms = sq_smem + 2 * SQ_SER * SQ_CH + SQ_SER * SQ_PAD;  // [SQ_SER][nbeams]
+  const int s0 = blockIdx.x * SQ_SER;
+  const int nb = min(SQ_SER, nser - s0);
+  const int tid = threadIdx.x;
+  const bool rms_smem = nbeams <= SQ_MAXB;
+  if (rms_smem)
+    for (int k = tid; k < nb * nbeams; k += SQ_THREADS) srms[k] = rms[(size_t)s0 * nbeams + k];
+  const unsigned nstage = (len + SQ_CH) / SQ_CH;  // covers outputs 0..len
+
+  auto load = [&](unsigned st, int buf) {
+    const unsigned base = st * SQ_CH;
+    for (int idx = tid; idx < nb * (SQ_CH / 4); idx += SQ_THREADS) {
+      const int sl = idx / (SQ_CH / 4), q = idx % (SQ_CH / 4);
+      const unsigned e0 = base + 4u * q;
+      const float* src = data + (size_t)(s0 + sl) * pitch + e0;
+      float* dst = &raw[buf][sl][4 * q];
+      if (e0 + 4 <= len) {
+        cp_async16(dst, src);
+      } else {
+        for (int k = 0; k < 4; k++) dst[k] = (e0 + k < len) ? src[k] : 0.f;
+      }
     }
-    size_t i = base + lane;
-    if (i < n_out) o[i] = mine;
-    if (norm_out && i < len) norm_out[(size_t)ser * pitch + i] = v;
+    cp_async_commit();
+  };
+
+  float sum = 0.f;  // running sum of series (s0 + lane), lanes < nb of warp 0
+  load(0, 0);
+  for (unsigned st = 0; st < nstage; st++) {
+    const int buf = st & 1;
+    cp_async_wait_all();
+    __syncthreads();
+    if (st + 1 < nstage) load(st + 1, buf ^ 1);  // overlaps this stage
+    // normalise (get_rms.cu:344-356): x / rms[beam of sample]
+    const unsigned base = st * SQ_CH;
+    const unsigned b0 = base / stride;
+    for (int idx = tid; idx < nb * SQ_CH; idx += SQ_THREADS) {
+      const int sl = idx / SQ_CH, e = idx % SQ_CH;
+      const unsigned i = base + e;
+      float v = 0.f;
+      if (i < len) {
+        unsigned b = b0;
+        unsigned bend = (b0 + 1) * stride;
+        while (i >= bend && b + 1 < (unsigned)nbeams) { b++; bend += stride; }
+        const float rb = rms_smem ? srms[sl * nbeams + b] : rms[(size_t)(s0 + sl) * nbeams + b];
+        v = __fdiv_rn(raw[buf][sl][e], rb);
+        if (norm_out) norm_out[(size_t)(s0 + sl) * pitch + i] = v;
+      }
+      val[sl][e] = v;
+    }
+    __syncthreads();
+    // the serial chain, one lane per series, exact left-to-right order
+    if (tid < nb) {
+      float* row = val[tid];
+      for (int e = 0; e < SQ_CH; e += 8) {
+        const float4 va = *reinterpret_cast<const float4*>(row + e);
+        const float4 vb = *reinterpret_cast<const float4*>(row + e + 4);
+        float4 oa, ob;
+        oa.x = sum; sum = __fadd_rn(sum, va.x);
+        oa.y = sum; sum = __fadd_rn(sum, va.y);
+        oa.z = sum; sum = __fadd_rn(sum, va.z);
+        oa.w = sum; sum = __fadd_rn(sum, va.w);
+        ob.x = sum; sum = __fadd_rn(sum, vb.x);
+        ob.y = sum; sum = __fadd_rn(sum, vb.y);
+        ob.z = sum; sum = __fadd_rn(sum, vb.z);
+        ob.w = sum; sum = __fadd_rn(sum, vb.w);
+        *reinterpret_cast<float4*>(row + e) = oa;
+        *reinterpret_cast<float4*>(row + e + 4) = ob;
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nb * SQ_CH; idx += SQ_THREADS) {
+      const int sl = idx / SQ_CH, e = idx % SQ_CH;
+      const unsigned i = base + e;
+      if (i <= len) scan[(size_t)(s0 + sl) * scan_pitch + i] = val[sl][e];
+    }
   }
 }
 
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
                            size_t scan_pitch, float* norm_out, cudaStream_t s) {
-  k_normalise_scan<<<(unsigned)((sb.nser + 3) / 4), 128, 0, s>>>(
-      sb.data, sb.pitch, sb.nser, sb.len, sb.stride, sb.nbeams, rms, scan, scan_pitch, norm_out); note_launch();
+  if (sb.len >= 0xFFFFFF00u || sb.pitch % 4) return cudaErrorInvalidValue;
+  const size_t smem = (2 * SQ_SER * SQ_CH + SQ_SER * SQ_PAD + SQ_SER * SQ_MAXB) * sizeof(float);
+  cudaFuncSetAttribute(k_normalise_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_normalise_scan<<<(unsigned)((sb.nser + SQ_SER - 1) / SQ_SER), SQ_THREADS, smem, s>>>(
+      sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
+      scan_pitch, norm_out); note_launch();
   return cudaGetLastError();
 }
 
@@ -433,6 +505,52 @@ __global__ void k_block_rms_pass1(WidthCtx ctx, int w0, int m, float* __restrict
   if (threadIdx.x == 0) out[(ser * gridDim.y + blockIdx.y) * out_pitch + g] = r;
 }
 
+// Pass 1 for several unscrunched widths at once: the group's prefix-sum window
+// is staged in shared memory once and every width's boxcar is read from it.
+// Falls back to global loads when the group's samples are not contiguous
+// (a multibeam group straddling a beam gap) or the window does not fit.
+constexpr int MULTI_SMEM_FLOATS = 12288;
+
+__global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m,
+                                        float* __restrict__ out, size_t out_pitch) {
+  extern __shared__ float dyn[];
+  float* tile = dyn;                         // MULTI_SMEM_FLOATS
+  float* sm = dyn + MULTI_SMEM_FLOATS;       // tree buffers
+  const size_t ser = blockIdx.y;
+  const size_t g = blockIdx.x;
+  const WidthInfo& w_first = ctx.winfo[w0];
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const float delta = (float)(ctx.stride - w_first.bn);
+  const size_t gsz = pow5(m);
+  const size_t q0 = g * gsz;
+  const size_t i_first = reblock_index((unsigned)q0 / w_first.bn, delta, (unsigned)q0);
+  const size_t q1 = q0 + gsz - 1;
+  const size_t i_last = reblock_index((unsigned)q1 / w_first.bn, delta, (unsigned)q1);
+  const int offset = ctx.offset;
+  const bool contig = (i_last - i_first == gsz - 1);
+  const size_t span = (i_last - i_first) + 2 * (size_t)offset + 2;
+  const bool staged = contig && span <= MULTI_SMEM_FLOATS;
+  if (staged) {
+    for (size_t k = threadIdx.x; k < span; k += blockDim.x) tile[k] = sc[i_first + k];
+    __syncthreads();
+  }
+  for (int wl = 0; wl < nwb; wl++) {
+    const WidthInfo& w = ctx.winfo[w0 + wl];
+    const int a = offset + w.ahead, b = offset - w.behind;
+    float r;
+    if (staged) {
+      r = block_tree([&](int k) { return fabsf(__fsub_rn(tile[k + a], tile[k + b])); }, m, sm);
+    } else {
+      r = block_tree([&](int k) {
+        unsigned q = (unsigned)(q0 + k);
+        size_t i = reblock_index(q / w.bn, delta, q);
+        return fabsf(__fsub_rn(sc[i + a], sc[i + b]));
+      }, m, sm);
+    }
+    if (threadIdx.x == 0) out[(ser * nwb + wl) * out_pitch + g] = r;
+  }
+}
+
 __global__ void k_block_rms_final(WidthCtx ctx, int w0, int nwb, const float* __restrict__ lev,
                                   size_t lev_pitch, size_t count, int from_window) {
   int seg = blockIdx.x * blockDim.x + threadIdx.x;
@@ -476,8 +594,18 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
   int m1 = levels < 5 ? levels : 5;
   size_t ng1 = cnt / pow5(m1);
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
-  k_block_rms_pass1<<<seg_grid(ng1, nwb, ctx.nser), TREE_THREADS, 0, s>>>(ctx, w_begin, m1,
-                                                                         ws.a, ng1); note_launch();
+  bool unscrunched = true;
+  for (int wi = w_begin; wi < w_end; wi++) unscrunched = unscrunched && hw[wi].ts == 1;
+  if (unscrunched) {
+    const size_t smem = (MULTI_SMEM_FLOATS + 625 + 125) * sizeof(float);
+    cudaFuncSetAttribute(k_block_rms_pass1_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    k_block_rms_pass1_multi<<<dim3((unsigned)ng1, ctx.nser), TREE_THREADS, smem, s>>>(
+        ctx, w_begin, nwb, m1, ws.a, ng1); note_launch();
+  } else {
+    k_block_rms_pass1<<<seg_grid(ng1, nwb, ctx.nser), TREE_THREADS, 0, s>>>(ctx, w_begin, m1,
+                                                                           ws.a, ng1); note_launch();
+  }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   float* fin;
   size_t fin_pitch, fin_count;
@@ -495,6 +623,10 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
 constexpr int HIT_TILE = 2048;
 constexpr int HIT_THREADS = 256;
 constexpr int HIT_PER_THREAD = HIT_TILE / HIT_THREADS;
+// The multi-width kernels use a longer tile so the boxcar_max halo of the
+// staged prefix-sum window costs less per sample.
+constexpr int MHIT_TILE = 2048;
+constexpr int MHIT_PER_THREAD = MHIT_TILE / HIT_THREADS;
 
 __device__ __forceinline__ bool hit_at(const WidthCtx& ctx, const float* sc, float norm,
                                        const WidthInfo& w, size_t i, float* val) {
@@ -505,8 +637,9 @@ __device__ __forceinline__ bool hit_at(const WidthCtx& ctx, const float* sc, flo
   return v > ctx.thresh;
 }
 
-__global__ void __launch_bounds__(HIT_THREADS) k_count_hits(WidthCtx ctx, HitBuffers hb) {
-  const int wi = blockIdx.y;
+__global__ void __launch_bounds__(HIT_THREADS) k_count_hits(WidthCtx ctx, HitBuffers hb,
+                                                            int w_base) {
+  const int wi = w_base + blockIdx.y;
   const size_t ser = blockIdx.z;
   const unsigned tile = blockIdx.x;
   const WidthInfo& w = ctx.winfo[wi];
@@ -555,8 +688,9 @@ __global__ void k_scan_tiles(const unsigned* __restrict__ cnt, unsigned* __restr
   }
 }
 
-__global__ void __launch_bounds__(HIT_THREADS) k_write_hits(WidthCtx ctx, HitBuffers hb) {
-  const int wi = blockIdx.y;
+__global__ void __launch_bounds__(HIT_THREADS) k_write_hits(WidthCtx ctx, HitBuffers hb,
+                                                            int w_base) {
+  const int wi = w_base + blockIdx.y;
   const size_t ser = blockIdx.z;
   const unsigned tile = blockIdx.x;
   const size_t sw = ser * ctx.nw + wi;
@@ -600,11 +734,146 @@ __global__ void __launch_bounds__(HIT_THREADS) k_write_hits(WidthCtx ctx, HitBuf
   }
 }
 
+// All unscrunched widths [0, nw1) of one tile, from one shared-memory window of
+// the prefix sum (tile + boxcar_max + 1 values).
+__device__ __forceinline__ void load_hit_tile(const float* sc, size_t i0, float* tile,
+                                              size_t span, size_t slen) {
+  for (size_t k = threadIdx.x; k < span; k += blockDim.x)
+    tile[k] = (i0 + k < slen) ? sc[i0 + k] : 0.f;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(HIT_THREADS) k_count_hits_multi(WidthCtx ctx, HitBuffers hb,
+                                                                  int nw1, size_t slen) {
+  extern __shared__ float tile[];
+  const size_t ser = blockIdx.y;
+  const unsigned t = blockIdx.x;
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const size_t i0 = (size_t)t * MHIT_TILE;
+  if (i0 >= ctx.winfo[0].n) {
+    // the grid is sized for the short per-width tiles: rows must read zero here
+    if (threadIdx.x < nw1) hb.tile_cnt[(ser * ctx.nw + threadIdx.x) * hb.ntiles + t] = 0;
+    return;
+  }
+  const size_t span = MHIT_TILE + 2 * (size_t)ctx.offset + 2;
+  load_hit_tile(sc, i0, tile, span, slen);
+  __shared__ unsigned red[HIT_THREADS / 32];
+  const unsigned ustride = (unsigned)ctx.stride;
+  const unsigned it0 = (unsigned)(i0 + (size_t)threadIdx.x * MHIT_PER_THREAD);
+  const unsigned samp0 = it0 % ustride;  // beam-local index of the thread's first sample
+  for (int wi = 0; wi < nw1; wi++) {
+    const WidthInfo& w = ctx.winfo[wi];
+    const float norm = ctx.norm[ser * ctx.nw + wi];
+    const int a = ctx.offset + w.ahead, b = ctx.offset - w.behind;
+    unsigned c = 0;
+    unsigned samp = samp0;
+#pragma unroll 8
+    for (int k = 0; k < MHIT_PER_THREAD; k++) {
+      const unsigned kl = threadIdx.x * MHIT_PER_THREAD + k;
+      const unsigned i = it0 + k;
+      if (i < w.n && samp < w.bn) {
+        float v = __fmul_rn(__fsub_rn(tile[kl + a], tile[kl + b]), norm);
+        c += (v > ctx.thresh);
+      }
+      if (++samp == ustride) samp = 0;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned tot = 0;
+      for (int k = 0; k < HIT_THREADS / 32; k++) tot += red[k];
+      const size_t sw = ser * ctx.nw + wi;
+      hb.tile_cnt[sw * hb.ntiles + t] = tot;
+      if (tot) atomicAdd(&hb.sw_cnt[sw], tot);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(HIT_THREADS) k_write_hits_multi(WidthCtx ctx, HitBuffers hb,
+                                                                  int nw1, size_t slen) {
+  extern __shared__ float tile[];
+  const size_t ser = blockIdx.y;
+  const unsigned t = blockIdx.x;
+  unsigned any = 0;
+  for (int wi = 0; wi < nw1; wi++) any |= hb.tile_cnt[(ser * ctx.nw + wi) * hb.ntiles + t];
+  if (!any) return;
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const size_t i0 = (size_t)t * MHIT_TILE;
+  const size_t span = MHIT_TILE + 2 * (size_t)ctx.offset + 2;
+  load_hit_tile(sc, i0, tile, span, slen);
+  __shared__ unsigned wsum[HIT_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned ustride = (unsigned)ctx.stride;
+  const unsigned it0 = (unsigned)(i0 + (size_t)threadIdx.x * MHIT_PER_THREAD);
+  const unsigned samp0 = it0 % ustride;
+  for (int wi = 0; wi < nw1; wi++) {
+    const size_t sw = ser * ctx.nw + wi;
+    if (hb.tile_cnt[sw * hb.ntiles + t] == 0) continue;  // uniform across the block
+    const WidthInfo& w = ctx.winfo[wi];
+    const float norm = ctx.norm[sw];
+    const int a = ctx.offset + w.ahead, b = ctx.offset - w.behind;
+    unsigned flags = 0;
+    float vals[MHIT_PER_THREAD];
+    unsigned samp = samp0;
+#pragma unroll
+    for (int k = 0; k < MHIT_PER_THREAD; k++) {
+      const unsigned kl = threadIdx.x * MHIT_PER_THREAD + k;
+      const unsigned i = it0 + k;
+      vals[k] = 0.f;
+      if (i < w.n && samp < w.bn) {
+        vals[k] = __fmul_rn(__fsub_rn(tile[kl + a], tile[kl + b]), norm);
+        if (vals[k] > ctx.thresh) flags |= 1u << k;
+      }
+      if (++samp == ustride) samp = 0;
+    }
+    unsigned c = __popc(flags);
+    unsigned x = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      unsigned y = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= d) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    unsigned wpre = 0;
+    for (int k = 0; k < warp; k++) wpre += wsum[k];
+    unsigned pos = hb.sw_off[sw] + hb.tile_off[sw * hb.ntiles + t] + wpre + x - c;
+#pragma unroll
+    for (int k = 0; k < HIT_PER_THREAD; k++) {
+      if (flags & (1u << k)) {
+        if (pos < hb.cap) {
+          hb.ind[pos] = it0 + k;
+          hb.val[pos] = vals[k];
+          hb.sw[pos] = (unsigned)sw;
+        }
+        pos++;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cudaStream_t s) {
   hb.ntiles = ntiles;
   cudaError_t e = cudaMemsetAsync(hb.sw_cnt, 0, ((size_t)ctx.nser * ctx.nw + 1) * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  k_count_hits<<<dim3(ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb); note_launch();
+  // unscrunched widths share one staged window per tile
+  int nw1 = 0;
+  while (nw1 < ctx.nw && ctx.host_winfo[nw1].ts == 1) nw1++;
+  const size_t smem = (MHIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
+  const size_t slen = ctx.scan_len;
+  if (nw1 > 0 && smem <= 200 * 1024) {
+    cudaFuncSetAttribute(k_count_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_count_hits_multi<<<dim3(ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
+  } else {
+    nw1 = 0;
+  }
+  if (nw1 < ctx.nw) {
+    k_count_hits<<<dim3(ntiles, ctx.nw - nw1, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb, nw1); note_launch();
+  }
   return cudaGetLastError();
 }
 
@@ -616,7 +885,19 @@ cudaError_t scan_hit_counts(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s)
 }
 
 cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
-  k_write_hits<<<dim3(hb.ntiles, ctx.nw, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb); note_launch();
+  int nw1 = 0;
+  while (nw1 < ctx.nw && ctx.host_winfo[nw1].ts == 1) nw1++;
+  const size_t smem = (MHIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
+  const size_t slen = ctx.scan_len;
+  if (nw1 > 0 && smem <= 200 * 1024) {
+    cudaFuncSetAttribute(k_write_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_write_hits_multi<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
+  } else {
+    nw1 = 0;
+  }
+  if (nw1 < ctx.nw) {
+    k_write_hits<<<dim3(hb.ntiles, ctx.nw - nw1, ctx.nser), HIT_THREADS, 0, s>>>(ctx, hb, nw1); note_launch();
+  }
   return cudaGetLastError();
 }
 
@@ -791,19 +1072,34 @@ cudaError_t giant_fill(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits
 // order; the final chain trace of the reference is then the identity.
 // ===========================================================================
 constexpr int CL_TILE = 128;
+constexpr int CL_JCHUNK = 1024;
 
 __global__ void k_cluster_init(int* label, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) label[i] = i;
 }
 
+// Block (x, y): giants [x*CL_TILE, +CL_TILE) against the y-th chunk of
+// CL_JCHUNK earlier giants inside their DM window.
 __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantBuffers gb,
                                                            unsigned* changed) {
   __shared__ unsigned long long s_samp[CL_TILE];
   __shared__ int s_f[CL_TILE], s_dm[CL_TILE], s_lab[CL_TILE];
-  const int i = blockIdx.x * CL_TILE + threadIdx.x;
   const int i_first = blockIdx.x * CL_TILE;
+  const int i = i_first + threadIdx.x;
   const int i_last = min(i_first + CL_TILE, a.ngiants) - 1;
+  // giants are in ascending DM order: the first candidate neighbour is the
+  // first giant within dm_tol of the tile's smallest DM
+  const int dm_first = gb.dm[i_first];
+  int lo = 0, hi = i_first;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if ((long long)gb.dm[mid] + (long long)a.dm_tol < (long long)dm_first) lo = mid + 1;
+    else hi = mid;
+  }
+  const int j_begin = lo + (int)blockIdx.y * CL_JCHUNK;
+  if (j_begin > i_last) return;  // uniform: this chunk lies past the tile
+  const int j_end = min(j_begin + CL_JCHUNK, i_last + 1);
   unsigned long long si = 0, bi = 0;
   int fi = 0, di = 0, best = 0x7FFFFFFF;
   if (i < a.ngiants) {
@@ -813,19 +1109,11 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
     di = gb.dm[i];
     best = gb.label[i];
   }
-  // giants are in ascending DM order: find the first giant within dm_tol of
-  // the tile's smallest DM
-  const int dm_first = gb.dm[i_first];
-  int lo = 0, hi = i_first;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if ((long long)gb.dm[mid] + (long long)a.dm_tol < (long long)dm_first) lo = mid + 1;
-    else hi = mid;
-  }
-  for (int j0 = lo; j0 <= i_last; j0 += CL_TILE) {
-    int j = j0 + threadIdx.x;
+  const int start_best = best;
+  for (int j0 = j_begin; j0 < j_end; j0 += CL_TILE) {
+    const int j = j0 + threadIdx.x;
     __syncthreads();
-    if (j <= i_last) {
+    if (j < j_end) {
       s_samp[threadIdx.x] = gb.ind[j];
       s_f[threadIdx.x] = gb.filter[j];
       s_dm[threadIdx.x] = gb.dm[j];
@@ -833,22 +1121,35 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
     }
     __syncthreads();
     if (i < a.ngiants) {
-      int jn = min(CL_TILE, i - j0);  // only j < i
+      const int jn = min(min(CL_TILE, j_end - j0), i - j0);  // only j < i
       for (int jj = 0; jj < jn; jj++) {
-        int fj = s_f[jj];
-        int wmax = max(1 << fi, 1 << fj);
-        unsigned long long tt = a.time_tol * (unsigned long long)wmax;
-        unsigned long long sj = s_samp[jj];
-        bool coinc = (sj / a.nsamps_beam) == bi &&
-                     (unsigned long long)abs((int)sj - (int)si) <= tt &&
-                     (unsigned long long)abs(fj - fi) <= a.filter_tol &&
-                     (unsigned long long)abs(s_dm[jj] - di) <= a.dm_tol;
+        const int fj = s_f[jj];
+        const int wmax = max(1 << fi, 1 << fj);
+        const unsigned long long tt = a.time_tol * (unsigned long long)wmax;
+        const unsigned long long sj = s_samp[jj];
+        const bool coinc = (sj / a.nsamps_beam) == bi &&
+                           (unsigned long long)abs((int)sj - (int)si) <= tt &&
+                           (unsigned long long)abs(fj - fi) <= a.filter_tol &&
+                           (unsigned long long)abs(s_dm[jj] - di) <= a.dm_tol;
         if (coinc && s_lab[jj] < best) best = s_lab[jj];
       }
     }
   }
-  if (i < a.ngiants && best < gb.label[i]) {
-    atomicMin(&gb.label[i], best);
+  if (i < a.ngiants && best < start_best) {
+    int old = atomicMin(&gb.label[i], best);
+    if (best < old) *changed = 1u;
+  }
+}
+
+// Path jumping: lab[i] is reachable from i, so anything reachable from lab[i]
+// is too; taking lab[lab[i]] keeps every label on the same fixed point.
+__global__ void k_cluster_jump(int* label, int n, unsigned* changed) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int l = label[i];
+  int ll = *((volatile int*)&label[l]);
+  if (ll < l) {
+    atomicMin(&label[i], ll);
     *changed = 1u;
   }
 }
@@ -862,7 +1163,9 @@ cudaError_t cluster_init(GiantBuffers& gb, int n, cudaStream_t s) {
 cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* changed,
                           cudaStream_t s) {
   if (a.ngiants == 0) return cudaSuccess;
-  k_cluster_sweep<<<(a.ngiants + CL_TILE - 1) / CL_TILE, CL_TILE, 0, s>>>(a, gb, changed); note_launch();
+  dim3 grid((a.ngiants + CL_TILE - 1) / CL_TILE, (a.ngiants + CL_JCHUNK - 1) / CL_JCHUNK);
+  k_cluster_sweep<<<grid, CL_TILE, 0, s>>>(a, gb, changed); note_launch();
+  k_cluster_jump<<<(a.ngiants + 255) / 256, 256, 0, s>>>(gb.label, a.ngiants, changed); note_launch();
   return cudaGetLastError();
 }
 

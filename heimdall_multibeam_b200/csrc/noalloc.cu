@@ -101,7 +101,7 @@ extern "C" hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size
                       kTreeFloats};
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t spitch = nsamps + 64;
+  const size_t spitch = (nsamps + 64 + 3) & ~(size_t)3;  // multiple of 4 floats
   // The array keeps the previous call's contents; the series (and the zero
   // the baseline stretch may read after its last sample) must start at zero.
   if (cudaMemsetAsync(x, 0, spitch * sizeof(float), s) != cudaSuccess) return HD_INTERNAL_GPU_ERROR;

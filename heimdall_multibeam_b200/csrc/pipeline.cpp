@@ -381,6 +381,8 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     wctx.offset = (int)cur_off;
     wctx.nw = nw;
     wctx.winfo = pl->winfo.as<hdb::WidthInfo>();
+    wctx.host_winfo = wi.data();
+    wctx.scan_len = nc + 1;
     wctx.norm = pl->norm.as<float>();
     wctx.thresh = P.detect_thresh;
     int n_ts1 = 0;
