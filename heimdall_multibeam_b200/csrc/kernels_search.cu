@@ -10,6 +10,8 @@
 // per block in shared memory: level-k value j of a tree depends only on the
 // aligned input block [j*5^k, (j+1)*5^k), and the reference's per-level
 // truncation (size/5) keeps exactly the complete blocks.
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -346,9 +348,9 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // float sum.  Loads run SCAN_AHEAD chunks ahead of the chain (the chain is
 // ~4 cycles per sample; a load round trip is hundreds of cycles).
 // ===========================================================================
-constexpr int SQ_SER = 8;        // series per block (one chain lane each)
+constexpr int SQ_SER = 2;        // series per block (one chain lane each)
 constexpr int SQ_CH = 256;       // samples per series per stage
-constexpr int SQ_THREADS = 64;
+constexpr int SQ_THREADS = 32;
 constexpr int SQ_PAD = SQ_CH + 4;  // 16-byte rows; lane s reads banks 4s..4s+3
 constexpr int SQ_MAXB = 64;      // beams whose RMS is kept in shared memory
 
@@ -511,11 +513,11 @@ __global__ void k_block_rms_pass1(WidthCtx ctx, int w0, int m, float* __restrict
 // (a multibeam group straddling a beam gap) or the window does not fit.
 constexpr int MULTI_SMEM_FLOATS = 12288;
 
-__global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m,
+__global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m, int win,
                                         float* __restrict__ out, size_t out_pitch) {
   extern __shared__ float dyn[];
-  float* tile = dyn;                         // MULTI_SMEM_FLOATS
-  float* sm = dyn + MULTI_SMEM_FLOATS;       // tree buffers
+  float* tile = dyn;                         // win floats
+  float* sm = dyn + win;                     // tree buffers
   const size_t ser = blockIdx.y;
   const size_t g = blockIdx.x;
   const WidthInfo& w_first = ctx.winfo[w0];
@@ -529,7 +531,7 @@ __global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m,
   const int offset = ctx.offset;
   const bool contig = (i_last - i_first == gsz - 1);
   const size_t span = (i_last - i_first) + 2 * (size_t)offset + 2;
-  const bool staged = contig && span <= MULTI_SMEM_FLOATS;
+  const bool staged = contig && span <= (size_t)win;
   if (staged) {
     for (size_t k = threadIdx.x; k < span; k += blockDim.x) tile[k] = sc[i_first + k];
     __syncthreads();
@@ -597,11 +599,13 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
   bool unscrunched = true;
   for (int wi = w_begin; wi < w_end; wi++) unscrunched = unscrunched && hw[wi].ts == 1;
   if (unscrunched) {
-    const size_t smem = (MULTI_SMEM_FLOATS + 625 + 125) * sizeof(float);
+    // window: one group of samples plus the widest boxcar on either side
+    const size_t win = std::min<size_t>(pow5(m1) + 2 * (size_t)ctx.offset + 2, MULTI_SMEM_FLOATS);
+    const size_t smem = (win + 625 + 125) * sizeof(float);
     cudaFuncSetAttribute(k_block_rms_pass1_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     k_block_rms_pass1_multi<<<dim3((unsigned)ng1, ctx.nser), TREE_THREADS, smem, s>>>(
-        ctx, w_begin, nwb, m1, ws.a, ng1); note_launch();
+        ctx, w_begin, nwb, m1, (int)win, ws.a, ng1); note_launch();
   } else {
     k_block_rms_pass1<<<seg_grid(ng1, nwb, ctx.nser), TREE_THREADS, 0, s>>>(ctx, w_begin, m1,
                                                                            ws.a, ng1); note_launch();
@@ -623,10 +627,6 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
 constexpr int HIT_TILE = 2048;
 constexpr int HIT_THREADS = 256;
 constexpr int HIT_PER_THREAD = HIT_TILE / HIT_THREADS;
-// The multi-width kernels use a longer tile so the boxcar_max halo of the
-// staged prefix-sum window costs less per sample.
-constexpr int MHIT_TILE = 2048;
-constexpr int MHIT_PER_THREAD = MHIT_TILE / HIT_THREADS;
 
 __device__ __forceinline__ bool hit_at(const WidthCtx& ctx, const float* sc, float norm,
                                        const WidthInfo& w, size_t i, float* val) {
@@ -743,39 +743,43 @@ __device__ __forceinline__ void load_hit_tile(const float* sc, size_t i0, float*
   __syncthreads();
 }
 
+// Sample j of a tile (j = k * HIT_THREADS + thread) so consecutive lanes read
+// consecutive words of the staged window (no bank conflicts).  The in-window
+// test (n, beam-local bn) is the same for every unscrunched width, so it is
+// evaluated once per sample.
+__device__ __forceinline__ unsigned hit_window_mask(const WidthCtx& ctx, const WidthInfo& w,
+                                                    size_t i0) {
+  unsigned m = 0;
+  const unsigned ustride = (unsigned)ctx.stride;
+#pragma unroll
+  for (int k = 0; k < HIT_PER_THREAD; k++) {
+    const unsigned i = (unsigned)(i0 + (size_t)k * HIT_THREADS + threadIdx.x);
+    if (i < w.n && (i % ustride) < w.bn) m |= 1u << k;
+  }
+  return m;
+}
+
 __global__ void __launch_bounds__(HIT_THREADS) k_count_hits_multi(WidthCtx ctx, HitBuffers hb,
                                                                   int nw1, size_t slen) {
   extern __shared__ float tile[];
   const size_t ser = blockIdx.y;
   const unsigned t = blockIdx.x;
   const float* sc = ctx.scan + ser * ctx.scan_pitch;
-  const size_t i0 = (size_t)t * MHIT_TILE;
-  if (i0 >= ctx.winfo[0].n) {
-    // the grid is sized for the short per-width tiles: rows must read zero here
-    if (threadIdx.x < nw1) hb.tile_cnt[(ser * ctx.nw + threadIdx.x) * hb.ntiles + t] = 0;
-    return;
-  }
-  const size_t span = MHIT_TILE + 2 * (size_t)ctx.offset + 2;
+  const size_t i0 = (size_t)t * HIT_TILE;
+  const size_t span = HIT_TILE + 2 * (size_t)ctx.offset + 2;
   load_hit_tile(sc, i0, tile, span, slen);
   __shared__ unsigned red[HIT_THREADS / 32];
-  const unsigned ustride = (unsigned)ctx.stride;
-  const unsigned it0 = (unsigned)(i0 + (size_t)threadIdx.x * MHIT_PER_THREAD);
-  const unsigned samp0 = it0 % ustride;  // beam-local index of the thread's first sample
+  const unsigned inwin = hit_window_mask(ctx, ctx.winfo[0], i0);
   for (int wi = 0; wi < nw1; wi++) {
     const WidthInfo& w = ctx.winfo[wi];
     const float norm = ctx.norm[ser * ctx.nw + wi];
     const int a = ctx.offset + w.ahead, b = ctx.offset - w.behind;
     unsigned c = 0;
-    unsigned samp = samp0;
-#pragma unroll 8
-    for (int k = 0; k < MHIT_PER_THREAD; k++) {
-      const unsigned kl = threadIdx.x * MHIT_PER_THREAD + k;
-      const unsigned i = it0 + k;
-      if (i < w.n && samp < w.bn) {
-        float v = __fmul_rn(__fsub_rn(tile[kl + a], tile[kl + b]), norm);
-        c += (v > ctx.thresh);
-      }
-      if (++samp == ustride) samp = 0;
+#pragma unroll
+    for (int k = 0; k < HIT_PER_THREAD; k++) {
+      const unsigned kl = k * HIT_THREADS + threadIdx.x;
+      const float v = __fmul_rn(__fsub_rn(tile[kl + a], tile[kl + b]), norm);
+      c += ((inwin >> k) & 1u) && (v > ctx.thresh);
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -801,56 +805,52 @@ __global__ void __launch_bounds__(HIT_THREADS) k_write_hits_multi(WidthCtx ctx, 
   for (int wi = 0; wi < nw1; wi++) any |= hb.tile_cnt[(ser * ctx.nw + wi) * hb.ntiles + t];
   if (!any) return;
   const float* sc = ctx.scan + ser * ctx.scan_pitch;
-  const size_t i0 = (size_t)t * MHIT_TILE;
-  const size_t span = MHIT_TILE + 2 * (size_t)ctx.offset + 2;
+  const size_t i0 = (size_t)t * HIT_TILE;
+  const size_t span = HIT_TILE + 2 * (size_t)ctx.offset + 2;
   load_hit_tile(sc, i0, tile, span, slen);
-  __shared__ unsigned wsum[HIT_THREADS / 32];
+  constexpr int NWARP = HIT_THREADS / 32;
+  __shared__ unsigned wcnt[HIT_PER_THREAD][NWARP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned ustride = (unsigned)ctx.stride;
-  const unsigned it0 = (unsigned)(i0 + (size_t)threadIdx.x * MHIT_PER_THREAD);
-  const unsigned samp0 = it0 % ustride;
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned inwin = hit_window_mask(ctx, ctx.winfo[0], i0);
   for (int wi = 0; wi < nw1; wi++) {
     const size_t sw = ser * ctx.nw + wi;
     if (hb.tile_cnt[sw * hb.ntiles + t] == 0) continue;  // uniform across the block
     const WidthInfo& w = ctx.winfo[wi];
     const float norm = ctx.norm[sw];
     const int a = ctx.offset + w.ahead, b = ctx.offset - w.behind;
-    unsigned flags = 0;
-    float vals[MHIT_PER_THREAD];
-    unsigned samp = samp0;
-#pragma unroll
-    for (int k = 0; k < MHIT_PER_THREAD; k++) {
-      const unsigned kl = threadIdx.x * MHIT_PER_THREAD + k;
-      const unsigned i = it0 + k;
-      vals[k] = 0.f;
-      if (i < w.n && samp < w.bn) {
-        vals[k] = __fmul_rn(__fsub_rn(tile[kl + a], tile[kl + b]), norm);
-        if (vals[k] > ctx.thresh) flags |= 1u << k;
-      }
-      if (++samp == ustride) samp = 0;
-    }
-    unsigned c = __popc(flags);
-    unsigned x = c;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      unsigned y = __shfl_up_sync(0xffffffffu, x, d);
-      if (lane >= d) x += y;
-    }
-    if (lane == 31) wsum[warp] = x;
-    __syncthreads();
-    unsigned wpre = 0;
-    for (int k = 0; k < warp; k++) wpre += wsum[k];
-    unsigned pos = hb.sw_off[sw] + hb.tile_off[sw * hb.ntiles + t] + wpre + x - c;
+    float vals[HIT_PER_THREAD];
+    unsigned bal[HIT_PER_THREAD];
 #pragma unroll
     for (int k = 0; k < HIT_PER_THREAD; k++) {
-      if (flags & (1u << k)) {
+      const unsigned kl = k * HIT_THREADS + threadIdx.x;
+      vals[k] = __fmul_rn(__fsub_rn(tile[kl + a], tile[kl + b]), norm);
+      const bool f = ((inwin >> k) & 1u) && (vals[k] > ctx.thresh);
+      bal[k] = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) wcnt[k][warp] = __popc(bal[k]);
+    }
+    __syncthreads();
+    // hits before this thread's sample k in index order: all samples of
+    // rounds < k, then lower warps and lower lanes of round k
+    unsigned base = hb.sw_off[sw] + hb.tile_off[sw * hb.ntiles + t];
+#pragma unroll
+    for (int k = 0; k < HIT_PER_THREAD; k++) {
+      unsigned before = 0, round = 0;
+#pragma unroll
+      for (int ww = 0; ww < NWARP; ww++) {
+        const unsigned cw = wcnt[k][ww];
+        round += cw;
+        before += (ww < warp) ? cw : 0u;
+      }
+      if ((bal[k] >> lane) & 1u) {
+        const unsigned pos = base + before + __popc(bal[k] & lt);
         if (pos < hb.cap) {
-          hb.ind[pos] = it0 + k;
+          hb.ind[pos] = (unsigned)(i0 + (size_t)k * HIT_THREADS + threadIdx.x);
           hb.val[pos] = vals[k];
           hb.sw[pos] = (unsigned)sw;
         }
-        pos++;
       }
+      base += round;
     }
     __syncthreads();
   }
@@ -863,7 +863,7 @@ cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cud
   // unscrunched widths share one staged window per tile
   int nw1 = 0;
   while (nw1 < ctx.nw && ctx.host_winfo[nw1].ts == 1) nw1++;
-  const size_t smem = (MHIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
+  const size_t smem = (HIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
   const size_t slen = ctx.scan_len;
   if (nw1 > 0 && smem <= 200 * 1024) {
     cudaFuncSetAttribute(k_count_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -887,7 +887,7 @@ cudaError_t scan_hit_counts(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s)
 cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
   int nw1 = 0;
   while (nw1 < ctx.nw && ctx.host_winfo[nw1].ts == 1) nw1++;
-  const size_t smem = (MHIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
+  const size_t smem = (HIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
   const size_t slen = ctx.scan_len;
   if (nw1 > 0 && smem <= 200 * 1024) {
     cudaFuncSetAttribute(k_write_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
