@@ -206,9 +206,13 @@ def run_product(args):
     barrier()
     e0.record()
     ncand = 0
+    stage_e2e = {k: 0.0 for k in stage}
     for _ in range(args.steps):
         err, proc = pl.execute_ptr(h_fb.data_ptr(), nsamps)
         ncand = len(pl.candidates())
+        t = pl.timing()
+        for k in stage_e2e:
+            stage_e2e[k] += t[k]
     e1.record()
     barrier()
     ms_e2e = e0.elapsed_time(e1) / args.steps
@@ -236,8 +240,13 @@ def run_product(args):
         int_ach = adds / (t_dd / 1e3) / 1e12
         traffic = None
         try:
-            with open(os.path.join(ROOT, "profiles", "dedisp_traffic.json")) as f:
-                traffic = json.load(f).get("bytes_per_launch")
+            # DRAM bytes per k_dedisp launch from the committed ncu summary
+            with open(os.path.join(ROOT, "profiles", "k_dedisp_c1024_n131072.md")) as f:
+                for ln in f:
+                    if ln.startswith("traffic_bytes_per_launch_full_size:"):
+                        traffic = int(ln.split(":")[1])
+            if nsamps != 262144:
+                traffic = None
         except Exception:
             pass
         hit, nstrong = recall(cands, b.pulses, w.dt)
@@ -253,7 +262,9 @@ def run_product(args):
                        "l2": "input 256 MiB > L2, no flush", "parallelism": f"replicas{world}"},
             "e2e": {"value": round(e2e, 3), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
                     "h2d_bytes_per_step": int(nsamps * nchans),
-                    "d2h_bytes_per_step": int(ncand * 64 + 128)},
+                    "d2h_bytes_per_step": int(ncand * 64 + 128),
+                    "stage_ms": {k: round(v / args.steps, 4) for k, v in stage_e2e.items()},
+                    "host_buffer": "pinned (torch pin_memory)"},
             "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},
             "roofline": {"kernel": "k_dedisp", "bound": "hbm", "achieved": round(achieved, 2),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",

@@ -12,7 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import subprocess
-from typing import Dict, Optional, Sequence, Tuple
+from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -129,6 +129,9 @@ SYMBOLS = {
                                           C.c_float, _SZ, _SZ]),
     "hd_set_cleaning": (C.c_int, [_P, C.c_int]),
     "hd_execute_device": (C.c_int, [_P, _P, _SZ, _SZ, _SZ, _SZ, _SZP]),
+    "hd_execute_beams": (C.c_int, [_P, C.POINTER(_P), _SZ, _SZ, _SZ, _SZ, _SZ, _SZP, C.c_int,
+                                   C.POINTER(C.c_int), _SZP]),
+    "hd_get_beam_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
     "hd_get_launch_count": (C.c_ulonglong, []),
     "hd_clean_filterbank_rfi_noalloc": (C.c_int, [_P, _SZ, _SZ, _SZ, _P, _P, C.c_float,
                                                   C.c_float, C.c_float, _SZ, _SZ, _P]),
@@ -280,12 +283,57 @@ class Pipeline:
                                       C.byref(proc))
         return err, proc.value
 
-    def candidates(self) -> np.ndarray:
+    def execute_beams(self, filterbanks: Sequence, nsamps: Optional[int] = None,
+                      nbeams: int = 1, first_idx: int = 0, beams: Optional[Sequence[int]] = None,
+                      on_device: bool = False,
+                      raise_on_error: bool = True) -> Tuple[int, int, List[int]]:
+        """hd_execute_beams over independent filterbanks: uint8 arrays of equal
+        shape (nsamps, nchans), or raw pointers (host, or device when
+        on_device) with nsamps given.  Returns (hd_error, nsamps_processed,
+        per-filterbank statuses)."""
+        keep = []
+        ptrs = (_P * max(len(filterbanks), 1))()
+        for u, fb in enumerate(filterbanks):
+            if isinstance(fb, int):
+                if nsamps is None:
+                    raise ValueError("nsamps is required with raw pointers")
+                ptrs[u] = fb
+            else:
+                a = _u8(fb)
+                if nsamps is None:
+                    nsamps = a.shape[0]
+                if a.shape[0] != nsamps:
+                    raise ValueError("all filterbanks need the same number of samples")
+                keep.append(a)
+                ptrs[u] = a.ctypes.data
+        n = len(filterbanks)
+        st = (C.c_int * max(n, 1))()
+        bm = None
+        if beams is not None:
+            bm = (C.c_size_t * n)(*beams)
+        proc = C.c_size_t(0)
+        err = lib().hd_execute_beams(self._p, ptrs, n, nsamps or 0, 8, first_idx, nbeams, bm,
+                                     1 if on_device else 0, st, C.byref(proc))
+        if raise_on_error and err not in (HD_NO_ERROR, HD_TOO_MANY_EVENTS):
+            raise HdError(err, "hd_execute_beams")
+        return err, proc.value, [int(st[u]) for u in range(n)]
+
+    def candidates(self, index: Optional[int] = None) -> np.ndarray:
+        """Candidates of the last execute (all), or of filterbank `index` of
+        the last execute_beams."""
         n = C.c_size_t(0)
-        lib().hd_get_candidates(self._p, None, C.byref(n))
+        if index is None:
+            lib().hd_get_candidates(self._p, None, C.byref(n))
+        else:
+            err = lib().hd_get_beam_candidates(self._p, index, None, C.byref(n))
+            if err != HD_NO_ERROR:
+                raise HdError(err, "hd_get_beam_candidates")
         out = np.zeros(n.value, CANDIDATE_DTYPE)
         if n.value:
-            lib().hd_get_candidates(self._p, out.ctypes.data, C.byref(n))
+            if index is None:
+                lib().hd_get_candidates(self._p, out.ctypes.data, C.byref(n))
+            else:
+                lib().hd_get_beam_candidates(self._p, index, out.ctypes.data, C.byref(n))
         return out
 
     def giants(self) -> Dict[str, np.ndarray]:

@@ -27,6 +27,9 @@ struct DedispArgs {
   size_t out_pitch;       // floats between DM rows (multiple of 4)
   int rowb;               // shared-memory row bytes (multiple of 16)
   unsigned* err;          // device error word (bit 0: staging wait timed out)
+  int units;              // independent filterbanks dedispersed by one launch
+  size_t in_unit;         // bytes between units' FT inputs
+  size_t out_unit;        // floats between units' outputs
 };
 
 int dedisp_dm_block();
@@ -103,6 +106,8 @@ struct WidthCtx {
   const WidthInfo* winfo;       // device copy
   const WidthInfo* host_winfo;  // host copy (launch decisions)
   size_t scan_len;              // valid prefix-sum entries per series (len + 1)
+  int dms_per_unit;             // series per independent unit (beam searched alone)
+  int dm_key_gap;               // giant DM key = unit * dm_key_gap + DM index
   float* norm;        // [nser][nw]  1 / block_rms
   float thresh;
 };
@@ -169,9 +174,12 @@ cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* chan
 struct GroupRow {
   float peak;
   float dm;
-  unsigned long long ind, begin, end, filter, dm_ind, members;
+  unsigned long long ind, begin, end, filter, dm_ind, members, unit;
 };
-cudaError_t merge_groups(const GiantBuffers& gb, int ngiants, const float* dm_list,
+// offs[u] = first giant of unit u (u = 0..units; offs[units] = n).
+cudaError_t unit_giant_offsets(const GiantBuffers& gb, int n, int dm_key_gap, int units,
+                               unsigned* offs, cudaStream_t s);
+cudaError_t merge_groups(const GiantBuffers& gb, int ngiants, int dm_key_gap, const float* dm_list,
                          unsigned* root_flag, unsigned* root_off, unsigned* nroots,
                          unsigned* scan_tmp, unsigned long long* gkey, GroupRow* rows,
                          cudaStream_t s);

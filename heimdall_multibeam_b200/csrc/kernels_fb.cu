@@ -213,6 +213,8 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
 
   if (warp == NW) {
     // ---------------- producer ----------------
+    // blockIdx.z selects the unit (an independent filterbank of the batch)
+    const uint8_t* __restrict__ in = a.in + (size_t)blockIdx.z * a.in_unit;
     int issued = 0;
     for (int st = 0; st < nstage; st++) {
       const int buf = st % NST;
@@ -240,7 +242,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
       if (lane < nk) {
         const int c = a.chans[k0 + lane];
         const size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
-        bulk_g2s(rows + (size_t)(buf * CH + lane) * a.rowb, a.in + (size_t)c * a.in_pitch + lo,
+        bulk_g2s(rows + (size_t)(buf * CH + lane) * a.rowb, in + (size_t)c * a.in_pitch + lo,
                  (uint32_t)a.rowb, &full[buf]);
       }
       issued = st + 1;
@@ -331,11 +333,12 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
   }
   if (failed) return;
   drain();
+  float* __restrict__ out = a.out + (size_t)blockIdx.z * a.out_unit;
 #pragma unroll
   for (int d = 0; d < 2; d++) {
     int dd = d_lo + 2 * warp + d;
     if (dd >= a.dm_count) continue;
-    float* o = a.out + (size_t)dd * a.out_pitch;
+    float* o = out + (size_t)dd * a.out_pitch;
 #pragma unroll
     for (int g = 0; g < G; g++) {
       size_t t = t0 + 4 * (lane + 32 * g);
@@ -395,7 +398,9 @@ cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s) {
                                        (int)smem);
   if (e != cudaSuccess) return e;
   const int DB = 2 * DD_NW, TB = 128 * DD_G;
-  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB));
+  if (a.units < 1 || a.units > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),
+            (unsigned)a.units);
   kern<<<grid, (DD_NW + 1) * 32, smem, s>>>(a); note_launch();
   return cudaGetLastError();
 }

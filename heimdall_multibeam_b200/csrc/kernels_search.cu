@@ -1025,8 +1025,11 @@ __global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, Gian
   if (is_head) gb.begin[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * scr;
   if (is_last) gb.end[g] = ((unsigned long long)hb.ind[k] + 1ull + w.rel_off) * scr;
   if (is_head) {
+    // DM key: units (beams searched independently) are kept dm_key_gap > dm_tol
+    // apart so clustering never links two units
+    const unsigned ser = sw / ctx.nw;
     gb.filter[g] = w.filter_idx;
-    gb.dm[g] = (int)(sw / ctx.nw);
+    gb.dm[g] = (int)((ser / ctx.dms_per_unit) * ctx.dm_key_gap + ser % ctx.dms_per_unit);
   }
 }
 
@@ -1189,7 +1192,7 @@ __global__ void k_merge_reduce(GiantBuffers gb, int n, const unsigned* root_off,
   atomicAdd(&members[g], 1ull);
 }
 
-__global__ void k_merge_emit(GiantBuffers gb, const unsigned* ngroups,
+__global__ void k_merge_emit(GiantBuffers gb, int dm_key_gap, const unsigned* ngroups,
                              const unsigned long long* gkey, const unsigned long long* members,
                              const float* dm_list, GroupRow* rows) {
   unsigned g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1201,13 +1204,39 @@ __global__ void k_merge_emit(GiantBuffers gb, const unsigned* ngroups,
   r.begin = gb.begin[i];
   r.end = gb.end[i];
   r.filter = (unsigned long long)gb.filter[i];
-  r.dm_ind = (unsigned long long)gb.dm[i];
+  const int key = gb.dm[i];
+  r.dm_ind = (unsigned long long)(key % dm_key_gap);
+  r.unit = (unsigned long long)(key / dm_key_gap);
   r.members = members[g];
-  r.dm = dm_list[gb.dm[i]];
+  r.dm = dm_list[key % dm_key_gap];
   rows[g] = r;
 }
 
-cudaError_t merge_groups(const GiantBuffers& gb, int n, const float* dm_list, unsigned* root_flag,
+// First giant of each unit: giants are ordered by DM key, and unit u's keys
+// lie in [u * dm_key_gap, (u + 1) * dm_key_gap).  offs[u] for u = 0..units.
+__global__ void k_unit_offsets(const int* __restrict__ dm, int n, int dm_key_gap, int units,
+                               unsigned* offs) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u > units) return;
+  const long long target = (long long)u * dm_key_gap;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = lo + (hi - lo) / 2;
+    if ((long long)dm[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  offs[u] = (unsigned)lo;
+}
+
+cudaError_t unit_giant_offsets(const GiantBuffers& gb, int n, int dm_key_gap, int units,
+                               unsigned* offs, cudaStream_t s) {
+  k_unit_offsets<<<(units + 1 + 127) / 128, 128, 0, s>>>(gb.dm, n, dm_key_gap, units, offs);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t merge_groups(const GiantBuffers& gb, int n, int dm_key_gap, const float* dm_list,
+                         unsigned* root_flag,
                          unsigned* root_off, unsigned* nroots, unsigned* scan_tmp,
                          unsigned long long* gkey, GroupRow* rows, cudaStream_t s) {
   if (n == 0) return cudaMemsetAsync(nroots, 0, sizeof(unsigned), s);
@@ -1221,7 +1250,8 @@ cudaError_t merge_groups(const GiantBuffers& gb, int n, const float* dm_list, un
   k_merge_reduce<<<(n + 255) / 256, 256, 0, s>>>(gb, n, root_off, gkey, members); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // emit for every possible group index; rows beyond nroots are never read
-  k_merge_emit<<<(n + 255) / 256, 256, 0, s>>>(gb, nroots, gkey, members, dm_list, rows); note_launch();
+  k_merge_emit<<<(n + 255) / 256, 256, 0, s>>>(gb, dm_key_gap, nroots, gkey, members, dm_list,
+                                               rows); note_launch();
   return cudaGetLastError();
 }
 

@@ -67,12 +67,14 @@ struct hd_pipeline_t {
   DevBuf tile_cnt, tile_off, sw_cnt, sw_off, hit_ind, hit_val, hit_sw;
   DevBuf head, gid, gkey, g_peak, g_ind, g_begin, g_end, g_filter, g_dm, g_label;
   DevBuf scan_tmp, small;  // small: totals / flags
-  DevBuf root_flag, root_off, mkey, rows;
+  DevBuf root_flag, root_off, mkey, rows, unit_off;
   DevBuf h_small_dev;
 
   unsigned* h_small = nullptr;  // pinned host words
 
-  std::vector<hd_candidate> cands;
+  std::vector<hd_candidate> cands;                     // all units, unit by unit
+  std::vector<std::vector<hd_candidate>> unit_cands;   // per unit
+  std::vector<unsigned> unit_first;                    // first giant of each unit
   std::vector<float> g_peaks;
   std::vector<hd_size> g_inds, g_begins, g_ends, g_filters, g_dms, g_labels;
 
@@ -126,43 +128,53 @@ size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Scratch needed by the median trees of `nseg` segments of `count` values.
 size_t tree_cap(size_t nseg, size_t count) { return nseg * (count / 3125 + 8) + 64; }
 
-// Device clean_filterbank_rfi on the TF filterbank in pl->fb_tf; writes the
-// zapped filterbank channel-major into fb_ft (pitch) and, if out_tf, also
-// time-major.  Pipeline/clean_filterbank_rfi.cu:256-528.
-hd_error clean_device(hd_pipeline pl, size_t nsamps, size_t nchans, float dt,
-                      float baseline_length, float rfi_tol, size_t boxcar_max, size_t nbeams,
-                      uint8_t* fb_ft, size_t pitch, uint8_t* out_tf) {
+// Device clean_filterbank_rfi (Pipeline/clean_filterbank_rfi.cu:256-528) of
+// `units` independent filterbanks (TF, nsamps x nchans bytes each, one after
+// the other at tf).  Writes each zapped filterbank channel-major into
+// fb_ft + u * nchans * pitch and, if out_tf, also time-major.  The zero-DM
+// series of all units are baselined, normalised and summed as one batch.
+hd_error clean_units(hd_pipeline pl, size_t units, const uint8_t* tf, size_t nsamps,
+                     size_t nchans, float dt, float baseline_length, float rfi_tol,
+                     size_t boxcar_max, size_t nbeams, uint8_t* fb_ft, size_t pitch,
+                     uint8_t* out_tf) {
   cudaStream_t s = pl->stream;
   const size_t nsmooth = (size_t)(baseline_length / (2 * dt));
   if (nsamps < boxcar_max + 1 || nsmooth / 4 >= nsamps) return HD_TOO_FEW_NSAMPS;
   const size_t spitch = round_up(nsamps + 8, 64);
-  HD_TRY(pl->dm0.ensure(spitch * sizeof(float)));
-  HD_TRY(pl->dm0_scan.ensure(spitch * sizeof(float)));
-  HD_TRY(pl->mask.ensure((nsamps + 64) * sizeof(int)));
+  const size_t U = units;
+  HD_TRY(pl->dm0.ensure(U * spitch * sizeof(float)));
+  HD_TRY(pl->dm0_scan.ensure(U * spitch * sizeof(float)));
+  HD_TRY(pl->mask.ensure((U * nsamps + 64) * sizeof(int)));
   HD_TRY(pl->fmask.ensure((nsamps + 256) * sizeof(int)));
-  HD_TRY(pl->rms0.ensure(nbeams * sizeof(float) + 64));
-  HD_TRY(pl->base.ensure((nbeams * hdb::baseline_samples(nsamps / nbeams, nsmooth) + 64) *
+  HD_TRY(pl->rms0.ensure(U * nbeams * sizeof(float) + 64));
+  HD_TRY(pl->base.ensure((U * nbeams * hdb::baseline_samples(nsamps / nbeams, nsmooth) + 64) *
                          sizeof(float)));
-  size_t cap = std::max(tree_cap(nbeams, nsamps),
-                        hdb::baseline_scratch(nsamps / nbeams, nsmooth, nbeams));
+  size_t cap = std::max(tree_cap(U * nbeams, nsamps),
+                        hdb::baseline_scratch(nsamps / nbeams, nsmooth, U * nbeams));
   HD_TRY(pl->ws_a.ensure(cap * sizeof(float)));
   HD_TRY(pl->ws_b.ensure(cap * sizeof(float)));
   float* x = pl->dm0.as<float>();
-  HD_TRY(cudaMemsetAsync(x, 0, spitch * sizeof(float), s));
-  HD_TRY(hdb::launch_dm0_sum(pl->fb_tf.as<uint8_t>(), nsamps, (int)nchans, x, s));
-  hdb::SeriesBatch sb{x, spitch, 1, nsamps, nsamps / nbeams, nsamps / nbeams, (int)nbeams};
+  HD_TRY(cudaMemsetAsync(x, 0, U * spitch * sizeof(float), s));
+  for (size_t u = 0; u < U; u++)
+    HD_TRY(hdb::launch_dm0_sum(tf + u * nsamps * nchans, nsamps, (int)nchans, x + u * spitch, s));
+  hdb::SeriesBatch sb{x, spitch, (int)U, nsamps, nsamps / nbeams, nsamps / nbeams, (int)nbeams};
   hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
   HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
   HD_TRY(hdb::rms_beams(sb, pl->rms0.as<float>(), ws, s));
   HD_TRY(hdb::normalise_scan(sb, pl->rms0.as<float>(), pl->dm0_scan.as<float>(), spitch, x, s));
-  HD_TRY(hdb::rfi_mask(x, pl->dm0_scan.as<float>(), nsamps, boxcar_max, rfi_tol,
-                       pl->mask.as<int>(), pl->fmask.as<int>(), s));
-  HD_TRY(hdb::launch_zap(pl->fb_tf.as<uint8_t>(), nsamps, (int)nchans, pl->mask.as<int>(),
-                         (unsigned)(nsmooth / 4), fb_ft, pitch, out_tf, s));
+  for (size_t u = 0; u < U; u++) {
+    int* mask = pl->mask.as<int>() + u * nsamps;
+    HD_TRY(hdb::rfi_mask(x + u * spitch, pl->dm0_scan.as<float>() + u * spitch, nsamps,
+                         boxcar_max, rfi_tol, mask, pl->fmask.as<int>(), s));
+    HD_TRY(hdb::launch_zap(tf + u * nsamps * nchans, nsamps, (int)nchans, mask,
+                           (unsigned)(nsmooth / 4), fb_ft ? fb_ft + u * nchans * pitch : nullptr,
+                           pitch, out_tf ? out_tf + u * nsamps * nchans : nullptr, s));
+  }
   return HD_NO_ERROR;
 }
 
-void write_cand_file(hd_pipeline pl, size_t first_idx) {
+void write_cand_file(hd_pipeline pl, const std::vector<hd_candidate>& cands, size_t beam,
+                     size_t first_idx) {
   if (!pl->has_output_dir) return;
   char buffer[64];
   time_t off = pl->params.spectra_per_second
@@ -172,15 +184,15 @@ void write_cand_file(hd_pipeline pl, size_t first_idx) {
   struct tm tmv;
   gmtime_r(&now, &tmv);
   strftime(buffer, sizeof(buffer), "%Y-%m-%d-%H:%M:%S", &tmv);
-  char beam[32];
-  snprintf(beam, sizeof(beam), "%02zu", (size_t)(pl->params.beam + 1));
-  std::string fn = pl->output_dir + "/" + buffer + "_" + beam + ".cand";
+  char bname[32];
+  snprintf(bname, sizeof(bname), "%02zu", beam + 1);
+  std::string fn = pl->output_dir + "/" + buffer + "_" + bname + ".cand";
   FILE* f = fopen(fn.c_str(), "w");
   if (!f) {
     fprintf(stdout, "Skipping dump due to bad file open on %s\n", fn.c_str());
     return;
   }
-  for (const hd_candidate& c : pl->cands)
+  for (const hd_candidate& c : cands)
     fprintf(f, "%g\t%zu\t%g\t%zu\t%zu\t%g\t%zu\t%zu\t%zu\t%zu\t\n", (double)c.snr, c.samp_idx,
             (double)c.time, c.filter, c.dm_trial, (double)c.dm, c.members, c.begin, c.end,
             c.beam);
@@ -253,11 +265,19 @@ hd_error hd_set_cleaning(hd_pipeline pl, int enable) {
   return HD_NO_ERROR;
 }
 
-static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool on_device,
-                             hd_size nsamps, hd_size nbits, hd_size first_idx, hd_size nbeams,
-                             hd_size* nsamps_processed) {
+// One gulp of `U` units (independent filterbanks of nsamps x nchans bytes,
+// each holding nbeams time-concatenated beams) through one batched pass:
+// every stage runs over all units' DM series at once; giants carry a DM key
+// that keeps units more than dm_tol apart, so clustering never links units
+// and each unit's result equals a separate hd_execute of it.
+static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t U, bool on_device,
+                              hd_size nsamps, hd_size nbits, hd_size first_idx, hd_size nbeams,
+                              const hd_size* beams, hd_error* statuses,
+                              hd_size* nsamps_processed) {
   if (!pl) return HD_INVALID_PIPELINE;
-  if (!h_filterbank || !nsamps_processed) return HD_INVALID_POINTER;
+  if (!fbs || !nsamps_processed || U == 0) return HD_INVALID_POINTER;
+  for (size_t u = 0; u < U; u++)
+    if (!fbs[u]) return HD_INVALID_POINTER;
   if (nbits != 8) return HD_INVALID_NBITS;
   const hd_params& P = pl->params;
   const size_t C = P.nchans;
@@ -266,8 +286,12 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
   if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
   cudaStream_t s = pl->stream;
   pl->cands.clear();
+  pl->unit_cands.assign(U, {});
+  pl->unit_first.assign(U + 1, 0);
   pl->g_peaks.clear();
   std::memset(pl->timing, 0, sizeof(pl->timing));
+  if (statuses)
+    for (size_t u = 0; u < U; u++) statuses[u] = HD_NO_ERROR;
 
   // killmask: manual channel zaps (clean_filterbank_rfi.cu:530-545)
   std::vector<int> km(C, 1);
@@ -279,6 +303,12 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
   if (de != DEDISP_NO_ERROR) return dedisp_err(de);
   const size_t max_delay = pl->plan->max_delay;
   const size_t D = pl->plan->dm_list.size();
+  // series of all units share the kernels' y/z grid dimensions
+  if (U * D > 65535) return HD_INVALID_STRIDE;
+  // DM keys: unit u's trial d is u * gap + d with gap - (D - 1) > dm_tol
+  const size_t dm_tol = std::min<size_t>(P.cand_sep_dm, D);
+  const size_t gap = D + dm_tol + 2;
+  if ((U + 1) * gap > 0x7FFFFFFFull) return HD_INVALID_STRIDE;
   if (nsamps <= max_delay) {
     *nsamps_processed = 0;
     return HD_TOO_FEW_NSAMPS;
@@ -289,32 +319,38 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
 
   cudaEventRecord(pl->ev[0], s);
   // ---- H2D ----------------------------------------------------------------
-  HD_TRY(pl->fb_tf.ensure(nsamps * C));
-  HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_filterbank, nsamps * C,
-                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  const size_t fb_bytes = nsamps * C;
+  HD_TRY(pl->fb_tf.ensure(U * fb_bytes));
+  for (size_t u = 0; u < U; u++)
+    HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes,
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   cudaEventRecord(pl->ev[1], s);
 
   // ---- clean + channel-major working copy ------------------------------------
   const size_t pitch = hdb::ft_pitch(pl->plan, nsamps);
-  HD_TRY(pl->fb_ft.ensure(pitch * C));
+  const size_t ft_unit = pitch * C;
+  HD_TRY(pl->fb_ft.ensure(U * ft_unit));
   if (pl->cleaning) {
-    hd_error he = clean_device(pl, nsamps, C, P.dt, P.baseline_length, P.rfi_tol, 64, nbeams,
-                               pl->fb_ft.as<uint8_t>(), pitch, nullptr);
+    hd_error he = clean_units(pl, U, pl->fb_tf.as<uint8_t>(), nsamps, C, P.dt, P.baseline_length,
+                              P.rfi_tol, 64, nbeams, pl->fb_ft.as<uint8_t>(), pitch, nullptr);
     if (he != HD_NO_ERROR) return he;
   } else {
-    HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>(), nsamps, (int)C,
-                                       pl->fb_ft.as<uint8_t>(), pitch, s));
+    for (size_t u = 0; u < U; u++)
+      HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>() + u * fb_bytes, nsamps, (int)C,
+                                         pl->fb_ft.as<uint8_t>() + u * ft_unit, pitch, s));
   }
   cudaEventRecord(pl->ev[2], s);
 
   // ---- dedispersion ----------------------------------------------------------
   const size_t dd_pitch = round_up(nc + 1, 4);
-  HD_TRY(pl->dd.ensure(D * dd_pitch * sizeof(float)));
+  const size_t NS = U * D;  // series of the batch, unit-major
+  HD_TRY(pl->dd.ensure(NS * dd_pitch * sizeof(float)));
   float* dd = pl->dd.as<float>();
-  de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>(), pitch, nsamps, dd, dd_pitch, s);
+  de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>(), pitch, nsamps, dd, dd_pitch, s,
+                               U, ft_unit, D * dd_pitch);
   if (de != DEDISP_NO_ERROR) return dedisp_err(de);
   // the element after each series is read (never used) by the baseline stretch
-  HD_TRY(cudaMemset2DAsync(dd + nc, dd_pitch * sizeof(float), 0, sizeof(float), D, s));
+  HD_TRY(cudaMemset2DAsync(dd + nc, dd_pitch * sizeof(float), 0, sizeof(float), NS, s));
   cudaEventRecord(pl->ev[3], s);
 
   const size_t stride = nsamps / nbeams;
@@ -328,22 +364,22 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
   if (search) {
     // ---- per-DM baseline, RMS, normalise + scan ------------------------------
     const size_t bcount = stride - max_delay;
-    hdb::SeriesBatch sb{dd, dd_pitch, (int)D, nc, stride, bcount, (int)nbeams};
+    hdb::SeriesBatch sb{dd, dd_pitch, (int)NS, nc, stride, bcount, (int)nbeams};
     const float cur_dt = P.dt * 1.0f;
     const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
-    size_t cap = std::max({tree_cap(D * nbeams, stride),
-                           tree_cap(D * (log2u(Bmax) + 1), nbeams * stride),
-                           hdb::baseline_scratch(stride, nsmooth, D * nbeams)});
+    size_t cap = std::max({tree_cap(NS * nbeams, stride),
+                           tree_cap(NS * (log2u(Bmax) + 1), nbeams * stride),
+                           hdb::baseline_scratch(stride, nsmooth, NS * nbeams)});
     HD_TRY(pl->ws_a.ensure(cap * sizeof(float)));
     HD_TRY(pl->ws_b.ensure(cap * sizeof(float)));
     hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
-    HD_TRY(pl->base.ensure((D * nbeams * hdb::baseline_samples(stride, nsmooth) + 64) *
+    HD_TRY(pl->base.ensure((NS * nbeams * hdb::baseline_samples(stride, nsmooth) + 64) *
                            sizeof(float)));
-    HD_TRY(pl->rms.ensure(D * nbeams * sizeof(float) + 64));
+    HD_TRY(pl->rms.ensure(NS * nbeams * sizeof(float) + 64));
     HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
     HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
     const size_t scan_pitch = round_up(nc + 1, 4);
-    HD_TRY(pl->scan.ensure(D * scan_pitch * sizeof(float)));
+    HD_TRY(pl->scan.ensure(NS * scan_pitch * sizeof(float)));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), pl->scan.as<float>(), scan_pitch,
                                nullptr, s));
     cudaEventRecord(pl->ev[4], s);
@@ -372,10 +408,10 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     HD_TRY(pl->winfo.ensure(nw * sizeof(hdb::WidthInfo)));
     HD_TRY(cudaMemcpyAsync(pl->winfo.p, wi.data(), nw * sizeof(hdb::WidthInfo),
                            cudaMemcpyHostToDevice, s));
-    HD_TRY(pl->norm.ensure(D * nw * sizeof(float)));
+    HD_TRY(pl->norm.ensure(NS * nw * sizeof(float)));
     wctx.scan = pl->scan.as<float>();
     wctx.scan_pitch = scan_pitch;
-    wctx.nser = (int)D;
+    wctx.nser = (int)NS;
     wctx.stride = stride;
     wctx.nbeams = (int)nbeams;
     wctx.offset = (int)cur_off;
@@ -383,6 +419,8 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     wctx.winfo = pl->winfo.as<hdb::WidthInfo>();
     wctx.host_winfo = wi.data();
     wctx.scan_len = nc + 1;
+    wctx.dms_per_unit = (int)D;
+    wctx.dm_key_gap = (int)gap;
     wctx.norm = pl->norm.as<float>();
     wctx.thresh = P.detect_thresh;
     int n_ts1 = 0;
@@ -392,7 +430,7 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
 
     // ---- threshold + ordered compaction -------------------------------------
     const unsigned ntiles = (unsigned)((wi[0].n + 2047) / 2048);
-    const size_t nsw = D * nw;
+    const size_t nsw = NS * nw;
     HD_TRY(pl->tile_cnt.ensure(nsw * ntiles * sizeof(unsigned)));
     HD_TRY(pl->tile_off.ensure(nsw * ntiles * sizeof(unsigned)));
     HD_TRY(pl->sw_cnt.ensure((nsw + 1) * sizeof(unsigned)));
@@ -456,20 +494,40 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
   }
   cudaEventRecord(pl->ev[6], s);
 
-  // giant-rate bail-out (pipeline.cu:779-787): the running count only grows,
-  // so it trips exactly when the final count does
-  bool too_many = false;
+  // giants of each unit: they are unit-major, so unit u holds [first[u], first[u+1])
+  std::vector<unsigned>& first = pl->unit_first;
+  if (U == 1 || ngiants == 0) {
+    for (size_t u = 1; u <= U; u++) first[u] = ngiants;
+  } else {
+    HD_TRY(pl->unit_off.ensure((U + 1) * sizeof(unsigned)));
+    HD_TRY(hdb::unit_giant_offsets(gb, (int)ngiants, (int)gap, (int)U,
+                                   pl->unit_off.as<unsigned>(), s));
+    HD_TRY(cudaMemcpyAsync(first.data(), pl->unit_off.p, (U + 1) * sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaStreamSynchronize(s));
+  }
+
+  // giant-rate bail-out per unit (pipeline.cu:779-787): the running count
+  // only grows, so it trips exactly when the final count does
+  std::vector<char> too_many(U, 0);
+  bool any_ok = false, any_too_many = false;
   {
     float mins = (float)((double)((float)nsamps * P.dt) / 60.0);
-    if (P.max_giant_rate != 0.0f && ((float)ngiants / mins > P.max_giant_rate)) too_many = true;
+    for (size_t u = 0; u < U; u++) {
+      unsigned gu = first[u + 1] - first[u];
+      if (P.max_giant_rate != 0.0f && ((float)gu / mins > P.max_giant_rate)) too_many[u] = 1;
+      if (too_many[u]) any_too_many = true;
+      else any_ok = true;
+      if (statuses && too_many[u]) statuses[u] = HD_TOO_MANY_EVENTS;
+    }
   }
 
   unsigned ngroups = 0;
   std::vector<hdb::GroupRow> rows;
-  if (!too_many && ngiants > 0) {
+  if (any_ok && ngiants > 0) {
     // ---- clustering ----------------------------------------------------------
     HD_TRY(hdb::cluster_init(gb, (int)ngiants, s));
-    hdb::ClusterArgs ca{(int)ngiants, P.cand_sep_time, P.cand_sep_filter, P.cand_sep_dm,
+    hdb::ClusterArgs ca{(int)ngiants, P.cand_sep_time, P.cand_sep_filter, dm_tol,
                         (unsigned long long)(nsamps / nbeams)};
     unsigned* changed = pl->small.as<unsigned>() + 8;
     for (unsigned it = 0; it <= ngiants; it++) {
@@ -487,9 +545,10 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     HD_TRY(pl->rows.ensure((G + 1) * sizeof(hdb::GroupRow)));
     HD_TRY(pl->scan_tmp.ensure(hdb::scan_tmp_words(G) * sizeof(unsigned)));
     unsigned* nroots = pl->small.as<unsigned>() + 16;
-    HD_TRY(hdb::merge_groups(gb, (int)G, pl->plan->d_dm_list, pl->root_flag.as<unsigned>(),
-                             pl->root_off.as<unsigned>(), nroots, pl->scan_tmp.as<unsigned>(),
-                             pl->mkey.as<unsigned long long>(), pl->rows.as<hdb::GroupRow>(), s));
+    HD_TRY(hdb::merge_groups(gb, (int)G, (int)gap, pl->plan->d_dm_list,
+                             pl->root_flag.as<unsigned>(), pl->root_off.as<unsigned>(), nroots,
+                             pl->scan_tmp.as<unsigned>(), pl->mkey.as<unsigned long long>(),
+                             pl->rows.as<hdb::GroupRow>(), s));
     HD_TRY(cudaMemcpyAsync(pl->h_small + 16, nroots, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     HD_TRY(cudaStreamSynchronize(s));
     ngroups = pl->h_small[16];
@@ -514,7 +573,8 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     pl->g_begins.assign(beg.begin(), beg.end());
     pl->g_ends.assign(end.begin(), end.end());
     pl->g_filters.assign(fil.begin(), fil.end());
-    pl->g_dms.assign(dmi.begin(), dmi.end());
+    pl->g_dms.resize(G);
+    for (size_t g = 0; g < G; g++) pl->g_dms[g] = (hd_size)((unsigned)dmi[g] % gap);
     pl->g_labels.assign(lab.begin(), lab.end());
   } else {
     cudaEventRecord(pl->ev[7], s);
@@ -526,11 +586,14 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
   cudaMemcpy(&derr, pl->plan->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
   if (derr) return HD_INTERNAL_GPU_ERROR;
 
-  // ---- candidate rows (pipeline.cu:1012-1039) ----------------------------------
+  // ---- candidate rows (pipeline.cu:1012-1039), split by unit -------------------
   const unsigned nsamps_beam = (unsigned)(nsamps / nbeams);
   const unsigned nsamps_valid = (unsigned)(*nsamps_processed / nbeams);
   for (unsigned i = 0; i < ngroups; i++) {
     const hdb::GroupRow& r = rows[i];
+    const size_t u = (size_t)r.unit;
+    if (u >= U || too_many[u]) continue;
+    const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
     size_t ind = (size_t)r.ind;
     size_t beam_idx = (size_t)std::floor((float)ind / (float)nsamps_beam);
     size_t beam_start = beam_idx * nsamps_beam + (P.boxcar_max / 2);
@@ -547,10 +610,14 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     c.members = (hd_size)r.members;
     c.begin = first_idx + ((size_t)r.begin % nsamps_beam);
     c.end = first_idx + ((size_t)r.end % nsamps_beam);
-    c.beam = P.beam + beam_idx + 1;
-    pl->cands.push_back(c);
+    c.beam = beam_base + beam_idx + 1;
+    pl->unit_cands[u].push_back(c);
   }
-  write_cand_file(pl, first_idx);
+  for (size_t u = 0; u < U; u++) {
+    const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
+    write_cand_file(pl, pl->unit_cands[u], beam_base, first_idx);
+    pl->cands.insert(pl->cands.end(), pl->unit_cands[u].begin(), pl->unit_cands[u].end());
+  }
 
   // stage timings
   auto el = [&](int a, int b) {
@@ -568,20 +635,30 @@ static hd_error execute_impl(hd_pipeline pl, const hd_byte* h_filterbank, bool o
     pl->timing[5] = el(5, 6);
   }
   pl->timing[6] = el(6, 7);
-  return too_many ? HD_TOO_MANY_EVENTS : HD_NO_ERROR;
+  return any_too_many ? HD_TOO_MANY_EVENTS : HD_NO_ERROR;
 }
 
 hd_error hd_execute(hd_pipeline pl, const hd_byte* h_filterbank, hd_size nsamps, hd_size nbits,
                     hd_size first_idx, hd_size nbeams, hd_size* nsamps_processed) {
-  return execute_impl(pl, h_filterbank, false, nsamps, nbits, first_idx, nbeams,
-                      nsamps_processed);
+  if (!h_filterbank) return pl ? HD_INVALID_POINTER : HD_INVALID_PIPELINE;
+  return execute_units(pl, &h_filterbank, 1, false, nsamps, nbits, first_idx, nbeams, nullptr,
+                       nullptr, nsamps_processed);
 }
 
 hd_error hd_execute_device(hd_pipeline pl, const hd_byte* d_filterbank, hd_size nsamps,
                            hd_size nbits, hd_size first_idx, hd_size nbeams,
                            hd_size* nsamps_processed) {
-  return execute_impl(pl, d_filterbank, true, nsamps, nbits, first_idx, nbeams,
-                      nsamps_processed);
+  if (!d_filterbank) return pl ? HD_INVALID_POINTER : HD_INVALID_PIPELINE;
+  return execute_units(pl, &d_filterbank, 1, true, nsamps, nbits, first_idx, nbeams, nullptr,
+                       nullptr, nsamps_processed);
+}
+
+hd_error hd_execute_beams(hd_pipeline pl, const hd_byte* const* filterbanks,
+                          hd_size nfilterbanks, hd_size nsamps, hd_size nbits,
+                          hd_size first_idx, hd_size nbeams, const hd_size* beams,
+                          int on_device, hd_error* statuses, hd_size* nsamps_processed) {
+  return execute_units(pl, filterbanks, nfilterbanks, on_device != 0, nsamps, nbits, first_idx,
+                       nbeams, beams, statuses, nsamps_processed);
 }
 
 unsigned long long hd_get_launch_count(void) { return hdb::launch_count(); }
@@ -606,8 +683,9 @@ hd_error hd_clean_filterbank_rfi(hd_pipeline pl, const hd_byte* h_in, hd_size ns
   HD_TRY(pl->fb_tf.ensure(nsamps * C));
   HD_TRY(pl->fb_tf_clean.ensure(nsamps * C));
   HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_in, nsamps * C, cudaMemcpyHostToDevice, s));
-  hd_error he = clean_device(pl, nsamps, C, dt, baseline_length, rfi_tol, boxcar_max, nbeams,
-                             nullptr, 0, pl->fb_tf_clean.as<uint8_t>());
+  hd_error he = clean_units(pl, 1, pl->fb_tf.as<uint8_t>(), nsamps, C, dt, baseline_length,
+                            rfi_tol, boxcar_max, nbeams, nullptr, 0,
+                            pl->fb_tf_clean.as<uint8_t>());
   if (he != HD_NO_ERROR) return he;
   HD_TRY(cudaMemcpyAsync(h_out, pl->fb_tf_clean.p, nsamps * C, cudaMemcpyDeviceToHost, s));
   if (h_mask)
@@ -622,6 +700,18 @@ hd_error hd_get_candidates(hd_pipeline pl, hd_candidate* out, hd_size* count) {
   size_t n = std::min(*count, pl->cands.size());
   if (out && n) std::memcpy(out, pl->cands.data(), n * sizeof(hd_candidate));
   *count = pl->cands.size();
+  return HD_NO_ERROR;
+}
+
+hd_error hd_get_beam_candidates(hd_pipeline pl, hd_size index, hd_candidate* out,
+                                hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!count) return HD_INVALID_POINTER;
+  if (index >= pl->unit_cands.size()) return HD_INVALID_STRIDE;
+  const std::vector<hd_candidate>& v = pl->unit_cands[index];
+  size_t n = std::min(*count, v.size());
+  if (out && n) std::memcpy(out, v.data(), n * sizeof(hd_candidate));
+  *count = v.size();
   return HD_NO_ERROR;
 }
 

@@ -135,15 +135,18 @@ size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
 }
 
 dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch, size_t nsamps,
-                                float* d_out, size_t out_pitch, cudaStream_t s) {
+                                float* d_out, size_t out_pitch, cudaStream_t s, size_t units,
+                                size_t in_unit, size_t out_unit) {
   dedisp_error de = plan_prepare(p);
   if (de != DEDISP_NO_ERROR) return de;
   if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
   size_t nout = nsamps - p->max_delay;
   if (nout == 0) return DEDISP_NO_ERROR;
+  if (units == 0) return DEDISP_NO_ERROR;
   if (p->active.empty()) {
-    for (size_t d = 0; d < p->dm_list.size(); d++)
-      if (cudaMemsetAsync(d_out + d * out_pitch, 0, nout * sizeof(float), s) != cudaSuccess)
+    for (size_t u = 0; u < units; u++)
+      if (cudaMemset2DAsync(d_out + u * out_unit, out_pitch * sizeof(float), 0,
+                            nout * sizeof(float), p->dm_list.size(), s) != cudaSuccess)
         return DEDISP_INTERNAL_GPU_ERROR;
     return DEDISP_NO_ERROR;
   }
@@ -161,6 +164,10 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   a.out_pitch = out_pitch;
   a.rowb = rowb_of(p);
   a.err = p->d_err;
+  a.units = (int)units;
+  a.in_unit = in_unit;
+  a.out_unit = out_unit;
+  if (units > 65535) return DEDISP_INVALID_STRIDE;
   if (dedisp_smem_bytes(a.rowb) > 200 * 1024) return DEDISP_NCHANS_EXCEEDS_LIMIT;
   if (launch_dedisp(a, s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
   return DEDISP_NO_ERROR;

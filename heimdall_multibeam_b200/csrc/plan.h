@@ -62,7 +62,10 @@ dedisp_error plan_prepare(dedisp_plan p);
 size_t ft_pitch(const dedisp_plan p, size_t nsamps);
 
 // Dedisperses the FT copy already on the device into out (device floats).
+// With units > 1, one launch dedisperses `units` filterbanks that lie
+// in_unit bytes (inputs) and out_unit floats (outputs) apart.
 dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch, size_t nsamps,
-                                float* d_out, size_t out_pitch, cudaStream_t s);
+                                float* d_out, size_t out_pitch, cudaStream_t s, size_t units = 1,
+                                size_t in_unit = 0, size_t out_unit = 0);
 
 }  // namespace hdb

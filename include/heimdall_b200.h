@@ -19,7 +19,8 @@
  *
  * Additions (no reference counterpart; the reference only writes candidates to
  * a .cand file or a socket): hd_set_cleaning, hd_execute_device,
- * hd_get_candidates, hd_get_giants, hd_get_timing, hd_get_launch_count.
+ * hd_execute_beams, hd_get_candidates, hd_get_beam_candidates, hd_get_giants,
+ * hd_get_timing, hd_get_launch_count.
  *
  * Ownership and threading: the caller owns every host buffer it passes; the
  * pipeline owns all device memory, its CUDA stream and events.  A pipeline
@@ -156,6 +157,31 @@ hd_error hd_execute_device(hd_pipeline pipeline, const hd_byte* d_filterbank, hd
                            hd_size nbits, hd_size first_idx, hd_size nbeams,
                            hd_size* nsamps_processed);
 
+/* Batched search of independent filterbanks.  No counterpart in the
+ * reference, which runs one heimdall process per beam of a multibeam receiver
+ * (each calling hd_execute on its own stream of data).
+ *
+ * Searches nfilterbanks filterbanks of the same shape (nsamps x nchans bytes
+ * each, every one holding nbeams time-concatenated beams as in hd_execute)
+ * with this pipeline's configuration in one pass: each stage runs over the
+ * DM trials of all of them at once, and giants are never clustered across
+ * filterbanks.  The result for filterbank u -- its candidates, its .cand file
+ * and its status -- is identical to hd_execute(filterbanks[u], nsamps, nbits,
+ * first_idx, nbeams, ...) on a pipeline whose params.beam is beams[u]
+ * (beams may be NULL: params.beam + u * nbeams).
+ *
+ * filterbanks: host pointers, or device pointers when on_device != 0.
+ * statuses (may be NULL): per filterbank HD_NO_ERROR or HD_TOO_MANY_EVENTS
+ * (giant-rate bail-out, whose candidates are dropped).  The call returns
+ * HD_TOO_MANY_EVENTS if any filterbank bailed out, else the first error.
+ * Limit: nfilterbanks x (number of DM trials) <= 65535 (HD_INVALID_STRIDE
+ * otherwise).  Candidates: hd_get_candidates (all, filterbank by filterbank)
+ * or hd_get_beam_candidates (one filterbank). */
+hd_error hd_execute_beams(hd_pipeline pipeline, const hd_byte* const* filterbanks,
+                          hd_size nfilterbanks, hd_size nsamps, hd_size nbits,
+                          hd_size first_idx, hd_size nbeams, const hd_size* beams,
+                          int on_device, hd_error* statuses, hd_size* nsamps_processed);
+
 /* Allocation-free zero-DM RFI cleaning.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory while they run -- a
@@ -206,9 +232,16 @@ typedef struct hd_candidate {
  * *count to the number available. */
 hd_error hd_get_candidates(hd_pipeline pipeline, hd_candidate* out, hd_size* count);
 
+/* Candidates of filterbank `index` of the last hd_execute_beams (index 0 after
+ * hd_execute), same copy rules as hd_get_candidates. */
+hd_error hd_get_beam_candidates(hd_pipeline pipeline, hd_size index, hd_candidate* out,
+                                hd_size* count);
+
 /* Every giant of the last hd_execute in detection order (DM, width, time),
  * before clustering, with its cluster label (the index of the cluster's first
- * giant).  Any pointer may be NULL. */
+ * giant).  After hd_execute_beams: filterbank by filterbank, dm_inds local to
+ * each filterbank, labels indexing the whole list.  Giants are reported only
+ * when some filterbank did not bail out.  Any pointer may be NULL. */
 hd_error hd_get_giants(hd_pipeline pipeline, hd_float* peaks, hd_size* inds, hd_size* begins,
                        hd_size* ends, hd_size* filter_inds, hd_size* dm_inds,
                        hd_size* labels, hd_size* count);
