@@ -1,23 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the per-gulp single-pulse search (Heimdall's hd_execute).
 
-Workload: one gulp of the plain single-beam search at survey size with RFI --
-1024 channels uint8, 1520 MHz top, -0.390625 MHz channels, 64 us, 2^18
-samples (16.78 beam-seconds), DM 0-2000 (tol 1.25, 40 us), boxcars 2^0..2^12,
-threshold 6, clean_filterbank_rfi on; seeded synthetic data (noise N(128,16^2),
-20 injected dispersed pulses, narrow-band and zero-DM RFI).
+Headline workload (default, --workload multibeam): one gulp of a 36-beam
+multibeam receiver -- 36 beams x 320 channels uint8, 851 MHz top,
+-0.09765625 MHz channels, 655.36 us, 2^15 samples per beam (773 beam-seconds
+per gulp), DM 0-2000 (tol 1.25, 40 us), boxcars 2^0..2^9, threshold 6; seeded
+synthetic data (noise N(128,16^2), 2 injected dispersed pulses per beam).
 
-Metric: beam-seconds searched per second.
-  value  -- K gulps through hd_execute_device with the filterbank resident in
-            HBM; CUDA events around the K calls (each call ends synchronised).
-  e2e    -- the same K gulps through hd_execute (the drop-in C entry point)
-            from pinned host memory: host->device copy of the gulp inside the
-            timed region, candidate rows read back every step.
-The input (256 MiB) is larger than L2 (126 MB), so no L2 flush is needed.
+Metric: beam-seconds searched per second, batched vs plain.
+  value  -- the batched form: K gulps through hd_execute_beams with the 36
+            filterbanks resident in HBM; CUDA events around the K calls (each
+            call ends synchronised).
+  plain  -- the plain per-beam GPU form on the same resident data: each gulp
+            is 36 hd_execute_device calls, one per beam.
+  e2e    -- the batched form through hd_execute_beams from pinned host memory:
+            the host->device copy of all 36 filterbanks is inside the timed
+            region, candidate rows are read back every step.
+  recall -- injected pulses with S/N >= 8 matched by a candidate of their beam.
+The input (360 MiB) is larger than L2 (126 MB), so no L2 flush is needed.
+--workload survey runs the plain single-beam survey gulp (1024 channels,
+2^18 samples, DM 0-2000, boxcars to 2^12, clean_filterbank_rfi on) instead;
+the default run also reports it as "survey_plain".
 
 `--impl reference` times the reference's own stage code (Pipeline/*.cu rebuilt
 on Thrust's OpenMP backend, oracle/_ref) with all host threads on a bounded
-sample of the same gulp (a DM-range subset) and scales by the DM count.
+sample of the same workload (whole beams of the multibeam gulp; a DM-range
+subset of the survey gulp, scaled by the DM count).
 
 Multi-GPU: beams are independent, so every rank searches its own gulp
 (replicas, weak scaling); the max over ranks of the device time is used.
@@ -39,6 +47,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "beam-sec searched per sec, batched vs plain; injected recall at S/N>=8"
 UNIT = "beam-s/s"
+
+# DRAM bytes per k_dedisp launch, read from the committed ncu summaries
+TRAFFIC = {
+    "multibeam_36x_c320_n32768": ("k_dedisp_multibeam_36x_c320_n32768.md",
+                                  "traffic_bytes_per_launch:"),
+    "plain_c1024_n262144_rfi": ("k_dedisp_c1024_n131072.md",
+                                "traffic_bytes_per_launch_full_size:"),
+}
 
 
 def _env_int(k, d):
@@ -71,7 +87,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -109,19 +125,39 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload(nsamps=None):
+class Work:
+    """One gulp: `beams` independent filterbanks (nsamps x nchans uint8 each)
+    with their injected pulses, and the search configuration `w`."""
+
+    def __init__(self, w, fbs, pulses):
+        self.w = w
+        self.fbs = fbs
+        self.pulses = pulses
+        self.nsamps, self.nchans = fbs[0].shape
+        self.units = len(fbs)
+        self.beam_s = self.units * self.nsamps * w.dt
+
+
+def workload(kind, nsamps=None, nbeams=None):
+    import dataclasses
     from heimdall_multibeam_b200 import synth
-    w = synth.SEARCH_C1
-    b = synth.make_c1(nsamps=nsamps)
-    if nsamps:
-        import dataclasses
-        w = dataclasses.replace(w, name=f"plain_c1024_n{nsamps}_rfi", nsamps=nsamps)
-    return w, b
+    if kind == "survey":
+        w = synth.SEARCH_C1
+        b = synth.make_c1(nsamps=nsamps)
+        if nsamps:
+            w = dataclasses.replace(w, name=f"plain_c1024_n{nsamps}_rfi", nsamps=nsamps)
+        return Work(w, [b.data], [b.pulses])
+    w = synth.SEARCH_C2
+    if nsamps or nbeams:
+        w = dataclasses.replace(w, nsamps=nsamps or w.nsamps, nbeams=nbeams or w.nbeams)
+        w = dataclasses.replace(w, name=f"multibeam_{w.nbeams}x_c320_n{w.nsamps}")
+    beams = synth.make_multibeam(w, seed=2026)
+    return Work(w, [b.data for b in beams], [b.pulses for b in beams])
 
 
-def params_for(H, w):
+def params_for(H, w, **kw):
     return H.default_params(nchans=w.nchans, dt=w.dt, f0=w.f0, df=w.df, dm_min=w.dm_min,
-                            dm_max=w.dm_max, boxcar_max=w.boxcar_max, output_dir=None)
+                            dm_max=w.dm_max, boxcar_max=w.boxcar_max, output_dir=None, **kw)
 
 
 def recall(cands, pulses, dt, snr_min=8.0):
@@ -143,6 +179,23 @@ def recall(cands, pulses, dt, snr_min=8.0):
     return hit, len(strong)
 
 
+def _timed(torch, dev, barrier, steps, fn, stage=None, timing=None):
+    """K calls of fn between CUDA events (each call ends synchronised)."""
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record()
+    for _ in range(steps):
+        fn()
+        if stage is not None:
+            t = timing()
+            for k in stage:
+                stage[k] += t[k]
+    e1.record()
+    barrier()
+    return e0.elapsed_time(e1) / steps
+
+
 def run_product(args):
     import torch
     import heimdall_multibeam_b200 as H
@@ -160,15 +213,18 @@ def run_product(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", local if world > 1 else 0)
 
-    w, b = workload(args.nsamps)
-    nsamps, nchans = b.data.shape
-    beam_s = nsamps * w.dt
+    wk = workload(args.workload, args.nsamps, args.nbeams)
+    w = wk.w
+    U, nsamps, nchans = wk.units, wk.nsamps, wk.nchans
     p = params_for(H, w)
     p.gpu_id = dev.index
-    pl = H.Pipeline(p, cleaning=True)
+    pl = H.Pipeline(p, cleaning=w.clean)
 
-    d_fb = torch.from_numpy(b.data).to(dev)
-    h_fb = torch.from_numpy(b.data).pin_memory()
+    d_all = torch.from_numpy(np.stack(wk.fbs)).to(dev)
+    h_all = torch.from_numpy(np.stack(wk.fbs)).pin_memory()
+    fb_bytes = nsamps * nchans
+    d_ptrs = [d_all.data_ptr() + u * fb_bytes for u in range(U)]
+    h_ptrs = [h_all.data_ptr() + u * fb_bytes for u in range(U)]
     torch.cuda.synchronize(dev)
 
     def barrier():
@@ -176,53 +232,78 @@ def run_product(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    # ---- device-resident input --------------------------------------------
+    def batched():
+        if U == 1:
+            err, _ = pl.execute_device(d_ptrs[0], nsamps)
+        else:
+            err, _, _ = pl.execute_beams(d_ptrs, nsamps=nsamps, on_device=True)
+        assert err in (H.HD_NO_ERROR, H.HD_TOO_MANY_EVENTS), H.error_string(err)
+
+    def batched_e2e():
+        if U == 1:
+            pl.execute_ptr(h_ptrs[0], nsamps)
+        else:
+            pl.execute_beams(h_ptrs, nsamps=nsamps, on_device=False)
+        return sum(len(pl.candidates(u)) for u in range(U)) if U > 1 else len(pl.candidates())
+
+    def plain():
+        for u in range(U):
+            pl.execute_device(d_ptrs[u], nsamps)
+
+    # ---- batched form, device-resident input ---------------------------------
     for _ in range(args.warmup):
-        err, proc = pl.execute_device(d_fb.data_ptr(), nsamps)
-        assert err == 0, H.error_string(err)
-    cands = pl.candidates()
+        batched()
     l0 = H.launch_count()
     stage = {k: 0.0 for k in pl.timing()}
     clk = ClockSampler(dev.index)
     clk.start()
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        err, proc = pl.execute_device(d_fb.data_ptr(), nsamps)
-        t = pl.timing()
-        for k in stage:
-            stage[k] += t[k]
-    e1.record()
-    barrier()
-    clocks = clk.stop()
+    ms = _timed(torch, dev, barrier, args.steps, batched, stage, pl.timing)
     launches = H.launch_count() - l0
-    ms = e0.elapsed_time(e1) / args.steps
+    cands = [pl.candidates(u) for u in range(U)] if U > 1 else [pl.candidates()]
 
-    # ---- end to end through hd_execute from pinned host memory --------------
-    for _ in range(max(1, args.warmup // 2)):
-        pl.execute_ptr(h_fb.data_ptr(), nsamps)
-    barrier()
-    e0.record()
+    # ---- plain per-beam form on the same data ---------------------------------
+    ms_plain = None
+    if U > 1 and not args.batched_only:
+        for _ in range(max(1, args.warmup // 2)):
+            plain()
+        lp = H.launch_count()
+        ms_plain = _timed(torch, dev, barrier, args.steps, plain)
+        launches_plain = H.launch_count() - lp
+
+    # ---- end to end from pinned host memory ------------------------------------
+    ms_e2e = None
     ncand = 0
     stage_e2e = {k: 0.0 for k in stage}
-    for _ in range(args.steps):
-        err, proc = pl.execute_ptr(h_fb.data_ptr(), nsamps)
-        ncand = len(pl.candidates())
-        t = pl.timing()
-        for k in stage_e2e:
-            stage_e2e[k] += t[k]
-    e1.record()
-    barrier()
-    ms_e2e = e0.elapsed_time(e1) / args.steps
+    if not args.batched_only:
+        for _ in range(max(1, args.warmup // 2)):
+            batched_e2e()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            ncand = batched_e2e()
+            t = pl.timing()
+            for k in stage_e2e:
+                stage_e2e[k] += t[k]
+        e1.record()
+        barrier()
+        ms_e2e = e0.elapsed_time(e1) / args.steps
 
-    tmax = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
+    # clocks sampled over the three timed regions (batched, plain, e2e)
+    clocks = clk.stop()
+    tm = [ms, ms_plain or 0.0, ms_e2e or 0.0]
+    tmax = torch.tensor(tm, dtype=torch.float64, device=dev)
     if dist is not None:
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = float(tmax[0]), float(tmax[1])
-    value = world * beam_s / (ms / 1e3)
-    e2e = world * beam_s / (ms_e2e / 1e3)
+    ms, ms_plain_m, ms_e2e_m = (float(x) for x in tmax)
+    value = world * wk.beam_s / (ms / 1e3)
+
+    pl.close()
+    # secondary: the plain survey-size single-beam gulp
+    survey = None
+    if args.workload == "multibeam" and not args.no_survey and not args.batched_only:
+        survey = survey_plain(args, H, torch, dev, barrier, dist, world)
 
     if rank == 0:
         peaks, peak_kind = _peaks()
@@ -232,39 +313,39 @@ def run_product(args):
         D = len(plan.dm_list)
         nout = nsamps - plan.max_delay
         t_dd = stage["dedisperse"] / args.steps  # ms, events on the pipeline stream
-        bytes_dd = nchans * nsamps + D * nout * 4
-        adds = D * nout * nchans
+        bytes_dd = U * (nchans * nsamps + D * nout * 4)
+        adds = U * D * nout * nchans
         achieved = bytes_dd / (t_dd / 1e3) / 1e9
         sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
         int_peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # Tadd/s, INT32 lanes x clock
         int_ach = adds / (t_dd / 1e3) / 1e12
         traffic = None
-        try:
-            # DRAM bytes per k_dedisp launch from the committed ncu summary
-            with open(os.path.join(ROOT, "profiles", "k_dedisp_c1024_n131072.md")) as f:
-                for ln in f:
-                    if ln.startswith("traffic_bytes_per_launch_full_size:"):
-                        traffic = int(ln.split(":")[1])
-            if nsamps != 262144:
-                traffic = None
-        except Exception:
-            pass
-        hit, nstrong = recall(cands, b.pulses, w.dt)
+        tf = TRAFFIC.get(w.name)
+        if tf:
+            try:
+                with open(os.path.join(ROOT, "profiles", tf[0])) as f:
+                    for ln in f:
+                        if ln.startswith(tf[1]):
+                            traffic = int(ln.split(":")[1])
+            except Exception:
+                pass
+        hit = nstrong = 0
+        for u in range(U):
+            h_, n_ = recall(cands[u], wk.pulses[u], w.dt)
+            hit += h_
+            nstrong += n_
         rec = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic",
-            "config": {"workload": w.name, "nchans": nchans, "nsamps": nsamps, "nbeams": 1,
+            "config": {"workload": w.name, "form": "batched" if U > 1 else "plain",
+                       "nbeams": U, "nchans": nchans, "nsamps_per_beam": nsamps,
                        "dt_s": w.dt, "dm_range": [w.dm_min, w.dm_max], "dm_trials": D,
-                       "boxcar_max": w.boxcar_max, "clean_filterbank_rfi": True,
-                       "beam_seconds_per_gulp": round(beam_s, 4),
-                       "l2": "input 256 MiB > L2, no flush", "parallelism": f"replicas{world}"},
-            "e2e": {"value": round(e2e, 3), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
-                    "h2d_bytes_per_step": int(nsamps * nchans),
-                    "d2h_bytes_per_step": int(ncand * 64 + 128),
-                    "stage_ms": {k: round(v / args.steps, 4) for k, v in stage_e2e.items()},
-                    "host_buffer": "pinned (torch pin_memory)"},
+                       "boxcar_max": w.boxcar_max, "clean_filterbank_rfi": bool(w.clean),
+                       "beam_seconds_per_gulp": round(wk.beam_s, 4),
+                       "l2": f"input {U * fb_bytes / 2**20:.0f} MiB > L2, no flush",
+                       "parallelism": f"replicas{world}"},
             "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},
             "roofline": {"kernel": "k_dedisp", "bound": "hbm", "achieved": round(achieved, 2),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -279,44 +360,129 @@ def run_product(args):
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if ms_plain is not None:
+            v_plain = world * wk.beam_s / (ms_plain_m / 1e3)
+            rec["plain"] = {"value": round(v_plain, 3), "unit": UNIT,
+                            "ms_per_step": round(ms_plain_m, 3),
+                            "form": f"{U} hd_execute_device calls per gulp",
+                            "gpu_launches": int(launches_plain)}
+            rec["batched_over_plain"] = round(value / v_plain, 3)
+        if ms_e2e is not None:
+            rec["e2e"] = {"value": round(world * wk.beam_s / (ms_e2e_m / 1e3), 3), "unit": UNIT,
+                          "ms_per_step": round(ms_e2e_m, 3),
+                          "h2d_bytes_per_step": int(U * fb_bytes),
+                          "d2h_bytes_per_step": int(ncand * 64 + 128),
+                          "stage_ms": {k: round(v / args.steps, 4)
+                                       for k, v in stage_e2e.items()},
+                          "host_buffer": "pinned (torch pin_memory)",
+                          "api": "hd_execute_beams" if U > 1 else "hd_execute"}
+        if survey is not None:
+            rec["survey_plain"] = survey
         if not args.no_cpu_baseline:
-            rec["cpu_baseline"] = cpu_baseline(args, b, w, beam_s)
+            rec["cpu_baseline"] = cpu_baseline(args, wk)
         print(json.dumps(rec), flush=True)
-    pl.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def _ref_sample(b, w, dm_max, threads):
+def survey_plain(args, H, torch, dev, barrier, dist, world):
+    """The plain single-beam survey gulp (1024 ch, 2^18 samples, RFI cleaning)
+    through hd_execute_device (value) and hd_execute from pinned memory (e2e)."""
+    wk = workload("survey")
+    w = wk.w
+    nsamps = wk.nsamps
+    p = params_for(H, w)
+    p.gpu_id = dev.index
+    pl = H.Pipeline(p, cleaning=True)
+    d_fb = torch.from_numpy(wk.fbs[0]).to(dev)
+    h_fb = torch.from_numpy(wk.fbs[0]).pin_memory()
+    for _ in range(args.warmup):
+        pl.execute_device(d_fb.data_ptr(), nsamps)
+    stage = {k: 0.0 for k in pl.timing()}
+    ms = _timed(torch, dev, barrier, args.steps,
+                lambda: pl.execute_device(d_fb.data_ptr(), nsamps), stage, pl.timing)
+    cands = pl.candidates()
+    pl.execute_ptr(h_fb.data_ptr(), nsamps)
+    ms_e2e = _timed(torch, dev, barrier, args.steps,
+                    lambda: pl.execute_ptr(h_fb.data_ptr(), nsamps))
+    pl.close()
+    tmax = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = float(tmax[0]), float(tmax[1])
+    hit, nstrong = recall(cands, wk.pulses[0], w.dt)
+    return {"workload": w.name, "value": round(world * wk.beam_s / (ms / 1e3), 3), "unit": UNIT,
+            "ms_per_step": round(ms, 3),
+            "e2e": round(world * wk.beam_s / (ms_e2e / 1e3), 3), "e2e_ms_per_step": round(ms_e2e, 3),
+            "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},
+            "recall": {"snr_ge_8_found": hit, "snr_ge_8_injected": nstrong}}
+
+
+class _QuietStdout:
+    """Sends file descriptor 1 to /dev/null (the reference prints a line per
+    gulp), so that the JSON line stays the only output."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        fd = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(fd, 1)
+        os.close(fd)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def _ref_run(fb, w, threads, dm_max=None):
+    """Seconds the reference pipeline takes on one filterbank (its own timer
+    around hd_execute) and the number of DM trials searched."""
     import oracle
+    dm_max = w.dm_max if dm_max is None else dm_max
     kw = dict(dt=w.dt, f0=w.f0, df=w.df, dm_min=w.dm_min, dm_max=dm_max,
-              boxcar_max=w.boxcar_max, clean=1)
-    err, proc, lines, secs = oracle.ref_execute(b.data, nthreads=threads, **kw)
+              boxcar_max=w.boxcar_max, clean=int(w.clean))
+    with _QuietStdout():
+        err, proc, lines, secs = oracle.ref_execute(fb, nthreads=threads, **kw)
     d = len(oracle.dm_list(w.dm_min, dm_max, w.dt, 40.0, w.f0, w.df, w.nchans, 1.25))
     return secs, d
 
 
-def cpu_baseline(args, b, w, beam_s):
-    """The reference's stage code (Thrust OpenMP build) on two DM-range
-    samples of the same gulp; gulp time extrapolated linearly in the DM count
-    (fixed cleaning cost + per-DM cost)."""
+def _ref_gulp(args, wk, threads):
+    """(seconds per gulp, description) of the reference on a bounded sample:
+    whole beams of the multibeam gulp (scaled by the beam count), or two
+    DM-range subsets of the single-beam gulp (extrapolated linearly in the DM
+    count: fixed cleaning cost + per-DM cost)."""
+    import oracle
+    w = wk.w
+    if wk.units > 1:
+        nb = max(1, min(args.ref_beams, wk.units))
+        secs = sum(_ref_run(wk.fbs[u], w, threads)[0] for u in range(nb))
+        t_gulp = secs / nb * wk.units
+        return t_gulp, (f"reference pipeline (Thrust OpenMP build), {threads} threads, on "
+                        f"{nb} whole beams of the {wk.units}-beam gulp ({secs:.1f} s), one "
+                        f"hd_execute per beam as the reference runs them; gulp time = "
+                        f"{wk.units} x per-beam time = {t_gulp:.1f} s")
+    d_full = len(oracle.dm_list(w.dm_min, w.dm_max, w.dt, 40.0, w.f0, w.df, w.nchans, 1.25))
+    s1, d1 = _ref_run(wk.fbs[0], w, threads, args.ref_dm1)
+    s2, d2 = _ref_run(wk.fbs[0], w, threads, args.ref_dm2)
+    per_dm = max((s2 - s1) / max(d2 - d1, 1), 0.0)
+    fixed = max(s1 - per_dm * d1, 0.0)
+    t_full = fixed + per_dm * d_full
+    return t_full, (f"reference pipeline (Thrust OpenMP build), {threads} threads, on DM "
+                    f"0-{args.ref_dm1} ({d1} trials, {s1:.1f} s) and 0-{args.ref_dm2} ({d2} "
+                    f"trials, {s2:.1f} s); gulp time extrapolated to {d_full} trials = "
+                    f"{t_full:.1f} s")
+
+
+def cpu_baseline(args, wk):
     import oracle
     threads = os.cpu_count() or 1
     if not oracle.ref_available():
         return {"unavailable": "reference build oracle/_ref not present"}
-    d_full = len(oracle.dm_list(w.dm_min, w.dm_max, w.dt, 40.0, w.f0, w.df, w.nchans, 1.25))
-    s1, d1 = _ref_sample(b, w, args.ref_dm1, threads)
-    s2, d2 = _ref_sample(b, w, args.ref_dm2, threads)
-    per_dm = max((s2 - s1) / max(d2 - d1, 1), 0.0)
-    fixed = max(s1 - per_dm * d1, 0.0)
-    t_full = fixed + per_dm * d_full
-    return {"value": round(beam_s / t_full, 4), "unit": UNIT, "cores": threads,
-            "kind": "reference",
-            "sample": f"reference pipeline on DM 0-{args.ref_dm1} ({d1} trials, {s1:.1f} s) and "
-                      f"0-{args.ref_dm2} ({d2} trials, {s2:.1f} s); gulp time extrapolated to "
-                      f"{d_full} trials = {t_full:.1f} s",
-            "seconds_per_gulp": round(t_full, 2)}
+    t_gulp, sample = _ref_gulp(args, wk, threads)
+    return {"value": round(wk.beam_s / t_gulp, 4), "unit": UNIT, "cores": threads,
+            "kind": "reference", "sample": sample, "seconds_per_gulp": round(t_gulp, 2)}
 
 
 def run_reference(args):
@@ -324,39 +490,28 @@ def run_reference(args):
     if rank != 0:
         return
     import oracle
-    w, b = workload(args.nsamps)
-    nsamps = b.data.shape[0]
-    beam_s = nsamps * w.dt
+    wk = workload(args.workload, args.nsamps, args.nbeams)
+    w = wk.w
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
         return
     threads = os.cpu_count() or 1
-    d_full = len(oracle.dm_list(w.dm_min, w.dm_max, w.dt, 40.0, w.f0, w.df, w.nchans, 1.25))
     for _ in range(args.warmup):
-        _ref_sample(b, w, args.ref_dm1, threads)
-    times = []
+        _ref_run(wk.fbs[0], w, threads, args.ref_dm1 if wk.units == 1 else None)
     t0 = time.time()
-    for _ in range(args.steps):
-        s1, d1 = _ref_sample(b, w, args.ref_dm1, threads)
-        times.append((s1, d1))
+    runs = [_ref_gulp(args, wk, threads) for _ in range(args.steps)]
     wall = time.time() - t0
-    s1 = float(np.median([t for t, _ in times]))
-    s2, d2 = _ref_sample(b, w, args.ref_dm2, threads)
-    per_dm = max((s2 - s1) / max(d2 - d1, 1), 0.0)
-    fixed = max(s1 - per_dm * d1, 0.0)
-    t_full = fixed + per_dm * d_full
-    value = beam_s / t_full
-    sample = (f"reference pipeline (Thrust OpenMP build) with {threads} threads on DM 0-"
-              f"{args.ref_dm1} ({d1} trials) per step and 0-{args.ref_dm2} ({d2} trials) once; "
-              f"gulp time extrapolated to {d_full} trials = {t_full:.1f} s")
+    t_gulp = float(np.median([t for t, _ in runs]))
+    value = wk.beam_s / t_gulp
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(t_full * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": round(t_gulp * 1e3, 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": w.name, "nchans": w.nchans, "nsamps": nsamps, "dm_trials": d_full},
+        "config": {"workload": w.name, "nbeams": wk.units, "nchans": wk.nchans,
+                   "nsamps_per_beam": wk.nsamps},
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": runs[-1][1]},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 1)}), flush=True)
@@ -365,12 +520,21 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="multibeam", choices=["multibeam", "survey"])
     ap.add_argument("--nsamps", type=int, default=None,
-                    help="gulp length (default 2^18); smaller gulps are for profiling")
+                    help="samples per beam (smaller gulps are for profiling)")
+    ap.add_argument("--nbeams", type=int, default=None,
+                    help="beams of the multibeam gulp (fewer are for profiling)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="time only the batched form (profiling)")
+    ap.add_argument("--no-survey", action="store_true",
+                    help="skip the secondary single-beam survey gulp")
+    ap.add_argument("--ref-beams", type=int, default=4,
+                    help="whole beams the reference runs per multibeam sample")
     ap.add_argument("--ref-dm1", type=float, default=20.0)
     ap.add_argument("--ref-dm2", type=float, default=60.0)
     args = ap.parse_args()

@@ -59,11 +59,16 @@ __device__ __forceinline__ unsigned f2u(float x) {
 }
 
 // Pipeline/median_filter.cu:451-479, one output of linear_stretch.
+// The reference tests `frac > 1e-5` with frac a float promoted to double.
+// 1e-5f (9.9999997e-06) lies below 1e-5 and the next float above it lies above
+// 1e-5, so `frac > 1e-5f` in float selects exactly the same values.
+constexpr float kStretchEps = 1e-5f;
+
 __device__ __forceinline__ float stretch_at(const float* in, unsigned i, float step) {
   float x = __fmul_rn(__uint2float_rn(i), step);
   unsigned j = f2u(x);
   float fr = __fsub_rn(x, __uint2float_rn(j));
-  float add = ((double)fr > 1e-5) ? __fmul_rn(fr, __fsub_rn(in[j + 1], in[j])) : 0.f;
+  float add = (fr > kStretchEps) ? __fmul_rn(fr, __fsub_rn(in[j + 1], in[j])) : 0.f;
   return __fadd_rn(in[j], add);
 }
 
@@ -75,7 +80,7 @@ __device__ __forceinline__ float stretch_beam_at(const float* in, unsigned i, fl
   float fb = __ull2float_rn(beam);
   unsigned k = f2u(__fadd_rn(x, fb));
   float o = __fadd_rn(__fsub_rn(x, __uint2float_rn(k)), fb);
-  float add = ((double)o > 1e-5) ? __fmul_rn(o, __fsub_rn(in[k + 1], in[k])) : 0.f;
+  float add = (o > kStretchEps) ? __fmul_rn(o, __fsub_rn(in[k + 1], in[k])) : 0.f;
   return __fadd_rn(in[k], add);
 }
 
@@ -90,6 +95,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_addr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {

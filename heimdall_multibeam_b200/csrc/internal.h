@@ -79,8 +79,10 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // of MatchedFilterPlan::prep (matched_filter.cu:21-32), sequential association:
 // scan[ser][0..len] (len + 1 values, pitch scan_pitch).  norm_out (nullable,
 // same layout as the batch) receives the normalised series.
+// err (nullable): bit 1 is set if a staging wait timed out.
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
-                           size_t scan_pitch, float* norm_out, cudaStream_t s);
+                           size_t scan_pitch, float* norm_out, cudaStream_t s,
+                           unsigned* err = nullptr);
 
 // Per-width constants of the boxcar loop (Pipeline/pipeline.cu:657-776).
 struct WidthInfo {

@@ -263,15 +263,21 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
       pk[d][g][0] = pk[d][g][1] = 0;
       acc[d][g][0] = acc[d][g][1] = acc[d][g][2] = acc[d][g][3] = 0;
     }
+  // pk[..][0] sums the raw words (bytes b0..b3 of 4 samples) modulo 2^32 and
+  // pk[..][1] the odd bytes (b1, b3) in two 16-bit lanes.  With at most 257
+  // channels between drains every byte-lane sum is <= 65535, so
+  // raw - (odd << 8) = E0 + 2^16 E2 exactly: the even-byte sums.
   auto drain = [&]() {
 #pragma unroll
     for (int d = 0; d < 2; d++)
 #pragma unroll
       for (int g = 0; g < G; g++) {
-        acc[d][g][0] += (int)(pk[d][g][0] & 0xFFFFu);
-        acc[d][g][2] += (int)(pk[d][g][0] >> 16);
-        acc[d][g][1] += (int)(pk[d][g][1] & 0xFFFFu);
-        acc[d][g][3] += (int)(pk[d][g][1] >> 16);
+        const uint32_t odd = pk[d][g][1];
+        const uint32_t even = pk[d][g][0] - (odd << 8);
+        acc[d][g][0] += (int)(even & 0xFFFFu);
+        acc[d][g][2] += (int)(even >> 16);
+        acc[d][g][1] += (int)(odd & 0xFFFFu);
+        acc[d][g][3] += (int)(odd >> 16);
         pk[d][g][0] = pk[d][g][1] = 0;
       }
   };
@@ -303,7 +309,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
         for (int g = 0; g < G; g++) {
           const uint32_t xa = __funnelshift_r(ra[wa + 32 * g], ra[wa + 32 * g + 1], sa);
           const uint32_t xb = __funnelshift_r(rb[wb + 32 * g], rb[wb + 32 * g + 1], sb);
-          pk[d][g][0] += (xa & 0x00FF00FFu) + (xb & 0x00FF00FFu);
+          pk[d][g][0] += xa + xb;
           pk[d][g][1] += __byte_perm(xa, 0u, 0x4341) + __byte_perm(xb, 0u, 0x4341);
         }
       }
@@ -320,7 +326,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
 #pragma unroll
         for (int g = 0; g < G; g++) {
           const uint32_t xa = __funnelshift_r(ra[wa + 32 * g], ra[wa + 32 * g + 1], sa);
-          pk[d][g][0] += xa & 0x00FF00FFu;
+          pk[d][g][0] += xa;
           pk[d][g][1] += __byte_perm(xa, 0u, 0x4341);
         }
       }

@@ -186,23 +186,39 @@ __global__ void k_baseline_stretch0(const float* __restrict__ data, size_t pitch
 }
 
 // data[i] -= stretched baseline, i < nbeams*stride - dm_delay
-__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, int nbeams, size_t stride,
-                               size_t beam_count, size_t nsub, const float* __restrict__ base,
+__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, int nbeams,
+                               unsigned stride, unsigned nsub, const float* __restrict__ base,
                                size_t sc, float step2, float step3) {
   const size_t ser = blockIdx.y;
   float* d = data + ser * pitch;
   const float* bs = base + ser * (size_t)nbeams * sc;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nsub;
-       i += (size_t)gridDim.x * blockDim.x) {
-    size_t b = i / stride;
-    float v;
-    if ((int)b < nbeams - 1) {
-      v = stretch_beam_at(bs, (unsigned)i, step2, (unsigned long long)b);
-    } else {
-      size_t t = i - (size_t)(nbeams - 1) * stride;
-      v = stretch_at(bs + (size_t)(nbeams - 1) * sc, (unsigned)t, step3);
+  const float* last = bs + (size_t)(nbeams - 1) * sc;
+  const unsigned last_start = (unsigned)(nbeams - 1) * stride;
+  // four consecutive samples per thread (rows are 16-byte aligned)
+  for (unsigned i = 4u * (blockIdx.x * blockDim.x + threadIdx.x); i < nsub;
+       i += 4u * gridDim.x * blockDim.x) {
+    float4 x;
+    const bool full = i + 3 < nsub;
+    if (full) x = *reinterpret_cast<const float4*>(d + i);
+    float* xs = reinterpret_cast<float*>(&x);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const unsigned ij = i + j;
+      if (!full) xs[j] = ij < nsub ? d[ij] : 0.f;
+      float v;
+      if (ij < last_start) {
+        v = stretch_beam_at(bs, ij, step2, (unsigned long long)(ij / stride));
+      } else {
+        v = stretch_at(last, ij - last_start, step3);
+      }
+      xs[j] = __fsub_rn(xs[j], v);
     }
-    d[i] = __fsub_rn(d[i], v);
+    if (full) {
+      *reinterpret_cast<float4*>(d + i) = x;
+    } else {
+      for (int j = 0; j < 4; j++)
+        if (i + j < nsub) d[i + j] = xs[j];
+    }
   }
 }
 
@@ -264,9 +280,12 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   const float step3 = (float)(sc - 1) / (float)(sb.beam_count - 1);    // last beam
   const size_t dm_delay = sb.stride - sb.beam_count;
   const size_t nsub = sb.stride * sb.nbeams - dm_delay;
-  dim3 grid((unsigned)((nsub + 255) / 256 < 4096 ? (nsub + 255) / 256 : 4096), sb.nser);
-  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, sb.nbeams, sb.stride, sb.beam_count,
-                                      nsub, base_out, sc, step2, step3); note_launch();
+  if (nsub >= 0xFFFFFF00u || sb.pitch % 4 || (reinterpret_cast<uintptr_t>(sb.data) & 15))
+    return cudaErrorInvalidValue;
+  const size_t nq = (nsub + 3) / 4;
+  dim3 grid((unsigned)((nq + 255) / 256 < 4096 ? (nq + 255) / 256 : 4096), sb.nser);
+  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, sb.nbeams, (unsigned)sb.stride,
+                                      (unsigned)nsub, base_out, sc, step2, step3); note_launch();
   return cudaGetLastError();
 }
 
@@ -342,122 +361,213 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // ===========================================================================
 // Normalise + exclusive prefix sum with the sequential association of the
 // reference's scan (Thrust's sequential exclusive_scan: out[0] = 0,
-// out[k+1] = out[k] + in[k]).  A segment of SCAN_SEG lanes owns one series;
-// every lane of the segment runs the same serial chain on broadcast values and
-// keeps the partial sum of its slot, so each output is the exact left-to-right
-// float sum.  Loads run SCAN_AHEAD chunks ahead of the chain (the chain is
-// ~4 cycles per sample; a load round trip is hundreds of cycles).
+// out[k+1] = out[k] + in[k]), for up to SC_MAXSER series per block.
+//
+// The left-to-right float sum of a series is one dependent chain (~4 cycles
+// per sample), so the block is split by role:
+//   warp 0       the chains: lane l owns series l of the block and runs its
+//                chain over one stage of SC_CH samples in shared memory;
+//   warps 1..np  a stage's rows arrive by TMA bulk copies requested SC_DEPTH
+//                stages ahead; these warps divide them in place by their
+//                beam's RMS, and write them out once the chain warp has
+//                replaced them with their prefix sums.
+// Stage k lives in buffer k % SC_NB.  At step k the producers normalise stage
+// k and store stage k - 2 while the chain warp scans stage k - 1, and stage
+// k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
+// step k - 1).  One block barrier ends each step.
 // ===========================================================================
-constexpr int SQ_SER = 2;        // series per block (one chain lane each)
-constexpr int SQ_CH = 256;       // samples per series per stage
-constexpr int SQ_THREADS = 32;
-constexpr int SQ_PAD = SQ_CH + 4;  // 16-byte rows; lane s reads banks 4s..4s+3
-constexpr int SQ_MAXB = 64;      // beams whose RMS is kept in shared memory
+constexpr int SC_CH = 128;           // samples per series per stage
+constexpr int SC_ROW = SC_CH + 4;    // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
+constexpr int SC_DEPTH = 5;          // stages in flight ahead of the one being normalised
+constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
+constexpr int SC_MAXSER = 32;
+constexpr int SC_MAXRMS = 2048;      // series x beams whose RMS stays in shared memory
+constexpr uint32_t SC_WAIT_LIMIT = 1u << 22;
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_addr(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-__global__ void __launch_bounds__(SQ_THREADS) k_normalise_scan(const float* __restrict__ data,
-                                                               size_t pitch, int nser,
-                                                               unsigned len, unsigned stride,
-                                                               int nbeams,
-                                                               const float* __restrict__ rms,
-                                                               float* __restrict__ scan,
-                                                               size_t scan_pitch,
-                                                               float* norm_out) {
-  extern __shared__ __align__(16) float sq_smem[];
-  float (*raw)[SQ_SER][SQ_CH] = reinterpret_cast<float (*)[SQ_SER][SQ_CH]>(sq_smem);
-  float (*val)[SQ_PAD] = reinterpret_cast<float (*)[SQ_PAD]>(sq_smem + 2 * SQ_SER * SQ_CH);
-  float* srms = sq_smem + 2 * SQ_SER * SQ_CH + SQ_SER * SQ_PAD;  // [SQ_SER][nbeams]
-  const int s0 = blockIdx.x * SQ_SER;
-  const int nb = min(SQ_SER, nser - s0);
-  const int tid = threadIdx.x;
-  const bool rms_smem = nbeams <= SQ_MAXB;
-  if (rms_smem)
-    for (int k = tid; k < nb * nbeams; k += SQ_THREADS) srms[k] = rms[(size_t)s0 * nbeams + k];
-  const unsigned nstage = (len + SQ_CH) / SQ_CH;  // covers outputs 0..len
-
-  auto load = [&](unsigned st, int buf) {
-    const unsigned base = st * SQ_CH;
-    for (int idx = tid; idx < nb * (SQ_CH / 4); idx += SQ_THREADS) {
-      const int sl = idx / (SQ_CH / 4), q = idx % (SQ_CH / 4);
-      const unsigned e0 = base + 4u * q;
-      const float* src = data + (size_t)(s0 + sl) * pitch + e0;
-      float* dst = &raw[buf][sl][4 * q];
-      if (e0 + 4 <= len) {
-        cp_async16(dst, src);
-      } else {
-        for (int k = 0; k < 4; k++) dst[k] = (e0 + k < len) ? src[k] : 0.f;
-      }
-    }
-    cp_async_commit();
-  };
-
-  float sum = 0.f;  // running sum of series (s0 + lane), lanes < nb of warp 0
-  load(0, 0);
-  for (unsigned st = 0; st < nstage; st++) {
-    const int buf = st & 1;
-    cp_async_wait_all();
-    __syncthreads();
-    if (st + 1 < nstage) load(st + 1, buf ^ 1);  // overlaps this stage
-    // normalise (get_rms.cu:344-356): x / rms[beam of sample]
-    const unsigned base = st * SQ_CH;
-    const unsigned b0 = base / stride;
-    for (int idx = tid; idx < nb * SQ_CH; idx += SQ_THREADS) {
-      const int sl = idx / SQ_CH, e = idx % SQ_CH;
-      const unsigned i = base + e;
-      float v = 0.f;
-      if (i < len) {
-        unsigned b = b0;
-        unsigned bend = (b0 + 1) * stride;
-        while (i >= bend && b + 1 < (unsigned)nbeams) { b++; bend += stride; }
-        const float rb = rms_smem ? srms[sl * nbeams + b] : rms[(size_t)(s0 + sl) * nbeams + b];
-        v = __fdiv_rn(raw[buf][sl][e], rb);
-        if (norm_out) norm_out[(size_t)(s0 + sl) * pitch + i] = v;
-      }
-      val[sl][e] = v;
-    }
-    __syncthreads();
-    // the serial chain, one lane per series, exact left-to-right order
-    if (tid < nb) {
-      float* row = val[tid];
-      for (int e = 0; e < SQ_CH; e += 8) {
-        const float4 va = *reinterpret_cast<const float4*>(row + e);
-        const float4 vb = *reinterpret_cast<const float4*>(row + e + 4);
-        float4 oa, ob;
-        oa.x = sum; sum = __fadd_rn(sum, va.x);
-        oa.y = sum; sum = __fadd_rn(sum, va.y);
-        oa.z = sum; sum = __fadd_rn(sum, va.z);
-        oa.w = sum; sum = __fadd_rn(sum, va.w);
-        ob.x = sum; sum = __fadd_rn(sum, vb.x);
-        ob.y = sum; sum = __fadd_rn(sum, vb.y);
-        ob.z = sum; sum = __fadd_rn(sum, vb.z);
-        ob.w = sum; sum = __fadd_rn(sum, vb.w);
-        *reinterpret_cast<float4*>(row + e) = oa;
-        *reinterpret_cast<float4*>(row + e + 4) = ob;
-      }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < nb * SQ_CH; idx += SQ_THREADS) {
-      const int sl = idx / SQ_CH, e = idx % SQ_CH;
-      const unsigned i = base + e;
-      if (i <= len) scan[(size_t)(s0 + sl) * scan_pitch + i] = val[sl][e];
-    }
+// a / b correctly rounded, given y = RN(1/b) (__frcp_rn): q0 = RN(a*y), the
+// residual a - b*q0 (exact by FMA), and one correction q0 + r*y (Markstein's
+// theorem: P. W. Markstein, IBM J. Res. Dev. 34(1):111-119, 1990; Muller et
+// al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018, ch. 4).  The
+// theorem needs the quotient and residual clear of underflow and overflow,
+// which |a|, |b| in [2^-40, 2^40] guarantees; other operands (zeros, tiny,
+// huge and non-finite values) take __fdiv_rn.
+__device__ __forceinline__ float div_rn_by(float a, float b, float y) {
+  const float aa = fabsf(a), ab = fabsf(b);
+  if (aa >= 0x1p-40f && aa <= 0x1p40f && ab >= 0x1p-40f && ab <= 0x1p40f) {
+    const float q0 = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-b, q0, a);
+    return __fmaf_rn(r, y, q0);
   }
+  return __fdiv_rn(a, b);
+}
+
+size_t scan_smem_bytes(int ser, int nbeams) {
+  size_t b = 128 + (size_t)SC_NB * ser * SC_ROW * sizeof(float);
+  if ((size_t)ser * nbeams <= SC_MAXRMS) b += 2 * (size_t)ser * nbeams * sizeof(float);
+  return b;
+}
+
+__global__ void __launch_bounds__(256) k_normalise_scan(
+    const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
+    int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
+    float* norm_out, int ser_per_block, unsigned* err) {
+  extern __shared__ __align__(128) float sc_smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(sc_smem);  // [SC_NB], first 128 bytes
+  const int S = ser_per_block;
+  float* rows = sc_smem + 32;                             // [SC_NB][S][SC_ROW]
+  float* srms = rows + (size_t)SC_NB * S * SC_ROW;        // [S][nbeams]
+  float* sy = srms + S * nbeams;                          // reciprocals
+  const int s0 = blockIdx.x * S;
+  const int nb = min(S, nser - s0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int np = (int)(blockDim.x >> 5) - 1;
+  const bool rms_smem = nb * nbeams <= SC_MAXRMS;
+  const unsigned nstage = len / SC_CH + 1;  // outputs 0..len
+  const unsigned len4 = (len + 3u) & ~3u;   // copies round up to 16 bytes (inside the row pitch)
+
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < SC_NB; b++) mbar_init(&full[b], 1);
+    fence_mbar_init();
+  }
+  if (rms_smem)
+    for (int k = threadIdx.x; k < nb * nbeams; k += blockDim.x) {
+      const float r = rms[(size_t)s0 * nbeams + k];
+      srms[k] = r;
+      sy[k] = __frcp_rn(r);
+    }
+  __syncthreads();
+
+  // stage st -> its buffer; warp 1, one row per lane; a stage past the data
+  // completes its barrier phase with a plain arrival
+  auto request = [&](unsigned st) {
+    uint64_t* bar = &full[st % SC_NB];
+    const unsigned base = st * SC_CH;
+    const unsigned end = min(base + (unsigned)SC_CH, len4);
+    const unsigned bytes = end > base ? (end - base) * 4u : 0u;
+    if (bytes == 0) {
+      if (lane == 0) mbar_arrive(bar);
+      return;
+    }
+    if (lane == 0) mbar_expect_tx(bar, bytes * (unsigned)nb);
+    __syncwarp();
+    // the buffer was last written by this block's threads (generic proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane < nb)
+      bulk_g2s(rows + ((size_t)(st % SC_NB) * S + lane) * SC_ROW,
+               data + (size_t)(s0 + lane) * pitch + base, bytes, bar);
+  };
+  if (warp == 1)
+    for (unsigned st = 0; st < (unsigned)SC_DEPTH && st < nstage; st++) request(st);
+
+  float sum = 0.f;     // chain of series s0 + lane (warp 0)
+  bool failed = false;
+  for (unsigned k = 0; k < nstage + 2; k++) {
+    if (warp == 0) {
+      // ---- the chains: stage k - 1 ----
+      if (k >= 1 && k - 1 < nstage && lane < nb) {
+        float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * SC_ROW;
+#pragma unroll 8
+        for (int e = 0; e < SC_CH; e += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(row + e);
+          float4 o;
+          o.x = sum; sum = __fadd_rn(sum, v.x);
+          o.y = sum; sum = __fadd_rn(sum, v.y);
+          o.z = sum; sum = __fadd_rn(sum, v.z);
+          o.w = sum; sum = __fadd_rn(sum, v.w);
+          *reinterpret_cast<float4*>(row + e) = o;
+        }
+      }
+    } else {
+      const int p = warp - 1;
+      if (warp == 1 && k + SC_DEPTH < nstage) request(k + SC_DEPTH);
+      // ---- store stage k - 2 ----
+      if (k >= 2 && k - 2 < nstage) {
+        const unsigned st = k - 2;
+        const unsigned i = st * SC_CH + 4u * lane;
+        for (int sl = p; sl < nb; sl += np) {
+          const float4 v =
+              *reinterpret_cast<const float4*>(rows + ((size_t)(st % SC_NB) * S + sl) * SC_ROW + 4 * lane);
+          float* o = scan + (size_t)(s0 + sl) * scan_pitch + i;
+          if (i + 3 <= len) {
+            *reinterpret_cast<float4*>(o) = v;
+          } else {
+            if (i <= len) o[0] = v.x;
+            if (i + 1 <= len) o[1] = v.y;
+            if (i + 2 <= len) o[2] = v.z;
+          }
+        }
+      }
+      // ---- normalise stage k (get_rms.cu:344-356): x / rms[beam of sample] ----
+      if (k < nstage) {
+        if (!mbar_wait(&full[k % SC_NB], (k / SC_NB) & 1u, SC_WAIT_LIMIT)) {
+          if (!failed && err && lane == 0) atomicOr(err, 2u);
+          failed = true;
+        }
+        const unsigned base = k * SC_CH;
+        const unsigned i = base + 4u * lane;
+        unsigned b0 = base / stride;
+        if (b0 > (unsigned)nbeams - 1) b0 = (unsigned)nbeams - 1;
+        const unsigned bend = (b0 + 1) * stride;
+        for (int sl = p; sl < nb; sl += np) {
+          float4* cell =
+              reinterpret_cast<float4*>(rows + ((size_t)(k % SC_NB) * S + sl) * SC_ROW + 4 * lane);
+          float x[4];
+          *reinterpret_cast<float4*>(x) = *cell;
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const unsigned ij = i + j;
+            if (ij >= len) { x[j] = 0.f; continue; }
+            unsigned b;
+            if (stride >= (unsigned)SC_CH) b = (ij >= bend && b0 + 1 < (unsigned)nbeams) ? b0 + 1 : b0;
+            else b = min(ij / stride, (unsigned)nbeams - 1);
+            if (rms_smem) {
+              const int q = sl * nbeams + (int)b;
+              x[j] = div_rn_by(x[j], srms[q], sy[q]);
+            } else {
+              x[j] = __fdiv_rn(x[j], rms[(size_t)(s0 + sl) * nbeams + b]);
+            }
+          }
+          *cell = *reinterpret_cast<float4*>(x);
+          if (norm_out) {
+            float* o = norm_out + (size_t)(s0 + sl) * pitch + i;
+            if (i + 3 < len) {
+              *reinterpret_cast<float4*>(o) = *reinterpret_cast<float4*>(x);
+            } else {
+              for (int j = 0; j < 4; j++)
+                if (i + j < len) o[j] = x[j];
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // every copy has been waited for at its normalise step; after a timed-out
+  // wait, let the buffers' last copies land before the block exits
+  if (failed && warp == 1)
+    for (unsigned st = (nstage > SC_NB ? nstage - SC_NB : 0); st < nstage; st++)
+      mbar_wait(&full[st % SC_NB], (st / SC_NB) & 1u, SC_WAIT_LIMIT);
 }
 
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
-                           size_t scan_pitch, float* norm_out, cudaStream_t s) {
-  if (sb.len >= 0xFFFFFF00u || sb.pitch % 4) return cudaErrorInvalidValue;
-  const size_t smem = (2 * SQ_SER * SQ_CH + SQ_SER * SQ_PAD + SQ_SER * SQ_MAXB) * sizeof(float);
-  cudaFuncSetAttribute(k_normalise_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_normalise_scan<<<(unsigned)((sb.nser + SQ_SER - 1) / SQ_SER), SQ_THREADS, smem, s>>>(
+                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err) {
+  if (sb.len >= 0xFFFFFF00u || sb.pitch % 4 || scan_pitch % 4 || sb.stride == 0 ||
+      sb.pitch < ((sb.len + 3) & ~(size_t)3) || scan_pitch < sb.len + 1 ||
+      (reinterpret_cast<uintptr_t>(sb.data) & 15) || (reinterpret_cast<uintptr_t>(scan) & 15) ||
+      (norm_out && (reinterpret_cast<uintptr_t>(norm_out) & 15)))
+    return cudaErrorInvalidValue;
+  if (sb.nser <= 0) return cudaSuccess;
+  // series per block: enough blocks to cover the SMs twice where possible
+  int ser = SC_MAXSER;
+  while (ser > 1 && (sb.nser + ser - 1) / ser < 296) ser /= 2;
+  const int np = ser < 7 ? ser : 7;
+  const size_t smem = scan_smem_bytes(ser, sb.nbeams);
+  cudaError_t e = cudaFuncSetAttribute(k_normalise_scan,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_normalise_scan<<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
       sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
-      scan_pitch, norm_out); note_launch();
+      scan_pitch, norm_out, ser, err); note_launch();
   return cudaGetLastError();
 }
 

@@ -161,7 +161,8 @@ hd_error clean_units(hd_pipeline pl, size_t units, const uint8_t* tf, size_t nsa
   hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
   HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
   HD_TRY(hdb::rms_beams(sb, pl->rms0.as<float>(), ws, s));
-  HD_TRY(hdb::normalise_scan(sb, pl->rms0.as<float>(), pl->dm0_scan.as<float>(), spitch, x, s));
+  HD_TRY(hdb::normalise_scan(sb, pl->rms0.as<float>(), pl->dm0_scan.as<float>(), spitch, x, s,
+                             pl->plan->d_err));
   for (size_t u = 0; u < U; u++) {
     int* mask = pl->mask.as<int>() + u * nsamps;
     HD_TRY(hdb::rfi_mask(x + u * spitch, pl->dm0_scan.as<float>() + u * spitch, nsamps,
@@ -318,6 +319,7 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   if (nsamps < nbeams * (P.boxcar_max + max_delay)) *nsamps_processed = 0;
 
   cudaEventRecord(pl->ev[0], s);
+  HD_TRY(cudaMemsetAsync(pl->plan->d_err, 0, sizeof(unsigned), s));
   // ---- H2D ----------------------------------------------------------------
   const size_t fb_bytes = nsamps * C;
   HD_TRY(pl->fb_tf.ensure(U * fb_bytes));
@@ -381,7 +383,7 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     const size_t scan_pitch = round_up(nc + 1, 4);
     HD_TRY(pl->scan.ensure(NS * scan_pitch * sizeof(float)));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), pl->scan.as<float>(), scan_pitch,
-                               nullptr, s));
+                               nullptr, s, pl->plan->d_err));
     cudaEventRecord(pl->ev[4], s);
 
     // ---- widths --------------------------------------------------------------

@@ -244,8 +244,14 @@ const dedisp_float* dedisp_generate_dm_list_guru(dedisp_float a, dedisp_float b,
 
 dedisp_error dedisp_set_killmask(dedisp_plan p, const dedisp_bool* km) {
   if (!p) return DEDISP_INVALID_PLAN;
-  for (size_t c = 0; c < p->nchans; c++) p->killmask[c] = km ? (km[c] != 0) : 1;
-  p->dirty = true;
+  // the device tables depend on the mask: rebuild them only when it changes
+  bool changed = false;
+  for (size_t c = 0; c < p->nchans; c++) {
+    const int v = km ? (km[c] != 0) : 1;
+    changed = changed || p->killmask[c] != v;
+    p->killmask[c] = v;
+  }
+  if (changed) p->dirty = true;
   return DEDISP_NO_ERROR;
 }
 
@@ -330,8 +336,9 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
     cudaMemsetAsync(p->d_in_ft, 0, need_ft, s);
     p->d_in_ft_cap = need_ft;
   }
-  if (hdb::launch_transpose_tf_ft(d_tf, nsamps, (int)p->nchans, p->d_in_ft, pitch, s) !=
-      cudaSuccess)
+  if (cudaMemsetAsync(p->d_err, 0, sizeof(unsigned), s) != cudaSuccess ||
+      hdb::launch_transpose_tf_ft(d_tf, nsamps, (int)p->nchans, p->d_in_ft, pitch, s) !=
+          cudaSuccess)
     return DEDISP_INTERNAL_GPU_ERROR;
   float* d_o = reinterpret_cast<float*>(out);
   size_t opitch = out_stride / 4;
