@@ -42,6 +42,16 @@ __device__ __forceinline__ float med5(float a, float b, float c, float d, float 
   return (c < b) ? c : b;
 }
 
+// Median of 5 by min/max: drop the smallest and the largest of a..d (the
+// larger of the pair minima and the smaller of the pair maxima remain), then
+// take the median of those two and e.  Equal to med5 for NaN-free input (both
+// select the middle value); callers use it only where NaN is excluded.
+__device__ __forceinline__ float med5_mm(float a, float b, float c, float d, float e) {
+  const float lo = fmaxf(fminf(a, b), fminf(c, d));
+  const float hi = fminf(fmaxf(a, b), fmaxf(c, d));
+  return fmaxf(fminf(lo, hi), fminf(fmaxf(lo, hi), e));
+}
+
 // Order-preserving 32-bit key of a float (larger float -> larger key).
 __device__ __forceinline__ uint32_t float_key(float f) {
   uint32_t u = __float_as_uint(f);

@@ -36,8 +36,11 @@ int dedisp_dm_block();
 int dedisp_time_block();
 size_t dedisp_smem_bytes(int rowb);
 cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s);
+// TF -> channel-major copy of `units` filterbanks (nsamps x nchans bytes each,
+// consecutive in `in`); unit u's copy starts at out + u * out_unit.
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
-                                   size_t pitch, cudaStream_t s);
+                                   size_t pitch, cudaStream_t s, size_t units = 1,
+                                   size_t out_unit = 0);
 cudaError_t launch_dm0_sum(const uint8_t* in, size_t nsamps, int nchans, float* out,
                            cudaStream_t s);
 cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* mask,

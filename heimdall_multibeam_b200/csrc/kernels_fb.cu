@@ -22,8 +22,11 @@ unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC
 __global__ void __launch_bounds__(256) k_transpose_tf_ft(const uint8_t* __restrict__ in,
                                                          size_t nsamps, int nchans,
                                                          uint8_t* __restrict__ out,
-                                                         size_t pitch) {
+                                                         size_t pitch, size_t out_unit) {
   __shared__ uint32_t tile[128][33];  // [t][channel word], +1 word against conflicts
+  // blockIdx.z: unit (independent filterbank) of a batch
+  in += (size_t)blockIdx.z * nsamps * (size_t)nchans;
+  out += (size_t)blockIdx.z * out_unit;
   const size_t t0 = (size_t)blockIdx.x * 128;
   const int c0 = blockIdx.y * 128;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -365,9 +368,10 @@ __global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
 // Host launchers
 // ---------------------------------------------------------------------------
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
-                                   size_t pitch, cudaStream_t s) {
-  dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128));
-  k_transpose_tf_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, out, pitch); note_launch();
+                                   size_t pitch, cudaStream_t s, size_t units, size_t out_unit) {
+  if (units < 1 || units > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128), (unsigned)units);
+  k_transpose_tf_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, out, pitch, out_unit); note_launch();
   return cudaGetLastError();
 }
 

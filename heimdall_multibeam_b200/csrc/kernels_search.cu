@@ -508,6 +508,26 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
         unsigned b0 = base / stride;
         if (b0 > (unsigned)nbeams - 1) b0 = (unsigned)nbeams - 1;
         const unsigned bend = (b0 + 1) * stride;
+        // common case: the stage lies inside the data and inside one beam, so
+        // one divisor (and its reciprocal) serves the whole row
+        const bool uniform = rms_smem && base + SC_CH <= len && stride >= (unsigned)SC_CH &&
+                             (b0 + 1 >= (unsigned)nbeams || bend >= base + SC_CH);
+        if (uniform) {
+          for (int sl = p; sl < nb; sl += np) {
+            float4* cell = reinterpret_cast<float4*>(rows + ((size_t)(k % SC_NB) * S + sl) * SC_ROW +
+                                                     4 * lane);
+            const int q = sl * nbeams + (int)b0;
+            const float rb = srms[q], y = sy[q];
+            float4 x = *cell;
+            x.x = div_rn_by(x.x, rb, y);
+            x.y = div_rn_by(x.y, rb, y);
+            x.z = div_rn_by(x.z, rb, y);
+            x.w = div_rn_by(x.w, rb, y);
+            *cell = x;
+            if (norm_out)
+              *reinterpret_cast<float4*>(norm_out + (size_t)(s0 + sl) * pitch + i) = x;
+          }
+        } else
         for (int sl = p; sl < nb; sl += np) {
           float4* cell =
               reinterpret_cast<float4*>(rows + ((size_t)(k % SC_NB) * S + sl) * SC_ROW + 4 * lane);
@@ -663,6 +683,139 @@ __global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m, in
   }
 }
 
+// Pass 1 for several unscrunched widths, one median level of every width per
+// block barrier.  Level 1 works on runs of 4 consecutive medians (20
+// consecutive samples): with the boxcar offset a multiple of 4, both ends of a
+// width >= 8 boxcar are 16-byte aligned in the staged window and load as
+// float4 (a thread stride of 80 bytes keeps the 8 lanes of each access phase
+// on distinct banks); widths 1, 2 and 4 read one 28-value window.
+constexpr int BRV_THREADS = 256;
+
+template <int AH, int BH>
+__device__ __forceinline__ void brv_small(const float* win, float* v) {
+#pragma unroll
+  for (int r = 0; r < 20; r++) v[r] = fabsf(__fsub_rn(win[4 + r + AH], win[4 + r - BH]));
+}
+
+template <bool MM>
+__device__ __forceinline__ float brv_med5(float a, float b, float c, float d, float e) {
+  return MM ? med5_mm(a, b, c, d, e) : med5(a, b, c, d, e);
+}
+
+template <bool MM>
+__device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, int w0, int nwb,
+                           int m, float* la, float* lb, float* __restrict__ out,
+                           size_t out_pitch, size_t ser, size_t g) {
+  const int n1 = (int)pow5(m - 1);
+  const int n1p = (n1 + 3) & ~3;
+
+  // ---- level 1 ----
+  const int nq = n1 / 4, rem = n1 - 4 * nq;
+  for (int item = threadIdx.x; item < nwb * nq; item += blockDim.x) {
+    const int wl = item / nq, k0 = 4 * (item - wl * nq);
+    const int wi = w0 + wl;
+    float v[20];
+    if (wi < 3) {
+      float wv[28];
+      const float4* p = reinterpret_cast<const float4*>(tile + 5 * k0 + offset - 4);
+#pragma unroll
+      for (int r = 0; r < 7; r++) {
+        const float4 x = p[r];
+        wv[4 * r] = x.x; wv[4 * r + 1] = x.y; wv[4 * r + 2] = x.z; wv[4 * r + 3] = x.w;
+      }
+      if (wi == 0) brv_small<1, 0>(wv, v);
+      else if (wi == 1) brv_small<1, 1>(wv, v);
+      else brv_small<2, 2>(wv, v);
+    } else {
+      const int h = ctx.winfo[wi].ahead;  // = behind = width / 2
+      const float4* pa = reinterpret_cast<const float4*>(tile + 5 * k0 + offset + h);
+      const float4* pb = reinterpret_cast<const float4*>(tile + 5 * k0 + offset - h);
+#pragma unroll
+      for (int r = 0; r < 5; r++) {
+        const float4 a = pa[r], b = pb[r];
+        v[4 * r] = fabsf(__fsub_rn(a.x, b.x));
+        v[4 * r + 1] = fabsf(__fsub_rn(a.y, b.y));
+        v[4 * r + 2] = fabsf(__fsub_rn(a.z, b.z));
+        v[4 * r + 3] = fabsf(__fsub_rn(a.w, b.w));
+      }
+    }
+    float4 o;
+    o.x = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+    o.y = brv_med5<MM>(v[5], v[6], v[7], v[8], v[9]);
+    o.z = brv_med5<MM>(v[10], v[11], v[12], v[13], v[14]);
+    o.w = brv_med5<MM>(v[15], v[16], v[17], v[18], v[19]);
+    *reinterpret_cast<float4*>(la + wl * n1p + k0) = o;
+  }
+  for (int item = threadIdx.x; item < nwb * rem; item += blockDim.x) {
+    const int wl = item / rem, k = 4 * nq + (item - wl * rem);
+    const WidthInfo& w = ctx.winfo[w0 + wl];
+    const int a = offset + w.ahead, b = offset - w.behind;
+    float v[5];
+#pragma unroll
+    for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
+    la[wl * n1p + k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+  }
+  __syncthreads();
+
+  // ---- levels 2..m, all widths per barrier ----
+  float* cur = la;
+  float* nxt = lb;
+  int n = n1, pitch_cur = n1p;
+  for (int lev = 2; lev <= m; lev++) {
+    const int nn = n / 5;
+    for (int item = threadIdx.x; item < nwb * nn; item += blockDim.x) {
+      const int wl = item / nn, k = item - wl * nn;
+      const float* c = cur + wl * pitch_cur + 5 * k;
+      nxt[wl * nn + k] = brv_med5<MM>(c[0], c[1], c[2], c[3], c[4]);
+    }
+    __syncthreads();
+    float* t = cur; cur = nxt; nxt = t;
+    n = nn;
+    pitch_cur = nn;
+  }
+  // n == 1: one value per width
+  for (int wl = threadIdx.x; wl < nwb; wl += blockDim.x)
+    out[(ser * nwb + wl) * out_pitch + g] = cur[wl * pitch_cur];
+}
+
+__global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ctx, int w0,
+                                                                     int nwb, int m, int win,
+                                                                     float* __restrict__ out,
+                                                                     size_t out_pitch) {
+  extern __shared__ __align__(16) float dyn[];
+  const int win4 = (win + 3) & ~3;
+  float* tile = dyn;                     // win floats
+  const int n1 = (int)pow5(m - 1);       // level-1 medians per width
+  const int n1p = (n1 + 3) & ~3;         // row pitch: 16-byte aligned rows
+  float* la = dyn + win4;                // [nwb][n1p]
+  float* lb = la + nwb * n1p;            // [nwb][n1 / 5]
+  const size_t ser = blockIdx.y;
+  const size_t g = blockIdx.x;
+  const WidthInfo& w_first = ctx.winfo[w0];
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
+  const float delta = (float)(ctx.stride - w_first.bn);
+  const size_t gsz = pow5(m);
+  const size_t q0 = g * gsz;
+  const size_t i_first = reblock_index((unsigned)q0 / w_first.bn, delta, (unsigned)q0);
+  const size_t q1 = q0 + gsz - 1;
+  const size_t i_last = reblock_index((unsigned)q1 / w_first.bn, delta, (unsigned)q1);
+  const int offset = ctx.offset;
+  const size_t span = (i_last - i_first) + 2 * (size_t)offset + 2;
+  // the launcher guarantees a contiguous group whose window fits (span <= win)
+  if (i_last - i_first != gsz - 1 || span > (size_t)win) return;
+  for (size_t k = threadIdx.x; k < span; k += blockDim.x) tile[k] = sc[i_first + k];
+  // A prefix sum that is finite at its end is finite everywhere (a non-finite
+  // term would stay non-finite), so every boxcar value is NaN-free and the
+  // min/max median network selects the same values as the reference's.
+  const float last = sc[ctx.scan_len - 1];
+  const bool finite = fabsf(last) <= 3.402823466e38f;
+  __syncthreads();
+  if (finite)
+    brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+  else
+    brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+}
+
 __global__ void k_block_rms_final(WidthCtx ctx, int w0, int nwb, const float* __restrict__ lev,
                                   size_t lev_pitch, size_t count, int from_window) {
   int seg = blockIdx.x * blockDim.x + threadIdx.x;
@@ -708,6 +861,34 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
   bool unscrunched = true;
   for (int wi = w_begin; wi < w_end; wi++) unscrunched = unscrunched && hw[wi].ts == 1;
+  bool vec = unscrunched && ctx.offset >= 4 && (ctx.offset & 3) == 0;
+  for (int wi = w_begin; vec && wi < w_end; wi++) {
+    const WidthInfo& w = hw[wi];
+    vec = w.width == (1 << wi) && w.ahead == (w.width - 1) / 2 + 1 && w.behind == w.width / 2;
+  }
+  // a group of samples is contiguous unless it straddles a beam gap
+  // (nbeams > 1); single-beam series always take the vector kernel
+  if (vec && ctx.nbeams == 1) {
+    const size_t win = pow5(m1) + 2 * (size_t)ctx.offset + 2;
+    const size_t n1 = pow5(m1 - 1);
+    const size_t smem =
+        (((win + 3) & ~(size_t)3) + nwb * ((n1 + 3) & ~(size_t)3) + nwb * (n1 / 5 + 1)) *
+        sizeof(float);
+    if (smem <= 200 * 1024) {
+      cudaFuncSetAttribute(k_block_rms_pass1_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      k_block_rms_pass1_vec<<<dim3((unsigned)ng1, ctx.nser), BRV_THREADS, smem, s>>>(
+          ctx, w_begin, nwb, m1, (int)win, ws.a, ng1); note_launch();
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      float* fin;
+      size_t fin_pitch, fin_count;
+      e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
+      if (e != cudaSuccess) return e;
+      k_block_rms_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(ctx, w_begin, nwb, fin,
+                                                                       fin_pitch, fin_count, 0); note_launch();
+      return cudaGetLastError();
+    }
+  }
   if (unscrunched) {
     // window: one group of samples plus the widest boxcar on either side
     const size_t win = std::min<size_t>(pow5(m1) + 2 * (size_t)ctx.offset + 2, MULTI_SMEM_FLOATS);
@@ -966,6 +1147,301 @@ __global__ void __launch_bounds__(HIT_THREADS) k_write_hits_multi(WidthCtx ctx, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Vector form of the unscrunched-width kernels, used when the boxcar offset is
+// a multiple of 4 (boxcar_max >= 8): every thread owns runs of 4 consecutive
+// samples (j = 4t + q and 1024 + 4t + q), so both ends of a boxcar of width
+// >= 8 are 16-byte aligned in the staged window and load as float4; widths
+// 1, 2 and 4 read one 12-value window around the run.  Consecutive lanes read
+// consecutive 16-byte words (no bank conflicts).  Per-width counts are kept
+// in 16-bit halves of registers and reduced once per tile.
+// ---------------------------------------------------------------------------
+constexpr int VH_MAXW = 16;
+
+struct VecTile {
+  float* tile;
+  unsigned valid;  // bit g*4+q: sample (g, q) of this thread is in a searched window
+};
+
+__device__ __forceinline__ VecTile vec_stage(const WidthCtx& ctx, const float* sc, size_t i0,
+                                             float* tile, size_t span4, size_t slen) {
+  for (size_t k = 4 * threadIdx.x; k < span4; k += 4 * blockDim.x) {
+    float4 v;
+    if (i0 + k + 3 < slen) {
+      v = *reinterpret_cast<const float4*>(sc + i0 + k);
+    } else {
+      v.x = (i0 + k < slen) ? sc[i0 + k] : 0.f;
+      v.y = (i0 + k + 1 < slen) ? sc[i0 + k + 1] : 0.f;
+      v.z = (i0 + k + 2 < slen) ? sc[i0 + k + 2] : 0.f;
+      v.w = 0.f;
+    }
+    *reinterpret_cast<float4*>(tile + k) = v;
+  }
+  // in-window test (find_giants.cu:47-60): i < n and (i mod beam stride) < bn,
+  // the same for every unscrunched width
+  const WidthInfo& w = ctx.winfo[0];
+  const unsigned stride = (unsigned)ctx.stride;
+  const unsigned ui0 = (unsigned)i0;
+  unsigned valid;
+  const unsigned r0 = ui0 % stride;
+  if (ui0 + HIT_TILE <= w.n && r0 + HIT_TILE <= w.bn) {
+    valid = 0xFFu;  // the whole tile lies inside one beam's searched window
+  } else {
+    valid = 0;
+#pragma unroll
+    for (int g = 0; g < 2; g++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const unsigned i = ui0 + 1024u * g + 4u * threadIdx.x + q;
+        if (i < w.n && (i % stride) < w.bn) valid |= 1u << (g * 4 + q);
+      }
+  }
+  __syncthreads();
+  return VecTile{tile, valid};
+}
+
+// Boxcar values of width wi for the 4 samples of run j0 (window: the 12 staged
+// values from j0 + offset - 4).
+template <int AH, int BH>
+__device__ __forceinline__ void win_boxcar(const float* win, float* d) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) d[q] = __fsub_rn(win[4 + q + AH], win[4 + q - BH]);
+}
+
+// widths 1, 2, 4: ahead = (w - 1) / 2 + 1, behind = w / 2 (matched_filter.cu:37-67)
+__device__ __forceinline__ void vec_boxcar(const float* tile, int j0, int offset, int wi,
+                                           int ahead, int behind, const float* win,
+                                           float* d) {
+  if (wi == 0) {
+    win_boxcar<1, 0>(win, d);
+  } else if (wi == 1) {
+    win_boxcar<1, 1>(win, d);
+  } else if (wi == 2) {
+    win_boxcar<2, 2>(win, d);
+  } else {
+    const float4 va = *reinterpret_cast<const float4*>(tile + j0 + offset + ahead);
+    const float4 vb = *reinterpret_cast<const float4*>(tile + j0 + offset - behind);
+    d[0] = __fsub_rn(va.x, vb.x);
+    d[1] = __fsub_rn(va.y, vb.y);
+    d[2] = __fsub_rn(va.z, vb.z);
+    d[3] = __fsub_rn(va.w, vb.w);
+  }
+}
+
+__device__ __forceinline__ void vec_window(const float* tile, int j0, int offset, float* win) {
+  const float4* p = reinterpret_cast<const float4*>(tile + j0 + offset - 4);
+  const float4 x0 = p[0], x1 = p[1], x2 = p[2];
+  win[0] = x0.x; win[1] = x0.y; win[2] = x0.z; win[3] = x0.w;
+  win[4] = x1.x; win[5] = x1.y; win[6] = x1.z; win[7] = x1.w;
+  win[8] = x2.x; win[9] = x2.y; win[10] = x2.z; win[11] = x2.w;
+}
+
+// For a positive finite norm, RN(d * norm) is non-decreasing in d, so the
+// threshold test RN(d * norm) > thresh holds exactly for d >= dmin, the
+// smallest float that passes it.  dmin starts from RN(thresh / norm) and is
+// moved by single ulps until it passes and its predecessor does not.
+// Returns false (use the product) when no such bound is found.
+__device__ bool hit_bound(float nrm, float thresh, float* dmin) {
+  if (!(nrm > 0.f) || !(nrm <= 3.402823466e38f)) return false;
+  float d = __fdiv_rn(thresh, nrm);
+  if (!(fabsf(d) <= 3.402823466e38f)) return false;
+  for (int it = 0; it < 16 && !(__fmul_rn(d, nrm) > thresh); it++) d = nextafterf(d, INFINITY);
+  for (int it = 0; it < 16; it++) {
+    const float p = nextafterf(d, -INFINITY);
+    if (__fmul_rn(p, nrm) > thresh) d = p;
+    else break;
+  }
+  if (!(__fmul_rn(d, nrm) > thresh) || __fmul_rn(nextafterf(d, -INFINITY), nrm) > thresh)
+    return false;
+  *dmin = d;
+  return true;
+}
+
+template <bool ALLV, bool MUL>
+__device__ __forceinline__ void count_vec_body(const float* tile, int offset, int nw1,
+                                               unsigned valid, const int* s_ahead,
+                                               const int* s_behind, const float* s_norm,
+                                               const float* s_dmin, float thresh,
+                                               unsigned* cnt) {
+#pragma unroll
+  for (int g = 0; g < 2; g++) {
+    const int j0 = 1024 * g + 4 * threadIdx.x;
+    float win[12];
+    vec_window(tile, j0, offset, win);
+    const unsigned vg = (valid >> (4 * g)) & 0xFu;
+#pragma unroll
+    for (int wi = 0; wi < VH_MAXW; wi++) {
+      if (wi >= nw1) break;
+      float d[4];
+      vec_boxcar(tile, j0, offset, wi, s_ahead[wi], s_behind[wi], win, d);
+      unsigned c = 0;
+      if (MUL) {
+        const float nrm = s_norm[wi];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          c += (ALLV || ((vg >> q) & 1u)) && (__fmul_rn(d[q], nrm) > thresh);
+      } else {
+        const float dm = s_dmin[wi];
+#pragma unroll
+        for (int q = 0; q < 4; q++) c += (ALLV || ((vg >> q) & 1u)) && (d[q] >= dm);
+      }
+      cnt[wi >> 1] += c << (16 * (wi & 1));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(HIT_THREADS) k_count_hits_vec(WidthCtx ctx, HitBuffers hb,
+                                                                int nw1, size_t slen,
+                                                                size_t span4) {
+  extern __shared__ __align__(16) float tile[];
+  __shared__ int s_ahead[VH_MAXW], s_behind[VH_MAXW];
+  __shared__ float s_norm[VH_MAXW], s_dmin[VH_MAXW];
+  __shared__ int s_mul;
+  __shared__ unsigned red[HIT_THREADS / 32][VH_MAXW / 2];
+  const size_t ser = blockIdx.y;
+  const unsigned t = blockIdx.x;
+  const float thresh = ctx.thresh;
+  if (threadIdx.x == 0) s_mul = 0;
+  __syncthreads();
+  if (threadIdx.x < (unsigned)nw1) {
+    s_ahead[threadIdx.x] = ctx.winfo[threadIdx.x].ahead;
+    s_behind[threadIdx.x] = ctx.winfo[threadIdx.x].behind;
+    const float nrm = ctx.norm[ser * ctx.nw + threadIdx.x];
+    s_norm[threadIdx.x] = nrm;
+    float dm = 0.f;
+    if (!hit_bound(nrm, thresh, &dm)) atomicOr(&s_mul, 1);
+    s_dmin[threadIdx.x] = dm;
+  }
+  const size_t i0 = (size_t)t * HIT_TILE;
+  const VecTile vt = vec_stage(ctx, ctx.scan + ser * ctx.scan_pitch, i0, tile, span4, slen);
+  const int offset = ctx.offset;
+  unsigned cnt[VH_MAXW / 2];
+#pragma unroll
+  for (int p = 0; p < VH_MAXW / 2; p++) cnt[p] = 0;
+  // both flags are uniform across the block
+  const bool allv = vt.valid == 0xFFu && ((unsigned)i0 % (unsigned)ctx.stride) + HIT_TILE <=
+                                            ctx.winfo[0].bn &&
+                    (unsigned)i0 + HIT_TILE <= ctx.winfo[0].n;
+  if (s_mul) {
+    if (allv) count_vec_body<true, true>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+    else count_vec_body<false, true>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+  } else {
+    if (allv) count_vec_body<true, false>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+    else count_vec_body<false, false>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int p = 0; p < VH_MAXW / 2; p++) {
+    if (2 * p >= nw1) break;
+    unsigned c = cnt[p];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) red[warp][p] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x < (unsigned)nw1) {
+    const int wi = threadIdx.x;
+    unsigned tot = 0;
+    for (int k = 0; k < HIT_THREADS / 32; k++) tot += (red[k][wi >> 1] >> (16 * (wi & 1))) & 0xFFFFu;
+    const size_t sw = ser * ctx.nw + wi;
+    hb.tile_cnt[sw * hb.ntiles + t] = tot;
+    if (tot) atomicAdd(&hb.sw_cnt[sw], tot);
+  }
+}
+
+__global__ void __launch_bounds__(HIT_THREADS) k_write_hits_vec(WidthCtx ctx, HitBuffers hb,
+                                                                int nw1, size_t slen,
+                                                                size_t span4) {
+  extern __shared__ __align__(16) float tile[];
+  __shared__ unsigned wsum[HIT_THREADS / 32];
+  const size_t ser = blockIdx.y;
+  const unsigned t = blockIdx.x;
+  unsigned any = 0;
+  for (int wi = 0; wi < nw1; wi++) any |= hb.tile_cnt[(ser * ctx.nw + wi) * hb.ntiles + t];
+  if (!any) return;  // uniform across the block
+  const size_t i0 = (size_t)t * HIT_TILE;
+  const VecTile vt = vec_stage(ctx, ctx.scan + ser * ctx.scan_pitch, i0, tile, span4, slen);
+  const float thresh = ctx.thresh;
+  const int offset = ctx.offset;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float win0[12], win1[12];
+  vec_window(tile, 4 * threadIdx.x, offset, win0);
+  vec_window(tile, 1024 + 4 * threadIdx.x, offset, win1);
+  for (int wi = 0; wi < nw1; wi++) {
+    const size_t sw = ser * ctx.nw + wi;
+    if (hb.tile_cnt[sw * hb.ntiles + t] == 0) continue;  // uniform across the block
+    const WidthInfo& w = ctx.winfo[wi];
+    const float nrm = ctx.norm[sw];
+    float v0[4], v1[4];
+    vec_boxcar(tile, 4 * threadIdx.x, offset, wi, w.ahead, w.behind, win0, v0);
+    vec_boxcar(tile, 1024 + 4 * threadIdx.x, offset, wi, w.ahead, w.behind, win1, v1);
+    unsigned f = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      v0[q] = __fmul_rn(v0[q], nrm);
+      v1[q] = __fmul_rn(v1[q], nrm);
+      if (((vt.valid >> q) & 1u) && v0[q] > thresh) f |= 1u << q;
+      if (((vt.valid >> (4 + q)) & 1u) && v1[q] > thresh) f |= 1u << (4 + q);
+    }
+    // hits in index order: all of run group 0 (samples 0..1023) by thread,
+    // then group 1; one block exclusive scan of (count0 | count1 << 16)
+    const unsigned c = (unsigned)__popc(f & 0xFu) | ((unsigned)__popc(f >> 4) << 16);
+    unsigned x = c;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, x, dd);
+      if (lane >= dd) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    unsigned pre = 0, tot = 0;
+    for (int k = 0; k < HIT_THREADS / 32; k++) {
+      const unsigned ws = wsum[k];
+      pre += (k < warp) ? ws : 0u;
+      tot += ws;
+    }
+    __syncthreads();
+    pre += x - c;  // exclusive, both halves
+    const unsigned base = hb.sw_off[sw] + hb.tile_off[sw * hb.ntiles + t];
+    const unsigned p0 = base + (pre & 0xFFFFu);
+    const unsigned p1 = base + (tot & 0xFFFFu) + (pre >> 16);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if ((f >> q) & 1u) {
+        const unsigned pos = p0 + __popc(f & ((1u << q) - 1u));
+        if (pos < hb.cap) {
+          hb.ind[pos] = (unsigned)(i0 + 4 * threadIdx.x + q);
+          hb.val[pos] = v0[q];
+          hb.sw[pos] = (unsigned)sw;
+        }
+      }
+      if ((f >> (4 + q)) & 1u) {
+        const unsigned pos = p1 + __popc((f >> 4) & ((1u << q) - 1u));
+        if (pos < hb.cap) {
+          hb.ind[pos] = (unsigned)(i0 + 1024 + 4 * threadIdx.x + q);
+          hb.val[pos] = v1[q];
+          hb.sw[pos] = (unsigned)sw;
+        }
+      }
+    }
+  }
+}
+
+// Vector kernels apply when the offset is a multiple of 4 (>= 4), the widths
+// are 1, 2, 4, ... and at most VH_MAXW of them are unscrunched.
+static bool vec_hits_ok(const WidthCtx& ctx, int nw1) {
+  if (nw1 < 1 || nw1 > VH_MAXW || ctx.offset < 4 || (ctx.offset & 3) || (ctx.scan_pitch & 3) ||
+      (reinterpret_cast<uintptr_t>(ctx.scan) & 15) || ctx.stride >= 0xFFFFFFFFull)
+    return false;
+  for (int wi = 0; wi < nw1; wi++) {
+    const WidthInfo& w = ctx.host_winfo[wi];
+    if (w.width != (1 << wi)) return false;
+    if (w.ahead != (w.width - 1) / 2 + 1 || w.behind != w.width / 2) return false;
+    if (wi >= 3 && (((w.ahead | w.behind) & 3) != 0)) return false;
+  }
+  return true;
+}
+
 cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cudaStream_t s) {
   hb.ntiles = ntiles;
   cudaError_t e = cudaMemsetAsync(hb.sw_cnt, 0, ((size_t)ctx.nser * ctx.nw + 1) * sizeof(unsigned), s);
@@ -974,8 +1450,14 @@ cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cud
   int nw1 = 0;
   while (nw1 < ctx.nw && ctx.host_winfo[nw1].ts == 1) nw1++;
   const size_t smem = (HIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
+  const size_t span4 = (HIT_TILE + 2 * (size_t)ctx.offset + 2 + 3) & ~(size_t)3;
   const size_t slen = ctx.scan_len;
-  if (nw1 > 0 && smem <= 200 * 1024) {
+  if (vec_hits_ok(ctx, nw1) && span4 * sizeof(float) <= 200 * 1024) {
+    cudaFuncSetAttribute(k_count_hits_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(span4 * sizeof(float)));
+    k_count_hits_vec<<<dim3(ntiles, ctx.nser), HIT_THREADS, span4 * sizeof(float), s>>>(
+        ctx, hb, nw1, slen, span4); note_launch();
+  } else if (nw1 > 0 && smem <= 200 * 1024) {
     cudaFuncSetAttribute(k_count_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_count_hits_multi<<<dim3(ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
   } else {
@@ -998,8 +1480,14 @@ cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
   int nw1 = 0;
   while (nw1 < ctx.nw && ctx.host_winfo[nw1].ts == 1) nw1++;
   const size_t smem = (HIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
+  const size_t span4 = (HIT_TILE + 2 * (size_t)ctx.offset + 2 + 3) & ~(size_t)3;
   const size_t slen = ctx.scan_len;
-  if (nw1 > 0 && smem <= 200 * 1024) {
+  if (vec_hits_ok(ctx, nw1) && span4 * sizeof(float) <= 200 * 1024) {
+    cudaFuncSetAttribute(k_write_hits_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(span4 * sizeof(float)));
+    k_write_hits_vec<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, span4 * sizeof(float), s>>>(
+        ctx, hb, nw1, slen, span4); note_launch();
+  } else if (nw1 > 0 && smem <= 200 * 1024) {
     cudaFuncSetAttribute(k_write_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_write_hits_multi<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
   } else {

@@ -47,6 +47,10 @@ struct DevBuf {
 
 }  // namespace
 
+// Host filterbanks of a batched gulp are copied in up to kMaxChunks pieces so
+// that the transpose and dedispersion of one piece overlap the next copy.
+constexpr int kMaxChunks = 8;
+
 struct hd_pipeline_t {
   hd_params params;
   std::string output_dir;
@@ -56,7 +60,9 @@ struct hd_pipeline_t {
   bool cleaning = true;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with compute
   cudaEvent_t ev[10] = {};
+  cudaEvent_t chunk_ev[kMaxChunks] = {};
   float timing[8] = {};
 
   DevBuf fb_tf, fb_ft, fb_tf_clean;
@@ -81,7 +87,9 @@ struct hd_pipeline_t {
   ~hd_pipeline_t() {
     if (plan) dedisp_destroy_plan(plan);
     for (auto& e : ev) if (e) cudaEventDestroy(e);
+    for (auto& e : chunk_ev) if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (h_small) cudaFreeHost(h_small);
   }
 };
@@ -222,11 +230,13 @@ hd_error hd_create_pipeline(hd_pipeline* pipeline_, hd_params params) {
   cudaError_t ce = cudaSetDevice(params.gpu_id);
   if (ce != cudaSuccess) { delete pl; return cuda_err(ce); }
   pl->device = params.gpu_id;
-  if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&pl->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete pl;
     return HD_PRIOR_GPU_ERROR;
   }
   for (auto& e : pl->ev) cudaEventCreate(&e);
+  for (auto& e : pl->chunk_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   if (cudaMallocHost(&pl->h_small, 64 * sizeof(unsigned)) != cudaSuccess) {
     delete pl;
     return HD_MEM_ALLOC_FAILED;
@@ -320,37 +330,61 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
 
   cudaEventRecord(pl->ev[0], s);
   HD_TRY(cudaMemsetAsync(pl->plan->d_err, 0, sizeof(unsigned), s));
-  // ---- H2D ----------------------------------------------------------------
+  // ---- H2D, clean or channel-major copy, dedispersion ------------------------
   const size_t fb_bytes = nsamps * C;
-  HD_TRY(pl->fb_tf.ensure(U * fb_bytes));
-  for (size_t u = 0; u < U; u++)
-    HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes,
-                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-  cudaEventRecord(pl->ev[1], s);
-
-  // ---- clean + channel-major working copy ------------------------------------
   const size_t pitch = hdb::ft_pitch(pl->plan, nsamps);
   const size_t ft_unit = pitch * C;
-  HD_TRY(pl->fb_ft.ensure(U * ft_unit));
-  if (pl->cleaning) {
-    hd_error he = clean_units(pl, U, pl->fb_tf.as<uint8_t>(), nsamps, C, P.dt, P.baseline_length,
-                              P.rfi_tol, 64, nbeams, pl->fb_ft.as<uint8_t>(), pitch, nullptr);
-    if (he != HD_NO_ERROR) return he;
-  } else {
-    for (size_t u = 0; u < U; u++)
-      HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>() + u * fb_bytes, nsamps, (int)C,
-                                         pl->fb_ft.as<uint8_t>() + u * ft_unit, pitch, s));
-  }
-  cudaEventRecord(pl->ev[2], s);
-
-  // ---- dedispersion ----------------------------------------------------------
   const size_t dd_pitch = round_up(nc + 1, 4);
   const size_t NS = U * D;  // series of the batch, unit-major
+  HD_TRY(pl->fb_tf.ensure(U * fb_bytes));
+  HD_TRY(pl->fb_ft.ensure(U * ft_unit));
   HD_TRY(pl->dd.ensure(NS * dd_pitch * sizeof(float)));
   float* dd = pl->dd.as<float>();
-  de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>(), pitch, nsamps, dd, dd_pitch, s,
-                               U, ft_unit, D * dd_pitch);
-  if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (!on_device && !pl->cleaning && U > 1) {
+    // pipelined: copy chunk k on the copy stream while chunk k - 1 is
+    // transposed and dedispersed on the compute stream
+    const size_t nch = std::min<size_t>(U, kMaxChunks);
+    HD_TRY(cudaEventRecord(pl->ev[9], s));
+    HD_TRY(cudaStreamWaitEvent(pl->copy_stream, pl->ev[9], 0));
+    for (size_t k = 0; k < nch; k++) {
+      const size_t u0 = U * k / nch, u1 = U * (k + 1) / nch;
+      for (size_t u = u0; u < u1; u++)
+        HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes, kind,
+                               pl->copy_stream));
+      HD_TRY(cudaEventRecord(pl->chunk_ev[k], pl->copy_stream));
+    }
+    HD_TRY(cudaEventRecord(pl->ev[1], pl->copy_stream));
+    for (size_t k = 0; k < nch; k++) {
+      const size_t u0 = U * k / nch, u1 = U * (k + 1) / nch;
+      HD_TRY(cudaStreamWaitEvent(s, pl->chunk_ev[k], 0));
+      HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>() + u0 * fb_bytes, nsamps,
+                                         (int)C, pl->fb_ft.as<uint8_t>() + u0 * ft_unit, pitch,
+                                         s, u1 - u0, ft_unit));
+      if (k + 1 == nch) cudaEventRecord(pl->ev[2], s);
+      de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>() + u0 * ft_unit, pitch,
+                                   nsamps, dd + u0 * D * dd_pitch, dd_pitch, s, u1 - u0, ft_unit,
+                                   D * dd_pitch);
+      if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+    }
+  } else {
+    for (size_t u = 0; u < U; u++)
+      HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes, kind, s));
+    cudaEventRecord(pl->ev[1], s);
+    if (pl->cleaning) {
+      hd_error he = clean_units(pl, U, pl->fb_tf.as<uint8_t>(), nsamps, C, P.dt,
+                                P.baseline_length, P.rfi_tol, 64, nbeams,
+                                pl->fb_ft.as<uint8_t>(), pitch, nullptr);
+      if (he != HD_NO_ERROR) return he;
+    } else {
+      HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>(), nsamps, (int)C,
+                                         pl->fb_ft.as<uint8_t>(), pitch, s, U, ft_unit));
+    }
+    cudaEventRecord(pl->ev[2], s);
+    de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>(), pitch, nsamps, dd, dd_pitch,
+                                 s, U, ft_unit, D * dd_pitch);
+    if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+  }
   // the element after each series is read (never used) by the baseline stretch
   HD_TRY(cudaMemset2DAsync(dd + nc, dd_pitch * sizeof(float), 0, sizeof(float), NS, s));
   cudaEventRecord(pl->ev[3], s);

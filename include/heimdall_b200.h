@@ -248,7 +248,11 @@ hd_error hd_get_giants(hd_pipeline pipeline, hd_float* peaks, hd_size* inds, hd_
 
 /* Device time of the last hd_execute per stage, milliseconds (CUDA events):
  * [0] total, [1] clean, [2] dedisperse, [3] baseline+normalise+scan,
- * [4] boxcar+threshold, [5] giants, [6] cluster+merge, [7] host->device copy. */
+ * [4] boxcar+threshold, [5] giants, [6] cluster+merge, [7] host->device copy.
+ * When hd_execute_beams copies host filterbanks in pieces overlapped with
+ * their transpose and dedispersion (cleaning off), [7] ends when the last
+ * piece has landed, [1] then covers the last piece's transpose and [2] its
+ * dedispersion. */
 hd_error hd_get_timing(hd_pipeline pipeline, float* ms, int n);
 
 #ifdef __cplusplus

@@ -113,6 +113,15 @@ def test_execute_c0(hdb, oracle_lib, clean):
     assert len(cands) >= 3
 
 
+@pytest.mark.parametrize("bmax", [1, 2, 4, 8])
+def test_execute_small_boxcar(hdb, oracle_lib, bmax):
+    """Boxcar offsets below 4 or not a multiple of 4 take the scalar
+    threshold and block-RMS kernels; 8 is the smallest vector case."""
+    b = synth.make_c0()
+    cands = _compare(b.data, 1, synth.SEARCH_C0, False, boxcar_max=bmax)
+    assert len(cands) >= 1
+
+
 def test_execute_multibeam(hdb, oracle_lib):
     w = synth.Workload("mb_small", 64, 655.36e-6, 851.0, -0.390625, 8192, 4, 0.0, 600.0, 256,
                        False, "")
