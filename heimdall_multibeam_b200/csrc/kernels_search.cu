@@ -1608,13 +1608,28 @@ __global__ void k_giant_heads(WidthCtx ctx, HitBuffers hb, unsigned nhits, unsig
 }
 
 __global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, GiantBuffers gb) {
-  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nhits) return;
-  unsigned g = gb.gid[k] + gb.head[k] - 1u;  // inclusive count of heads - 1
-  // first maximum: larger value wins, ties to the smaller hit position
-  unsigned long long key = ((unsigned long long)float_key(hb.val[k]) << 32) |
-                           (unsigned long long)(0xFFFFFFFFu - (unsigned)k);
-  atomicMax(&gb.key[g], key);
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = k < nhits;
+  const int lane = threadIdx.x & 31;
+  unsigned g = 0xFFFFFFFFu;
+  unsigned long long key = 0;
+  if (live) {
+    g = gb.gid[k] + gb.head[k] - 1u;  // inclusive count of heads - 1
+    // first maximum: larger value wins, ties to the smaller hit position
+    key = ((unsigned long long)float_key(hb.val[k]) << 32) |
+          (unsigned long long)(0xFFFFFFFFu - (unsigned)k);
+  }
+  // a giant's hits are consecutive: reduce each run inside the warp, then one
+  // atomic per run (max is order-independent, so the result is the same)
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned long long ok = __shfl_down_sync(0xffffffffu, key, off);
+    const unsigned og = __shfl_down_sync(0xffffffffu, g, off);
+    if (lane + off < 32 && og == g && ok > key) key = ok;
+  }
+  const unsigned gp = __shfl_up_sync(0xffffffffu, g, 1);
+  if (!live) return;
+  if (lane == 0 || gp != g) atomicMax(&gb.key[g], key);
   unsigned sw = hb.sw[k];
   const WidthInfo& w = ctx.winfo[sw % ctx.nw];
   bool is_head = gb.head[k] != 0;
@@ -1684,7 +1699,7 @@ __global__ void k_cluster_init(int* label, int n) {
 // CL_JCHUNK earlier giants inside their DM window.
 __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantBuffers gb,
                                                            unsigned* changed) {
-  __shared__ unsigned long long s_samp[CL_TILE];
+  __shared__ unsigned s_samp[CL_TILE], s_beam[CL_TILE];
   __shared__ int s_f[CL_TILE], s_dm[CL_TILE], s_lab[CL_TILE];
   const int i_first = blockIdx.x * CL_TILE;
   const int i = i_first + threadIdx.x;
@@ -1701,21 +1716,29 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
   const int j_begin = lo + (int)blockIdx.y * CL_JCHUNK;
   if (j_begin > i_last) return;  // uniform: this chunk lies past the tile
   const int j_end = min(j_begin + CL_JCHUNK, i_last + 1);
-  unsigned long long si = 0, bi = 0;
+  // sample indices fit 31 bits (checked by the host); the test below is
+  // are_coincident_beam (are_coincident.cuh:47-68): same beam, time within
+  // time_tol x the wider boxcar (a power of two), filter and DM within tolerance.
+  // A giant's beam is computed once, when it is staged.
+  unsigned si = 0, bi = 0;
   int fi = 0, di = 0, best = 0x7FFFFFFF;
   if (i < a.ngiants) {
-    si = gb.ind[i];
-    bi = si / a.nsamps_beam;
+    si = (unsigned)gb.ind[i];
+    bi = (unsigned)(gb.ind[i] / a.nsamps_beam);
     fi = gb.filter[i];
     di = gb.dm[i];
     best = gb.label[i];
   }
   const int start_best = best;
+  const unsigned ftol = (unsigned)min(a.filter_tol, 0x7FFFFFFFull);
+  const unsigned dtol = (unsigned)min(a.dm_tol, 0x7FFFFFFFull);
   for (int j0 = j_begin; j0 < j_end; j0 += CL_TILE) {
     const int j = j0 + threadIdx.x;
     __syncthreads();
     if (j < j_end) {
-      s_samp[threadIdx.x] = gb.ind[j];
+      const unsigned long long sj = gb.ind[j];
+      s_samp[threadIdx.x] = (unsigned)sj;
+      s_beam[threadIdx.x] = (unsigned)(sj / a.nsamps_beam);
       s_f[threadIdx.x] = gb.filter[j];
       s_dm[threadIdx.x] = gb.dm[j];
       s_lab[threadIdx.x] = *((volatile int*)&gb.label[j]);
@@ -1724,14 +1747,13 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
     if (i < a.ngiants) {
       const int jn = min(min(CL_TILE, j_end - j0), i - j0);  // only j < i
       for (int jj = 0; jj < jn; jj++) {
+        const unsigned sj = s_samp[jj];
         const int fj = s_f[jj];
-        const int wmax = max(1 << fi, 1 << fj);
-        const unsigned long long tt = a.time_tol * (unsigned long long)wmax;
-        const unsigned long long sj = s_samp[jj];
-        const bool coinc = (sj / a.nsamps_beam) == bi &&
-                           (unsigned long long)abs((int)sj - (int)si) <= tt &&
-                           (unsigned long long)abs(fj - fi) <= a.filter_tol &&
-                           (unsigned long long)abs(s_dm[jj] - di) <= a.dm_tol;
+        const unsigned dt = sj > si ? sj - si : si - sj;
+        const unsigned long long tt = a.time_tol << max(fi, fj);
+        const bool coinc = s_beam[jj] == bi && (unsigned long long)dt <= tt &&
+                           (unsigned)abs(fj - fi) <= ftol &&
+                           (unsigned)abs(s_dm[jj] - di) <= dtol;
         if (coinc && s_lab[jj] < best) best = s_lab[jj];
       }
     }

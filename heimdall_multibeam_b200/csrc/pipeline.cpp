@@ -294,6 +294,8 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   const size_t C = P.nchans;
   if (C % 4 != 0 || nbeams == 0) return HD_INVALID_STRIDE;
   if (P.min_tscrunch_width < 2) return HD_INVALID_STRIDE;
+  // sample, hit and giant indices are kept in 31/32 bits on the device
+  if (nsamps >= 0x7FFFFFFFull) return HD_INVALID_STRIDE;
   if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
   cudaStream_t s = pl->stream;
   pl->cands.clear();
