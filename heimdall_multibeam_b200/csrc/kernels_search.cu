@@ -366,7 +366,7 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // The left-to-right float sum of a series is one dependent chain (~4 cycles
 // per sample), so the block is split by role:
 //   warp 0       the chains: lane l owns series l of the block and runs its
-//                chain over one stage of SC_CH samples in shared memory;
+//                chain over one stage of its row in shared memory;
 //   warps 1..np  a stage's rows arrive by TMA bulk copies requested SC_DEPTH
 //                stages ahead; these warps divide them in place by their
 //                beam's RMS, and write them out once the chain warp has
@@ -376,8 +376,6 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
 // step k - 1).  One block barrier ends each step.
 // ===========================================================================
-constexpr int SC_CH = 128;           // samples per series per stage
-constexpr int SC_ROW = SC_CH + 4;    // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
 constexpr int SC_DEPTH = 5;          // stages in flight ahead of the one being normalised
 constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
 constexpr int SC_MAXSER = 32;
@@ -401,28 +399,35 @@ __device__ __forceinline__ float div_rn_by(float a, float b, float y) {
   return __fdiv_rn(a, b);
 }
 
-size_t scan_smem_bytes(int ser, int nbeams) {
-  size_t b = 128 + (size_t)SC_NB * ser * SC_ROW * sizeof(float);
+size_t scan_smem_bytes(int ser, int nbeams, int ch) {
+  size_t b = 128 + (size_t)SC_NB * ser * (ch + 4) * sizeof(float);
   if ((size_t)ser * nbeams <= SC_MAXRMS) b += 2 * (size_t)ser * nbeams * sizeof(float);
   return b;
 }
 
+// CH samples per series per stage (128, 256 or 512): blocks of few series use
+// long stages, so the per-stage fixed cost (barrier, copy issue, waits) is
+// spread over more samples and each producer lane has CH / 128 independent
+// float4 values in flight.
+template <int CH>
 __global__ void __launch_bounds__(256) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
     float* norm_out, int ser_per_block, unsigned* err) {
+  constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
+  constexpr int QN = CH / 128; // float4 per lane per row
   extern __shared__ __align__(128) float sc_smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(sc_smem);  // [SC_NB], first 128 bytes
   const int S = ser_per_block;
-  float* rows = sc_smem + 32;                             // [SC_NB][S][SC_ROW]
-  float* srms = rows + (size_t)SC_NB * S * SC_ROW;        // [S][nbeams]
+  float* rows = sc_smem + 32;                             // [SC_NB][S][ROW]
+  float* srms = rows + (size_t)SC_NB * S * ROW;           // [S][nbeams]
   float* sy = srms + S * nbeams;                          // reciprocals
   const int s0 = blockIdx.x * S;
   const int nb = min(S, nser - s0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int np = (int)(blockDim.x >> 5) - 1;
   const bool rms_smem = nb * nbeams <= SC_MAXRMS;
-  const unsigned nstage = len / SC_CH + 1;  // outputs 0..len
+  const unsigned nstage = len / CH + 1;     // outputs 0..len
   const unsigned len4 = (len + 3u) & ~3u;   // copies round up to 16 bytes (inside the row pitch)
 
   if (threadIdx.x == 0) {
@@ -441,8 +446,8 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
   // completes its barrier phase with a plain arrival
   auto request = [&](unsigned st) {
     uint64_t* bar = &full[st % SC_NB];
-    const unsigned base = st * SC_CH;
-    const unsigned end = min(base + (unsigned)SC_CH, len4);
+    const unsigned base = st * CH;
+    const unsigned end = min(base + (unsigned)CH, len4);
     const unsigned bytes = end > base ? (end - base) * 4u : 0u;
     if (bytes == 0) {
       if (lane == 0) mbar_arrive(bar);
@@ -453,7 +458,7 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
     // the buffer was last written by this block's threads (generic proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (lane < nb)
-      bulk_g2s(rows + ((size_t)(st % SC_NB) * S + lane) * SC_ROW,
+      bulk_g2s(rows + ((size_t)(st % SC_NB) * S + lane) * ROW,
                data + (size_t)(s0 + lane) * pitch + base, bytes, bar);
   };
   if (warp == 1)
@@ -465,9 +470,9 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
     if (warp == 0) {
       // ---- the chains: stage k - 1 ----
       if (k >= 1 && k - 1 < nstage && lane < nb) {
-        float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * SC_ROW;
+        float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * ROW;
 #pragma unroll 8
-        for (int e = 0; e < SC_CH; e += 4) {
+        for (int e = 0; e < CH; e += 4) {
           const float4 v = *reinterpret_cast<const float4*>(row + e);
           float4 o;
           o.x = sum; sum = __fadd_rn(sum, v.x);
@@ -483,17 +488,22 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       // ---- store stage k - 2 ----
       if (k >= 2 && k - 2 < nstage) {
         const unsigned st = k - 2;
-        const unsigned i = st * SC_CH + 4u * lane;
         for (int sl = p; sl < nb; sl += np) {
-          const float4 v =
-              *reinterpret_cast<const float4*>(rows + ((size_t)(st % SC_NB) * S + sl) * SC_ROW + 4 * lane);
-          float* o = scan + (size_t)(s0 + sl) * scan_pitch + i;
-          if (i + 3 <= len) {
-            *reinterpret_cast<float4*>(o) = v;
-          } else {
-            if (i <= len) o[0] = v.x;
-            if (i + 1 <= len) o[1] = v.y;
-            if (i + 2 <= len) o[2] = v.z;
+          const float* rrow = rows + ((size_t)(st % SC_NB) * S + sl) * ROW;
+          float* orow = scan + (size_t)(s0 + sl) * scan_pitch;
+#pragma unroll
+          for (int q = 0; q < QN; q++) {
+            const unsigned e = 4u * lane + 128u * q;
+            const unsigned i = st * CH + e;
+            const float4 v = *reinterpret_cast<const float4*>(rrow + e);
+            float* o = orow + i;
+            if (i + 3 <= len) {
+              *reinterpret_cast<float4*>(o) = v;
+            } else {
+              if (i <= len) o[0] = v.x;
+              if (i + 1 <= len) o[1] = v.y;
+              if (i + 2 <= len) o[2] = v.z;
+            }
           }
         }
       }
@@ -503,58 +513,67 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
           if (!failed && err && lane == 0) atomicOr(err, 2u);
           failed = true;
         }
-        const unsigned base = k * SC_CH;
-        const unsigned i = base + 4u * lane;
+        const unsigned base = k * CH;
         unsigned b0 = base / stride;
         if (b0 > (unsigned)nbeams - 1) b0 = (unsigned)nbeams - 1;
         const unsigned bend = (b0 + 1) * stride;
         // common case: the stage lies inside the data and inside one beam, so
         // one divisor (and its reciprocal) serves the whole row
-        const bool uniform = rms_smem && base + SC_CH <= len && stride >= (unsigned)SC_CH &&
-                             (b0 + 1 >= (unsigned)nbeams || bend >= base + SC_CH);
+        const bool uniform = rms_smem && base + CH <= len && stride >= (unsigned)CH &&
+                             (b0 + 1 >= (unsigned)nbeams || bend >= base + CH);
         if (uniform) {
           for (int sl = p; sl < nb; sl += np) {
-            float4* cell = reinterpret_cast<float4*>(rows + ((size_t)(k % SC_NB) * S + sl) * SC_ROW +
-                                                     4 * lane);
-            const int q = sl * nbeams + (int)b0;
-            const float rb = srms[q], y = sy[q];
-            float4 x = *cell;
-            x.x = div_rn_by(x.x, rb, y);
-            x.y = div_rn_by(x.y, rb, y);
-            x.z = div_rn_by(x.z, rb, y);
-            x.w = div_rn_by(x.w, rb, y);
-            *cell = x;
-            if (norm_out)
-              *reinterpret_cast<float4*>(norm_out + (size_t)(s0 + sl) * pitch + i) = x;
-          }
-        } else
-        for (int sl = p; sl < nb; sl += np) {
-          float4* cell =
-              reinterpret_cast<float4*>(rows + ((size_t)(k % SC_NB) * S + sl) * SC_ROW + 4 * lane);
-          float x[4];
-          *reinterpret_cast<float4*>(x) = *cell;
+            float* crow = rows + ((size_t)(k % SC_NB) * S + sl) * ROW;
+            const int q0 = sl * nbeams + (int)b0;
+            const float rb = srms[q0], y = sy[q0];
+            float4 x[QN];
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const unsigned ij = i + j;
-            if (ij >= len) { x[j] = 0.f; continue; }
-            unsigned b;
-            if (stride >= (unsigned)SC_CH) b = (ij >= bend && b0 + 1 < (unsigned)nbeams) ? b0 + 1 : b0;
-            else b = min(ij / stride, (unsigned)nbeams - 1);
-            if (rms_smem) {
-              const int q = sl * nbeams + (int)b;
-              x[j] = div_rn_by(x[j], srms[q], sy[q]);
-            } else {
-              x[j] = __fdiv_rn(x[j], rms[(size_t)(s0 + sl) * nbeams + b]);
+            for (int q = 0; q < QN; q++) x[q] = *reinterpret_cast<const float4*>(crow + 4 * lane + 128 * q);
+#pragma unroll
+            for (int q = 0; q < QN; q++) {
+              x[q].x = div_rn_by(x[q].x, rb, y);
+              x[q].y = div_rn_by(x[q].y, rb, y);
+              x[q].z = div_rn_by(x[q].z, rb, y);
+              x[q].w = div_rn_by(x[q].w, rb, y);
+              *reinterpret_cast<float4*>(crow + 4 * lane + 128 * q) = x[q];
+              if (norm_out)
+                *reinterpret_cast<float4*>(norm_out + (size_t)(s0 + sl) * pitch + base + 4 * lane +
+                                           128 * q) = x[q];
             }
           }
-          *cell = *reinterpret_cast<float4*>(x);
-          if (norm_out) {
-            float* o = norm_out + (size_t)(s0 + sl) * pitch + i;
-            if (i + 3 < len) {
-              *reinterpret_cast<float4*>(o) = *reinterpret_cast<float4*>(x);
-            } else {
-              for (int j = 0; j < 4; j++)
-                if (i + j < len) o[j] = x[j];
+        } else {
+          for (int sl = p; sl < nb; sl += np) {
+#pragma unroll
+            for (int q = 0; q < QN; q++) {
+              const unsigned i = base + 4u * lane + 128u * q;
+              float4* cell = reinterpret_cast<float4*>(rows + ((size_t)(k % SC_NB) * S + sl) * ROW +
+                                                       4 * lane + 128 * q);
+              float x[4];
+              *reinterpret_cast<float4*>(x) = *cell;
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                const unsigned ij = i + j;
+                if (ij >= len) { x[j] = 0.f; continue; }
+                unsigned b;
+                if (stride >= (unsigned)CH) b = (ij >= bend && b0 + 1 < (unsigned)nbeams) ? b0 + 1 : b0;
+                else b = min(ij / stride, (unsigned)nbeams - 1);
+                if (rms_smem) {
+                  const int qq = sl * nbeams + (int)b;
+                  x[j] = div_rn_by(x[j], srms[qq], sy[qq]);
+                } else {
+                  x[j] = __fdiv_rn(x[j], rms[(size_t)(s0 + sl) * nbeams + b]);
+                }
+              }
+              *cell = *reinterpret_cast<float4*>(x);
+              if (norm_out) {
+                float* o = norm_out + (size_t)(s0 + sl) * pitch + i;
+                if (i + 3 < len) {
+                  *reinterpret_cast<float4*>(o) = *reinterpret_cast<float4*>(x);
+                } else {
+                  for (int j = 0; j < 4; j++)
+                    if (i + j < len) o[j] = x[j];
+                }
+              }
             }
           }
         }
@@ -569,6 +588,21 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       mbar_wait(&full[st % SC_NB], (st / SC_NB) & 1u, SC_WAIT_LIMIT);
 }
 
+template <int CH>
+static cudaError_t launch_scan(const SeriesBatch& sb, const float* rms, float* scan,
+                               size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
+                               int ser) {
+  const int np = ser < 7 ? ser : 7;
+  const size_t smem = scan_smem_bytes(ser, sb.nbeams, CH);
+  cudaError_t e = cudaFuncSetAttribute(k_normalise_scan<CH>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_normalise_scan<CH><<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
+      sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
+      scan_pitch, norm_out, ser, err); note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
                            size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err) {
   if (sb.len >= 0xFFFFFF00u || sb.pitch % 4 || scan_pitch % 4 || sb.stride == 0 ||
@@ -580,15 +614,9 @@ cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
   // series per block: enough blocks to cover the SMs twice where possible
   int ser = SC_MAXSER;
   while (ser > 1 && (sb.nser + ser - 1) / ser < 296) ser /= 2;
-  const int np = ser < 7 ? ser : 7;
-  const size_t smem = scan_smem_bytes(ser, sb.nbeams);
-  cudaError_t e = cudaFuncSetAttribute(k_normalise_scan,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k_normalise_scan<<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
-      sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
-      scan_pitch, norm_out, ser, err); note_launch();
-  return cudaGetLastError();
+  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
+  if (ser <= 8) return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
+  return launch_scan<128>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
 }
 
 // ===========================================================================
