@@ -361,7 +361,7 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // ===========================================================================
 // Normalise + exclusive prefix sum with the sequential association of the
 // reference's scan (Thrust's sequential exclusive_scan: out[0] = 0,
-// out[k+1] = out[k] + in[k]), for up to SC_MAXSER series per block.
+// out[k+1] = out[k] + in[k]), for up to 8 series per block.
 //
 // The left-to-right float sum of a series is one dependent chain (~4 cycles
 // per sample), so the block is split by role:
@@ -378,7 +378,6 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // ===========================================================================
 constexpr int SC_DEPTH = 5;          // stages in flight ahead of the one being normalised
 constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
-constexpr int SC_MAXSER = 32;
 constexpr int SC_MAXRMS = 2048;      // series x beams whose RMS stays in shared memory
 constexpr uint32_t SC_WAIT_LIMIT = 1u << 22;
 
@@ -611,12 +610,13 @@ cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
       (norm_out && (reinterpret_cast<uintptr_t>(norm_out) & 15)))
     return cudaErrorInvalidValue;
   if (sb.nser <= 0) return cudaSuccess;
-  // series per block: enough blocks to cover the SMs twice where possible
-  int ser = SC_MAXSER;
+  // series per block: enough blocks to cover the SMs twice where possible, at
+  // most 8 (measured: 8 series with 256-sample stages beat 16 with 128 on the
+  // multibeam gulp, and 4 with 512 beat 2 with 512 on the survey gulp)
+  int ser = 8;
   while (ser > 1 && (sb.nser + ser - 1) / ser < 296) ser /= 2;
   if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
-  if (ser <= 8) return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
-  return launch_scan<128>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
+  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
 }
 
 // ===========================================================================
@@ -806,42 +806,75 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
     out[(ser * nwb + wl) * out_pitch + g] = cur[wl * pitch_cur];
 }
 
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
+
+// Block (x, y): groups [x * gpb, (x + 1) * gpb) of series y.  The next
+// group's window is copied into the other half of a double buffer (cp.async)
+// while the current group's medians are computed.
 __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ctx, int w0,
                                                                      int nwb, int m, int win,
                                                                      float* __restrict__ out,
-                                                                     size_t out_pitch) {
+                                                                     size_t out_pitch,
+                                                                     int ngroups, int gpb) {
   extern __shared__ __align__(16) float dyn[];
   const int win4 = (win + 3) & ~3;
-  float* tile = dyn;                     // win floats
+  float* tiles = dyn;                    // [2][win4]
   const int n1 = (int)pow5(m - 1);       // level-1 medians per width
   const int n1p = (n1 + 3) & ~3;         // row pitch: 16-byte aligned rows
-  float* la = dyn + win4;                // [nwb][n1p]
+  float* la = dyn + 2 * win4;            // [nwb][n1p]
   float* lb = la + nwb * n1p;            // [nwb][n1 / 5]
   const size_t ser = blockIdx.y;
-  const size_t g = blockIdx.x;
+  const int g_begin = blockIdx.x * gpb;
+  const int g_end = min(g_begin + gpb, ngroups);
   const WidthInfo& w_first = ctx.winfo[w0];
   const float* sc = ctx.scan + ser * ctx.scan_pitch;
   const float delta = (float)(ctx.stride - w_first.bn);
   const size_t gsz = pow5(m);
-  const size_t q0 = g * gsz;
-  const size_t i_first = reblock_index((unsigned)q0 / w_first.bn, delta, (unsigned)q0);
-  const size_t q1 = q0 + gsz - 1;
-  const size_t i_last = reblock_index((unsigned)q1 / w_first.bn, delta, (unsigned)q1);
   const int offset = ctx.offset;
-  const size_t span = (i_last - i_first) + 2 * (size_t)offset + 2;
-  // the launcher guarantees a contiguous group whose window fits (span <= win)
-  if (i_last - i_first != gsz - 1 || span > (size_t)win) return;
-  for (size_t k = threadIdx.x; k < span; k += blockDim.x) tile[k] = sc[i_first + k];
+  // the launcher guarantees contiguous groups (one beam) whose window fits
+  auto first_of = [&](int g) {
+    const size_t q0 = (size_t)g * gsz;
+    return reblock_index((unsigned)q0 / w_first.bn, delta, (unsigned)q0);
+  };
+  const size_t span = gsz - 1 + 2 * (size_t)offset + 2;
+  auto prefetch = [&](int g, float* tile) {
+    const float* src = sc + first_of(g);
+    for (size_t k = threadIdx.x; k < span; k += blockDim.x) cp_async4(tile + k, src + k);
+    cp_async_commit();
+  };
   // A prefix sum that is finite at its end is finite everywhere (a non-finite
   // term would stay non-finite), so every boxcar value is NaN-free and the
   // min/max median network selects the same values as the reference's.
   const float last = sc[ctx.scan_len - 1];
   const bool finite = fabsf(last) <= 3.402823466e38f;
-  __syncthreads();
-  if (finite)
-    brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
-  else
-    brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+  if (g_begin >= g_end || span > (size_t)win) return;
+  prefetch(g_begin, tiles);
+  for (int g = g_begin; g < g_end; g++) {
+    float* tile = tiles + (size_t)((g - g_begin) & 1) * win4;
+    // the previous group's levels (and final reads of la/lb) are finished
+    __syncthreads();
+    if (g + 1 < g_end) {
+      prefetch(g + 1, tiles + (size_t)((g + 1 - g_begin) & 1) * win4);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    if (finite)
+      brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+    else
+      brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+  }
 }
 
 __global__ void k_block_rms_final(WidthCtx ctx, int w0, int nwb, const float* __restrict__ lev,
@@ -900,13 +933,17 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
     const size_t win = pow5(m1) + 2 * (size_t)ctx.offset + 2;
     const size_t n1 = pow5(m1 - 1);
     const size_t smem =
-        (((win + 3) & ~(size_t)3) + nwb * ((n1 + 3) & ~(size_t)3) + nwb * (n1 / 5 + 1)) *
+        (2 * ((win + 3) & ~(size_t)3) + nwb * ((n1 + 3) & ~(size_t)3) + nwb * (n1 / 5 + 1)) *
         sizeof(float);
     if (smem <= 200 * 1024) {
       cudaFuncSetAttribute(k_block_rms_pass1_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-      k_block_rms_pass1_vec<<<dim3((unsigned)ng1, ctx.nser), BRV_THREADS, smem, s>>>(
-          ctx, w_begin, nwb, m1, (int)win, ws.a, ng1); note_launch();
+      // about 8 consecutive groups per block, spread evenly
+      const size_t nblk_x = (ng1 + 7) / 8;
+      const size_t gpb = (ng1 + nblk_x - 1) / nblk_x;
+      k_block_rms_pass1_vec<<<dim3((unsigned)((ng1 + gpb - 1) / gpb), ctx.nser), BRV_THREADS,
+                              smem, s>>>(ctx, w_begin, nwb, m1, (int)win, ws.a, ng1, (int)ng1,
+                                         (int)gpb); note_launch();
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       float* fin;
       size_t fin_pitch, fin_count;
