@@ -810,6 +810,10 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_addr(dst)), "l"(src)
                : "memory");
 }
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -1228,6 +1232,47 @@ struct VecTile {
   unsigned valid;  // bit g*4+q: sample (g, q) of this thread is in a searched window
 };
 
+// In-window bits of this thread's 8 samples of the tile at i0
+// (find_giants.cu:47-60): i < n and (i mod beam stride) < bn, the same for
+// every unscrunched width.  *all is set when the whole tile is inside one
+// beam's searched window (uniform across the block).
+__device__ __forceinline__ unsigned vec_valid(const WidthCtx& ctx, size_t i0, bool* all) {
+  const WidthInfo& w = ctx.winfo[0];
+  const unsigned stride = (unsigned)ctx.stride;
+  const unsigned ui0 = (unsigned)i0;
+  if (ui0 + HIT_TILE <= w.n && (ui0 % stride) + HIT_TILE <= w.bn) {
+    *all = true;
+    return 0xFFu;
+  }
+  *all = false;
+  unsigned valid = 0;
+#pragma unroll
+  for (int g = 0; g < 2; g++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const unsigned i = ui0 + 1024u * g + 4u * threadIdx.x + q;
+      if (i < w.n && (i % stride) < w.bn) valid |= 1u << (g * 4 + q);
+    }
+  return valid;
+}
+
+// Asynchronous copy of the window of the tile at i0 (span4 floats, zero past
+// slen) into shared memory; completes with cp_async_wait + a barrier.
+__device__ __forceinline__ void vec_prefetch(const float* sc, size_t i0, float* tile,
+                                             size_t span4, size_t slen) {
+  for (size_t k = 4 * threadIdx.x; k < span4; k += 4 * blockDim.x) {
+    if (i0 + k + 3 < slen) {
+      cp_async16(tile + k, sc + i0 + k);
+    } else {
+      tile[k] = (i0 + k < slen) ? sc[i0 + k] : 0.f;
+      tile[k + 1] = (i0 + k + 1 < slen) ? sc[i0 + k + 1] : 0.f;
+      tile[k + 2] = (i0 + k + 2 < slen) ? sc[i0 + k + 2] : 0.f;
+      tile[k + 3] = 0.f;
+    }
+  }
+  cp_async_commit();
+}
+
 __device__ __forceinline__ VecTile vec_stage(const WidthCtx& ctx, const float* sc, size_t i0,
                                              float* tile, size_t span4, size_t slen) {
   for (size_t k = 4 * threadIdx.x; k < span4; k += 4 * blockDim.x) {
@@ -1355,17 +1400,21 @@ __device__ __forceinline__ void count_vec_body(const float* tile, int offset, in
   }
 }
 
+// Block (x, y): tiles [x * tpb, (x + 1) * tpb) of series y; the next tile's
+// window is copied (cp.async, double buffer) while the current one is counted.
 __global__ void __launch_bounds__(HIT_THREADS) k_count_hits_vec(WidthCtx ctx, HitBuffers hb,
                                                                 int nw1, size_t slen,
-                                                                size_t span4) {
-  extern __shared__ __align__(16) float tile[];
+                                                                size_t span4, int tpb) {
+  extern __shared__ __align__(16) float tiles[];  // [2][span4]
   __shared__ int s_ahead[VH_MAXW], s_behind[VH_MAXW];
   __shared__ float s_norm[VH_MAXW], s_dmin[VH_MAXW];
   __shared__ int s_mul;
   __shared__ unsigned red[HIT_THREADS / 32][VH_MAXW / 2];
   const size_t ser = blockIdx.y;
-  const unsigned t = blockIdx.x;
+  const unsigned t_begin = blockIdx.x * (unsigned)tpb;
+  const unsigned t_end = min(t_begin + (unsigned)tpb, hb.ntiles);
   const float thresh = ctx.thresh;
+  const float* sc = ctx.scan + ser * ctx.scan_pitch;
   if (threadIdx.x == 0) s_mul = 0;
   __syncthreads();
   if (threadIdx.x < (unsigned)nw1) {
@@ -1377,42 +1426,55 @@ __global__ void __launch_bounds__(HIT_THREADS) k_count_hits_vec(WidthCtx ctx, Hi
     if (!hit_bound(nrm, thresh, &dm)) atomicOr(&s_mul, 1);
     s_dmin[threadIdx.x] = dm;
   }
-  const size_t i0 = (size_t)t * HIT_TILE;
-  const VecTile vt = vec_stage(ctx, ctx.scan + ser * ctx.scan_pitch, i0, tile, span4, slen);
+  if (t_begin >= t_end) return;  // uniform
   const int offset = ctx.offset;
-  unsigned cnt[VH_MAXW / 2];
-#pragma unroll
-  for (int p = 0; p < VH_MAXW / 2; p++) cnt[p] = 0;
-  // both flags are uniform across the block
-  const bool allv = vt.valid == 0xFFu && ((unsigned)i0 % (unsigned)ctx.stride) + HIT_TILE <=
-                                            ctx.winfo[0].bn &&
-                    (unsigned)i0 + HIT_TILE <= ctx.winfo[0].n;
-  if (s_mul) {
-    if (allv) count_vec_body<true, true>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
-    else count_vec_body<false, true>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
-  } else {
-    if (allv) count_vec_body<true, false>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
-    else count_vec_body<false, false>(tile, offset, nw1, vt.valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
-  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  vec_prefetch(sc, (size_t)t_begin * HIT_TILE, tiles, span4, slen);
+  for (unsigned t = t_begin; t < t_end; t++) {
+    float* tile = tiles + (size_t)((t - t_begin) & 1) * span4;
+    // the previous tile is counted and its reduction slots are read
+    __syncthreads();
+    if (t + 1 < t_end) {
+      vec_prefetch(sc, (size_t)(t + 1) * HIT_TILE, tiles + (size_t)((t + 1 - t_begin) & 1) * span4,
+                   span4, slen);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const size_t i0 = (size_t)t * HIT_TILE;
+    bool allv;
+    const unsigned valid = vec_valid(ctx, i0, &allv);
+    unsigned cnt[VH_MAXW / 2];
 #pragma unroll
-  for (int p = 0; p < VH_MAXW / 2; p++) {
-    if (2 * p >= nw1) break;
-    unsigned c = cnt[p];
+    for (int p = 0; p < VH_MAXW / 2; p++) cnt[p] = 0;
+    if (s_mul) {
+      if (allv) count_vec_body<true, true>(tile, offset, nw1, valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+      else count_vec_body<false, true>(tile, offset, nw1, valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+    } else {
+      if (allv) count_vec_body<true, false>(tile, offset, nw1, valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+      else count_vec_body<false, false>(tile, offset, nw1, valid, s_ahead, s_behind, s_norm, s_dmin, thresh, cnt);
+    }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) red[warp][p] = c;
-  }
-  __syncthreads();
-  if (threadIdx.x < (unsigned)nw1) {
-    const int wi = threadIdx.x;
-    unsigned tot = 0;
-    for (int k = 0; k < HIT_THREADS / 32; k++) tot += (red[k][wi >> 1] >> (16 * (wi & 1))) & 0xFFFFu;
-    const size_t sw = ser * ctx.nw + wi;
-    hb.tile_cnt[sw * hb.ntiles + t] = tot;
-    if (tot) atomicAdd(&hb.sw_cnt[sw], tot);
+    for (int p = 0; p < VH_MAXW / 2; p++) {
+      if (2 * p >= nw1) break;
+      unsigned c = cnt[p];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == 0) red[warp][p] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)nw1) {
+      const int wi = threadIdx.x;
+      unsigned tot = 0;
+      for (int k = 0; k < HIT_THREADS / 32; k++) tot += (red[k][wi >> 1] >> (16 * (wi & 1))) & 0xFFFFu;
+      const size_t sw = ser * ctx.nw + wi;
+      hb.tile_cnt[sw * hb.ntiles + t] = tot;
+      if (tot) atomicAdd(&hb.sw_cnt[sw], tot);
+    }
   }
 }
+
 
 __global__ void __launch_bounds__(HIT_THREADS) k_write_hits_vec(WidthCtx ctx, HitBuffers hb,
                                                                 int nw1, size_t slen,
@@ -1517,11 +1579,14 @@ cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cud
   const size_t smem = (HIT_TILE + 2 * (size_t)ctx.offset + 2) * sizeof(float);
   const size_t span4 = (HIT_TILE + 2 * (size_t)ctx.offset + 2 + 3) & ~(size_t)3;
   const size_t slen = ctx.scan_len;
-  if (vec_hits_ok(ctx, nw1) && span4 * sizeof(float) <= 200 * 1024) {
+  if (vec_hits_ok(ctx, nw1) && 2 * span4 * sizeof(float) <= 200 * 1024) {
     cudaFuncSetAttribute(k_count_hits_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(span4 * sizeof(float)));
-    k_count_hits_vec<<<dim3(ntiles, ctx.nser), HIT_THREADS, span4 * sizeof(float), s>>>(
-        ctx, hb, nw1, slen, span4); note_launch();
+                         (int)(2 * span4 * sizeof(float)));
+    // about 8 consecutive tiles per block, spread evenly
+    const unsigned nbx = (ntiles + 7) / 8;
+    const unsigned tpb = (ntiles + nbx - 1) / nbx;
+    k_count_hits_vec<<<dim3((ntiles + tpb - 1) / tpb, ctx.nser), HIT_THREADS,
+                       2 * span4 * sizeof(float), s>>>(ctx, hb, nw1, slen, span4, (int)tpb); note_launch();
   } else if (nw1 > 0 && smem <= 200 * 1024) {
     cudaFuncSetAttribute(k_count_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_count_hits_multi<<<dim3(ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
