@@ -52,8 +52,6 @@ UNIT = "beam-s/s"
 TRAFFIC = {
     "multibeam_36x_c320_n32768": ("k_dedisp_multibeam_36x_c320_n32768.md",
                                   "traffic_bytes_per_launch:"),
-    "plain_c1024_n262144_rfi": ("k_dedisp_c1024_n131072.md",
-                                "traffic_bytes_per_launch_full_size:"),
 }
 
 
