@@ -138,6 +138,19 @@ SYMBOLS = {
     "hd_get_candidates": (C.c_int, [_P, _P, _SZP]),
     "hd_get_giants": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _SZP]),
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
+    "hd_extract_patches": (C.c_int, [_P, _FP, _FP, _SZP]),
+    "hd_classifier_param_count": (_SZ, []),
+    "hd_classifier_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_ulonglong]),
+    "hd_classifier_destroy": (None, [_P]),
+    "hd_classifier_get_params": (C.c_int, [_P, _FP, _SZ]),
+    "hd_classifier_set_params": (C.c_int, [_P, _FP, _SZ]),
+    "hd_classifier_gradients": (C.c_int, [_P, _FP, _FP, C.POINTER(C.c_int), _SZ, _FP, _FP]),
+    "hd_classifier_train": (C.c_int, [_P, _FP, _FP, C.POINTER(C.c_int), _SZ, C.c_int, C.c_int,
+                                      C.c_float, C.c_ulonglong, _FP]),
+    "hd_classifier_score": (C.c_int, [_P, _FP, _FP, _SZ, _FP]),
+    "hd_bf16_gemm": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, C.c_longlong, C.c_longlong, _P,
+                               C.c_longlong, C.c_longlong, _FP, C.c_longlong, C.c_longlong,
+                               C.c_int, C.c_int]),
     "dedisp_create_plan": (C.c_int, [C.POINTER(_P), _SZ, C.c_float, C.c_float, C.c_float]),
     "dedisp_destroy_plan": (None, [_P]),
     "dedisp_set_dm_list": (C.c_int, [_P, _FP, _SZ]),
@@ -349,6 +362,20 @@ class Pipeline:
                                 g["labels"].ctypes.data, C.byref(n))
         return g
 
+    def patches(self) -> Tuple[np.ndarray, np.ndarray]:
+        """hd_extract_patches: (dm_time [n, 64, 64], freq_time [n, 64, 256]) of
+        the last execute's candidates, in candidates() order."""
+        n = C.c_size_t(0)
+        lib().hd_extract_patches(self._p, None, None, C.byref(n))
+        dm = np.zeros((n.value, 64, 64), np.float32)
+        ft = np.zeros((n.value, 64, 256), np.float32)
+        if n.value:
+            err = lib().hd_extract_patches(self._p, dm.ctypes.data_as(_FP), ft.ctypes.data_as(_FP),
+                                           C.byref(n))
+            if err != HD_NO_ERROR:
+                raise HdError(err, "hd_extract_patches")
+        return dm, ft
+
     def timing(self) -> Dict[str, float]:
         t = (C.c_float * 8)()
         lib().hd_get_timing(self._p, t, 8)
@@ -447,3 +474,85 @@ def dm_list_guru(dm_min, dm_max, dt, pulse_width, f0, df, nchans, tol) -> np.nda
     p = lib().dedisp_generate_dm_list_guru(dm_min, dm_max, dt, pulse_width, f0, df, nchans, tol,
                                            C.byref(n))
     return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Classifier:
+    """hd_classifier_*: the candidate classifier (two-branch CNN on the
+    DM-time and freq-time patches, BF16 tensor-core GEMMs on the GPU)."""
+
+    def __init__(self, seed: int = 1, gpu_id: int = 0):
+        h = C.c_void_p()
+        err = lib().hd_classifier_create(C.byref(h), gpu_id, seed)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_classifier_create")
+        self._p = h
+        self.nparam = int(lib().hd_classifier_param_count())
+
+    def close(self) -> None:
+        if self._p:
+            lib().hd_classifier_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.nparam, np.float32)
+        err = lib().hd_classifier_get_params(self._p, out.ctypes.data_as(_FP), self.nparam)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_classifier_get_params")
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = _f32(p)
+        err = lib().hd_classifier_set_params(self._p, p.ctypes.data_as(_FP), self.nparam)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_classifier_set_params")
+
+    def gradients(self, dm_time, freq_time, labels) -> Tuple[np.ndarray, float]:
+        dm, ft = _f32(dm_time), _f32(freq_time)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        g = np.zeros(self.nparam, np.float32)
+        loss = C.c_float(0)
+        err = lib().hd_classifier_gradients(self._p, dm.ctypes.data_as(_FP), ft.ctypes.data_as(_FP),
+                                            lab.ctypes.data_as(C.POINTER(C.c_int)), len(lab),
+                                            g.ctypes.data_as(_FP), C.byref(loss))
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_classifier_gradients")
+        return g, loss.value
+
+    def train(self, dm_time, freq_time, labels, epochs: int = 10, batch: int = 128,
+              lr: float = 1e-3, seed: int = 7) -> np.ndarray:
+        dm, ft = _f32(dm_time), _f32(freq_time)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        losses = np.zeros(epochs, np.float32)
+        err = lib().hd_classifier_train(self._p, dm.ctypes.data_as(_FP), ft.ctypes.data_as(_FP),
+                                        lab.ctypes.data_as(C.POINTER(C.c_int)), len(lab), epochs,
+                                        batch, lr, seed, losses.ctypes.data_as(_FP))
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_classifier_train")
+        return losses
+
+    def score(self, dm_time, freq_time) -> np.ndarray:
+        dm, ft = _f32(dm_time), _f32(freq_time)
+        n = dm.shape[0]
+        out = np.zeros(n, np.float32)
+        if n:
+            err = lib().hd_classifier_score(self._p, dm.ctypes.data_as(_FP), ft.ctypes.data_as(_FP),
+                                            n, out.ctypes.data_as(_FP))
+            if err != HD_NO_ERROR:
+                raise HdError(err, "hd_classifier_score")
+        return out

@@ -1,0 +1,916 @@
+// classifier.cu -- the learned candidate classifier: a two-branch CNN over a
+// candidate's DM-time patch (64 x 64) and frequency-time patch (64 x 256),
+// trained and evaluated by BF16 tensor-core GEMMs with FP32 accumulation.
+//
+// Network (175 666 parameters):
+//   branch A (DM-time, 1 x 64 x 64) and branch B (freq-time, 1 x 64 x 256),
+//   each: conv3x3(1->8) ReLU maxpool2, conv3x3(8->16) ReLU maxpool2,
+//         conv3x3(16->32) ReLU maxpool2   -> A: 32x8x8, B: 32x8x32
+//   concat (10240) -> FC 16 ReLU -> FC 2 -> softmax (class 1 = pulse)
+// Convolutions run as implicit GEMMs over an im2col matrix: forward
+// (W x col), backward-data (W^T x dOut, then col2im) and backward-weights
+// (dOut x col^T, split over the pixel dimension).  Every GEMM takes BF16
+// operands (weights rounded from FP32 master copies, activations stored in
+// BF16) and accumulates in FP32 with mma.sync m16n8k16.  Adam updates the
+// FP32 master weights.  Activation layout: [channel][batch][row][col].
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <vector>
+
+#include "heimdall_b200.h"
+#include "internal.h"
+
+namespace hdb {
+namespace clf {
+
+using bf16 = __nv_bfloat16;
+
+// ===========================================================================
+// BF16 GEMM, FP32 accumulation: C(m, n) (+)= sum_k A(m, k) B(k, n) with
+// element strides A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn],
+// C(m, n) = C[m*scm + n*scn].  Block tile 32 x 64 x 32, 4 warps of 16 x 32.
+// blockIdx.z splits K into chunks of kchunk; with more than one split the
+// partial sums are added atomically (C must hold the initial value).
+// ===========================================================================
+constexpr int GBM = 32, GBN = 64, GBK = 32, GPAD = 8;
+
+struct GemmArgs {
+  int M, N, K;
+  const bf16* A;
+  long long sam, sak;
+  const bf16* B;
+  long long sbk, sbn;
+  float* C;
+  long long scm, scn;
+  int accumulate;  // add to C (single split) instead of overwriting
+  int kchunk;      // K per blockIdx.z
+};
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
+  __shared__ __align__(16) bf16 As[GBM][GBK + GPAD];  // [m][k]
+  __shared__ __align__(16) bf16 Bs[GBN][GBK + GPAD];  // [n][k]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m0 = blockIdx.y * GBM, n0 = blockIdx.x * GBN;
+  const int kb = blockIdx.z * g.kchunk;
+  const int ke = min(g.K, kb + g.kchunk);
+  const int wm = (warp & 1) * 16, wn = (warp >> 1) * 32;
+  const int gr = lane >> 2, tq = lane & 3;
+  float acc[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const bf16 zero = __float2bfloat16(0.f);
+  for (int k0 = kb; k0 < ke; k0 += GBK) {
+    // tiles, zero outside the matrix; the faster index follows the unit stride
+    for (int e = tid; e < GBM * GBK; e += 128) {
+      int m, k;
+      if (g.sak == 1) { m = e / GBK; k = e % GBK; } else { k = e / GBM; m = e % GBM; }
+      const int gm = m0 + m, gk = k0 + k;
+      As[m][k] = (gm < g.M && gk < ke) ? g.A[gm * g.sam + gk * g.sak] : zero;
+    }
+    for (int e = tid; e < GBN * GBK; e += 128) {
+      int n, k;
+      if (g.sbn == 1) { k = e / GBN; n = e % GBN; } else { n = e / GBK; k = e % GBK; }
+      const int gn = n0 + n, gk = k0 + k;
+      Bs[n][k] = (gn < g.N && gk < ke) ? g.B[gk * g.sbk + gn * g.sbn] : zero;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GBK; kk += 16) {
+      uint32_t a[4];
+      a[0] = *reinterpret_cast<const uint32_t*>(&As[wm + gr][kk + 2 * tq]);
+      a[1] = *reinterpret_cast<const uint32_t*>(&As[wm + gr + 8][kk + 2 * tq]);
+      a[2] = *reinterpret_cast<const uint32_t*>(&As[wm + gr][kk + 2 * tq + 8]);
+      a[3] = *reinterpret_cast<const uint32_t*>(&As[wm + gr + 8][kk + 2 * tq + 8]);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        uint32_t b[2];
+        b[0] = *reinterpret_cast<const uint32_t*>(&Bs[wn + 8 * j + gr][kk + 2 * tq]);
+        b[1] = *reinterpret_cast<const uint32_t*>(&Bs[wn + 8 * j + gr][kk + 2 * tq + 8]);
+        mma_bf16(acc[j], a, b);
+      }
+    }
+    __syncthreads();
+  }
+  const bool split = gridDim.z > 1;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const int m = m0 + wm + gr + (h >> 1) * 8;
+      const int n = n0 + wn + 8 * j + 2 * tq + (h & 1);
+      if (m < g.M && n < g.N) {
+        float* c = g.C + m * g.scm + n * g.scn;
+        if (split) atomicAdd(c, acc[j][h]);
+        else *c = g.accumulate ? *c + acc[j][h] : acc[j][h];
+      }
+    }
+  }
+}
+
+cudaError_t gemm(const GemmArgs& a0, int splits, cudaStream_t s) {
+  GemmArgs a = a0;
+  if (a.M <= 0 || a.N <= 0 || a.K <= 0) return cudaSuccess;
+  splits = std::max(1, std::min(splits, (a.K + GBK - 1) / GBK));
+  a.kchunk = ((a.K + splits - 1) / splits + GBK - 1) / GBK * GBK;
+  splits = (a.K + a.kchunk - 1) / a.kchunk;
+  dim3 grid((unsigned)((a.N + GBN - 1) / GBN), (unsigned)((a.M + GBM - 1) / GBM), (unsigned)splits);
+  if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidValue;
+  k_gemm_bf16<<<grid, 128, 0, s>>>(a); note_launch();
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Elementwise and layout kernels
+// ===========================================================================
+__global__ void k_to_bf16(const float* __restrict__ in, bf16* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16(in[i]);
+}
+
+// network input: patch values (in units of the row's robust deviation)
+// limited to +-kInputClip, so that very bright rows do not saturate training
+constexpr float kInputClip = 16.f;
+__global__ void k_input_bf16(const float* __restrict__ in, bf16* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16(fminf(fmaxf(in[i], -kInputClip), kInputClip));
+}
+
+// weights [co][k] (k < kw) -> BF16 [co][kp], zero columns kw..kp-1
+__global__ void k_weights_bf16(const float* __restrict__ w, int co, int kw, int kp,
+                               bf16* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= co * kp) return;
+  const int o = i / kp, k = i % kp;
+  out[i] = __float2bfloat16(k < kw ? w[o * kw + k] : 0.f);
+}
+
+// im2col of a 3x3, pad-1 convolution: in [ci][b][h][w] -> col [kp][b*h*w]
+// (row ci*9 + ky*3 + kx; rows >= ci*9 are zero)
+__global__ void k_im2col3(const bf16* __restrict__ in, int ci, int nb, int h, int w, int kp,
+                          bf16* __restrict__ col) {
+  const size_t P = (size_t)nb * h * w;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P * kp) return;
+  const int r = (int)(i / P);
+  const size_t p = i % P;
+  bf16 v = __float2bfloat16(0.f);
+  if (r < ci * 9) {
+    const int c = r / 9, ky = (r % 9) / 3, kx = r % 3;
+    const int x = (int)(p % w), y = (int)((p / w) % h);
+    const size_t b = p / ((size_t)w * h);
+    const int yy = y + ky - 1, xx = x + kx - 1;
+    if (yy >= 0 && yy < h && xx >= 0 && xx < w)
+      v = in[(((size_t)c * nb + b) * h + yy) * w + xx];
+  }
+  col[i] = v;
+}
+
+// col2im: dcol [kp][b*h*w] (FP32) -> din [ci][b][h][w], summing the 9 taps
+// that read each input pixel
+__global__ void k_col2im3(const float* __restrict__ dcol, int ci, int nb, int h, int w,
+                          float* __restrict__ din) {
+  const size_t P = (size_t)nb * h * w;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P * ci) return;
+  const int c = (int)(i / P);
+  const size_t p = i % P;
+  const int x = (int)(p % w), y = (int)((p / w) % h);
+  const size_t bo = (p / ((size_t)w * h)) * (size_t)w * h;
+  float sum = 0.f;
+#pragma unroll
+  for (int ky = 0; ky < 3; ky++)
+#pragma unroll
+    for (int kx = 0; kx < 3; kx++) {
+      // output pixel (y - ky + 1, x - kx + 1) read this input through tap (ky, kx)
+      const int yo = y - ky + 1, xo = x - kx + 1;
+      if (yo >= 0 && yo < h && xo >= 0 && xo < w)
+        sum += dcol[(size_t)(c * 9 + ky * 3 + kx) * P + bo + (size_t)yo * w + xo];
+    }
+  din[i] = sum;
+}
+
+// conv output [co][b][h][w] (FP32) + bias -> ReLU -> 2x2 max pool ->
+// act [co][b][h/2][w/2] (BF16), arg = position of the maximum (0..3)
+__global__ void k_bias_relu_pool(const float* __restrict__ z, const float* __restrict__ bias,
+                                 int co, int nb, int h, int w, bf16* __restrict__ act,
+                                 unsigned char* __restrict__ arg) {
+  const int h2 = h / 2, w2 = w / 2;
+  const size_t n = (size_t)co * nb * h2 * w2;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int x2 = (int)(i % w2), y2 = (int)((i / w2) % h2);
+  const size_t cb = i / ((size_t)w2 * h2);  // c * nb + b
+  const int c = (int)(cb / nb);
+  const float* zp = z + cb * (size_t)h * w;
+  float best = -INFINITY;
+  int bi = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const float v = fmaxf(zp[(size_t)(2 * y2 + (q >> 1)) * w + 2 * x2 + (q & 1)] + bias[c], 0.f);
+    if (v > best) { best = v; bi = q; }
+  }
+  act[i] = __float2bfloat16(best);
+  arg[i] = (unsigned char)bi;
+}
+
+// backward of bias/ReLU/pool: dact [co][b][h/2][w/2] (FP32) -> dz [co][b][h][w]
+// (BF16, the next GEMM's operand), and the bias gradient
+__global__ void k_pool_relu_back(const float* __restrict__ dact, const bf16* __restrict__ act,
+                                 const unsigned char* __restrict__ arg, int co, int nb, int h,
+                                 int w, bf16* __restrict__ dz, float* __restrict__ dbias) {
+  const int h2 = h / 2, w2 = w / 2;
+  const size_t n = (size_t)co * nb * h * w;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float v = 0.f;
+  int c = -1;
+  if (i < n) {
+    const int x = (int)(i % w), y = (int)((i / w) % h);
+    const size_t cb = i / ((size_t)w * h);
+    c = (int)(cb / nb);
+    const size_t j = (cb * h2 + y / 2) * w2 + x / 2;
+    const int q = (y & 1) * 2 + (x & 1);
+    if (y / 2 < h2 && x / 2 < w2 && arg[j] == q && __bfloat162float(act[j]) > 0.f) v = dact[j];
+    dz[i] = __float2bfloat16(v);
+  }
+  // per-block partial bias sums (a block may span two channels)
+  __shared__ float s_sum[2];
+  __shared__ int s_c0;
+  if (threadIdx.x == 0) {
+    s_sum[0] = s_sum[1] = 0.f;
+    const size_t i0 = (size_t)blockIdx.x * blockDim.x;
+    s_c0 = (int)(i0 / ((size_t)w * h) / nb);
+  }
+  __syncthreads();
+  if (c >= 0 && v != 0.f) atomicAdd(&s_sum[c - s_c0 > 0 ? 1 : 0], v);
+  __syncthreads();
+  if (threadIdx.x < 2 && s_sum[threadIdx.x] != 0.f && s_c0 + (int)threadIdx.x < co)
+    atomicAdd(&dbias[s_c0 + threadIdx.x], s_sum[threadIdx.x]);
+}
+
+// pooled activations of both branches -> x [b][10240] (A: 2048, B: 8192)
+__global__ void k_flatten(const bf16* __restrict__ a, const bf16* __restrict__ bb, int nb,
+                          bf16* __restrict__ x) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nb * 10240) return;
+  const int n = (int)(i / 10240), f = (int)(i % 10240);
+  if (f < 2048) {
+    const int c = f / 64, s = f % 64;  // A: 32 x (8 x 8)
+    x[i] = a[((size_t)c * nb + n) * 64 + s];
+  } else {
+    const int g = f - 2048, c = g / 256, s = g % 256;  // B: 32 x (8 x 32)
+    x[i] = bb[((size_t)c * nb + n) * 256 + s];
+  }
+}
+
+__global__ void k_unflatten(const float* __restrict__ dx, int nb, float* __restrict__ da,
+                            float* __restrict__ db) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nb * 10240) return;
+  const int n = (int)(i / 10240), f = (int)(i % 10240);
+  if (f < 2048) {
+    const int c = f / 64, s = f % 64;
+    da[((size_t)c * nb + n) * 64 + s] = dx[i];
+  } else {
+    const int g = f - 2048, c = g / 256, s = g % 256;
+    db[((size_t)c * nb + n) * 256 + s] = dx[i];
+  }
+}
+
+// FC1 bias + ReLU: z1 [16][b] -> h [b][16] (FP32)
+__global__ void k_fc1_act(const float* __restrict__ z1, const float* __restrict__ b1, int nb,
+                          float* __restrict__ h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb * 16) return;
+  const int n = i / 16, o = i % 16;
+  h[i] = fmaxf(z1[o * nb + n] + b1[o], 0.f);
+}
+
+// FC2, softmax, cross-entropy and their backward, FC2 weight/bias gradients,
+// the FC1 pre-activation gradient dz1 [16][b] (BF16) and its bias gradient.
+// One thread per sample; w2 [2][16], b2 [2].
+__global__ void k_head(const float* __restrict__ h, const float* __restrict__ w2,
+                       const float* __restrict__ b2, const int* __restrict__ labels, int nb,
+                       int backward, float* __restrict__ prob, float* __restrict__ loss,
+                       float* __restrict__ gw2, float* __restrict__ gb2, bf16* __restrict__ dz1,
+                       float* __restrict__ gb1) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nb) return;
+  const float* hn = h + n * 16;
+  float l0 = b2[0], l1 = b2[1];
+  for (int o = 0; o < 16; o++) {
+    l0 += w2[o] * hn[o];
+    l1 += w2[16 + o] * hn[o];
+  }
+  const float mx = fmaxf(l0, l1);
+  const float e0 = expf(l0 - mx), e1 = expf(l1 - mx);
+  const float p1 = e1 / (e0 + e1);
+  prob[n] = p1;
+  if (!backward) return;
+  const int y = labels[n];
+  const float lse = mx + logf(e0 + e1);
+  atomicAdd(loss, (lse - (y ? l1 : l0)) / nb);
+  const float d1 = (p1 - (y ? 1.f : 0.f)) / nb;  // dL/dl1; dL/dl0 = -d1
+  const float d0 = -d1;
+  atomicAdd(&gb2[0], d0);
+  atomicAdd(&gb2[1], d1);
+  for (int o = 0; o < 16; o++) {
+    atomicAdd(&gw2[o], d0 * hn[o]);
+    atomicAdd(&gw2[16 + o], d1 * hn[o]);
+    const float dh = d0 * w2[o] + d1 * w2[16 + o];
+    const float dz = hn[o] > 0.f ? dh : 0.f;
+    dz1[o * nb + n] = __float2bfloat16(dz);
+    atomicAdd(&gb1[o], dz);
+  }
+}
+
+// per-sample batch gather: dataset [n][len] (BF16) rows idx -> [b][len]
+__global__ void k_gather(const bf16* __restrict__ src, const int* __restrict__ idx, int nb,
+                         int len, bf16* __restrict__ dst) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)nb * len) return;
+  const int n = (int)(i / len), k = (int)(i % len);
+  dst[i] = src[(size_t)idx[n] * len + k];
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master weights
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace clf
+
+// ===========================================================================
+// Candidate patches (Applications/candidate_profiler.C)
+// ===========================================================================
+// DM-time: row r = DM trial dm - 32 + r (zero outside 0..D-1), column t = the
+// width-w boxcar sum starting at first + t, first = ind - 32 - w/2 (0 if
+// ind <= 32 + w/2), from the series' prefix sums S: S[first+t+w] - S[first+t]
+// (zero when it would read past S[len]); gen_dm_time_plot:232-415 with
+// do_filter (its boxcar spans scanned[t + w/2 + (w-1)/2 + 1] - scanned[t]).
+__global__ void k_patch_dm(const float* __restrict__ scan, size_t scan_pitch, size_t len,
+                           const PatchJob* __restrict__ jobs, float* __restrict__ out) {
+  const PatchJob jb = jobs[blockIdx.x];
+  const unsigned w = 1u << jb.filter;
+  const long long first = (jb.ind > 32u + w / 2) ? (long long)jb.ind - 32 - w / 2 : 0;
+  float* o = out + (size_t)blockIdx.x * 4096;
+  for (int e = threadIdx.x; e < 4096; e += blockDim.x) {
+    const int r = e / 64, t = e % 64;
+    const int d = jb.dm - 32 + r;
+    float v = 0.f;
+    const long long a = first + t, b = a + w;
+    if (d >= 0 && d < jb.ndm && b <= (long long)len) {
+      const float* S = scan + (size_t)(jb.series0 + d) * scan_pitch;
+      v = __fsub_rn(S[b], S[a]);
+    }
+    o[e] = v;
+  }
+}
+
+// Freq-time: gen_freq_time_plot:136-230 on the undispersed filterbank (TF
+// bytes): 64 sub-bands of fs = nchans/64 channels x 256 bins of ts samples
+// from first; each pixel the float sum, time outer and channel inner, of
+// x / 255 * 255 divided by ts * fs; samples outside the gulp read as 0.
+__global__ void k_patch_ft(const uint8_t* __restrict__ tf, size_t nsamps, int nchans,
+                           const PatchJob* __restrict__ jobs, float* __restrict__ out) {
+  const PatchJob jb = jobs[blockIdx.x];
+  const int fs = nchans / 64;
+  const uint8_t* fb = tf + (size_t)jb.unit * nsamps * nchans;
+  float* o = out + (size_t)blockIdx.x * 16384;
+  const float npix = (float)((size_t)jb.ft_ts * (size_t)fs);
+  for (int e = threadIdx.x; e < 16384; e += blockDim.x) {
+    const int cs = e / 256, ti = e % 256;
+    const long long t0 = jb.ft_first + (long long)ti * jb.ft_ts;
+    float sum = 0.f;
+    for (unsigned sidx = 0; sidx < jb.ft_ts; sidx++) {
+      const long long t = t0 + sidx;
+      const bool in = t >= 0 && t < (long long)nsamps;
+      const uint8_t* row = fb + (in ? (size_t)t * nchans : 0) + (size_t)cs * fs;
+      for (int f = 0; f < fs; f++) {
+        const float x = in ? (float)row[f] : 0.f;
+        sum = __fadd_rn(sum, __fmul_rn(__fdiv_rn(x, 255.f), 255.f));
+      }
+    }
+    o[e] = __fdiv_rn(sum, npix);
+  }
+}
+
+// k-th smallest (0-based) of v[lo..hi) in shared memory, by ranks
+__device__ float warp_kth(const float* v, int lo, int hi, int k) {
+  const int lane = threadIdx.x & 31;
+  float found = 0.f;
+  bool have = false;
+  for (int i = lo + lane; i < hi; i += 32) {
+    const float x = v[i];
+    int lt = 0, le = 0;
+    for (int j = lo; j < hi; j++) {
+      lt += v[j] < x;
+      le += v[j] <= x;
+    }
+    if (lt <= k && k < le) { found = x; have = true; }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, have);
+  return __shfl_sync(0xffffffffu, found, m ? __ffs(m) - 1 : 0);
+}
+
+// normalise_series_array (candidate_profiler.C:88-134) on rows of n values,
+// one warp per row; a row whose deviation is zero becomes zero (the
+// reference would divide by zero)
+__global__ void k_normalise_rows(float* __restrict__ data, int n, size_t nrows) {
+  extern __shared__ float nr_smem[];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t row = (size_t)blockIdx.x * (blockDim.x >> 5) + wib;
+  float* v = nr_smem + (size_t)wib * 2 * n;  // [n] values, [n] scratch
+  float* a = v + n;
+  if (row >= nrows) return;  // whole warp
+  float* x = data + row * n;
+  for (int j = lane; j < n; j += 32) v[j] = x[j];
+  __syncwarp();
+  const float m1 = warp_kth(v, 0, n / 2, n / 4);
+  const float m2 = warp_kth(v, n / 2, n, n / 4);
+  const double gradient = (double)__fdiv_rn(__fsub_rn(m2, m1), (float)(n / 2));
+  const float median0 = (float)((double)m1 - gradient * (double)(n / 4));
+  for (int j = lane; j < n; j += 32) {
+    const float base = (float)((double)median0 + (double)j * gradient);
+    const float y = __fsub_rn(v[j], base);
+    v[j] = y;
+    a[j] = fabsf(y);
+  }
+  __syncwarp();
+  const float mad = warp_kth(a, 0, n, n / 2);
+  const float stddev = (float)((double)mad * 1.4826);
+  const float val = (float)(1.0 / (double)stddev);
+  for (int j = lane; j < n; j += 32) x[j] = stddev > 0.f ? __fmul_rn(v[j], val) : 0.f;
+}
+
+cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, const uint8_t* tf,
+                            size_t nsamps, int nchans, const PatchJob* jobs, int njobs,
+                            float* dm_out, float* ft_out, cudaStream_t s) {
+  if (njobs <= 0) return cudaSuccess;
+  k_patch_dm<<<njobs, 256, 0, s>>>(scan, scan_pitch, len, jobs, dm_out); note_launch();
+  k_patch_ft<<<njobs, 256, 0, s>>>(tf, nsamps, nchans, jobs, ft_out); note_launch();
+  const size_t r1 = (size_t)njobs * 64;
+  k_normalise_rows<<<clf::nblk(r1, 4), 128, 4 * 2 * 64 * sizeof(float), s>>>(dm_out, 64, r1); note_launch();
+  k_normalise_rows<<<clf::nblk(r1, 4), 128, 4 * 2 * 256 * sizeof(float), s>>>(ft_out, 256, r1); note_launch();
+  return cudaGetLastError();
+}
+}  // namespace hdb
+
+// ===========================================================================
+// The model
+// ===========================================================================
+using hdb::clf::bf16;
+
+namespace {
+
+struct ConvSpec {
+  int ci, co, h, w;  // input channels, output channels, input rows, cols
+  int kw() const { return ci * 9; }
+  int kp() const { return (ci * 9 + 15) / 16 * 16; }
+};
+// branch A: 64 x 64 input; branch B: 64 x 256 input
+const ConvSpec kConv[2][3] = {{{1, 8, 64, 64}, {8, 16, 32, 32}, {16, 32, 16, 16}},
+                              {{1, 8, 64, 256}, {8, 16, 32, 128}, {16, 32, 16, 64}}};
+constexpr int kFeat = 10240, kHid = 16;
+
+struct DBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  ~DBuf() { if (p) cudaFree(p); }
+  template <class T> T* as() { return reinterpret_cast<T*>(p); }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+    if (e == cudaSuccess) cap = std::max<size_t>(bytes, 256);
+    return e;
+  }
+};
+
+}  // namespace
+
+struct hd_classifier_t {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // flat FP32 parameters: per conv layer W [co][ci*9] then b [co], branch A
+  // then B, then W1 [16][10240], b1 [16], W2 [2][16], b2 [2]
+  size_t off_w[2][3], off_b[2][3], off_w1, off_b1, off_w2, off_b2, nparam;
+  DBuf w, g, m, v;          // parameters, gradients, Adam moments
+  DBuf wb_conv[2][3], wb1;  // BF16 weight copies
+  long long step = 0;
+  // per-batch work buffers
+  int cap_batch = 0;
+  DBuf in[2], col, z, act[2][3], arg[2][3], dz, dcol, dact_a[2], dact_b[2], x, z1, h, dz1,
+      dx, prob, loss, labels, idx;
+  DBuf data_dm, data_ft, data_lab;  // resident training set
+  size_t data_n = 0;
+
+  ~hd_classifier_t() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+using namespace hdb::clf;
+
+#define CK(x)                                               \
+  do {                                                      \
+    cudaError_t e_ = (x);                                   \
+    if (e_ != cudaSuccess) return e_;                       \
+  } while (0)
+
+cudaError_t alloc_batch(hd_classifier c, int nb) {
+  if (nb <= c->cap_batch) return cudaSuccess;
+  size_t maxcol = 0, maxz = 0;
+  for (int br = 0; br < 2; br++)
+    for (int l = 0; l < 3; l++) {
+      const ConvSpec& s = kConv[br][l];
+      const size_t P = (size_t)nb * s.h * s.w;
+      maxcol = std::max(maxcol, (size_t)s.kp() * P);
+      maxz = std::max(maxz, (size_t)s.co * P);
+      CK(c->act[br][l].ensure((size_t)s.co * P / 4 * sizeof(bf16)));
+      CK(c->arg[br][l].ensure((size_t)s.co * P / 4));
+    }
+  CK(c->in[0].ensure((size_t)nb * 64 * 64 * sizeof(bf16)));
+  CK(c->in[1].ensure((size_t)nb * 64 * 256 * sizeof(bf16)));
+  CK(c->col.ensure(maxcol * sizeof(bf16)));
+  CK(c->dcol.ensure(maxcol * sizeof(float)));
+  CK(c->z.ensure(maxz * sizeof(float)));
+  CK(c->dz.ensure(maxz * sizeof(bf16)));
+  for (int br = 0; br < 2; br++) {
+    CK(c->dact_a[br].ensure(maxz / 4 * sizeof(float)));
+    CK(c->dact_b[br].ensure(maxz / 4 * sizeof(float)));
+  }
+  CK(c->x.ensure((size_t)nb * kFeat * sizeof(bf16)));
+  CK(c->dx.ensure((size_t)nb * kFeat * sizeof(float)));
+  CK(c->z1.ensure((size_t)nb * kHid * sizeof(float)));
+  CK(c->h.ensure((size_t)nb * kHid * sizeof(float)));
+  CK(c->dz1.ensure((size_t)nb * kHid * sizeof(bf16)));
+  CK(c->prob.ensure((size_t)nb * sizeof(float)));
+  CK(c->loss.ensure(sizeof(float)));
+  CK(c->labels.ensure((size_t)nb * sizeof(int)));
+  CK(c->idx.ensure((size_t)nb * sizeof(int)));
+  c->cap_batch = nb;
+  return cudaSuccess;
+}
+
+cudaError_t refresh_bf16(hd_classifier c) {
+  cudaStream_t s = c->stream;
+  float* w = c->w.as<float>();
+  for (int br = 0; br < 2; br++)
+    for (int l = 0; l < 3; l++) {
+      const ConvSpec& sp = kConv[br][l];
+      CK(c->wb_conv[br][l].ensure((size_t)sp.co * sp.kp() * sizeof(bf16)));
+      k_weights_bf16<<<nblk((size_t)sp.co * sp.kp()), 256, 0, s>>>(
+          w + c->off_w[br][l], sp.co, sp.kw(), sp.kp(), c->wb_conv[br][l].as<bf16>()); hdb::note_launch();
+    }
+  CK(c->wb1.ensure((size_t)kHid * kFeat * sizeof(bf16)));
+  k_to_bf16<<<nblk((size_t)kHid * kFeat), 256, 0, s>>>(w + c->off_w1, c->wb1.as<bf16>(),
+                                                       (size_t)kHid * kFeat); hdb::note_launch();
+  return cudaGetLastError();
+}
+
+// Forward over the batch already in c->in[]; with backward, accumulates the
+// gradients of the mean cross-entropy into c->g (which the caller zeroes).
+cudaError_t run_batch(hd_classifier c, int nb, bool backward) {
+  cudaStream_t s = c->stream;
+  float* w = c->w.as<float>();
+  float* g = c->g.as<float>();
+  CK(refresh_bf16(c));
+  // ---- forward ----
+  for (int br = 0; br < 2; br++) {
+    const bf16* cur = c->in[br].as<bf16>();
+    for (int l = 0; l < 3; l++) {
+      const ConvSpec& sp = kConv[br][l];
+      const size_t P = (size_t)nb * sp.h * sp.w;
+      k_im2col3<<<nblk(P * sp.kp()), 256, 0, s>>>(cur, sp.ci, nb, sp.h, sp.w, sp.kp(),
+                                                   c->col.as<bf16>()); hdb::note_launch();
+      GemmArgs ga{sp.co, (int)P, sp.kp(), c->wb_conv[br][l].as<bf16>(), sp.kp(), 1,
+                  c->col.as<bf16>(), (long long)P, 1, c->z.as<float>(), (long long)P, 1, 0, 0};
+      CK(gemm(ga, 1, s));
+      k_bias_relu_pool<<<nblk(P / 4 * sp.co), 256, 0, s>>>(
+          c->z.as<float>(), w + c->off_b[br][l], sp.co, nb, sp.h, sp.w,
+          c->act[br][l].as<bf16>(), c->arg[br][l].as<unsigned char>()); hdb::note_launch();
+      cur = c->act[br][l].as<bf16>();
+    }
+  }
+  k_flatten<<<nblk((size_t)nb * kFeat), 256, 0, s>>>(c->act[0][2].as<bf16>(),
+                                                     c->act[1][2].as<bf16>(), nb,
+                                                     c->x.as<bf16>()); hdb::note_launch();
+  {
+    GemmArgs ga{kHid, nb, kFeat, c->wb1.as<bf16>(), kFeat, 1, c->x.as<bf16>(), 1, kFeat,
+                c->z1.as<float>(), nb, 1, 0, 0};
+    CK(gemm(ga, 1, s));
+  }
+  k_fc1_act<<<nblk((size_t)nb * kHid), 256, 0, s>>>(c->z1.as<float>(), w + c->off_b1, nb,
+                                                    c->h.as<float>()); hdb::note_launch();
+  if (backward) CK(cudaMemsetAsync(c->loss.p, 0, sizeof(float), s));
+  k_head<<<nblk(nb, 128), 128, 0, s>>>(c->h.as<float>(), w + c->off_w2, w + c->off_b2,
+                                       c->labels.as<int>(), nb, backward ? 1 : 0,
+                                       c->prob.as<float>(), c->loss.as<float>(), g + c->off_w2,
+                                       g + c->off_b2, c->dz1.as<bf16>(), g + c->off_b1); hdb::note_launch();
+  if (!backward) return cudaGetLastError();
+  // ---- backward ----
+  {
+    // dW1 [16][10240] += dz1 [16][b] x x [b][10240]
+    GemmArgs ga{kHid, kFeat, nb, c->dz1.as<bf16>(), nb, 1, c->x.as<bf16>(), kFeat, 1,
+                g + c->off_w1, kFeat, 1, 1, 0};
+    CK(gemm(ga, 1, s));
+    // dx [b][10240] = dz1^T x W1
+    GemmArgs gd{kFeat, nb, kHid, c->wb1.as<bf16>(), 1, kFeat, c->dz1.as<bf16>(), nb, 1,
+                c->dx.as<float>(), 1, kFeat, 0, 0};
+    CK(gemm(gd, 1, s));
+  }
+  k_unflatten<<<nblk((size_t)nb * kFeat), 256, 0, s>>>(c->dx.as<float>(), nb,
+                                                       c->dact_a[0].as<float>(),
+                                                       c->dact_a[1].as<float>()); hdb::note_launch();
+  for (int br = 0; br < 2; br++) {
+    float* dcur = c->dact_a[br].as<float>();   // gradient of this layer's pooled output
+    float* dnext = c->dact_b[br].as<float>();  // gradient of its input
+    for (int l = 2; l >= 0; l--) {
+      const ConvSpec& sp = kConv[br][l];
+      const size_t P = (size_t)nb * sp.h * sp.w;
+      k_pool_relu_back<<<nblk(P * sp.co), 256, 0, s>>>(
+          dcur, c->act[br][l].as<bf16>(), c->arg[br][l].as<unsigned char>(), sp.co, nb, sp.h,
+          sp.w, c->dz.as<bf16>(), g + c->off_b[br][l]); hdb::note_launch();
+      // the layer's input again, as im2col (recomputed rather than stored)
+      const bf16* lin = l == 0 ? c->in[br].as<bf16>() : c->act[br][l - 1].as<bf16>();
+      k_im2col3<<<nblk(P * sp.kp()), 256, 0, s>>>(lin, sp.ci, nb, sp.h, sp.w, sp.kp(),
+                                                   c->col.as<bf16>()); hdb::note_launch();
+      // dW [co][kw] += dz [co][P] x col^T; the padded columns kw..kp are dropped
+      // by writing into a [co][kp] scratch is avoided: N = kw with row stride kw
+      GemmArgs gw{sp.co, sp.kw(), (int)P, c->dz.as<bf16>(), (long long)P, 1, c->col.as<bf16>(),
+                  1, (long long)P, g + c->off_w[br][l], sp.kw(), 1, 0, 0};
+      const int splits = (int)std::min<size_t>(256, (P + 4095) / 4096);
+      CK(gemm(gw, splits, s));
+      if (l > 0) {
+        // dcol [kp][P] = W^T x dz, then col2im into the previous layer's output gradient
+        GemmArgs gd{sp.kp(), (int)P, sp.co, c->wb_conv[br][l].as<bf16>(), 1, sp.kp(),
+                    c->dz.as<bf16>(), (long long)P, 1, c->dcol.as<float>(), (long long)P, 1, 0, 0};
+        CK(gemm(gd, 1, s));
+        k_col2im3<<<nblk(P * sp.ci), 256, 0, s>>>(c->dcol.as<float>(), sp.ci, nb, sp.h, sp.w,
+                                                 dnext); hdb::note_launch();
+        std::swap(dcur, dnext);
+      }
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t upload_patches(hd_classifier c, const float* dm, const float* ft, int nb) {
+  cudaStream_t s = c->stream;
+  // host floats -> device BF16 through a temporary FP32 copy in dcol
+  CK(c->dcol.ensure((size_t)nb * 16384 * sizeof(float)));
+  CK(cudaMemcpyAsync(c->dcol.p, dm, (size_t)nb * 4096 * sizeof(float), cudaMemcpyHostToDevice, s));
+  k_input_bf16<<<nblk((size_t)nb * 4096), 256, 0, s>>>(c->dcol.as<float>(), c->in[0].as<bf16>(),
+                                                       (size_t)nb * 4096); hdb::note_launch();
+  CK(cudaMemcpyAsync(c->dcol.p, ft, (size_t)nb * 16384 * sizeof(float), cudaMemcpyHostToDevice, s));
+  k_input_bf16<<<nblk((size_t)nb * 16384), 256, 0, s>>>(c->dcol.as<float>(), c->in[1].as<bf16>(),
+                                                        (size_t)nb * 16384); hdb::note_launch();
+  return cudaGetLastError();
+}
+
+hd_error to_hd(cudaError_t e) {
+  if (e == cudaSuccess) return HD_NO_ERROR;
+  if (e == cudaErrorMemoryAllocation) return HD_MEM_ALLOC_FAILED;
+  return HD_INTERNAL_GPU_ERROR;
+}
+
+}  // namespace
+
+extern "C" {
+
+hd_size hd_classifier_param_count(void) {
+  size_t n = 0;
+  for (int br = 0; br < 2; br++)
+    for (int l = 0; l < 3; l++) n += (size_t)kConv[br][l].co * kConv[br][l].kw() + kConv[br][l].co;
+  return n + (size_t)kHid * kFeat + kHid + 2 * kHid + 2;
+}
+
+hd_error hd_classifier_create(hd_classifier* out, int gpu_id, unsigned long long seed) {
+  if (!out) return HD_INVALID_POINTER;
+  *out = nullptr;
+  if (cudaSetDevice(gpu_id) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  hd_classifier c = new (std::nothrow) hd_classifier_t();
+  if (!c) return HD_MEM_ALLOC_FAILED;
+  c->device = gpu_id;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return HD_PRIOR_GPU_ERROR;
+  }
+  size_t o = 0;
+  for (int br = 0; br < 2; br++)
+    for (int l = 0; l < 3; l++) {
+      c->off_w[br][l] = o; o += (size_t)kConv[br][l].co * kConv[br][l].kw();
+      c->off_b[br][l] = o; o += kConv[br][l].co;
+    }
+  c->off_w1 = o; o += (size_t)kHid * kFeat;
+  c->off_b1 = o; o += kHid;
+  c->off_w2 = o; o += 2 * kHid;
+  c->off_b2 = o; o += 2;
+  c->nparam = o;
+  // He-normal initial weights (std sqrt(2 / fan_in)), zero conv biases
+  std::vector<float> h(o, 0.f);
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  auto fill = [&](size_t off, size_t n, int fan_in) {
+    const float sd = std::sqrt(2.f / (float)fan_in);
+    for (size_t i = 0; i < n; i++) h[off + i] = nd(rng) * sd;
+  };
+  for (int br = 0; br < 2; br++)
+    for (int l = 0; l < 3; l++)
+      fill(c->off_w[br][l], (size_t)kConv[br][l].co * kConv[br][l].kw(), kConv[br][l].kw());
+  fill(c->off_w1, (size_t)kHid * kFeat, kFeat);
+  fill(c->off_w2, 2 * kHid, kHid);
+  // small positive FC1 biases keep the 16 hidden units active at the start
+  for (int o = 0; o < kHid; o++) h[c->off_b1 + o] = 0.1f;
+  cudaError_t e = c->w.ensure(o * sizeof(float));
+  if (e == cudaSuccess) e = c->g.ensure(o * sizeof(float));
+  if (e == cudaSuccess) e = c->m.ensure(o * sizeof(float));
+  if (e == cudaSuccess) e = c->v.ensure(o * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(c->w.p, h.data(), o * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(c->m.p, 0, o * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(c->v.p, 0, o * sizeof(float));
+  if (e != cudaSuccess) {
+    delete c;
+    return to_hd(e);
+  }
+  *out = c;
+  return HD_NO_ERROR;
+}
+
+void hd_classifier_destroy(hd_classifier c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  delete c;
+}
+
+hd_error hd_classifier_get_params(hd_classifier c, float* params, hd_size count) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!params || count != c->nparam) return HD_INVALID_POINTER;
+  cudaSetDevice(c->device);
+  return to_hd(cudaMemcpy(params, c->w.p, c->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+}
+
+hd_error hd_classifier_set_params(hd_classifier c, const float* params, hd_size count) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!params || count != c->nparam) return HD_INVALID_POINTER;
+  cudaSetDevice(c->device);
+  c->step = 0;
+  cudaError_t e = cudaMemcpy(c->w.p, params, c->nparam * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(c->m.p, 0, c->nparam * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(c->v.p, 0, c->nparam * sizeof(float));
+  return to_hd(e);
+}
+
+hd_error hd_classifier_gradients(hd_classifier c, const float* dm_time, const float* freq_time,
+                                 const int* labels, hd_size n, float* grads, float* loss) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!dm_time || !freq_time || !labels || n == 0 || n > 4096) return HD_INVALID_POINTER;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  cudaError_t e = alloc_batch(c, (int)n);
+  if (e == cudaSuccess) e = upload_patches(c, dm_time, freq_time, (int)n);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->labels.p, labels, n * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->g.p, 0, c->nparam * sizeof(float), s);
+  if (e == cudaSuccess) e = run_batch(c, (int)n, true);
+  if (e == cudaSuccess && grads)
+    e = cudaMemcpyAsync(grads, c->g.p, c->nparam * sizeof(float), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && loss) e = cudaMemcpyAsync(loss, c->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return to_hd(e);
+}
+
+hd_error hd_classifier_train(hd_classifier c, const float* dm_time, const float* freq_time,
+                             const int* labels, hd_size n, int epochs, int batch, float lr,
+                             unsigned long long seed, float* epoch_loss) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!dm_time || !freq_time || !labels || n == 0 || epochs <= 0 || batch <= 0 || batch > 4096)
+    return HD_INVALID_POINTER;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int nb = (int)std::min<size_t>(batch, n);
+  cudaError_t e = alloc_batch(c, nb);
+  // the training set stays on the device in BF16
+  if (e == cudaSuccess) e = c->data_dm.ensure(n * 4096 * sizeof(bf16));
+  if (e == cudaSuccess) e = c->data_ft.ensure(n * 16384 * sizeof(bf16));
+  if (e == cudaSuccess) e = c->data_lab.ensure(n * sizeof(int));
+  if (e != cudaSuccess) return to_hd(e);
+  for (size_t i0 = 0; i0 < n && e == cudaSuccess; i0 += (size_t)nb) {
+    const int k = (int)std::min<size_t>(nb, n - i0);
+    e = upload_patches(c, dm_time + i0 * 4096, freq_time + i0 * 16384, k);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->data_dm.as<bf16>() + i0 * 4096, c->in[0].p, (size_t)k * 4096 * sizeof(bf16),
+                          cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->data_ft.as<bf16>() + i0 * 16384, c->in[1].p, (size_t)k * 16384 * sizeof(bf16),
+                          cudaMemcpyDeviceToDevice, s);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->data_lab.p, labels, n * sizeof(int), cudaMemcpyHostToDevice, s);
+  std::vector<int> order(n);
+  for (size_t i = 0; i < n; i++) order[i] = (int)i;
+  std::mt19937_64 rng(seed);
+  std::vector<int> bidx(nb);
+  for (int ep = 0; ep < epochs && e == cudaSuccess; ep++) {
+    std::shuffle(order.begin(), order.end(), rng);
+    double lsum = 0.0;
+    int nbatches = 0;
+    for (size_t i0 = 0; i0 + (size_t)nb <= n && e == cudaSuccess; i0 += (size_t)nb) {
+      for (int j = 0; j < nb; j++) bidx[j] = order[i0 + j];
+      e = cudaMemcpyAsync(c->idx.p, bidx.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) break;
+      k_gather<<<nblk((size_t)nb * 4096), 256, 0, s>>>(c->data_dm.as<bf16>(), c->idx.as<int>(), nb, 4096,
+                                                       c->in[0].as<bf16>()); hdb::note_launch();
+      k_gather<<<nblk((size_t)nb * 16384), 256, 0, s>>>(c->data_ft.as<bf16>(), c->idx.as<int>(), nb, 16384,
+                                                        c->in[1].as<bf16>()); hdb::note_launch();
+      // labels of the batch (gather of one int per sample)
+      {
+        std::vector<int> hl(nb);
+        for (int j = 0; j < nb; j++) hl[j] = labels[bidx[j]];
+        e = cudaMemcpyAsync(c->labels.p, hl.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // hl and bidx are reused
+      }
+      if (e == cudaSuccess) e = cudaMemsetAsync(c->g.p, 0, c->nparam * sizeof(float), s);
+      if (e == cudaSuccess) e = run_batch(c, nb, true);
+      if (e != cudaSuccess) break;
+      c->step++;
+      const float b1 = 0.9f, b2 = 0.999f;
+      const float c1 = 1.f - (float)std::pow(b1, (double)c->step);
+      const float c2 = 1.f - (float)std::pow(b2, (double)c->step);
+      k_adam<<<nblk(c->nparam), 256, 0, s>>>(c->w.as<float>(), c->g.as<float>(), c->m.as<float>(),
+                                             c->v.as<float>(), c->nparam, lr, b1, b2, 1e-8f, c1, c2); hdb::note_launch();
+      float l = 0.f;
+      e = cudaMemcpyAsync(&l, c->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      lsum += l;
+      nbatches++;
+    }
+    if (epoch_loss) epoch_loss[ep] = nbatches ? (float)(lsum / nbatches) : 0.f;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return to_hd(e);
+}
+
+hd_error hd_classifier_score(hd_classifier c, const float* dm_time, const float* freq_time,
+                             hd_size n, float* scores) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!dm_time || !freq_time || !scores) return HD_INVALID_POINTER;
+  if (n == 0) return HD_NO_ERROR;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int nb = (int)std::min<size_t>(n, 512);
+  cudaError_t e = alloc_batch(c, nb);
+  for (size_t i0 = 0; i0 < n && e == cudaSuccess; i0 += (size_t)nb) {
+    const int k = (int)std::min<size_t>(nb, n - i0);
+    e = upload_patches(c, dm_time + i0 * 4096, freq_time + i0 * 16384, k);
+    if (e == cudaSuccess) e = run_batch(c, k, false);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(scores + i0, c->prob.p, k * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  return to_hd(e);
+}
+
+hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long long sak,
+                      const void* d_b, long long sbk, long long sbn, float* d_c, long long scm,
+                      long long scn, int accumulate, int splits) {
+  if (!d_a || !d_b || !d_c) return HD_INVALID_POINTER;
+  GemmArgs a{m, n, k, static_cast<const bf16*>(d_a), sam, sak, static_cast<const bf16*>(d_b),
+             sbk, sbn, d_c, scm, scn, accumulate, 0};
+  cudaError_t e = gemm(a, splits, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  return to_hd(e);
+}
+
+}  // extern "C"

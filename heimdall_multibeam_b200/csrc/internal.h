@@ -194,4 +194,20 @@ cudaError_t merge_groups(const GiantBuffers& gb, int ngiants, int dm_key_gap, co
 cudaError_t rfi_mask(const float* x, const float* scan, size_t count, size_t boxcar_max,
                      float rfi_tol, int* mask, int* fmask, cudaStream_t s);
 
+// One candidate's patch extraction (Applications/candidate_profiler.C).
+struct PatchJob {
+  unsigned series0;    // first series of the candidate's filterbank (unit x D)
+  int dm, ndm;         // DM trial, trials per filterbank
+  unsigned ind;        // sample index in the dedispersed series
+  int filter;          // boxcar width index (width 2^filter)
+  unsigned unit;       // filterbank of the batch
+  long long ft_first;  // first input sample of the freq-time window (may be < 0)
+  unsigned ft_ts;      // samples per freq-time bin
+};
+// DM-time (64 x 64) and freq-time (64 x 256) patches of njobs candidates
+// (device job list), normalised per row; outputs njobs x 4096 / 16384 floats.
+cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, const uint8_t* tf,
+                            size_t nsamps, int nchans, const PatchJob* jobs, int njobs,
+                            float* dm_out, float* ft_out, cudaStream_t s);
+
 }  // namespace hdb

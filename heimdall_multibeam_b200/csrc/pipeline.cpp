@@ -80,6 +80,15 @@ struct hd_pipeline_t {
 
   std::vector<hd_candidate> cands;                     // all units, unit by unit
   std::vector<std::vector<hd_candidate>> unit_cands;   // per unit
+  // per candidate (parallel to cands): filterbank, series index, DM trial,
+  // width index -- what the patch extraction needs
+  struct CandMeta { unsigned unit, ind; int dm, filter; };
+  std::vector<std::vector<CandMeta>> unit_meta;
+  std::vector<CandMeta> meta;
+  // the last gulp's search geometry (valid when searched)
+  bool searched = false;
+  size_t last_nsamps = 0, last_len = 0, last_scan_pitch = 0, last_units = 0;
+  DevBuf patch_jobs, patch_dm, patch_ft;
   std::vector<unsigned> unit_first;                    // first giant of each unit
   std::vector<float> g_peaks;
   std::vector<hd_size> g_inds, g_begins, g_ends, g_filters, g_dms, g_labels;
@@ -300,6 +309,9 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   cudaStream_t s = pl->stream;
   pl->cands.clear();
   pl->unit_cands.assign(U, {});
+  pl->meta.clear();
+  pl->unit_meta.assign(U, {});
+  pl->searched = false;
   pl->unit_first.assign(U + 1, 0);
   pl->g_peaks.clear();
   std::memset(pl->timing, 0, sizeof(pl->timing));
@@ -417,6 +429,11 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
     HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
     const size_t scan_pitch = round_up(nc + 1, 4);
+    pl->searched = true;
+    pl->last_nsamps = nsamps;
+    pl->last_len = nc;
+    pl->last_scan_pitch = scan_pitch;
+    pl->last_units = U;
     HD_TRY(pl->scan.ensure(NS * scan_pitch * sizeof(float)));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), pl->scan.as<float>(), scan_pitch,
                                nullptr, s, pl->plan->d_err));
@@ -650,11 +667,13 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     c.end = first_idx + ((size_t)r.end % nsamps_beam);
     c.beam = beam_base + beam_idx + 1;
     pl->unit_cands[u].push_back(c);
+    pl->unit_meta[u].push_back({(unsigned)u, (unsigned)ind, (int)r.dm_ind, (int)r.filter});
   }
   for (size_t u = 0; u < U; u++) {
     const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
     write_cand_file(pl, pl->unit_cands[u], beam_base, first_idx);
     pl->cands.insert(pl->cands.end(), pl->unit_cands[u].begin(), pl->unit_cands[u].end());
+    pl->meta.insert(pl->meta.end(), pl->unit_meta[u].begin(), pl->unit_meta[u].end());
   }
 
   // stage timings
@@ -750,6 +769,64 @@ hd_error hd_get_beam_candidates(hd_pipeline pl, hd_size index, hd_candidate* out
   size_t n = std::min(*count, v.size());
   if (out && n) std::memcpy(out, v.data(), n * sizeof(hd_candidate));
   *count = v.size();
+  return HD_NO_ERROR;
+}
+
+hd_error hd_extract_patches(hd_pipeline pl, hd_float* dm_time, hd_float* freq_time,
+                            hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!count) return HD_INVALID_POINTER;
+  const size_t n = pl->cands.size();
+  const size_t k = std::min(*count, n);
+  *count = n;
+  if (k == 0 || (!dm_time && !freq_time)) return HD_NO_ERROR;
+  const size_t C = pl->params.nchans;
+  if (!pl->searched || C % 64 != 0) return HD_INVALID_STRIDE;
+  if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  cudaStream_t s = pl->stream;
+  const size_t D = pl->plan->dm_list.size();
+  std::vector<hdb::PatchJob> jobs(k);
+  for (size_t i = 0; i < k; i++) {
+    const hd_pipeline_t::CandMeta& m = pl->meta[i];
+    hdb::PatchJob& j = jobs[i];
+    j.series0 = (unsigned)(m.unit * D);
+    j.dm = m.dm;
+    j.ndm = (int)D;
+    j.ind = m.ind;
+    j.filter = m.filter;
+    j.unit = m.unit;
+    // gen_freq_time_plot: window of 256 bins of 2^filter samples, widened to
+    // the next power of two >= the DM's largest delay, centred half a sweep
+    // after the candidate
+    size_t md = 0;
+    for (size_t c = 0; c < C; c++) md = std::max(md, (size_t)pl->plan->delays[(size_t)m.dm * C + c]);
+    size_t ts = (size_t)1 << m.filter;
+    size_t in_n = 256 * ts;
+    if (in_n < md) {
+      size_t delay = 2;
+      while (delay < md) delay *= 2;
+      in_n = delay;
+      ts = in_n / 256;
+    }
+    j.ft_ts = (unsigned)ts;
+    j.ft_first = (long long)(m.ind + md / 2) - (long long)(in_n / 2);
+  }
+  HD_TRY(pl->patch_jobs.ensure(k * sizeof(hdb::PatchJob)));
+  HD_TRY(pl->patch_dm.ensure(k * HD_PATCH_DM_TIME * sizeof(float)));
+  HD_TRY(pl->patch_ft.ensure(k * HD_PATCH_FREQ_TIME * sizeof(float)));
+  HD_TRY(cudaMemcpyAsync(pl->patch_jobs.p, jobs.data(), k * sizeof(hdb::PatchJob),
+                         cudaMemcpyHostToDevice, s));
+  HD_TRY(hdb::extract_patches(pl->scan.as<float>(), pl->last_scan_pitch, pl->last_len,
+                              pl->fb_tf.as<uint8_t>(), pl->last_nsamps, (int)C,
+                              pl->patch_jobs.as<hdb::PatchJob>(), (int)k,
+                              pl->patch_dm.as<float>(), pl->patch_ft.as<float>(), s));
+  if (dm_time)
+    HD_TRY(cudaMemcpyAsync(dm_time, pl->patch_dm.p, k * HD_PATCH_DM_TIME * sizeof(float),
+                           cudaMemcpyDeviceToHost, s));
+  if (freq_time)
+    HD_TRY(cudaMemcpyAsync(freq_time, pl->patch_ft.p, k * HD_PATCH_FREQ_TIME * sizeof(float),
+                           cudaMemcpyDeviceToHost, s));
+  HD_TRY(cudaStreamSynchronize(s));
   return HD_NO_ERROR;
 }
 

@@ -22,7 +22,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import List, Optional, Sequence
+from typing import Tuple, List, Optional, Sequence
 
 import numpy as np
 
@@ -202,3 +202,84 @@ def stf(beams: Sequence[Beam]) -> np.ndarray:
     """Concatenates beams in time (the reference's multibeam "STF" layout,
     Formats/PSRDadaRingBuffer.C:194-198)."""
     return np.ascontiguousarray(np.concatenate([b.data for b in beams], axis=0))
+
+
+# ---------------------------------------------------------------------------
+# Classifier training data: gulps with injected pulses and labelled RFI
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class RfiEvent:
+    kind: str       # "burst" (zero-DM broadband), "narrow" (few channels), "drift"
+    t0: float       # first sample
+    length: float   # samples
+
+
+TRAIN = Workload("train_c256_n32768", 256, 128e-6, 1500.0, -1.5625, 1 << 15, 1, 0.0, 500.0,
+                 256, False, "classifier training gulps: 256 ch, 128 us, 2^15 samples, DM 0-500")
+
+
+def make_training_beam(seed: int, w: Workload = TRAIN, n_pulses: int = 4, n_rfi: int = 2
+                       ) -> Tuple[Beam, List[RfiEvent]]:
+    """Noise + n_pulses dispersed pulses (DM 30..dm_max, FWHM 0.5-20 ms,
+    S/N 8-40) + n_rfi RFI events, each event in its own slot of the gulp
+    (separated by more than the clustering time window, so that an RFI
+    cluster does not absorb a pulse).  RFI kinds: zero-DM broadband bursts
+    (1-64 samples, +1..+3 sigma per channel), narrowband bursts (1-8 adjacent
+    channels, 16-512 samples, +3..+8 sigma) and sinusoidal baseline drifts
+    over all channels (period 5-50 ms, 1-3 periods, 0.3-1 sigma)."""
+    g = _rng(seed, 0x7A11)
+    md = max_delay_samples(w.dm_max, w.nchans, w.dt, w.f0, w.df)
+    lo = 2 * w.boxcar_max
+    hi = w.nsamps - md - 2 * w.boxcar_max
+    nev = n_pulses + n_rfi
+    slot = (hi - lo) / max(nev, 1)
+    kinds = ["pulse"] * n_pulses + ["rfi"] * n_rfi
+    g.shuffle(kinds)
+    pulses: List[Pulse] = []
+    events: List[RfiEvent] = []
+    plan = []
+    for k, kind in enumerate(kinds):
+        t = lo + slot * (k + float(g.uniform(0.3, 0.7)))
+        if kind == "pulse":
+            dm = float(g.uniform(30.0, w.dm_max))
+            fw = float(math.exp(g.uniform(math.log(0.5e-3), math.log(20e-3))))
+            pulses.append(Pulse(t, dm, fw, float(g.uniform(8.0, 40.0))))
+        else:
+            plan.append((t, ("burst", "narrow", "drift")[int(g.integers(0, 3))]))
+    b = make_beam(w.nsamps, w.nchans, w.dt, w.f0, w.df, pulses, seed=seed, beam=1, rng=g)
+    x = b.data.astype(np.float32)
+    for t, kind in plan:
+        if kind == "burst":
+            ln = int(g.integers(1, 65))
+            t0 = int(t)
+            x[t0:t0 + ln, :] += float(g.uniform(1.0, 3.0)) * 16.0
+        elif kind == "narrow":
+            ln = int(2 ** g.uniform(4, 9))
+            t0 = int(t)
+            nc = int(g.integers(1, 9))
+            c0 = int(g.integers(0, w.nchans - nc))
+            x[t0:t0 + ln, c0:c0 + nc] += float(g.uniform(3.0, 8.0)) * 16.0
+        else:
+            period = float(g.uniform(0.005, 0.05)) / w.dt
+            ln = int(min(slot * 0.5, period * float(g.uniform(1.0, 3.0))))
+            t0 = int(t)
+            amp = float(g.uniform(0.3, 1.0)) * 16.0
+            tt = np.arange(ln, dtype=np.float32)
+            x[t0:t0 + ln, :] += (amp * np.sin(2.0 * np.pi * tt / period))[:, None]
+        events.append(RfiEvent(kind, float(t0), float(ln)))
+    np.rint(x, out=x)
+    np.clip(x, 0, 255, out=x)
+    b.data = x.astype(np.uint8)
+    return b, events
+
+
+def match_pulse(cand, pulses: Sequence[Pulse], dt: float) -> int:
+    """Index of the injected pulse a candidate row recovers, or -1: |samp -
+    t0| <= max(2^filter, FWHM/dt) + 2 and DM within max(5 %, 2 trial steps)
+    (the recall rule of the benchmark)."""
+    for k, p in enumerate(pulses):
+        tol_t = max(2 ** int(cand["filter"]), p.fwhm_s / dt) + 2
+        tol_dm = max(0.05 * p.dm, 2 * 1.25 * max(p.dm, 1.0) * 0.01)
+        if abs(int(cand["samp_idx"]) - p.t0) <= tol_t and abs(float(cand["dm"]) - p.dm) <= tol_dm:
+            return k
+    return -1

@@ -210,6 +210,62 @@ hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size nsamps, hd
                                          hd_float rfi_tol, hd_size boxcar_max, hd_size nbeams,
                                          void* stream);
 
+/* ---- Learned candidate classifier (no counterpart in the reference) ----
+ *
+ * Patches per candidate (float, row-major): a DM-time patch of 64 DM trials
+ * (the candidate's trial at row 32) x 64 boxcar-filtered samples, and a
+ * frequency-time patch of 64 sub-bands x 256 time bins of the undispersed
+ * filterbank around the candidate, each row detrended and scaled as the
+ * reference's candidate profiler does (Applications/candidate_profiler.C:
+ * 88-134 normalise_series_array, 136-230 gen_freq_time_plot, 232-415
+ * gen_dm_time_plot).  The classifier is a two-branch CNN (3 conv layers per
+ * branch, 2 fully connected layers, 175666 parameters) trained and evaluated
+ * on the GPU with BF16 tensor-core GEMMs accumulating in FP32; patch values
+ * enter the network limited to +-16.  Its score
+ * (probability of a dispersed pulse) only ranks or flags candidates; the
+ * candidate list itself is unchanged. */
+#define HD_PATCH_DM_TIME   4096   /* 64 x 64 floats per candidate */
+#define HD_PATCH_FREQ_TIME 16384  /* 64 x 256 floats per candidate */
+typedef struct hd_classifier_t* hd_classifier;
+
+/* Patches of every candidate of the last hd_execute / hd_execute_beams, in
+ * hd_get_candidates order.  Copies min(*count, available) patches (either
+ * output may be NULL) and sets *count to the number available.  Needs
+ * nchans a multiple of 64.  Call before the next execute (it reads that
+ * gulp's device buffers). */
+hd_error hd_extract_patches(hd_pipeline pipeline, hd_float* dm_time, hd_float* freq_time,
+                            hd_size* count);
+
+hd_size  hd_classifier_param_count(void);
+hd_error hd_classifier_create(hd_classifier* classifier, int gpu_id, unsigned long long seed);
+void     hd_classifier_destroy(hd_classifier classifier);
+/* FP32 parameters, layout: per conv layer (branch A layers 1-3, then branch
+ * B) W [co][ci*9] then b [co]; W1 [16][10240], b1 [16], W2 [2][16], b2 [2]. */
+hd_error hd_classifier_get_params(hd_classifier classifier, hd_float* params, hd_size count);
+hd_error hd_classifier_set_params(hd_classifier classifier, const hd_float* params,
+                                  hd_size count);
+/* Gradient of the mean cross-entropy over n labelled patches (one batch,
+ * n <= 4096), without updating the parameters. */
+hd_error hd_classifier_gradients(hd_classifier classifier, const hd_float* dm_time,
+                                 const hd_float* freq_time, const int* labels, hd_size n,
+                                 hd_float* grads, hd_float* loss);
+/* Adam training on n labelled patches (label 1 = dispersed pulse); the mean
+ * loss of each epoch goes to epoch_loss[epoch] (may be NULL). */
+hd_error hd_classifier_train(hd_classifier classifier, const hd_float* dm_time,
+                             const hd_float* freq_time, const int* labels, hd_size n,
+                             int epochs, int batch, hd_float lr, unsigned long long seed,
+                             hd_float* epoch_loss);
+/* Probability of a dispersed pulse for each of n patches. */
+hd_error hd_classifier_score(hd_classifier classifier, const hd_float* dm_time,
+                             const hd_float* freq_time, hd_size n, hd_float* scores);
+/* The classifier's GEMM on device operands, for testing: C (m x n, FP32) =
+ * A (m x k, BF16) x B (k x n, BF16) with element strides A(i, l) =
+ * A[i*sam + l*sak], B(l, j) = B[l*sbk + j*sbn], C(i, j) = C[i*scm + j*scn];
+ * accumulate adds to C; splits > 1 sums K in parts atomically into C. */
+hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long long sak,
+                      const void* d_b, long long sbk, long long sbn, float* d_c,
+                      long long scm, long long scn, int accumulate, int splits);
+
 /* Number of kernels this library has launched in this process. */
 unsigned long long hd_get_launch_count(void);
 

@@ -121,6 +121,16 @@ def lib():
         L.or_baseline_plan.argtypes = [C.c_size_t, C.c_size_t, _szp, _szp, _szp]
         L.or_exclusive_scan.argtypes = [_fp, C.c_size_t, _fp]
         L.or_linear_stretch.argtypes = [_fp, C.c_size_t, _fp, C.c_size_t]
+        L.or_set_scan_capture.argtypes = [C.c_void_p, C.c_size_t]
+        L.or_normalise_rows.argtypes = [_fp, C.c_size_t, C.c_size_t]
+        L.or_patch_dm.argtypes = [_fp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                  C.c_size_t, C.c_size_t, _fp]
+        L.or_patch_ft.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                                  C.c_size_t, _fp]
+        L.or_cnn_param_count.restype = C.c_size_t
+        L.or_bf16.restype = C.c_float
+        L.or_bf16.argtypes = [C.c_float]
+        L.or_cnn_run.argtypes = [_fp, _fp, _fp, C.c_void_p, C.c_size_t, _fp, _fp, _fp]
         _lib = L
     return _lib
 
@@ -300,3 +310,73 @@ def ref_execute(fb: np.ndarray, nbeams: int = 1, first_idx: int = 0, nthreads: i
             with open(f) as fh:
                 lines += [ln.rstrip("\n") for ln in fh if ln.strip()]
     return err, proc.value, lines, secs.value
+
+
+# ---------------------------------------------------------------------------
+# Classifier restatement (oracle/classifier.c)
+# ---------------------------------------------------------------------------
+def execute_with_scans(fb: np.ndarray, nbeams: int = 1, **kw):
+    """execute() that also returns every DM trial's prefix sum
+    ([dm_count, nc + 1] float32, nc = nsamps - max_delay)."""
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    okw = {k: v for k, v in kw.items() if k not in ("output_dir",)}
+    dms = dm_list(okw.get("dm_min", 0.0), okw.get("dm_max", 1000.0), okw.get("dt", 64e-6),
+                  okw.get("dm_pulse_width", 40.0), okw.get("f0", 1400.0), okw.get("df", -0.39),
+                  nchans, okw.get("dm_tol", 1.25))
+    table = delay_table(nchans, okw.get("dt", 64e-6), okw.get("f0", 1400.0), okw.get("df", -0.39))
+    md = int(lib().or_max_delay(_fptr(dms), len(dms), _fptr(table), nchans))
+    pitch = nsamps - md + 8
+    scans = np.zeros((len(dms), pitch), np.float32)
+    lib().or_set_scan_capture(scans.ctypes.data, pitch)
+    try:
+        r = execute(fb, nbeams=nbeams, **okw)
+    finally:
+        lib().or_set_scan_capture(None, 0)
+    return r, scans[:, :nsamps - md + 1], dms, table
+
+
+def normalise_rows(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32).copy()
+    lib().or_normalise_rows(_fptr(a), a.shape[-1], a.size // a.shape[-1])
+    return a
+
+
+def patch_dm(scans: np.ndarray, dm: int, ind: int, filt: int) -> np.ndarray:
+    scans = np.ascontiguousarray(scans, dtype=np.float32)
+    out = np.zeros((64, 64), np.float32)
+    lib().or_patch_dm(_fptr(scans), scans.shape[1], scans.shape[1] - 1, scans.shape[0], dm, ind,
+                      filt, _fptr(out))
+    return out
+
+
+def patch_ft(fb: np.ndarray, max_delay: int, ind: int, filt: int) -> np.ndarray:
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    out = np.zeros((64, 256), np.float32)
+    lib().or_patch_ft(fb.ctypes.data, fb.shape[0], fb.shape[1], max_delay, ind, filt, _fptr(out))
+    return out
+
+
+def cnn_param_count() -> int:
+    return int(lib().or_cnn_param_count())
+
+
+def cnn_run(params: np.ndarray, dm_time: np.ndarray, freq_time: np.ndarray, labels=None):
+    """(probabilities, gradients or None, loss or None) of the CPU network."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    dm_time = np.ascontiguousarray(dm_time, dtype=np.float32)
+    freq_time = np.ascontiguousarray(freq_time, dtype=np.float32)
+    n = dm_time.shape[0]
+    probs = np.zeros(n, np.float32)
+    grads = loss = None
+    if labels is not None:
+        labels = np.ascontiguousarray(labels, dtype=np.int32)
+        grads = np.zeros_like(params)
+        lossv = np.zeros(1, np.float32)
+        lib().or_cnn_run(_fptr(params), _fptr(dm_time), _fptr(freq_time), labels.ctypes.data, n,
+                         _fptr(probs), _fptr(grads), _fptr(lossv))
+        loss = float(lossv[0])
+    else:
+        lib().or_cnn_run(_fptr(params), _fptr(dm_time), _fptr(freq_time), None, n, _fptr(probs),
+                         None, None)
+    return probs, grads, loss

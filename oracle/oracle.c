@@ -605,6 +605,15 @@ typedef struct {
   int       stopped;  /* a break condition fired before this DM */
 } or_dm_out;
 
+/* Test hook: when set, or_hd_execute copies each DM trial's prefix sum
+ * (nc + 1 values) to g_scan_capture + d * pitch. */
+static float* g_scan_capture = NULL;
+static size_t g_scan_capture_pitch = 0;
+void or_set_scan_capture(float* buf, size_t pitch) {
+  g_scan_capture = buf;
+  g_scan_capture_pitch = pitch;
+}
+
 int or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t nbits,
                   size_t first_idx, size_t nbeams, or_result* res) {
   (void)first_idx;
@@ -677,6 +686,8 @@ int or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t n
       size_t cur_off = rel_bmax / 2;
       float* S = (float*)calloc(cur_nsamps + 8, sizeof(float));
       or_exclusive_scan(x, cur_nsamps + 1, S);
+      if (g_scan_capture)
+        memcpy(g_scan_capture + d * g_scan_capture_pitch, S, (cur_nsamps + 1) * sizeof(float));
       float* F = (float*)calloc(nc + 8, sizeof(float));
       int wi = 0;
       for (size_t fw = scr; fw <= Bmax; fw *= 2, wi++) {

@@ -129,6 +129,19 @@ typedef struct {
 int  or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t nbits,
                    size_t first_idx, size_t nbeams, or_result* res);
 void or_result_free(or_result* res);
+/* Test hook: keep every DM trial's prefix sum of the last or_hd_execute. */
+void or_set_scan_capture(float* buf, size_t pitch);
+
+/* ---- classifier (Applications/candidate_profiler.C and the CNN) ---- */
+void or_normalise_rows(float* data, size_t n, size_t nrows);
+void or_patch_dm(const float* scans, size_t pitch, size_t len, size_t ndm, size_t dm,
+                 size_t ind, size_t filter, float* out);
+void or_patch_ft(const uint8_t* tf, size_t nsamps, size_t nchans, size_t max_delay,
+                 size_t ind, size_t filter, float* out);
+size_t or_cnn_param_count(void);
+float or_bf16(float x);
+void or_cnn_run(const float* params, const float* dm_time, const float* freq_time,
+                const int* labels, size_t n, float* probs, float* grads, float* loss);
 
 #ifdef __cplusplus
 }
