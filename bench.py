@@ -297,6 +297,9 @@ def run_product(args):
     ms, ms_plain_m, ms_e2e_m = (float(x) for x in tmax)
     value = world * wk.beam_s / (ms / 1e3)
 
+    clf_rec = None
+    if not args.batched_only and not args.no_classifier:
+        clf_rec = classifier_bench(args, H, torch, dev, pl)
     pl.close()
     # secondary: the plain survey-size single-beam gulp
     survey = None
@@ -376,12 +379,75 @@ def run_product(args):
                           "api": "hd_execute_beams" if U > 1 else "hd_execute"}
         if survey is not None:
             rec["survey_plain"] = survey
+        if clf_rec is not None:
+            rec["classifier"] = clf_rec
         if not args.no_cpu_baseline:
             rec["cpu_baseline"] = cpu_baseline(args, wk)
         print(json.dumps(rec), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# forward multiply-adds of the classifier per candidate: 3x3 convolutions
+# (rows x cols x c_out x c_in x 9 per layer, both branches) and the two
+# fully connected layers
+CLF_CONV = [(1, 8, 64, 64), (8, 16, 32, 32), (16, 32, 16, 16),
+            (1, 8, 64, 256), (8, 16, 32, 128), (16, 32, 16, 64)]
+CLF_MACS = sum(h * w_ * co * ci * 9 for ci, co, h, w_ in CLF_CONV) + 10240 * 16 + 16 * 2
+CLF_PATCH_BYTES = (4096 + 16384) * 4
+
+
+def classifier_bench(args, H, torch, dev, pl):
+    """Classifier inference: (1) hd_score_candidates on the last gulp's
+    candidates (patches extracted and scored on the GPU, scores to host);
+    (2) throughput of hd_classifier_score_device on 4096 device-resident
+    patch pairs.  Device times from the classifier's own CUDA events."""
+    peaks, peak_kind = _peaks()
+    out = {}
+    with H.Classifier(seed=1, gpu_id=dev.index) as clf:
+        n = len(pl.candidates())
+        if n:
+            for _ in range(2):
+                pl.scores(clf)
+            dev_ms, wall = 0.0, 0.0
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                pl.scores(clf)
+                wall += time.perf_counter() - t0
+                dev_ms += clf.last_score_ms()
+            out["gulp"] = {"api": "hd_score_candidates", "candidates": n,
+                           "network_ms": round(dev_ms / args.steps, 4),
+                           "call_ms_host_clock": round(wall * 1e3 / args.steps, 4)}
+        nb = 4096
+        g = torch.Generator(device=dev).manual_seed(5)
+        dm = torch.randn((nb, 64, 64), generator=g, device=dev, dtype=torch.float32)
+        ft = torch.randn((nb, 64, 256), generator=g, device=dev, dtype=torch.float32)
+        torch.cuda.synchronize(dev)
+        for _ in range(2):
+            clf.score_device(dm.data_ptr(), ft.data_ptr(), nb)
+        ms = 0.0
+        for _ in range(args.steps):
+            clf.score_device(dm.data_ptr(), ft.data_ptr(), nb)
+            ms += clf.last_score_ms()
+        ms /= args.steps
+        flops = 2.0 * CLF_MACS * nb
+        tflops = flops / (ms / 1e3) / 1e12
+        gbs = CLF_PATCH_BYTES * nb / (ms / 1e3) / 1e9
+        out["throughput"] = {
+            "api": "hd_classifier_score_device", "candidates": nb,
+            "ms": round(ms, 4), "candidates_per_s": round(nb / (ms / 1e3), 1),
+            "flop_per_candidate": int(2 * CLF_MACS),
+            "tensor": {"achieved_tflops": round(tflops, 3), "peak": peaks["bf16_tflops"],
+                       "frac": round(tflops / peaks["bf16_tflops"], 5),
+                       "peak_kind": f"of {peak_kind}"},
+            "patch_read": {"achieved_gbs": round(gbs, 2), "peak": peaks["hbm_gbs"],
+                           "frac": round(gbs / peaks["hbm_gbs"], 5),
+                           "bytes_per_candidate": CLF_PATCH_BYTES},
+            "note": "untrained weights (the work does not depend on their values); one "
+                    "persistent fused kernel (k_clf_infer, one CTA per SM): mma.sync BF16 "
+                    "convolutions with FP32 accumulation, FC layers in the same kernel"}
+    return out
 
 
 def survey_plain(args, H, torch, dev, barrier, dist, world):
@@ -529,6 +595,8 @@ def main():
                     help="beams of the multibeam gulp (fewer are for profiling)")
     ap.add_argument("--batched-only", action="store_true",
                     help="time only the batched form (profiling)")
+    ap.add_argument("--no-classifier", action="store_true",
+                    help="skip the classifier inference measurement")
     ap.add_argument("--no-survey", action="store_true",
                     help="skip the secondary single-beam survey gulp")
     ap.add_argument("--ref-beams", type=int, default=4,

@@ -148,6 +148,9 @@ SYMBOLS = {
     "hd_classifier_train": (C.c_int, [_P, _FP, _FP, C.POINTER(C.c_int), _SZ, C.c_int, C.c_int,
                                       C.c_float, C.c_ulonglong, _FP]),
     "hd_classifier_score": (C.c_int, [_P, _FP, _FP, _SZ, _FP]),
+    "hd_classifier_score_device": (C.c_int, [_P, C.c_void_p, C.c_void_p, _SZ, _FP]),
+    "hd_score_candidates": (C.c_int, [_P, _P, _FP, _SZP]),
+    "hd_classifier_get_timing": (C.c_int, [_P, _FP]),
     "hd_bf16_gemm": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, C.c_longlong, C.c_longlong, _P,
                                C.c_longlong, C.c_longlong, _FP, C.c_longlong, C.c_longlong,
                                C.c_int, C.c_int]),
@@ -376,6 +379,19 @@ class Pipeline:
                 raise HdError(err, "hd_extract_patches")
         return dm, ft
 
+    def scores(self, classifier: "Classifier") -> np.ndarray:
+        """hd_score_candidates: the classifier's P(pulse) for each candidate
+        of the last execute (patches extracted and scored on the GPU)."""
+        n = C.c_size_t(0)
+        lib().hd_score_candidates(self._p, classifier._p, None, C.byref(n))
+        out = np.zeros(n.value, np.float32)
+        if n.value:
+            err = lib().hd_score_candidates(self._p, classifier._p, out.ctypes.data_as(_FP),
+                                            C.byref(n))
+            if err != HD_NO_ERROR:
+                raise HdError(err, "hd_score_candidates")
+        return out
+
     def timing(self) -> Dict[str, float]:
         t = (C.c_float * 8)()
         lib().hd_get_timing(self._p, t, 8)
@@ -555,4 +571,20 @@ class Classifier:
                                             n, out.ctypes.data_as(_FP))
             if err != HD_NO_ERROR:
                 raise HdError(err, "hd_classifier_score")
+        return out
+
+    def last_score_ms(self) -> float:
+        """hd_classifier_get_timing: device ms of the last scoring call."""
+        ms = C.c_float(0.0)
+        lib().hd_classifier_get_timing(self._p, C.byref(ms))
+        return float(ms.value)
+
+    def score_device(self, dm_ptr: int, ft_ptr: int, n: int) -> np.ndarray:
+        """hd_classifier_score_device on device pointers (n patch pairs)."""
+        out = np.zeros(n, np.float32)
+        if n:
+            err = lib().hd_classifier_score_device(self._p, C.c_void_p(dm_ptr), C.c_void_p(ft_ptr),
+                                                   n, out.ctypes.data_as(_FP))
+            if err != HD_NO_ERROR:
+                raise HdError(err, "hd_classifier_score_device")
         return out

@@ -368,6 +368,282 @@ inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t)
 }  // namespace clf
 
 // ===========================================================================
+// Fused inference: the whole network for one candidate per CTA iteration.
+//
+// A persistent CTA of 16 warps takes candidates in turn.  Activations live in
+// shared memory as [row + 1][col + 1][channel] BF16 with a zero ring (the
+// convolutions' padding).  Each 3x3 convolution is an implicit GEMM on the
+// tensor cores (mma.sync m16n8k16, FP32 accumulation) with the 16 rows of an
+// MMA tile = 2 image rows x 8 columns and its columns = output channels; the
+// K dimension runs over taps and input channels: one tap x 16 channels
+// (c_in = 16), two taps x 8 channels (c_in = 8) or the 9 taps of the single
+// input channel.  Bias, ReLU and the 2x2 max-pool are applied to the
+// accumulators in registers (the vertical pair sits in one thread, the
+// horizontal pair in lanes 4 apart) and the pooled value is rounded to BF16
+// once, as in the training path.  The last layer of each branch writes the
+// flattened feature vector (10240 BF16) to shared memory; each warp then
+// computes one FC1 unit (fixed lane order and shuffle tree), and thread 0 the
+// FC2 logits and the softmax.  Every candidate is summed in the same order
+// whatever the grid, so all scoring entry points agree bit for bit.
+// ===========================================================================
+namespace inf {
+using namespace clf;
+constexpr int kWarps = 16, kThreads = kWarps * 32;
+// shared-memory regions (bytes)
+constexpr int kR0 = 18 * 66 * 16 * 2;   // B input [66][258]; B pool-2 [18][66][16]; A pool-1 [34][34][8]
+constexpr int kR1 = 34 * 130 * 8 * 2;   // B pool-1 [34][130][8]; A input [66][66]; A pool-2 [18][18][16]
+constexpr int kF = 10240 * 2;           // flattened features
+// weight fragments per layer: ksteps x (c_out / 8) x 32 lanes of uint2
+constexpr int kFragL1 = 1 * 1 * 32, kFragL2 = 5 * 2 * 32, kFragL3 = 9 * 4 * 32;
+constexpr int kFragBranch = kFragL1 + kFragL2 + kFragL3;
+constexpr int kWF = 2 * kFragBranch * 8;
+constexpr size_t kSmem = (size_t)kR0 + kR1 + kF + kWF + 256 * sizeof(float);
+
+struct Args {
+  const float* dm;   // [n][64][64] FP32 patches
+  const float* ft;   // [n][64][256]
+  int n;
+  const float* w;    // FP32 parameters
+  int off_w[2][3], off_b[2][3], off_b1, off_w2, off_b2;
+  const bf16* wb1;   // FC1 weights [16][10240] BF16
+  float* prob;       // [n]
+};
+
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// weight fragment b0/b1 of k-step s, n-tile j for this lane; K order as the
+// A fragments below
+template <int CI>
+__device__ uint2 weight_frag(const float* W, int s, int j, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int co = 8 * j + g;
+  auto wk = [&](int k) -> bf16 {
+    int tap, ci;
+    if (CI == 16) { tap = s; ci = k; }
+    else if (CI == 8) { tap = 2 * s + (k >> 3); ci = k & 7; }
+    else { tap = k; ci = 0; }
+    if (tap >= 9) return __float2bfloat16(0.f);
+    return __float2bfloat16(W[co * (CI * 9) + ci * 9 + tap]);
+  };
+  uint2 r;
+  r.x = pack2(wk(2 * t), wk(2 * t + 1));
+  r.y = pack2(wk(2 * t + 8), wk(2 * t + 9));
+  return r;
+}
+
+template <int CI, int CO>
+__device__ void build_frags(const float* W, uint2* wf) {
+  constexpr int KS = CI == 16 ? 9 : (CI == 8 ? 5 : 1);
+  constexpr int NT = CO / 8;
+  for (int e = threadIdx.x; e < KS * NT * 32; e += blockDim.x) {
+    const int lane = e & 31, j = (e >> 5) % NT, s = (e >> 5) / NT;
+    wf[e] = weight_frag<CI>(W, s, j, lane);
+  }
+}
+
+// zero ring of a [H2 + 2][W2 + 2][C] buffer
+__device__ void zero_ring(bf16* buf, int H2, int W2, int C) {
+  const int Wp = W2 + 2, Hp = H2 + 2;
+  const int ring = 2 * Wp + 2 * H2;  // pixels
+  const bf16 z = __float2bfloat16(0.f);
+  for (int e = threadIdx.x; e < ring * C; e += blockDim.x) {
+    const int px = e / C, c = e % C;
+    int y, x;
+    if (px < Wp) { y = 0; x = px; }
+    else if (px < 2 * Wp) { y = Hp - 1; x = px - Wp; }
+    else { const int q = px - 2 * Wp; y = 1 + (q >> 1); x = (q & 1) ? Wp - 1 : 0; }
+    buf[((size_t)y * Wp + x) * C + c] = z;
+  }
+}
+
+// patch rows (FP32, global) -> BF16 [66][W + 2] with a zero ring, limited to
+// +-kInputClip as the training input
+__device__ void load_input(const float* __restrict__ src, int W, bf16* dst) {
+  zero_ring(dst, 64, W, 1);
+  const int n4 = 64 * W / 4;
+  for (int e = threadIdx.x; e < n4; e += blockDim.x) {
+    const float4 v = reinterpret_cast<const float4*>(src)[e];
+    const int y = (4 * e) / W, x = (4 * e) % W;
+    bf16* o = dst + (size_t)(y + 1) * (W + 2) + x + 1;
+    o[0] = __float2bfloat16(fminf(fmaxf(v.x, -kInputClip), kInputClip));
+    o[1] = __float2bfloat16(fminf(fmaxf(v.y, -kInputClip), kInputClip));
+    o[2] = __float2bfloat16(fminf(fmaxf(v.z, -kInputClip), kInputClip));
+    o[3] = __float2bfloat16(fminf(fmaxf(v.w, -kInputClip), kInputClip));
+  }
+}
+
+// conv 3x3 (pad 1) + bias + ReLU + 2x2 max-pool of an H x W x CI image.
+// out: [H/2 + 2][W/2 + 2][CO] interior, or (feat) the flattened features at
+// feat[c * (H/2 * W/2) + y * W/2 + x].
+template <int CI, int CO>
+__device__ void conv_layer(const bf16* __restrict__ in, int H, int W, const uint2* __restrict__ wf,
+                           const float* __restrict__ bias, bf16* __restrict__ out,
+                           bf16* __restrict__ feat) {
+  constexpr int KS = CI == 16 ? 9 : (CI == 8 ? 5 : 1);
+  constexpr int NT = CO / 8;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int Wp = W + 2, W2 = W / 2, H2 = H / 2;
+  const int ntx = W / 8, ntiles = H2 * ntx;
+  float bia[NT][2];
+#pragma unroll
+  for (int j = 0; j < NT; j++) {
+    bia[j][0] = bias[8 * j + 2 * t];
+    bia[j][1] = bias[8 * j + 2 * t + 1];
+  }
+  for (int tile = warp; tile < ntiles; tile += kWarps) {
+    const int ty = tile / ntx, tx = tile % ntx;
+    // pixel rows of the MMA tile: row g -> (2ty, 8tx + g), row g + 8 -> (2ty + 1, 8tx + g);
+    // padded index of pixel (y, x) at tap (ky, kx) = (y + ky) * Wp + x + kx
+    const int p0 = (2 * ty) * Wp + 8 * tx + g;
+    const int p1 = p0 + Wp;
+    float acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+#pragma unroll
+    for (int s = 0; s < KS; s++) {
+      uint32_t a[4];
+      if (CI == 16) {
+        const int o = (s / 3) * Wp + (s % 3);
+        a[0] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o) * CI + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o) * CI + 2 * t);
+        a[2] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o) * CI + 2 * t + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o) * CI + 2 * t + 8);
+      } else if (CI == 8) {
+        const int j0 = 2 * s, j1 = 2 * s + 1;
+        const int o0 = (j0 / 3) * Wp + (j0 % 3);
+        a[0] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o0) * CI + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o0) * CI + 2 * t);
+        if (j1 < 9) {
+          const int o1 = (j1 / 3) * Wp + (j1 % 3);
+          a[2] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o1) * CI + 2 * t);
+          a[3] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o1) * CI + 2 * t);
+        } else {
+          a[2] = a[3] = 0u;
+        }
+      } else {
+        // K = tap; taps 2t, 2t + 1 and (t = 0 only) tap 8
+        const int ta = 2 * t, tb = 2 * t + 1;
+        const int oa = (ta / 3) * Wp + (ta % 3), ob = (tb / 3) * Wp + (tb % 3);
+        a[0] = pack2(in[p0 + oa], in[p0 + ob]);
+        a[1] = pack2(in[p1 + oa], in[p1 + ob]);
+        const bf16 z = __float2bfloat16(0.f);
+        const int o8 = 2 * Wp + 2;
+        a[2] = t == 0 ? pack2(in[p0 + o8], z) : 0u;
+        a[3] = t == 0 ? pack2(in[p1 + o8], z) : 0u;
+      }
+#pragma unroll
+      for (int j = 0; j < NT; j++) {
+        const uint2 b = wf[(s * NT + j) * 32 + lane];
+        const uint32_t bb[2] = {b.x, b.y};
+        mma_bf16(acc[j], a, bb);
+      }
+    }
+    // epilogue: c0 (row g, co 2t), c1 (row g, co 2t+1), c2/c3 the same for row g + 8
+    const int py = ty, px = 4 * tx + (g >> 1);
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+      float m0 = fmaxf(fmaxf(acc[j][0] + bia[j][0], 0.f), fmaxf(acc[j][2] + bia[j][0], 0.f));
+      float m1 = fmaxf(fmaxf(acc[j][1] + bia[j][1], 0.f), fmaxf(acc[j][3] + bia[j][1], 0.f));
+      m0 = fmaxf(m0, __shfl_xor_sync(0xffffffffu, m0, 4));
+      m1 = fmaxf(m1, __shfl_xor_sync(0xffffffffu, m1, 4));
+      if ((g & 1) == 0) {
+        const int co = 8 * j + 2 * t;
+        if (feat) {
+          feat[(size_t)co * (H2 * W2) + py * W2 + px] = __float2bfloat16(m0);
+          feat[(size_t)(co + 1) * (H2 * W2) + py * W2 + px] = __float2bfloat16(m1);
+        } else {
+          *reinterpret_cast<uint32_t*>(out + ((size_t)(py + 1) * (W2 + 2) + px + 1) * CO + co) =
+              pack2(__float2bfloat16(m0), __float2bfloat16(m1));
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_clf_infer(Args a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  bf16* r0 = reinterpret_cast<bf16*>(smem);
+  bf16* r1 = reinterpret_cast<bf16*>(smem + kR0);
+  bf16* feat = reinterpret_cast<bf16*>(smem + kR0 + kR1);
+  uint2* wf = reinterpret_cast<uint2*>(smem + kR0 + kR1 + kF);
+  float* hid = reinterpret_cast<float*>(smem + kR0 + kR1 + kF + kWF);
+  // weight fragments of both branches, once per CTA
+  for (int br = 0; br < 2; br++) {
+    uint2* f = wf + br * kFragBranch;
+    build_frags<1, 8>(a.w + a.off_w[br][0], f);
+    build_frags<8, 16>(a.w + a.off_w[br][1], f + kFragL1);
+    build_frags<16, 32>(a.w + a.off_w[br][2], f + kFragL1 + kFragL2);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int cand = blockIdx.x; cand < a.n; cand += gridDim.x) {
+    __syncthreads();  // fragments ready / previous candidate's FC done
+    // ---- branch B (freq-time, 64 x 256): features 2048.. ----
+    const uint2* fB = wf + kFragBranch;
+    load_input(a.ft + (size_t)cand * 16384, 256, r0);
+    zero_ring(r1, 32, 128, 8);
+    __syncthreads();
+    conv_layer<1, 8>(r0, 64, 256, fB, a.w + a.off_b[1][0], r1, nullptr);
+    __syncthreads();
+    zero_ring(r0, 16, 64, 16);
+    conv_layer<8, 16>(r1, 32, 128, fB + kFragL1, a.w + a.off_b[1][1], r0, nullptr);
+    __syncthreads();
+    conv_layer<16, 32>(r0, 16, 64, fB + kFragL1 + kFragL2, a.w + a.off_b[1][2], nullptr,
+                       feat + 2048);
+    __syncthreads();
+    // ---- branch A (DM-time, 64 x 64): features 0..2047 ----
+    const uint2* fA = wf;
+    load_input(a.dm + (size_t)cand * 4096, 64, r1);
+    zero_ring(r0, 32, 32, 8);
+    __syncthreads();
+    conv_layer<1, 8>(r1, 64, 64, fA, a.w + a.off_b[0][0], r0, nullptr);
+    __syncthreads();
+    zero_ring(r1, 16, 16, 16);
+    conv_layer<8, 16>(r0, 32, 32, fA + kFragL1, a.w + a.off_b[0][1], r1, nullptr);
+    __syncthreads();
+    conv_layer<16, 32>(r1, 16, 16, fA + kFragL1 + kFragL2, a.w + a.off_b[0][2], nullptr, feat);
+    __syncthreads();
+    // ---- FC1: warp o computes hidden unit o ----
+    {
+      const int o = warp;
+      const uint4* wrow = reinterpret_cast<const uint4*>(a.wb1 + (size_t)o * 10240);
+      const uint4* x = reinterpret_cast<const uint4*>(feat);
+      float sum = 0.f;
+      for (int i = lane; i < 10240 / 8; i += 32) {
+        const uint4 wv = wrow[i], xv = x[i];
+        const uint32_t wa[4] = {wv.x, wv.y, wv.z, wv.w}, xa[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const float2 wf2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&wa[q]));
+          const float2 xf2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&xa[q]));
+          sum = __fadd_rn(sum, __fmul_rn(wf2.x, xf2.x));
+          sum = __fadd_rn(sum, __fmul_rn(wf2.y, xf2.y));
+        }
+      }
+#pragma unroll
+      for (int off = 16; off; off >>= 1) sum = __fadd_rn(sum, __shfl_xor_sync(0xffffffffu, sum, off));
+      if (lane == 0) hid[o] = fmaxf(sum + a.w[a.off_b1 + o], 0.f);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const float* w2 = a.w + a.off_w2;
+      const float* b2 = a.w + a.off_b2;
+      float l0 = b2[0], l1 = b2[1];
+      for (int o = 0; o < 16; o++) {
+        l0 += w2[o] * hid[o];
+        l1 += w2[16 + o] * hid[o];
+      }
+      const float mx = fmaxf(l0, l1);
+      const float e0 = expf(l0 - mx), e1 = expf(l1 - mx);
+      a.prob[cand] = e1 / (e0 + e1);
+    }
+  }
+}
+}  // namespace inf
+
+// ===========================================================================
 // Candidate patches (Applications/candidate_profiler.C)
 // ===========================================================================
 // DM-time: row r = DM trial dm - 32 + r (zero outside 0..D-1), column t = the
@@ -398,28 +674,33 @@ __global__ void k_patch_dm(const float* __restrict__ scan, size_t scan_pitch, si
 // bytes): 64 sub-bands of fs = nchans/64 channels x 256 bins of ts samples
 // from first; each pixel the float sum, time outer and channel inner, of
 // x / 255 * 255 divided by ts * fs; samples outside the gulp read as 0.
-__global__ void k_patch_ft(const uint8_t* __restrict__ tf, size_t nsamps, int nchans,
-                           const PatchJob* __restrict__ jobs, float* __restrict__ out) {
+// x / 255 * 255 comes from a 256-entry table of the same rounded operations;
+// rows outside the gulp are skipped (they add +0 to a sum that is >= +0, which
+// leaves it unchanged).  Grid: x = candidate, y = 64 groups of 4 time bins;
+// block = 4 bins x 64 sub-bands, so a warp reads 32 adjacent sub-bands of one
+// row.
+__global__ void __launch_bounds__(256) k_patch_ft(const uint8_t* __restrict__ tf, size_t nsamps,
+                                                  int nchans, const PatchJob* __restrict__ jobs,
+                                                  float* __restrict__ out) {
+  __shared__ float lut[256];
+  lut[threadIdx.x] = __fmul_rn(__fdiv_rn((float)threadIdx.x, 255.f), 255.f);
+  __syncthreads();
   const PatchJob jb = jobs[blockIdx.x];
   const int fs = nchans / 64;
-  const uint8_t* fb = tf + (size_t)jb.unit * nsamps * nchans;
-  float* o = out + (size_t)blockIdx.x * 16384;
-  const float npix = (float)((size_t)jb.ft_ts * (size_t)fs);
-  for (int e = threadIdx.x; e < 16384; e += blockDim.x) {
-    const int cs = e / 256, ti = e % 256;
-    const long long t0 = jb.ft_first + (long long)ti * jb.ft_ts;
-    float sum = 0.f;
-    for (unsigned sidx = 0; sidx < jb.ft_ts; sidx++) {
-      const long long t = t0 + sidx;
-      const bool in = t >= 0 && t < (long long)nsamps;
-      const uint8_t* row = fb + (in ? (size_t)t * nchans : 0) + (size_t)cs * fs;
-      for (int f = 0; f < fs; f++) {
-        const float x = in ? (float)row[f] : 0.f;
-        sum = __fadd_rn(sum, __fmul_rn(__fdiv_rn(x, 255.f), 255.f));
-      }
-    }
-    o[e] = __fdiv_rn(sum, npix);
+  const int cs = threadIdx.x & 63;
+  const int ti = blockIdx.y * 4 + (threadIdx.x >> 6);
+  const uint8_t* fb = tf + (size_t)jb.unit * nsamps * nchans + (size_t)cs * fs;
+  const long long t0 = jb.ft_first + (long long)ti * jb.ft_ts;
+  const long long lo = t0 > 0 ? t0 : 0;
+  const long long end = t0 + (long long)jb.ft_ts;
+  const long long hi = end < (long long)nsamps ? end : (long long)nsamps;
+  float sum = 0.f;
+  for (long long t = lo; t < hi; t++) {
+    const uint8_t* row = fb + (size_t)t * nchans;
+    for (int f = 0; f < fs; f++) sum = __fadd_rn(sum, lut[row[f]]);
   }
+  const float npix = (float)((size_t)jb.ft_ts * (size_t)fs);
+  out[(size_t)blockIdx.x * 16384 + cs * 256 + ti] = __fdiv_rn(sum, npix);
 }
 
 // k-th smallest (0-based) of v[lo..hi) in shared memory, by ranks
@@ -475,7 +756,7 @@ cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, co
                             float* dm_out, float* ft_out, cudaStream_t s) {
   if (njobs <= 0) return cudaSuccess;
   k_patch_dm<<<njobs, 256, 0, s>>>(scan, scan_pitch, len, jobs, dm_out); note_launch();
-  k_patch_ft<<<njobs, 256, 0, s>>>(tf, nsamps, nchans, jobs, ft_out); note_launch();
+  k_patch_ft<<<dim3((unsigned)njobs, 64), 256, 0, s>>>(tf, nsamps, nchans, jobs, ft_out); note_launch();
   const size_t r1 = (size_t)njobs * 64;
   k_normalise_rows<<<clf::nblk(r1, 4), 128, 4 * 2 * 64 * sizeof(float), s>>>(dm_out, 64, r1); note_launch();
   k_normalise_rows<<<clf::nblk(r1, 4), 128, 4 * 2 * 256 * sizeof(float), s>>>(ft_out, 256, r1); note_launch();
@@ -532,9 +813,15 @@ struct hd_classifier_t {
   DBuf in[2], col, z, act[2][3], arg[2][3], dz, dcol, dact_a[2], dact_b[2], x, z1, h, dz1,
       dx, prob, loss, labels, idx;
   DBuf data_dm, data_ft, data_lab;  // resident training set
+  DBuf stage_dm, stage_ft, sprob;    // scoring: host patches staged in FP32, scores
+  int nsm = 0;
   size_t data_n = 0;
+  cudaEvent_t ev[2] = {};  // around the last scoring call, on `stream`
+  float score_ms = 0.f;
 
   ~hd_classifier_t() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -700,6 +987,71 @@ cudaError_t upload_patches(hd_classifier c, const float* dm, const float* ft, in
   return cudaGetLastError();
 }
 
+// The fused inference kernel over n device FP32 patch pairs -> d_prob.
+cudaError_t infer(hd_classifier c, const float* d_dm, const float* d_ft, size_t n, float* d_prob) {
+  cudaStream_t s = c->stream;
+  if (n > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+  CK(refresh_bf16(c));
+  if (c->nsm == 0) {
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
+    CK(cudaFuncSetAttribute(hdb::inf::k_clf_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)hdb::inf::kSmem));
+  }
+  hdb::inf::Args a{};
+  a.dm = d_dm;
+  a.ft = d_ft;
+  a.n = (int)n;
+  a.w = c->w.as<float>();
+  for (int br = 0; br < 2; br++)
+    for (int l = 0; l < 3; l++) {
+      a.off_w[br][l] = (int)c->off_w[br][l];
+      a.off_b[br][l] = (int)c->off_b[br][l];
+    }
+  a.off_b1 = (int)c->off_b1;
+  a.off_w2 = (int)c->off_w2;
+  a.off_b2 = (int)c->off_b2;
+  a.wb1 = c->wb1.as<bf16>();
+  a.prob = d_prob;
+  const unsigned grid = (unsigned)std::min<size_t>(n, (size_t)c->nsm);
+  hdb::inf::k_clf_infer<<<grid, hdb::inf::kThreads, hdb::inf::kSmem, s>>>(a); hdb::note_launch();
+  return cudaGetLastError();
+}
+
+// Scores of n patch pairs (device FP32, or host FP32 staged in chunks); after
+// `after` (an event on another stream, or null) when the patches come from
+// that stream.  Device time between the events ev[0] and ev[1].
+constexpr size_t kStageChunk = 2048;
+cudaError_t score_batches(hd_classifier c, const float* dm, const float* ft, size_t n,
+                          bool on_device, cudaEvent_t after, float* scores) {
+  cudaStream_t s = c->stream;
+  if (after) CK(cudaStreamWaitEvent(s, after, 0));
+  CK(cudaEventRecord(c->ev[0], s));
+  if (on_device) {
+    CK(c->sprob.ensure(n * sizeof(float)));
+    CK(infer(c, dm, ft, n, c->sprob.as<float>()));
+    CK(cudaMemcpyAsync(scores, c->sprob.p, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+  } else {
+    const size_t ch = std::min(n, kStageChunk);
+    CK(c->stage_dm.ensure(ch * 4096 * sizeof(float)));
+    CK(c->stage_ft.ensure(ch * 16384 * sizeof(float)));
+    CK(c->sprob.ensure(ch * sizeof(float)));
+    for (size_t i0 = 0; i0 < n; i0 += ch) {
+      // the staging buffers are reused by the next chunk, whose copies are
+      // ordered after this chunk's kernel on the same stream
+      const size_t k = std::min(ch, n - i0);
+      CK(cudaMemcpyAsync(c->stage_dm.p, dm + i0 * 4096, k * 4096 * sizeof(float),
+                         cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(c->stage_ft.p, ft + i0 * 16384, k * 16384 * sizeof(float),
+                         cudaMemcpyHostToDevice, s));
+      CK(infer(c, c->stage_dm.as<float>(), c->stage_ft.as<float>(), k, c->sprob.as<float>()));
+      CK(cudaMemcpyAsync(scores + i0, c->sprob.p, k * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+  }
+  CK(cudaEventRecord(c->ev[1], s));
+  CK(cudaStreamSynchronize(s));
+  return cudaEventElapsedTime(&c->score_ms, c->ev[0], c->ev[1]);
+}
+
 hd_error to_hd(cudaError_t e) {
   if (e == cudaSuccess) return HD_NO_ERROR;
   if (e == cudaErrorMemoryAllocation) return HD_MEM_ALLOC_FAILED;
@@ -724,7 +1076,8 @@ hd_error hd_classifier_create(hd_classifier* out, int gpu_id, unsigned long long
   hd_classifier c = new (std::nothrow) hd_classifier_t();
   if (!c) return HD_MEM_ALLOC_FAILED;
   c->device = gpu_id;
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev[0]) != cudaSuccess || cudaEventCreate(&c->ev[1]) != cudaSuccess) {
     delete c;
     return HD_PRIOR_GPU_ERROR;
   }
@@ -888,18 +1241,23 @@ hd_error hd_classifier_score(hd_classifier c, const float* dm_time, const float*
   if (!dm_time || !freq_time || !scores) return HD_INVALID_POINTER;
   if (n == 0) return HD_NO_ERROR;
   cudaSetDevice(c->device);
-  cudaStream_t s = c->stream;
-  const int nb = (int)std::min<size_t>(n, 512);
-  cudaError_t e = alloc_batch(c, nb);
-  for (size_t i0 = 0; i0 < n && e == cudaSuccess; i0 += (size_t)nb) {
-    const int k = (int)std::min<size_t>(nb, n - i0);
-    e = upload_patches(c, dm_time + i0 * 4096, freq_time + i0 * 16384, k);
-    if (e == cudaSuccess) e = run_batch(c, k, false);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(scores + i0, c->prob.p, k * sizeof(float), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  }
-  return to_hd(e);
+  return to_hd(score_batches(c, dm_time, freq_time, n, false, nullptr, scores));
+}
+
+hd_error hd_classifier_score_device(hd_classifier c, const float* d_dm_time,
+                                    const float* d_freq_time, hd_size n, float* scores) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!d_dm_time || !d_freq_time || !scores) return HD_INVALID_POINTER;
+  if (n == 0) return HD_NO_ERROR;
+  cudaSetDevice(c->device);
+  return to_hd(score_batches(c, d_dm_time, d_freq_time, n, true, nullptr, scores));
+}
+
+hd_error hd_classifier_get_timing(hd_classifier c, float* ms) {
+  if (!c) return HD_INVALID_PIPELINE;
+  if (!ms) return HD_INVALID_POINTER;
+  *ms = c->score_ms;
+  return HD_NO_ERROR;
 }
 
 hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long long sak,
@@ -914,3 +1272,12 @@ hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long 
 }
 
 }  // extern "C"
+
+namespace hdb {
+cudaError_t classifier_score_device(hd_classifier c, const float* d_dm, const float* d_ft,
+                                    size_t n, cudaEvent_t after, float* scores) {
+  if (n == 0) return cudaSuccess;
+  return score_batches(c, d_dm, d_ft, n, true, after, scores);
+}
+int classifier_device(hd_classifier c) { return c->device; }
+}  // namespace hdb

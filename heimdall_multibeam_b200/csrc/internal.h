@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+struct hd_classifier_t;
+
 namespace hdb {
 
 // Kernel launches made by this library in this process (additive counter,
@@ -209,5 +211,12 @@ struct PatchJob {
 cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, const uint8_t* tf,
                             size_t nsamps, int nchans, const PatchJob* jobs, int njobs,
                             float* dm_out, float* ft_out, cudaStream_t s);
+
+// Scores of n device-resident patch pairs with the classifier, after `after`
+// (an event recorded where the patches were written); scores to host memory.
+cudaError_t classifier_score_device(struct ::hd_classifier_t* c, const float* d_dm,
+                                    const float* d_ft, size_t n, cudaEvent_t after,
+                                    float* scores);
+int classifier_device(struct ::hd_classifier_t* c);
 
 }  // namespace hdb

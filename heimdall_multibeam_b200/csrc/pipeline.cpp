@@ -772,14 +772,10 @@ hd_error hd_get_beam_candidates(hd_pipeline pl, hd_size index, hd_candidate* out
   return HD_NO_ERROR;
 }
 
-hd_error hd_extract_patches(hd_pipeline pl, hd_float* dm_time, hd_float* freq_time,
-                            hd_size* count) {
-  if (!pl) return HD_INVALID_PIPELINE;
-  if (!count) return HD_INVALID_POINTER;
-  const size_t n = pl->cands.size();
-  const size_t k = std::min(*count, n);
-  *count = n;
-  if (k == 0 || (!dm_time && !freq_time)) return HD_NO_ERROR;
+namespace {
+// Patches of the first k candidates of the last gulp into pl->patch_dm /
+// pl->patch_ft (device), on the pipeline's stream.
+hd_error patches_on_device(hd_pipeline pl, size_t k) {
   const size_t C = pl->params.nchans;
   if (!pl->searched || C % 64 != 0) return HD_INVALID_STRIDE;
   if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
@@ -820,6 +816,21 @@ hd_error hd_extract_patches(hd_pipeline pl, hd_float* dm_time, hd_float* freq_ti
                               pl->fb_tf.as<uint8_t>(), pl->last_nsamps, (int)C,
                               pl->patch_jobs.as<hdb::PatchJob>(), (int)k,
                               pl->patch_dm.as<float>(), pl->patch_ft.as<float>(), s));
+  return HD_NO_ERROR;
+}
+}  // namespace
+
+hd_error hd_extract_patches(hd_pipeline pl, hd_float* dm_time, hd_float* freq_time,
+                            hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!count) return HD_INVALID_POINTER;
+  const size_t n = pl->cands.size();
+  const size_t k = std::min(*count, n);
+  *count = n;
+  if (k == 0 || (!dm_time && !freq_time)) return HD_NO_ERROR;
+  hd_error he = patches_on_device(pl, k);
+  if (he != HD_NO_ERROR) return he;
+  cudaStream_t s = pl->stream;
   if (dm_time)
     HD_TRY(cudaMemcpyAsync(dm_time, pl->patch_dm.p, k * HD_PATCH_DM_TIME * sizeof(float),
                            cudaMemcpyDeviceToHost, s));
@@ -827,6 +838,27 @@ hd_error hd_extract_patches(hd_pipeline pl, hd_float* dm_time, hd_float* freq_ti
     HD_TRY(cudaMemcpyAsync(freq_time, pl->patch_ft.p, k * HD_PATCH_FREQ_TIME * sizeof(float),
                            cudaMemcpyDeviceToHost, s));
   HD_TRY(cudaStreamSynchronize(s));
+  return HD_NO_ERROR;
+}
+
+hd_error hd_score_candidates(hd_pipeline pl, hd_classifier clf, hd_float* scores,
+                             hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!clf) return HD_INVALID_PIPELINE;
+  if (!count) return HD_INVALID_POINTER;
+  const size_t n = pl->cands.size();
+  const size_t k = std::min(*count, n);
+  *count = n;
+  if (k == 0) return HD_NO_ERROR;
+  if (!scores) return HD_INVALID_POINTER;
+  if (hdb::classifier_device(clf) != pl->device) return HD_INVALID_DEVICE_INDEX;
+  hd_error he = patches_on_device(pl, k);
+  if (he != HD_NO_ERROR) return he;
+  // the classifier's stream waits for the patches; nothing leaves the device
+  // but the scores
+  HD_TRY(cudaEventRecord(pl->ev[8], pl->stream));
+  HD_TRY(hdb::classifier_score_device(clf, pl->patch_dm.as<float>(), pl->patch_ft.as<float>(),
+                                      k, pl->ev[8], scores));
   return HD_NO_ERROR;
 }
 

@@ -258,6 +258,20 @@ hd_error hd_classifier_train(hd_classifier classifier, const hd_float* dm_time,
 /* Probability of a dispersed pulse for each of n patches. */
 hd_error hd_classifier_score(hd_classifier classifier, const hd_float* dm_time,
                              const hd_float* freq_time, hd_size n, hd_float* scores);
+/* The same with the patches in device memory of the classifier's GPU
+ * (n x HD_PATCH_DM_TIME and n x HD_PATCH_FREQ_TIME floats); scores to host. */
+hd_error hd_classifier_score_device(hd_classifier classifier, const hd_float* d_dm_time,
+                                    const hd_float* d_freq_time, hd_size n, hd_float* scores);
+/* Scores of the candidates of the last hd_execute / hd_execute_beams, in
+ * hd_get_candidates order: patches are extracted and scored on the GPU (the
+ * pipeline and the classifier must share it) and only the scores are copied
+ * back.  Writes min(*count, available) scores and sets *count to the number
+ * available.  The candidate list is not changed. */
+hd_error hd_score_candidates(hd_pipeline pipeline, hd_classifier classifier, hd_float* scores,
+                             hd_size* count);
+/* Device time (ms, CUDA events on the classifier's stream) of the last
+ * scoring call, from its first upload or conversion to its last score copy. */
+hd_error hd_classifier_get_timing(hd_classifier classifier, hd_float* ms);
 /* The classifier's GEMM on device operands, for testing: C (m x n, FP32) =
  * A (m x k, BF16) x B (k x n, BF16) with element strides A(i, l) =
  * A[i*sam + l*sak], B(l, j) = B[l*sbk + j*sbn], C(i, j) = C[i*scm + j*scn];

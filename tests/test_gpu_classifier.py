@@ -69,6 +69,32 @@ def test_patches_match_oracle(hdb, oracle_lib):
         np.testing.assert_array_equal(ft[i], oracle.patch_ft(b.data, md, ind, f), err_msg=f"ft {i}")
 
 
+def test_score_candidates_matches_host_path(hdb):
+    """hd_score_candidates (patches extracted and scored on the GPU) gives the
+    same scores as hd_extract_patches + hd_classifier_score through host
+    memory, and hd_classifier_score_device the same on device patches."""
+    w = synth.SEARCH_C0
+    b = synth.make_c0()
+    kw = dict(dt=w.dt, f0=w.f0, df=w.df, dm_min=w.dm_min, dm_max=w.dm_max,
+              boxcar_max=w.boxcar_max)
+    with H.Pipeline(H.default_params(nchans=w.nchans, output_dir=None, **kw), cleaning=False) as pl, \
+            H.Classifier(seed=7) as clf:
+        pl.execute(b.data)
+        n = len(pl.candidates())
+        assert n >= 3
+        fused = pl.scores(clf)
+        dm, ft = pl.patches()
+        host = clf.score(dm, ft)
+        ddm = torch.from_numpy(dm).cuda()
+        dft = torch.from_numpy(ft).cuda()
+        torch.cuda.synchronize()
+        dev = clf.score_device(ddm.data_ptr(), dft.data_ptr(), n)
+    assert fused.shape == (n,)
+    np.testing.assert_array_equal(fused, host)
+    np.testing.assert_array_equal(dev, host)
+    assert np.all((fused >= 0) & (fused <= 1))
+
+
 def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
 
