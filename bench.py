@@ -301,6 +301,9 @@ def run_product(args):
     if not args.batched_only and not args.no_classifier:
         clf_rec = classifier_bench(args, H, torch, dev, pl)
     pl.close()
+    uneven = None
+    if args.workload == "multibeam" and not args.batched_only and args.uneven_beams > 0:
+        uneven = uneven_bench(args, H, torch, dev, barrier, dist, world)
     # secondary: the plain survey-size single-beam gulp
     survey = None
     if args.workload == "multibeam" and not args.no_survey and not args.batched_only:
@@ -381,6 +384,8 @@ def run_product(args):
             rec["survey_plain"] = survey
         if clf_rec is not None:
             rec["classifier"] = clf_rec
+        if uneven is not None:
+            rec["uneven"] = uneven
         if not args.no_cpu_baseline:
             rec["cpu_baseline"] = cpu_baseline(args, wk)
         print(json.dumps(rec), flush=True)
@@ -448,6 +453,84 @@ def classifier_bench(args, H, torch, dev, pl):
                     "persistent fused kernel (k_clf_infer, one CTA per SM): mma.sync BF16 "
                     "convolutions with FP32 accumulation, FC layers in the same kernel"}
     return out
+
+
+def uneven_bench(args, H, torch, dev, barrier, dist, world):
+    """Beams of different shapes (channel counts 128/512/2048/4096, 64/128 us,
+    gulp lengths uniform in [2^14, nsamps_max], DM ranges 0-500/2000/5000 as
+    fit) from device memory: the plain per-beam loop (one pipeline per
+    configuration, hd_execute_device beam by beam) against one
+    hd_execute_beam_set call.  Data: Gaussian noise (128, 16) with the
+    survey beam's RFI (5 % of channels at +40 sd, zero-DM bursts of 1-50
+    samples at +8 sd), generated on the GPU; injected-pulse recall is covered
+    by the parity tests."""
+    from heimdall_multibeam_b200 import synth
+    ws = synth.uneven_shapes(args.uneven_beams, nsamps_range=(1 << 14, args.uneven_nsamps_max))
+    g = torch.Generator(device=dev).manual_seed(2027)
+    data = []
+    for b, w in enumerate(ws):
+        x = torch.randn((w.nsamps, w.nchans), generator=g, device=dev) * 16.0 + 128.0
+        bad = torch.randperm(w.nchans, generator=g, device=dev)[: max(1, w.nchans // 20)]
+        x[:, bad] += 640.0
+        frac = w.nsamps * w.dt / ((1 << 18) * 64e-6)
+        for _ in range(max(1, int(round(10 * frac)))):
+            t0 = int(torch.randint(0, w.nsamps - 50, (1,), generator=g, device=dev))
+            wd = int(torch.randint(1, 51, (1,), generator=g, device=dev))
+            x[t0:t0 + wd, :] += 128.0
+        data.append(x.round_().clamp_(0, 255).to(torch.uint8))
+        del x
+    torch.cuda.synchronize(dev)
+    params = []
+    for b, w in enumerate(ws):
+        p = params_for(H, w)
+        p.gpu_id = dev.index
+        p.beam = b
+        params.append(p)
+    ptrs = [d.data_ptr() for d in data]
+    ns = [w.nsamps for w in ws]
+    beam_s = sum(w.nsamps * w.dt for w in ws)
+    steps = max(1, args.uneven_steps)
+    # plain per-beam loop
+    pls = {}
+    for w, p in zip(ws, params):
+        key = (w.nchans, w.dt, w.dm_max)
+        if key not in pls:
+            pls[key] = H.Pipeline(p, cleaning=True)
+
+    def plain():
+        for w, ptr in zip(ws, ptrs):
+            pls[(w.nchans, w.dt, w.dm_max)].execute_device(ptr, w.nsamps)
+
+    plain()
+    ms_plain = _timed(torch, dev, barrier, steps, plain)
+    for pl in pls.values():
+        pl.close()
+    pls.clear()
+    # one call for all beams
+    with H.BeamSet(params, workers=args.uneven_workers, cleaning=True) as bs:
+        def batched():
+            err, _, _ = bs.execute(ptrs, nsamps=ns, on_device=True)
+            assert err in (H.HD_NO_ERROR, H.HD_TOO_MANY_EVENTS, H.HD_TOO_FEW_NSAMPS), err
+        batched()
+        ms_set = _timed(torch, dev, barrier, steps, batched)
+        nconf = bs.nconfigs
+        ncand = sum(len(bs.candidates(b)) for b in range(len(ws)))
+    tmax = torch.tensor([ms_plain, ms_set], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    ms_plain, ms_set = float(tmax[0]), float(tmax[1])
+    return {"workload": f"uneven_{len(ws)}x_c128-4096_n16384-{args.uneven_nsamps_max}",
+            "nbeams": len(ws), "configurations": nconf,
+            "input_gib": round(sum(w.nchans * w.nsamps for w in ws) / 2**30, 3),
+            "beam_seconds": round(beam_s, 3), "steps": steps,
+            "beam_set": {"value": round(world * beam_s / (ms_set / 1e3), 3), "unit": UNIT,
+                         "ms_per_step": round(ms_set, 3), "workers": args.uneven_workers,
+                         "api": "hd_execute_beam_set"},
+            "plain": {"value": round(world * beam_s / (ms_plain / 1e3), 3), "unit": UNIT,
+                      "ms_per_step": round(ms_plain, 3),
+                      "form": "one pipeline per configuration, hd_execute_device per beam"},
+            "set_over_plain": round(ms_plain / ms_set, 3), "candidates": ncand,
+            "data": "GPU-generated noise + RFI (no injections)"}
 
 
 def survey_plain(args, H, torch, dev, barrier, dist, world):
@@ -595,6 +678,12 @@ def main():
                     help="beams of the multibeam gulp (fewer are for profiling)")
     ap.add_argument("--batched-only", action="store_true",
                     help="time only the batched form (profiling)")
+    ap.add_argument("--uneven-beams", type=int, default=64,
+                    help="beams of the uneven-beam section (0 skips it; 256 is the full size)")
+    ap.add_argument("--uneven-nsamps-max", type=int, default=1 << 16,
+                    help="longest gulp of the uneven-beam section (2^17 at full size)")
+    ap.add_argument("--uneven-workers", type=int, default=4)
+    ap.add_argument("--uneven-steps", type=int, default=2)
     ap.add_argument("--no-classifier", action="store_true",
                     help="skip the classifier inference measurement")
     ap.add_argument("--no-survey", action="store_true",

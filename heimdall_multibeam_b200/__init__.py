@@ -132,6 +132,13 @@ SYMBOLS = {
     "hd_execute_beams": (C.c_int, [_P, C.POINTER(_P), _SZ, _SZ, _SZ, _SZ, _SZ, _SZP, C.c_int,
                                    C.POINTER(C.c_int), _SZP]),
     "hd_get_beam_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
+    "hd_create_beam_set": (C.c_int, [C.POINTER(_P), C.c_void_p, _SZ, C.c_int]),
+    "hd_set_beam_set_cleaning": (C.c_int, [_P, C.c_int]),
+    "hd_get_beam_set_config_count": (_SZ, [_P]),
+    "hd_execute_beam_set": (C.c_int, [_P, C.POINTER(_P), _SZP, _SZ, _SZ, C.c_int,
+                                      C.POINTER(C.c_int), _SZP]),
+    "hd_get_beam_set_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
+    "hd_destroy_beam_set": (None, [_P]),
     "hd_get_launch_count": (C.c_ulonglong, []),
     "hd_clean_filterbank_rfi_noalloc": (C.c_int, [_P, _SZ, _SZ, _SZ, _P, _P, C.c_float,
                                                   C.c_float, C.c_float, _SZ, _SZ, _P]),
@@ -494,6 +501,83 @@ def dm_list_guru(dm_min, dm_max, dt, pulse_width, f0, df, nchans, tol) -> np.nda
 
 def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class BeamSet:
+    """hd_create_beam_set / hd_execute_beam_set: beams of different shapes
+    (one HdParams each) searched in one call; beam b's results equal a
+    separate Pipeline(params[b]).execute of its filterbank."""
+
+    def __init__(self, params: Sequence[HdParams], workers: int = 4, cleaning: bool = True):
+        self._p = None
+        self._params = (HdParams * len(params))(*params)
+        h = C.c_void_p()
+        err = lib().hd_create_beam_set(C.byref(h), C.cast(self._params, C.c_void_p), len(params),
+                                       workers)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_create_beam_set")
+        self._p = h
+        self.nbeams = len(params)
+        lib().hd_set_beam_set_cleaning(self._p, 1 if cleaning else 0)
+
+    @property
+    def nconfigs(self) -> int:
+        return int(lib().hd_get_beam_set_config_count(self._p))
+
+    def close(self) -> None:
+        if self._p:
+            lib().hd_destroy_beam_set(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def execute(self, filterbanks: Sequence, nsamps: Optional[Sequence[int]] = None,
+                first_idx: int = 0, on_device: bool = False) -> Tuple[int, List[int], List[int]]:
+        """filterbanks: uint8 arrays (nsamps_b, nchans_b), or raw pointers
+        (host, or device when on_device) with nsamps given.  Returns
+        (hd_error, per-beam statuses, per-beam nsamps_processed)."""
+        n = self.nbeams
+        if len(filterbanks) != n:
+            raise ValueError(f"{n} filterbanks expected")
+        keep = []
+        ptrs = (_P * n)()
+        ns = (C.c_size_t * n)()
+        for b, fb in enumerate(filterbanks):
+            if isinstance(fb, int):
+                if nsamps is None:
+                    raise ValueError("nsamps is required with raw pointers")
+                ptrs[b] = fb
+                ns[b] = nsamps[b]
+            else:
+                a = _u8(fb)
+                keep.append(a)
+                ptrs[b] = a.ctypes.data
+                ns[b] = a.shape[0] if nsamps is None else nsamps[b]
+        st = (C.c_int * n)()
+        proc = (C.c_size_t * n)()
+        err = lib().hd_execute_beam_set(self._p, ptrs, ns, 8, first_idx, 1 if on_device else 0,
+                                        st, proc)
+        return err, list(st), list(proc)
+
+    def candidates(self, beam: int) -> np.ndarray:
+        n = C.c_size_t(0)
+        err = lib().hd_get_beam_set_candidates(self._p, beam, None, C.byref(n))
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_get_beam_set_candidates")
+        out = np.zeros(n.value, CANDIDATE_DTYPE)
+        if n.value:
+            lib().hd_get_beam_set_candidates(self._p, beam, out.ctypes.data, C.byref(n))
+        return out
 
 
 class Classifier:

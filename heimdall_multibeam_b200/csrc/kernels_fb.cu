@@ -391,28 +391,53 @@ cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* 
 }
 
 namespace {
-constexpr int DD_NW = 8, DD_G = 4, DD_CH = 8, DD_NST = 3;
+constexpr int DD_NW = 8, DD_G = 4, DD_NST = 3;
+// Shared memory of the variant with `ch` channel rows per stage.
+size_t dd_smem(int ch, int rowb) {
+  return 128 + (size_t)DD_NST * 2 * DD_NW * ch * sizeof(int) + (size_t)DD_NST * ch * rowb;
 }
+// Channel rows per stage: the most that keep three CTAs on an SM (72 KB
+// each), else two (110 KB), else one (200 KB).  Rows are long when few
+// channels cover a wide DM range (a DM block's delay span is long).  The
+// sums are exact integers, so the choice does not change the result.
+int dd_rows_per_stage(int rowb) {
+  for (size_t cap : {(size_t)72 * 1024, (size_t)110 * 1024, (size_t)200 * 1024})
+    for (int ch = 8; ch >= 1; ch /= 2)
+      if (dd_smem(ch, rowb) <= cap) return ch;
+  return 0;
+}
+template <int CH>
+cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
+  auto kern = k_dedisp<DD_NW, DD_G, CH, DD_NST>;
+  const size_t smem = dd_smem(CH, a.rowb);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const int DB = 2 * DD_NW, TB = 128 * DD_G;
+  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),
+            (unsigned)a.units);
+  kern<<<grid, (DD_NW + 1) * 32, smem, s>>>(a); note_launch();
+  return cudaGetLastError();
+}
+}  // namespace
 
 int dedisp_dm_block() { return 2 * DD_NW; }
 int dedisp_time_block() { return 128 * DD_G; }
 
 size_t dedisp_smem_bytes(int rowb) {
-  return 128 + (size_t)DD_NST * 2 * DD_NW * DD_CH * sizeof(int) + (size_t)DD_NST * DD_CH * rowb;
+  const int ch = dd_rows_per_stage(rowb);
+  return ch ? dd_smem(ch, rowb) : (size_t)-1;
 }
 
 cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s) {
-  auto kern = k_dedisp<DD_NW, DD_G, DD_CH, DD_NST>;
-  size_t smem = dedisp_smem_bytes(a.rowb);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  const int DB = 2 * DD_NW, TB = 128 * DD_G;
   if (a.units < 1 || a.units > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),
-            (unsigned)a.units);
-  kern<<<grid, (DD_NW + 1) * 32, smem, s>>>(a); note_launch();
-  return cudaGetLastError();
+  switch (dd_rows_per_stage(a.rowb)) {
+    case 8: return launch_dd<8>(a, s);
+    case 4: return launch_dd<4>(a, s);
+    case 2: return launch_dd<2>(a, s);
+    case 1: return launch_dd<1>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace hdb

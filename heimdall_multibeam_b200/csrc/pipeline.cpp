@@ -124,6 +124,8 @@ hd_error dedisp_err(dedisp_error e) {
     case DEDISP_TOO_FEW_NSAMPS: return HD_TOO_FEW_NSAMPS;
     case DEDISP_PRIOR_GPU_ERROR: return HD_PRIOR_GPU_ERROR;
     case DEDISP_INTERNAL_GPU_ERROR: return HD_INTERNAL_GPU_ERROR;
+    // a block's delay span too long for one staged row (dedispersion limit)
+    case DEDISP_NCHANS_EXCEEDS_LIMIT: return HD_INVALID_STRIDE;
     default: return HD_UNKNOWN_ERROR;
   }
 }

@@ -168,6 +168,7 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   a.in_unit = in_unit;
   a.out_unit = out_unit;
   if (units > 65535) return DEDISP_INVALID_STRIDE;
+  // one channel row of the widest block's delay span must fit shared memory
   if (dedisp_smem_bytes(a.rowb) > 200 * 1024) return DEDISP_NCHANS_EXCEEDS_LIMIT;
   if (launch_dedisp(a, s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
   return DEDISP_NO_ERROR;

@@ -205,6 +205,61 @@ def stf(beams: Sequence[Beam]) -> np.ndarray:
 
 
 # ---------------------------------------------------------------------------
+# Uneven beams: channel count, gulp length, sampling time and DM range differ
+# from beam to beam (a 400 MHz band below 1520 MHz split into C channels)
+# ---------------------------------------------------------------------------
+UNEVEN_NCHANS = (128, 512, 2048, 4096)
+UNEVEN_DT = (64e-6, 128e-6)
+UNEVEN_DM_MAX = (500.0, 2000.0, 5000.0)
+UNEVEN_F_TOP, UNEVEN_BW = 1520.0, 400.0
+UNEVEN_BOXCAR_MAX = 1 << 12
+UNEVEN_NSAMPS = (1 << 14, 1 << 17)
+
+
+def uneven_shapes(nbeams: int, seed: int = 2027, nchans: Sequence[int] = UNEVEN_NCHANS,
+                  nsamps_range: Tuple[int, int] = UNEVEN_NSAMPS,
+                  dm_maxes: Sequence[float] = UNEVEN_DM_MAX,
+                  boxcar_max: int = UNEVEN_BOXCAR_MAX) -> List[Workload]:
+    """Per-beam shapes: channel counts in turn from `nchans`, sampling time
+    alternating 64/128 us every len(nchans) beams, gulp length uniform in
+    nsamps_range, and a DM range drawn among those of `dm_maxes` whose
+    largest delay plus the widest boxcar (plus 5 % margin) fits the gulp
+    (the smallest range otherwise; that beam then reports HD_TOO_FEW_NSAMPS
+    or is not searched, as the reference would)."""
+    g = _rng(seed, 0x0E7E)
+    out = []
+    for b in range(nbeams):
+        c = int(nchans[b % len(nchans)])
+        dt = UNEVEN_DT[(b // len(nchans)) % len(UNEVEN_DT)]
+        n = int(g.integers(nsamps_range[0], nsamps_range[1] + 1))
+        df = -UNEVEN_BW / c
+        fits = [d for d in dm_maxes
+                if 1.05 * max_delay_samples(d, c, dt, UNEVEN_F_TOP, df) + boxcar_max < n]
+        dm_max = float(fits[int(g.integers(0, len(fits)))]) if fits else float(min(dm_maxes))
+        out.append(Workload(f"uneven_b{b}_c{c}_n{n}", c, dt, UNEVEN_F_TOP, df, n, 1, 0.0, dm_max,
+                            boxcar_max, True,
+                            f"uneven beam {b}: {c} ch, {dt * 1e6:.0f} us, {n} samples, "
+                            f"DM 0-{dm_max:.0f}"))
+    return out
+
+
+def make_uneven_beam(w: Workload, seed: int = 2027, beam: int = 0, rfi: bool = True) -> Beam:
+    """Noise, injections and RFI as the survey-size beam, scaled to this
+    beam's duration: 20 pulses and 10 zero-DM bursts per 2^18 x 64 us
+    (at least one each; DM 50..dm_max, FWHM 0.1-30 ms, S/N 6-50) and 5 % of
+    the channels persistently at +40 sd."""
+    g = _rng(seed, 0x0E7E00 + beam)
+    frac = w.nsamps * w.dt / ((1 << 18) * 64e-6)
+    md = max_delay_samples(w.dm_max, w.nchans, w.dt, w.f0, w.df)
+    hi = max(w.nsamps - md - 2 * w.boxcar_max, w.boxcar_max + 1)
+    pulses = random_pulses(g, max(1, int(round(20 * frac))), w.boxcar_max, hi,
+                           min(50.0, w.dm_max), w.dm_max, 0.1e-3, 30e-3, 6.0, 50.0)
+    return make_beam(w.nsamps, w.nchans, w.dt, w.f0, w.df, pulses, seed=seed, beam=beam,
+                     rfi_chan_frac=0.05 if rfi else 0.0,
+                     n_bursts=max(1, int(round(10 * frac))) if rfi else 0, rng=g)
+
+
+# ---------------------------------------------------------------------------
 # Classifier training data: gulps with injected pulses and labelled RFI
 # ---------------------------------------------------------------------------
 @dataclasses.dataclass

@@ -307,6 +307,34 @@ hd_error hd_get_candidates(hd_pipeline pipeline, hd_candidate* out, hd_size* cou
 hd_error hd_get_beam_candidates(hd_pipeline pipeline, hd_size index, hd_candidate* out,
                                 hd_size* count);
 
+/* Beams of different shapes in one call.  No counterpart in the reference,
+ * which runs one heimdall process (one pipeline) per beam
+ * (Applications/heimdall.C).  params[b] describes beam b (channel count,
+ * sampling time, band, DM range, boxcar_max ...; all on one gpu_id); beam b's
+ * candidates, .cand file and status are those hd_execute gives for
+ * filterbanks[b] (nsamps[b] spectra of one beam, 8-bit) with a pipeline made
+ * from params[b].  Beams are grouped by configuration (every field but
+ * `beam`); runs of equal configuration and gulp length are searched by one
+ * hd_execute_beams, and nworkers host threads, each with its own pipelines
+ * and streams, search runs concurrently on the GPU.  hd_execute_beam_set
+ * returns HD_NO_ERROR, or the status of the lowest-numbered beam that did
+ * not succeed; statuses[b] and nsamps_processed[b] (both may be NULL) give
+ * every beam's.  Filterbanks are host pointers, or device pointers with
+ * on_device != 0. */
+typedef struct hd_beam_set_t* hd_beam_set;
+hd_error hd_create_beam_set(hd_beam_set* set, const struct hd_params* params, hd_size nbeams,
+                            int nworkers);
+hd_error hd_set_beam_set_cleaning(hd_beam_set set, int enable);
+hd_size  hd_get_beam_set_config_count(hd_beam_set set);
+hd_error hd_execute_beam_set(hd_beam_set set, const hd_byte* const* filterbanks,
+                             const hd_size* nsamps, hd_size nbits, hd_size first_idx,
+                             int on_device, hd_error* statuses, hd_size* nsamps_processed);
+/* Candidates of beam `beam` of the last hd_execute_beam_set (copy rules of
+ * hd_get_candidates). */
+hd_error hd_get_beam_set_candidates(hd_beam_set set, hd_size beam, hd_candidate* out,
+                                    hd_size* count);
+void     hd_destroy_beam_set(hd_beam_set set);
+
 /* Every giant of the last hd_execute in detection order (DM, width, time),
  * before clustering, with its cluster label (the index of the cluster's first
  * giant).  After hd_execute_beams: filterbank by filterbank, dm_inds local to

@@ -93,6 +93,34 @@ def test_dedisp_odd_sizes(hdb, oracle_lib):
     np.testing.assert_array_equal(plan.execute(fb), oracle.dedisperse(fb, dms, table))
 
 
+@pytest.mark.parametrize("nchans,dt,dm_max,nsamps,rows", [
+    (128, 128e-6, 2000.0, 26000, 2),   # 6.5 KB staged rows: 2 rows per stage
+    (128, 64e-6, 2000.0, 50000, 1),    # 13 KB rows: 1 row per stage
+    (512, 128e-6, 5000.0, 62000, 4),   # 5 KB rows: 4 rows per stage
+])
+def test_dedisp_long_delay_spans(hdb, oracle_lib, nchans, dt, dm_max, nsamps, rows):
+    """Few channels over a wide DM range (a 400 MHz band below 1520 MHz):
+    the delay span of a 16-trial DM block is thousands of samples, so the
+    staged channel rows are long and the kernel stages fewer rows per
+    stage (`rows`, from the rows' length); the sums stay bit-exact."""
+    rng = np.random.default_rng(nchans + nsamps)
+    fb = rng.integers(0, 256, size=(nsamps, nchans), dtype=np.uint8)
+    df = -400.0 / nchans
+    plan = H.DedispPlan(nchans, dt, 1520.0, df)
+    plan.generate_dm_list(0.0, dm_max, 40.0, 1.25)
+    dms = plan.dm_list
+    table = oracle.delay_table(nchans, dt, 1520.0, df)
+    dl = oracle.delays(dms, table).astype(np.int64)
+    span = max(int((dl[b:b + 16].max(0) - dl[b:b + 16].min(0)).max()) for b in range(0, len(dms), 16))
+    rowb = (span + 16 + 512 + 8 + 15) // 16 * 16
+    smem = [128 + 3 * 16 * ch * 4 + 3 * ch * rowb for ch in (8, 4, 2, 1)]
+    want = next(ch for cap in (72 << 10, 110 << 10, 200 << 10)
+                for ch, sm in zip((8, 4, 2, 1), smem) if sm <= cap)
+    assert want == rows
+    out = plan.execute(fb)
+    np.testing.assert_array_equal(out, oracle.dedisperse(fb, dms, table))
+
+
 def test_clean_bit_exact(hdb, oracle_lib):
     w = synth.SEARCH_C1
     b = synth.make_beam(1 << 15, 64, w.dt, w.f0, w.df * 16,
