@@ -411,7 +411,7 @@ def classifier_bench(args, H, torch, dev, pl):
     peaks, peak_kind = _peaks()
     out = {}
     with H.Classifier(seed=1, gpu_id=dev.index) as clf:
-        n = len(pl.candidates())
+        n = len(pl.candidates()) if pl is not None else 0
         if n:
             for _ in range(2):
                 pl.scores(clf)
@@ -686,6 +686,8 @@ def main():
     ap.add_argument("--uneven-steps", type=int, default=2)
     ap.add_argument("--no-classifier", action="store_true",
                     help="skip the classifier inference measurement")
+    ap.add_argument("--only-classifier", action="store_true",
+                    help="only the classifier throughput (profiling); prints its object")
     ap.add_argument("--no-survey", action="store_true",
                     help="skip the secondary single-beam survey gulp")
     ap.add_argument("--ref-beams", type=int, default=4,
@@ -693,6 +695,14 @@ def main():
     ap.add_argument("--ref-dm1", type=float, default=20.0)
     ap.add_argument("--ref-dm2", type=float, default=60.0)
     args = ap.parse_args()
+    if args.only_classifier:
+        import torch
+        import heimdall_multibeam_b200 as H
+        torch.cuda.set_device(0)
+        print(json.dumps({"classifier": classifier_bench(args, H, torch,
+                                                         torch.device("cuda", 0), None)}),
+              flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
