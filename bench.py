@@ -258,6 +258,7 @@ def run_product(args):
     ms = _timed(torch, dev, barrier, args.steps, batched, stage, pl.timing)
     launches = H.launch_count() - l0
     cands = [pl.candidates(u) for u in range(U)] if U > 1 else [pl.candidates()]
+    tile = pl.dedisp_tile()
 
     # ---- plain per-beam form on the same data ---------------------------------
     ms_plain = None
@@ -348,6 +349,8 @@ def run_product(args):
                        "dt_s": w.dt, "dm_range": [w.dm_min, w.dm_max], "dm_trials": D,
                        "boxcar_max": w.boxcar_max, "clean_filterbank_rfi": bool(w.clean),
                        "beam_seconds_per_gulp": round(wk.beam_s, 4),
+                       "dedisp_tile": {"dm_block": tile[0], "time_block": tile[1],
+                                       "rows_per_stage": tile[2], "chosen_by": "autotuner"},
                        "l2": f"input {U * fb_bytes / 2**20:.0f} MiB > L2, no flush",
                        "parallelism": f"replicas{world}"},
             "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},

@@ -145,6 +145,8 @@ SYMBOLS = {
     "hd_get_candidates": (C.c_int, [_P, _P, _SZP]),
     "hd_get_giants": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _SZP]),
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
+    "hd_get_dedisp_tile": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]),
     "hd_extract_patches": (C.c_int, [_P, _FP, _FP, _SZP]),
     "hd_classifier_param_count": (_SZ, []),
     "hd_classifier_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_ulonglong]),
@@ -398,6 +400,13 @@ class Pipeline:
             if err != HD_NO_ERROR:
                 raise HdError(err, "hd_score_candidates")
         return out
+
+    def dedisp_tile(self) -> Tuple[int, int, int]:
+        """hd_get_dedisp_tile: (DM block, time block, rows per stage) of the
+        last gulp's dedispersion."""
+        v = [C.c_int(0) for _ in range(3)]
+        lib().hd_get_dedisp_tile(self._p, *(C.byref(x) for x in v))
+        return tuple(int(x.value) for x in v)
 
     def timing(self) -> Dict[str, float]:
         t = (C.c_float * 8)()

@@ -34,10 +34,18 @@ struct DedispArgs {
   size_t out_unit;        // floats between units' outputs
 };
 
-int dedisp_dm_block();
-int dedisp_time_block();
-size_t dedisp_smem_bytes(int rowb);
-cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s);
+// Dedispersion tile: DMs and output samples per CTA, channel rows staged per
+// pipeline stage.  Every tile gives the same (exact integer) sums.
+struct DedispTile {
+  int dm_block, time_block, rows;
+};
+constexpr int kDedispDmBlocks[3] = {8, 16, 32};
+// candidate {dm_block, time_block} pairs (32 x 512 would spill registers)
+constexpr int kDedispTiles[5][2] = {{8, 256}, {8, 512}, {16, 256}, {16, 512}, {32, 256}};
+// rows per stage that fit shared memory for staged rows of rowb bytes (0: none)
+int dedisp_rows_per_stage(int dm_block, int rowb);
+size_t dedisp_smem_bytes(int dm_block, int rows, int rowb);
+cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t s);
 // TF -> channel-major copy of `units` filterbanks (nsamps x nchans bytes each,
 // consecutive in `in`); unit u's copy starts at out + u * out_unit.
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,

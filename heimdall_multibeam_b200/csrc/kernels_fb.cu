@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256) k_zap_to_ft(const uint8_t* __restrict__ i
 constexpr uint32_t DD_WAIT_LIMIT = 1u << 22;
 
 template <int NW, int G, int CH, int NST>
-__global__ void __launch_bounds__((NW + 1) * 32, 3) k_dedisp(DedispArgs a) {
+__global__ void __launch_bounds__((NW + 1) * 32, NW >= 16 ? 2 : 3) k_dedisp(DedispArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr int DB = 2 * NW;
   constexpr int TB = 128 * G;
@@ -391,53 +391,59 @@ cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* 
 }
 
 namespace {
-constexpr int DD_NW = 8, DD_G = 4, DD_NST = 3;
-// Shared memory of the variant with `ch` channel rows per stage.
-size_t dd_smem(int ch, int rowb) {
-  return 128 + (size_t)DD_NST * 2 * DD_NW * ch * sizeof(int) + (size_t)DD_NST * ch * rowb;
+constexpr int DD_NST = 3;
+// Shared memory of a variant: DB = dm_block DMs, `ch` channel rows per stage.
+size_t dd_smem(int dm_block, int ch, int rowb) {
+  return 128 + (size_t)DD_NST * dm_block * ch * sizeof(int) + (size_t)DD_NST * ch * rowb;
 }
+template <int NW, int G, int CH>
+cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
+  auto kern = k_dedisp<NW, G, CH, DD_NST>;
+  const size_t smem = dd_smem(2 * NW, CH, a.rowb);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  const int DB = 2 * NW, TB = 128 * G;
+  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),
+            (unsigned)a.units);
+  kern<<<grid, (NW + 1) * 32, smem, s>>>(a); note_launch();
+  return cudaGetLastError();
+}
+template <int NW, int G>
+cudaError_t launch_rows(const DedispArgs& a, int rows, cudaStream_t s) {
+  switch (rows) {
+    case 8: return launch_dd<NW, G, 8>(a, s);
+    case 4: return launch_dd<NW, G, 4>(a, s);
+    case 2: return launch_dd<NW, G, 2>(a, s);
+    case 1: return launch_dd<NW, G, 1>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+}  // namespace
+
 // Channel rows per stage: the most that keep three CTAs on an SM (72 KB
 // each), else two (110 KB), else one (200 KB).  Rows are long when few
 // channels cover a wide DM range (a DM block's delay span is long).  The
 // sums are exact integers, so the choice does not change the result.
-int dd_rows_per_stage(int rowb) {
+int dedisp_rows_per_stage(int dm_block, int rowb) {
   for (size_t cap : {(size_t)72 * 1024, (size_t)110 * 1024, (size_t)200 * 1024})
     for (int ch = 8; ch >= 1; ch /= 2)
-      if (dd_smem(ch, rowb) <= cap) return ch;
+      if (dd_smem(dm_block, ch, rowb) <= cap) return ch;
   return 0;
 }
-template <int CH>
-cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
-  auto kern = k_dedisp<DD_NW, DD_G, CH, DD_NST>;
-  const size_t smem = dd_smem(CH, a.rowb);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  const int DB = 2 * DD_NW, TB = 128 * DD_G;
-  dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),
-            (unsigned)a.units);
-  kern<<<grid, (DD_NW + 1) * 32, smem, s>>>(a); note_launch();
-  return cudaGetLastError();
-}
-}  // namespace
 
-int dedisp_dm_block() { return 2 * DD_NW; }
-int dedisp_time_block() { return 128 * DD_G; }
-
-size_t dedisp_smem_bytes(int rowb) {
-  const int ch = dd_rows_per_stage(rowb);
-  return ch ? dd_smem(ch, rowb) : (size_t)-1;
+size_t dedisp_smem_bytes(int dm_block, int rows, int rowb) {
+  return dd_smem(dm_block, rows, rowb);
 }
 
-cudaError_t launch_dedisp(const DedispArgs& a, cudaStream_t s) {
+cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t s) {
   if (a.units < 1 || a.units > 65535) return cudaErrorInvalidValue;
-  switch (dd_rows_per_stage(a.rowb)) {
-    case 8: return launch_dd<8>(a, s);
-    case 4: return launch_dd<4>(a, s);
-    case 2: return launch_dd<2>(a, s);
-    case 1: return launch_dd<1>(a, s);
-    default: return cudaErrorInvalidValue;
-  }
+  if (t.dm_block == 8 && t.time_block == 256) return launch_rows<4, 2>(a, t.rows, s);
+  if (t.dm_block == 8 && t.time_block == 512) return launch_rows<4, 4>(a, t.rows, s);
+  if (t.dm_block == 16 && t.time_block == 256) return launch_rows<8, 2>(a, t.rows, s);
+  if (t.dm_block == 16 && t.time_block == 512) return launch_rows<8, 4>(a, t.rows, s);
+  if (t.dm_block == 32 && t.time_block == 256) return launch_rows<16, 2>(a, t.rows, s);
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace hdb

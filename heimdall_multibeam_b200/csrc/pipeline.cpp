@@ -13,6 +13,7 @@
 // Host synchronisations: the hit and giant totals (to size buffers), the
 // clustering convergence flag and the final candidate rows.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -878,6 +879,15 @@ hd_error hd_get_giants(hd_pipeline pl, hd_float* peaks, hd_size* inds, hd_size* 
   if (dm_inds) std::memcpy(dm_inds, pl->g_dms.data(), n * sizeof(hd_size));
   if (labels) std::memcpy(labels, pl->g_labels.data(), n * sizeof(hd_size));
   *count = pl->g_peaks.size();
+  return HD_NO_ERROR;
+}
+
+hd_error hd_get_dedisp_tile(hd_pipeline pl, int* dm_block, int* time_block, int* rows) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  const std::array<int, 3>& t = pl->plan->last_tile;
+  if (dm_block) *dm_block = t[0];
+  if (time_block) *time_block = t[1];
+  if (rows) *rows = t[2];
   return HD_NO_ERROR;
 }
 

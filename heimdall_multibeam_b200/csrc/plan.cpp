@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -67,8 +69,6 @@ dedisp_error plan_prepare(dedisp_plan p) {
   if (!p->dirty) return DEDISP_NO_ERROR;
   if (p->dm_list.empty()) return DEDISP_NO_DM_LIST_SET;
   const size_t D = p->dm_list.size(), C = p->nchans;
-  const int DB = dedisp_dm_block();
-  const size_t nblk = (D + DB - 1) / DB;
   p->delays.assign(D * C, 0);
   p->max_delay = 0;
   for (size_t d = 0; d < D; d++)
@@ -78,36 +78,45 @@ dedisp_error plan_prepare(dedisp_plan p) {
       p->delays[d * C + c] = (int)v;
       p->max_delay = std::max(p->max_delay, v);
     }
-  p->blk_min.assign(nblk * C, 0);
-  p->max_span = 0;
-  for (size_t b = 0; b < nblk; b++)
-    for (size_t c = 0; c < C; c++) {
-      int lo = 0x7FFFFFFF, hi = 0;
-      for (size_t d = b * DB; d < std::min(D, (b + 1) * DB); d++) {
-        lo = std::min(lo, p->delays[d * C + c]);
-        hi = std::max(hi, p->delays[d * C + c]);
+  for (int k = 0; k < 3; k++) {
+    const size_t DB = (size_t)kDedispDmBlocks[k];
+    const size_t nblk = (D + DB - 1) / DB;
+    p->blk_min[k].assign(nblk * C, 0);
+    p->max_span[k] = 0;
+    for (size_t b = 0; b < nblk; b++)
+      for (size_t c = 0; c < C; c++) {
+        int lo = 0x7FFFFFFF, hi = 0;
+        for (size_t d = b * DB; d < std::min(D, (b + 1) * DB); d++) {
+          lo = std::min(lo, p->delays[d * C + c]);
+          hi = std::max(hi, p->delays[d * C + c]);
+        }
+        p->blk_min[k][b * C + c] = lo;
+        p->max_span[k] = std::max(p->max_span[k], (size_t)(hi - lo));
       }
-      p->blk_min[b * C + c] = lo;
-      p->max_span = std::max(p->max_span, (size_t)(hi - lo));
-    }
+  }
   p->active.clear();
   for (size_t c = 0; c < C; c++)
     if (p->killmask[c]) p->active.push_back((int)c);
+  p->tiles.clear();
   int dev = 0;
   cudaGetDevice(&dev);
-  free_dev(p->d_delays); free_dev(p->d_blk_min); free_dev(p->d_active); free_dev(p->d_dm_list);
-  p->d_delays = nullptr; p->d_blk_min = nullptr; p->d_active = nullptr; p->d_dm_list = nullptr;
+  free_dev(p->d_delays); free_dev(p->d_active); free_dev(p->d_dm_list);
+  p->d_delays = nullptr; p->d_active = nullptr; p->d_dm_list = nullptr;
+  for (auto& b : p->d_blk_min) {
+    free_dev(b);
+    b = nullptr;
+  }
   if (cudaMalloc(&p->d_delays, p->delays.size() * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&p->d_blk_min, p->blk_min.size() * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&p->d_active, (p->active.size() + 1) * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&p->d_dm_list, D * sizeof(float)) != cudaSuccess)
     return DEDISP_MEM_ALLOC_FAILED;
+  for (int k = 0; k < 3; k++)
+    if (cudaMalloc(&p->d_blk_min[k], p->blk_min[k].size() * sizeof(int)) != cudaSuccess)
+      return DEDISP_MEM_ALLOC_FAILED;
   if (!p->d_err && cudaMalloc(&p->d_err, sizeof(unsigned)) != cudaSuccess)
     return DEDISP_MEM_ALLOC_FAILED;
   cudaMemset(p->d_err, 0, sizeof(unsigned));
   if (cudaMemcpy(p->d_delays, p->delays.data(), p->delays.size() * sizeof(int),
-                 cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(p->d_blk_min, p->blk_min.data(), p->blk_min.size() * sizeof(int),
                  cudaMemcpyHostToDevice) != cudaSuccess ||
       (!p->active.empty() &&
        cudaMemcpy(p->d_active, p->active.data(), p->active.size() * sizeof(int),
@@ -115,22 +124,39 @@ dedisp_error plan_prepare(dedisp_plan p) {
       cudaMemcpy(p->d_dm_list, p->dm_list.data(), D * sizeof(float), cudaMemcpyHostToDevice) !=
           cudaSuccess)
     return DEDISP_MEM_COPY_FAILED;
+  for (int k = 0; k < 3; k++)
+    if (cudaMemcpy(p->d_blk_min[k], p->blk_min[k].data(), p->blk_min[k].size() * sizeof(int),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return DEDISP_MEM_COPY_FAILED;
   p->device = dev;
   p->dirty = false;
   return DEDISP_NO_ERROR;
 }
 
-static int rowb_of(const dedisp_plan p) {
-  size_t tb = (size_t)dedisp_time_block();
-  size_t r = p->max_span + 16 + tb + 8;
+static int dm_block_index(int dm_block) {
+  for (int k = 0; k < 3; k++)
+    if (kDedispDmBlocks[k] == dm_block) return k;
+  return -1;
+}
+
+// Staged row bytes of a tile: the DM block's delay span for one channel, the
+// time block, the 16-byte alignment of the copy and one word of look-ahead.
+static int rowb_of(const dedisp_plan p, int dm_block, int time_block) {
+  size_t r = p->max_span[dm_block_index(dm_block)] + 16 + (size_t)time_block + 8;
   return (int)((r + 15) & ~(size_t)15);
 }
 
 size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
-  size_t tb = (size_t)dedisp_time_block();
+  // room for the longest staged row of every candidate tile past the last
+  // time block
   size_t nout = nsamps > p->max_delay ? nsamps - p->max_delay : 0;
-  size_t ntb = (nout + tb - 1) / tb;
-  size_t need = std::max(nsamps + 4, ntb * tb + p->max_delay + (size_t)rowb_of(p)) + 64;
+  size_t need = nsamps + 4;
+  for (const auto& t : kDedispTiles) {
+    const size_t tb = (size_t)t[1];
+    const size_t ntb = (nout + tb - 1) / tb;
+    need = std::max(need, ntb * tb + p->max_delay + (size_t)rowb_of(p, t[0], t[1]));
+  }
+  need += 64;
   return (need + 63) & ~(size_t)63;
 }
 
@@ -154,7 +180,6 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   a.in = d_ft;
   a.in_pitch = pitch;
   a.delays = p->d_delays;
-  a.blk_min = p->d_blk_min;
   a.chans = p->d_active;
   a.nact = (int)p->active.size();
   a.nchans = (int)p->nchans;
@@ -162,15 +187,68 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   a.nout = nout;
   a.out = d_out;
   a.out_pitch = out_pitch;
-  a.rowb = rowb_of(p);
   a.err = p->d_err;
   a.units = (int)units;
   a.in_unit = in_unit;
   a.out_unit = out_unit;
   if (units > 65535) return DEDISP_INVALID_STRIDE;
+  auto with_tile = [&](const std::array<int, 3>& t) {
+    a.blk_min = p->d_blk_min[dm_block_index(t[0])];
+    a.rowb = rowb_of(p, t[0], t[1]);
+    return DedispTile{t[0], t[1], t[2]};
+  };
+  // candidate tiles whose staged rows fit shared memory
+  std::vector<std::array<int, 3>> cand;
+  for (const auto& t : kDedispTiles) {
+    const int rows = dedisp_rows_per_stage(t[0], rowb_of(p, t[0], t[1]));
+    if (rows) cand.push_back({t[0], t[1], rows});
+  }
   // one channel row of the widest block's delay span must fit shared memory
-  if (dedisp_smem_bytes(a.rowb) > 200 * 1024) return DEDISP_NCHANS_EXCEEDS_LIMIT;
-  if (launch_dedisp(a, s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
+  if (cand.empty()) return DEDISP_NCHANS_EXCEEDS_LIMIT;
+  const auto key = std::make_pair(nsamps, units);
+  auto it = p->tiles.find(key);
+  if (it == p->tiles.end()) {
+    // default: 16 DMs x 512 samples when it fits
+    std::array<int, 3> best = cand[0];
+    bool forced = false;
+    for (const auto& t : cand)
+      if (t[0] == 16 && t[1] == 512) best = t;
+    for (const auto& t : cand)
+      if (t[0] == p->forced_dm_block && t[1] == p->forced_time_block) {
+        best = t;
+        forced = true;
+      }
+    if (p->tune && !forced && cand.size() > 1) {
+      // autotuner: each candidate once to warm up and once timed; all give the
+      // same sums, so the output of the last run stands
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+        float best_ms = 0.f;
+        bool have = false;
+        for (const auto& t : cand) {
+          const DedispTile dt = with_tile(t);
+          if (launch_dedisp(a, dt, s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
+          cudaEventRecord(e0, s);
+          if (launch_dedisp(a, dt, s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
+          cudaEventRecord(e1, s);
+          float ms = 0.f;
+          if (cudaEventSynchronize(e1) != cudaSuccess ||
+              cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            return DEDISP_INTERNAL_GPU_ERROR;
+          if (!have || ms < best_ms) {
+            best_ms = ms;
+            best = t;
+            have = true;
+          }
+        }
+      }
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+    it = p->tiles.emplace(key, best).first;
+  }
+  p->last_tile = it->second;
+  if (launch_dedisp(a, with_tile(it->second), s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
   return DEDISP_NO_ERROR;
 }
 
@@ -178,7 +256,7 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
 
 dedisp_plan_struct::~dedisp_plan_struct() {
   hdb::free_dev(d_delays);
-  hdb::free_dev(d_blk_min);
+  for (int* b : d_blk_min) hdb::free_dev(b);
   hdb::free_dev(d_active);
   hdb::free_dev(d_dm_list);
   hdb::free_dev(d_err);
@@ -209,6 +287,16 @@ dedisp_error dedisp_create_plan(dedisp_plan* plan, dedisp_size nchans, dedisp_fl
   p->table.resize(nchans);
   hdb::delay_table(nchans, dt, f0, df, p->table.data());
   p->killmask.assign(nchans, 1);
+  // HDB_DEDISP_TUNE=0 keeps the default tile; HDB_DEDISP_TILE=DBxTB forces one
+  if (const char* e = std::getenv("HDB_DEDISP_TUNE"))
+    if (e[0] == '0') p->tune = false;
+  if (const char* e = std::getenv("HDB_DEDISP_TILE")) {
+    int db = 0, tb = 0;
+    if (std::sscanf(e, "%dx%d", &db, &tb) == 2) {
+      p->forced_dm_block = db;
+      p->forced_time_block = tb;
+    }
+  }
   *plan = p;
   return DEDISP_NO_ERROR;
 }

@@ -2,9 +2,12 @@
 // the hd_* pipeline.
 #pragma once
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -24,12 +27,19 @@ struct dedisp_plan_struct {
   // derived / device state (rebuilt lazily when the list or killmask change)
   bool dirty = true;
   std::vector<int> delays;         // [dm][chan]
-  std::vector<int> blk_min;        // [dm block][chan]
+  // per DM-block size (8, 16, 32 trials): [dm block][chan] minimum delay
+  std::vector<int> blk_min[3];
   std::vector<int> active;         // channels with killmask != 0
   size_t max_delay = 0;
-  size_t max_span = 0;             // max over blocks/chans of (max - min) delay
+  size_t max_span[3] = {0, 0, 0};  // max over blocks/chans of (max - min) delay
   int* d_delays = nullptr;
-  int* d_blk_min = nullptr;
+  int* d_blk_min[3] = {nullptr, nullptr, nullptr};
+  // dedispersion tile {dm_block, time_block, rows} per (nsamps, units): the
+  // fastest of the candidates, timed on first use (autotuner)
+  std::map<std::pair<size_t, size_t>, std::array<int, 3>> tiles;
+  std::array<int, 3> last_tile = {16, 512, 8};
+  bool tune = true;
+  int forced_dm_block = 0, forced_time_block = 0;  // HDB_DEDISP_TILE="DBxTB"
   int* d_active = nullptr;
   float* d_dm_list = nullptr;
   unsigned* d_err = nullptr;

@@ -280,6 +280,13 @@ hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long 
                       const void* d_b, long long sbk, long long sbn, float* d_c,
                       long long scm, long long scn, int accumulate, int splits);
 
+/* Dedispersion tile of the last gulp: DM trials and output samples per CTA
+ * and channel rows staged per pipeline stage.  The first gulp of each shape
+ * times every tile that fits shared memory and keeps the fastest (environment:
+ * HDB_DEDISP_TUNE=0 keeps 16 x 512, HDB_DEDISP_TILE=DBxTB forces one); all
+ * tiles give the same sums. */
+hd_error hd_get_dedisp_tile(hd_pipeline pipeline, int* dm_block, int* time_block, int* rows);
+
 /* Number of kernels this library has launched in this process. */
 unsigned long long hd_get_launch_count(void);
 

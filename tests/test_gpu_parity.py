@@ -121,6 +121,50 @@ def test_dedisp_long_delay_spans(hdb, oracle_lib, nchans, dt, dm_max, nsamps, ro
     np.testing.assert_array_equal(out, oracle.dedisperse(fb, dms, table))
 
 
+@pytest.mark.parametrize("tile", ["8x256", "8x512", "16x256", "16x512", "32x256"])
+def test_dedisp_every_tile(hdb, oracle_lib, tile, monkeypatch):
+    """Every dedispersion tile the autotuner may pick (DM trials x output
+    samples per CTA, forced through HDB_DEDISP_TILE) gives the oracle's sums,
+    for short rows and for long ones (128 channels over DM 0-2000)."""
+    monkeypatch.setenv("HDB_DEDISP_TILE", tile)
+    db, tb = (int(x) for x in tile.split("x"))
+    for nchans, dt, f0, df, dm_max, nsamps in [(256, 64e-6, 1500.0, -1.5625, 1000.0, 30000),
+                                               (128, 64e-6, 1520.0, -3.125, 2000.0, 50000)]:
+        rng = np.random.default_rng(nchans)
+        fb = rng.integers(0, 256, size=(nsamps, nchans), dtype=np.uint8)
+        plan = H.DedispPlan(nchans, dt, f0, df)
+        plan.generate_dm_list(0.0, dm_max, 40.0, 1.25)
+        table = oracle.delay_table(nchans, dt, f0, df)
+        np.testing.assert_array_equal(plan.execute(fb), oracle.dedisperse(fb, plan.dm_list, table))
+    # the pipeline reports the tile it used
+    w = synth.SEARCH_C0
+    b = synth.make_c0()
+    with H.Pipeline(H.default_params(nchans=w.nchans, dt=w.dt, f0=w.f0, df=w.df, dm_max=w.dm_max,
+                                     boxcar_max=w.boxcar_max, output_dir=None),
+                    cleaning=False) as pl:
+        pl.execute(b.data)
+        assert pl.dedisp_tile()[:2] == (db, tb)
+
+
+def test_dedisp_autotuner_keeps_results(hdb, monkeypatch):
+    """The autotuned tile is one of the candidates and the gulp's candidates
+    equal those of the default tile."""
+    w = synth.SEARCH_C0
+    b = synth.make_c0()
+    kw = dict(nchans=w.nchans, dt=w.dt, f0=w.f0, df=w.df, dm_max=w.dm_max,
+              boxcar_max=w.boxcar_max, output_dir=None)
+    out = {}
+    for mode in ("tuned", "default"):
+        if mode == "default":
+            monkeypatch.setenv("HDB_DEDISP_TUNE", "0")
+        with H.Pipeline(H.default_params(**kw), cleaning=False) as pl:
+            pl.execute(b.data)
+            out[mode] = (pl.candidates(), pl.dedisp_tile())
+    assert out["default"][1][:2] == (16, 512)
+    assert out["tuned"][1][:2] in [(8, 256), (8, 512), (16, 256), (16, 512), (32, 256)]
+    np.testing.assert_array_equal(out["tuned"][0], out["default"][0])
+
+
 def test_clean_bit_exact(hdb, oracle_lib):
     w = synth.SEARCH_C1
     b = synth.make_beam(1 << 15, 64, w.dt, w.f0, w.df * 16,
