@@ -41,7 +41,8 @@ struct DedispTile {
 };
 constexpr int kDedispDmBlocks[3] = {8, 16, 32};
 // candidate {dm_block, time_block} pairs (32 x 512 would spill registers)
-constexpr int kDedispTiles[5][2] = {{8, 256}, {8, 512}, {16, 256}, {16, 512}, {32, 256}};
+constexpr int kDedispTiles[7][2] = {{8, 256},  {8, 512},  {8, 1024}, {16, 256},
+                                    {16, 512}, {16, 1024}, {32, 256}};
 // rows per stage that fit shared memory for staged rows of rowb bytes (0: none)
 int dedisp_rows_per_stage(int dm_block, int rowb);
 size_t dedisp_smem_bytes(int dm_block, int rows, int rowb);

@@ -189,7 +189,9 @@ __global__ void __launch_bounds__(256) k_zap_to_ft(const uint8_t* __restrict__ i
 constexpr uint32_t DD_WAIT_LIMIT = 1u << 22;
 
 template <int NW, int G, int CH, int NST>
-__global__ void __launch_bounds__((NW + 1) * 32, NW >= 16 ? 2 : 3) k_dedisp(DedispArgs a) {
+__global__ void __launch_bounds__((NW + 1) * 32,
+                                  (NW >= 8 && G >= 8) ? 1 : (NW >= 16 || G >= 8) ? 2 : 3)
+    k_dedisp(DedispArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr int DB = 2 * NW;
   constexpr int TB = 128 * G;
@@ -440,6 +442,8 @@ cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t
   if (a.units < 1 || a.units > 65535) return cudaErrorInvalidValue;
   if (t.dm_block == 8 && t.time_block == 256) return launch_rows<4, 2>(a, t.rows, s);
   if (t.dm_block == 8 && t.time_block == 512) return launch_rows<4, 4>(a, t.rows, s);
+  if (t.dm_block == 8 && t.time_block == 1024) return launch_rows<4, 8>(a, t.rows, s);
+  if (t.dm_block == 16 && t.time_block == 1024) return launch_rows<8, 8>(a, t.rows, s);
   if (t.dm_block == 16 && t.time_block == 256) return launch_rows<8, 2>(a, t.rows, s);
   if (t.dm_block == 16 && t.time_block == 512) return launch_rows<8, 4>(a, t.rows, s);
   if (t.dm_block == 32 && t.time_block == 256) return launch_rows<16, 2>(a, t.rows, s);

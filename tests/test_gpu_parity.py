@@ -121,7 +121,8 @@ def test_dedisp_long_delay_spans(hdb, oracle_lib, nchans, dt, dm_max, nsamps, ro
     np.testing.assert_array_equal(out, oracle.dedisperse(fb, dms, table))
 
 
-@pytest.mark.parametrize("tile", ["8x256", "8x512", "16x256", "16x512", "32x256"])
+@pytest.mark.parametrize("tile", ["8x256", "8x512", "8x1024", "16x256", "16x512", "16x1024",
+                                  "32x256"])
 def test_dedisp_every_tile(hdb, oracle_lib, tile, monkeypatch):
     """Every dedispersion tile the autotuner may pick (DM trials x output
     samples per CTA, forced through HDB_DEDISP_TILE) gives the oracle's sums,
@@ -161,7 +162,8 @@ def test_dedisp_autotuner_keeps_results(hdb, monkeypatch):
             pl.execute(b.data)
             out[mode] = (pl.candidates(), pl.dedisp_tile())
     assert out["default"][1][:2] == (16, 512)
-    assert out["tuned"][1][:2] in [(8, 256), (8, 512), (16, 256), (16, 512), (32, 256)]
+    assert out["tuned"][1][:2] in [(8, 256), (8, 512), (8, 1024), (16, 256), (16, 512),
+                                   (16, 1024), (32, 256)]
     np.testing.assert_array_equal(out["tuned"][0], out["default"][0])
 
 
