@@ -350,7 +350,9 @@ def run_product(args):
                        "boxcar_max": w.boxcar_max, "clean_filterbank_rfi": bool(w.clean),
                        "beam_seconds_per_gulp": round(wk.beam_s, 4),
                        "dedisp_tile": {"dm_block": tile[0], "time_block": tile[1],
-                                       "rows_per_stage": tile[2], "chosen_by": "autotuner"},
+                                       "rows_per_stage": tile[2],
+                                       "chosen_by": "HDB_DEDISP_TILE"
+                                       if os.environ.get("HDB_DEDISP_TILE") else "autotuner"},
                        "l2": f"input {U * fb_bytes / 2**20:.0f} MiB > L2, no flush",
                        "parallelism": f"replicas{world}"},
             "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},
