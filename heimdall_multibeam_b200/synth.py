@@ -338,3 +338,95 @@ def match_pulse(cand, pulses: Sequence[Pulse], dt: float) -> int:
         if abs(int(cand["samp_idx"]) - p.t0) <= tol_t and abs(float(cand["dm"]) - p.dm) <= tol_dm:
             return k
     return -1
+
+
+# ---------------------------------------------------------------------------
+# Classifier training gulps at survey size, generated on the GPU
+# ---------------------------------------------------------------------------
+def inject_pulse_device(torch, x, p: Pulse, dt: float, f0: float, df: float,
+                        sigma: float = 16.0) -> None:
+    """inject_pulse on a device tensor x (nsamps, nchans) float32: the same
+    dispersed Gaussian (channel centre times, width, +-6 sigma window,
+    amplitude for the integrated S/N over the whole window)."""
+    nsamps, nchans = x.shape
+    dev = x.device
+    f = f0 + df * torch.arange(nchans, dtype=torch.float64, device=dev)
+    centres = p.t0 + DISPERSION_K * p.dm * (f ** -2.0 - f0 ** -2.0) / dt
+    s = max(p.fwhm_s / dt / (2.0 * math.sqrt(2.0 * math.log(2.0))), 0.3)
+    half = int(math.ceil(6.0 * s)) + 1
+    t = torch.floor(centres).long()[:, None] - half + torch.arange(2 * half + 1, device=dev)[None, :]
+    g = torch.exp(-0.5 * ((t.double() - centres[:, None]) / s) ** 2)
+    energy = float((g * g).sum())
+    if energy <= 0.0:
+        return
+    amp = p.snr * sigma / math.sqrt(energy)
+    keep = (t >= 0) & (t < nsamps)
+    c = torch.arange(nchans, device=dev)[:, None].expand_as(t)
+    x.index_put_((t[keep], c[keep]), (amp * g[keep]).float(), accumulate=True)
+
+
+def make_training_gulps_device(torch, seeds: Sequence[int], w: Workload = None,
+                               n_pulses: int = 40, n_rfi: int = 20, device: str = "cuda"):
+    """Survey-shaped classifier training gulps (default: 1024 channels, 64 us,
+    2^18 samples) generated on the GPU.  Each gulp: Gaussian noise (128, 16),
+    n_pulses dispersed pulses (DM 50-dm_max, FWHM log-uniform 0.1-30 ms, S/N
+    6-50) and n_rfi RFI events, each event in its own time slot: zero-DM
+    broadband bursts (1-64 samples, +0.1..+0.5 sd per channel), narrowband
+    bursts (1-32 adjacent channels, 16-512 samples, +1..+4 sd) and sinusoidal
+    baseline drifts over all channels (period 5-50 ms, 1-3 periods,
+    0.05-0.2 sd).  Over 1024 channels these integrate at DM 0 to S/N of a few
+    to about a hundred (stronger events flood the list with candidates along
+    the whole DM range and swallow neighbouring pulses).  Returns (uint8
+    tensor [U, nsamps, nchans] on the device, pulses per gulp, RFI events per
+    gulp)."""
+    w = w or SEARCH_C1
+    dev = torch.device(device)
+    seeds = list(seeds)
+    out = torch.empty((len(seeds), w.nsamps, w.nchans), dtype=torch.uint8, device=dev)
+    md = max_delay_samples(w.dm_max, w.nchans, w.dt, w.f0, w.df)
+    lo = 2 * w.boxcar_max
+    hi = w.nsamps - md - 2 * w.boxcar_max
+    nev = n_pulses + n_rfi
+    slot = (hi - lo) / max(nev, 1)
+    all_pulses, all_events = [], []
+    for u, seed in enumerate(seeds):
+        g = _rng(seed, 0xC1C1)
+        tg = torch.Generator(device=dev).manual_seed(int(seed) * 7919 + 17)
+        x = torch.randn((w.nsamps, w.nchans), generator=tg, device=dev)
+        x.mul_(16.0).add_(128.0)
+        kinds = ["pulse"] * n_pulses + ["rfi"] * n_rfi
+        g.shuffle(kinds)
+        pulses: List[Pulse] = []
+        events: List[RfiEvent] = []
+        for k, kind in enumerate(kinds):
+            t = lo + slot * (k + float(g.uniform(0.3, 0.7)))
+            if kind == "pulse":
+                dm = float(g.uniform(50.0, w.dm_max))
+                fw = float(math.exp(g.uniform(math.log(0.1e-3), math.log(30e-3))))
+                pu = Pulse(t, dm, fw, float(g.uniform(6.0, 50.0)))
+                inject_pulse_device(torch, x, pu, w.dt, w.f0, w.df)
+                pulses.append(pu)
+                continue
+            kind = ("burst", "narrow", "drift")[int(g.integers(0, 3))]
+            t0 = int(t)
+            if kind == "burst":
+                ln = int(g.integers(1, 65))
+                x[t0:t0 + ln, :] += float(g.uniform(0.1, 0.5)) * 16.0
+            elif kind == "narrow":
+                ln = int(2 ** g.uniform(4, 9))
+                nc = int(g.integers(1, 33))
+                c0 = int(g.integers(0, w.nchans - nc))
+                x[t0:t0 + ln, c0:c0 + nc] += float(g.uniform(1.0, 4.0)) * 16.0
+            else:
+                period = float(g.uniform(0.005, 0.05)) / w.dt
+                ln = int(min(slot * 0.5, period * float(g.uniform(1.0, 3.0))))
+                amp = float(g.uniform(0.05, 0.2)) * 16.0
+                tt = torch.arange(ln, dtype=torch.float32, device=dev)
+                x[t0:t0 + ln, :] += (amp * torch.sin(2.0 * math.pi * tt / period))[:, None]
+            events.append(RfiEvent(kind, float(t0), float(ln)))
+        out[u] = x.round_().clamp_(0, 255).to(torch.uint8)
+        del x
+        all_pulses.append(pulses)
+        all_events.append(events)
+    return out, all_pulses, all_events
+
