@@ -177,6 +177,22 @@ def recall(cands, pulses, dt, snr_min=8.0):
     return hit, len(strong)
 
 
+def max_over_ranks(torch, dist, values, device):
+    """Element-wise maximum over all ranks of this rank's timings (ms): a
+    multi-GPU step takes as long as its slowest rank."""
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def whole_job_value(world, beam_s, ms):
+    """Beam-seconds searched per second by the whole job: every rank searches
+    its own gulp of beam_s beam-seconds (replicas, weak scaling) in at most
+    ms milliseconds."""
+    return world * beam_s / (ms / 1e3)
+
+
 def _timed(torch, dev, barrier, steps, fn, stage=None, timing=None):
     """K calls of fn between CUDA events (each call ends synchronised)."""
     e0 = torch.cuda.Event(enable_timing=True)
@@ -291,12 +307,9 @@ def run_product(args):
 
     # clocks sampled over the three timed regions (batched, plain, e2e)
     clocks = clk.stop()
-    tm = [ms, ms_plain or 0.0, ms_e2e or 0.0]
-    tmax = torch.tensor(tm, dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    ms, ms_plain_m, ms_e2e_m = (float(x) for x in tmax)
-    value = world * wk.beam_s / (ms / 1e3)
+    ms, ms_plain_m, ms_e2e_m = max_over_ranks(torch, dist, [ms, ms_plain or 0.0, ms_e2e or 0.0],
+                                              dev)
+    value = whole_job_value(world, wk.beam_s, ms)
 
     clf_rec = None
     if not args.batched_only and not args.no_classifier:
@@ -324,6 +337,8 @@ def run_product(args):
         sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
         int_peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # Tadd/s, INT32 lanes x clock
         int_ach = adds / (t_dd / 1e3) / 1e12
+        smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e12  # TB/s of shared-memory wavefronts
+        smem_ach = 2.0 * adds / (t_dd / 1e3) / 1e12
         traffic = None
         tf = TRAFFIC.get(w.name)
         if tf:
@@ -364,20 +379,27 @@ def run_product(args):
                                      "peak_tadds": round(int_peak, 3),
                                      "frac": round(int_ach / int_peak, 4),
                                      "basis": "148 SMs x 128 INT32 lanes x median SM clock"},
-                         "binding": "int_add"},
+                         "smem": {"achieved_tbs": round(smem_ach, 3),
+                                  "peak_tbs": round(smem_peak, 3),
+                                  "frac": round(smem_ach / smem_peak, 4),
+                                  "basis": "2 bytes of shared memory read per sample-channel-"
+                                           "trial add (two 4-byte words per 4-sample output "
+                                           "word); 148 SMs x 128 B x median SM clock"},
+                         "binding": "shared_memory"},
             "recall": {"snr_ge_8_found": hit, "snr_ge_8_injected": nstrong},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
         if ms_plain is not None:
-            v_plain = world * wk.beam_s / (ms_plain_m / 1e3)
+            v_plain = whole_job_value(world, wk.beam_s, ms_plain_m)
             rec["plain"] = {"value": round(v_plain, 3), "unit": UNIT,
                             "ms_per_step": round(ms_plain_m, 3),
                             "form": f"{U} hd_execute_device calls per gulp",
                             "gpu_launches": int(launches_plain)}
             rec["batched_over_plain"] = round(value / v_plain, 3)
         if ms_e2e is not None:
-            rec["e2e"] = {"value": round(world * wk.beam_s / (ms_e2e_m / 1e3), 3), "unit": UNIT,
+            rec["e2e"] = {"value": round(whole_job_value(world, wk.beam_s, ms_e2e_m), 3),
+                          "unit": UNIT,
                           "ms_per_step": round(ms_e2e_m, 3),
                           "h2d_bytes_per_step": int(U * fb_bytes),
                           "d2h_bytes_per_step": int(ncand * 64 + 128),
@@ -520,18 +542,15 @@ def uneven_bench(args, H, torch, dev, barrier, dist, world):
         ms_set = _timed(torch, dev, barrier, steps, batched)
         nconf = bs.nconfigs
         ncand = sum(len(bs.candidates(b)) for b in range(len(ws)))
-    tmax = torch.tensor([ms_plain, ms_set], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    ms_plain, ms_set = float(tmax[0]), float(tmax[1])
+    ms_plain, ms_set = max_over_ranks(torch, dist, [ms_plain, ms_set], dev)
     return {"workload": f"uneven_{len(ws)}x_c128-4096_n16384-{args.uneven_nsamps_max}",
             "nbeams": len(ws), "configurations": nconf,
             "input_gib": round(sum(w.nchans * w.nsamps for w in ws) / 2**30, 3),
             "beam_seconds": round(beam_s, 3), "steps": steps,
-            "beam_set": {"value": round(world * beam_s / (ms_set / 1e3), 3), "unit": UNIT,
+            "beam_set": {"value": round(whole_job_value(world, beam_s, ms_set), 3), "unit": UNIT,
                          "ms_per_step": round(ms_set, 3), "workers": args.uneven_workers,
                          "api": "hd_execute_beam_set"},
-            "plain": {"value": round(world * beam_s / (ms_plain / 1e3), 3), "unit": UNIT,
+            "plain": {"value": round(whole_job_value(world, beam_s, ms_plain), 3), "unit": UNIT,
                       "ms_per_step": round(ms_plain, 3),
                       "form": "one pipeline per configuration, hd_execute_device per beam"},
             "set_over_plain": round(ms_plain / ms_set, 3), "candidates": ncand,
@@ -559,14 +578,13 @@ def survey_plain(args, H, torch, dev, barrier, dist, world):
     ms_e2e = _timed(torch, dev, barrier, args.steps,
                     lambda: pl.execute_ptr(h_fb.data_ptr(), nsamps))
     pl.close()
-    tmax = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = float(tmax[0]), float(tmax[1])
+    ms, ms_e2e = max_over_ranks(torch, dist, [ms, ms_e2e], dev)
     hit, nstrong = recall(cands, wk.pulses[0], w.dt)
-    return {"workload": w.name, "value": round(world * wk.beam_s / (ms / 1e3), 3), "unit": UNIT,
+    return {"workload": w.name, "value": round(whole_job_value(world, wk.beam_s, ms), 3),
+            "unit": UNIT,
             "ms_per_step": round(ms, 3),
-            "e2e": round(world * wk.beam_s / (ms_e2e / 1e3), 3), "e2e_ms_per_step": round(ms_e2e, 3),
+            "e2e": round(whole_job_value(world, wk.beam_s, ms_e2e), 3),
+            "e2e_ms_per_step": round(ms_e2e, 3),
             "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},
             "recall": {"snr_ge_8_found": hit, "snr_ge_8_injected": nstrong}}
 
