@@ -390,8 +390,13 @@ namespace inf {
 using namespace clf;
 constexpr int kWarps = 16, kThreads = kWarps * 32;
 // shared-memory regions (bytes)
-constexpr int kR0 = 18 * 66 * 16 * 2;   // B input [66][258]; B pool-2 [18][66][16]; A pool-1 [34][34][8]
-constexpr int kR1 = 34 * 130 * 8 * 2;   // B pool-1 [34][130][8]; A input [66][66]; A pool-2 [18][18][16]
+// Pixels of 16 channels are stored 24 elements (48 bytes) apart, so that the
+// 8 pixels of an MMA fragment load fall on distinct banks; 1 and 8 channels
+// are dense.
+template <int C>
+__host__ __device__ constexpr int pix_stride() { return C == 16 ? 24 : C; }
+constexpr int kR0 = 18 * 66 * 24 * 2;   // B input [66][258]; B pool-2 [18][66][24]; A pool-1 [34][34][8]
+constexpr int kR1 = 34 * 130 * 8 * 2;   // B pool-1 [34][130][8]; A input [66][66]; A pool-2 [18][18][24]
 constexpr int kF = 10240 * 2;           // flattened features
 // weight fragments per layer: ksteps x (c_out / 8) x 32 lanes of uint2
 constexpr int kFragL1 = 1 * 1 * 32, kFragL2 = 5 * 2 * 32, kFragL3 = 9 * 4 * 32;
@@ -474,8 +479,9 @@ __device__ void load_input(const float* __restrict__ src, int W, bf16* dst) {
   }
 }
 
-// conv 3x3 (pad 1) + bias + ReLU + 2x2 max-pool of an H x W x CI image.
-// out: [H/2 + 2][W/2 + 2][CO] interior, or (feat) the flattened features at
+// conv 3x3 (pad 1) + bias + ReLU + 2x2 max-pool of an H x W x CI image
+// (pixels pix_stride<CI>() elements apart).
+// out: [H/2 + 2][W/2 + 2][pix_stride<CO>()] interior, or (feat) the flattened features at
 // feat[c * (H/2 * W/2) + y * W/2 + x].
 template <int CI, int CO>
 __device__ void conv_layer(const bf16* __restrict__ in, int H, int W, const uint2* __restrict__ wf,
@@ -483,6 +489,7 @@ __device__ void conv_layer(const bf16* __restrict__ in, int H, int W, const uint
                            bf16* __restrict__ feat) {
   constexpr int KS = CI == 16 ? 9 : (CI == 8 ? 5 : 1);
   constexpr int NT = CO / 8;
+  constexpr int PSI = pix_stride<CI>(), PSO = pix_stride<CO>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int Wp = W + 2, W2 = W / 2, H2 = H / 2;
@@ -507,19 +514,19 @@ __device__ void conv_layer(const bf16* __restrict__ in, int H, int W, const uint
       uint32_t a[4];
       if (CI == 16) {
         const int o = (s / 3) * Wp + (s % 3);
-        a[0] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o) * CI + 2 * t);
-        a[1] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o) * CI + 2 * t);
-        a[2] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o) * CI + 2 * t + 8);
-        a[3] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o) * CI + 2 * t + 8);
+        a[0] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o) * PSI + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o) * PSI + 2 * t);
+        a[2] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o) * PSI + 2 * t + 8);
+        a[3] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o) * PSI + 2 * t + 8);
       } else if (CI == 8) {
         const int j0 = 2 * s, j1 = 2 * s + 1;
         const int o0 = (j0 / 3) * Wp + (j0 % 3);
-        a[0] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o0) * CI + 2 * t);
-        a[1] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o0) * CI + 2 * t);
+        a[0] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o0) * PSI + 2 * t);
+        a[1] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o0) * PSI + 2 * t);
         if (j1 < 9) {
           const int o1 = (j1 / 3) * Wp + (j1 % 3);
-          a[2] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o1) * CI + 2 * t);
-          a[3] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o1) * CI + 2 * t);
+          a[2] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p0 + o1) * PSI + 2 * t);
+          a[3] = *reinterpret_cast<const uint32_t*>(in + (size_t)(p1 + o1) * PSI + 2 * t);
         } else {
           a[2] = a[3] = 0u;
         }
@@ -555,7 +562,7 @@ __device__ void conv_layer(const bf16* __restrict__ in, int H, int W, const uint
           feat[(size_t)co * (H2 * W2) + py * W2 + px] = __float2bfloat16(m0);
           feat[(size_t)(co + 1) * (H2 * W2) + py * W2 + px] = __float2bfloat16(m1);
         } else {
-          *reinterpret_cast<uint32_t*>(out + ((size_t)(py + 1) * (W2 + 2) + px + 1) * CO + co) =
+          *reinterpret_cast<uint32_t*>(out + ((size_t)(py + 1) * (W2 + 2) + px + 1) * PSO + co) =
               pack2(__float2bfloat16(m0), __float2bfloat16(m1));
         }
       }
@@ -587,7 +594,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_clf_infer(Args a) {
     __syncthreads();
     conv_layer<1, 8>(r0, 64, 256, fB, a.w + a.off_b[1][0], r1, nullptr);
     __syncthreads();
-    zero_ring(r0, 16, 64, 16);
+    zero_ring(r0, 16, 64, pix_stride<16>());
     conv_layer<8, 16>(r1, 32, 128, fB + kFragL1, a.w + a.off_b[1][1], r0, nullptr);
     __syncthreads();
     conv_layer<16, 32>(r0, 16, 64, fB + kFragL1 + kFragL2, a.w + a.off_b[1][2], nullptr,
@@ -600,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_clf_infer(Args a) {
     __syncthreads();
     conv_layer<1, 8>(r1, 64, 64, fA, a.w + a.off_b[0][0], r0, nullptr);
     __syncthreads();
-    zero_ring(r1, 16, 16, 16);
+    zero_ring(r1, 16, 16, pix_stride<16>());
     conv_layer<8, 16>(r0, 32, 32, fA + kFragL1, a.w + a.off_b[0][1], r1, nullptr);
     __syncthreads();
     conv_layer<16, 32>(r1, 16, 16, fA + kFragL1 + kFragL2, a.w + a.off_b[0][2], nullptr, feat);
@@ -807,6 +814,7 @@ struct hd_classifier_t {
   size_t off_w[2][3], off_b[2][3], off_w1, off_b1, off_w2, off_b2, nparam;
   DBuf w, g, m, v;          // parameters, gradients, Adam moments
   DBuf wb_conv[2][3], wb1;  // BF16 weight copies
+  bool bf16_stale = true;   // the FP32 weights changed since the BF16 copies
   long long step = 0;
   // per-batch work buffers
   int cap_batch = 0;
@@ -872,6 +880,8 @@ cudaError_t alloc_batch(hd_classifier c, int nb) {
 }
 
 cudaError_t refresh_bf16(hd_classifier c) {
+  if (!c->bf16_stale) return cudaSuccess;
+  c->bf16_stale = false;
   cudaStream_t s = c->stream;
   float* w = c->w.as<float>();
   for (int br = 0; br < 2; br++)
@@ -1139,6 +1149,7 @@ hd_error hd_classifier_set_params(hd_classifier c, const float* params, hd_size 
   if (!c) return HD_INVALID_PIPELINE;
   if (!params || count != c->nparam) return HD_INVALID_POINTER;
   cudaSetDevice(c->device);
+  c->bf16_stale = true;
   c->step = 0;
   cudaError_t e = cudaMemcpy(c->w.p, params, c->nparam * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(c->m.p, 0, c->nparam * sizeof(float));
@@ -1221,6 +1232,7 @@ hd_error hd_classifier_train(hd_classifier c, const float* dm_time, const float*
       const float b1 = 0.9f, b2 = 0.999f;
       const float c1 = 1.f - (float)std::pow(b1, (double)c->step);
       const float c2 = 1.f - (float)std::pow(b2, (double)c->step);
+      c->bf16_stale = true;
       k_adam<<<nblk(c->nparam), 256, 0, s>>>(c->w.as<float>(), c->g.as<float>(), c->m.as<float>(),
                                              c->v.as<float>(), c->nparam, lr, b1, b2, 1e-8f, c1, c2); hdb::note_launch();
       float l = 0.f;
