@@ -110,6 +110,26 @@ CANDIDATE_DTYPE = np.dtype([("snr", "<f4"), ("samp_idx", "<u8"), ("time", "<f4")
                             ("members", "<u8"), ("begin", "<u8"), ("end", "<u8"),
                             ("beam", "<u8")], align=True)
 
+class HdSigprocHeader(C.Structure):
+    """hd_sigproc_header (include/heimdall_b200.h)."""
+    _fields_ = [("source_name", C.c_char * 80), ("rawdatafile", C.c_char * 80)] + \
+        [(k, C.c_double) for k in ("az_start", "za_start", "src_raj", "src_dej", "tstart", "tsamp",
+                                   "period", "fch1", "foff", "refdm")] + \
+        [(k, C.c_int) for k in ("nchans", "telescope_id", "machine_id", "data_type", "ibeam",
+                                "nbeams", "nbits", "barycentric", "pulsarcentric", "nbins",
+                                "nsamples", "nifs", "npuls")] + \
+        [("signed_data", C.c_ubyte), ("size", C.c_int), ("unknown_keys", C.c_int)]
+
+    def as_dict(self) -> Dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["source_name"] = self.source_name.decode()
+        d["rawdatafile"] = self.rawdatafile.decode()
+        return d
+
+
+GULP_CALLBACK = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t)
+
+
 # symbol -> (restype, argtypes); every function include/*.h declares
 _P = C.c_void_p
 _SZ = C.c_size_t
@@ -147,6 +167,11 @@ SYMBOLS = {
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
     "hd_get_dedisp_tile": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
+    "hd_read_sigproc_header": (C.c_int, [C.c_char_p, C.POINTER(HdSigprocHeader)]),
+    "hd_mjd_to_utc": (C.c_longlong, [C.c_double]),
+    "hd_params_from_sigproc": (C.c_int, [C.POINTER(HdSigprocHeader), C.POINTER(HdParams)]),
+    "hd_search_sigproc_file": (C.c_int, [_P, C.c_char_p, _SZ, GULP_CALLBACK, C.c_void_p, _SZP,
+                                         _SZP]),
     "hd_extract_patches": (C.c_int, [_P, _FP, _FP, _SZP]),
     "hd_classifier_param_count": (_SZ, []),
     "hd_classifier_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_ulonglong]),
@@ -233,6 +258,28 @@ def _u8(a: np.ndarray) -> np.ndarray:
     if a.dtype != np.uint8:
         raise TypeError("filterbank must be uint8")
     return a
+
+
+def read_sigproc_header(path: str) -> Dict:
+    """hd_read_sigproc_header as a dict (raises HdError on failure)."""
+    h = HdSigprocHeader()
+    err = lib().hd_read_sigproc_header(path.encode(), C.byref(h))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_read_sigproc_header")
+    return h.as_dict()
+
+
+def params_from_sigproc(path: str, params: Optional[HdParams] = None) -> HdParams:
+    """hd_params_from_sigproc on the file's header, over default parameters."""
+    h = HdSigprocHeader()
+    err = lib().hd_read_sigproc_header(path.encode(), C.byref(h))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_read_sigproc_header")
+    p = params if params is not None else default_params()
+    err = lib().hd_params_from_sigproc(C.byref(h), C.byref(p))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_params_from_sigproc")
+    return p
 
 
 class Pipeline:
@@ -400,6 +447,25 @@ class Pipeline:
             if err != HD_NO_ERROR:
                 raise HdError(err, "hd_score_candidates")
         return out
+
+    def search_sigproc_file(self, path: str, nsamps_gulp: int):
+        """hd_search_sigproc_file: (hd_error, total spectra searched per beam,
+        [(first_idx, candidates) per gulp])."""
+        gulps = []
+
+        def cb(user, cands, n, first_idx):
+            a = np.zeros(n, CANDIDATE_DTYPE)
+            if n:
+                C.memmove(a.ctypes.data, cands, n * CANDIDATE_DTYPE.itemsize)
+            gulps.append((int(first_idx), a))
+
+        fn = GULP_CALLBACK(cb)
+        total = C.c_size_t(0)
+        ng = C.c_size_t(0)
+        err = lib().hd_search_sigproc_file(self._p, path.encode(), nsamps_gulp, fn, None,
+                                           C.byref(total), C.byref(ng))
+        assert ng.value == len(gulps)
+        return err, total.value, gulps
 
     def dedisp_tile(self) -> Tuple[int, int, int]:
         """hd_get_dedisp_tile: (DM block, time block, rows per stage) of the

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 struct hd_classifier_t;
+struct hd_pipeline_t;
 
 namespace hdb {
 
@@ -227,5 +228,6 @@ cudaError_t classifier_score_device(struct ::hd_classifier_t* c, const float* d_
                                     const float* d_ft, size_t n, cudaEvent_t after,
                                     float* scores);
 int classifier_device(struct ::hd_classifier_t* c);
+int pipeline_device(struct ::hd_pipeline_t* p);
 
 }  // namespace hdb

@@ -882,6 +882,14 @@ hd_error hd_get_giants(hd_pipeline pl, hd_float* peaks, hd_size* inds, hd_size* 
   return HD_NO_ERROR;
 }
 
+}  // extern "C"
+
+namespace hdb {
+int pipeline_device(hd_pipeline pl) { return pl ? pl->device : 0; }
+}  // namespace hdb
+
+extern "C" {
+
 hd_error hd_get_dedisp_tile(hd_pipeline pl, int* dm_block, int* time_block, int* rows) {
   if (!pl) return HD_INVALID_PIPELINE;
   const std::array<int, 3>& t = pl->plan->last_tile;

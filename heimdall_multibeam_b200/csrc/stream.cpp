@@ -1,0 +1,308 @@
+// stream.cpp -- sigproc filterbank input and the gulp loop with overlap carry.
+//
+//   hd_read_sigproc_header   Formats/hd/header.h:133-198 (read_header) and
+//                            Formats/SigprocFile.C:16-51
+//   hd_params_from_sigproc   the data-source fields Applications/heimdall.C:
+//                            103-119 copies into hd_params, with
+//                            Formats/hd/DataSource.h:49-82 (mjd2utctm)
+//   hd_search_sigproc_file   the gulp loop of Applications/heimdall.C:153-292
+//
+// The loop keeps the overlap on the device: two device buffers alternate, the
+// overlap of each beam is copied device to device from the one just searched
+// into the next, and only the new block crosses PCIe.  A host thread reads the
+// next block from the file into pinned memory while the GPU searches the
+// current gulp.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "heimdall_b200.h"
+#include "internal.h"
+
+namespace {
+
+// One header string: a 4-byte length (1..79) and the characters
+// (header.h:120-129).
+bool read_str(FILE* f, std::string& s) {
+  int len = 0;
+  if (std::fread(&len, sizeof(int), 1, f) != 1) return false;
+  if (len <= 0 || len >= 80) return false;
+  char buf[80];
+  if (std::fread(buf, 1, (size_t)len, f) != (size_t)len) return false;
+  s.assign(buf, (size_t)len);
+  return true;
+}
+
+template <class T>
+bool read_val(FILE* f, T& v) {
+  return std::fread(&v, sizeof(T), 1, f) == 1;
+}
+
+void copy_str(char* dst, const std::string& s) {
+  const size_t n = std::min<size_t>(s.size(), 79);
+  std::memcpy(dst, s.data(), n);
+  dst[n] = '\0';
+}
+
+// Days since the start of the Julian period of a Julian day number -> civil
+// date, by the integer algorithm of Fliegel and Van Flandern (Comm. ACM 11,
+// 657, 1968).
+void jd_to_civil(long jd, int& year, int& month, int& day) {
+  long l = jd + 68569;
+  const long n = 4 * l / 146097;
+  l = l - (146097 * n + 3) / 4;
+  const long i = 4000 * (l + 1) / 1461001;
+  l = l - 1461 * i / 4 + 31;
+  const long j = 80 * l / 2447;
+  day = (int)(l - 2447 * j / 80);
+  l = j / 11;
+  month = (int)(j + 2 - 12 * l);
+  year = (int)(100 * (n - 49) + i + l);
+}
+
+}  // namespace
+
+extern "C" {
+
+hd_error hd_read_sigproc_header(const char* path, hd_sigproc_header* h) {
+  if (!path || !h) return HD_INVALID_POINTER;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return HD_INVALID_POINTER;
+  std::memset(h, 0, sizeof(*h));
+  std::string s;
+  if (!read_str(f, s) || s != "HEADER_START") {
+    std::fclose(f);
+    return HD_UNKNOWN_ERROR;
+  }
+  bool want_source = false, want_raw = false, ok = true;
+  for (;;) {
+    if (!read_str(f, s)) {
+      ok = false;
+      break;
+    }
+    if (s == "HEADER_END") break;
+    if (s == "source_name") want_source = true;
+    else if (s == "rawdatafile") want_raw = true;
+    else if (s == "az_start") ok = read_val(f, h->az_start);
+    else if (s == "za_start") ok = read_val(f, h->za_start);
+    else if (s == "src_raj") ok = read_val(f, h->src_raj);
+    else if (s == "src_dej") ok = read_val(f, h->src_dej);
+    else if (s == "tstart") ok = read_val(f, h->tstart);
+    else if (s == "tsamp") ok = read_val(f, h->tsamp);
+    else if (s == "period") ok = read_val(f, h->period);
+    else if (s == "fch1") ok = read_val(f, h->fch1);
+    else if (s == "foff") ok = read_val(f, h->foff);
+    else if (s == "nchans") ok = read_val(f, h->nchans);
+    else if (s == "telescope_id") ok = read_val(f, h->telescope_id);
+    else if (s == "machine_id") ok = read_val(f, h->machine_id);
+    else if (s == "data_type") ok = read_val(f, h->data_type);
+    else if (s == "ibeam") ok = read_val(f, h->ibeam);
+    else if (s == "nbeams") ok = read_val(f, h->nbeams);
+    else if (s == "nbits") ok = read_val(f, h->nbits);
+    else if (s == "barycentric") ok = read_val(f, h->barycentric);
+    else if (s == "pulsarcentric") ok = read_val(f, h->pulsarcentric);
+    else if (s == "nbins") ok = read_val(f, h->nbins);
+    else if (s == "nsamples") ok = read_val(f, h->nsamples);
+    else if (s == "nifs") ok = read_val(f, h->nifs);
+    else if (s == "npuls") ok = read_val(f, h->npuls);
+    else if (s == "refdm") ok = read_val(f, h->refdm);
+    else if (s == "signed") ok = read_val(f, h->signed_data);
+    else if (want_source) {
+      copy_str(h->source_name, s);
+      want_source = false;
+    } else if (want_raw) {
+      copy_str(h->rawdatafile, s);
+      want_raw = false;
+    } else {
+      h->unknown_keys++;  // the reference warns and carries on
+    }
+    if (!ok) break;
+  }
+  if (!ok) {
+    std::fclose(f);
+    return HD_UNKNOWN_ERROR;
+  }
+  h->size = (int)std::ftell(f);
+  if (h->nsamples == 0 && h->nchans > 0 && h->nbits > 0) {
+    // header.h:190-193: the whole file's size (header included) over the
+    // bytes of one spectrum
+    std::fseek(f, 0, SEEK_END);
+    const long long fsize = (long long)std::ftell(f);
+    h->nsamples = (int)(fsize / h->nchans * 8 / h->nbits);
+  }
+  std::fclose(f);
+  return HD_NO_ERROR;
+}
+
+long long hd_mjd_to_utc(double mjd) {
+  // DataSource.h:49-82: whole seconds of the day, one second added when the
+  // fraction left is below 1 (always, as written), the civil date of the
+  // Julian day, and mktime in the local time zone
+  const int days = (int)mjd;
+  const double fdays = mjd - (double)days;
+  const double seconds = fdays * 86400.0;
+  int secs = (int)seconds;
+  const double fracsec = seconds - (double)secs;
+  if (fracsec - 1 < 0.0000001) secs++;
+  int year = 0, month = 0, day = 0;
+  jd_to_civil((long)days + 2400001L, year, month, day);
+  struct tm t;
+  std::memset(&t, 0, sizeof(t));
+  t.tm_year = year - 1900;
+  t.tm_mon = month - 1;
+  t.tm_mday = day;
+  t.tm_hour = secs / 3600;
+  secs -= 3600 * t.tm_hour;
+  t.tm_min = secs / 60;
+  secs -= 60 * t.tm_min;
+  t.tm_sec = secs;
+  t.tm_isdst = -1;
+  return (long long)std::mktime(&t);
+}
+
+hd_error hd_params_from_sigproc(const hd_sigproc_header* h, struct hd_params* p) {
+  if (!h || !p) return HD_INVALID_POINTER;
+  if (h->nchans <= 0 || h->tsamp <= 0.0) return HD_INVALID_STRIDE;
+  p->nchans = (hd_size)h->nchans;
+  p->dt = (hd_float)h->tsamp;
+  p->f0 = (hd_float)h->fch1;
+  p->df = (hd_float)h->foff;
+  p->nbeams = h->nbeams > 0 ? (hd_size)h->nbeams : 1;
+  if (!p->override_beam) p->beam = h->ibeam > 0 ? (hd_size)(h->ibeam - 1) : 0;
+  p->utc_start = (time_t)hd_mjd_to_utc(h->tstart);
+  // the data source keeps tsamp as a float and its rate as 1 / that float
+  // (SigprocFile.C:38-39, DataSource.h:90)
+  const float ts = (float)h->tsamp;
+  const double rate = 1 / ts;
+  p->spectra_per_second = (hd_size)rate;
+  return HD_NO_ERROR;
+}
+
+hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps_gulp,
+                                hd_gulp_callback on_gulp, void* user, hd_size* total_nsamps,
+                                hd_size* ngulps) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!path) return HD_INVALID_POINTER;
+  hd_sigproc_header h;
+  hd_error e = hd_read_sigproc_header(path, &h);
+  if (e != HD_NO_ERROR) return e;
+  if (h.nbits != 8) return HD_INVALID_NBITS;
+  const size_t nbeams = h.nbeams > 0 ? (size_t)h.nbeams : 1;
+  const size_t stride = (size_t)h.nchans;  // bytes per spectrum (8-bit)
+  if (nsamps_gulp == 0 || nsamps_gulp % nbeams != 0) return HD_INVALID_STRIDE;
+  if (cudaSetDevice(hdb::pipeline_device(pl)) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return HD_INVALID_POINTER;
+  std::fseek(f, h.size, SEEK_SET);
+
+  const size_t max_overlap = hd_get_max_overlap(pl, nbeams);  // all beams
+  const size_t cap = (nsamps_gulp + max_overlap) * stride;
+  const size_t block = nsamps_gulp * stride;
+  hd_byte* d_buf[2] = {nullptr, nullptr};
+  hd_byte* h_blk[2] = {nullptr, nullptr};
+  cudaStream_t s = nullptr;
+  auto cleanup = [&]() {
+    for (auto p : d_buf) if (p) cudaFree(p);
+    for (auto p : h_blk) if (p) cudaFreeHost(p);
+    if (s) cudaStreamDestroy(s);
+    std::fclose(f);
+  };
+  if (cudaMalloc(&d_buf[0], cap) != cudaSuccess || cudaMalloc(&d_buf[1], cap) != cudaSuccess ||
+      cudaMallocHost(&h_blk[0], block) != cudaSuccess ||
+      cudaMallocHost(&h_blk[1], block) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    cleanup();
+    return HD_MEM_ALLOC_FAILED;
+  }
+  auto read_block = [&](hd_byte* dst) -> size_t {
+    return std::fread(dst, 1, block, f) / stride;  // SigprocFile.C:59-68
+  };
+
+  // the first block is searched as it is (overlap 0)
+  size_t nsamps_read = read_block(h_blk[0]);
+  int cur = 0, hb = 0;
+  size_t overlap = 0;      // per beam
+  size_t total = 0;        // samples per beam searched so far
+  size_t gulps = 0;
+  std::vector<hd_candidate> cands;
+  hd_error result = HD_NO_ERROR;
+  // the first block lands at the start of buffer 0 (beams in sequence)
+  if (nsamps_read &&
+      cudaMemcpyAsync(d_buf[0], h_blk[0], nsamps_read * stride, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess) {
+    cleanup();
+    return HD_MEM_COPY_FAILED;
+  }
+  bool stop = nsamps_read < nsamps_gulp;  // a short first block is never searched
+  while (nsamps_read && !stop) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      result = HD_MEM_COPY_FAILED;
+      break;
+    }
+    const size_t to_process = nsamps_gulp + overlap * nbeams;
+    // read the next block on the host while the GPU searches this gulp
+    size_t next_read = 0;
+    std::thread reader([&]() { next_read = read_block(h_blk[hb ^ 1]); });
+    hd_size processed = 0;
+    e = hd_execute_device(pl, d_buf[cur], to_process, 8, total, nbeams, &processed);
+    reader.join();
+    if (e != HD_NO_ERROR && e != HD_TOO_MANY_EVENTS) {
+      result = e;
+      break;
+    }
+    gulps++;
+    hd_size n = 0;
+    hd_get_candidates(pl, nullptr, &n);
+    cands.resize(n);
+    if (n) hd_get_candidates(pl, cands.data(), &n);
+    if (on_gulp) on_gulp(user, cands.data(), n, (hd_size)total);
+    // heimdall.C:209-265: overlap per beam, samples searched, and the copy
+    // of each beam's overlap to the front of its region in the next buffer
+    overlap = (to_process - processed) / nbeams;
+    total += processed / nbeams;
+    const size_t per_beam = to_process / nbeams;
+    const size_t done_per_beam = per_beam - overlap;
+    const size_t next_per_beam = overlap + nsamps_gulp / nbeams;
+    const int nxt = cur ^ 1;
+    for (size_t b = 0; b < nbeams && overlap > 0; b++) {
+      const size_t from = b * per_beam + done_per_beam;
+      const size_t to = b * next_per_beam;
+      if (cudaMemcpyAsync(d_buf[nxt] + to * stride, d_buf[cur] + from * stride, overlap * stride,
+                          cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        result = HD_MEM_COPY_FAILED;
+        break;
+      }
+    }
+    if (result != HD_NO_ERROR) break;
+    nsamps_read = next_read;
+    hb ^= 1;
+    // a short block ends the search (heimdall.C:269-272,285-287)
+    if (nsamps_read < nsamps_gulp) break;
+    for (size_t b = 0; b < nbeams; b++) {
+      const size_t from = b * nsamps_gulp / nbeams;
+      const size_t to_b = (b + 1) * nsamps_gulp / nbeams;
+      const size_t to = overlap + b * (nsamps_gulp / nbeams + overlap);
+      if (cudaMemcpyAsync(d_buf[nxt] + to * stride, h_blk[hb] + from * stride,
+                          (to_b - from) * stride, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        result = HD_MEM_COPY_FAILED;
+        break;
+      }
+    }
+    if (result != HD_NO_ERROR) break;
+    cur = nxt;
+  }
+  cudaStreamSynchronize(s);
+  cleanup();
+  if (total_nsamps) *total_nsamps = total;
+  if (ngulps) *ngulps = gulps;
+  return result;
+}
+
+}  // extern "C"

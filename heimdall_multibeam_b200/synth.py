@@ -430,3 +430,48 @@ def make_training_gulps_device(torch, seeds: Sequence[int], w: Workload = None,
         all_events.append(events)
     return out, all_pulses, all_events
 
+
+# ---------------------------------------------------------------------------
+# Sigproc filterbank files
+# ---------------------------------------------------------------------------
+SIGPROC_INT = ("nchans", "telescope_id", "machine_id", "data_type", "ibeam", "nbeams", "nbits",
+               "barycentric", "pulsarcentric", "nbins", "nsamples", "nifs", "npuls")
+SIGPROC_DOUBLE = ("az_start", "za_start", "src_raj", "src_dej", "tstart", "tsamp", "period",
+                  "fch1", "foff", "refdm")
+SIGPROC_STR = ("source_name", "rawdatafile")
+
+
+def write_sigproc(path: str, data: Optional[np.ndarray] = None, order: Sequence[str] = (),
+                  **fields) -> int:
+    """Writes a sigproc file: HEADER_START, each field as its keyword string
+    (4-byte length + characters) followed by its value (int32, float64, a
+    string, or one byte for `signed`; an unknown keyword is written alone),
+    HEADER_END, then data (time-major uint8 spectra).  `order` fixes the
+    keyword order (the remaining fields follow).  Returns the header size."""
+    import struct
+
+    def w_str(f, t: str):
+        b = t.encode()
+        f.write(struct.pack("<i", len(b)))
+        f.write(b)
+
+    keys = list(order) + [k for k in fields if k not in order]
+    with open(path, "wb") as f:
+        w_str(f, "HEADER_START")
+        for k in keys:
+            v = fields[k]
+            w_str(f, k)
+            if k in SIGPROC_INT:
+                f.write(struct.pack("<i", int(v)))
+            elif k in SIGPROC_DOUBLE:
+                f.write(struct.pack("<d", float(v)))
+            elif k in SIGPROC_STR:
+                w_str(f, str(v))
+            elif k == "signed":
+                f.write(struct.pack("<B", int(v)))
+        w_str(f, "HEADER_END")
+        size = f.tell()
+        if data is not None:
+            f.write(np.ascontiguousarray(data, dtype=np.uint8).tobytes())
+    return size
+

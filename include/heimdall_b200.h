@@ -304,6 +304,49 @@ typedef struct hd_candidate {
   hd_size  beam;
 } hd_candidate;
 
+/* Sigproc filterbank input and the gulp loop (no C counterpart in the
+ * reference: Formats/hd/header.h and SigprocFile.C read the file in C++,
+ * Applications/heimdall.C:153-292 runs the loop).
+ *
+ * The header fields the reference reads (Formats/hd/header.h:26-56);
+ * strings are NUL-terminated, size is the header's length in bytes, and a
+ * missing nsamples is the whole file's size over one spectrum's bytes
+ * (header.h:190-193, header included). */
+typedef struct {
+  char   source_name[80];
+  char   rawdatafile[80];
+  double az_start, za_start, src_raj, src_dej, tstart, tsamp, period, fch1, foff, refdm;
+  int    nchans, telescope_id, machine_id, data_type, ibeam, nbeams, nbits, barycentric,
+         pulsarcentric, nbins, nsamples, nifs, npuls;
+  unsigned char signed_data;
+  int    size;
+  int    unknown_keys;   /* keywords the reader does not know (the reference warns) */
+} hd_sigproc_header;
+
+hd_error hd_read_sigproc_header(const char* path, hd_sigproc_header* header);
+/* MJD -> Unix time as the reference's data sources convert tstart
+ * (Formats/hd/DataSource.h:49-82, local time zone through mktime). */
+long long hd_mjd_to_utc(double mjd);
+/* The hd_params fields heimdall.C takes from its data source: nchans, dt,
+ * f0, df, nbeams, beam (ibeam - 1 unless override_beam), utc_start and
+ * spectra_per_second. */
+hd_error hd_params_from_sigproc(const hd_sigproc_header* header, struct hd_params* params);
+/* Called after every gulp with that gulp's candidates (as hd_get_candidates)
+ * and the first sample index of the gulp. */
+typedef void (*hd_gulp_callback)(void* user, const hd_candidate* candidates, hd_size count,
+                                 hd_size first_idx);
+/* Searches an 8-bit sigproc file gulp by gulp as heimdall.C's loop does: the
+ * first gulp is nsamps_gulp spectra, each later one the previous gulp's
+ * unprocessed overlap (boxcar_max + max_delay per beam) followed by
+ * nsamps_gulp new spectra; a block shorter than nsamps_gulp ends the search
+ * and is not searched.  With nbeams > 1 in the header each block holds the
+ * beams in sequence.  The overlap stays on the device; the next block is
+ * read from the file while the GPU searches.  Candidates go to the
+ * pipeline's .cand files and to on_gulp (may be NULL). */
+hd_error hd_search_sigproc_file(hd_pipeline pipeline, const char* path, hd_size nsamps_gulp,
+                                hd_gulp_callback on_gulp, void* user, hd_size* total_nsamps,
+                                hd_size* ngulps);
+
 /* Candidates of the last hd_execute, in .cand order.  Copies
  * min(*count, available) rows into out (out may be NULL to query) and sets
  * *count to the number available. */

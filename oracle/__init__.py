@@ -380,3 +380,50 @@ def cnn_run(params: np.ndarray, dm_time: np.ndarray, freq_time: np.ndarray, labe
         lib().or_cnn_run(_fptr(params), _fptr(dm_time), _fptr(freq_time), None, n, _fptr(probs),
                          None, None)
     return probs, grads, loss
+
+
+# ---------------------------------------------------------------------------
+# Sigproc input and the gulp loop (Applications/heimdall.C:153-292)
+# ---------------------------------------------------------------------------
+def ref_sigproc_dump(path: str, mjds=()) -> dict:
+    """The reference's own header reader (Formats/hd/header.h:133-198) and
+    mjd2utctm (Formats/hd/DataSource.h:49-82), run through
+    _ref/sigproc_dump (built from the reference's headers)."""
+    import json
+    import subprocess
+    exe = os.path.join(HERE, "_ref", "sigproc_dump")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    r = subprocess.run([exe, path] + ["%.17g" % m for m in mjds], capture_output=True,
+                       text=True, check=True)
+    return json.loads(r.stdout)
+
+
+def ref_sigproc_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "sigproc_dump"))
+
+
+def gulp_plan(nsamps_file: int, nsamps_gulp: int, overlap: int):
+    """heimdall.C's loop on one beam as a list of (first spectrum of the file
+    in the gulp, spectra in the gulp, first_idx): the first gulp is the first
+    block; after a gulp of n spectra the pipeline processes n - overlap
+    (overlap = boxcar_max + max_delay), which the next gulp carries in front
+    of the next block; a block shorter than nsamps_gulp ends the loop
+    unsearched."""
+    plan = []
+    if nsamps_file < nsamps_gulp:
+        return plan
+    start, n, total = 0, nsamps_gulp, 0
+    block = 0
+    while True:
+        plan.append((start, n, total))
+        processed = n - overlap if n > overlap else 0
+        carry = n - processed
+        total += processed
+        block += 1
+        if (block + 1) * nsamps_gulp > nsamps_file:
+            break
+        start = block * nsamps_gulp - carry
+        n = carry + nsamps_gulp
+    return plan
+

@@ -58,7 +58,8 @@ int main(void) {{
 
 
 @pytest.mark.parametrize("cls,cname", [(hdb.HdParams, "struct hd_params"),
-                                       (hdb.HdCandidate, "hd_candidate")])
+                                       (hdb.HdCandidate, "hd_candidate"),
+                                       (hdb.HdSigprocHeader, "hd_sigproc_header")])
 def test_struct_layout_matches_c(cls, cname):
     fields = [f for f, _ in cls._fields_]
     size, lay = _c_layout(cname, fields)
