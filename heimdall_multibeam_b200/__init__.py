@@ -130,6 +130,11 @@ class HdSigprocHeader(C.Structure):
 GULP_CALLBACK = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t)
 
 
+class HdCoincidence(C.Structure):
+    """hd_coincidence (include/heimdall_b200.h)."""
+    _fields_ = [("nbeams", C.c_uint), ("primary_beam", C.c_uint), ("max_snr", C.c_float)]
+
+
 # symbol -> (restype, argtypes); every function include/*.h declares
 _P = C.c_void_p
 _SZ = C.c_size_t
@@ -168,6 +173,8 @@ SYMBOLS = {
     "hd_get_dedisp_tile": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
     "hd_read_sigproc_header": (C.c_int, [C.c_char_p, C.POINTER(HdSigprocHeader)]),
+    "hd_coincide": (C.c_int, [_P, _SZ, _SZ, C.c_uint, C.c_uint, C.c_int, _P]),
+    "hd_write_coincident_candidates": (C.c_int, [C.c_char_p, _P, _P, _SZ]),
     "hd_mjd_to_utc": (C.c_longlong, [C.c_double]),
     "hd_params_from_sigproc": (C.c_int, [C.POINTER(HdSigprocHeader), C.POINTER(HdParams)]),
     "hd_search_sigproc_file": (C.c_int, [_P, C.c_char_p, _SZ, GULP_CALLBACK, C.c_void_p, _SZP,
@@ -280,6 +287,53 @@ def params_from_sigproc(path: str, params: Optional[HdParams] = None) -> HdParam
     if err != HD_NO_ERROR:
         raise HdError(err, "hd_params_from_sigproc")
     return p
+
+
+def coincide(cands: np.ndarray, nbeams: int, sep_time: int = 3, sep_filter: int = 4,
+             gpu_id: int = 0) -> np.ndarray:
+    """hd_coincide on a CANDIDATE_DTYPE array: per candidate (nbeams,
+    primary_beam, max_snr) as a structured array."""
+    c = np.ascontiguousarray(cands, dtype=CANDIDATE_DTYPE)
+    out = (HdCoincidence * max(len(c), 1))()
+    err = lib().hd_coincide(c.ctypes.data, len(c), nbeams, sep_time, sep_filter, gpu_id,
+                            C.cast(out, C.c_void_p))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_coincide")
+    res = np.zeros(len(c), [("nbeams", "<u4"), ("primary_beam", "<u4"), ("max_snr", "<f4")])
+    if len(c):
+        C.memmove(res.ctypes.data, out, len(c) * C.sizeof(HdCoincidence))
+    return res
+
+
+def write_coincident_candidates(path: str, cands: np.ndarray, co: np.ndarray) -> None:
+    c = np.ascontiguousarray(cands, dtype=CANDIDATE_DTYPE)
+    o = np.ascontiguousarray(co)
+    err = lib().hd_write_coincident_candidates(path.encode(), c.ctypes.data, o.ctypes.data,
+                                               len(c))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_write_coincident_candidates")
+
+
+def parse_cand_lines(lines) -> np.ndarray:
+    """.cand text lines -> CANDIDATE_DTYPE, numbers read as the reference's
+    istream does (floats by strtof, integers exactly)."""
+    libc = C.CDLL(None)
+    libc.strtof.restype = C.c_float
+    libc.strtof.argtypes = [C.c_char_p, C.c_void_p]
+    out = np.zeros(len(lines), CANDIDATE_DTYPE)
+    for i, ln in enumerate(lines):
+        f = ln.split()
+        out[i]["snr"] = libc.strtof(f[0].encode(), None)
+        out[i]["samp_idx"] = int(f[1])
+        out[i]["time"] = libc.strtof(f[2].encode(), None)
+        out[i]["filter"] = int(f[3])
+        out[i]["dm_trial"] = int(f[4])
+        out[i]["dm"] = libc.strtof(f[5].encode(), None)
+        out[i]["members"] = int(f[6])
+        out[i]["begin"] = int(f[7])
+        out[i]["end"] = int(f[8])
+        out[i]["beam"] = int(f[9])
+    return out
 
 
 class Pipeline:

@@ -304,6 +304,27 @@ typedef struct hd_candidate {
   hd_size  beam;
 } hd_candidate;
 
+/* Cross-beam coincidence of candidate lists on the GPU (no C counterpart:
+ * the reference's coincidencer does it in C++, Applications/Candidates.C
+ * compute_coincidence 236-291 with Candidate::is_coincident 64-77).
+ * cands[i].beam (1..nbeams) selects each candidate's beam list; within a
+ * beam, the input order is the list order.  For every candidate, out[i]
+ * holds the number of beams with a coincident candidate (itself included),
+ * the beam and S/N of the brightest first-coincident one (itself when none
+ * is brighter). */
+typedef struct {
+  unsigned int nbeams;
+  unsigned int primary_beam;
+  hd_float     max_snr;
+} hd_coincidence;
+hd_error hd_coincide(const hd_candidate* candidates, hd_size count, hd_size nbeams,
+                     unsigned int sep_time, unsigned int sep_filter, int gpu_id,
+                     hd_coincidence* out);
+/* The reference's _all.cand lines (Candidates.C:85-93, 293-326): beam by
+ * beam, each with the coincidence columns. */
+hd_error hd_write_coincident_candidates(const char* path, const hd_candidate* candidates,
+                                        const hd_coincidence* coincidence, hd_size count);
+
 /* Sigproc filterbank input and the gulp loop (no C counterpart in the
  * reference: Formats/hd/header.h and SigprocFile.C read the file in C++,
  * Applications/heimdall.C:153-292 runs the loop).

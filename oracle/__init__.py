@@ -427,3 +427,59 @@ def gulp_plan(nsamps_file: int, nsamps_gulp: int, overlap: int):
         n = carry + nsamps_gulp
     return plan
 
+
+# ---------------------------------------------------------------------------
+# Cross-beam coincidence (Applications/Candidates.C)
+# ---------------------------------------------------------------------------
+def coincide(beams, sep_time: int, sep_filter: int):
+    """compute_coincidence (Candidates.C:236-291) with is_coincident (64-77):
+    beams is one list of candidate dicts (snr, samp_idx, filter, dm_trial,
+    beam) per beam in list order; returns per beam the list of (nbeams,
+    primary_beam, max_snr).  S/N arithmetic in float32 as the reference's."""
+    f32 = np.float32
+    out = []
+    for i, bi in enumerate(beams):
+        res = []
+        for cj in bi:
+            nb, prim, best = 1, int(cj["beam"]), f32(cj["snr"])
+            for k, bk in enumerate(beams):
+                if k == i:
+                    continue
+                for cl in bk:
+                    fmax = max(int(cl["filter"]), int(cj["filter"]))
+                    tol = int(f32(sep_time) * f32(2.0 ** fmax))
+                    if abs(int(cl["samp_idx"]) - int(cj["samp_idx"])) > tol:
+                        continue
+                    if abs(int(cl["dm_trial"]) - int(cj["dm_trial"])) > 9999:
+                        continue
+                    if abs(int(cl["filter"]) - int(cj["filter"])) > sep_filter:
+                        continue
+                    a, b = f32(cl["snr"]), f32(cj["snr"])
+                    if not (f32(abs(f32(a - b))) / f32(a + b) <= f32(0.4)):
+                        continue
+                    nb += 1
+                    if a > best:
+                        prim, best = int(cl["beam"]), a
+                    break
+            res.append((nb, prim, best))
+        out.append(res)
+    return out
+
+
+def ref_coinc_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "coinc_ref"))
+
+
+def ref_coincide(files, nbeams: int, sep_time: int, sep_filter: int) -> List[str]:
+    """The reference's coincidencer (Candidates.C, _ref/coinc_ref) on .cand
+    files that sit in one directory; returns the lines of the _all.cand it
+    writes there."""
+    exe = os.path.join(HERE, "_ref", "coinc_ref")
+    d = os.path.dirname(os.path.abspath(files[0]))
+    names = [os.path.basename(f) for f in files]
+    subprocess.run([exe, str(nbeams), str(sep_time), str(sep_filter)] + names, cwd=d,
+                   check=True, capture_output=True)
+    out = os.path.join(d, names[0].split("_")[0] + "_all.cand")
+    with open(out) as f:
+        return f.read().splitlines()
+

@@ -59,7 +59,8 @@ int main(void) {{
 
 @pytest.mark.parametrize("cls,cname", [(hdb.HdParams, "struct hd_params"),
                                        (hdb.HdCandidate, "hd_candidate"),
-                                       (hdb.HdSigprocHeader, "hd_sigproc_header")])
+                                       (hdb.HdSigprocHeader, "hd_sigproc_header"),
+                                       (hdb.HdCoincidence, "hd_coincidence")])
 def test_struct_layout_matches_c(cls, cname):
     fields = [f for f, _ in cls._fields_]
     size, lay = _c_layout(cname, fields)
