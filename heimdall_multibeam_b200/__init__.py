@@ -153,6 +153,7 @@ SYMBOLS = {
     "hd_clean_filterbank_rfi": (C.c_int, [_P, _P, _SZ, _SZ, _P, _P, C.c_float, C.c_float,
                                           C.c_float, _SZ, _SZ]),
     "hd_set_cleaning": (C.c_int, [_P, C.c_int]),
+    "hd_set_narrow_band": (C.c_int, [_P, C.c_int]),
     "hd_execute_device": (C.c_int, [_P, _P, _SZ, _SZ, _SZ, _SZ, _SZP]),
     "hd_execute_beams": (C.c_int, [_P, C.POINTER(_P), _SZ, _SZ, _SZ, _SZ, _SZ, _SZP, C.c_int,
                                    C.POINTER(C.c_int), _SZP]),
@@ -340,7 +341,8 @@ class Pipeline:
     """hd_create_pipeline / hd_execute / hd_destroy_pipeline."""
 
     def __init__(self, params: Optional[HdParams] = None, cleaning: bool = True,
-                 channel_zaps: Sequence[Tuple[int, int]] = (), **overrides):
+                 channel_zaps: Sequence[Tuple[int, int]] = (), narrow_band: bool = False,
+                 **overrides):
         L = lib()
         self._p = None
         if params is None:
@@ -361,6 +363,7 @@ class Pipeline:
             raise HdError(err, "hd_create_pipeline")
         self._p = h
         L.hd_set_cleaning(self._p, 1 if cleaning else 0)
+        L.hd_set_narrow_band(self._p, 1 if narrow_band else 0)
 
     def close(self) -> None:
         if self._p:

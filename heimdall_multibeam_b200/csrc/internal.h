@@ -53,6 +53,13 @@ cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
                                    size_t pitch, cudaStream_t s, size_t units = 1,
                                    size_t out_unit = 0);
+// Narrow-band RFI zapping of `units` TF filterbanks of nsamps spectra in
+// place (the branch Pipeline/clean_filterbank_rfi.cu:303-351 disables);
+// scratch of narrow_band_scratch_bytes().
+size_t narrow_band_scratch_bytes(size_t units, size_t nsamps, int nchans, float dt,
+                                 float baseline_length);
+cudaError_t narrow_band(uint8_t* tf, size_t units, size_t nsamps, int nchans, float dt,
+                        float baseline_length, float rfi_tol, void* scratch, cudaStream_t s);
 cudaError_t launch_dm0_sum(const uint8_t* in, size_t nsamps, int nchans, float* out,
                            cudaStream_t s);
 cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* mask,

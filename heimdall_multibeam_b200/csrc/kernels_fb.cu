@@ -7,6 +7,9 @@
 //   FT  (device working copy): channel c at ft + c*pitch, one byte per sample,
 //       pitch a multiple of 64 bytes with zero padding past nsamps so the
 //       dedispersion tiles can be fetched with 16-byte-aligned bulk copies.
+#include <algorithm>
+#include <vector>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -162,6 +165,166 @@ __global__ void __launch_bounds__(256) k_zap_to_ft(const uint8_t* __restrict__ i
     }
     size_t t = t0 + 4 * lane;
     if (t < nsamps) reinterpret_cast<uint32_t*>(out_ft + (size_t)c * pitch + t)[0] = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Narrow-band RFI: the branch of Pipeline/clean_filterbank_rfi.cu:303-351 that
+// the reference disables (measure_bandpass.cu:45-275 and
+// zap_narrow_rfi_functor, clean_filterbank_rfi.cu:114-193).  The data are cut
+// into stretches of baseline_length / dt spectra per filterbank (unit); each
+// stretch gets its own bandpass and band deviation from 3125 spectra drawn
+// with thrust::default_random_engine(123456), and its bytes are zapped
+// against them.
+// ---------------------------------------------------------------------------
+constexpr int NB_SPECTRA = 3125;
+
+// spectrum draws of each stretch, in order (measure_bandpass.cu:95-108)
+__global__ void k_nb_indices(const unsigned* __restrict__ len, int nstretch,
+                             unsigned* __restrict__ idx) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nstretch) return;
+  uint32_t st = 123456u;
+  for (int i = 0; i < NB_SPECTRA; i++)
+    idx[(size_t)g * NB_SPECTRA + i] = uniform_uint(st, 0u, len[g] - 1u);
+}
+
+// spectra[g][i][c] = (float) fb[(start[g] + idx[g][i]) * C + c]
+__global__ void k_nb_gather(const uint8_t* __restrict__ fb, int C,
+                            const unsigned long long* __restrict__ start,
+                            const unsigned* __restrict__ idx, size_t total,
+                            float* __restrict__ out) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t gi = e / C;
+    const int c = (int)(e % C);
+    const size_t g = gi / NB_SPECTRA;
+    out[e] = (float)fb[(size_t)(start[g] + idx[gi]) * C + c];
+  }
+}
+
+// one level of the recursive median: out[g][a][c] = median of in[g][5a..5a+4][c]
+__global__ void k_nb_scrunch5(const float* __restrict__ in, int C, int count_in, int nstretch,
+                              float* __restrict__ out) {
+  const int count_out = count_in / 5;
+  const size_t total = (size_t)nstretch * count_out * C;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e % C);
+    const size_t r = e / C;
+    const size_t a = r % count_out, g = r / count_out;
+    const float* b = in + ((size_t)g * count_in + 5 * a) * C + c;
+    out[e] = med5(b[0], b[C], b[2 * (size_t)C], b[3 * (size_t)C], b[4 * (size_t)C]);
+  }
+}
+
+// median_filter5_kernel (median_filter.cu:99-124): window shrunk at the ends
+__device__ __forceinline__ float nb_filter5(const float* in, unsigned count, unsigned i) {
+  if (i > 1 && i < count - 2) return med5(in[i - 2], in[i - 1], in[i], in[i + 1], in[i + 2]);
+  if (i == 0) return med3(in[i], in[i + 1], in[i + 2]);
+  if (i == 1) return med4(in[i - 1], in[i], in[i + 1], in[i + 2]);
+  if (i == count - 1) return med3(in[i], in[i - 1], in[i - 2]);
+  return med4(in[i + 1], in[i], in[i - 1], in[i - 2]);
+}
+
+// measure_bandpass.cu:141-163 / 220-245 on v[g] (C values, scaled first by
+// `scale` unless it is 1): scrunch by 5, 5-wide median, mean of neighbours
+// (thrust::adjacent_difference), stretch to C/5*5 and extrapolate the rest.
+// One block per stretch; tmp[g] holds C/5 values.
+__global__ void k_nb_smooth(float* __restrict__ v, float* __restrict__ tmp, int C, float scale) {
+  float* x = v + (size_t)blockIdx.x * C;
+  const unsigned n5 = (unsigned)C / 5;
+  float* t = tmp + (size_t)blockIdx.x * (n5 + 1);
+  if (scale != 1.f) {
+    for (int i = threadIdx.x; i < C; i += blockDim.x) x[i] = __fmul_rn(x[i], scale);
+    __syncthreads();
+  }
+  for (unsigned j = threadIdx.x; j < n5; j += blockDim.x)
+    t[j] = med5(x[5 * j], x[5 * j + 1], x[5 * j + 2], x[5 * j + 3], x[5 * j + 4]);
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < n5; j += blockDim.x) x[j] = nb_filter5(t, n5, j);
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < n5; j += blockDim.x)
+    t[j] = j == 0 ? x[0] : __fmul_rn(0.5f, __fadd_rn(x[j], x[j - 1]));
+  // for some channel counts (1140, 2220, ...) the last stretched sample lands
+  // just past the last input with a fraction above 1e-5 and reads t[n5] (the
+  // reference reads past its vector there): defined as 0
+  if (threadIdx.x == 0) t[n5] = 0.f;
+  __syncthreads();
+  const float step = __fdiv_rn((float)(n5 - 1), (float)(n5 * 5 - 1));
+  for (unsigned j = threadIdx.x; j < n5 * 5; j += blockDim.x) x[j] = stretch_at(t, j, step);
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (unsigned i = n5 * 5; i < (unsigned)C; i++)
+      x[i] = __fsub_rn(__fmul_rn(2.f, x[i - 1]), x[i - 2]);
+}
+
+// spectra[g][i][c] = |spectra[g][i][c] - bandpass[g][c]|
+__global__ void k_nb_absdev(float* __restrict__ sp, const float* __restrict__ bp, int C,
+                            size_t total) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t g = e / ((size_t)NB_SPECTRA * C);
+    sp[e] = fabsf(__fsub_rn(sp[e], bp[g * C + e % C]));
+  }
+}
+
+// rms[g] = the (C/2)-th smallest of mad[g] (std::nth_element), by ranks
+__global__ void k_nb_rms(const float* __restrict__ mad, int C, float* __restrict__ rms) {
+  const float* m = mad + (size_t)blockIdx.x * C;
+  const int k = C / 2;
+  for (int i = threadIdx.x; i < C; i += blockDim.x) {
+    const float x = m[i];
+    int lt = 0, le = 0;
+    for (int j = 0; j < C; j++) {
+      lt += m[j] < x;
+      le += m[j] <= x;
+    }
+    if (lt <= k && k < le) rms[blockIdx.x] = x;  // equal values only
+  }
+}
+
+// zap_narrow_rfi_functor over each spectrum's words in order (one thread per
+// spectrum; draws read the spectrum as earlier words left it, the sequential
+// semantics of the functor's in-place reads).  Bandpass entry and draw range
+// use channel w + k as the reference does; the hash takes the word's index
+// within its filterbank.
+__global__ void k_nb_zap(uint32_t* __restrict__ data, size_t nsamps, int units, int C,
+                         size_t nsmooth, int nsub, const float* __restrict__ bp,
+                         const float* __restrict__ rms, float rfi_tol, unsigned max_dist) {
+  const size_t tg = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tg >= nsamps * (size_t)units) return;
+  const size_t u = tg / nsamps, tl = tg % nsamps;
+  const size_t g = u * nsub + tl / nsmooth;
+  const float* b = bp + g * C;
+  const float thresh = __fmul_rn(rfi_tol, rms[g]);
+  const unsigned stride = (unsigned)C / 4, nch = (unsigned)C;
+  uint32_t* row = data + tg * stride;
+  for (unsigned w = 0; w < stride; w++) {
+    const unsigned i = (unsigned)(tl * stride + w);
+    uint32_t word = row[w];
+    uint32_t st = mix32(i) % 2147483647u;
+    if (st == 0) st = 1;
+    bool any = false;
+    for (unsigned k = 0; k < 4; k++) {
+      const unsigned c = w + k;
+      const uint32_t val = (word >> (k * 8)) & 0xFFu;
+      if (fabsf(__fsub_rn(__uint2float_rn(val), b[c])) > thresh) {
+        any = true;
+        const unsigned min_c = c > max_dist ? c - max_dist : 0;
+        const unsigned max_c = c < nch - 1 - max_dist ? c + max_dist : nch - 1;
+        unsigned nc = uniform_uint(st, min_c, max_c);
+        uint32_t nv = (row[nc / 4] >> ((nc % 4) * 8)) & 0xFFu;
+        int attempts = 0;
+        while (fabsf(__fsub_rn(__uint2float_rn(nv), b[nc])) > thresh && ++attempts < 11) {
+          nc = uniform_uint(st, min_c, max_c);
+          nv = (row[nc / 4] >> ((nc % 4) * 8)) & 0xFFu;
+        }
+        word &= ~(0xFFu << (k * 8));
+        word |= nv << (k * 8);
+      }
+    }
+    if (any) row[w] = word;
   }
 }
 
@@ -389,6 +552,105 @@ cudaError_t launch_zap(const uint8_t* in, size_t nsamps, int nchans, const int* 
   dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128));
   k_zap_to_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, mask, max_resample_dist, out_ft, pitch,
                                    out_tf); note_launch();
+  return cudaGetLastError();
+}
+
+// Scratch layout of the narrow-band stage (bytes, 256-aligned pieces).
+struct NbLayout {
+  size_t idx, start, len, s1, s2, s3, s4, s5, bp, mad, tmp, rms, total;
+};
+static NbLayout nb_layout(size_t nstretch, int C) {
+  NbLayout L{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  const size_t n = nstretch;
+  L.idx = take(n * NB_SPECTRA * sizeof(unsigned));
+  L.start = take(n * sizeof(unsigned long long));
+  L.len = take(n * sizeof(unsigned));
+  L.s1 = take(n * NB_SPECTRA * C * sizeof(float));
+  L.s2 = take(n * (NB_SPECTRA / 5) * C * sizeof(float));
+  L.s3 = take(n * (NB_SPECTRA / 25) * C * sizeof(float));
+  L.s4 = take(n * (NB_SPECTRA / 125) * C * sizeof(float));
+  L.s5 = take(n * (NB_SPECTRA / 625) * C * sizeof(float));
+  L.bp = take(n * C * sizeof(float));
+  L.mad = take(n * C * sizeof(float));
+  L.tmp = take(n * (C / 5 + 1) * sizeof(float));
+  L.rms = take(n * sizeof(float));
+  L.total = o;
+  return L;
+}
+
+size_t narrow_band_stretches(size_t nsamps, float dt, float baseline_length) {
+  const size_t nsmooth = (size_t)(baseline_length / (1 * dt));
+  return nsmooth ? (nsamps + nsmooth - 1) / nsmooth : 0;
+}
+
+size_t narrow_band_scratch_bytes(size_t units, size_t nsamps, int nchans, float dt,
+                                 float baseline_length) {
+  return nb_layout(units * narrow_band_stretches(nsamps, dt, baseline_length), nchans).total;
+}
+
+cudaError_t narrow_band(uint8_t* tf, size_t units, size_t nsamps, int nchans, float dt,
+                        float baseline_length, float rfi_tol, void* scratch, cudaStream_t s) {
+  const size_t nsmooth = (size_t)(baseline_length / (1 * dt));
+  const int C = nchans;
+  if (nsmooth == 0 || C % 4 != 0 || C < 20 || units == 0) return cudaErrorInvalidValue;
+  if (nsamps * (size_t)(C / 4) >= 0xFFFFFFFFull) return cudaErrorInvalidValue;
+  const size_t nsub = (nsamps + nsmooth - 1) / nsmooth;
+  const size_t ns = units * nsub;
+  const NbLayout L = nb_layout(ns, C);
+  uint8_t* base = static_cast<uint8_t*>(scratch);
+  auto F = [&](size_t off) { return reinterpret_cast<float*>(base + off); };
+  unsigned* idx = reinterpret_cast<unsigned*>(base + L.idx);
+  unsigned long long* start = reinterpret_cast<unsigned long long*>(base + L.start);
+  unsigned* len = reinterpret_cast<unsigned*>(base + L.len);
+  std::vector<unsigned long long> h_start(ns);
+  std::vector<unsigned> h_len(ns);
+  for (size_t u = 0; u < units; u++)
+    for (size_t g = 0; g < nsub; g++) {
+      h_start[u * nsub + g] = u * nsamps + g * nsmooth;
+      h_len[u * nsub + g] = (unsigned)std::min(nsmooth, nsamps - g * nsmooth);
+    }
+  cudaError_t e = cudaMemcpyAsync(start, h_start.data(), ns * sizeof(unsigned long long),
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(len, h_len.data(), ns * sizeof(unsigned), cudaMemcpyHostToDevice, s);
+  // both copies read host vectors that go out of scope: finish them here
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  auto blocks = [](size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); };
+  k_nb_indices<<<(unsigned)((ns + 63) / 64), 64, 0, s>>>(len, (int)ns, idx); note_launch();
+  const size_t tot1 = ns * NB_SPECTRA * (size_t)C;
+  k_nb_gather<<<blocks(tot1), 256, 0, s>>>(tf, C, start, idx, tot1, F(L.s1)); note_launch();
+  // bandpass: recursive median, smoothing
+  const size_t lev[6] = {L.s1, L.s2, L.s3, L.s4, L.s5, L.bp};
+  int count = NB_SPECTRA;
+  for (int l = 0; l < 5; l++, count /= 5) {
+    k_nb_scrunch5<<<blocks(ns * (count / 5) * (size_t)C), 256, 0, s>>>(F(lev[l]), C, count,
+                                                                      (int)ns, F(lev[l + 1]));
+    note_launch();
+  }
+  k_nb_smooth<<<(unsigned)ns, 256, 0, s>>>(F(L.bp), F(L.tmp), C, 1.f); note_launch();
+  // band deviation: |spectra - bandpass|, recursive median, x 1.4826, smoothing
+  k_nb_absdev<<<blocks(tot1), 256, 0, s>>>(F(L.s1), F(L.bp), C, tot1); note_launch();
+  const size_t lev2[6] = {L.s1, L.s2, L.s3, L.s4, L.s5, L.mad};
+  count = NB_SPECTRA;
+  for (int l = 0; l < 5; l++, count /= 5) {
+    k_nb_scrunch5<<<blocks(ns * (count / 5) * (size_t)C), 256, 0, s>>>(F(lev2[l]), C, count,
+                                                                       (int)ns, F(lev2[l + 1]));
+    note_launch();
+  }
+  k_nb_smooth<<<(unsigned)ns, 256, 0, s>>>(F(L.mad), F(L.tmp), C, 1.4826f); note_launch();
+  k_nb_rms<<<(unsigned)ns, 256, 0, s>>>(F(L.mad), C, F(L.rms)); note_launch();
+  const size_t nspec = units * nsamps;
+  k_nb_zap<<<(unsigned)((nspec + 127) / 128), 128, 0, s>>>(
+      reinterpret_cast<uint32_t*>(tf), nsamps, (int)units, C, nsmooth, (int)nsub, F(L.bp),
+      F(L.rms), rfi_tol, (unsigned)(C / 60));
+  note_launch();
   return cudaGetLastError();
 }
 

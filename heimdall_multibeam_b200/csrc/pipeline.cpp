@@ -59,6 +59,7 @@ struct hd_pipeline_t {
   std::vector<hd_range_t> zaps;
   dedisp_plan plan = nullptr;
   bool cleaning = true;
+  bool narrow_band = false;  // the reference's disabled narrow-band branch
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with compute
@@ -67,7 +68,7 @@ struct hd_pipeline_t {
   float timing[8] = {};
 
   DevBuf fb_tf, fb_ft, fb_tf_clean;
-  DevBuf dm0, dm0_scan, base, rms, mask, fmask, rms0;
+  DevBuf dm0, dm0_scan, base, rms, mask, fmask, rms0, nb_scratch;
   DevBuf dd, scan;
   DevBuf ws_a, ws_b;
   DevBuf winfo, norm;
@@ -173,6 +174,16 @@ hd_error clean_units(hd_pipeline pl, size_t units, const uint8_t* tf, size_t nsa
                         hdb::baseline_scratch(nsamps / nbeams, nsmooth, U * nbeams));
   HD_TRY(pl->ws_a.ensure(cap * sizeof(float)));
   HD_TRY(pl->ws_b.ensure(cap * sizeof(float)));
+  if (pl->narrow_band) {
+    // clean_filterbank_rfi.cu:303-351 with its `&& false` removed: zap
+    // narrow-band RFI first; the broadband branch then reads the result.
+    // tf is the pipeline's own device copy of the input.
+    if (nchans < 20 || (size_t)(baseline_length / (1 * dt)) == 0) return HD_INVALID_STRIDE;
+    HD_TRY(pl->nb_scratch.ensure(
+        hdb::narrow_band_scratch_bytes(U, nsamps, (int)nchans, dt, baseline_length)));
+    HD_TRY(hdb::narrow_band(const_cast<uint8_t*>(tf), U, nsamps, (int)nchans, dt,
+                            baseline_length, rfi_tol, pl->nb_scratch.p, s));
+  }
   float* x = pl->dm0.as<float>();
   HD_TRY(cudaMemsetAsync(x, 0, U * spitch * sizeof(float), s));
   for (size_t u = 0; u < U; u++)
@@ -279,6 +290,12 @@ hd_error hd_preallocate(hd_pipeline pl, hd_size nsamps, hd_size nbeams) {
   if (!pl) return HD_INVALID_PIPELINE;
   (void)nsamps;
   (void)nbeams;
+  return HD_NO_ERROR;
+}
+
+hd_error hd_set_narrow_band(hd_pipeline pl, int enable) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  pl->narrow_band = enable != 0;
   return HD_NO_ERROR;
 }
 

@@ -150,6 +150,15 @@ hd_error hd_clean_filterbank_rfi(hd_pipeline pipeline, const hd_byte* h_in, hd_s
  * selects it at compile time (Pipeline/pipeline.cu:72-74,255-299, #ifdef
  * CLEANING); its shipped build leaves it off. */
 hd_error hd_set_cleaning(hd_pipeline pipeline, int enable);
+/* Narrow-band RFI zapping before the broadband stage when cleaning is on: the
+ * branch of Pipeline/clean_filterbank_rfi.cu:303-351 that the reference
+ * disables (`nbits > 4 && false`), with measure_bandpass.cu:45-275.  Off by
+ * default, as in the reference.  Per stretch of baseline_length / dt spectra
+ * the bandpass and its deviation are measured from 3125 drawn spectra and
+ * bytes further than rfi_tol deviations from the bandpass are replaced by
+ * nearby channels; the reference's functor reads the bytes it is rewriting,
+ * and the result here is the one it gives in index order.  Needs nchans >= 20. */
+hd_error hd_set_narrow_band(hd_pipeline pipeline, int enable);
 
 /* hd_execute on a filterbank already in device memory (same layout; a
  * device-to-device copy replaces the host-to-device one). */

@@ -131,6 +131,11 @@ def lib():
         L.or_bf16.restype = C.c_float
         L.or_bf16.argtypes = [C.c_float]
         L.or_cnn_run.argtypes = [_fp, _fp, _fp, C.c_void_p, C.c_size_t, _fp, _fp, _fp]
+        L.or_measure_bandpass.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, _fp, _fp]
+        L.or_narrow_band.restype = C.c_int
+        L.or_narrow_band.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_float, C.c_float,
+                                     C.c_float]
+        L.or_set_narrow_band.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -151,6 +156,11 @@ def ref_lib(clean: bool = True):
         R.ref_execute.argtypes = [C.POINTER(OrParams), C.c_void_p, C.c_size_t, C.c_size_t,
                                   C.c_size_t, C.c_size_t, C.c_char_p, _szp,
                                   C.POINTER(C.c_double), C.c_int]
+        R.ref_measure_bandpass.restype = C.c_int
+        R.ref_measure_bandpass.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, _fp, _fp]
+        R.ref_narrow_band.restype = C.c_int
+        R.ref_narrow_band.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_float, C.c_float,
+                                      C.c_float]
         _ref[path] = R
     return _ref[path]
 
@@ -482,4 +492,38 @@ def ref_coincide(files, nbeams: int, sep_time: int, sep_filter: int) -> List[str
     out = os.path.join(d, names[0].split("_")[0] + "_all.cand")
     with open(out) as f:
         return f.read().splitlines()
+
+
+# ---------------------------------------------------------------------------
+# Narrow-band RFI (the branch Pipeline/clean_filterbank_rfi.cu:303 disables)
+# ---------------------------------------------------------------------------
+def measure_bandpass(fb: np.ndarray, ref: bool = False):
+    """(bandpass [nchans], rms) of an 8-bit (nsamps, nchans) filterbank:
+    the restatement, or (ref=True) the reference's own measure_bandpass."""
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    bp = np.zeros(nchans, np.float32)
+    rms = np.zeros(1, np.float32)
+    if ref:
+        ref_lib().ref_measure_bandpass(fb.ctypes.data, nsamps, nchans, _fptr(bp), _fptr(rms))
+    else:
+        lib().or_measure_bandpass(fb.ctypes.data, nsamps, nchans, _fptr(bp), _fptr(rms))
+    return bp, float(rms[0])
+
+
+def narrow_band(fb: np.ndarray, dt: float, baseline_length: float = 2.0, rfi_tol: float = 5.0,
+                ref: bool = False) -> np.ndarray:
+    """The narrow-band zapping of an 8-bit filterbank (a copy): the
+    restatement, or (ref=True) the reference's own code in index order."""
+    out = np.ascontiguousarray(fb, dtype=np.uint8).copy()
+    nsamps, nchans = out.shape
+    f = ref_lib().ref_narrow_band if ref else lib().or_narrow_band
+    if f(out.ctypes.data, nsamps, nchans, dt, baseline_length, rfi_tol) != 0:
+        raise ValueError("narrow-band zapping needs nchans a multiple of 4, >= 20")
+    return out
+
+
+def set_narrow_band(enable: bool) -> None:
+    """Whether the oracle's cleaning runs the narrow-band branch first."""
+    lib().or_set_narrow_band(1 if enable else 0)
 

@@ -545,6 +545,174 @@ static void or_zap(const int* mask, const uint8_t* in, size_t nsamps, size_t nbi
   }
 }
 
+/* ---- narrow-band RFI (the branch clean_filterbank_rfi.cu:303 disables) --- */
+
+/* Pipeline/median_filter.cu:99-124 (median_filter5_kernel): a 5-wide
+ * running median with the window shrunk to 3 or 4 at the ends. */
+static void or_median_filter5(const float* in, size_t count, float* out) {
+  for (size_t i = 0; i < count; i++) {
+    if (i > 1 && i < count - 2)
+      out[i] = or_median5(in[i - 2], in[i - 1], in[i], in[i + 1], in[i + 2]);
+    else if (i == 0)
+      out[i] = or_median3(in[i], in[i + 1], in[i + 2]);
+    else if (i == 1)
+      out[i] = or_median4(in[i - 1], in[i], in[i + 1], in[i + 2]);
+    else if (i == count - 1)
+      out[i] = or_median3(in[i], in[i - 1], in[i - 2]);
+    else
+      out[i] = or_median4(in[i + 1], in[i], in[i - 1], in[i - 2]);
+  }
+}
+
+/* Pipeline/median_filter.cu:422-432 (thrust::adjacent_difference with the
+ * mean of neighbours): out[0] = in[0], out[i] = 0.5 (in[i] + in[i-1]). */
+static void or_mean_filter2(const float* in, size_t count, float* out) {
+  if (count == 0) return;
+  out[0] = in[0];
+  for (size_t i = 1; i < count; i++) out[i] = 0.5f * (in[i] + in[i - 1]);
+}
+
+/* Pipeline/median_filter.cu:345-361: median5 of corresponding elements of
+ * five consecutive arrays of `size` values. */
+static void or_median_scrunch5_array(const float* in, size_t size, size_t count, float* out) {
+  size_t oc = count / 5;
+  for (size_t a = 0; a < oc; a++)
+    for (size_t j = 0; j < size; j++)
+      out[a * size + j] = or_median5(in[(5 * a) * size + j], in[(5 * a + 1) * size + j],
+                                     in[(5 * a + 2) * size + j], in[(5 * a + 3) * size + j],
+                                     in[(5 * a + 4) * size + j]);
+}
+
+/* measure_bandpass.cu:141-163 / 223-245: scrunch by 5, 5-wide median, mean of
+ * neighbours, stretch back to nchans/5*5 and extrapolate the rest linearly
+ * (v in place; tmp holds nchans/5 values). */
+static void or_smooth_band(float* v, size_t nchans, float* tmp) {
+  size_t n5 = nchans / 5;
+  or_median_scrunch5(v, nchans, tmp);
+  or_median_filter5(tmp, n5, v);
+  or_mean_filter2(v, n5, tmp);
+  /* for some channel counts (1140, 2220, ...) float rounding puts the last
+   * stretched sample just past the last input with a fraction above 1e-5,
+   * so the stretch reads one element past the nchans/5 values (the
+   * reference reads past its vector there); that element is defined as 0 */
+  tmp[n5] = 0.f;
+  or_linear_stretch(tmp, n5, v, n5 * 5);
+  for (size_t i = n5 * 5; i < nchans; i++) v[i] = 2 * v[i - 1] - v[i - 2];
+}
+
+static int or_cmp_float(const void* a, const void* b) {
+  float x = *(const float*)a, y = *(const float*)b;
+  return (x > y) - (x < y);
+}
+
+/* Pipeline/measure_bandpass.cu:45-275: 3125 spectra drawn with
+ * thrust::default_random_engine(123456) and uniform_int(0, nsamps-1), their
+ * recursive median per channel (5 levels of median-of-5), smoothed: the
+ * bandpass; the recursive median of |spectrum - bandpass| times 1.4826,
+ * smoothed: the band's deviation, whose median over channels is *rms. */
+void or_measure_bandpass(const uint8_t* fb, size_t nsamps, size_t nchans, float* bp,
+                         float* rms) {
+  const size_t N = 3125;
+  float* s1 = (float*)malloc(N * nchans * sizeof(float));
+  float* s2 = (float*)malloc(N / 5 * nchans * sizeof(float));
+  float* s3 = (float*)malloc(N / 25 * nchans * sizeof(float));
+  float* s4 = (float*)malloc(N / 125 * nchans * sizeof(float));
+  float* s5 = (float*)malloc(N / 625 * nchans * sizeof(float));
+  float* tmp = (float*)malloc((nchans / 5 + 1) * sizeof(float));
+  float* mad = (float*)malloc(nchans * sizeof(float));
+  uint32_t st = or_minstd_seed(123456u);
+  for (size_t i = 0; i < N; i++) {
+    uint32_t t = or_uniform_uint(&st, 0u, (uint32_t)(nsamps - 1));
+    for (size_t c = 0; c < nchans; c++) s1[i * nchans + c] = (float)fb[(size_t)t * nchans + c];
+  }
+  or_median_scrunch5_array(s1, nchans, N, s2);
+  or_median_scrunch5_array(s2, nchans, N / 5, s3);
+  or_median_scrunch5_array(s3, nchans, N / 25, s4);
+  or_median_scrunch5_array(s4, nchans, N / 125, s5);
+  or_median_scrunch5_array(s5, nchans, N / 625, bp);
+  or_smooth_band(bp, nchans, tmp);
+  for (size_t i = 0; i < N; i++)
+    for (size_t c = 0; c < nchans; c++)
+      s1[i * nchans + c] = fabsf(s1[i * nchans + c] - bp[c]);
+  or_median_scrunch5_array(s1, nchans, N, s2);
+  or_median_scrunch5_array(s2, nchans, N / 5, s3);
+  or_median_scrunch5_array(s3, nchans, N / 25, s4);
+  or_median_scrunch5_array(s4, nchans, N / 125, s5);
+  or_median_scrunch5_array(s5, nchans, N / 625, mad);
+  for (size_t c = 0; c < nchans; c++) mad[c] = mad[c] * 1.4826f;
+  or_smooth_band(mad, nchans, tmp);
+  memcpy(s2, mad, nchans * sizeof(float));
+  qsort(s2, nchans, sizeof(float), or_cmp_float);
+  *rms = s2[nchans / 2];
+  free(s1); free(s2); free(s3); free(s4); free(s5); free(tmp); free(mad);
+}
+
+/* zap_narrow_rfi_functor (clean_filterbank_rfi.cu:114-193) over words
+ * [w0, w1) in index order, in place: a byte whose |value - bandpass| is
+ * above thresh is replaced by the byte of a channel drawn within
+ * max_dist (up to 10 redraws while the drawn one is bad too).  As in the
+ * reference, the bandpass entry and the draw range use channel w + k (w the
+ * word's index in its spectrum, k the byte), and draws read the spectrum as
+ * already zapped by earlier words. */
+static void or_zap_narrow(uint8_t* data, size_t w0, size_t w1, const float* bp, float thresh,
+                          unsigned stride, unsigned nchans, unsigned max_dist) {
+  uint32_t* d = (uint32_t*)data;
+  for (size_t i = w0; i < w1; i++) {
+    unsigned t = (unsigned)(i / stride), w = (unsigned)(i % stride);
+    uint32_t word = d[i];
+    uint32_t st = or_minstd_seed(or_hash((uint32_t)i));
+    int any = 0;
+    for (unsigned k = 0; k < 4; k++) {
+      unsigned c = w + k;
+      uint32_t val = (word >> (k * 8)) & 0xFFu;
+      if (fabsf((float)val - bp[c]) > thresh) {
+        any = 1;
+        unsigned min_c = c > max_dist ? c - max_dist : 0;
+        unsigned max_c = c < nchans - 1 - max_dist ? c + max_dist : nchans - 1;
+        unsigned nc = or_uniform_uint(&st, min_c, max_c);
+        int attempts = 0;
+        uint32_t nv = (d[(size_t)t * stride + nc / 4] >> ((nc % 4) * 8)) & 0xFFu;
+        while (fabsf((float)nv - bp[nc]) > thresh && ++attempts < 11) {
+          nc = or_uniform_uint(&st, min_c, max_c);
+          nv = (d[(size_t)t * stride + nc / 4] >> ((nc % 4) * 8)) & 0xFFu;
+        }
+        word &= ~(0xFFu << (k * 8));
+        word |= nv << (k * 8);
+      }
+    }
+    if (any) d[i] = word;
+  }
+}
+
+/* The narrow-band branch (clean_filterbank_rfi.cu:303-351) on 8-bit data, in
+ * place: per stretch of baseline_length / dt spectra, measure the bandpass
+ * and zap with thresh = rfi_tol * rms and a draw radius of nchans / 60.
+ * Returns -1 if the stretch is empty or nchans is not a multiple of 4 of at
+ * least 20 (the reference's filters read outside the band then). */
+int or_narrow_band(uint8_t* data, size_t nsamps, size_t nchans, float dt, float baseline_length,
+                   float rfi_tol) {
+  size_t nsmooth = (size_t)(baseline_length / (1 * dt));
+  if (nsmooth == 0 || nchans % 4 != 0 || nchans < 20) return -1;
+  unsigned stride = (unsigned)(nchans / 4);
+  unsigned maxd = (unsigned)(nchans / 60);
+  float* bp = (float*)malloc(nchans * sizeof(float));
+  for (size_t g = 0; g < nsamps; g += nsmooth) {
+    size_t ng = nsmooth < nsamps - g ? nsmooth : nsamps - g;
+    float rms = 0.f;
+    or_measure_bandpass(data + g * nchans, ng, nchans, bp, &rms);
+    or_zap_narrow(data, g * stride, (g + ng) * stride, bp, rfi_tol * rms, stride,
+                  (unsigned)nchans, maxd);
+  }
+  free(bp);
+  return 0;
+}
+
+/* Test hook: when set, or_clean_filterbank_rfi runs the narrow-band branch
+ * first and the broadband branch on its output (the reference with the
+ * branch enabled: both read h_in_copy). */
+static int g_narrow_band = 0;
+void or_set_narrow_band(int enable) { g_narrow_band = enable; }
+
 /* clean_filterbank_rfi (clean_filterbank_rfi.cu:256-528), broadband branch
  * only (the narrow-band branch is disabled at :303).  Returns 0, or -1 if the
  * resample radius is not below nsamps (the reference then reads outside the
@@ -558,6 +726,16 @@ int or_clean_filterbank_rfi(const uint8_t* in, size_t nsamps, size_t nbits,
   size_t beam_nsamps = beam_stride;
   size_t nsamps_smooth = (size_t)(baseline_length / (2 * dt));
   if (nsamps_smooth / 4 >= nsamps) return -1;
+  uint8_t* nb = NULL;
+  if (g_narrow_band) {
+    nb = (uint8_t*)malloc(nsamps * nchans + 16);
+    memcpy(nb, in, nsamps * nchans);
+    if (or_narrow_band(nb, nsamps, nchans, dt, baseline_length, rfi_tol) != 0) {
+      free(nb);
+      return -1;
+    }
+    in = nb;
+  }
   float* s = (float*)calloc(count + 8, sizeof(float));
   for (size_t t = 0; t < count; t++) {
     int32_t acc = 0;
@@ -591,6 +769,7 @@ int or_clean_filterbank_rfi(const uint8_t* in, size_t nsamps, size_t nbits,
   or_zap(mask, in, count, nbits, nchans, nsamps_smooth / 4, out);
   if (mask_out) memcpy(mask_out, mask, count * sizeof(int));
   free(s); free(rms); free(mask); free(fm); free(sm); free(S); free(F);
+  free(nb);
   return 0;
 }
 

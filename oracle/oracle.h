@@ -91,6 +91,11 @@ void   or_merge(size_t count, const size_t* labels, const or_giants* g,
 /* ---- RFI cleaning (Pipeline/clean_filterbank_rfi.cu) --------------------- */
 uint32_t or_hash(uint32_t a);
 uint32_t or_uniform_uint(uint32_t* state, uint32_t lo, uint32_t hi);
+void     or_measure_bandpass(const uint8_t* fb, size_t nsamps, size_t nchans, float* bandpass,
+                             float* rms);
+int      or_narrow_band(uint8_t* data, size_t nsamps, size_t nchans, float dt,
+                        float baseline_length, float rfi_tol);
+void     or_set_narrow_band(int enable);
 int      or_clean_filterbank_rfi(const uint8_t* in, size_t nsamps, size_t nbits,
                                  size_t nchans, float dt, float baseline_length,
                                  float rfi_tol, size_t boxcar_max, size_t nbeams,
