@@ -130,6 +130,13 @@ class HdSigprocHeader(C.Structure):
 GULP_CALLBACK = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t)
 
 
+class RawCandidates(C.Structure):
+    """struct RawCandidates (Pipeline/hd/types.h:18-26)."""
+    _fields_ = [("peaks", C.POINTER(C.c_float))] + \
+        [(k, C.POINTER(C.c_size_t)) for k in ("inds", "begins", "ends", "filter_inds",
+                                              "dm_inds", "members")]
+
+
 class HdCoincidence(C.Structure):
     """hd_coincidence (include/heimdall_b200.h)."""
     _fields_ = [("nbeams", C.c_uint), ("primary_beam", C.c_uint), ("max_snr", C.c_float)]
@@ -158,6 +165,7 @@ SYMBOLS = {
     "hd_execute_beams": (C.c_int, [_P, C.POINTER(_P), _SZ, _SZ, _SZ, _SZ, _SZ, _SZP, C.c_int,
                                    C.POINTER(C.c_int), _SZP]),
     "hd_get_beam_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
+    "hd_get_raw_candidates": (C.c_int, [_P, C.c_void_p, _SZP]),
     "hd_create_beam_set": (C.c_int, [C.POINTER(_P), C.c_void_p, _SZ, C.c_int]),
     "hd_set_beam_set_cleaning": (C.c_int, [_P, C.c_int]),
     "hd_get_beam_set_config_count": (_SZ, [_P]),

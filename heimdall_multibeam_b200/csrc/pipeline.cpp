@@ -792,6 +792,25 @@ hd_error hd_get_beam_candidates(hd_pipeline pl, hd_size index, hd_candidate* out
   return HD_NO_ERROR;
 }
 
+hd_error hd_get_raw_candidates(hd_pipeline pl, struct RawCandidates* out, hd_size* count) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!out || !count) return HD_INVALID_POINTER;
+  const std::vector<hd_candidate>& v = pl->cands;
+  const size_t n = std::min(*count, v.size());
+  for (size_t i = 0; i < n; i++) {
+    const hd_candidate& c = v[i];
+    if (out->peaks) out->peaks[i] = c.snr;
+    if (out->inds) out->inds[i] = c.samp_idx;
+    if (out->begins) out->begins[i] = c.begin;
+    if (out->ends) out->ends[i] = c.end;
+    if (out->filter_inds) out->filter_inds[i] = c.filter;
+    if (out->dm_inds) out->dm_inds[i] = c.dm_trial;
+    if (out->members) out->members[i] = c.members;
+  }
+  *count = v.size();
+  return HD_NO_ERROR;
+}
+
 namespace {
 // Patches of the first k candidates of the last gulp into pl->patch_dm /
 // pl->patch_ft (device), on the pipeline's stream.

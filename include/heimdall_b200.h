@@ -7,7 +7,8 @@
  * error codes and ownership rules:
  *
  *   Pipeline/hd/types.h:12-48           hd_byte/hd_size/hd_float, hd_pipeline,
- *                                       hd_range_t
+ *                                       RawCandidates, ConstRawCandidates,
+ *                                       Candidates (C++), hd_range_t
  *   Pipeline/hd/params.h:19-78          struct hd_params (same fields, order)
  *   Pipeline/hd/error.h:19-41           hd_error codes, hd_get_error_string
  *   Pipeline/hd/pipeline.h:10-28        hd_create_pipeline, hd_preallocate,
@@ -18,9 +19,15 @@
  *   Pipeline/hd/clean_filterbank_rfi.h  hd_clean_filterbank_rfi
  *
  * Additions (no reference counterpart; the reference only writes candidates to
- * a .cand file or a socket): hd_set_cleaning, hd_execute_device,
- * hd_execute_beams, hd_get_candidates, hd_get_beam_candidates, hd_get_giants,
- * hd_get_timing, hd_get_launch_count.
+ * a .cand file or a socket): hd_set_cleaning, hd_set_narrow_band,
+ * hd_execute_device, hd_execute_beams, hd_get_candidates,
+ * hd_get_beam_candidates, hd_get_raw_candidates, hd_get_giants, hd_get_timing,
+ * hd_get_dedisp_tile, hd_get_launch_count, hd_clean_filterbank_rfi_noalloc;
+ * beam sets (hd_*_beam_set*); sigproc input and the gulp loop
+ * (hd_read_sigproc_header, hd_mjd_to_utc, hd_params_from_sigproc,
+ * hd_search_sigproc_file); the coincidencer (hd_coincide,
+ * hd_write_coincident_candidates); the candidate classifier
+ * (hd_extract_patches, hd_score_candidates, hd_classifier_*).
  *
  * Ownership and threading: the caller owns every host buffer it passes; the
  * pipeline owns all device memory, its CUDA stream and events.  A pipeline
@@ -48,6 +55,27 @@ typedef unsigned char          hd_byte;
 typedef size_t                 hd_size;
 typedef float                  hd_float;
 typedef struct hd_pipeline_t*  hd_pipeline;
+
+/* Candidate arrays (Pipeline/hd/types.h:18-42): one entry per candidate in
+ * each array. */
+struct RawCandidates {
+  hd_float* peaks;
+  hd_size*  inds;
+  hd_size*  begins;
+  hd_size*  ends;
+  hd_size*  filter_inds;
+  hd_size*  dm_inds;
+  hd_size*  members;
+};
+struct ConstRawCandidates {
+  const hd_float* peaks;
+  const hd_size*  inds;
+  const hd_size*  begins;
+  const hd_size*  ends;
+  const hd_size*  filter_inds;
+  const hd_size*  dm_inds;
+  const hd_size*  members;
+};
 
 typedef struct hd_range {
   hd_size start;
@@ -386,6 +414,12 @@ hd_error hd_get_candidates(hd_pipeline pipeline, hd_candidate* out, hd_size* cou
  * hd_execute), same copy rules as hd_get_candidates. */
 hd_error hd_get_beam_candidates(hd_pipeline pipeline, hd_size index, hd_candidate* out,
                                 hd_size* count);
+/* The candidates of the last gulp (hd_get_candidates order) as RawCandidates
+ * arrays the caller provides, each of *count entries: peaks = S/N, inds =
+ * sample index, begins/ends, filter_inds, dm_inds = DM trial, members.  Any
+ * array pointer may be NULL; copies min(*count, available) and sets *count
+ * to the number available. */
+hd_error hd_get_raw_candidates(hd_pipeline pipeline, struct RawCandidates* out, hd_size* count);
 
 /* Beams of different shapes in one call.  No counterpart in the reference,
  * which runs one heimdall process (one pipeline) per beam
@@ -434,7 +468,15 @@ hd_error hd_get_giants(hd_pipeline pipeline, hd_float* peaks, hd_size* inds, hd_
 hd_error hd_get_timing(hd_pipeline pipeline, float* ms, int n);
 
 #ifdef __cplusplus
-}
+}  /* extern "C" */
+
+/* Full candidate info including derived quantities (Pipeline/hd/types.h:38-43). */
+struct Candidates : public RawCandidates {
+  hd_float* dms;
+  hd_size*  flags;
+  hd_size*  beam_counts;
+  hd_size*  beam_masks;
+};
 #endif
 
 #endif /* HEIMDALL_B200_H */

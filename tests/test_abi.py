@@ -60,7 +60,8 @@ int main(void) {{
 @pytest.mark.parametrize("cls,cname", [(hdb.HdParams, "struct hd_params"),
                                        (hdb.HdCandidate, "hd_candidate"),
                                        (hdb.HdSigprocHeader, "hd_sigproc_header"),
-                                       (hdb.HdCoincidence, "hd_coincidence")])
+                                       (hdb.HdCoincidence, "hd_coincidence"),
+                                       (hdb.RawCandidates, "struct RawCandidates")])
 def test_struct_layout_matches_c(cls, cname):
     fields = [f for f, _ in cls._fields_]
     size, lay = _c_layout(cname, fields)
@@ -101,3 +102,28 @@ def test_dm_list_guru_matches_golden(hdb):
     golden = open(os.path.join(ROOT, "tests", "golden", "dm2000.list")).read().split()
     dms = hdb.dm_list_guru(0.0, 2000.0, 64e-6, 40.0, 1581.804688, -0.390625, 1024, 1.25)
     assert ["%g" % float(x) for x in dms[1:]] == golden
+
+
+def test_header_compiles_as_cxx_with_reference_types():
+    """The reference's C++ Candidates type (Pipeline/hd/types.h:38-43) derives
+    from RawCandidates as there."""
+    prog = """#include "heimdall_b200.h"
+int main() {
+  Candidates c;
+  RawCandidates* r = &c;
+  r->peaks = 0;
+  c.dms = 0;
+  ConstRawCandidates k;
+  k.inds = 0;
+  hd_range_t z = {1, 2};
+  return (int)(z.end - z.start) - 1;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.cpp")
+        open(src, "w").write(prog)
+        exe = os.path.join(d, "t")
+        subprocess.run(["/usr/bin/g++", "-I", os.path.join(ROOT, "include"), src, "-o", exe],
+                       check=True)
+        assert subprocess.run([exe]).returncode == 0
+

@@ -240,3 +240,31 @@ def test_execute_c1_full(hdb, oracle_lib):
     b = synth.make_c1()
     cands = _compare(b.data, 1, synth.SEARCH_C1, True)
     assert len(cands) >= 20
+
+
+def test_raw_candidates_match_rows(hdb):
+    """hd_get_raw_candidates gives the rows of hd_get_candidates as the
+    reference's RawCandidates arrays."""
+    import ctypes as C
+    w = synth.SEARCH_C0
+    b = synth.make_c0()
+    with H.Pipeline(H.default_params(output_dir=None, **_params(w)), cleaning=False) as pl:
+        pl.execute(b.data)
+        rows = pl.candidates()
+        n = len(rows)
+        assert n >= 3
+        arrs = {"peaks": np.zeros(n, np.float32)}
+        for k in ("inds", "begins", "ends", "filter_inds", "dm_inds", "members"):
+            arrs[k] = np.zeros(n, np.uint64)
+        raw = H.RawCandidates(arrs["peaks"].ctypes.data_as(C.POINTER(C.c_float)),
+                              *(arrs[k].ctypes.data_as(C.POINTER(C.c_size_t))
+                                for k in ("inds", "begins", "ends", "filter_inds", "dm_inds",
+                                          "members")))
+        cnt = C.c_size_t(n)
+        assert H.lib().hd_get_raw_candidates(pl._p, C.byref(raw), C.byref(cnt)) == 0
+        assert cnt.value == n
+    np.testing.assert_array_equal(arrs["peaks"], rows["snr"])
+    for k, f in (("inds", "samp_idx"), ("begins", "begin"), ("ends", "end"),
+                 ("filter_inds", "filter"), ("dm_inds", "dm_trial"), ("members", "members")):
+        np.testing.assert_array_equal(arrs[k], rows[f])
+
