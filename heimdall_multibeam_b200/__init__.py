@@ -166,6 +166,8 @@ SYMBOLS = {
                                    C.POINTER(C.c_int), _SZP]),
     "hd_get_beam_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
     "hd_get_raw_candidates": (C.c_int, [_P, C.c_void_p, _SZP]),
+    "hd_prefetch_beams": (C.c_int, [_P, C.POINTER(_P), _SZ, _SZ, _SZ]),
+    "hd_execute_prefetched": (C.c_int, [_P, _SZ, _SZ, _SZP, C.POINTER(C.c_int), _SZP]),
     "hd_create_beam_set": (C.c_int, [C.POINTER(_P), C.c_void_p, _SZ, C.c_int]),
     "hd_set_beam_set_cleaning": (C.c_int, [_P, C.c_int]),
     "hd_get_beam_set_config_count": (_SZ, [_P]),
@@ -512,6 +514,20 @@ class Pipeline:
             if err != HD_NO_ERROR:
                 raise HdError(err, "hd_score_candidates")
         return out
+
+    def prefetch_beams(self, host_ptrs: Sequence[int], nsamps: int) -> int:
+        """hd_prefetch_beams on raw host pointers (pinned for overlap)."""
+        ptrs = (_P * len(host_ptrs))(*host_ptrs)
+        return lib().hd_prefetch_beams(self._p, ptrs, len(host_ptrs), nsamps, 8)
+
+    def execute_prefetched(self, nunits: int, first_idx: int = 0, nbeams: int = 1,
+                           beams: Optional[Sequence[int]] = None) -> Tuple[int, int, List[int]]:
+        """hd_execute_prefetched: (hd_error, nsamps_processed, statuses)."""
+        st = (C.c_int * max(nunits, 1))()
+        bm = (C.c_size_t * nunits)(*beams) if beams is not None else None
+        proc = C.c_size_t(0)
+        err = lib().hd_execute_prefetched(self._p, first_idx, nbeams, bm, st, C.byref(proc))
+        return err, proc.value, list(st)[:nunits]
 
     def search_sigproc_file(self, path: str, nsamps_gulp: int):
         """hd_search_sigproc_file: (hd_error, total spectra searched per beam,

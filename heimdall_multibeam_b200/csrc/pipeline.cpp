@@ -65,6 +65,19 @@ struct hd_pipeline_t {
   cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with compute
   cudaEvent_t ev[10] = {};
   cudaEvent_t chunk_ev[kMaxChunks] = {};
+  // double-buffered ingest (hd_prefetch_beams / hd_execute_prefetched): two
+  // slots of filterbanks copied on copy_stream ahead of their search
+  struct Prefetch {
+    DevBuf buf;
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+    unsigned long long tag = 0;
+    size_t units = 0, nsamps = 0;
+  } pf[2];
+  unsigned long long pf_seq = 0;
+  // set by hd_execute_prefetched: the gulp already sits in fb_tf (the slot's
+  // buffer was swapped in), so execute_units copies nothing
+  bool fb_resident = false;
   float timing[8] = {};
 
   DevBuf fb_tf, fb_ft, fb_tf_clean;
@@ -99,6 +112,7 @@ struct hd_pipeline_t {
     if (plan) dedisp_destroy_plan(plan);
     for (auto& e : ev) if (e) cudaEventDestroy(e);
     for (auto& e : chunk_ev) if (e) cudaEventDestroy(e);
+    for (auto& q : pf) if (q.done) cudaEventDestroy(q.done);
     if (stream) cudaStreamDestroy(stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (h_small) cudaFreeHost(h_small);
@@ -260,6 +274,7 @@ hd_error hd_create_pipeline(hd_pipeline* pipeline_, hd_params params) {
   }
   for (auto& e : pl->ev) cudaEventCreate(&e);
   for (auto& e : pl->chunk_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  for (auto& q : pl->pf) cudaEventCreateWithFlags(&q.done, cudaEventDisableTiming);
   if (cudaMallocHost(&pl->h_small, 64 * sizeof(unsigned)) != cudaSuccess) {
     delete pl;
     return HD_MEM_ALLOC_FAILED;
@@ -315,6 +330,8 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
                               const hd_size* beams, hd_error* statuses,
                               hd_size* nsamps_processed) {
   if (!pl) return HD_INVALID_PIPELINE;
+  const bool resident = pl->fb_resident;
+  pl->fb_resident = false;
   if (!fbs || !nsamps_processed || U == 0) return HD_INVALID_POINTER;
   for (size_t u = 0; u < U; u++)
     if (!fbs[u]) return HD_INVALID_POINTER;
@@ -402,8 +419,10 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
       if (de != DEDISP_NO_ERROR) return dedisp_err(de);
     }
   } else {
-    for (size_t u = 0; u < U; u++)
-      HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes, kind, s));
+    if (!resident)
+      for (size_t u = 0; u < U; u++)
+        HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes, kind,
+                               s));
     cudaEventRecord(pl->ev[1], s);
     if (pl->cleaning) {
       hd_error he = clean_units(pl, U, pl->fb_tf.as<uint8_t>(), nsamps, C, P.dt,
@@ -736,6 +755,64 @@ hd_error hd_execute_beams(hd_pipeline pl, const hd_byte* const* filterbanks,
                           int on_device, hd_error* statuses, hd_size* nsamps_processed) {
   return execute_units(pl, filterbanks, nfilterbanks, on_device != 0, nsamps, nbits, first_idx,
                        nbeams, beams, statuses, nsamps_processed);
+}
+
+hd_error hd_prefetch_beams(hd_pipeline pl, const hd_byte* const* filterbanks,
+                           hd_size nfilterbanks, hd_size nsamps, hd_size nbits) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!filterbanks || nfilterbanks == 0) return HD_INVALID_POINTER;
+  for (size_t u = 0; u < nfilterbanks; u++)
+    if (!filterbanks[u]) return HD_INVALID_POINTER;
+  if (nbits != 8) return HD_INVALID_NBITS;
+  int slot = -1;
+  for (int i = 0; i < 2; i++)
+    if (!pl->pf[i].pending) {
+      slot = i;
+      break;
+    }
+  if (slot < 0) return HD_INVALID_STRIDE;  // two gulps already queued
+  if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  hd_pipeline_t::Prefetch& q = pl->pf[slot];
+  const size_t fb_bytes = nsamps * pl->params.nchans;
+  HD_TRY(q.buf.ensure(nfilterbanks * fb_bytes + 64));
+  // the slot may still be read by a search queued earlier on the compute stream
+  HD_TRY(cudaEventRecord(q.done, pl->stream));
+  HD_TRY(cudaStreamWaitEvent(pl->copy_stream, q.done, 0));
+  for (size_t u = 0; u < nfilterbanks; u++)
+    HD_TRY(cudaMemcpyAsync(q.buf.as<uint8_t>() + u * fb_bytes, filterbanks[u], fb_bytes,
+                           cudaMemcpyHostToDevice, pl->copy_stream));
+  HD_TRY(cudaEventRecord(q.done, pl->copy_stream));
+  q.pending = true;
+  q.tag = ++pl->pf_seq;
+  q.units = nfilterbanks;
+  q.nsamps = nsamps;
+  return HD_NO_ERROR;
+}
+
+hd_error hd_execute_prefetched(hd_pipeline pl, hd_size first_idx, hd_size nbeams,
+                               const hd_size* beams, hd_error* statuses,
+                               hd_size* nsamps_processed) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  int slot = -1;
+  for (int i = 0; i < 2; i++)
+    if (pl->pf[i].pending && (slot < 0 || pl->pf[i].tag < pl->pf[slot].tag)) slot = i;
+  if (slot < 0) return HD_INVALID_POINTER;  // nothing queued
+  if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  hd_pipeline_t::Prefetch& q = pl->pf[slot];
+  HD_TRY(cudaStreamWaitEvent(pl->stream, q.done, 0));
+  // the slot's buffer becomes the pipeline's time-major input (no copy); the
+  // previous input buffer becomes the slot's, to be filled by a later
+  // hd_prefetch_beams once the work queued on the compute stream is done
+  std::swap(pl->fb_tf.p, q.buf.p);
+  std::swap(pl->fb_tf.cap, q.buf.cap);
+  const size_t fb_bytes = q.nsamps * pl->params.nchans;
+  std::vector<const hd_byte*> fbs(q.units);
+  for (size_t u = 0; u < q.units; u++) fbs[u] = pl->fb_tf.as<uint8_t>() + u * fb_bytes;
+  pl->fb_resident = true;
+  const hd_error e = execute_units(pl, fbs.data(), q.units, true, q.nsamps, 8, first_idx,
+                                   nbeams, beams, statuses, nsamps_processed);
+  q.pending = false;
+  return e;
 }
 
 unsigned long long hd_get_launch_count(void) { return hdb::launch_count(); }

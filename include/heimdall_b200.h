@@ -410,6 +410,23 @@ hd_error hd_search_sigproc_file(hd_pipeline pipeline, const char* path, hd_size 
  * *count to the number available. */
 hd_error hd_get_candidates(hd_pipeline pipeline, hd_candidate* out, hd_size* count);
 
+/* Double-buffered ingest for streaming callers (no reference counterpart:
+ * heimdall.C copies and searches each gulp in turn).  hd_prefetch_beams
+ * queues the copy of the next gulp's filterbanks (host memory, pinned for the
+ * copy to overlap) on the pipeline's copy stream and returns at once; up to
+ * two gulps may be queued.  hd_execute_prefetched searches the oldest queued
+ * gulp exactly as hd_execute_beams would (same arguments after the data).
+ * Calling hd_prefetch_beams for gulp k+1 before hd_execute_prefetched for
+ * gulp k overlaps the copy of one gulp with the search of the other.  The
+ * host buffers must stay unchanged until the gulp's search returns.  A third
+ * hd_prefetch_beams while two gulps are queued returns HD_INVALID_STRIDE;
+ * hd_execute_prefetched with nothing queued returns HD_INVALID_POINTER. */
+hd_error hd_prefetch_beams(hd_pipeline pipeline, const hd_byte* const* filterbanks,
+                           hd_size nfilterbanks, hd_size nsamps, hd_size nbits);
+hd_error hd_execute_prefetched(hd_pipeline pipeline, hd_size first_idx, hd_size nbeams,
+                               const hd_size* beams, hd_error* statuses,
+                               hd_size* nsamps_processed);
+
 /* Candidates of filterbank `index` of the last hd_execute_beams (index 0 after
  * hd_execute), same copy rules as hd_get_candidates. */
 hd_error hd_get_beam_candidates(hd_pipeline pipeline, hd_size index, hd_candidate* out,

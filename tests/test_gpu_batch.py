@@ -171,3 +171,35 @@ def test_batch_errors(hdb):
         assert err == H.HD_NO_ERROR and st == [0, 0] and len(pl.candidates()) == 0
         n = H.C.c_size_t(0)
         assert H.lib().hd_get_beam_candidates(pl._p, 5, None, H.C.byref(n)) != H.HD_NO_ERROR
+
+
+def test_prefetched_equals_execute_beams(hdb):
+    """hd_prefetch_beams / hd_execute_prefetched: gulps queued ahead (two
+    slots) are searched in queue order with exactly the results that
+    hd_execute_beams gives for the same filterbanks."""
+    gulps = [[np.ascontiguousarray(x) for x in _beams(seed=s)[:3]] for s in (31, 57, 31)]
+    kw = _kw(W)
+    beams = [4, 9, 10]
+
+    def snapshot(pl, err, proc, st):
+        g = pl.giants()
+        return (err, proc, st, [H.cand_lines(pl.candidates(u)) for u in range(3)],
+                g["inds"].tolist(), g["peaks"].view(np.uint32).tolist(), g["labels"].tolist())
+
+    with H.Pipeline(H.default_params(**kw), cleaning=True) as ref:
+        want = [snapshot(ref, *ref.execute_beams(g, first_idx=700 * k, beams=beams))
+                for k, g in enumerate(gulps)]
+    assert sum(len(c) for c in want[0][3]) >= 3
+    ptrs = [[x.ctypes.data for x in g] for g in gulps]
+    with H.Pipeline(H.default_params(**kw), cleaning=True) as pl:
+        assert pl.execute_prefetched(3)[0] == H.HD_INVALID_POINTER  # nothing queued
+        assert pl.prefetch_beams(ptrs[0], W.nsamps) == H.HD_NO_ERROR
+        assert pl.prefetch_beams(ptrs[1], W.nsamps) == H.HD_NO_ERROR
+        assert pl.prefetch_beams(ptrs[2], W.nsamps) == H.HD_INVALID_STRIDE  # both slots busy
+        got = [snapshot(pl, *pl.execute_prefetched(3, first_idx=0, beams=beams))]
+        assert pl.prefetch_beams(ptrs[2], W.nsamps) == H.HD_NO_ERROR
+        for k in (1, 2):
+            got.append(snapshot(pl, *pl.execute_prefetched(3, first_idx=700 * k, beams=beams)))
+        assert pl.execute_prefetched(3)[0] == H.HD_INVALID_POINTER
+    for k in range(3):
+        assert got[k] == want[k], k
