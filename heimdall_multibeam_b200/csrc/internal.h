@@ -15,6 +15,17 @@ namespace hdb {
 void note_launch();
 unsigned long long launch_count();
 
+// Raises the dynamic shared-memory limit of kernel `func` on the current
+// device to at least `bytes`.  The limit is a process-wide attribute of the
+// function and is never lowered here: host threads that launch the same
+// kernel with different shared-memory sizes (the workers of a beam set) can
+// then not pull it below what another thread's launch needs.
+cudaError_t raise_smem_limit(const void* func, size_t bytes);
+template <class F>
+cudaError_t raise_smem_limit(F* func, size_t bytes) {
+  return raise_smem_limit(reinterpret_cast<const void*>(func), bytes);
+}
+
 // ---- filterbank kernels (kernels_fb.cu) ------------------------------------
 struct DedispArgs {
   const uint8_t* in;      // FT rows, channel c at in + c*in_pitch

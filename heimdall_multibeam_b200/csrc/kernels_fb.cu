@@ -8,6 +8,8 @@
 //       pitch a multiple of 64 bytes with zero padding past nsamps so the
 //       dedispersion tiles can be fetched with 16-byte-aligned bulk copies.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -18,6 +20,20 @@ namespace hdb {
 static unsigned long long g_launches = 0;
 void note_launch() { __atomic_add_fetch(&g_launches, 1ull, __ATOMIC_RELAXED); }
 unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+cudaError_t raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<int, const void*>, size_t> limit;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(m);
+  size_t& cur = limit[{dev, func}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 
 // ---------------------------------------------------------------------------
 // TF -> FT byte transpose, 128 x 128 tiles through shared memory.
@@ -664,8 +680,7 @@ template <int NW, int G, int CH>
 cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
   auto kern = k_dedisp<NW, G, CH, DD_NST>;
   const size_t smem = dd_smem(2 * NW, CH, a.rowb);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = raise_smem_limit(kern, smem);
   if (e != cudaSuccess) return e;
   const int DB = 2 * NW, TB = 128 * G;
   dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),

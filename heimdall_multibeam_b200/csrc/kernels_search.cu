@@ -593,8 +593,7 @@ static cudaError_t launch_scan(const SeriesBatch& sb, const float* rms, float* s
                                int ser) {
   const int np = ser < 7 ? ser : 7;
   const size_t smem = scan_smem_bytes(ser, sb.nbeams, CH);
-  cudaError_t e = cudaFuncSetAttribute(k_normalise_scan<CH>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = raise_smem_limit(k_normalise_scan<CH>, smem);
   if (e != cudaSuccess) return e;
   k_normalise_scan<CH><<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
       sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
@@ -940,8 +939,7 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
         (2 * ((win + 3) & ~(size_t)3) + nwb * ((n1 + 3) & ~(size_t)3) + nwb * (n1 / 5 + 1)) *
         sizeof(float);
     if (smem <= 200 * 1024) {
-      cudaFuncSetAttribute(k_block_rms_pass1_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
+      if ((e = raise_smem_limit(k_block_rms_pass1_vec, smem)) != cudaSuccess) return e;
       // about 8 consecutive groups per block, spread evenly
       const size_t nblk_x = (ng1 + 7) / 8;
       const size_t gpb = (ng1 + nblk_x - 1) / nblk_x;
@@ -962,8 +960,7 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
     // window: one group of samples plus the widest boxcar on either side
     const size_t win = std::min<size_t>(pow5(m1) + 2 * (size_t)ctx.offset + 2, MULTI_SMEM_FLOATS);
     const size_t smem = (win + 625 + 125) * sizeof(float);
-    cudaFuncSetAttribute(k_block_rms_pass1_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    if ((e = raise_smem_limit(k_block_rms_pass1_multi, smem)) != cudaSuccess) return e;
     k_block_rms_pass1_multi<<<dim3((unsigned)ng1, ctx.nser), TREE_THREADS, smem, s>>>(
         ctx, w_begin, nwb, m1, (int)win, ws.a, ng1); note_launch();
   } else {
@@ -1580,15 +1577,15 @@ cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cud
   const size_t span4 = (HIT_TILE + 2 * (size_t)ctx.offset + 2 + 3) & ~(size_t)3;
   const size_t slen = ctx.scan_len;
   if (vec_hits_ok(ctx, nw1) && 2 * span4 * sizeof(float) <= 200 * 1024) {
-    cudaFuncSetAttribute(k_count_hits_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(2 * span4 * sizeof(float)));
+    if ((e = raise_smem_limit(k_count_hits_vec, 2 * span4 * sizeof(float))) != cudaSuccess)
+      return e;
     // about 8 consecutive tiles per block, spread evenly
     const unsigned nbx = (ntiles + 7) / 8;
     const unsigned tpb = (ntiles + nbx - 1) / nbx;
     k_count_hits_vec<<<dim3((ntiles + tpb - 1) / tpb, ctx.nser), HIT_THREADS,
                        2 * span4 * sizeof(float), s>>>(ctx, hb, nw1, slen, span4, (int)tpb); note_launch();
   } else if (nw1 > 0 && smem <= 200 * 1024) {
-    cudaFuncSetAttribute(k_count_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if ((e = raise_smem_limit(k_count_hits_multi, smem)) != cudaSuccess) return e;
     k_count_hits_multi<<<dim3(ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
   } else {
     nw1 = 0;
@@ -1613,12 +1610,12 @@ cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
   const size_t span4 = (HIT_TILE + 2 * (size_t)ctx.offset + 2 + 3) & ~(size_t)3;
   const size_t slen = ctx.scan_len;
   if (vec_hits_ok(ctx, nw1) && span4 * sizeof(float) <= 200 * 1024) {
-    cudaFuncSetAttribute(k_write_hits_vec, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(span4 * sizeof(float)));
+    if (cudaError_t e = raise_smem_limit(k_write_hits_vec, span4 * sizeof(float)))
+      return e;
     k_write_hits_vec<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, span4 * sizeof(float), s>>>(
         ctx, hb, nw1, slen, span4); note_launch();
   } else if (nw1 > 0 && smem <= 200 * 1024) {
-    cudaFuncSetAttribute(k_write_hits_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaError_t e = raise_smem_limit(k_write_hits_multi, smem)) return e;
     k_write_hits_multi<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();
   } else {
     nw1 = 0;
