@@ -98,3 +98,24 @@ def test_beam_set_one_worker_equals_many(hdb):
     for b in range(len(ws)):
         for f in FIELDS:
             np.testing.assert_array_equal(out[0][b][f], out[1][b][f])
+
+
+def test_beam_set_concurrent_workers_repeat(hdb):
+    """Many workers launching the same kernels with different shared-memory
+    sizes at once (every configuration differs): repeated calls never fail
+    and always give the same lists."""
+    ws, beams = _beams()
+    ws, beams = ws[:-1], beams[:-1]
+    params = [_params(w, 10 + b) for b, w in enumerate(ws)]
+    dev = [torch.from_numpy(b.data).cuda() for b in beams]
+    torch.cuda.synchronize()
+    with H.BeamSet(params, workers=len(ws), cleaning=True) as bs:
+        first = None
+        for _ in range(6):
+            err, st, _ = bs.execute([d.data_ptr() for d in dev], nsamps=[w.nsamps for w in ws],
+                                    on_device=True)
+            assert err in (H.HD_NO_ERROR, H.HD_TOO_MANY_EVENTS), st
+            lists = [H.cand_lines(bs.candidates(b)) for b in range(len(ws))]
+            if first is None:
+                first = lists
+            assert lists == first
