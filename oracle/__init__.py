@@ -122,6 +122,9 @@ def lib():
         L.or_exclusive_scan.argtypes = [_fp, C.c_size_t, _fp]
         L.or_linear_stretch.argtypes = [_fp, C.c_size_t, _fp, C.c_size_t]
         L.or_set_scan_capture.argtypes = [C.c_void_p, C.c_size_t]
+        L.or64_giant_snr.restype = C.c_int
+        L.or64_giant_snr.argtypes = [C.POINTER(OrParams), C.c_void_p, C.c_size_t, C.c_size_t,
+                                     C.c_size_t, _szp, _szp, _szp, C.POINTER(C.c_double)]
         L.or_normalise_rows.argtypes = [_fp, C.c_size_t, C.c_size_t]
         L.or_patch_dm.argtypes = [_fp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
                                   C.c_size_t, C.c_size_t, _fp]
@@ -344,6 +347,30 @@ def execute_with_scans(fb: np.ndarray, nbeams: int = 1, **kw):
     finally:
         lib().or_set_scan_capture(None, 0)
     return r, scans[:, :nsamps - md + 1], dms, table
+
+
+def giant_snr_fp64(fb: np.ndarray, dm_inds, filter_inds, inds, nbeams: int = 1,
+                   **kw) -> np.ndarray:
+    """S/N of the given giants (DM trial, filter index, giant sample index as
+    execute() reports them in "groups"/"giants") from the same chain with
+    every value held in double (snr64.c)."""
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    okw = {k: v for k, v in kw.items() if k not in ("output_dir",)}
+    p = make_params(nchans=nchans, **okw)
+    d = np.ascontiguousarray(dm_inds, dtype=np.uint64)
+    f = np.ascontiguousarray(filter_inds, dtype=np.uint64)
+    i = np.ascontiguousarray(inds, dtype=np.uint64)
+    n = len(d)
+    assert len(f) == n and len(i) == n
+    out = np.zeros(max(n, 1), np.float64)
+    err = lib().or64_giant_snr(C.byref(p), fb.ctypes.data, nsamps, nbeams, n,
+                               d.ctypes.data_as(_szp), f.ctypes.data_as(_szp),
+                               i.ctypes.data_as(_szp),
+                               out.ctypes.data_as(C.POINTER(C.c_double)))
+    if err:
+        raise RuntimeError(f"or64_giant_snr failed ({err})")
+    return out[:n]
 
 
 def normalise_rows(a: np.ndarray) -> np.ndarray:

@@ -136,6 +136,12 @@ int  or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t 
 void or_result_free(or_result* res);
 /* Test hook: keep every DM trial's prefix sum of the last or_hd_execute. */
 void or_set_scan_capture(float* buf, size_t pitch);
+/* The S/N of giants (DM trial, filter index, giant sample index as
+ * or_hd_execute reports them) from the same chain with every value in
+ * double (snr64.c).  Returns 0, or non-zero for a giant it cannot place. */
+int  or64_giant_snr(const or_params* p, const uint8_t* fb, size_t nsamps, size_t nbeams,
+                    size_t n, const size_t* dm_inds, const size_t* filter_inds,
+                    const size_t* inds, double* snr);
 
 /* ---- classifier (Applications/candidate_profiler.C and the CNN) ---- */
 void or_normalise_rows(float* data, size_t n, size_t nrows);

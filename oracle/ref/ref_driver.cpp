@@ -10,11 +10,9 @@
 #include "hd/default_params.h"
 #include "oracle.h"
 
-extern "C" int ref_execute(const or_params* p, const unsigned char* fb, size_t nsamps,
-                           size_t nbits, size_t first_idx, size_t nbeams,
-                           const char* output_dir, size_t* nsamps_processed,
-                           double* seconds, int nthreads) {
-  if (nthreads > 0) omp_set_num_threads(nthreads);
+static int run(const or_params* p, const unsigned char* fb, size_t nsamps, size_t nbits,
+               size_t first_idx, size_t nbeams, const char* output_dir,
+               size_t* nsamps_processed, double* seconds) {
   hd_params hp;
   hd_set_default_params(&hp);
   hp.verbosity = 0;
@@ -55,5 +53,19 @@ extern "C" int ref_execute(const or_params* p, const unsigned char* fb, size_t n
   auto t1 = std::chrono::steady_clock::now();
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   hd_destroy_pipeline(pl);
+  return e;
+}
+
+/* The thread count applies to this call only: the process's OpenMP default
+ * is put back, so later OpenMP work in the process keeps every thread. */
+extern "C" int ref_execute(const or_params* p, const unsigned char* fb, size_t nsamps,
+                           size_t nbits, size_t first_idx, size_t nbeams,
+                           const char* output_dir, size_t* nsamps_processed,
+                           double* seconds, int nthreads) {
+  const int prev = omp_get_max_threads();
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int e = run(p, fb, nsamps, nbits, first_idx, nbeams, output_dir, nsamps_processed,
+                    seconds);
+  omp_set_num_threads(prev);
   return e;
 }
