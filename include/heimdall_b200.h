@@ -155,7 +155,9 @@ hd_error hd_create_pipeline(hd_pipeline* pipeline, struct hd_params params);
 hd_error hd_preallocate(hd_pipeline pipeline, hd_size nsamps, hd_size nbeams);
 hd_size  hd_get_max_overlap(hd_pipeline pipeline, hd_size nbeams);
 /* One gulp: nsamps spectra (nbeams beams of nsamps/nbeams spectra each, time
- * concatenated) of nchans*nbits/8 bytes.  Candidates go to
+ * concatenated) of nchans*nbits/8 bytes; nbits 8 and nchans a multiple of 4
+ * (whole 32-bit words per spectrum, as Pipeline/clean_filterbank_rfi.cu:202-212
+ * assumes), else HD_INVALID_NBITS / HD_INVALID_STRIDE.  Candidates go to
  * <output_dir>/<UTC>_<beam+1>.cand as in Pipeline/pipeline.cu:1001-1044
  * (output_dir == NULL: no file).  Returns HD_TOO_MANY_EVENTS (soft) when the
  * giant rate exceeds max_giant_rate. */
