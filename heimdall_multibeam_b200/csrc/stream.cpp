@@ -9,9 +9,10 @@
 //
 // The loop keeps the overlap on the device: two device buffers alternate, the
 // overlap of each beam is copied device to device from the one just searched
-// into the next, and only the new block crosses PCIe.  A host thread reads the
-// next block from the file into pinned memory while the GPU searches the
-// current gulp.
+// into the next, and only the new block crosses PCIe.  While the GPU searches
+// the current gulp, a host thread reads the next block from the file into
+// pinned memory and copies it, with the overlap carry, into the other device
+// buffer on a separate stream.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -203,26 +204,51 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
   std::fseek(f, h.size, SEEK_SET);
 
   const size_t max_overlap = hd_get_max_overlap(pl, nbeams);  // all beams
+  const size_t M = hd_get_max_overlap(pl, 1);  // per beam: boxcar_max + max delay
+  const int dev = hdb::pipeline_device(pl);
   const size_t cap = (nsamps_gulp + max_overlap) * stride;
   const size_t block = nsamps_gulp * stride;
   hd_byte* d_buf[2] = {nullptr, nullptr};
   hd_byte* h_blk[2] = {nullptr, nullptr};
-  cudaStream_t s = nullptr;
+  cudaStream_t cs = nullptr;  // copies into the next gulp's buffer
   auto cleanup = [&]() {
+    if (cs) cudaStreamSynchronize(cs);
     for (auto p : d_buf) if (p) cudaFree(p);
     for (auto p : h_blk) if (p) cudaFreeHost(p);
-    if (s) cudaStreamDestroy(s);
+    if (cs) cudaStreamDestroy(cs);
     std::fclose(f);
   };
   if (cudaMalloc(&d_buf[0], cap) != cudaSuccess || cudaMalloc(&d_buf[1], cap) != cudaSuccess ||
       cudaMallocHost(&h_blk[0], block) != cudaSuccess ||
       cudaMallocHost(&h_blk[1], block) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
     cleanup();
     return HD_MEM_ALLOC_FAILED;
   }
   auto read_block = [&](hd_byte* dst) -> size_t {
     return std::fread(dst, 1, block, f) / stride;  // SigprocFile.C:59-68
+  };
+  // heimdall.C:209-265: the next gulp holds, beam by beam, the last `ov`
+  // spectra of that beam's region in the gulp just searched (per_beam
+  // spectra each, in d_buf[from]) followed by the beam's part of the new
+  // block (pinned h_blk[hb_new]).  The searched buffer is only read.
+  auto stage_next = [&](int from, int hb_new, size_t per_beam, size_t ov) -> bool {
+    const int to_buf = from ^ 1;
+    const size_t done_pb = per_beam - ov;
+    const size_t next_pb = ov + nsamps_gulp / nbeams;
+    for (size_t b = 0; b < nbeams && ov > 0; b++)
+      if (cudaMemcpyAsync(d_buf[to_buf] + b * next_pb * stride,
+                          d_buf[from] + (b * per_beam + done_pb) * stride, ov * stride,
+                          cudaMemcpyDeviceToDevice, cs) != cudaSuccess)
+        return false;
+    for (size_t b = 0; b < nbeams; b++) {
+      const size_t lo = b * nsamps_gulp / nbeams;
+      const size_t hi = (b + 1) * nsamps_gulp / nbeams;
+      if (cudaMemcpyAsync(d_buf[to_buf] + (ov + b * next_pb) * stride, h_blk[hb_new] + lo * stride,
+                          (hi - lo) * stride, cudaMemcpyHostToDevice, cs) != cudaSuccess)
+        return false;
+    }
+    return true;
   };
 
   // the first block is searched as it is (overlap 0)
@@ -235,21 +261,32 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
   hd_error result = HD_NO_ERROR;
   // the first block lands at the start of buffer 0 (beams in sequence)
   if (nsamps_read &&
-      cudaMemcpyAsync(d_buf[0], h_blk[0], nsamps_read * stride, cudaMemcpyHostToDevice, s) !=
+      cudaMemcpyAsync(d_buf[0], h_blk[0], nsamps_read * stride, cudaMemcpyHostToDevice, cs) !=
           cudaSuccess) {
     cleanup();
     return HD_MEM_COPY_FAILED;
   }
   bool stop = nsamps_read < nsamps_gulp;  // a short first block is never searched
   while (nsamps_read && !stop) {
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
+    // this gulp's spectra are in d_buf[cur]
+    if (cudaStreamSynchronize(cs) != cudaSuccess) {
       result = HD_MEM_COPY_FAILED;
       break;
     }
     const size_t to_process = nsamps_gulp + overlap * nbeams;
-    // read the next block on the host while the GPU searches this gulp
+    const size_t per_beam = to_process / nbeams;
+    // the overlap this search leaves: hd_execute sets nsamps_processed =
+    // nsamps - nbeams * M before any kernel runs (0 below that)
+    const size_t ov_pred = to_process >= nbeams * M ? M : per_beam;
+    // while the GPU searches this gulp, a host thread reads the next block
+    // and stages the next gulp (overlap carry and new block) on the copy stream
     size_t next_read = 0;
-    std::thread reader([&]() { next_read = read_block(h_blk[hb ^ 1]); });
+    bool staged = false;
+    std::thread reader([&]() {
+      next_read = read_block(h_blk[hb ^ 1]);
+      if (next_read < nsamps_gulp || cudaSetDevice(dev) != cudaSuccess) return;
+      staged = stage_next(cur, hb ^ 1, per_beam, ov_pred);
+    });
     hd_size processed = 0;
     e = hd_execute_device(pl, d_buf[cur], to_process, 8, total, nbeams, &processed);
     reader.join();
@@ -263,42 +300,22 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
     cands.resize(n);
     if (n) hd_get_candidates(pl, cands.data(), &n);
     if (on_gulp) on_gulp(user, cands.data(), n, (hd_size)total);
-    // heimdall.C:209-265: overlap per beam, samples searched, and the copy
-    // of each beam's overlap to the front of its region in the next buffer
     overlap = (to_process - processed) / nbeams;
     total += processed / nbeams;
-    const size_t per_beam = to_process / nbeams;
-    const size_t done_per_beam = per_beam - overlap;
-    const size_t next_per_beam = overlap + nsamps_gulp / nbeams;
-    const int nxt = cur ^ 1;
-    for (size_t b = 0; b < nbeams && overlap > 0; b++) {
-      const size_t from = b * per_beam + done_per_beam;
-      const size_t to = b * next_per_beam;
-      if (cudaMemcpyAsync(d_buf[nxt] + to * stride, d_buf[cur] + from * stride, overlap * stride,
-                          cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
-        result = HD_MEM_COPY_FAILED;
-        break;
-      }
-    }
-    if (result != HD_NO_ERROR) break;
     nsamps_read = next_read;
     hb ^= 1;
     // a short block ends the search (heimdall.C:269-272,285-287)
     if (nsamps_read < nsamps_gulp) break;
-    for (size_t b = 0; b < nbeams; b++) {
-      const size_t from = b * nsamps_gulp / nbeams;
-      const size_t to_b = (b + 1) * nsamps_gulp / nbeams;
-      const size_t to = overlap + b * (nsamps_gulp / nbeams + overlap);
-      if (cudaMemcpyAsync(d_buf[nxt] + to * stride, h_blk[hb] + from * stride,
-                          (to_b - from) * stride, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+    if (!staged || overlap != ov_pred) {
+      // the staging did not happen or assumed another overlap: place the
+      // next gulp again once the copy stream is idle
+      if (cudaStreamSynchronize(cs) != cudaSuccess || !stage_next(cur, hb, per_beam, overlap)) {
         result = HD_MEM_COPY_FAILED;
         break;
       }
     }
-    if (result != HD_NO_ERROR) break;
-    cur = nxt;
+    cur ^= 1;
   }
-  cudaStreamSynchronize(s);
   cleanup();
   if (total_nsamps) *total_nsamps = total;
   if (ngulps) *ngulps = gulps;

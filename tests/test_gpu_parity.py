@@ -221,6 +221,25 @@ def test_too_few_samples(hdb):
     assert err == H.HD_TOO_FEW_NSAMPS and len(c) == 0
 
 
+@pytest.mark.parametrize("clean", [False, True])
+def test_channel_count_not_whole_words(hdb, clean):
+    """8-bit spectra of 130 channels are not whole 32-bit words: rejected
+    before any work, and the pipeline still searches a valid gulp after."""
+    fb = np.zeros((8192, 130), np.uint8)
+    p = H.default_params(nchans=130, dt=655.36e-6, f0=851.0, df=-0.3125, dm_max=300.0,
+                         boxcar_max=64, output_dir=None)
+    with H.Pipeline(p, cleaning=clean) as pl:
+        err, _ = pl.execute(fb, raise_on_error=False)
+        assert err == H.HD_INVALID_STRIDE
+        err, _, _ = pl.execute_beams([fb, fb], raise_on_error=False)
+        assert err == H.HD_INVALID_STRIDE
+        assert len(pl.candidates()) == 0
+    w = synth.SEARCH_C0
+    b = synth.make_c0()
+    err, _, c, _ = _run_gpu(b.data, clean=clean, **_params(w))
+    assert err == H.HD_NO_ERROR and len(c) >= 3
+
+
 def test_cand_file_written(hdb, tmp_path):
     b = synth.make_c0()
     p = H.default_params(output_dir=str(tmp_path), spectra_per_second=15625,

@@ -53,3 +53,46 @@ def test_sigproc_gulp_loop(hdb, oracle_lib, tmp_path):
             assert H.cand_lines(got) == lines
             found += len(got)
     assert found >= 9
+
+
+def test_sigproc_gulp_loop_two_beams(hdb, tmp_path):
+    """A file of 2 beams (nbeams = 2 in the header): each block of GULP
+    spectra holds beam 0's GULP / 2 spectra and then beam 1's.  Every gulp is
+    the STF concatenation of each beam's overlap carry and its part of the
+    block, and its candidates equal an hd_execute of that gulp (cleaning on,
+    so the per-beam cleaning of the loop's gulps is covered too)."""
+    half = GULP // 2
+    nfull, tail = 3, 3000
+    per_beam = nfull * half + tail
+    rng = np.random.default_rng(91)
+    streams = []
+    for b in range(2):
+        pulses = [synth.Pulse(float(t), float(dm), 1e-3, 25.0)
+                  for t, dm in zip(rng.uniform(2000, per_beam - 3000, 5), rng.uniform(20, 280, 5))]
+        streams.append(synth.make_beam(per_beam, NCH, DT, F0, DF, pulses, seed=92 + b).data)
+    rows = []
+    for k in range(nfull):
+        rows += [streams[0][k * half:(k + 1) * half], streams[1][k * half:(k + 1) * half]]
+    rows.append(streams[0][nfull * half:])  # a short last block: not searched
+    data = np.concatenate(rows)
+    path = str(tmp_path / "two_beams.fil")
+    synth.write_sigproc(path, data, nchans=NCH, nbits=8, tsamp=DT, fch1=F0, foff=DF,
+                        tstart=60000.5, nifs=1, nbeams=2, ibeam=1, source_name="two_beams")
+    kw = dict(dm_min=0.0, dm_max=300.0, boxcar_max=256)
+    params = H.params_from_sigproc(path, H.default_params(output_dir=None, **kw))
+    with H.Pipeline(params, cleaning=True) as pl:
+        overlap = pl.max_overlap()  # per beam
+        err, total, gulps = pl.search_sigproc_file(path, GULP)
+    assert err == H.HD_NO_ERROR
+    plan = oracle.gulp_plan(per_beam, half, overlap)
+    assert len(gulps) == len(plan) == nfull
+    assert total == sum(n - overlap for _, n, _ in plan)
+    found = 0
+    with H.Pipeline(params, cleaning=True) as ref:
+        for (start, n, first), (first_got, got) in zip(plan, gulps):
+            assert first_got == first
+            g = np.concatenate([s[start:start + n] for s in streams])
+            ref.execute(g, nbeams=2, first_idx=first)
+            assert H.cand_lines(got) == H.cand_lines(ref.candidates())
+            found += len(got)
+    assert found >= 5
