@@ -11,9 +11,10 @@
 // overlap of each beam is copied device to device from the one just searched
 // into the next, and only the new block crosses PCIe.  While the GPU searches
 // the current gulp, a host thread reads the next block from the file into
-// pinned memory and copies it, with the overlap carry, into the other device
-// buffer on a separate stream.
+// pinned memory (in parallel pieces) and copies it, with the overlap carry,
+// into the other device buffer on a separate stream.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -21,6 +22,9 @@
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <cuda_runtime.h>
 
@@ -201,7 +205,6 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
   if (cudaSetDevice(hdb::pipeline_device(pl)) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
   FILE* f = std::fopen(path, "rb");
   if (!f) return HD_INVALID_POINTER;
-  std::fseek(f, h.size, SEEK_SET);
 
   const size_t max_overlap = hd_get_max_overlap(pl, nbeams);  // all beams
   const size_t M = hd_get_max_overlap(pl, 1);  // per beam: boxcar_max + max delay
@@ -225,8 +228,34 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
     cleanup();
     return HD_MEM_ALLOC_FAILED;
   }
+  // SigprocFile.C:59-68 reads up to a block of whole spectra.  Here the
+  // block's bytes are read by up to 8 threads at disjoint offsets (positioned
+  // reads), which a single stream read cannot keep up with at gulp sizes.
+  const int fd = fileno(f);
+  struct stat st;
+  const size_t file_size = fstat(fd, &st) == 0 ? (size_t)st.st_size : 0;
+  size_t pos = (size_t)h.size;
   auto read_block = [&](hd_byte* dst) -> size_t {
-    return std::fread(dst, 1, block, f) / stride;  // SigprocFile.C:59-68
+    const size_t want = std::min(block, file_size > pos ? file_size - pos : (size_t)0);
+    const size_t nt = std::min<size_t>(8, std::max<size_t>(1, want >> 23));
+    std::atomic<bool> ok{true};
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < nt; i++)
+      th.emplace_back([&, i]() {
+        size_t lo = want * i / nt;
+        const size_t hi = want * (i + 1) / nt;
+        while (lo < hi) {
+          const ssize_t r = pread(fd, dst + lo, hi - lo, (off_t)(pos + lo));
+          if (r <= 0) {
+            ok = false;
+            return;
+          }
+          lo += (size_t)r;
+        }
+      });
+    for (auto& t : th) t.join();
+    pos += want;
+    return ok ? want / stride : 0;  // a read error ends the loop
   };
   // heimdall.C:209-265: the next gulp holds, beam by beam, the last `ov`
   // spectra of that beam's region in the gulp just searched (per_beam
