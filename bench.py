@@ -723,6 +723,60 @@ def run_reference(args):
         "wall_s": round(wall, 1)}), flush=True)
 
 
+def stream_file_bench(args, H, torch):
+    """hd_search_sigproc_file on a survey-shaped sigproc file (1024 ch, 64 us,
+    DM 0-2000, boxcars to 4096, cleaning on; gulps of 2^18 new spectra):
+    the time between consecutive gulps' callbacks (steady state) against the
+    device-resident search of one full gulp, and the start-up before the
+    first gulp.  The file is written to a temporary directory and read once
+    before timing (page cache)."""
+    import ctypes as C
+    import tempfile
+    from heimdall_multibeam_b200 import synth
+    w = synth.SEARCH_C1
+    G = 1 << 18
+    nblocks = max(3, args.stream_blocks)
+    rng = np.random.default_rng(5)
+    data = rng.integers(100, 156, size=(nblocks * G + 1000, w.nchans), dtype=np.uint8)
+    out = {"workload": f"sigproc_file_c{w.nchans}_{nblocks}x{G}", "api": "hd_search_sigproc_file"}
+    with tempfile.TemporaryDirectory(dir=args.stream_dir) as tmp:
+        path = os.path.join(tmp, "survey.fil")
+        synth.write_sigproc(path, data, nchans=w.nchans, nbits=8, tsamp=w.dt, fch1=w.f0,
+                            foff=w.df, tstart=60000.5, nifs=1, source_name="survey")
+        with open(path, "rb") as f:
+            while f.read(1 << 26):
+                pass
+        kw = dict(dm_min=w.dm_min, dm_max=w.dm_max, boxcar_max=w.boxcar_max, output_dir=None)
+        params = H.params_from_sigproc(path, H.default_params(**kw))
+        with H.Pipeline(params, cleaning=True) as pl:
+            M = pl.max_overlap()
+            stamps = []
+            fn = H.GULP_CALLBACK(lambda user, cands, n, first: stamps.append(time.perf_counter()))
+            tot, ng = C.c_size_t(0), C.c_size_t(0)
+            for rep in range(2):  # the first pass tunes and allocates
+                stamps.clear()
+                t0 = time.perf_counter()
+                err = H.lib().hd_search_sigproc_file(pl._p, path.encode(), G, fn, None,
+                                                     C.byref(tot), C.byref(ng))
+                t1 = time.perf_counter()
+                assert err == H.HD_NO_ERROR, err
+            gaps = [1e3 * (b - a) for a, b in zip(stamps, stamps[1:])]
+            d = torch.from_numpy(data[:G + M]).cuda()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(4):
+                pl.execute_device(d.data_ptr(), G + M)
+                ts.append(pl.timing()["total"])
+    steady = float(np.median(gaps))
+    out.update({"gulps": ng.value, "ms_between_gulps": round(steady, 2),
+                "ms_between_gulps_all": [round(g, 2) for g in gaps],
+                "device_search_ms": round(min(ts[1:]), 2),
+                "startup_ms": round(1e3 * (stamps[0] - t0), 1),
+                "beam_s_per_s_steady": round(G * w.dt / (steady * 1e-3), 1),
+                "beam_s_per_s_whole_call": round(tot.value * w.dt / (t1 - t0), 1)})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -753,7 +807,18 @@ def main():
                     help="whole beams the reference runs per multibeam sample")
     ap.add_argument("--ref-dm1", type=float, default=20.0)
     ap.add_argument("--ref-dm2", type=float, default=60.0)
+    ap.add_argument("--only-stream-file", action="store_true",
+                    help="only the sigproc file gulp loop (writes a temporary file)")
+    ap.add_argument("--stream-blocks", type=int, default=7)
+    ap.add_argument("--stream-dir", default=None,
+                    help="directory for the temporary file (default: the system's)")
     args = ap.parse_args()
+    if args.only_stream_file:
+        import torch
+        import heimdall_multibeam_b200 as H
+        torch.cuda.set_device(0)
+        print(json.dumps({"stream_file": stream_file_bench(args, H, torch)}), flush=True)
+        return
     if args.only_classifier:
         import torch
         import heimdall_multibeam_b200 as H
