@@ -190,6 +190,8 @@ SYMBOLS = {
     "hd_params_from_sigproc": (C.c_int, [C.POINTER(HdSigprocHeader), C.POINTER(HdParams)]),
     "hd_search_sigproc_file": (C.c_int, [_P, C.c_char_p, _SZ, GULP_CALLBACK, C.c_void_p, _SZP,
                                          _SZP]),
+    "hd_search_sigproc_files": (C.c_int, [_P, C.POINTER(C.c_char_p), _SZ, _SZ, GULP_CALLBACK,
+                                          C.c_void_p, _SZP, _SZP]),
     "hd_extract_patches": (C.c_int, [_P, _FP, _FP, _SZP]),
     "hd_classifier_param_count": (_SZ, []),
     "hd_classifier_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_ulonglong]),
@@ -528,6 +530,27 @@ class Pipeline:
         proc = C.c_size_t(0)
         err = lib().hd_execute_prefetched(self._p, first_idx, nbeams, bm, st, C.byref(proc))
         return err, proc.value, list(st)[:nunits]
+
+    def search_sigproc_files(self, paths: Sequence[str], nsamps_gulp: int):
+        """hd_search_sigproc_files over files read in lockstep: (hd_error,
+        total spectra searched per beam, [(first_idx, candidates of all
+        files) per gulp])."""
+        gulps = []
+
+        def cb(user, cands, n, first_idx):
+            a = np.zeros(n, CANDIDATE_DTYPE)
+            if n:
+                C.memmove(a.ctypes.data, cands, n * CANDIDATE_DTYPE.itemsize)
+            gulps.append((int(first_idx), a))
+
+        fn = GULP_CALLBACK(cb)
+        arr = (C.c_char_p * len(paths))(*[p.encode() for p in paths])
+        total = C.c_size_t(0)
+        ng = C.c_size_t(0)
+        err = lib().hd_search_sigproc_files(self._p, arr, len(paths), nsamps_gulp, fn, None,
+                                            C.byref(total), C.byref(ng))
+        assert ng.value == len(gulps)
+        return err, total.value, gulps
 
     def search_sigproc_file(self, path: str, nsamps_gulp: int):
         """hd_search_sigproc_file: (hd_error, total spectra searched per beam,

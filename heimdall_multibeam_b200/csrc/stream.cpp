@@ -190,26 +190,52 @@ hd_error hd_params_from_sigproc(const hd_sigproc_header* h, struct hd_params* p)
   return HD_NO_ERROR;
 }
 
-hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps_gulp,
-                                hd_gulp_callback on_gulp, void* user, hd_size* total_nsamps,
-                                hd_size* ngulps) {
+}  // extern "C"
+
+namespace {
+
+// The gulp loop over nfiles files read in lockstep.  File u is unit u of
+// each gulp: one file is searched with hd_execute_device, several with one
+// hd_execute_beams call per gulp.  Every file has the same header fields
+// that shape the search (channels, bits, sampling time, band, beams per
+// file); the first short block of any file ends the loop.
+hd_error search_files(hd_pipeline pl, const char* const* paths, size_t nfiles,
+                      hd_size nsamps_gulp, hd_gulp_callback on_gulp, void* user,
+                      hd_size* total_nsamps, hd_size* ngulps) {
   if (!pl) return HD_INVALID_PIPELINE;
-  if (!path) return HD_INVALID_POINTER;
-  hd_sigproc_header h;
-  hd_error e = hd_read_sigproc_header(path, &h);
-  if (e != HD_NO_ERROR) return e;
+  if (!paths || nfiles == 0) return HD_INVALID_POINTER;
+  for (size_t u = 0; u < nfiles; u++)
+    if (!paths[u]) return HD_INVALID_POINTER;
+  std::vector<hd_sigproc_header> hs(nfiles);
+  for (size_t u = 0; u < nfiles; u++) {
+    const hd_error e = hd_read_sigproc_header(paths[u], &hs[u]);
+    if (e != HD_NO_ERROR) return e;
+  }
+  const hd_sigproc_header& h = hs[0];
   if (h.nbits != 8) return HD_INVALID_NBITS;
+  for (size_t u = 1; u < nfiles; u++) {
+    const hd_sigproc_header& g = hs[u];
+    if (g.nbits != h.nbits || g.nchans != h.nchans || g.tsamp != h.tsamp || g.fch1 != h.fch1 ||
+        g.foff != h.foff || g.nbeams != h.nbeams)
+      return HD_INVALID_STRIDE;
+  }
   const size_t nbeams = h.nbeams > 0 ? (size_t)h.nbeams : 1;
   const size_t stride = (size_t)h.nchans;  // bytes per spectrum (8-bit)
   if (nsamps_gulp == 0 || nsamps_gulp % nbeams != 0) return HD_INVALID_STRIDE;
   if (cudaSetDevice(hdb::pipeline_device(pl)) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
-  FILE* f = std::fopen(path, "rb");
-  if (!f) return HD_INVALID_POINTER;
+  std::vector<FILE*> fs(nfiles, nullptr);
+  for (size_t u = 0; u < nfiles; u++) {
+    fs[u] = std::fopen(paths[u], "rb");
+    if (!fs[u]) {
+      for (FILE* f : fs) if (f) std::fclose(f);
+      return HD_INVALID_POINTER;
+    }
+  }
 
-  const size_t max_overlap = hd_get_max_overlap(pl, nbeams);  // all beams
+  const size_t max_overlap = hd_get_max_overlap(pl, nbeams);  // all beams of a file
   const size_t M = hd_get_max_overlap(pl, 1);  // per beam: boxcar_max + max delay
   const int dev = hdb::pipeline_device(pl);
-  const size_t cap = (nsamps_gulp + max_overlap) * stride;
+  const size_t cap = (nsamps_gulp + max_overlap) * stride;  // one file's region
   const size_t block = nsamps_gulp * stride;
   hd_byte* d_buf[2] = {nullptr, nullptr};
   hd_byte* h_blk[2] = {nullptr, nullptr};
@@ -219,25 +245,31 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
     for (auto p : d_buf) if (p) cudaFree(p);
     for (auto p : h_blk) if (p) cudaFreeHost(p);
     if (cs) cudaStreamDestroy(cs);
-    std::fclose(f);
+    for (FILE* f : fs) std::fclose(f);
   };
-  if (cudaMalloc(&d_buf[0], cap) != cudaSuccess || cudaMalloc(&d_buf[1], cap) != cudaSuccess ||
-      cudaMallocHost(&h_blk[0], block) != cudaSuccess ||
-      cudaMallocHost(&h_blk[1], block) != cudaSuccess ||
+  if (cudaMalloc(&d_buf[0], nfiles * cap) != cudaSuccess ||
+      cudaMalloc(&d_buf[1], nfiles * cap) != cudaSuccess ||
+      cudaMallocHost(&h_blk[0], nfiles * block) != cudaSuccess ||
+      cudaMallocHost(&h_blk[1], nfiles * block) != cudaSuccess ||
       cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
     cleanup();
     return HD_MEM_ALLOC_FAILED;
   }
-  // SigprocFile.C:59-68 reads up to a block of whole spectra.  Here the
+  // SigprocFile.C:59-68 reads up to a block of whole spectra.  Here each
   // block's bytes are read by up to 8 threads at disjoint offsets (positioned
   // reads), which a single stream read cannot keep up with at gulp sizes.
-  const int fd = fileno(f);
-  struct stat st;
-  const size_t file_size = fstat(fd, &st) == 0 ? (size_t)st.st_size : 0;
-  size_t pos = (size_t)h.size;
-  auto read_block = [&](hd_byte* dst) -> size_t {
-    const size_t want = std::min(block, file_size > pos ? file_size - pos : (size_t)0);
+  std::vector<size_t> pos(nfiles), file_size(nfiles);
+  for (size_t u = 0; u < nfiles; u++) {
+    struct stat st;
+    file_size[u] = fstat(fileno(fs[u]), &st) == 0 ? (size_t)st.st_size : 0;
+    pos[u] = (size_t)hs[u].size;
+  }
+  auto read_one = [&](size_t u, hd_byte* dst) -> size_t {
+    const int fd = fileno(fs[u]);
+    const size_t want =
+        std::min(block, file_size[u] > pos[u] ? file_size[u] - pos[u] : (size_t)0);
     const size_t nt = std::min<size_t>(8, std::max<size_t>(1, want >> 23));
+    const size_t base = pos[u];
     std::atomic<bool> ok{true};
     std::vector<std::thread> th;
     for (size_t i = 0; i < nt; i++)
@@ -245,7 +277,7 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
         size_t lo = want * i / nt;
         const size_t hi = want * (i + 1) / nt;
         while (lo < hi) {
-          const ssize_t r = pread(fd, dst + lo, hi - lo, (off_t)(pos + lo));
+          const ssize_t r = pread(fd, dst + lo, hi - lo, (off_t)(base + lo));
           if (r <= 0) {
             ok = false;
             return;
@@ -254,48 +286,63 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
         }
       });
     for (auto& t : th) t.join();
-    pos += want;
+    pos[u] += want;
     return ok ? want / stride : 0;  // a read error ends the loop
   };
-  // heimdall.C:209-265: the next gulp holds, beam by beam, the last `ov`
-  // spectra of that beam's region in the gulp just searched (per_beam
-  // spectra each, in d_buf[from]) followed by the beam's part of the new
-  // block (pinned h_blk[hb_new]).  The searched buffer is only read.
+  // the next block of every file into h_blk[hb] (file u at u * block); the
+  // fewest whole spectra any file gave
+  auto read_blocks = [&](int hb_) -> size_t {
+    size_t least = block / stride;
+    for (size_t u = 0; u < nfiles; u++)
+      least = std::min(least, read_one(u, h_blk[hb_] + u * block));
+    return least;
+  };
+  // heimdall.C:209-265: the next gulp of file u holds, beam by beam, the
+  // last `ov` spectra of that beam's region in the gulp just searched
+  // (per_beam spectra each, in d_buf[from]) followed by the beam's part of
+  // the file's new block (pinned h_blk[hb_new]).  The searched buffer is
+  // only read.
   auto stage_next = [&](int from, int hb_new, size_t per_beam, size_t ov) -> bool {
     const int to_buf = from ^ 1;
     const size_t done_pb = per_beam - ov;
     const size_t next_pb = ov + nsamps_gulp / nbeams;
-    for (size_t b = 0; b < nbeams && ov > 0; b++)
-      if (cudaMemcpyAsync(d_buf[to_buf] + b * next_pb * stride,
-                          d_buf[from] + (b * per_beam + done_pb) * stride, ov * stride,
-                          cudaMemcpyDeviceToDevice, cs) != cudaSuccess)
-        return false;
-    for (size_t b = 0; b < nbeams; b++) {
-      const size_t lo = b * nsamps_gulp / nbeams;
-      const size_t hi = (b + 1) * nsamps_gulp / nbeams;
-      if (cudaMemcpyAsync(d_buf[to_buf] + (ov + b * next_pb) * stride, h_blk[hb_new] + lo * stride,
-                          (hi - lo) * stride, cudaMemcpyHostToDevice, cs) != cudaSuccess)
-        return false;
+    for (size_t u = 0; u < nfiles; u++) {
+      hd_byte* dst = d_buf[to_buf] + u * cap;
+      const hd_byte* src = d_buf[from] + u * cap;
+      const hd_byte* blk = h_blk[hb_new] + u * block;
+      for (size_t b = 0; b < nbeams && ov > 0; b++)
+        if (cudaMemcpyAsync(dst + b * next_pb * stride, src + (b * per_beam + done_pb) * stride,
+                            ov * stride, cudaMemcpyDeviceToDevice, cs) != cudaSuccess)
+          return false;
+      for (size_t b = 0; b < nbeams; b++) {
+        const size_t lo = b * nsamps_gulp / nbeams;
+        const size_t hi = (b + 1) * nsamps_gulp / nbeams;
+        if (cudaMemcpyAsync(dst + (ov + b * next_pb) * stride, blk + lo * stride,
+                            (hi - lo) * stride, cudaMemcpyHostToDevice, cs) != cudaSuccess)
+          return false;
+      }
     }
     return true;
   };
 
-  // the first block is searched as it is (overlap 0)
-  size_t nsamps_read = read_block(h_blk[0]);
+  // the first block of every file is searched as it is (overlap 0)
+  size_t nsamps_read = read_blocks(0);
   int cur = 0, hb = 0;
   size_t overlap = 0;      // per beam
   size_t total = 0;        // samples per beam searched so far
   size_t gulps = 0;
   std::vector<hd_candidate> cands;
+  std::vector<const hd_byte*> units(nfiles);
+  std::vector<hd_error> statuses(nfiles);
   hd_error result = HD_NO_ERROR;
-  // the first block lands at the start of buffer 0 (beams in sequence)
-  if (nsamps_read &&
-      cudaMemcpyAsync(d_buf[0], h_blk[0], nsamps_read * stride, cudaMemcpyHostToDevice, cs) !=
-          cudaSuccess) {
-    cleanup();
-    return HD_MEM_COPY_FAILED;
-  }
   bool stop = nsamps_read < nsamps_gulp;  // a short first block is never searched
+  // the first blocks land at the start of each file's region of buffer 0
+  for (size_t u = 0; u < nfiles && !stop; u++)
+    if (cudaMemcpyAsync(d_buf[0] + u * cap, h_blk[0] + u * block, block, cudaMemcpyHostToDevice,
+                        cs) != cudaSuccess) {
+      cleanup();
+      return HD_MEM_COPY_FAILED;
+    }
   while (nsamps_read && !stop) {
     // this gulp's spectra are in d_buf[cur]
     if (cudaStreamSynchronize(cs) != cudaSuccess) {
@@ -307,17 +354,24 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
     // the overlap this search leaves: hd_execute sets nsamps_processed =
     // nsamps - nbeams * M before any kernel runs (0 below that)
     const size_t ov_pred = to_process >= nbeams * M ? M : per_beam;
-    // while the GPU searches this gulp, a host thread reads the next block
-    // and stages the next gulp (overlap carry and new block) on the copy stream
+    // while the GPU searches this gulp, a host thread reads the next blocks
+    // and stages the next gulp (overlap carry and new blocks) on the copy stream
     size_t next_read = 0;
     bool staged = false;
     std::thread reader([&]() {
-      next_read = read_block(h_blk[hb ^ 1]);
+      next_read = read_blocks(hb ^ 1);
       if (next_read < nsamps_gulp || cudaSetDevice(dev) != cudaSuccess) return;
       staged = stage_next(cur, hb ^ 1, per_beam, ov_pred);
     });
     hd_size processed = 0;
-    e = hd_execute_device(pl, d_buf[cur], to_process, 8, total, nbeams, &processed);
+    hd_error e;
+    if (nfiles == 1) {
+      e = hd_execute_device(pl, d_buf[cur], to_process, 8, total, nbeams, &processed);
+    } else {
+      for (size_t u = 0; u < nfiles; u++) units[u] = d_buf[cur] + u * cap;
+      e = hd_execute_beams(pl, units.data(), nfiles, to_process, 8, total, nbeams, nullptr, 1,
+                           statuses.data(), &processed);
+    }
     reader.join();
     if (e != HD_NO_ERROR && e != HD_TOO_MANY_EVENTS) {
       result = e;
@@ -349,6 +403,24 @@ hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps
   if (total_nsamps) *total_nsamps = total;
   if (ngulps) *ngulps = gulps;
   return result;
+}
+
+}  // namespace
+
+extern "C" {
+
+hd_error hd_search_sigproc_file(hd_pipeline pl, const char* path, hd_size nsamps_gulp,
+                                hd_gulp_callback on_gulp, void* user, hd_size* total_nsamps,
+                                hd_size* ngulps) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  if (!path) return HD_INVALID_POINTER;
+  return search_files(pl, &path, 1, nsamps_gulp, on_gulp, user, total_nsamps, ngulps);
+}
+
+hd_error hd_search_sigproc_files(hd_pipeline pl, const char* const* paths, hd_size nfiles,
+                                 hd_size nsamps_gulp, hd_gulp_callback on_gulp, void* user,
+                                 hd_size* total_nsamps, hd_size* ngulps) {
+  return search_files(pl, paths, nfiles, nsamps_gulp, on_gulp, user, total_nsamps, ngulps);
 }
 
 }  // extern "C"

@@ -25,7 +25,7 @@
  * hd_get_dedisp_tile, hd_get_launch_count, hd_clean_filterbank_rfi_noalloc;
  * beam sets (hd_*_beam_set*); sigproc input and the gulp loop
  * (hd_read_sigproc_header, hd_mjd_to_utc, hd_params_from_sigproc,
- * hd_search_sigproc_file); the coincidencer (hd_coincide,
+ * hd_search_sigproc_file, hd_search_sigproc_files); the coincidencer (hd_coincide,
  * hd_write_coincident_candidates); the candidate classifier
  * (hd_extract_patches, hd_score_candidates, hd_classifier_*).
  *
@@ -406,6 +406,16 @@ typedef void (*hd_gulp_callback)(void* user, const hd_candidate* candidates, hd_
 hd_error hd_search_sigproc_file(hd_pipeline pipeline, const char* path, hd_size nsamps_gulp,
                                 hd_gulp_callback on_gulp, void* user, hd_size* total_nsamps,
                                 hd_size* ngulps);
+/* The same loop over nfiles files read in lockstep, e.g. one file per beam
+ * of a multibeam receiver (no reference counterpart: heimdall.C runs one
+ * process per file).  Every file needs the same channels, bits, sampling
+ * time, band and beams per file (else HD_INVALID_STRIDE).  Each gulp is one
+ * hd_execute_beams call over the files' gulps, with file u as unit u (beam
+ * numbers params.beam + u * nbeams); the first short block of any file ends
+ * the search.  on_gulp receives all files' candidates, unit by unit. */
+hd_error hd_search_sigproc_files(hd_pipeline pipeline, const char* const* paths, hd_size nfiles,
+                                 hd_size nsamps_gulp, hd_gulp_callback on_gulp, void* user,
+                                 hd_size* total_nsamps, hd_size* ngulps);
 
 /* Candidates of the last hd_execute, in .cand order.  Copies
  * min(*count, available) rows into out (out may be NULL to query) and sets

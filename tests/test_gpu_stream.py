@@ -96,3 +96,58 @@ def test_sigproc_gulp_loop_two_beams(hdb, tmp_path):
             assert H.cand_lines(got) == H.cand_lines(ref.candidates())
             found += len(got)
     assert found >= 5
+
+
+def test_sigproc_files_lockstep(hdb, tmp_path):
+    """hd_search_sigproc_files over three single-beam files: every gulp is one
+    hd_execute_beams call over the three files' gulps, and its candidates are,
+    file by file, those of hd_search_sigproc_file on that file alone (with
+    the file's beam number).  The shortest file ends the loop; files of
+    another channel count are refused."""
+    rng = np.random.default_rng(101)
+    paths, lengths = [], [3 * GULP + 5000, 3 * GULP + 9000, 2 * GULP + 7000]
+    for u, nsamps in enumerate(lengths):
+        pulses = [synth.Pulse(float(t), float(dm), 1e-3, 25.0)
+                  for t, dm in zip(rng.uniform(2000, nsamps - 4000, 6), rng.uniform(20, 280, 6))]
+        b = synth.make_beam(nsamps, NCH, DT, F0, DF, pulses, seed=110 + u)
+        path = str(tmp_path / f"beam{u}.fil")
+        synth.write_sigproc(path, b.data, nchans=NCH, nbits=8, tsamp=DT, fch1=F0, foff=DF,
+                            tstart=60000.5, nifs=1, ibeam=u + 1, source_name="lockstep")
+        paths.append(path)
+    kw = dict(dm_min=0.0, dm_max=300.0, boxcar_max=256, output_dir=None)
+
+    def params(beam):
+        q = H.default_params(**kw)
+        q.override_beam = True
+        q.beam = beam
+        return H.params_from_sigproc(paths[0], q)
+
+    singles = []
+    for u, path in enumerate(paths):
+        with H.Pipeline(params(u), cleaning=True) as pl:
+            err, total, gulps = pl.search_sigproc_file(path, GULP)
+            assert err == H.HD_NO_ERROR
+            singles.append((total, gulps))
+    with H.Pipeline(params(0), cleaning=True) as pl:
+        err, total, gulps = pl.search_sigproc_files(paths, GULP)
+    assert err == H.HD_NO_ERROR
+    ng = min(len(g) for _, g in singles)
+    assert ng == 2 and len(gulps) == ng
+    assert total == singles[2][0]  # the shortest file's two gulps
+    found = 0
+    for k in range(ng):
+        first, got = gulps[k]
+        want = []
+        for _, g_u in singles:
+            assert g_u[k][0] == first
+            want += H.cand_lines(g_u[k][1])
+        assert H.cand_lines(got) == want
+        found += len(got)
+    assert found >= 6
+    # files that do not share the search's shape are refused
+    other = str(tmp_path / "other.fil")
+    synth.write_sigproc(other, np.zeros((GULP, NCH // 2), np.uint8), nchans=NCH // 2, nbits=8,
+                        tsamp=DT, fch1=F0, foff=DF, tstart=60000.5, nifs=1)
+    with H.Pipeline(params(0), cleaning=True) as pl:
+        err, _, gulps = pl.search_sigproc_files([paths[0], other], GULP)
+    assert err == H.HD_INVALID_STRIDE and gulps == []
