@@ -724,56 +724,71 @@ def run_reference(args):
 
 
 def stream_file_bench(args, H, torch):
-    """hd_search_sigproc_file on a survey-shaped sigproc file (1024 ch, 64 us,
-    DM 0-2000, boxcars to 4096, cleaning on; gulps of 2^18 new spectra):
-    the time between consecutive gulps' callbacks (steady state) against the
-    device-resident search of one full gulp, and the start-up before the
-    first gulp.  The file is written to a temporary directory and read once
-    before timing (page cache)."""
+    """The sigproc file gulp loop's steady state.  "survey": one file of the
+    survey beam's shape (1024 ch, 64 us, DM 0-2000, boxcars to 4096,
+    cleaning on; gulps of 2^18 new spectra) through hd_search_sigproc_file.
+    "multibeam": 36 one-beam files of the multibeam gulp's shape (320 ch,
+    655.36 us, DM 0-2000, boxcars to 512, cleaning off; gulps of 2^15 new
+    spectra per file) through hd_search_sigproc_files, one batched search
+    per gulp.  Reported: the time between consecutive gulps' callbacks
+    against the device-resident search of one full gulp, and the start-up
+    before the first gulp.  The files are written to a temporary directory
+    and read once before timing (page cache)."""
     import ctypes as C
     import tempfile
     from heimdall_multibeam_b200 import synth
-    w = synth.SEARCH_C1
-    G = 1 << 18
+    multi = args.stream_workload == "multibeam"
+    w = synth.SEARCH_C2 if multi else synth.SEARCH_C1
+    nfiles = w.nbeams if multi else 1
+    G = 1 << 15 if multi else 1 << 18
     nblocks = max(3, args.stream_blocks)
     rng = np.random.default_rng(5)
     data = rng.integers(100, 156, size=(nblocks * G + 1000, w.nchans), dtype=np.uint8)
-    out = {"workload": f"sigproc_file_c{w.nchans}_{nblocks}x{G}", "api": "hd_search_sigproc_file"}
+    out = {"workload": f"sigproc_files_{nfiles}x_c{w.nchans}_{nblocks}x{G}",
+           "api": "hd_search_sigproc_files" if multi else "hd_search_sigproc_file"}
     with tempfile.TemporaryDirectory(dir=args.stream_dir) as tmp:
-        path = os.path.join(tmp, "survey.fil")
-        synth.write_sigproc(path, data, nchans=w.nchans, nbits=8, tsamp=w.dt, fch1=w.f0,
-                            foff=w.df, tstart=60000.5, nifs=1, source_name="survey")
-        with open(path, "rb") as f:
-            while f.read(1 << 26):
-                pass
+        paths = []
+        for u in range(nfiles):
+            path = os.path.join(tmp, f"beam{u:02d}.fil")
+            synth.write_sigproc(path, data, nchans=w.nchans, nbits=8, tsamp=w.dt, fch1=w.f0,
+                                foff=w.df, tstart=60000.5, nifs=1, ibeam=u + 1,
+                                source_name="stream")
+            with open(path, "rb") as f:
+                while f.read(1 << 26):
+                    pass
+            paths.append(path)
         kw = dict(dm_min=w.dm_min, dm_max=w.dm_max, boxcar_max=w.boxcar_max, output_dir=None)
-        params = H.params_from_sigproc(path, H.default_params(**kw))
-        with H.Pipeline(params, cleaning=True) as pl:
+        q = H.default_params(**kw)
+        q.override_beam = True
+        params = H.params_from_sigproc(paths[0], q)
+        with H.Pipeline(params, cleaning=not multi) as pl:
             M = pl.max_overlap()
             stamps = []
             fn = H.GULP_CALLBACK(lambda user, cands, n, first: stamps.append(time.perf_counter()))
             tot, ng = C.c_size_t(0), C.c_size_t(0)
+            arr = (C.c_char_p * nfiles)(*[p.encode() for p in paths])
             for rep in range(2):  # the first pass tunes and allocates
                 stamps.clear()
                 t0 = time.perf_counter()
-                err = H.lib().hd_search_sigproc_file(pl._p, path.encode(), G, fn, None,
-                                                     C.byref(tot), C.byref(ng))
+                err = H.lib().hd_search_sigproc_files(pl._p, arr, nfiles, G, fn, None,
+                                                      C.byref(tot), C.byref(ng))
                 t1 = time.perf_counter()
-                assert err == H.HD_NO_ERROR, err
+                assert err in (H.HD_NO_ERROR, H.HD_TOO_MANY_EVENTS), err
             gaps = [1e3 * (b - a) for a, b in zip(stamps, stamps[1:])]
             d = torch.from_numpy(data[:G + M]).cuda()
             torch.cuda.synchronize()
             ts = []
             for _ in range(4):
-                pl.execute_device(d.data_ptr(), G + M)
+                err, _, _ = pl.execute_beams([d.data_ptr()] * nfiles, nsamps=G + M,
+                                             on_device=True, raise_on_error=False)
                 ts.append(pl.timing()["total"])
     steady = float(np.median(gaps))
-    out.update({"gulps": ng.value, "ms_between_gulps": round(steady, 2),
+    out.update({"files": nfiles, "gulps": ng.value, "ms_between_gulps": round(steady, 2),
                 "ms_between_gulps_all": [round(g, 2) for g in gaps],
                 "device_search_ms": round(min(ts[1:]), 2),
                 "startup_ms": round(1e3 * (stamps[0] - t0), 1),
-                "beam_s_per_s_steady": round(G * w.dt / (steady * 1e-3), 1),
-                "beam_s_per_s_whole_call": round(tot.value * w.dt / (t1 - t0), 1)})
+                "beam_s_per_s_steady": round(nfiles * G * w.dt / (steady * 1e-3), 1),
+                "beam_s_per_s_whole_call": round(nfiles * tot.value * w.dt / (t1 - t0), 1)})
     return out
 
 
@@ -810,6 +825,7 @@ def main():
     ap.add_argument("--only-stream-file", action="store_true",
                     help="only the sigproc file gulp loop (writes a temporary file)")
     ap.add_argument("--stream-blocks", type=int, default=7)
+    ap.add_argument("--stream-workload", default="survey", choices=["survey", "multibeam"])
     ap.add_argument("--stream-dir", default=None,
                     help="directory for the temporary file (default: the system's)")
     args = ap.parse_args()

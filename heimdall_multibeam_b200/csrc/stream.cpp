@@ -289,12 +289,23 @@ hd_error search_files(hd_pipeline pl, const char* const* paths, size_t nfiles,
     pos[u] += want;
     return ok ? want / stride : 0;  // a read error ends the loop
   };
-  // the next block of every file into h_blk[hb] (file u at u * block); the
-  // fewest whole spectra any file gave
+  // the next block of every file into h_blk[hb] (file u at u * block), up
+  // to 16 files at a time; the fewest whole spectra any file gave
   auto read_blocks = [&](int hb_) -> size_t {
+    std::vector<size_t> got(nfiles, 0);
+    const size_t nw = std::min<size_t>(16, nfiles);
+    if (nw == 1) {
+      got[0] = read_one(0, h_blk[hb_]);
+    } else {
+      std::vector<std::thread> th;
+      for (size_t i = 0; i < nw; i++)
+        th.emplace_back([&, i]() {
+          for (size_t u = i; u < nfiles; u += nw) got[u] = read_one(u, h_blk[hb_] + u * block);
+        });
+      for (auto& t : th) t.join();
+    }
     size_t least = block / stride;
-    for (size_t u = 0; u < nfiles; u++)
-      least = std::min(least, read_one(u, h_blk[hb_] + u * block));
+    for (size_t u = 0; u < nfiles; u++) least = std::min(least, got[u]);
     return least;
   };
   // heimdall.C:209-265: the next gulp of file u holds, beam by beam, the
