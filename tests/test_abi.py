@@ -6,6 +6,7 @@ import re
 import subprocess
 import tempfile
 
+import numpy as np
 import pytest
 
 import heimdall_multibeam_b200 as hdb
@@ -127,3 +128,37 @@ int main() {
                        check=True)
         assert subprocess.run([exe]).returncode == 0
 
+
+
+def test_c_caller_links_with_documented_line(hdb, tmp_path):
+    """A plain C caller built with the include and link flags given to C
+    callers (-I include, -L ... -lhdb200 with an rpath) links and runs the
+    calls that need no GPU: default parameters, command-line parsing, error
+    strings and the sigproc header reader."""
+    from heimdall_multibeam_b200 import synth
+    fil = str(tmp_path / "h.fil")
+    synth.write_sigproc(fil, np.zeros((50, 64), np.uint8), nchans=64, nbits=8, tsamp=1e-4,
+                        fch1=1400.0, foff=-1.0, tstart=60000.25, nbeams=3, ibeam=2)
+    src = tmp_path / "caller.c"
+    src.write_text(r'''#include <stdio.h>
+#include "heimdall_b200.h"
+int main(int argc, char** argv) {
+  struct hd_params p;
+  hd_set_default_params(&p);
+  char* args[] = {"heimdall", "-dm", "0", "500", "-boxcar_max", "256", "-f", argv[1]};
+  if (hd_parse_command_line(8, args, &p) != 0) return 2;
+  if (p.sigproc_file == NULL) return 3;
+  hd_sigproc_header h;
+  hd_error e = hd_read_sigproc_header(argv[1], &h);
+  printf("%d %g %zu %d %d %d %s\n", (int)e, (double)p.dm_max, (size_t)p.boxcar_max,
+         (int)h.nchans, (int)h.nbeams, (int)h.ibeam, hd_get_error_string(HD_TOO_FEW_NSAMPS));
+  return e == HD_NO_ERROR ? 0 : 1;
+}
+''')
+    libdir = os.path.join(ROOT, "heimdall_multibeam_b200")
+    exe = str(tmp_path / "caller")
+    subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", exe,
+                    "-L" + libdir, "-lhdb200", "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([exe, fil], capture_output=True, text=True, check=True).stdout.split()
+    assert out[:6] == ["0", "500", "256", "64", "3", "2"], out
+    assert " ".join(out[6:]) == hdb.lib().hd_get_error_string(hdb.HD_TOO_FEW_NSAMPS).decode()
