@@ -401,8 +401,8 @@ typedef void (*hd_gulp_callback)(void* user, const hd_candidate* candidates, hd_
  * nsamps_gulp new spectra; a block shorter than nsamps_gulp ends the search
  * and is not searched.  With nbeams > 1 in the header each block holds the
  * beams in sequence.  The overlap stays on the device; the next block is
- * read from the file while the GPU searches.  Candidates go to the
- * pipeline's .cand files and to on_gulp (may be NULL). */
+ * read from the file and copied to the device while the GPU searches.
+ * Candidates go to the pipeline's .cand files and to on_gulp (may be NULL). */
 hd_error hd_search_sigproc_file(hd_pipeline pipeline, const char* path, hd_size nsamps_gulp,
                                 hd_gulp_callback on_gulp, void* user, hd_size* total_nsamps,
                                 hd_size* ngulps);
