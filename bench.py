@@ -66,7 +66,7 @@ def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return json.load(f), "measured"
-    except Exception:
+    except (OSError, ValueError):
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
@@ -89,7 +89,7 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
-        except Exception:
+        except OSError:  # no nvidia-smi: the line says so
             self.proc = None
 
     def _read(self):
@@ -102,7 +102,7 @@ class ClockSampler:
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
-        except Exception:
+        except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -372,8 +372,8 @@ def run_product(args):
                     for ln in f:
                         if ln.startswith(tf[1]):
                             traffic = int(ln.split(":")[1])
-            except Exception:
-                pass
+            except (OSError, ValueError, IndexError):
+                traffic = None  # no committed capture: the line reports traffic null
         hit = nstrong = 0
         for u in range(U):
             h_, n_ = recall(cands[u], wk.pulses[u], w.dt)
