@@ -176,8 +176,9 @@ SYMBOLS = {
     "hd_get_beam_set_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
     "hd_destroy_beam_set": (None, [_P]),
     "hd_get_launch_count": (C.c_ulonglong, []),
+    "hd_measure_int_add_rate": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "hd_clean_filterbank_rfi_noalloc": (C.c_int, [_P, _SZ, _SZ, _SZ, _P, _P, C.c_float,
-                                                  C.c_float, C.c_float, _SZ, _SZ, _P]),
+                                                  C.c_float, C.c_float, _SZ, _SZ, _P, _P]),
     "hd_get_candidates": (C.c_int, [_P, _P, _SZP]),
     "hd_get_giants": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _SZP]),
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
@@ -600,6 +601,16 @@ class Pipeline:
 
 def launch_count() -> int:
     return int(lib().hd_get_launch_count())
+
+
+def int_add_rate(device: int = 0) -> float:
+    """Measured 32-bit integer adds per second of the device
+    (hd_measure_int_add_rate)."""
+    v = C.c_double(0.0)
+    err = lib().hd_measure_int_add_rate(device, C.byref(v))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_measure_int_add_rate")
+    return float(v.value)
 
 
 def cand_lines(c: np.ndarray) -> list:

@@ -798,7 +798,7 @@ struct DBuf {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 256));
+    cudaError_t e = hdb::dev_malloc(&p, std::max<size_t>(bytes, 256));
     if (e == cudaSuccess) cap = std::max<size_t>(bytes, 256);
     return e;
   }

@@ -117,11 +117,11 @@ hd_error hd_coincide(const hd_candidate* cands, hd_size n, hd_size nbeams, unsig
   float* d_max = nullptr;
   cudaStream_t s = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&d_c, n * sizeof(CoincCand));
-  if (e == cudaSuccess) e = cudaMalloc(&d_first, (nbeams + 1) * sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMalloc(&d_nb, n * sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMalloc(&d_prim, n * sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMalloc(&d_max, n * sizeof(float));
+  if (e == cudaSuccess) e = hdb::dev_malloc(&d_c, n * sizeof(CoincCand));
+  if (e == cudaSuccess) e = hdb::dev_malloc(&d_first, (nbeams + 1) * sizeof(unsigned));
+  if (e == cudaSuccess) e = hdb::dev_malloc(&d_nb, n * sizeof(unsigned));
+  if (e == cudaSuccess) e = hdb::dev_malloc(&d_prim, n * sizeof(unsigned));
+  if (e == cudaSuccess) e = hdb::dev_malloc(&d_max, n * sizeof(float));
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_c, h.data(), n * sizeof(CoincCand), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)

@@ -10,6 +10,19 @@ struct hd_pipeline_t;
 
 namespace hdb {
 
+// cudaMalloc that, when it fails, also clears the failure from the runtime's
+// last-error state (an allocation failure is not sticky; left there, it would
+// be reported by the next launch check of an unrelated call).
+template <class T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+  }
+  return e;
+}
+
 // Kernel launches made by this library in this process (additive counter,
 // read through hd_get_launch_count).
 void note_launch();
@@ -44,6 +57,10 @@ struct DedispArgs {
   int units;              // independent filterbanks dedispersed by one launch
   size_t in_unit;         // bytes between units' FT inputs
   size_t out_unit;        // floats between units' outputs
+  unsigned wait_limit;    // polls of each bounded mbarrier wait
+  // test of the error path: the producer issues no copy for the last stage,
+  // so the consumers' wait on it runs out (HDB_TEST_WITHHOLD_STAGE=1)
+  int withhold_last;
 };
 
 // Dedispersion tile: DMs and output samples per CTA, channel rows staged per
@@ -52,9 +69,14 @@ struct DedispTile {
   int dm_block, time_block, rows;
 };
 constexpr int kDedispDmBlocks[3] = {8, 16, 32};
-// candidate {dm_block, time_block} pairs (32 x 512 would spill registers)
-constexpr int kDedispTiles[7][2] = {{8, 256},  {8, 512},  {8, 1024}, {16, 256},
-                                    {16, 512}, {16, 1024}, {32, 256}};
+// polls of a dedispersion mbarrier wait before it gives up and reports
+constexpr unsigned kDedispWaitLimit = 1u << 22;
+// candidate {dm_block, time_block} pairs: time_block = 128 K G with K output
+// words per lane (1, 3 or 5) in G groups; the launcher maps each pair to its
+// kernel instance
+constexpr int kDedispTiles[11][2] = {{8, 1024}, {8, 640},  {8, 768},  {8, 1152},
+                                     {8, 1280}, {16, 512}, {16, 384}, {16, 640},
+                                     {16, 768}, {32, 256}, {32, 384}};
 // rows per stage that fit shared memory for staged rows of rowb bytes (0: none)
 int dedisp_rows_per_stage(int dm_block, int rowb);
 size_t dedisp_smem_bytes(int dm_block, int rows, int rowb);

@@ -349,7 +349,7 @@ __global__ void k_nb_zap(uint32_t* __restrict__ data, size_t nsamps, int units, 
 //
 //   out[d][t] = (float) sum_{c active} in[c][t + delay[d][c]],  t < nout
 //
-// CTA = DB = 2*NW DMs x TB = 128*G samples, NW consumer warps + 1 producer
+// CTA = DB = 2*NW DMs x TB = 128*K*G samples, NW consumer warps + 1 producer
 // warp.  The producer walks the active channels in stages of CH: for each
 // stage it tabulates the byte offset of every (DM, channel) pair in shared
 // memory and issues one 1-D bulk async copy (TMA, cp.async.bulk) per channel
@@ -357,23 +357,38 @@ __global__ void k_nb_zap(uint32_t* __restrict__ data, size_t nsamps, int units, 
 // buffers, signalling a `full` mbarrier; consumer warps release a buffer
 // through an `empty` mbarrier (one arrival per warp).  There is no block-wide
 // barrier in the main loop, so warps drift freely within the ring.
-// Warp w owns DMs 2w and 2w+1; lane l owns samples 4(l + 32g) .. +3.  Each
-// 4-byte window is realigned with a funnel shift and split into two 16-bit
-// lane pairs (even/odd samples); two channels are summed per 3-input add, so
-// one add accumulates four sample-channel terms.  The 16-bit lanes are drained
-// into 32-bit sums after at most 257 channels (255 * 257 = 65535), so the
-// sums are exact.  Every mbarrier wait is bounded; a wait that gives up sets
-// bit 0 of a.err and the warp leaves its loop.
+//
+// Warp w owns DMs 2w and 2w+1.  In each of G groups of 32*K words, lane l
+// owns the K consecutive output words (4K samples) starting at word K*l.  A
+// (DM, channel) term reads the K+1 row words that cover the lane's window
+// shifted by the delay, and realigns each output word with a funnel shift.
+// Because K is odd, the 32 lanes' j-th loads (word K*l + j) fall in 32
+// distinct banks: every shared load is one wavefront, and a term costs
+// 4 (K+1) / (4 K) bytes of shared-memory bandwidth per sample (2 at K = 1,
+// 1.33 at K = 3, 1.2 at K = 5).  Each realigned word is split into two
+// 16-bit lane pairs (even/odd samples); two channels are summed per 3-input
+// add, so one add accumulates four sample-channel terms.  The 16-bit lanes
+// are drained into 32-bit sums after at most 257 channels (255 * 257 =
+// 65535), so the sums are exact.  Every mbarrier wait is bounded; a wait that
+// gives up sets bit 0 of a.err and the warp leaves its loop.
 // ---------------------------------------------------------------------------
-constexpr uint32_t DD_WAIT_LIMIT = 1u << 22;
+// CTAs per SM the register budget allows: per lane about 12 registers per
+// owned output word (two DMs x {2 packed, 4 drained} sums) plus ~48 others.
+constexpr int dd_min_blocks(int nw, int k, int g) {
+  return (65536 / ((nw + 1) * 32 * (12 * k * g + 48))) < 1
+             ? 1
+             : (65536 / ((nw + 1) * 32 * (12 * k * g + 48))) > 3
+                   ? 3
+                   : (65536 / ((nw + 1) * 32 * (12 * k * g + 48)));
+}
 
-template <int NW, int G, int CH, int NST>
-__global__ void __launch_bounds__((NW + 1) * 32,
-                                  (NW >= 8 && G >= 8) ? 1 : (NW >= 16 || G >= 8) ? 2 : 3)
+template <int NW, int K, int G, int CH, int NST>
+__global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
     k_dedisp(DedispArgs a) {
+  static_assert(K % 2 == 1, "odd K keeps the strided shared loads conflict-free");
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr int DB = 2 * NW;
-  constexpr int TB = 128 * G;
+  constexpr int TB = 128 * K * G;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + NST;
   int* s_off = reinterpret_cast<int*>(smem + 128);          // [NST][DB*CH]
@@ -403,11 +418,14 @@ __global__ void __launch_bounds__((NW + 1) * 32,
     for (int st = 0; st < nstage; st++) {
       const int buf = st % NST;
       if (st >= NST) {
-        if (!mbar_wait(&empty[buf], (uint32_t)(((st / NST) - 1) & 1), DD_WAIT_LIMIT)) {
+        if (!mbar_wait(&empty[buf], (uint32_t)(((st / NST) - 1) & 1), a.wait_limit)) {
           if (lane == 0) atomicOr(a.err, 1u);
           break;
         }
       }
+      // error-path test: the last stage is never copied (nor announced), so
+      // its `full` phase never completes and the consumers' wait gives up
+      if (a.withhold_last && st == nstage - 1) break;
       const int k0 = st * CH;
       const int nk = min(CH, a.nact - k0);
       int* off = s_off + buf * DB * CH;
@@ -433,44 +451,47 @@ __global__ void __launch_bounds__((NW + 1) * 32,
     }
     // let every copy this CTA issued land before the warp exits
     for (int st = (issued > NST ? issued - NST : 0); st < issued; st++)
-      mbar_wait(&full[st % NST], (uint32_t)((st / NST) & 1), DD_WAIT_LIMIT);
+      mbar_wait(&full[st % NST], (uint32_t)((st / NST) & 1), a.wait_limit);
     return;
   }
 
   // ---------------- consumers ----------------
-  uint32_t pk[2][G][2];
-  int acc[2][G][4];
-#pragma unroll
-  for (int d = 0; d < 2; d++)
-#pragma unroll
-    for (int g = 0; g < G; g++) {
-      pk[d][g][0] = pk[d][g][1] = 0;
-      acc[d][g][0] = acc[d][g][1] = acc[d][g][2] = acc[d][g][3] = 0;
-    }
   // pk[..][0] sums the raw words (bytes b0..b3 of 4 samples) modulo 2^32 and
   // pk[..][1] the odd bytes (b1, b3) in two 16-bit lanes.  With at most 257
   // channels between drains every byte-lane sum is <= 65535, so
   // raw - (odd << 8) = E0 + 2^16 E2 exactly: the even-byte sums.
+  constexpr int W = K * G;  // output words per lane and DM
+  uint32_t pk[2][W][2];
+  int acc[2][W][4];
+#pragma unroll
+  for (int d = 0; d < 2; d++)
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      pk[d][w][0] = pk[d][w][1] = 0;
+      acc[d][w][0] = acc[d][w][1] = acc[d][w][2] = acc[d][w][3] = 0;
+    }
   auto drain = [&]() {
 #pragma unroll
     for (int d = 0; d < 2; d++)
 #pragma unroll
-      for (int g = 0; g < G; g++) {
-        const uint32_t odd = pk[d][g][1];
-        const uint32_t even = pk[d][g][0] - (odd << 8);
-        acc[d][g][0] += (int)(even & 0xFFFFu);
-        acc[d][g][2] += (int)(even >> 16);
-        acc[d][g][1] += (int)(odd & 0xFFFFu);
-        acc[d][g][3] += (int)(odd >> 16);
-        pk[d][g][0] = pk[d][g][1] = 0;
+      for (int w = 0; w < W; w++) {
+        const uint32_t odd = pk[d][w][1];
+        const uint32_t even = pk[d][w][0] - (odd << 8);
+        acc[d][w][0] += (int)(even & 0xFFFFu);
+        acc[d][w][2] += (int)(even >> 16);
+        acc[d][w][1] += (int)(odd & 0xFFFFu);
+        acc[d][w][3] += (int)(odd >> 16);
+        pk[d][w][0] = pk[d][w][1] = 0;
       }
   };
+  // first word of this lane in group 0; group g adds 32*K*g words
+  const int lw = K * lane;
 
   int nsum = 0;
   bool failed = false;
   for (int st = 0; st < nstage; st++) {
     const int buf = st % NST;
-    if (!mbar_wait(&full[buf], (uint32_t)((st / NST) & 1), DD_WAIT_LIMIT)) {
+    if (!mbar_wait(&full[buf], (uint32_t)((st / NST) & 1), a.wait_limit)) {
       if (lane == 0) atomicOr(a.err, 1u);
       failed = true;
       break;
@@ -488,13 +509,23 @@ __global__ void __launch_bounds__((NW + 1) * 32,
         const int oa = off[d * CH + k];
         const int ob = off[d * CH + k + 1];
         const int sa = (oa & 3) * 8, sb = (ob & 3) * 8;
-        const int wa = (oa >> 2) + lane, wb = (ob >> 2) + lane;
+        const uint32_t* pa = ra + (oa >> 2) + lw;
+        const uint32_t* pb = rb + (ob >> 2) + lw;
 #pragma unroll
         for (int g = 0; g < G; g++) {
-          const uint32_t xa = __funnelshift_r(ra[wa + 32 * g], ra[wa + 32 * g + 1], sa);
-          const uint32_t xb = __funnelshift_r(rb[wb + 32 * g], rb[wb + 32 * g + 1], sb);
-          pk[d][g][0] += xa + xb;
-          pk[d][g][1] += __byte_perm(xa, 0u, 0x4341) + __byte_perm(xb, 0u, 0x4341);
+          uint32_t wa[K + 1], wb[K + 1];
+#pragma unroll
+          for (int j = 0; j <= K; j++) {
+            wa[j] = pa[32 * K * g + j];
+            wb[j] = pb[32 * K * g + j];
+          }
+#pragma unroll
+          for (int j = 0; j < K; j++) {
+            const uint32_t xa = __funnelshift_r(wa[j], wa[j + 1], sa);
+            const uint32_t xb = __funnelshift_r(wb[j], wb[j + 1], sb);
+            pk[d][K * g + j][0] += xa + xb;
+            pk[d][K * g + j][1] += __byte_perm(xa, 0u, 0x4341) + __byte_perm(xb, 0u, 0x4341);
+          }
         }
       }
       nsum += 2;
@@ -506,12 +537,18 @@ __global__ void __launch_bounds__((NW + 1) * 32,
       for (int d = 0; d < 2; d++) {
         const int oa = off[d * CH + k];
         const int sa = (oa & 3) * 8;
-        const int wa = (oa >> 2) + lane;
+        const uint32_t* pa = ra + (oa >> 2) + lw;
 #pragma unroll
         for (int g = 0; g < G; g++) {
-          const uint32_t xa = __funnelshift_r(ra[wa + 32 * g], ra[wa + 32 * g + 1], sa);
-          pk[d][g][0] += xa;
-          pk[d][g][1] += __byte_perm(xa, 0u, 0x4341);
+          uint32_t wa[K + 1];
+#pragma unroll
+          for (int j = 0; j <= K; j++) wa[j] = pa[32 * K * g + j];
+#pragma unroll
+          for (int j = 0; j < K; j++) {
+            const uint32_t xa = __funnelshift_r(wa[j], wa[j + 1], sa);
+            pk[d][K * g + j][0] += xa;
+            pk[d][K * g + j][1] += __byte_perm(xa, 0u, 0x4341);
+          }
         }
       }
       nsum += 1;
@@ -530,18 +567,21 @@ __global__ void __launch_bounds__((NW + 1) * 32,
     if (dd >= a.dm_count) continue;
     float* o = out + (size_t)dd * a.out_pitch;
 #pragma unroll
-    for (int g = 0; g < G; g++) {
-      size_t t = t0 + 4 * (lane + 32 * g);
-      float4 v = make_float4((float)acc[d][g][0], (float)acc[d][g][1], (float)acc[d][g][2],
-                             (float)acc[d][g][3]);
-      if (t + 3 < a.nout) {
-        *reinterpret_cast<float4*>(o + t) = v;
-      } else {
-        if (t < a.nout) o[t] = v.x;
-        if (t + 1 < a.nout) o[t + 1] = v.y;
-        if (t + 2 < a.nout) o[t + 2] = v.z;
+    for (int g = 0; g < G; g++)
+#pragma unroll
+      for (int j = 0; j < K; j++) {
+        const int w = K * g + j;
+        size_t t = t0 + 4 * (32 * K * g + lw + j);
+        float4 v = make_float4((float)acc[d][w][0], (float)acc[d][w][1], (float)acc[d][w][2],
+                               (float)acc[d][w][3]);
+        if (t + 3 < a.nout) {
+          *reinterpret_cast<float4*>(o + t) = v;
+        } else {
+          if (t < a.nout) o[t] = v.x;
+          if (t + 1 < a.nout) o[t + 1] = v.y;
+          if (t + 2 < a.nout) o[t + 2] = v.z;
+        }
       }
-    }
   }
 }
 
@@ -676,25 +716,25 @@ constexpr int DD_NST = 3;
 size_t dd_smem(int dm_block, int ch, int rowb) {
   return 128 + (size_t)DD_NST * dm_block * ch * sizeof(int) + (size_t)DD_NST * ch * rowb;
 }
-template <int NW, int G, int CH>
+template <int NW, int K, int G, int CH>
 cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
-  auto kern = k_dedisp<NW, G, CH, DD_NST>;
+  auto kern = k_dedisp<NW, K, G, CH, DD_NST>;
   const size_t smem = dd_smem(2 * NW, CH, a.rowb);
   cudaError_t e = raise_smem_limit(kern, smem);
   if (e != cudaSuccess) return e;
-  const int DB = 2 * NW, TB = 128 * G;
+  const int DB = 2 * NW, TB = 128 * K * G;
   dim3 grid((unsigned)((a.dm_count + DB - 1) / DB), (unsigned)((a.nout + TB - 1) / TB),
             (unsigned)a.units);
   kern<<<grid, (NW + 1) * 32, smem, s>>>(a); note_launch();
   return cudaGetLastError();
 }
-template <int NW, int G>
+template <int NW, int K, int G>
 cudaError_t launch_rows(const DedispArgs& a, int rows, cudaStream_t s) {
   switch (rows) {
-    case 8: return launch_dd<NW, G, 8>(a, s);
-    case 4: return launch_dd<NW, G, 4>(a, s);
-    case 2: return launch_dd<NW, G, 2>(a, s);
-    case 1: return launch_dd<NW, G, 1>(a, s);
+    case 8: return launch_dd<NW, K, G, 8>(a, s);
+    case 4: return launch_dd<NW, K, G, 4>(a, s);
+    case 2: return launch_dd<NW, K, G, 2>(a, s);
+    case 1: return launch_dd<NW, K, G, 1>(a, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -717,13 +757,22 @@ size_t dedisp_smem_bytes(int dm_block, int rows, int rowb) {
 
 cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t s) {
   if (a.units < 1 || a.units > 65535) return cudaErrorInvalidValue;
-  if (t.dm_block == 8 && t.time_block == 256) return launch_rows<4, 2>(a, t.rows, s);
-  if (t.dm_block == 8 && t.time_block == 512) return launch_rows<4, 4>(a, t.rows, s);
-  if (t.dm_block == 8 && t.time_block == 1024) return launch_rows<4, 8>(a, t.rows, s);
-  if (t.dm_block == 16 && t.time_block == 1024) return launch_rows<8, 8>(a, t.rows, s);
-  if (t.dm_block == 16 && t.time_block == 256) return launch_rows<8, 2>(a, t.rows, s);
-  if (t.dm_block == 16 && t.time_block == 512) return launch_rows<8, 4>(a, t.rows, s);
-  if (t.dm_block == 32 && t.time_block == 256) return launch_rows<16, 2>(a, t.rows, s);
+  // {dm_block, time_block} -> consumer warps NW = dm_block / 2, words per
+  // lane K, groups G with time_block = 128 K G (kDedispTiles)
+#define HDB_DD_TILE(DBk, NWk, Kk, Gk) \
+  if (t.dm_block == DBk && t.time_block == 128 * Kk * Gk) return launch_rows<NWk, Kk, Gk>(a, t.rows, s);
+  HDB_DD_TILE(8, 4, 1, 8)
+  HDB_DD_TILE(8, 4, 5, 1)
+  HDB_DD_TILE(8, 4, 3, 2)
+  HDB_DD_TILE(8, 4, 3, 3)
+  HDB_DD_TILE(8, 4, 5, 2)
+  HDB_DD_TILE(16, 8, 1, 4)
+  HDB_DD_TILE(16, 8, 3, 1)
+  HDB_DD_TILE(16, 8, 5, 1)
+  HDB_DD_TILE(16, 8, 3, 2)
+  HDB_DD_TILE(32, 16, 1, 2)
+  HDB_DD_TILE(32, 16, 3, 1)
+#undef HDB_DD_TILE
   return cudaErrorInvalidValue;
 }
 

@@ -2009,9 +2009,15 @@ cudaError_t merge_groups(const GiantBuffers& gb, int n, int dm_key_gap, const fl
 //   where j in [off, count+1-boxcar_max+off) is flagged when
 //   |boxcar_w(j-off) * (1/sqrt(w))| > tol  (off = boxcar_max/2).
 // ===========================================================================
+// Width norm 1/sqrt(w) of clean_filterbank_rfi.cu:476-477: sqrtf in float,
+// the reciprocal in double, rounded to float (each step correctly rounded, as
+// on the host).
+__device__ __forceinline__ float rfi_width_norm(int w) {
+  return __double2float_rn(__ddiv_rn(1.0, (double)__fsqrt_rn(__int2float_rn(w))));
+}
+
 __global__ void k_rfi_flags(const float* __restrict__ scan, size_t count, int bmax, int nwid,
-                            const float* __restrict__ wnorm, float tol,
-                            unsigned char* __restrict__ flags) {
+                            float tol, unsigned char* __restrict__ flags) {
   size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= count) return;
   const int off = bmax / 2;
@@ -2023,7 +2029,7 @@ __global__ void k_rfi_flags(const float* __restrict__ scan, size_t count, int bm
       int w = 1 << wi;
       int ahead = (w - 1) / 2 + 1, behind = w / 2;
       float v = __fsub_rn(scan[off + ahead + k], scan[off - behind + k]);
-      v = __fmul_rn(v, wnorm[wi]);
+      v = __fmul_rn(v, rfi_width_norm(w));
       if (fabsf(v) > tol) f |= (unsigned char)(1u << wi);
     }
   }
@@ -2052,16 +2058,14 @@ __global__ void k_rfi_mask(const float* __restrict__ x, size_t count, int bmax, 
 cudaError_t rfi_mask(const float* x, const float* scan, size_t count, size_t boxcar_max,
                      float rfi_tol, int* mask, int* fmask, cudaStream_t s) {
   int nwid = 0;
-  float wn[32];
-  for (size_t w = 1; w <= boxcar_max && nwid < 32; w *= 2, nwid++)
-    wn[nwid] = (float)(1.0 / (double)sqrtf((float)w));  // clean_filterbank_rfi.cu:476-477
-  float* dwn = reinterpret_cast<float*>(fmask);
+  for (size_t w = 1; w <= boxcar_max && nwid < 8; w *= 2) nwid++;
+  // one flag bit per width (boxcar_max <= 128 keeps them in a byte)
+  if (boxcar_max > 128) return cudaErrorInvalidValue;
   unsigned char* flags = reinterpret_cast<unsigned char*>(fmask + 32);
-  cudaError_t e = cudaMemcpyAsync(dwn, wn, nwid * sizeof(float), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return e;
   unsigned nb = (unsigned)((count + 255) / 256);
-  k_rfi_flags<<<nb, 256, 0, s>>>(scan, count, (int)boxcar_max, nwid, dwn, rfi_tol, flags); note_launch();
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_rfi_flags<<<nb, 256, 0, s>>>(scan, count, (int)boxcar_max, nwid, rfi_tol, flags); note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   k_rfi_mask<<<nb, 256, 0, s>>>(x, count, (int)boxcar_max, nwid, rfi_tol, flags, mask); note_launch();
   return cudaGetLastError();
 }

@@ -35,8 +35,9 @@ constexpr size_t kBaseFloats = kMaxN + 64;                             // scrunc
 constexpr size_t kBaseBytes = up(kBaseFloats * sizeof(float));
 constexpr size_t kTreeFloats = kMaxN + 8 * kMaxBeams + 1024;           // median-tree ping-pong
 constexpr size_t kTreeBytes = up(kTreeFloats * sizeof(float));
-constexpr size_t kTotal =
-    kSeriesBytes + kScanBytes + kFlagBytes + kRmsBytes + kBaseBytes + 2 * kTreeBytes;
+constexpr size_t kErrBytes = kAlign;                                   // error word
+constexpr size_t kTotal = kSeriesBytes + kScanBytes + kFlagBytes + kRmsBytes + kBaseBytes +
+                          2 * kTreeBytes + kErrBytes;
 static_assert(kTotal <= HD_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the stated size");
 
 // The scratch array.  Host code must not use this name as an address: on the
@@ -48,7 +49,9 @@ std::mutex g_mu;
 unsigned char* g_dev_addr[64] = {};
 
 // Device address of g_scratch on the current device, looked up once per
-// device (the lookup is the only runtime call this set-up makes).
+// device (the lookup is the only runtime call this set-up makes).  The
+// address belongs to the device's primary context: after cudaDeviceReset the
+// cached value is stale, so the entry point is not for use after a reset.
 hd_error scratch_address(unsigned char** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HD_INVALID_DEVICE_INDEX;
@@ -70,7 +73,7 @@ extern "C" hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size
                                                     hd_byte* d_out, int* d_mask, hd_float dt,
                                                     hd_float baseline_length, hd_float rfi_tol,
                                                     hd_size boxcar_max, hd_size nbeams,
-                                                    void* stream) {
+                                                    void* stream, unsigned* d_status) {
   if (!d_in || !d_out || !d_mask) return HD_INVALID_POINTER;
   if (nbits != 8) return HD_INVALID_NBITS;
   if (nchans == 0 || nchans % 4 != 0 || nbeams == 0) return HD_INVALID_STRIDE;
@@ -81,12 +84,27 @@ extern "C" hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size
             (size_t)nsamps, (size_t)nbeams, kMaxN, kMaxBeams);
     return HD_INVALID_STRIDE;
   }
+  // one flag bit per boxcar width in a byte: widths 1..128
+  if (boxcar_max > 128) {
+    fprintf(stderr, "hd_clean_filterbank_rfi_noalloc: boxcar_max %zu exceeds 128\n",
+            (size_t)boxcar_max);
+    return HD_INVALID_STRIDE;
+  }
   const size_t nsmooth = (size_t)(baseline_length / (2 * dt));
   if (nsamps < boxcar_max + 1 || nsmooth / 4 >= nsamps) return HD_TOO_FEW_NSAMPS;
   const size_t stride = nsamps / nbeams;
   const size_t need_base = nbeams * hdb::baseline_samples(stride, nsmooth) + 64;
   const size_t need_tree = hdb::baseline_scratch(stride, nsmooth, nbeams);
-  if (need_base > kBaseFloats || need_tree > kTreeFloats) return HD_INVALID_STRIDE;
+  if (need_base > kBaseFloats || need_tree > kTreeFloats) {
+    // short beams with a long baseline need more median-tree scratch per
+    // spectrum than the fixed array holds
+    fprintf(stderr,
+            "hd_clean_filterbank_rfi_noalloc: %zu beams of %zu spectra with a %zu-spectrum "
+            "baseline need %zu baseline and %zu tree floats; the fixed scratch holds %zu and "
+            "%zu\n",
+            (size_t)nbeams, stride, nsmooth, need_base, need_tree, kBaseFloats, kTreeFloats);
+    return HD_INVALID_STRIDE;
+  }
 
   unsigned char* base = nullptr;
   hd_error he = scratch_address(&base);
@@ -99,21 +117,29 @@ extern "C" hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size
   unsigned char* tree = base + kSeriesBytes + kScanBytes + kFlagBytes + kRmsBytes + kBaseBytes;
   hdb::TreeScratch ws{reinterpret_cast<float*>(tree), reinterpret_cast<float*>(tree + kTreeBytes),
                       kTreeFloats};
+  unsigned* err = reinterpret_cast<unsigned*>(tree + 2 * kTreeBytes);
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t spitch = (nsamps + 64 + 3) & ~(size_t)3;  // multiple of 4 floats
   // The array keeps the previous call's contents; the series (and the zero
-  // the baseline stretch may read after its last sample) must start at zero.
-  if (cudaMemsetAsync(x, 0, spitch * sizeof(float), s) != cudaSuccess) return HD_INTERNAL_GPU_ERROR;
+  // the baseline stretch may read after its last sample) and the error word
+  // must start at zero.
+  if (cudaMemsetAsync(x, 0, spitch * sizeof(float), s) != cudaSuccess ||
+      cudaMemsetAsync(err, 0, sizeof(unsigned), s) != cudaSuccess)
+    return HD_INTERNAL_GPU_ERROR;
   if (hdb::launch_dm0_sum(d_in, nsamps, (int)nchans, x, s) != cudaSuccess)
     return HD_INTERNAL_GPU_ERROR;
   hdb::SeriesBatch sb{x, spitch, 1, nsamps, stride, stride, (int)nbeams};
   if (hdb::remove_baseline(sb, nsmooth, bl, ws, s) != cudaSuccess ||
       hdb::rms_beams(sb, rms, ws, s) != cudaSuccess ||
-      hdb::normalise_scan(sb, rms, scan, spitch, x, s) != cudaSuccess ||
+      hdb::normalise_scan(sb, rms, scan, spitch, x, s, err) != cudaSuccess ||
       hdb::rfi_mask(x, scan, nsamps, boxcar_max, rfi_tol, d_mask, flags, s) != cudaSuccess ||
       hdb::launch_zap(d_in, nsamps, (int)nchans, d_mask, (unsigned)(nsmooth / 4), nullptr, 0,
                       d_out, s) != cudaSuccess)
+    return HD_INTERNAL_GPU_ERROR;
+  // the error word, for a caller that reads it once the stream is done
+  if (d_status &&
+      cudaMemcpyAsync(d_status, err, sizeof(unsigned), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return HD_INTERNAL_GPU_ERROR;
   return HD_NO_ERROR;
 }

@@ -40,7 +40,7 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     size_t b = std::max<size_t>(bytes, 256);
-    cudaError_t e = cudaMalloc(&p, b);
+    cudaError_t e = hdb::dev_malloc(&p, b);
     if (e == cudaSuccess) cap = b;
     return e;
   }
@@ -832,8 +832,14 @@ hd_error hd_clean_filterbank_rfi(hd_pipeline pl, const hd_byte* h_in, hd_size ns
   if (nbits != 8) return HD_INVALID_NBITS;
   const size_t C = pl->params.nchans;
   if (C % 4 != 0 || nbeams == 0) return HD_INVALID_STRIDE;
+  // one flag bit per boxcar width in a byte: widths 1..128
+  if (boxcar_max > 128) return HD_INVALID_STRIDE;
   cudaSetDevice(pl->device);
   cudaStream_t s = pl->stream;
+  // the plan's device error word records a bounded wait that gave up
+  dedisp_error de = hdb::plan_prepare(pl->plan);
+  if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+  HD_TRY(cudaMemsetAsync(pl->plan->d_err, 0, sizeof(unsigned), s));
   HD_TRY(pl->fb_tf.ensure(nsamps * C));
   HD_TRY(pl->fb_tf_clean.ensure(nsamps * C));
   HD_TRY(cudaMemcpyAsync(pl->fb_tf.p, h_in, nsamps * C, cudaMemcpyHostToDevice, s));
@@ -844,7 +850,10 @@ hd_error hd_clean_filterbank_rfi(hd_pipeline pl, const hd_byte* h_in, hd_size ns
   HD_TRY(cudaMemcpyAsync(h_out, pl->fb_tf_clean.p, nsamps * C, cudaMemcpyDeviceToHost, s));
   if (h_mask)
     HD_TRY(cudaMemcpyAsync(h_mask, pl->mask.p, nsamps * sizeof(int), cudaMemcpyDeviceToHost, s));
+  HD_TRY(cudaMemcpyAsync(pl->h_small + 24, pl->plan->d_err, sizeof(unsigned),
+                         cudaMemcpyDeviceToHost, s));
   HD_TRY(cudaStreamSynchronize(s));
+  if (pl->h_small[24]) return HD_INTERNAL_GPU_ERROR;
   return HD_NO_ERROR;
 }
 

@@ -106,14 +106,14 @@ dedisp_error plan_prepare(dedisp_plan p) {
     free_dev(b);
     b = nullptr;
   }
-  if (cudaMalloc(&p->d_delays, p->delays.size() * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&p->d_active, (p->active.size() + 1) * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&p->d_dm_list, D * sizeof(float)) != cudaSuccess)
+  if (hdb::dev_malloc(&p->d_delays, p->delays.size() * sizeof(int)) != cudaSuccess ||
+      hdb::dev_malloc(&p->d_active, (p->active.size() + 1) * sizeof(int)) != cudaSuccess ||
+      hdb::dev_malloc(&p->d_dm_list, D * sizeof(float)) != cudaSuccess)
     return DEDISP_MEM_ALLOC_FAILED;
   for (int k = 0; k < 3; k++)
-    if (cudaMalloc(&p->d_blk_min[k], p->blk_min[k].size() * sizeof(int)) != cudaSuccess)
+    if (hdb::dev_malloc(&p->d_blk_min[k], p->blk_min[k].size() * sizeof(int)) != cudaSuccess)
       return DEDISP_MEM_ALLOC_FAILED;
-  if (!p->d_err && cudaMalloc(&p->d_err, sizeof(unsigned)) != cudaSuccess)
+  if (!p->d_err && hdb::dev_malloc(&p->d_err, sizeof(unsigned)) != cudaSuccess)
     return DEDISP_MEM_ALLOC_FAILED;
   cudaMemset(p->d_err, 0, sizeof(unsigned));
   if (cudaMemcpy(p->d_delays, p->delays.data(), p->delays.size() * sizeof(int),
@@ -191,6 +191,15 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   a.units = (int)units;
   a.in_unit = in_unit;
   a.out_unit = out_unit;
+  a.wait_limit = kDedispWaitLimit;
+  a.withhold_last = 0;
+  // error-path test (read per call so a test can clear it between gulps):
+  // the last channel stage is withheld and the waits give up quickly
+  if (const char* e = std::getenv("HDB_TEST_WITHHOLD_STAGE"))
+    if (e[0] == '1') {
+      a.withhold_last = 1;
+      a.wait_limit = 1u << 12;
+    }
   if (units > 65535) return DEDISP_INVALID_STRIDE;
   auto with_tile = [&](const std::array<int, 3>& t) {
     a.blk_min = p->d_blk_min[dm_block_index(t[0])];
@@ -410,7 +419,7 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
     if (p->d_in_tf_cap < need) {
       hdb::free_dev(p->d_in_tf);
       p->d_in_tf = nullptr;
-      if (cudaMalloc(&p->d_in_tf, need) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
+      if (hdb::dev_malloc(&p->d_in_tf, need) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
       p->d_in_tf_cap = need;
     }
     if (cudaMemcpyAsync(p->d_in_tf, in, need, cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -421,7 +430,7 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
   if (p->d_in_ft_cap < need_ft) {
     hdb::free_dev(p->d_in_ft);
     p->d_in_ft = nullptr;
-    if (cudaMalloc(&p->d_in_ft, need_ft) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
+    if (hdb::dev_malloc(&p->d_in_ft, need_ft) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
     cudaMemsetAsync(p->d_in_ft, 0, need_ft, s);
     p->d_in_ft_cap = need_ft;
   }
@@ -437,7 +446,7 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
     if (p->d_out_cap < need) {
       hdb::free_dev(p->d_out);
       p->d_out = nullptr;
-      if (cudaMalloc(&p->d_out, need * sizeof(float)) != cudaSuccess)
+      if (hdb::dev_malloc(&p->d_out, need * sizeof(float)) != cudaSuccess)
         return DEDISP_MEM_ALLOC_FAILED;
       p->d_out_cap = need;
     }

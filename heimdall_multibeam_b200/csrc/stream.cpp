@@ -247,8 +247,8 @@ hd_error search_files(hd_pipeline pl, const char* const* paths, size_t nfiles,
     if (cs) cudaStreamDestroy(cs);
     for (FILE* f : fs) std::fclose(f);
   };
-  if (cudaMalloc(&d_buf[0], nfiles * cap) != cudaSuccess ||
-      cudaMalloc(&d_buf[1], nfiles * cap) != cudaSuccess ||
+  if (hdb::dev_malloc(&d_buf[0], nfiles * cap) != cudaSuccess ||
+      hdb::dev_malloc(&d_buf[1], nfiles * cap) != cudaSuccess ||
       cudaMallocHost(&h_blk[0], nfiles * block) != cudaSuccess ||
       cudaMallocHost(&h_blk[1], nfiles * block) != cudaSuccess ||
       cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {

@@ -22,7 +22,8 @@
  * a .cand file or a socket): hd_set_cleaning, hd_set_narrow_band,
  * hd_execute_device, hd_execute_beams, hd_get_candidates,
  * hd_get_beam_candidates, hd_get_raw_candidates, hd_get_giants, hd_get_timing,
- * hd_get_dedisp_tile, hd_get_launch_count, hd_clean_filterbank_rfi_noalloc;
+ * hd_get_dedisp_tile, hd_get_launch_count, hd_measure_int_add_rate,
+ * hd_clean_filterbank_rfi_noalloc;
  * beam sets (hd_*_beam_set*); sigproc input and the gulp loop
  * (hd_read_sigproc_header, hd_mjd_to_utc, hd_params_from_sigproc,
  * hd_search_sigproc_file, hd_search_sigproc_files); the coincidencer (hd_coincide,
@@ -234,12 +235,20 @@ hd_error hd_execute_beams(hd_pipeline pipeline, const hd_byte* const* filterbank
  * GPU where its device code is loaded, until the process exits.  It performs
  * no cudaMalloc, cudaFree or other allocating call.
  *
- * Limits: nsamps <= HD_NOALLOC_MAX_NSAMPS and nbeams <= HD_NOALLOC_MAX_BEAMS;
- * larger requests return HD_INVALID_STRIDE (with a message on stderr).
- * The first call on each device looks up the scratch array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the one array: calls whose work overlaps on the GPU (e.g. on
- * two streams at once) race and must be serialised by the caller. */
+ * Limits: nsamps <= HD_NOALLOC_MAX_NSAMPS, nbeams <= HD_NOALLOC_MAX_BEAMS,
+ * boxcar_max <= 128, and beams long enough for the baseline's median trees to
+ * fit the array; other requests return HD_INVALID_STRIDE (with a message on
+ * stderr).  The first call on each device looks up the scratch array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture; the address is kept for the life of the process, so the call is not
+ * for use after cudaDeviceReset.  All calls share the one array: calls whose
+ * work overlaps on the GPU (e.g. on two streams at once) race and must be
+ * serialised by the caller.
+ *
+ * d_status (a caller-owned device word, may be NULL) receives 0, or a nonzero
+ * value if a bounded wait inside the cleaning kernels gave up (the mask and
+ * the cleaned bytes are then not valid); it is written on `stream`, so read
+ * it after the stream has finished the call's work. */
 #define HD_NOALLOC_MAX_NSAMPS    524288u
 #define HD_NOALLOC_MAX_BEAMS     64u
 #define HD_NOALLOC_SCRATCH_BYTES 11534336u
@@ -247,7 +256,7 @@ hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size nsamps, hd
                                          hd_size nbits, hd_byte* d_out, int* d_mask,
                                          hd_float dt, hd_float baseline_length,
                                          hd_float rfi_tol, hd_size boxcar_max, hd_size nbeams,
-                                         void* stream);
+                                         void* stream, unsigned* d_status);
 
 /* ---- Learned candidate classifier (no counterpart in the reference) ----
  *
@@ -328,6 +337,12 @@ hd_error hd_get_dedisp_tile(hd_pipeline pipeline, int* dm_block, int* time_block
 
 /* Number of kernels this library has launched in this process. */
 unsigned long long hd_get_launch_count(void);
+
+/* Measured throughput of 32-bit integer adds on `device` (adds per second):
+ * independent add chains on every SM, timed with CUDA events (best of three
+ * launches after one warm-up).  The denominator of the integer-add roofline
+ * of the dedispersion kernel.  No reference counterpart. */
+hd_error hd_measure_int_add_rate(int device, double* adds_per_second);
 
 /* One row of the .cand file (Pipeline/pipeline.cu:1028-1038). */
 typedef struct hd_candidate {

@@ -49,6 +49,8 @@ class OrParams(C.Structure):
         ("num_channel_zaps", C.c_uint),
         ("channel_zaps", _szp),
         ("nthreads", C.c_int),
+        ("use_scrunching", C.c_int),
+        ("scrunch_tol", C.c_float),
     ]
 
 
@@ -62,7 +64,7 @@ class OrResult(C.Structure):
     _fields_ = [("error", C.c_int), ("nsamps_processed", C.c_size_t),
                 ("dm_count", C.c_size_t), ("max_delay", C.c_size_t),
                 ("giants", OrGiants), ("labels", _szp), ("label_count", C.c_size_t),
-                ("groups", OrGiants), ("group_dms", _fp)]
+                ("groups", OrGiants), ("group_dms", _fp), ("scrunch", _szp)]
 
 
 DEFAULTS = dict(  # Pipeline/default_params.C:10-66
@@ -70,7 +72,7 @@ DEFAULTS = dict(  # Pipeline/default_params.C:10-66
     dm_tol=1.25, dm_pulse_width=40.0, baseline_length=2.0, rfi_tol=5.0, boxcar_max=4096,
     detect_thresh=6.0, cand_sep_time=3, cand_sep_filter=3, cand_sep_dm=200,
     max_giant_rate=0.0, min_tscrunch_width=4096, clean=0, channel_zaps=(), nthreads=0,
-    beam=0)
+    beam=0, use_scrunching=0, scrunch_tol=1.15)
 
 _lib = None
 _ref = {}
@@ -98,6 +100,11 @@ def lib():
         L.or_max_delay.argtypes = [_fp, C.c_size_t, _fp, C.c_size_t]
         L.or_dedisperse.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t,
                                     C.c_void_p, _fp, C.c_size_t, _fp, _fp, C.c_size_t, C.c_int]
+        L.or_dedisperse_scrunched.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                              C.c_void_p, _fp, C.c_size_t, _fp, _szp, _fp,
+                                              C.c_size_t, C.c_int]
+        L.or_scrunch_factors.argtypes = [_fp, C.c_size_t, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_size_t, C.c_double, _szp]
         for n in ("or_median3", "or_median4", "or_median5"):
             getattr(L, n).restype = C.c_float
         L.or_median3.argtypes = [C.c_float] * 3
@@ -143,6 +150,12 @@ def lib():
     return _lib
 
 
+def reference_dir() -> str:
+    """Where the reference tree lies: HEIMDALL_REFERENCE, else the location
+    the build recipe (oracle/Makefile REF) reads by default."""
+    return os.environ.get("HEIMDALL_REFERENCE", "/root/reference")
+
+
 def ref_available() -> bool:
     return os.path.exists(REF_PATH) and os.path.exists(REF_NOCLEAN_PATH)
 
@@ -164,6 +177,8 @@ def ref_lib(clean: bool = True):
         R.ref_narrow_band.restype = C.c_int
         R.ref_narrow_band.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_float, C.c_float,
                                       C.c_float]
+        R.dedisp_cpu_set_threads.restype = None
+        R.dedisp_cpu_set_threads.argtypes = [C.c_int]
         _ref[path] = R
     return _ref[path]
 
@@ -206,6 +221,35 @@ def delays(dms: np.ndarray, table: np.ndarray) -> np.ndarray:
     """delay(d, c) = (size_t)(dm * table[c] + 0.5f), float arithmetic."""
     v = np.float32(dms)[:, None] * np.float32(table)[None, :] + np.float32(0.5)
     return np.where(v > 0, v, 0).astype(np.uint64)
+
+
+def scrunch_factors(dms, dt, ti, f0, df, nchans, tol) -> np.ndarray:
+    """Per-trial scrunch factors of adaptive dt (or_scrunch_factors)."""
+    dms = np.ascontiguousarray(dms, np.float32)
+    out = np.zeros(len(dms), np.uint64)
+    lib().or_scrunch_factors(_fptr(dms), len(dms), dt, ti, f0, df, nchans, tol,
+                             out.ctypes.data_as(_szp))
+    return out
+
+
+def dedisperse_scrunched(fb: np.ndarray, dms: np.ndarray, table: np.ndarray,
+                         scrunch: np.ndarray, killmask: Optional[np.ndarray] = None,
+                         nthreads: int = 0) -> List[np.ndarray]:
+    """Dedispersion with per-trial scrunch factors: row d holds
+    (nsamps - max_delay) // scrunch[d] samples."""
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    dms = np.ascontiguousarray(dms, np.float32)
+    table = np.ascontiguousarray(table, np.float32)
+    sc = np.ascontiguousarray(scrunch, np.uint64)
+    km = np.ones(nchans, np.int32) if killmask is None else np.ascontiguousarray(killmask, np.int32)
+    md = lib().or_max_delay(_fptr(dms), len(dms), _fptr(table), nchans)
+    nout = nsamps - md
+    out = np.zeros((len(dms), nout), np.float32)
+    lib().or_dedisperse_scrunched(fb.ctypes.data, nsamps, nchans, nchans, km.ctypes.data,
+                                  _fptr(dms), len(dms), _fptr(table), sc.ctypes.data_as(_szp),
+                                  _fptr(out), nout, nthreads)
+    return [out[d, : nout // int(sc[d])].copy() for d in range(len(dms))]
 
 
 def dedisperse(fb: np.ndarray, dms: np.ndarray, table: np.ndarray,
@@ -274,6 +318,9 @@ def execute(fb: np.ndarray, nbeams: int = 1, first_idx: int = 0, **kw) -> dict:
     grp["dms"] = (np.ctypeslib.as_array(res.group_dms, shape=(L,)).astype(np.float32).copy()
                   if L else np.zeros(0, np.float32))
     out["groups"] = grp
+    D = res.dm_count
+    out["scrunch"] = (np.ctypeslib.as_array(res.scrunch, shape=(D,)).astype(np.uint64).copy()
+                      if res.scrunch and D else np.ones(D, np.uint64))
     lib().or_result_free(C.byref(res))
     return out
 
@@ -302,6 +349,13 @@ def cand_lines(groups: dict, nsamps: int, nbeams: int, first_idx: int,
             first_idx + int(groups["begins"][i]) % int(nsamps_beam),
             first_idx + int(groups["ends"][i]) % int(nsamps_beam), beam + beam_idx + 1))
     return lines
+
+
+def ref_set_dedisp_threads(n: int) -> None:
+    """Threads of the CPU dedisperser the reference pipeline links
+    (0: every host core), for both reference builds."""
+    for clean in (True, False):
+        ref_lib(clean).dedisp_cpu_set_threads(int(n))
 
 
 def ref_execute(fb: np.ndarray, nbeams: int = 1, first_idx: int = 0, nthreads: int = 1,

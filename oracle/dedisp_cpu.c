@@ -8,6 +8,7 @@
  * one (config/dedisp.m4).  The product implements the same interface in
  * heimdall_multibeam_b200/csrc with sm_100a kernels.
  */
+#include <omp.h>
 #include "dedisp.h"
 #include "oracle.h"
 
@@ -23,6 +24,7 @@ struct dedisp_plan_struct {
   int*         killmask;
   dedisp_size* dt_factors;
   int          adaptive;
+  double       adaptive_width, adaptive_tol;
 };
 
 dedisp_error dedisp_create_plan(dedisp_plan* plan, dedisp_size nchans, dedisp_float dt,
@@ -51,6 +53,9 @@ static void set_list(dedisp_plan p, const float* l, dedisp_size n) {
   p->dm_count = n;
   p->dt_factors = (dedisp_size*)malloc((n + 1) * sizeof(dedisp_size));
   for (dedisp_size i = 0; i < n; i++) p->dt_factors[i] = 1;
+  if (p->adaptive)
+    or_scrunch_factors(p->dm_list, n, p->dt, p->adaptive_width, p->f0, p->df, p->nchans,
+                       p->adaptive_tol, (size_t*)p->dt_factors);
 }
 
 dedisp_error dedisp_set_dm_list(dedisp_plan p, const dedisp_float* l, dedisp_size n) {
@@ -89,15 +94,23 @@ dedisp_error dedisp_set_killmask(dedisp_plan p, const dedisp_bool* km) {
   return DEDISP_NO_ERROR;
 }
 
-/* Adaptive dt is not restated: the reference pipeline is compared with
- * use_scrunching = 0, and a request for it reports an error. */
+/* Adaptive dt: the per-trial scrunch factors of the oracle's restated rule
+ * (or_scrunch_factors), recomputed whenever the DM list changes; execution
+ * then dedisperses each trial at its factor (or_dedisperse_scrunched). */
 dedisp_error dedisp_enable_adaptive_dt(dedisp_plan p, dedisp_float w, dedisp_float tol) {
-  (void)p; (void)w; (void)tol;
-  return DEDISP_INVALID_FLAG_COMBINATION;
+  if (!p) return DEDISP_INVALID_PLAN;
+  p->adaptive = 1;
+  p->adaptive_width = w;
+  p->adaptive_tol = tol;
+  if (p->dm_count)
+    or_scrunch_factors(p->dm_list, p->dm_count, p->dt, w, p->f0, p->df, p->nchans, tol,
+                       (size_t*)p->dt_factors);
+  return DEDISP_NO_ERROR;
 }
 dedisp_error dedisp_disable_adaptive_dt(dedisp_plan p) {
   if (!p) return DEDISP_INVALID_PLAN;
   p->adaptive = 0;
+  for (dedisp_size i = 0; i < p->dm_count; i++) p->dt_factors[i] = 1;
   return DEDISP_NO_ERROR;
 }
 
@@ -115,6 +128,11 @@ dedisp_float dedisp_get_dt(const dedisp_plan p) { return p->dt; }
 dedisp_float dedisp_get_f0(const dedisp_plan p) { return p->f0; }
 dedisp_float dedisp_get_df(const dedisp_plan p) { return p->df; }
 
+/* Threads of the brute-force dedisperser (0: every host core).  A caller that
+ * runs several pipelines in parallel processes gives each its share. */
+static int g_dedisp_threads = 0;
+void dedisp_cpu_set_threads(int n) { g_dedisp_threads = n; }
+
 dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const dedisp_byte* in,
                                 dedisp_size in_nbits, dedisp_size in_stride, dedisp_byte* out,
                                 dedisp_size out_nbits, dedisp_size out_stride, unsigned flags) {
@@ -127,8 +145,14 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
   if (out_stride % 4) return DEDISP_INVALID_STRIDE;
   size_t md = dedisp_get_max_delay(p);
   if (nsamps < md) return DEDISP_TOO_FEW_NSAMPS;
-  or_dedisperse(in, nsamps, in_stride, p->nchans, p->killmask, p->dm_list, p->dm_count,
-                p->table, (float*)out, out_stride / 4, 0);
+  /* every host core unless dedisp_cpu_set_threads() says otherwise, whatever
+   * thread count the caller set for the stage code: the integer sums do not
+   * depend on it */
+  or_dedisperse_scrunched(in, nsamps, in_stride, p->nchans, p->killmask, p->dm_list,
+                          p->dm_count, p->table,
+                          p->adaptive ? (const size_t*)p->dt_factors : NULL, (float*)out,
+                          out_stride / 4,
+                          g_dedisp_threads > 0 ? g_dedisp_threads : omp_get_num_procs());
   return DEDISP_NO_ERROR;
 }
 

@@ -124,18 +124,68 @@ size_t or_max_delay(const float* dm_list, size_t dm_count, const float* table,
   return m;
 }
 
+/* Adaptive time resolution (dedisp_enable_adaptive_dt, pipeline.cu:187-196;
+ * the external dedisp library is not in the tree, so this is a restatement of
+ * the published method, Barsdell et al. 2012, MNRAS 422, 379: a trial is
+ * searched at a coarser sampling time while the coarsening adds little to its
+ * total smearing).  Choices made here: the smearing of trial DM at sampling
+ * time T is the generator's model above, W(DM, T)^2 = T^2 + ti^2 + (a DM)^2
+ * (microseconds, the same a and band centre); factors start at 1 for the
+ * first trial and never decrease; trial d takes twice the previous factor s
+ * when W(DM_d, 2 s dt) / W(DM_d, s dt) < tol, else keeps s; double
+ * precision throughout. */
+void or_scrunch_factors(const float* dm_list, size_t dm_count, double dt, double ti,
+                        double f0, double df, size_t nchans, double tol, size_t* out) {
+  double dt_us = dt * 1e6;
+  double f = (f0 + ((double)(nchans / 2) - 0.5) * df) * 1e-3;
+  double a = 8.3 * df / (f * f * f);
+  size_t s = 1;
+  for (size_t d = 0; d < dm_count; d++) {
+    if (d > 0) {
+      double sm = a * (double)dm_list[d];
+      double t1 = (double)s * dt_us, t2 = 2.0 * (double)s * dt_us;
+      double w1 = sqrt(t1 * t1 + ti * ti + sm * sm);
+      double w2 = sqrt(t2 * t2 + ti * ti + sm * sm);
+      if (w2 / w1 < tol) s *= 2;
+    }
+    out[d] = s;
+  }
+}
+
 /* out[d][t] = (float) sum_c killmask[c] * in[t + delay(d,c)][c] for
- * t < nsamps - max_delay; exact integer sums (8-bit input). */
-void or_dedisperse(const uint8_t* in, size_t nsamps, size_t in_stride,
-                   size_t nchans, const int* killmask, const float* dm_list,
-                   size_t dm_count, const float* table, float* out,
-                   size_t out_stride, int nthreads) {
+ * t < nsamps - max_delay; exact integer sums (8-bit input).
+ * With scrunch factors (NULL: all 1), trial d with factor s is computed at
+ * sampling time s dt from the scrunched input
+ *   in_s[c][u] = (sum_{j<s} in[s u + j][c] + s/2) / s   (a byte: the mean,
+ *                                                        rounded half up)
+ * as out[d][u] = sum_c killmask[c] * in_s[c][u + delay(d,c) / s] for
+ * u < (nsamps - max_delay) / s (integer divisions; every index stays below
+ * nsamps / s). */
+void or_dedisperse_scrunched(const uint8_t* in, size_t nsamps, size_t in_stride,
+                             size_t nchans, const int* killmask, const float* dm_list,
+                             size_t dm_count, const float* table, const size_t* scrunch,
+                             float* out, size_t out_stride, int nthreads) {
   size_t max_delay = or_max_delay(dm_list, dm_count, table, nchans);
   size_t nout = nsamps - max_delay;
-  /* channel-major copy so the inner loop runs along time */
-  uint8_t* ft = (uint8_t*)malloc(nchans * nsamps + 1);
-  for (size_t t = 0; t < nsamps; t++)
-    for (size_t c = 0; c < nchans; c++) ft[c * nsamps + t] = in[t * in_stride + c];
+  /* channel-major copies (one per scrunch factor) so the inner loop runs
+   * along time */
+  uint8_t* ft[32] = {0};
+  size_t flen[32] = {0};
+  for (size_t d = 0; d < dm_count; d++) {
+    size_t s = scrunch ? scrunch[d] : 1;
+    int k = 0;
+    while (((size_t)1 << k) < s) k++;
+    if (k >= 32 || ft[k]) continue;
+    size_t ns = nsamps / s;
+    flen[k] = ns;
+    ft[k] = (uint8_t*)malloc(nchans * ns + 1);
+    for (size_t u = 0; u < ns; u++)
+      for (size_t c = 0; c < nchans; c++) {
+        unsigned sum = 0;
+        for (size_t j = 0; j < s; j++) sum += in[(s * u + j) * in_stride + c];
+        ft[k][c * ns + u] = (uint8_t)((sum + (unsigned)(s / 2)) / (unsigned)s);
+      }
+  }
   const size_t TB = 4096;
   size_t ntb = (nout + TB - 1) / TB;
 #ifdef _OPENMP
@@ -144,17 +194,30 @@ void or_dedisperse(const uint8_t* in, size_t nsamps, size_t in_stride,
 #endif
   for (long long job = 0; job < (long long)(dm_count * ntb); job++) {
     size_t d = (size_t)job / ntb, tb = (size_t)job % ntb;
-    size_t t0 = tb * TB, t1 = t0 + TB < nout ? t0 + TB : nout;
+    size_t s = scrunch ? scrunch[d] : 1;
+    int k = 0;
+    while (((size_t)1 << k) < s) k++;
+    size_t nout_s = nout / s, ns = flen[k];
+    size_t t0 = tb * TB, t1 = t0 + TB < nout_s ? t0 + TB : nout_s;
+    if (t0 >= t1) continue;
     int32_t acc[4096];
     memset(acc, 0, sizeof(acc));
     for (size_t c = 0; c < nchans; c++) {
       if (!killmask[c]) continue;
-      const uint8_t* row = ft + c * nsamps + or_delay(dm_list[d], table[c]);
+      const uint8_t* row = ft[k] + c * ns + or_delay(dm_list[d], table[c]) / s;
       for (size_t t = t0; t < t1; t++) acc[t - t0] += row[t];
     }
     for (size_t t = t0; t < t1; t++) out[d * out_stride + t] = (float)acc[t - t0];
   }
-  free(ft);
+  for (int k = 0; k < 32; k++) free(ft[k]);
+}
+
+void or_dedisperse(const uint8_t* in, size_t nsamps, size_t in_stride,
+                   size_t nchans, const int* killmask, const float* dm_list,
+                   size_t dm_count, const float* table, float* out,
+                   size_t out_stride, int nthreads) {
+  or_dedisperse_scrunched(in, nsamps, in_stride, nchans, killmask, dm_list, dm_count, table,
+                          NULL, out, out_stride, nthreads);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -834,13 +897,30 @@ int or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t n
 
   size_t ostr = nc + 1;
   float* dd = (float*)malloc(D * ostr * sizeof(float));
-  or_dedisperse(in, nsamps, C, C, km, dml, D, table, dd, ostr, p->nthreads);
+  /* per-trial scrunch factors (pipeline.cu:187-196,344-345), all 1 without
+   * adaptive dt */
+  size_t* scr_list = (size_t*)malloc(D * sizeof(size_t));
+  if (p->use_scrunching)
+    or_scrunch_factors(dml, D, p->dt, p->dm_pulse_width, p->f0, p->df, C, p->scrunch_tol,
+                       scr_list);
+  else
+    for (size_t d = 0; d < D; d++) scr_list[d] = 1;
+  res->scrunch = scr_list;
+  or_dedisperse_scrunched(in, nsamps, C, C, km, dml, D, table, scr_list, dd, ostr,
+                          p->nthreads);
 
-  size_t beam_stride = nsamps / nbeams;
   size_t Bmax = p->boxcar_max;
   size_t nwidths = or_log2(Bmax) + 1;
   or_dm_out* per = (or_dm_out*)calloc(D, sizeof(or_dm_out));
-  int stop_all = (max_delay >= beam_stride) || (max_delay + Bmax > beam_stride);
+  /* the DM loop's break conditions (pipeline.cu:497-502,632-637), per trial;
+   * the first trial that trips one ends the search */
+  for (size_t d = 0; d < D; d++) {
+    size_t scr = scr_list[d];
+    size_t cur_delay = max_delay / scr;
+    size_t cur_bs = nsamps / nbeams / scr;
+    per[d].stopped = (cur_delay >= cur_bs) || (cur_delay + Bmax / scr > cur_bs);
+  }
+  int stop_all = per[0].stopped;
   if (!stop_all) {
 #ifdef _OPENMP
     int nt = p->nthreads > 0 ? p->nthreads : omp_get_max_threads();
@@ -848,7 +928,8 @@ int or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t n
 #endif
     for (long long dl = 0; dl < (long long)D; dl++) {
       size_t d = (size_t)dl;
-      size_t scr = 1, cur_nsamps = nc;
+      if (per[d].stopped) continue;
+      size_t scr = scr_list[d], cur_nsamps = nc / scr;
       float cur_dt = p->dt * (float)scr;
       size_t cur_delay = max_delay / scr;
       size_t cur_bs = nsamps / nbeams / scr;
@@ -905,6 +986,7 @@ int or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t n
   int too_many = 0;
   float mins = (float)((double)((float)nsamps * p->dt) / 60.0);
   for (size_t d = 0; d < D && !stop_all && !too_many; d++) {
+    if (per[d].stopped) break;
     for (int w = 0; w < per[d].nw && !too_many; w++) {
       or_giants* G = &per[d].g[w];
       or_giants_reserve(all, all->count + G->count + 1);
@@ -945,5 +1027,6 @@ void or_result_free(or_result* res) {
   or_giants_free(&res->groups);
   free(res->labels);
   free(res->group_dms);
+  free(res->scrunch);
   memset(res, 0, sizeof(*res));
 }

@@ -42,6 +42,14 @@ void   or_dedisperse(const uint8_t* in, size_t nsamps, size_t in_stride,
                      size_t nchans, const int* killmask, const float* dm_list,
                      size_t dm_count, const float* table, float* out,
                      size_t out_stride, int nthreads);
+/* Per-trial scrunch factors of adaptive dt, and dedispersion with them
+ * (oracle.c documents the restated rule and the scrunched input). */
+void   or_scrunch_factors(const float* dm_list, size_t dm_count, double dt, double ti,
+                          double f0, double df, size_t nchans, double tol, size_t* out);
+void   or_dedisperse_scrunched(const uint8_t* in, size_t nsamps, size_t in_stride,
+                               size_t nchans, const int* killmask, const float* dm_list,
+                               size_t dm_count, const float* table, const size_t* scrunch,
+                               float* out, size_t out_stride, int nthreads);
 
 /* ---- stage restatements -------------------------------------------------- */
 void  or_linear_stretch(const float* in, size_t in_count, float* out, size_t out_count);
@@ -117,6 +125,8 @@ typedef struct {
   unsigned num_channel_zaps;
   const size_t* channel_zaps;  /* 2*num_channel_zaps: [start, end) pairs */
   int    nthreads;
+  int    use_scrunching;     /* adaptive dt (pipeline.cu:187-196) */
+  float  scrunch_tol;
 } or_params;
 
 typedef struct {
@@ -129,6 +139,7 @@ typedef struct {
   size_t  label_count;
   or_giants groups;            /* merged candidates, label order */
   float*  group_dms;
+  size_t* scrunch;             /* dm_count scrunch factors */
 } or_result;
 
 int  or_hd_execute(const or_params* p, const uint8_t* fb, size_t nsamps, size_t nbits,

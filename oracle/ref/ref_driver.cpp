@@ -33,7 +33,8 @@ static int run(const or_params* p, const unsigned char* fb, size_t nsamps, size_
   hp.cand_sep_dm = p->cand_sep_dm;
   hp.max_giant_rate = p->max_giant_rate;
   hp.min_tscrunch_width = p->min_tscrunch_width;
-  hp.use_scrunching = false;
+  hp.use_scrunching = p->use_scrunching != 0;
+  hp.scrunch_tol = p->scrunch_tol;
   hp.output_dir = output_dir;
   hp.utc_start = 0;
   hp.spectra_per_second = (hd_size)(1.0 / p->dt + 0.5);

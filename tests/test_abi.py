@@ -162,3 +162,58 @@ int main(int argc, char** argv) {
     out = subprocess.run([exe, fil], capture_output=True, text=True, check=True).stdout.split()
     assert out[:6] == ["0", "500", "256", "64", "3", "2"], out
     assert " ".join(out[6:]) == hdb.lib().hd_get_error_string(hdb.HD_TOO_FEW_NSAMPS).decode()
+
+
+def _layout_probe(tmp, include_line, defines, extra_inc):
+    """sizeof(hd_params) and every field's offset/size, as a C++ compiler
+    lays out the struct that `include_line` declares."""
+    import oracle
+    names = [f for f, _ in hdb.HdParams._fields_]
+    if "HAVE_PSRDADA" in defines:
+        names = names[:1] + ["dada_id"] + names[1:]
+    body = "\n".join(
+        f'  printf("{n} %zu %zu\\n", offsetof(hd_params, {n}), sizeof(((hd_params*)0)->{n}));'
+        for n in names)
+    src = os.path.join(tmp, "probe.cpp")
+    with open(src, "w") as f:
+        f.write(f"""#include <cstdio>
+#include <cstddef>
+{include_line}
+int main() {{
+  printf("size %zu\\n", sizeof(hd_params));
+{body}
+  return 0;
+}}
+""")
+    exe = os.path.join(tmp, "probe")
+    cmd = ["/usr/bin/g++", "-w"] + [f"-D{d}" for d in defines]
+    for d in extra_inc:
+        cmd += ["-I", d]
+    subprocess.run(cmd + [src, "-o", exe], check=True)
+    return subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+
+
+@pytest.mark.parametrize("psrdada", [False, True])
+def test_params_layout_equals_reference_headers(tmp_path, psrdada):
+    """include/heimdall_b200.h lays out hd_params field for field as the
+    reference's own Pipeline/hd/params.h and hd/types.h, compiled here with
+    stand-ins for what they pull in (config.h; dada_hdu.h, which only needs
+    to supply key_t), with HAVE_PSRDADA off and on."""
+    import oracle
+    ref = oracle.reference_dir()
+    if not os.path.exists(os.path.join(ref, "Pipeline", "hd", "params.h")):
+        pytest.skip("reference tree not present")
+    stub = tmp_path / "stub"
+    stub.mkdir()
+    (stub / "config.h").write_text("/* stand-in for the autotools config.h */\n")
+    (stub / "dada_hdu.h").write_text("#include <sys/types.h>\n")
+    defines = ["HAVE_PSRDADA"] if psrdada else []
+    theirs = _layout_probe(str(tmp_path), '#include "hd/params.h"', defines,
+                           [str(stub), os.path.join(ref, "Pipeline")])
+    (tmp_path / "ours").mkdir()
+    ours = _layout_probe(str(tmp_path / "ours"), '#include "heimdall_b200.h"', defines,
+                         [os.path.join(ROOT, "include")])
+    assert len(ours) > 30
+    assert ours == theirs
+    if not psrdada:
+        assert ours[0] == f"size {C.sizeof(hdb.HdParams)}"

@@ -121,12 +121,16 @@ def test_dedisp_long_delay_spans(hdb, oracle_lib, nchans, dt, dm_max, nsamps, ro
     np.testing.assert_array_equal(out, oracle.dedisperse(fb, dms, table))
 
 
-@pytest.mark.parametrize("tile", ["8x256", "8x512", "8x1024", "16x256", "16x512", "16x1024",
-                                  "32x256"])
+TILES = ["8x1024", "8x640", "8x768", "8x1152", "8x1280", "16x512", "16x384", "16x640",
+         "16x768", "32x256", "32x384"]
+
+
+@pytest.mark.parametrize("tile", TILES)
 def test_dedisp_every_tile(hdb, oracle_lib, tile, monkeypatch):
     """Every dedispersion tile the autotuner may pick (DM trials x output
-    samples per CTA, forced through HDB_DEDISP_TILE) gives the oracle's sums,
-    for short rows and for long ones (128 channels over DM 0-2000)."""
+    samples per CTA, forced through HDB_DEDISP_TILE; lanes owning 1, 3 or 5
+    consecutive output words) gives the oracle's sums, for short rows and for
+    long ones (128 channels over DM 0-2000)."""
     monkeypatch.setenv("HDB_DEDISP_TILE", tile)
     db, tb = (int(x) for x in tile.split("x"))
     for nchans, dt, f0, df, dm_max, nsamps in [(256, 64e-6, 1500.0, -1.5625, 1000.0, 30000),
@@ -162,8 +166,7 @@ def test_dedisp_autotuner_keeps_results(hdb, monkeypatch):
             pl.execute(b.data)
             out[mode] = (pl.candidates(), pl.dedisp_tile())
     assert out["default"][1][:2] == (16, 512)
-    assert out["tuned"][1][:2] in [(8, 256), (8, 512), (8, 1024), (16, 256), (16, 512),
-                                   (16, 1024), (32, 256)]
+    assert "%dx%d" % out["tuned"][1][:2] in TILES
     np.testing.assert_array_equal(out["tuned"][0], out["default"][0])
 
 

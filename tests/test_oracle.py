@@ -156,3 +156,43 @@ def test_clustering_sequential_semantics(oracle_lib):
                                     C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]
     nl = L.or_label_clusters(n, C.byref(g), 3, 3, 200, 1 << 20, labels)
     assert list(labels) == [0, 1, 0] and nl == 2
+
+
+@needs_ref
+def test_oracle_equals_reference_headline_beam(oracle_lib):
+    """One beam of the benchmarked multibeam gulp exactly as the benchmark
+    draws it (320 channels, 851 MHz top, 655.36 us, 2^15 samples, DM 0-2000,
+    boxcars to 512, seed 2026): the restatement writes the reference
+    pipeline's .cand lines."""
+    w = synth.SEARCH_C2
+    beams = synth.make_multibeam(w, seed=2026)
+    for u in (0, 17):
+        fb = beams[u].data
+        kw = _small_params(w, clean=int(w.clean))
+        r = oracle.execute(fb, **kw)
+        lines = oracle.cand_lines(r["groups"], fb.shape[0], 1, 0, r["nsamps_processed"],
+                                  w.boxcar_max, w.dt)
+        err, proc, ref_lines, _ = oracle.ref_execute(fb, nthreads=1, **kw)
+        assert err == 0 and proc == r["nsamps_processed"]
+        assert len(lines) >= 1
+        assert lines == ref_lines, u
+
+
+@needs_ref
+def test_oracle_equals_reference_survey_gulp(oracle_lib):
+    """The full survey gulp (1024 channels, 2^18 samples, 64 us, boxcars to
+    4096, persistent narrow-band channels and zero-DM bursts, cleaning on),
+    searched over the DM 240-300 trials of its list (77 of 1482, to keep the
+    single-threaded reference stage code within seconds): the same .cand
+    lines as the reference."""
+    w = synth.SEARCH_C1
+    b = synth.make_c1()
+    kw = _small_params(w, clean=1, dm_min=240.0, dm_max=300.0)
+    r = oracle.execute(b.data, **kw)
+    assert r["dm_count"] == 77
+    lines = oracle.cand_lines(r["groups"], b.data.shape[0], 1, 0, r["nsamps_processed"],
+                              w.boxcar_max, w.dt)
+    err, proc, ref_lines, _ = oracle.ref_execute(b.data, nthreads=1, **kw)
+    assert err == 0 and proc == r["nsamps_processed"]
+    assert len(lines) >= 5
+    assert lines == ref_lines
