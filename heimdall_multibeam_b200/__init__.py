@@ -142,6 +142,18 @@ class HdCoincidence(C.Structure):
     _fields_ = [("nbeams", C.c_uint), ("primary_beam", C.c_uint), ("max_snr", C.c_float)]
 
 
+class HdProfileRequest(C.Structure):
+    """hd_profile_request (include/heimdall_b200.h)."""
+    _fields_ = [("samp", C.c_size_t), ("filter", C.c_size_t), ("dm_idx", C.c_size_t)]
+
+
+class HdProfile(C.Structure):
+    """hd_profile (include/heimdall_b200.h)."""
+    _fields_ = [("dm_time", C.c_void_p), ("dm0_time", C.c_void_p), ("freq_time", C.c_void_p),
+                ("snr_dm", C.c_void_p), ("snr_time", C.c_void_p), ("max_idx", C.c_size_t),
+                ("n_dm", C.c_size_t), ("dm_begin", C.c_size_t), ("snr_dm_first", C.c_size_t)]
+
+
 # symbol -> (restype, argtypes); every function include/*.h declares
 _P = C.c_void_p
 _SZ = C.c_size_t
@@ -186,6 +198,9 @@ SYMBOLS = {
                                      C.POINTER(C.c_int)]),
     "hd_read_sigproc_header": (C.c_int, [C.c_char_p, C.POINTER(HdSigprocHeader)]),
     "hd_coincide": (C.c_int, [_P, _SZ, _SZ, C.c_uint, C.c_uint, C.c_int, _P]),
+    "hd_profile_candidates": (C.c_int, [_P, _SZ, _SZ, C.c_int, C.c_double, C.c_double,
+                                        C.c_double, _FP, _SZ, _P, _SZ, _SZ, _SZ, _SZ, C.c_int,
+                                        _P]),
     "hd_write_coincident_candidates": (C.c_int, [C.c_char_p, _P, _P, _SZ]),
     "hd_mjd_to_utc": (C.c_longlong, [C.c_double]),
     "hd_params_from_sigproc": (C.c_int, [C.POINTER(HdSigprocHeader), C.POINTER(HdParams)]),
@@ -265,8 +280,12 @@ def error_string(code: int) -> str:
 
 
 def default_params(**overrides) -> HdParams:
+    """hd_set_default_params (the reference's defaults) with overrides.  This
+    helper turns adaptive dt off unless use_scrunching is given: the search at
+    the native sampling time is what the parity tests and the benchmark run."""
     p = HdParams()
     lib().hd_set_default_params(C.byref(p))
+    p.use_scrunching = False
     for k, v in overrides.items():
         if k == "output_dir" or k == "sigproc_file":
             v = None if v is None else v.encode()
@@ -661,6 +680,19 @@ class DedispPlan:
         self._check(lib().dedisp_set_killmask(self._p, a.ctypes.data_as(C.POINTER(C.c_int))),
                     "dedisp_set_killmask")
 
+    def enable_adaptive_dt(self, pulse_width=40.0, tol=1.15):
+        self._check(lib().dedisp_enable_adaptive_dt(self._p, pulse_width, tol),
+                    "dedisp_enable_adaptive_dt")
+
+    def disable_adaptive_dt(self):
+        self._check(lib().dedisp_disable_adaptive_dt(self._p), "dedisp_disable_adaptive_dt")
+
+    @property
+    def dt_factors(self) -> np.ndarray:
+        n = lib().dedisp_get_dm_count(self._p)
+        p = lib().dedisp_get_dt_factors(self._p)
+        return np.ctypeslib.as_array(p, shape=(n,)).astype(np.uint64) if n else np.zeros(0, np.uint64)
+
     @property
     def dm_list(self) -> np.ndarray:
         n = lib().dedisp_get_dm_count(self._p)
@@ -862,3 +894,44 @@ class Classifier:
             if err != HD_NO_ERROR:
                 raise HdError(err, "hd_classifier_score_device")
         return out
+
+
+def profile_candidates(filterbank, tsamp: float, fch1: float, foff: float, dm_list,
+                       requests: Sequence[Tuple[int, int, int]], out_nsamps: int = 64,
+                       out_dm_count: int = 32, fscrunch: int = 16, do_filter: bool = False,
+                       nsamps: Optional[int] = None, nchans: Optional[int] = None,
+                       on_device: bool = False) -> List[Dict]:
+    """hd_profile_candidates: the candidate profiler's arrays for each
+    (samp, filter, dm_idx) request.  filterbank: (nsamps, nchans) uint8, or a
+    device pointer with nsamps, nchans and on_device."""
+    if isinstance(filterbank, int):
+        ptr, ns, nc = filterbank, nsamps, nchans
+        keep = None
+    else:
+        keep = _u8(filterbank)
+        ptr, (ns, nc) = keep.ctypes.data, keep.shape
+    dms = np.ascontiguousarray(dm_list, np.float32)
+    n = len(requests)
+    reqs = (HdProfileRequest * n)(*[HdProfileRequest(int(a), int(b), int(c))
+                                    for a, b, c in requests])
+    outs = (HdProfile * n)()
+    arrays = []
+    for i in range(n):
+        a = dict(dm_time=np.zeros((out_dm_count, out_nsamps), np.float32),
+                 dm0_time=np.zeros(out_nsamps, np.float32),
+                 freq_time=np.zeros((nc // fscrunch, out_nsamps), np.float32),
+                 snr_dm=np.zeros(out_dm_count, np.float32),
+                 snr_time=np.zeros((out_nsamps, 5), np.float32))
+        for k, v in a.items():
+            setattr(outs[i], k, v.ctypes.data)
+        arrays.append(a)
+    err = lib().hd_profile_candidates(C.c_void_p(ptr), ns, nc, 1 if on_device else 0, tsamp,
+                                      fch1, foff, dms.ctypes.data_as(_FP), len(dms),
+                                      C.cast(reqs, C.c_void_p), n, out_nsamps, out_dm_count,
+                                      fscrunch, 1 if do_filter else 0, C.cast(outs, C.c_void_p))
+    if err != HD_NO_ERROR:
+        raise HdError(err, "hd_profile_candidates")
+    for i in range(n):
+        arrays[i].update(max_idx=outs[i].max_idx, n_dm=outs[i].n_dm, dm_begin=outs[i].dm_begin,
+                         snr_dm_first=outs[i].snr_dm_first)
+    return arrays

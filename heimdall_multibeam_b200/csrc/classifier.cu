@@ -729,16 +729,20 @@ __device__ float warp_kth(const float* v, int lo, int hi, int k) {
 }
 
 // normalise_series_array (candidate_profiler.C:88-134) on rows of n values,
-// one warp per row; a row whose deviation is zero becomes zero (the
-// reference would divide by zero)
-__global__ void k_normalise_rows(float* __restrict__ data, int n, size_t nrows) {
+// one warp per row.  A row whose deviation is zero becomes zero for the
+// classifier's patches (zero_flat); the profiler keeps the reference's
+// arithmetic there (a division by zero: NaN or +-inf).
+template <bool ZERO_FLAT>
+__global__ void k_normalise_rows_t(float* __restrict__ data, int n, size_t nrows, size_t pitch,
+                                   int rows_per_group, size_t group_pitch) {
   extern __shared__ float nr_smem[];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t row = (size_t)blockIdx.x * (blockDim.x >> 5) + wib;
   float* v = nr_smem + (size_t)wib * 2 * n;  // [n] values, [n] scratch
   float* a = v + n;
   if (row >= nrows) return;  // whole warp
-  float* x = data + row * n;
+  // rows come in groups (e.g. the trials of one candidate's plot)
+  float* x = data + (row / rows_per_group) * group_pitch + (row % rows_per_group) * pitch;
   for (int j = lane; j < n; j += 32) v[j] = x[j];
   __syncwarp();
   const float m1 = warp_kth(v, 0, n / 2, n / 4);
@@ -755,7 +759,30 @@ __global__ void k_normalise_rows(float* __restrict__ data, int n, size_t nrows) 
   const float mad = warp_kth(a, 0, n, n / 2);
   const float stddev = (float)((double)mad * 1.4826);
   const float val = (float)(1.0 / (double)stddev);
-  for (int j = lane; j < n; j += 32) x[j] = stddev > 0.f ? __fmul_rn(v[j], val) : 0.f;
+  for (int j = lane; j < n; j += 32)
+    x[j] = (!ZERO_FLAT || stddev > 0.f) ? __fmul_rn(v[j], val) : 0.f;
+}
+
+cudaError_t normalise_rows(float* data, int n, size_t nrows, size_t pitch, int rows_per_group,
+                           size_t group_pitch, bool zero_flat, cudaStream_t s) {
+  if (n < 2 || nrows == 0) return cudaSuccess;
+  const size_t smem = 2 * (size_t)n * sizeof(float);
+  // rows of up to 1024 values: four warps per block; longer: one
+  const int wpb = n <= 1024 ? 4 : 1;
+  if (smem * wpb > 200 * 1024) return cudaErrorInvalidValue;
+  const void* fn = zero_flat ? reinterpret_cast<const void*>(k_normalise_rows_t<true>)
+                             : reinterpret_cast<const void*>(k_normalise_rows_t<false>);
+  cudaError_t e = raise_smem_limit(fn, smem * wpb);
+  if (e != cudaSuccess) return e;
+  const unsigned nb = (unsigned)((nrows + wpb - 1) / wpb);
+  if (zero_flat)
+    k_normalise_rows_t<true><<<nb, 32 * wpb, smem * wpb, s>>>(data, n, nrows, pitch,
+                                                             rows_per_group, group_pitch);
+  else
+    k_normalise_rows_t<false><<<nb, 32 * wpb, smem * wpb, s>>>(data, n, nrows, pitch,
+                                                              rows_per_group, group_pitch);
+  note_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, const uint8_t* tf,
@@ -765,9 +792,9 @@ cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, co
   k_patch_dm<<<njobs, 256, 0, s>>>(scan, scan_pitch, len, jobs, dm_out); note_launch();
   k_patch_ft<<<dim3((unsigned)njobs, 64), 256, 0, s>>>(tf, nsamps, nchans, jobs, ft_out); note_launch();
   const size_t r1 = (size_t)njobs * 64;
-  k_normalise_rows<<<clf::nblk(r1, 4), 128, 4 * 2 * 64 * sizeof(float), s>>>(dm_out, 64, r1); note_launch();
-  k_normalise_rows<<<clf::nblk(r1, 4), 128, 4 * 2 * 256 * sizeof(float), s>>>(ft_out, 256, r1); note_launch();
-  return cudaGetLastError();
+  cudaError_t e = normalise_rows(dm_out, 64, r1, 64, 1, 64, true, s);
+  if (e == cudaSuccess) e = normalise_rows(ft_out, 256, r1, 256, 1, 256, true, s);
+  return e == cudaSuccess ? cudaGetLastError() : e;
 }
 }  // namespace hdb
 

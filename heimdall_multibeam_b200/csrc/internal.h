@@ -86,6 +86,12 @@ cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
                                    size_t pitch, cudaStream_t s, size_t units = 1,
                                    size_t out_unit = 0);
+// Scrunched channel-major copy of `units` inputs: out[c][u] = the mean of
+// in[c][s u .. s u + s), rounded half up, for u < nsamps / s, and 0 from
+// there to out_pitch.
+cudaError_t launch_scrunch_ft(const uint8_t* in, size_t in_pitch, size_t nsamps, int nchans,
+                              int s, uint8_t* out, size_t out_pitch, size_t units,
+                              size_t in_unit, size_t out_unit, cudaStream_t st);
 // Narrow-band RFI zapping of `units` TF filterbanks of nsamps spectra in
 // place (the branch Pipeline/clean_filterbank_rfi.cu:303-351 disables);
 // scratch of narrow_band_scratch_bytes().
@@ -150,6 +156,7 @@ struct WidthInfo {
   unsigned merge_dist;
   unsigned rel_off;   // rel_cur_filtered_offset
   int prev_cover;     // index of the latest earlier width whose n covers more
+  int scr;            // cur_scrunch: trial scrunch x ts (index rescale)
 };
 
 struct WidthCtx {
@@ -165,6 +172,7 @@ struct WidthCtx {
   size_t scan_len;              // valid prefix-sum entries per series (len + 1)
   int dms_per_unit;             // series per independent unit (beam searched alone)
   int dm_key_gap;               // giant DM key = unit * dm_key_gap + DM index
+  int dm_offset;                // DM index of each unit's first series
   float* norm;        // [nser][nw]  1 / block_rms
   float thresh;
 };
@@ -217,6 +225,13 @@ cudaError_t giant_heads(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhit
 cudaError_t giant_fill(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,
                        unsigned ngiants, GiantBuffers& gb, cudaStream_t s);
 
+// Places the n giants of one scrunch group (unit-major within the group) at
+// dst_base[u] + (i - first[u]) of the combined list (unit u from the DM key);
+// labels and keys are not copied.
+cudaError_t giant_place(const GiantBuffers& src, unsigned n, int dm_key_gap,
+                        const unsigned* first, const unsigned* dst_base, GiantBuffers& dst,
+                        cudaStream_t s);
+
 // label_candidate_clusters (Pipeline/label_candidate_clusters.cu:203-394),
 // sequential-sweep semantics; iterates until stable.
 struct ClusterArgs {
@@ -261,6 +276,17 @@ struct PatchJob {
 cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, const uint8_t* tf,
                             size_t nsamps, int nchans, const PatchJob* jobs, int njobs,
                             float* dm_out, float* ft_out, cudaStream_t s);
+
+// normalise_series_array (candidate_profiler.C:88-134) on nrows rows of n
+// floats: row r at data + (r / rows_per_group) * group_pitch + (r %
+// rows_per_group) * pitch.  zero_flat: a row with zero deviation becomes 0
+// (else the reference's division by zero is kept).
+cudaError_t normalise_rows(float* data, int n, size_t nrows, size_t pitch, int rows_per_group,
+                           size_t group_pitch, bool zero_flat, cudaStream_t s);
+// 256 entries of x / 255 * 255 in float (the profiler's sample scaling)
+__device__ __forceinline__ float prof_scale(unsigned x) {
+  return __fmul_rn(__fdiv_rn((float)x, 255.f), 255.f);
+}
 
 // Scores of n device-resident patch pairs with the classifier, after `after`
 // (an event recorded where the patches were written); scores to host memory.

@@ -596,6 +596,38 @@ cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans,
   return cudaGetLastError();
 }
 
+// Scrunched input of adaptive dt: the byte mean of s consecutive samples
+// (rounded half up) of each channel row, zero past nsamps / s.
+__global__ void __launch_bounds__(256) k_scrunch_ft(const uint8_t* __restrict__ in,
+                                                    size_t in_pitch, size_t ns, int s,
+                                                    uint8_t* __restrict__ out, size_t out_pitch,
+                                                    size_t in_unit, size_t out_unit) {
+  const size_t u = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= out_pitch) return;
+  const size_t c = blockIdx.y;
+  in += (size_t)blockIdx.z * in_unit + c * in_pitch;
+  out += (size_t)blockIdx.z * out_unit + c * out_pitch;
+  unsigned v = 0;
+  if (u < ns) {
+    unsigned sum = 0;
+    for (int j = 0; j < s; j++) sum += in[(size_t)s * u + j];
+    v = (sum + (unsigned)(s / 2)) / (unsigned)s;
+  }
+  out[u] = (uint8_t)v;
+}
+
+cudaError_t launch_scrunch_ft(const uint8_t* in, size_t in_pitch, size_t nsamps, int nchans,
+                              int s, uint8_t* out, size_t out_pitch, size_t units,
+                              size_t in_unit, size_t out_unit, cudaStream_t st) {
+  if (s < 1 || units < 1 || units > 65535 || nchans < 1 || nchans > 65535)
+    return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((out_pitch + 255) / 256), (unsigned)nchans, (unsigned)units);
+  k_scrunch_ft<<<grid, 256, 0, st>>>(in, in_pitch, nsamps / (size_t)s, s, out, out_pitch,
+                                      in_unit, out_unit);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dm0_sum(const uint8_t* in, size_t nsamps, int nchans, float* out,
                            cudaStream_t s) {
   k_dm0_sum<<<(unsigned)((nsamps + 7) / 8), 256, 0, s>>>(in, nsamps, nchans, out); note_launch();

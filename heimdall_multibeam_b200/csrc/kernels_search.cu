@@ -1761,7 +1761,7 @@ __global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, Gian
   const WidthInfo& w = ctx.winfo[sw % ctx.nw];
   bool is_head = gb.head[k] != 0;
   bool is_last = (k + 1 == nhits) || gb.head[k + 1] != 0;
-  unsigned long long scr = (unsigned long long)w.ts;
+  unsigned long long scr = (unsigned long long)w.scr;
   if (is_head) gb.begin[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * scr;
   if (is_last) gb.end[g] = ((unsigned long long)hb.ind[k] + 1ull + w.rel_off) * scr;
   if (is_head) {
@@ -1769,7 +1769,8 @@ __global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, Gian
     // apart so clustering never links two units
     const unsigned ser = sw / ctx.nw;
     gb.filter[g] = w.filter_idx;
-    gb.dm[g] = (int)((ser / ctx.dms_per_unit) * ctx.dm_key_gap + ser % ctx.dms_per_unit);
+    gb.dm[g] = (int)((ser / ctx.dms_per_unit) * ctx.dm_key_gap + ctx.dm_offset +
+                     ser % ctx.dms_per_unit);
   }
 }
 
@@ -1781,7 +1782,31 @@ __global__ void k_giant_finish(HitBuffers hb, unsigned ngiants, GiantBuffers gb,
   unsigned k = 0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull);
   const WidthInfo& w = winfo[hb.sw[k] % nw];
   gb.peak[g] = hb.val[k];
-  gb.ind[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * (unsigned long long)w.ts;
+  gb.ind[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * (unsigned long long)w.scr;
+}
+
+__global__ void k_giant_place(GiantBuffers src, unsigned n, int dm_key_gap,
+                              const unsigned* __restrict__ first,
+                              const unsigned* __restrict__ dst_base, GiantBuffers dst) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned u = (unsigned)src.dm[i] / (unsigned)dm_key_gap;
+  const unsigned j = dst_base[u] + (i - first[u]);
+  dst.peak[j] = src.peak[i];
+  dst.ind[j] = src.ind[i];
+  dst.begin[j] = src.begin[i];
+  dst.end[j] = src.end[i];
+  dst.filter[j] = src.filter[i];
+  dst.dm[j] = src.dm[i];
+}
+
+cudaError_t giant_place(const GiantBuffers& src, unsigned n, int dm_key_gap,
+                        const unsigned* first, const unsigned* dst_base, GiantBuffers& dst,
+                        cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_giant_place<<<(n + 255) / 256, 256, 0, s>>>(src, n, dm_key_gap, first, dst_base, dst);
+  note_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t giant_heads(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits,

@@ -30,9 +30,8 @@ void hd_set_default_params(hd_params* p) {
   p->dm_tol = 1.25f;
   p->dm_pulse_width = 40;
   p->dm_nbits = 32;
-  // The reference defaults to adaptive time resolution; this library searches
-  // every DM at the native resolution, so the default is off.
-  p->use_scrunching = false;
+  // adaptive time resolution, as the reference defaults
+  p->use_scrunching = true;
   p->scrunch_tol = 1.15f;
   p->rfi_tol = 5.0f;
   p->rfi_min_beams = 8;

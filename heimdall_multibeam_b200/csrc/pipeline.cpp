@@ -58,7 +58,9 @@ struct hd_pipeline_t {
   bool has_output_dir = true;
   std::vector<hd_range_t> zaps;
   dedisp_plan plan = nullptr;
-  bool cleaning = true;
+  // clean_filterbank_rfi: off as in the reference's shipped build (it is
+  // compiled in only under -DCLEANING); hd_set_cleaning turns it on
+  bool cleaning = false;
   bool narrow_band = false;  // the reference's disabled narrow-band branch
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -86,7 +88,24 @@ struct hd_pipeline_t {
   DevBuf ws_a, ws_b;
   DevBuf winfo, norm;
   DevBuf tile_cnt, tile_off, sw_cnt, sw_off, hit_ind, hit_val, hit_sw;
-  DevBuf head, gid, gkey, g_peak, g_ind, g_begin, g_end, g_filter, g_dm, g_label;
+  DevBuf head, gid;
+  // a giant list's arrays
+  struct GiantSet {
+    DevBuf key, peak, ind, begin, end, filter, dm, label;
+    void view(hdb::GiantBuffers& g) {
+      g.key = key.as<unsigned long long>();
+      g.peak = peak.as<float>();
+      g.ind = ind.as<unsigned long long>();
+      g.begin = begin.as<unsigned long long>();
+      g.end = end.as<unsigned long long>();
+      g.filter = filter.as<int>();
+      g.dm = dm.as<int>();
+      g.label = label.as<int>();
+    }
+  };
+  GiantSet main_giants;           // the gulp's giant list
+  std::vector<GiantSet> gsets;    // per scrunch group (adaptive dt)
+  DevBuf place_base;
   DevBuf scan_tmp, small;  // small: totals / flags
   DevBuf root_flag, root_off, mkey, rows, unit_off;
   DevBuf h_small_dev;
@@ -279,15 +298,13 @@ hd_error hd_create_pipeline(hd_pipeline* pipeline_, hd_params params) {
     delete pl;
     return HD_MEM_ALLOC_FAILED;
   }
-  if (params.use_scrunching) {
-    // adaptive dt is not provided (dedisp_enable_adaptive_dt reports it)
-    delete pl;
-    return HD_UNKNOWN_ERROR;
-  }
   dedisp_error de = dedisp_create_plan(&pl->plan, params.nchans, params.dt, params.f0, params.df);
   if (de == DEDISP_NO_ERROR)
     de = dedisp_generate_dm_list(pl->plan, params.dm_min, params.dm_max, params.dm_pulse_width,
                                  params.dm_tol);
+  // adaptive dt (pipeline.cu:187-196)
+  if (de == DEDISP_NO_ERROR && params.use_scrunching)
+    de = dedisp_enable_adaptive_dt(pl->plan, params.dm_pulse_width, params.scrunch_tol);
   if (de != DEDISP_NO_ERROR) {
     delete pl;
     return dedisp_err(de);
@@ -392,9 +409,11 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   HD_TRY(pl->dd.ensure(NS * dd_pitch * sizeof(float)));
   float* dd = pl->dd.as<float>();
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if (!on_device && !pl->cleaning && U > 1) {
+  if (!on_device && !pl->cleaning && U > 1 && pl->plan->groups.empty()) {
     // pipelined: copy chunk k on the copy stream while chunk k - 1 is
-    // transposed and dedispersed on the compute stream
+    // transposed and dedispersed on the compute stream (the unit-major series
+    // layout; adaptive dt lays series out by scrunch factor and dedisperses
+    // all units at once)
     const size_t nch = std::min<size_t>(U, kMaxChunks);
     HD_TRY(cudaEventRecord(pl->ev[9], s));
     HD_TRY(cudaStreamWaitEvent(pl->copy_stream, pl->ev[9], 0));
@@ -439,82 +458,133 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     if (de != DEDISP_NO_ERROR) return dedisp_err(de);
   }
   // the element after each series is read (never used) by the baseline stretch
-  HD_TRY(cudaMemset2DAsync(dd + nc, dd_pitch * sizeof(float), 0, sizeof(float), NS, s));
+  if (pl->plan->groups.empty()) {
+    HD_TRY(cudaMemset2DAsync(dd + nc, dd_pitch * sizeof(float), 0, sizeof(float), NS, s));
+  } else {
+    for (const auto& g : pl->plan->groups)
+      HD_TRY(cudaMemset2DAsync(dd + U * g.d0 * dd_pitch + nc / g.s, dd_pitch * sizeof(float), 0,
+                               sizeof(float), U * (g.d1 - g.d0), s));
+  }
   cudaEventRecord(pl->ev[3], s);
 
   const size_t stride = nsamps / nbeams;
   const size_t Bmax = P.boxcar_max;
-  bool search = !(max_delay >= stride) && !(max_delay + Bmax > stride);
+  // scrunch groups: trials [d0, d1) searched at factor s (one group of factor
+  // 1 without adaptive dt); the series rows are group-major, group g's U * (d1
+  // - d0) rows (unit-major inside) starting at row U * d0
+  struct GroupSpec { size_t d0, d1, s; };
+  std::vector<GroupSpec> groups;
+  if (pl->plan->groups.empty()) {
+    groups.push_back({0, D, 1});
+  } else {
+    for (const auto& g : pl->plan->groups) groups.push_back({g.d0, g.d1, g.s});
+  }
+  // the DM loop's break conditions (pipeline.cu:497-502,632-637): the first
+  // trial that trips one ends the search, so only the groups before it run
+  size_t ngs = 0;
+  while (ngs < groups.size()) {
+    const size_t scr = groups[ngs].s;
+    const size_t cur_delay = max_delay / scr, stride_s = nsamps / nbeams / scr;
+    if (cur_delay >= stride_s || cur_delay + Bmax / scr > stride_s) break;
+    ngs++;
+  }
+  // the first (unscrunched) width of a trial must not be time-scrunched: its
+  // block-RMS window would read the previous trial's filtered output
+  for (size_t gi = 0; gi < ngs; gi++)
+    if (std::max<size_t>(P.min_tscrunch_width / groups[gi].s, 1) < 2) return HD_INVALID_STRIDE;
+  const bool search = ngs > 0;
+  const bool multi = groups.size() > 1;
   unsigned nhits = 0, ngiants = 0;
   std::vector<hdb::WidthInfo> wi;
   hdb::WidthCtx wctx{};
   hdb::HitBuffers hb{};
   hdb::GiantBuffers gb{};
+  std::vector<unsigned> group_giants(ngs, 0);
+  const size_t scan_pitch = round_up(nc + 1, 4);
   if (search) {
-    // ---- per-DM baseline, RMS, normalise + scan ------------------------------
-    const size_t bcount = stride - max_delay;
-    hdb::SeriesBatch sb{dd, dd_pitch, (int)NS, nc, stride, bcount, (int)nbeams};
-    const float cur_dt = P.dt * 1.0f;
-    const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
-    size_t cap = std::max({tree_cap(NS * nbeams, stride),
-                           tree_cap(NS * (log2u(Bmax) + 1), nbeams * stride),
-                           hdb::baseline_scratch(stride, nsmooth, NS * nbeams)});
+    const size_t cap = std::max({tree_cap(NS * nbeams, stride),
+                                 tree_cap(NS * (log2u(Bmax) + 1), nbeams * stride),
+                                 hdb::baseline_scratch(stride, (size_t)(P.baseline_length /
+                                                                        (2 * P.dt)),
+                                                       NS * nbeams)});
     HD_TRY(pl->ws_a.ensure(cap * sizeof(float)));
     HD_TRY(pl->ws_b.ensure(cap * sizeof(float)));
-    hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
-    HD_TRY(pl->base.ensure((NS * nbeams * hdb::baseline_samples(stride, nsmooth) + 64) *
-                           sizeof(float)));
+    HD_TRY(pl->base.ensure((NS * nbeams *
+                                hdb::baseline_samples(stride, (size_t)(P.baseline_length /
+                                                                       (2 * P.dt))) +
+                            64) * sizeof(float)));
     HD_TRY(pl->rms.ensure(NS * nbeams * sizeof(float) + 64));
-    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
-    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
-    const size_t scan_pitch = round_up(nc + 1, 4);
-    pl->searched = true;
+    HD_TRY(pl->scan.ensure(NS * scan_pitch * sizeof(float)));
+    HD_TRY(pl->small.ensure(64 * sizeof(unsigned)));
+    pl->searched = !multi;  // patches read unscrunched series only
     pl->last_nsamps = nsamps;
     pl->last_len = nc;
     pl->last_scan_pitch = scan_pitch;
     pl->last_units = U;
-    HD_TRY(pl->scan.ensure(NS * scan_pitch * sizeof(float)));
-    HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), pl->scan.as<float>(), scan_pitch,
-                               nullptr, s, pl->plan->d_err));
-    cudaEventRecord(pl->ev[4], s);
+    if (multi && pl->gsets.size() < ngs) pl->gsets.resize(ngs);
+  }
+  for (size_t gi = 0; gi < ngs; gi++) {
+    const GroupSpec& G = groups[gi];
+    const size_t scr = G.s, Dg = G.d1 - G.d0, NSg = U * Dg, row0 = U * G.d0;
+    const size_t nc_s = nc / scr;
+    const size_t cur_delay = max_delay / scr;
+    const size_t stride_s = nsamps / nbeams / scr;
+    const size_t rel_bmax = Bmax / scr;
+    // ---- per-DM baseline, RMS, normalise + scan ------------------------------
+    const size_t bcount = stride_s - cur_delay;
+    float* ddg = dd + row0 * dd_pitch;
+    float* scan_g = pl->scan.as<float>() + row0 * scan_pitch;
+    hdb::SeriesBatch sb{ddg, dd_pitch, (int)NSg, nc_s, stride_s, bcount, (int)nbeams};
+    const float cur_dt = P.dt * (float)scr;
+    const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
+    hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
+    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
+    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
+    HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan_g, scan_pitch, nullptr, s,
+                               pl->plan->d_err));
+    if (gi == 0) cudaEventRecord(pl->ev[4], s);
 
-    // ---- widths --------------------------------------------------------------
-    const size_t rel_bmax = Bmax;
-    const size_t max_nf = nc + 1 - rel_bmax;
+    // ---- widths (pipeline.cu:657-776 at this group's factor) ------------------
+    wi.clear();
+    const size_t max_nf = nc_s + 1 - rel_bmax;
     const size_t cur_off = rel_bmax / 2;
-    for (size_t fw = 1; fw <= Bmax; fw *= 2) {
+    for (size_t fw = scr; fw <= Bmax; fw *= 2) {
       hdb::WidthInfo w{};
-      size_t rel_min_ts = std::max<size_t>(P.min_tscrunch_width / 1, 1);
-      size_t ts = std::max<size_t>(2 * fw / rel_min_ts, 1);
-      w.width = (int)fw;
+      const size_t rel_fw = fw / scr;
+      size_t rel_min_ts = std::max<size_t>(P.min_tscrunch_width / scr, 1);
+      size_t ts = std::max<size_t>(2 * rel_fw / rel_min_ts, 1);
+      w.width = (int)rel_fw;
       w.ts = (int)ts;
-      w.ahead = (int)((fw - 1) / 2 + 1);
-      w.behind = (int)(fw / 2);
+      w.ahead = (int)((rel_fw - 1) / 2 + 1);
+      w.behind = (int)(rel_fw / 2);
       w.filter_idx = (int)log2u(fw);
       w.n = (unsigned)((max_nf - 1) / ts + 1);
-      w.bn = (unsigned)(stride - (max_delay + rel_bmax));
-      w.merge_dist = (unsigned)(P.cand_sep_time * (fw / ts));
+      w.bn = (unsigned)(stride_s - (cur_delay + rel_bmax));
+      w.merge_dist = (unsigned)(P.cand_sep_time * (rel_fw / ts));
       w.rel_off = (unsigned)(cur_off / ts);
       w.prev_cover = (int)wi.size() - 1;
+      w.scr = (int)(scr * ts);
       wi.push_back(w);
     }
     const int nw = (int)wi.size();
+    if (nw == 0) continue;  // the trials' factor exceeds the widest boxcar
     HD_TRY(pl->winfo.ensure(nw * sizeof(hdb::WidthInfo)));
     HD_TRY(cudaMemcpyAsync(pl->winfo.p, wi.data(), nw * sizeof(hdb::WidthInfo),
                            cudaMemcpyHostToDevice, s));
-    HD_TRY(pl->norm.ensure(NS * nw * sizeof(float)));
-    wctx.scan = pl->scan.as<float>();
+    HD_TRY(pl->norm.ensure(NSg * nw * sizeof(float)));
+    wctx.scan = scan_g;
     wctx.scan_pitch = scan_pitch;
-    wctx.nser = (int)NS;
-    wctx.stride = stride;
+    wctx.nser = (int)NSg;
+    wctx.stride = stride_s;
     wctx.nbeams = (int)nbeams;
     wctx.offset = (int)cur_off;
     wctx.nw = nw;
     wctx.winfo = pl->winfo.as<hdb::WidthInfo>();
     wctx.host_winfo = wi.data();
-    wctx.scan_len = nc + 1;
-    wctx.dms_per_unit = (int)D;
+    wctx.scan_len = nc_s + 1;
+    wctx.dms_per_unit = (int)Dg;
     wctx.dm_key_gap = (int)gap;
+    wctx.dm_offset = (int)G.d0;
     wctx.norm = pl->norm.as<float>();
     wctx.thresh = P.detect_thresh;
     int n_ts1 = 0;
@@ -524,12 +594,11 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
 
     // ---- threshold + ordered compaction -------------------------------------
     const unsigned ntiles = (unsigned)((wi[0].n + 2047) / 2048);
-    const size_t nsw = NS * nw;
+    const size_t nsw = NSg * nw;
     HD_TRY(pl->tile_cnt.ensure(nsw * ntiles * sizeof(unsigned)));
     HD_TRY(pl->tile_off.ensure(nsw * ntiles * sizeof(unsigned)));
     HD_TRY(pl->sw_cnt.ensure((nsw + 1) * sizeof(unsigned)));
     HD_TRY(pl->sw_off.ensure((nsw + 1) * sizeof(unsigned)));
-    HD_TRY(pl->small.ensure(64 * sizeof(unsigned)));
     hb.tile_cnt = pl->tile_cnt.as<unsigned>();
     hb.tile_off = pl->tile_off.as<unsigned>();
     hb.sw_cnt = pl->sw_cnt.as<unsigned>();
@@ -541,50 +610,105 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(hdb::scan_u32(hb.sw_cnt, hb.sw_off, nsw, totals, pl->scan_tmp.as<unsigned>(), s));
     HD_TRY(cudaMemcpyAsync(pl->h_small, totals, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     HD_TRY(cudaStreamSynchronize(s));
-    nhits = pl->h_small[0];
-    HD_TRY(pl->hit_ind.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
-    HD_TRY(pl->hit_val.ensure((size_t)(nhits + 1) * sizeof(float)));
-    HD_TRY(pl->hit_sw.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
+    const unsigned gh = pl->h_small[0];
+    nhits += gh;
+    HD_TRY(pl->hit_ind.ensure((size_t)(gh + 1) * sizeof(unsigned)));
+    HD_TRY(pl->hit_val.ensure((size_t)(gh + 1) * sizeof(float)));
+    HD_TRY(pl->hit_sw.ensure((size_t)(gh + 1) * sizeof(unsigned)));
     hb.ind = pl->hit_ind.as<unsigned>();
     hb.val = pl->hit_val.as<float>();
     hb.sw = pl->hit_sw.as<unsigned>();
-    hb.cap = nhits;
-    if (nhits) HD_TRY(hdb::write_hits(wctx, hb, s));
-    cudaEventRecord(pl->ev[5], s);
+    hb.cap = gh;
+    if (gh) HD_TRY(hdb::write_hits(wctx, hb, s));
+    if (gi == 0) cudaEventRecord(pl->ev[5], s);
 
     // ---- giants ------------------------------------------------------------
-    if (nhits) {
-      HD_TRY(pl->head.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
-      HD_TRY(pl->gid.ensure((size_t)(nhits + 1) * sizeof(unsigned)));
-      gb.head = pl->head.as<unsigned>();
-      gb.gid = pl->gid.as<unsigned>();
-      HD_TRY(hdb::giant_heads(wctx, hb, nhits, gb, s));
-      HD_TRY(pl->scan_tmp.ensure(hdb::scan_tmp_words(nhits) * sizeof(unsigned)));
-      HD_TRY(hdb::scan_u32(gb.head, gb.gid, nhits, totals + 1, pl->scan_tmp.as<unsigned>(), s));
-      HD_TRY(cudaMemcpyAsync(pl->h_small + 1, totals + 1, sizeof(unsigned),
+    if (!gh) continue;
+    HD_TRY(pl->head.ensure((size_t)(gh + 1) * sizeof(unsigned)));
+    HD_TRY(pl->gid.ensure((size_t)(gh + 1) * sizeof(unsigned)));
+    hdb::GiantBuffers gg{};
+    gg.head = pl->head.as<unsigned>();
+    gg.gid = pl->gid.as<unsigned>();
+    HD_TRY(hdb::giant_heads(wctx, hb, gh, gg, s));
+    HD_TRY(pl->scan_tmp.ensure(hdb::scan_tmp_words(gh) * sizeof(unsigned)));
+    HD_TRY(hdb::scan_u32(gg.head, gg.gid, gh, totals + 1, pl->scan_tmp.as<unsigned>(), s));
+    HD_TRY(cudaMemcpyAsync(pl->h_small + 1, totals + 1, sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaStreamSynchronize(s));
+    const unsigned gn = pl->h_small[1];
+    group_giants[gi] = gn;
+    ngiants += gn;
+    // one group: straight into the giant list; several: into the group's
+    // own buffers, placed unit-major once every group is done
+    hd_pipeline_t::GiantSet& gs = multi ? pl->gsets[gi] : pl->main_giants;
+    const size_t Gc = (size_t)gn + 1;
+    HD_TRY(gs.key.ensure(Gc * sizeof(unsigned long long)));
+    HD_TRY(gs.peak.ensure(Gc * sizeof(float)));
+    HD_TRY(gs.ind.ensure(Gc * sizeof(unsigned long long)));
+    HD_TRY(gs.begin.ensure(Gc * sizeof(unsigned long long)));
+    HD_TRY(gs.end.ensure(Gc * sizeof(unsigned long long)));
+    HD_TRY(gs.filter.ensure(Gc * sizeof(int)));
+    HD_TRY(gs.dm.ensure(Gc * sizeof(int)));
+    HD_TRY(gs.label.ensure(Gc * sizeof(int)));
+    gs.view(gg);
+    gg.cap = gn;
+    HD_TRY(hdb::giant_fill(wctx, hb, gh, gn, gg, s));
+  }
+  if (search && ngiants) {
+    hd_pipeline_t::GiantSet& m = pl->main_giants;
+    if (multi) {
+      // giants unit-major across groups: unit u's giants of group 0, then of
+      // group 1, ... (the order the reference's DM loop appends them in)
+      const size_t Gc = (size_t)ngiants + 1;
+      HD_TRY(m.key.ensure(Gc * sizeof(unsigned long long)));
+      HD_TRY(m.peak.ensure(Gc * sizeof(float)));
+      HD_TRY(m.ind.ensure(Gc * sizeof(unsigned long long)));
+      HD_TRY(m.begin.ensure(Gc * sizeof(unsigned long long)));
+      HD_TRY(m.end.ensure(Gc * sizeof(unsigned long long)));
+      HD_TRY(m.filter.ensure(Gc * sizeof(int)));
+      HD_TRY(m.dm.ensure(Gc * sizeof(int)));
+      HD_TRY(m.label.ensure(Gc * sizeof(int)));
+      hdb::GiantBuffers dst{};
+      m.view(dst);
+      // per-group unit offsets, then each group's destination per unit
+      std::vector<unsigned> firsts(ngs * (U + 1), 0);
+      HD_TRY(pl->unit_off.ensure(ngs * (U + 1) * sizeof(unsigned)));
+      HD_TRY(pl->place_base.ensure(ngs * (U + 1) * sizeof(unsigned)));
+      for (size_t gi = 0; gi < ngs; gi++) {
+        if (!group_giants[gi]) continue;
+        hdb::GiantBuffers src{};
+        pl->gsets[gi].view(src);
+        HD_TRY(hdb::unit_giant_offsets(src, (int)group_giants[gi], (int)gap, (int)U,
+                                       pl->unit_off.as<unsigned>() + gi * (U + 1), s));
+      }
+      HD_TRY(cudaMemcpyAsync(firsts.data(), pl->unit_off.p, ngs * (U + 1) * sizeof(unsigned),
                              cudaMemcpyDeviceToHost, s));
       HD_TRY(cudaStreamSynchronize(s));
-      ngiants = pl->h_small[1];
-      size_t G = (size_t)ngiants + 1;
-      HD_TRY(pl->gkey.ensure(G * sizeof(unsigned long long)));
-      HD_TRY(pl->g_peak.ensure(G * sizeof(float)));
-      HD_TRY(pl->g_ind.ensure(G * sizeof(unsigned long long)));
-      HD_TRY(pl->g_begin.ensure(G * sizeof(unsigned long long)));
-      HD_TRY(pl->g_end.ensure(G * sizeof(unsigned long long)));
-      HD_TRY(pl->g_filter.ensure(G * sizeof(int)));
-      HD_TRY(pl->g_dm.ensure(G * sizeof(int)));
-      HD_TRY(pl->g_label.ensure(G * sizeof(int)));
-      gb.key = pl->gkey.as<unsigned long long>();
-      gb.peak = pl->g_peak.as<float>();
-      gb.ind = pl->g_ind.as<unsigned long long>();
-      gb.begin = pl->g_begin.as<unsigned long long>();
-      gb.end = pl->g_end.as<unsigned long long>();
-      gb.filter = pl->g_filter.as<int>();
-      gb.dm = pl->g_dm.as<int>();
-      gb.label = pl->g_label.as<int>();
-      gb.cap = ngiants;
-      HD_TRY(hdb::giant_fill(wctx, hb, nhits, ngiants, gb, s));
+      std::vector<unsigned> base(ngs * (U + 1), 0);
+      unsigned at = 0;
+      for (size_t u = 0; u < U; u++)
+        for (size_t gi = 0; gi < ngs; gi++) {
+          base[gi * (U + 1) + u] = at;
+          if (group_giants[gi])
+            at += firsts[gi * (U + 1) + u + 1] - firsts[gi * (U + 1) + u];
+        }
+      HD_TRY(cudaMemcpyAsync(pl->place_base.p, base.data(), base.size() * sizeof(unsigned),
+                             cudaMemcpyHostToDevice, s));
+      for (size_t gi = 0; gi < ngs; gi++) {
+        if (!group_giants[gi]) continue;
+        hdb::GiantBuffers src{};
+        pl->gsets[gi].view(src);
+        HD_TRY(hdb::giant_place(src, group_giants[gi], (int)gap,
+                                pl->unit_off.as<unsigned>() + gi * (U + 1),
+                                pl->place_base.as<unsigned>() + gi * (U + 1), dst, s));
+      }
+      // the host base table must outlive the copy
+      HD_TRY(cudaStreamSynchronize(s));
     }
+    m.view(gb);
+    gb.head = pl->head.as<unsigned>();
+    gb.gid = pl->gid.as<unsigned>();
+    gb.cap = ngiants;
   }
   cudaEventRecord(pl->ev[6], s);
 

@@ -61,8 +61,95 @@ std::vector<float> generate_dm_list(float dm_start, float dm_end, double dt, dou
   return out;
 }
 
+// Adaptive dt (dedisp_enable_adaptive_dt; the rule of Barsdell et al. 2012,
+// MNRAS 422, 379, restated): the smearing of trial DM at sampling time T is
+// the generator's model W(DM, T)^2 = T^2 + ti^2 + (a DM)^2 (microseconds,
+// same a and band centre); factors start at 1, never decrease, and trial d
+// takes twice the previous factor s when W(DM_d, 2 s dt) / W(DM_d, s dt) <
+// tol.  Double precision throughout.
+std::vector<dedisp_size> scrunch_factors(const std::vector<float>& dm_list, double dt,
+                                         double ti, double f0, double df, size_t nchans,
+                                         double tol) {
+  const double dt_us = dt * 1e6;
+  const double f = (f0 + ((double)(nchans / 2) - 0.5) * df) * 1e-3;
+  const double a = 8.3 * df / (f * f * f);
+  std::vector<dedisp_size> out(dm_list.size(), 1);
+  dedisp_size s = 1;
+  for (size_t d = 1; d < dm_list.size(); d++) {
+    const double sm = a * (double)dm_list[d];
+    const double t1 = (double)s * dt_us, t2 = 2.0 * (double)s * dt_us;
+    const double w1 = std::sqrt(t1 * t1 + ti * ti + sm * sm);
+    const double w2 = std::sqrt(t2 * t2 + ti * ti + sm * sm);
+    if (w2 / w1 < tol) s *= 2;
+    out[d] = s;
+  }
+  return out;
+}
+
 static void free_dev(void* p) {
   if (p) cudaFree(p);
+}
+
+static void free_groups(dedisp_plan p) {
+  for (auto& g : p->groups) {
+    free_dev(g.d_delays);
+    for (int* b : g.d_blk_min) free_dev(b);
+  }
+  p->groups.clear();
+}
+
+// Trials of one scrunch factor: delays at that factor, per DM-block minima
+// and spans, uploaded.
+static dedisp_error build_groups(dedisp_plan p) {
+  free_groups(p);
+  if (!p->adaptive) return DEDISP_NO_ERROR;
+  const size_t D = p->dm_list.size(), C = p->nchans;
+  size_t d = 0;
+  while (d < D) {
+    dedisp_plan_struct::Group g;
+    g.d0 = d;
+    g.s = p->dt_factors[d];
+    while (d < D && p->dt_factors[d] == g.s) d++;
+    g.d1 = d;
+    const size_t Dg = g.d1 - g.d0;
+    g.delays.resize(Dg * C);
+    for (size_t i = 0; i < Dg; i++)
+      for (size_t c = 0; c < C; c++) {
+        const int v = p->delays[(g.d0 + i) * C + c] / (int)g.s;
+        g.delays[i * C + c] = v;
+        g.max_delay = std::max(g.max_delay, (size_t)v);
+      }
+    for (int k = 0; k < 3; k++) {
+      const size_t DB = (size_t)kDedispDmBlocks[k];
+      const size_t nblk = (Dg + DB - 1) / DB;
+      g.blk_min[k].assign(nblk * C, 0);
+      for (size_t b = 0; b < nblk; b++)
+        for (size_t c = 0; c < C; c++) {
+          int lo = 0x7FFFFFFF, hi = 0;
+          for (size_t i = b * DB; i < std::min(Dg, (b + 1) * DB); i++) {
+            lo = std::min(lo, g.delays[i * C + c]);
+            hi = std::max(hi, g.delays[i * C + c]);
+          }
+          g.blk_min[k][b * C + c] = lo;
+          g.max_span[k] = std::max(g.max_span[k], (size_t)(hi - lo));
+        }
+    }
+    p->groups.push_back(std::move(g));
+    dedisp_plan_struct::Group& G = p->groups.back();
+    if (dev_malloc(&G.d_delays, G.delays.size() * sizeof(int)) != cudaSuccess)
+      return DEDISP_MEM_ALLOC_FAILED;
+    if (cudaMemcpy(G.d_delays, G.delays.data(), G.delays.size() * sizeof(int),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return DEDISP_MEM_COPY_FAILED;
+    for (int k = 0; k < 3; k++) {
+      if (dev_malloc(&G.d_blk_min[k], G.blk_min[k].size() * sizeof(int)) != cudaSuccess)
+        return DEDISP_MEM_ALLOC_FAILED;
+      if (cudaMemcpy(G.d_blk_min[k], G.blk_min[k].data(), G.blk_min[k].size() * sizeof(int),
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return DEDISP_MEM_COPY_FAILED;
+    }
+  }
+  return DEDISP_NO_ERROR;
 }
 
 dedisp_error plan_prepare(dedisp_plan p) {
@@ -128,6 +215,8 @@ dedisp_error plan_prepare(dedisp_plan p) {
     if (cudaMemcpy(p->d_blk_min[k], p->blk_min[k].data(), p->blk_min[k].size() * sizeof(int),
                    cudaMemcpyHostToDevice) != cudaSuccess)
       return DEDISP_MEM_COPY_FAILED;
+  dedisp_error ge = build_groups(p);
+  if (ge != DEDISP_NO_ERROR) return ge;
   p->device = dev;
   p->dirty = false;
   return DEDISP_NO_ERROR;
@@ -141,49 +230,56 @@ static int dm_block_index(int dm_block) {
 
 // Staged row bytes of a tile: the DM block's delay span for one channel, the
 // time block, the 16-byte alignment of the copy and one word of look-ahead.
-static int rowb_of(const dedisp_plan p, int dm_block, int time_block) {
-  size_t r = p->max_span[dm_block_index(dm_block)] + 16 + (size_t)time_block + 8;
+static int rowb_of(const size_t* max_span, int dm_block, int time_block) {
+  size_t r = max_span[dm_block_index(dm_block)] + 16 + (size_t)time_block + 8;
   return (int)((r + 15) & ~(size_t)15);
 }
 
-size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
-  // room for the longest staged row of every candidate tile past the last
-  // time block
-  size_t nout = nsamps > p->max_delay ? nsamps - p->max_delay : 0;
+// Row pitch of a channel-major input of nsamps samples whose trials reach
+// max_delay and produce nout samples: room for the longest staged row of
+// every candidate tile past the last time block.
+static size_t ft_pitch_for(const size_t* max_span, size_t max_delay, size_t nsamps,
+                           size_t nout) {
   size_t need = nsamps + 4;
   for (const auto& t : kDedispTiles) {
     const size_t tb = (size_t)t[1];
     const size_t ntb = (nout + tb - 1) / tb;
-    need = std::max(need, ntb * tb + p->max_delay + (size_t)rowb_of(p, t[0], t[1]));
+    need = std::max(need, ntb * tb + max_delay + (size_t)rowb_of(max_span, t[0], t[1]));
   }
   need += 64;
   return (need + 63) & ~(size_t)63;
 }
 
-dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch, size_t nsamps,
-                                float* d_out, size_t out_pitch, cudaStream_t s, size_t units,
-                                size_t in_unit, size_t out_unit) {
-  dedisp_error de = plan_prepare(p);
-  if (de != DEDISP_NO_ERROR) return de;
-  if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
-  size_t nout = nsamps - p->max_delay;
-  if (nout == 0) return DEDISP_NO_ERROR;
-  if (units == 0) return DEDISP_NO_ERROR;
+size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
+  size_t nout = nsamps > p->max_delay ? nsamps - p->max_delay : 0;
+  return ft_pitch_for(p->max_span, p->max_delay, nsamps, nout);
+}
+
+// One launch set over trials whose delays are d_delays (dm_count rows) on a
+// channel-major input of nsamps samples, nout output samples per trial; the
+// tile is tuned per (nsamps, units, tune_key).
+static dedisp_error dedisperse_tables(dedisp_plan p, const int* d_delays, int* const* d_blk_min,
+                                      const size_t* max_span, int dm_count, size_t nout,
+                                      size_t tune_key, const uint8_t* d_ft, size_t pitch,
+                                      size_t nsamps, float* d_out, size_t out_pitch,
+                                      cudaStream_t s, size_t units, size_t in_unit,
+                                      size_t out_unit) {
+  if (nout == 0 || units == 0 || dm_count == 0) return DEDISP_NO_ERROR;
   if (p->active.empty()) {
     for (size_t u = 0; u < units; u++)
       if (cudaMemset2DAsync(d_out + u * out_unit, out_pitch * sizeof(float), 0,
-                            nout * sizeof(float), p->dm_list.size(), s) != cudaSuccess)
+                            nout * sizeof(float), (size_t)dm_count, s) != cudaSuccess)
         return DEDISP_INTERNAL_GPU_ERROR;
     return DEDISP_NO_ERROR;
   }
   DedispArgs a;
   a.in = d_ft;
   a.in_pitch = pitch;
-  a.delays = p->d_delays;
+  a.delays = d_delays;
   a.chans = p->d_active;
   a.nact = (int)p->active.size();
   a.nchans = (int)p->nchans;
-  a.dm_count = (int)p->dm_list.size();
+  a.dm_count = dm_count;
   a.nout = nout;
   a.out = d_out;
   a.out_pitch = out_pitch;
@@ -202,19 +298,19 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
     }
   if (units > 65535) return DEDISP_INVALID_STRIDE;
   auto with_tile = [&](const std::array<int, 3>& t) {
-    a.blk_min = p->d_blk_min[dm_block_index(t[0])];
-    a.rowb = rowb_of(p, t[0], t[1]);
+    a.blk_min = d_blk_min[dm_block_index(t[0])];
+    a.rowb = rowb_of(max_span, t[0], t[1]);
     return DedispTile{t[0], t[1], t[2]};
   };
   // candidate tiles whose staged rows fit shared memory
   std::vector<std::array<int, 3>> cand;
   for (const auto& t : kDedispTiles) {
-    const int rows = dedisp_rows_per_stage(t[0], rowb_of(p, t[0], t[1]));
+    const int rows = dedisp_rows_per_stage(t[0], rowb_of(max_span, t[0], t[1]));
     if (rows) cand.push_back({t[0], t[1], rows});
   }
   // one channel row of the widest block's delay span must fit shared memory
   if (cand.empty()) return DEDISP_NCHANS_EXCEEDS_LIMIT;
-  const auto key = std::make_pair(nsamps, units);
+  const std::array<size_t, 3> key = {nsamps, units, tune_key};
   auto it = p->tiles.find(key);
   if (it == p->tiles.end()) {
     // default: 16 DMs x 512 samples when it fits
@@ -261,6 +357,53 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   return DEDISP_NO_ERROR;
 }
 
+
+dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch, size_t nsamps,
+                                float* d_out, size_t out_pitch, cudaStream_t s, size_t units,
+                                size_t in_unit, size_t out_unit) {
+  dedisp_error de = plan_prepare(p);
+  if (de != DEDISP_NO_ERROR) return de;
+  if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
+  const size_t nout = nsamps - p->max_delay;
+  if (p->groups.empty())
+    return dedisperse_tables(p, p->d_delays, p->d_blk_min, p->max_span,
+                             (int)p->dm_list.size(), nout, 0, d_ft, pitch, nsamps, d_out,
+                             out_pitch, s, units, in_unit, out_unit);
+  // adaptive dt: group g's trials [d0, d1) of every unit are rows
+  // units * d0 + u * (d1 - d0) + i of the output (group-major)
+  const size_t C = p->nchans;
+  for (size_t gi = 0; gi < p->groups.size(); gi++) {
+    const dedisp_plan_struct::Group& g = p->groups[gi];
+    const size_t Dg = g.d1 - g.d0;
+    const size_t nout_s = nout / g.s;
+    float* out_g = d_out + units * g.d0 * out_pitch;
+    if (g.s == 1) {
+      de = dedisperse_tables(p, g.d_delays, g.d_blk_min, g.max_span, (int)Dg, nout_s, gi + 1,
+                             d_ft, pitch, nsamps, out_g, out_pitch, s, units, in_unit,
+                             Dg * out_pitch);
+    } else {
+      const size_t ns = nsamps / g.s;
+      const size_t pitch_s = ft_pitch_for(g.max_span, g.max_delay, ns, nout_s);
+      const size_t need = units * pitch_s * C;
+      if (p->d_scr_cap < need) {
+        free_dev(p->d_scr);
+        p->d_scr = nullptr;
+        p->d_scr_cap = 0;
+        if (dev_malloc(&p->d_scr, need) != cudaSuccess) return DEDISP_MEM_ALLOC_FAILED;
+        p->d_scr_cap = need;
+      }
+      if (launch_scrunch_ft(d_ft, pitch, nsamps, (int)C, (int)g.s, p->d_scr, pitch_s, units,
+                            in_unit, pitch_s * C, s) != cudaSuccess)
+        return DEDISP_INTERNAL_GPU_ERROR;
+      de = dedisperse_tables(p, g.d_delays, g.d_blk_min, g.max_span, (int)Dg, nout_s, gi + 1,
+                             p->d_scr, pitch_s, ns, out_g, out_pitch, s, units, pitch_s * C,
+                             Dg * out_pitch);
+    }
+    if (de != DEDISP_NO_ERROR) return de;
+  }
+  return DEDISP_NO_ERROR;
+}
+
 }  // namespace hdb
 
 dedisp_plan_struct::~dedisp_plan_struct() {
@@ -272,6 +415,8 @@ dedisp_plan_struct::~dedisp_plan_struct() {
   hdb::free_dev(d_in_tf);
   hdb::free_dev(d_in_ft);
   hdb::free_dev(d_out);
+  hdb::free_dev(d_scr);
+  hdb::free_groups(this);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -312,12 +457,21 @@ dedisp_error dedisp_create_plan(dedisp_plan* plan, dedisp_size nchans, dedisp_fl
 
 void dedisp_destroy_plan(dedisp_plan plan) { delete plan; }
 
+// The per-trial scrunch factors follow the DM list (all 1 without adaptive dt).
+static void set_factors(dedisp_plan p) {
+  if (p->adaptive)
+    p->dt_factors = hdb::scrunch_factors(p->dm_list, p->dt, p->adaptive_width, p->f0, p->df,
+                                         p->nchans, p->adaptive_tol);
+  else
+    p->dt_factors.assign(p->dm_list.size(), 1);
+  p->dirty = true;
+}
+
 dedisp_error dedisp_set_dm_list(dedisp_plan p, const dedisp_float* l, dedisp_size n) {
   if (!p) return DEDISP_INVALID_PLAN;
   if (!l) return DEDISP_INVALID_POINTER;
   p->dm_list.assign(l, l + n);
-  p->dt_factors.assign(n, 1);
-  p->dirty = true;
+  set_factors(p);
   return DEDISP_NO_ERROR;
 }
 
@@ -325,8 +479,7 @@ dedisp_error dedisp_generate_dm_list(dedisp_plan p, dedisp_float a, dedisp_float
                                      dedisp_float ti, dedisp_float tol) {
   if (!p) return DEDISP_INVALID_PLAN;
   p->dm_list = hdb::generate_dm_list(a, b, p->dt, ti, p->f0, p->df, p->nchans, tol);
-  p->dt_factors.assign(p->dm_list.size(), 1);
-  p->dirty = true;
+  set_factors(p);
   return DEDISP_NO_ERROR;
 }
 
@@ -353,17 +506,22 @@ dedisp_error dedisp_set_killmask(dedisp_plan p, const dedisp_bool* km) {
   return DEDISP_NO_ERROR;
 }
 
-// Adaptive time resolution is not provided: the search is run at the native
-// sampling time for every DM (the reference's use_scrunching = 0 path).
+// Adaptive time resolution: per-trial scrunch factors (hdb::scrunch_factors),
+// recomputed whenever the DM list changes.
 dedisp_error dedisp_enable_adaptive_dt(dedisp_plan p, dedisp_float w, dedisp_float tol) {
   if (!p) return DEDISP_INVALID_PLAN;
-  (void)w; (void)tol;
-  return DEDISP_INVALID_FLAG_COMBINATION;
+  if (!(tol > 1.0f) || !(w >= 0.0f)) return DEDISP_INVALID_FLAG_COMBINATION;
+  p->adaptive = true;
+  p->adaptive_width = w;
+  p->adaptive_tol = tol;
+  set_factors(p);
+  return DEDISP_NO_ERROR;
 }
 
 dedisp_error dedisp_disable_adaptive_dt(dedisp_plan p) {
   if (!p) return DEDISP_INVALID_PLAN;
   p->adaptive = false;
+  set_factors(p);
   return DEDISP_NO_ERROR;
 }
 

@@ -34,9 +34,10 @@ struct dedisp_plan_struct {
   size_t max_span[3] = {0, 0, 0};  // max over blocks/chans of (max - min) delay
   int* d_delays = nullptr;
   int* d_blk_min[3] = {nullptr, nullptr, nullptr};
-  // dedispersion tile {dm_block, time_block, rows} per (nsamps, units): the
-  // fastest of the candidates, timed on first use (autotuner)
-  std::map<std::pair<size_t, size_t>, std::array<int, 3>> tiles;
+  // dedispersion tile {dm_block, time_block, rows} per (nsamps, units,
+  // scrunch group): the fastest of the candidates, timed on first use
+  // (autotuner)
+  std::map<std::array<size_t, 3>, std::array<int, 3>> tiles;
   std::array<int, 3> last_tile = {16, 512, 8};
   bool tune = true;
   int forced_dm_block = 0, forced_time_block = 0;  // HDB_DEDISP_TILE="DBxTB"
@@ -44,6 +45,22 @@ struct dedisp_plan_struct {
   float* d_dm_list = nullptr;
   unsigned* d_err = nullptr;
   int device = -1;
+
+  // adaptive dt: trials [d0, d1) share scrunch factor s and are dedispersed
+  // at sampling time s dt from the scrunched input with delays delay / s
+  // (one group of factor 1 over all trials when adaptive dt is off)
+  struct Group {
+    size_t d0 = 0, d1 = 0, s = 1;
+    size_t max_delay = 0;            // largest scrunched delay of the group
+    size_t max_span[3] = {0, 0, 0};  // per DM-block size
+    std::vector<int> delays;         // [d1 - d0][chan]
+    std::vector<int> blk_min[3];
+    int* d_delays = nullptr;
+    int* d_blk_min[3] = {nullptr, nullptr, nullptr};
+  };
+  std::vector<Group> groups;          // built only with adaptive dt
+  uint8_t* d_scr = nullptr;           // scrunched channel-major input
+  size_t d_scr_cap = 0;
 
   // scratch for dedisp_execute* with host pointers
   uint8_t* d_in_tf = nullptr;
@@ -61,6 +78,11 @@ namespace hdb {
 
 // include/dedisp.h restatement (float arithmetic as documented there).
 void delay_table(size_t nchans, float dt, float f0, float df, float* table);
+// Per-trial scrunch factors of adaptive dt (include/dedisp.h documents the
+// rule).
+std::vector<dedisp_size> scrunch_factors(const std::vector<float>& dm_list, double dt,
+                                         double ti, double f0, double df, size_t nchans,
+                                         double tol);
 size_t delay_of(float dm, float table_c);
 std::vector<float> generate_dm_list(float dm_start, float dm_end, double dt, double ti,
                                     double f0, double df, size_t nchans, double tol);

@@ -25,6 +25,19 @@
  *   delay(d, c)    = (dedisp_size)(dm_list[d] * delay_table[c] + 0.5f)
  *   out[d][t]      = (float) sum_c killmask[c] * in[t + delay(d,c)][c],
  *                    t in [0, nsamps - max_delay), summed exactly in int32.
+ * With adaptive dt, trial d has a scrunch factor s_d (dedisp_get_dt_factors)
+ * and is computed at sampling time s_d dt:
+ *   in_s[c][u]     = (sum_{j<s} in[s u + j][c] + s/2) / s   (byte mean,
+ *                    rounded half up), u < nsamps / s;
+ *   out[d][u]      = (float) sum_c killmask[c] * in_s[c][u + delay(d,c) / s],
+ *                    u in [0, (nsamps - max_delay) / s)   (integer divisions);
+ * the rest of row d is left as it was.  Scrunch factors (the rule of
+ * Barsdell et al. 2012, MNRAS 422, 379, restated; unpinned): the smearing of
+ * trial DM at sampling time T is W(DM, T)^2 = T^2 + pulse_width^2 +
+ * (a DM)^2 in microseconds, with the DM-list generator's a = 8.3 df / f^3
+ * (df in MHz, f in GHz at the band centre); factors start at 1, never
+ * decrease, and trial d doubles the previous factor s when
+ * W(DM_d, 2 s dt) / W(DM_d, s dt) < tol.
  */
 #ifndef HEIMDALL_B200_DEDISP_H
 #define HEIMDALL_B200_DEDISP_H
@@ -95,8 +108,9 @@ const dedisp_float* dedisp_generate_dm_list_guru(dedisp_float dm_start, dedisp_f
 /* Channel killmask: nchans ints, 0 = channel excluded.  pipeline.cu:363 */
 dedisp_error dedisp_set_killmask(dedisp_plan plan, const dedisp_bool* killmask);
 
-/* Adaptive time resolution (per-DM power-of-two scrunch).  pipeline.cu:190,
- * clean_filterbank_rfi.cu:369 */
+/* Adaptive time resolution (per-DM power-of-two scrunch, rule above);
+ * tol must exceed 1.  The factors follow later changes of the DM list.
+ * pipeline.cu:190, clean_filterbank_rfi.cu:369 */
 dedisp_error dedisp_enable_adaptive_dt(dedisp_plan plan, dedisp_float pulse_width,
                                        dedisp_float tol);
 dedisp_error dedisp_disable_adaptive_dt(dedisp_plan plan);

@@ -28,7 +28,8 @@
  * (hd_read_sigproc_header, hd_mjd_to_utc, hd_params_from_sigproc,
  * hd_search_sigproc_file, hd_search_sigproc_files); the coincidencer (hd_coincide,
  * hd_write_coincident_candidates); the candidate classifier
- * (hd_extract_patches, hd_score_candidates, hd_classifier_*).
+ * (hd_extract_patches, hd_score_candidates, hd_classifier_*); the candidate
+ * profiler (hd_profile_candidates, Applications/candidate_profiler.C).
  *
  * Ownership and threading: the caller owns every host buffer it passes; the
  * pipeline owns all device memory, its CUDA stream and events.  A pipeline
@@ -177,9 +178,10 @@ hd_error hd_clean_filterbank_rfi(hd_pipeline pipeline, const hd_byte* h_in, hd_s
 
 /* ---- additions ---------------------------------------------------------- */
 
-/* Switches the zero-DM RFI cleaning stage on (default) or off.  The reference
- * selects it at compile time (Pipeline/pipeline.cu:72-74,255-299, #ifdef
- * CLEANING); its shipped build leaves it off. */
+/* Switches the zero-DM RFI cleaning stage on or off (default: off).  The
+ * reference selects it at compile time (Pipeline/pipeline.cu:72-74,255-299,
+ * #ifdef CLEANING) and its shipped build leaves it off; enabling it here is
+ * the reference built with -DCLEANING. */
 hd_error hd_set_cleaning(hd_pipeline pipeline, int enable);
 /* Narrow-band RFI zapping before the broadband stage when cleaning is on: the
  * branch of Pipeline/clean_filterbank_rfi.cu:303-351 that the reference
@@ -258,6 +260,54 @@ hd_error hd_clean_filterbank_rfi_noalloc(const hd_byte* d_in, hd_size nsamps, hd
                                          hd_float rfi_tol, hd_size boxcar_max, hd_size nbeams,
                                          void* stream, unsigned* d_status);
 
+/* ---- Candidate profiler (Applications/candidate_profiler.C) on the GPU ----
+ *
+ * The reference's candidate_profiler application makes, for one candidate of
+ * a sigproc file, a DM-time plot (candidate_profiler.C:232-415, the trials
+ * around the candidate re-dedispersed over a window of the file with adaptive
+ * dt), a DM-0 series, a freq-time plot (:136-230), SNR vs DM and SNR vs time
+ * (:560-640), and writes them to freq_time.dat, snr_dm.dat, snr_time.dat and
+ * dm_time.pgm.  hd_profile_candidates computes the same arrays on the GPU for
+ * a batch of candidates of one filterbank (nsamps x nchans bytes, 8-bit,
+ * time-major; host memory, or device memory with on_device) whose header
+ * values are tsamp, fch1 and foff, with the DM list dm_list.  Samples past the
+ * end of the filterbank read as 0, as past the end of the file; a freq-time
+ * window that would start before the first sample reads 0 there.  Rows with
+ * no deviation come out NaN or +-inf (the reference's division by zero).
+ * Per candidate (out[i]; any array may be NULL):
+ *   dm_time   out_dm_count x out_nsamps: rows [0, n_dm) are trials
+ *             dm_begin ... of the window, later rows 0;
+ *   dm0_time  out_nsamps;
+ *   freq_time (nchans / fscrunch) x out_nsamps;
+ *   max_idx   index of the first maximum of dm_time;
+ *   snr_dm    out_dm_count: dm_time at max_idx's time for trial
+ *             snr_dm_first + d (0 for d >= n_dm);
+ *   snr_time  out_nsamps x 5: time (s), dm_time on max_idx's row, on the rows
+ *             above and below it (0 outside the plot), and dm0_time.
+ * Limits: out_nsamps in [2, 4096], nchans a multiple of fscrunch, at most
+ * 65535 dedispersed rows (candidates x (window trials + 1)) per call.  The
+ * call allocates its device memory and returns when the results are on the
+ * host. */
+typedef struct hd_profile_request {
+  hd_size samp;     /* sample index of the candidate in the filterbank */
+  hd_size filter;   /* boxcar width index (width 2^filter) */
+  hd_size dm_idx;   /* trial of dm_list */
+} hd_profile_request;
+typedef struct hd_profile {
+  hd_float* dm_time;
+  hd_float* dm0_time;
+  hd_float* freq_time;
+  hd_float* snr_dm;
+  hd_float* snr_time;
+  hd_size   max_idx, n_dm, dm_begin, snr_dm_first;
+} hd_profile;
+hd_error hd_profile_candidates(const hd_byte* filterbank, hd_size nsamps, hd_size nchans,
+                               int on_device, double tsamp, double fch1, double foff,
+                               const hd_float* dm_list, hd_size dm_count,
+                               const hd_profile_request* cands, hd_size ncands,
+                               hd_size out_nsamps, hd_size out_dm_count, hd_size fscrunch,
+                               int do_filter, hd_profile* out);
+
 /* ---- Learned candidate classifier (no counterpart in the reference) ----
  *
  * Patches per candidate (float, row-major): a DM-time patch of 64 DM trials
@@ -279,8 +329,10 @@ typedef struct hd_classifier_t* hd_classifier;
 /* Patches of every candidate of the last hd_execute / hd_execute_beams, in
  * hd_get_candidates order.  Copies min(*count, available) patches (either
  * output may be NULL) and sets *count to the number available.  Needs
- * nchans a multiple of 64.  Call before the next execute (it reads that
- * gulp's device buffers). */
+ * nchans a multiple of 64 and a gulp searched at the native resolution
+ * (HD_INVALID_STRIDE after a gulp with adaptive dt, whose trials have
+ * different lengths).  Call before the next execute (it reads that gulp's
+ * device buffers). */
 hd_error hd_extract_patches(hd_pipeline pipeline, hd_float* dm_time, hd_float* freq_time,
                             hd_size* count);
 

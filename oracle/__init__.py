@@ -608,3 +608,62 @@ def set_narrow_band(enable: bool) -> None:
     """Whether the oracle's cleaning runs the narrow-band branch first."""
     lib().or_set_narrow_band(1 if enable else 0)
 
+
+
+# ---------------------------------------------------------------------------
+# Candidate profiler restatement (oracle/profiler.c) and the reference's own
+# application (oracle/_ref/ref_profiler)
+# ---------------------------------------------------------------------------
+REF_PROFILER = os.path.join(HERE, "_ref", "ref_profiler")
+
+
+def profile(fb: np.ndarray, tsamp: float, fch1: float, foff: float, dm_list, samp: int,
+            filt: int, dm_idx: int, out_nsamps: int, out_dm_count: int, fscrunch: int,
+            do_filter: bool = False) -> dict:
+    """or_profile: the candidate profiler's plots and extractions."""
+    L = lib()
+    fb = np.ascontiguousarray(fb, dtype=np.uint8)
+    nsamps, nchans = fb.shape
+    dms = np.ascontiguousarray(dm_list, np.float32)
+    dm_time = np.zeros((out_dm_count, out_nsamps), np.float32)
+    dm0 = np.zeros(out_nsamps, np.float32)
+    ft = np.zeros((nchans // fscrunch, out_nsamps), np.float32)
+    snr_dm = np.zeros(out_dm_count, np.float32)
+    snr_time = np.zeros((out_nsamps, 5), np.float32)
+    mx = C.c_size_t(0)
+    first = C.c_size_t(0)
+    L.or_profile.restype = C.c_size_t
+    L.or_profile.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_double, C.c_double,
+                             C.c_double, _fp, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t,
+                             C.c_size_t, C.c_size_t, C.c_size_t, C.c_int, _fp, _fp, _fp, _szp,
+                             _szp, _fp, _fp]
+    n = L.or_profile(fb.ctypes.data, nsamps, nchans, tsamp, fch1, foff, _fptr(dms), len(dms),
+                     samp, filt, dm_idx, out_nsamps, out_dm_count, fscrunch, int(do_filter),
+                     _fptr(dm_time), _fptr(dm0), _fptr(ft), C.byref(mx), C.byref(first),
+                     _fptr(snr_dm), _fptr(snr_time))
+    return dict(n_dm=int(n), dm_time=dm_time, dm0_time=dm0, freq_time=ft, max_idx=mx.value,
+                snr_dm_first=first.value, snr_dm=snr_dm, snr_time=snr_time)
+
+
+def ref_profiler_available() -> bool:
+    return os.path.exists(REF_PROFILER)
+
+
+def ref_profile(path: str, dm_list, samp: int, filt: int, dm_idx: int, out_nsamps: int,
+                out_dm_count: int, fscrunch: int, do_filter: bool = False) -> dict:
+    """Runs the reference's candidate_profiler on a sigproc file; returns the
+    text of the files it writes (freq_time.dat, snr_dm.dat, snr_time.dat,
+    dm_time.pgm) as lists of lines."""
+    with tempfile.TemporaryDirectory() as d:
+        dml = os.path.join(d, "dm.list")
+        with open(dml, "w") as f:
+            for v in np.asarray(dm_list, np.float32):
+                f.write("%.9g\n" % float(v))
+        args = [REF_PROFILER, os.path.abspath(path), dml, str(samp), str(filt), str(dm_idx),
+                str(out_nsamps), str(out_dm_count), str(fscrunch), str(int(do_filter))]
+        subprocess.run(args, cwd=d, check=True, capture_output=True)
+        out = {}
+        for name in ("freq_time.dat", "snr_dm.dat", "snr_time.dat", "dm_time.pgm"):
+            p = os.path.join(d, name)
+            out[name] = open(p).read().splitlines() if os.path.exists(p) else None
+    return out

@@ -154,6 +154,21 @@ int  or64_giant_snr(const or_params* p, const uint8_t* fb, size_t nsamps, size_t
                     size_t n, const size_t* dm_inds, const size_t* filter_inds,
                     const size_t* inds, double* snr);
 
+/* ---- candidate profiler (Applications/candidate_profiler.C; profiler.c) ---- */
+int    or_profile_ft(const uint8_t* fb, size_t nsamps, size_t nchans, float dt, float f0,
+                     float df, size_t samp, size_t filter, float dm, size_t out_nsamps,
+                     size_t fscrunch, float* out);
+size_t or_profile_dm(const uint8_t* fb, size_t nsamps, size_t nchans, float dt, float f0,
+                     float df, const float* dm_list, size_t dm_count, size_t samp,
+                     size_t filter, size_t dm_idx, size_t out_nsamps, size_t out_dm_count,
+                     int do_filter, float* out, size_t* dm_begin_out);
+size_t or_profile(const uint8_t* fb, size_t nsamps, size_t nchans, double tsamp, double fch1,
+                  double foff, const float* dm_list, size_t dm_count, size_t samp,
+                  size_t filter, size_t dm_idx, size_t out_nsamps, size_t out_dm_count,
+                  size_t fscrunch, int do_filter, float* dm_time, float* dm0_time,
+                  float* freq_time, size_t* max_idx_out, size_t* snr_dm_first, float* snr_dm,
+                  float* snr_time);
+
 /* ---- classifier (Applications/candidate_profiler.C and the CNN) ---- */
 void or_normalise_rows(float* data, size_t n, size_t nrows);
 void or_patch_dm(const float* scans, size_t pitch, size_t len, size_t ndm, size_t dm,

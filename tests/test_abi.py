@@ -62,6 +62,8 @@ int main(void) {{
                                        (hdb.HdCandidate, "hd_candidate"),
                                        (hdb.HdSigprocHeader, "hd_sigproc_header"),
                                        (hdb.HdCoincidence, "hd_coincidence"),
+                                       (hdb.HdProfileRequest, "hd_profile_request"),
+                                       (hdb.HdProfile, "hd_profile"),
                                        (hdb.RawCandidates, "struct RawCandidates")])
 def test_struct_layout_matches_c(cls, cname):
     fields = [f for f, _ in cls._fields_]

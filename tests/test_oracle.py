@@ -196,3 +196,55 @@ def test_oracle_equals_reference_survey_gulp(oracle_lib):
     assert err == 0 and proc == r["nsamps_processed"]
     assert len(lines) >= 5
     assert lines == ref_lines
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["c0", "c0_clean", "headline_beam", "stf4"])
+def test_oracle_equals_reference_adaptive_dt(oracle_lib, case):
+    """use_scrunching = 1: the reference pipeline's own scrunched path
+    (pipeline.cu:489-775 with per-trial factors > 1: scrunched series and
+    strides, widths from the factor up, indices rescaled by factor x
+    tscrunch) run on the CPU dedisperser with the restated adaptive-dt rule
+    writes the same .cand lines as the restatement."""
+    if case.startswith("c0"):
+        w = synth.SEARCH_C0
+        fb, nbeams = synth.make_c0().data, 1
+        kw = _small_params(w, clean=int(case == "c0_clean"))
+    elif case == "headline_beam":
+        w = synth.SEARCH_C2
+        fb, nbeams = synth.make_multibeam(w, seed=2026)[0].data, 1
+        kw = _small_params(w, clean=0)
+    else:
+        w = synth.Workload("mb_small", 64, 655.36e-6, 851.0, -0.390625, 8192, 4, 0.0, 600.0,
+                           256, False, "")
+        fb = synth.stf(synth.make_multibeam(w, seed=7, snr_lo=15, snr_hi=30))
+        nbeams = 4
+        kw = _small_params(w, clean=1, baseline_length=1.0)
+    kw["use_scrunching"] = 1
+    r = oracle.execute(fb, nbeams=nbeams, **kw)
+    assert int(r["scrunch"].max()) >= 2
+    lines = oracle.cand_lines(r["groups"], fb.shape[0], nbeams, 0, r["nsamps_processed"],
+                              w.boxcar_max, w.dt)
+    err, proc, ref_lines, _ = oracle.ref_execute(fb, nbeams=nbeams, nthreads=1, **kw)
+    assert err == 0 and proc == r["nsamps_processed"]
+    assert len(lines) >= 3
+    assert lines == ref_lines
+
+
+def test_scrunch_factors_rule(oracle_lib):
+    """The restated rule: factors start at 1, never decrease, only double,
+    and a trial doubles exactly when the smearing at twice the previous
+    sampling time is below tol times that at the previous one."""
+    w = synth.SEARCH_C1
+    dms = oracle.dm_list(0.0, 2000.0, w.dt, 40.0, w.f0, w.df, w.nchans, 1.25)
+    sc = oracle.scrunch_factors(dms, w.dt, 40.0, w.f0, w.df, w.nchans, 1.15).astype(np.int64)
+    assert sc[0] == 1 and np.all(np.diff(sc) >= 0)
+    assert set(np.unique(sc[1:] // sc[:-1])) <= {1, 2}
+    f = (w.f0 + (w.nchans // 2 - 0.5) * w.df) * 1e-3
+    a = 8.3 * w.df / f ** 3
+    for d in range(1, len(dms)):
+        s = sc[d - 1]
+        w1 = np.sqrt((s * w.dt * 1e6) ** 2 + 40.0 ** 2 + (a * float(dms[d])) ** 2)
+        w2 = np.sqrt((2 * s * w.dt * 1e6) ** 2 + 40.0 ** 2 + (a * float(dms[d])) ** 2)
+        assert sc[d] == (2 * s if w2 / w1 < 1.15 else s), d
+    assert sc[-1] >= 8
