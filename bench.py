@@ -932,10 +932,10 @@ def main():
                     help="beams of the multibeam gulp (fewer are for profiling)")
     ap.add_argument("--batched-only", action="store_true",
                     help="time only the batched form (profiling)")
-    ap.add_argument("--uneven-beams", type=int, default=64,
-                    help="beams of the uneven-beam section (0 skips it; 256 is the full size)")
-    ap.add_argument("--uneven-nsamps-max", type=int, default=1 << 16,
-                    help="longest gulp of the uneven-beam section (2^17 at full size)")
+    ap.add_argument("--uneven-beams", type=int, default=256,
+                    help="beams of the uneven-beam section (0 skips it)")
+    ap.add_argument("--uneven-nsamps-max", type=int, default=1 << 17,
+                    help="longest gulp of the uneven-beam section")
     ap.add_argument("--uneven-workers", type=int, default=4)
     ap.add_argument("--uneven-steps", type=int, default=2)
     ap.add_argument("--no-classifier", action="store_true",

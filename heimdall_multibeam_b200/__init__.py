@@ -224,6 +224,9 @@ SYMBOLS = {
     "hd_bf16_gemm": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, C.c_longlong, C.c_longlong, _P,
                                C.c_longlong, C.c_longlong, _FP, C.c_longlong, C.c_longlong,
                                C.c_int, C.c_int]),
+    "hd_bf16_gemm_tc": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, C.c_longlong, C.c_longlong, _P,
+                               C.c_longlong, C.c_longlong, _FP, C.c_longlong, C.c_longlong,
+                               C.c_int, C.c_int]),
     "dedisp_create_plan": (C.c_int, [C.POINTER(_P), _SZ, C.c_float, C.c_float, C.c_float]),
     "dedisp_destroy_plan": (None, [_P]),
     "dedisp_set_dm_list": (C.c_int, [_P, _FP, _SZ]),

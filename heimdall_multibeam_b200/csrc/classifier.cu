@@ -181,6 +181,27 @@ __global__ void k_im2col3(const bf16* __restrict__ in, int ci, int nb, int h, in
   col[i] = v;
 }
 
+// im2col in K-major order for the tensor-core GEMM: colT [b*h*w][kp], the kp
+// taps of one output pixel contiguous (the same values as k_im2col3)
+__global__ void k_im2col3_t(const bf16* __restrict__ in, int ci, int nb, int h, int w, int kp,
+                            bf16* __restrict__ colT) {
+  const size_t P = (size_t)nb * h * w;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P * kp) return;
+  const size_t p = i / kp;
+  const int r = (int)(i % kp);
+  bf16 v = __float2bfloat16(0.f);
+  if (r < ci * 9) {
+    const int c = r / 9, ky = (r % 9) / 3, kx = r % 3;
+    const int x = (int)(p % w), y = (int)((p / w) % h);
+    const size_t b = p / ((size_t)w * h);
+    const int yy = y + ky - 1, xx = x + kx - 1;
+    if (yy >= 0 && yy < h && xx >= 0 && xx < w)
+      v = in[(((size_t)c * nb + b) * h + yy) * w + xx];
+  }
+  colT[i] = v;
+}
+
 // col2im: dcol [kp][b*h*w] (FP32) -> din [ci][b][h][w], summing the 9 taps
 // that read each input pixel
 __global__ void k_col2im3(const float* __restrict__ dcol, int ci, int nb, int h, int w,
@@ -248,19 +269,40 @@ __global__ void k_pool_relu_back(const float* __restrict__ dact, const bf16* __r
     if (y / 2 < h2 && x / 2 < w2 && arg[j] == q && __bfloat162float(act[j]) > 0.f) v = dact[j];
     dz[i] = __float2bfloat16(v);
   }
-  // per-block partial bias sums (a block may span two channels)
-  __shared__ float s_sum[2];
-  __shared__ int s_c0;
-  if (threadIdx.x == 0) {
-    s_sum[0] = s_sum[1] = 0.f;
-    const size_t i0 = (size_t)blockIdx.x * blockDim.x;
-    s_c0 = (int)(i0 / ((size_t)w * h) / nb);
+  (void)c;
+  (void)dbias;
+}
+
+// bias gradient of the same layer: dbias[c] += the sum over c's pixels of the
+// pre-activation gradient, one block per channel, in a fixed order (each
+// thread's strided partial, then a fixed tree), so every run gives the same
+// bits
+__global__ void __launch_bounds__(256) k_bias_grad(const float* __restrict__ dact,
+                                                   const bf16* __restrict__ act,
+                                                   const unsigned char* __restrict__ arg,
+                                                   int nb, int h, int w,
+                                                   float* __restrict__ dbias) {
+  __shared__ float part[256];
+  const int c = blockIdx.x;
+  const int h2 = h / 2, w2 = w / 2;
+  const size_t per = (size_t)nb * h * w;
+  float acc = 0.f;
+  for (size_t k = threadIdx.x; k < per; k += blockDim.x) {
+    const size_t i = (size_t)c * per + k;
+    const int x = (int)(i % w), y = (int)((i / w) % h);
+    const size_t cb = i / ((size_t)w * h);
+    const size_t j = (cb * h2 + y / 2) * w2 + x / 2;
+    const int q = (y & 1) * 2 + (x & 1);
+    if (y / 2 < h2 && x / 2 < w2 && arg[j] == q && __bfloat162float(act[j]) > 0.f)
+      acc = __fadd_rn(acc, dact[j]);
   }
+  part[threadIdx.x] = acc;
   __syncthreads();
-  if (c >= 0 && v != 0.f) atomicAdd(&s_sum[c - s_c0 > 0 ? 1 : 0], v);
-  __syncthreads();
-  if (threadIdx.x < 2 && s_sum[threadIdx.x] != 0.f && s_c0 + (int)threadIdx.x < co)
-    atomicAdd(&dbias[s_c0 + threadIdx.x], s_sum[threadIdx.x]);
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) part[threadIdx.x] = __fadd_rn(part[threadIdx.x], part[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) dbias[c] = __fadd_rn(dbias[c], part[0]);
 }
 
 // pooled activations of both branches -> x [b][10240] (A: 2048, B: 8192)
@@ -304,11 +346,14 @@ __global__ void k_fc1_act(const float* __restrict__ z1, const float* __restrict_
 // FC2, softmax, cross-entropy and their backward, FC2 weight/bias gradients,
 // the FC1 pre-activation gradient dz1 [16][b] (BF16) and its bias gradient.
 // One thread per sample; w2 [2][16], b2 [2].
+// The per-sample terms of the loss and of the FC2/FC1-bias gradients go to
+// hs [b][18] (loss / nb, dL/dl1, the 16 dz) and k_head_reduce sums them over
+// the batch in sample order.
+constexpr int kHeadTerms = 18;
 __global__ void k_head(const float* __restrict__ h, const float* __restrict__ w2,
                        const float* __restrict__ b2, const int* __restrict__ labels, int nb,
-                       int backward, float* __restrict__ prob, float* __restrict__ loss,
-                       float* __restrict__ gw2, float* __restrict__ gb2, bf16* __restrict__ dz1,
-                       float* __restrict__ gb1) {
+                       int backward, float* __restrict__ prob, bf16* __restrict__ dz1,
+                       float* __restrict__ hs) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nb) return;
   const float* hn = h + n * 16;
@@ -324,19 +369,43 @@ __global__ void k_head(const float* __restrict__ h, const float* __restrict__ w2
   if (!backward) return;
   const int y = labels[n];
   const float lse = mx + logf(e0 + e1);
-  atomicAdd(loss, (lse - (y ? l1 : l0)) / nb);
+  float* t = hs + (size_t)n * kHeadTerms;
+  t[0] = (lse - (y ? l1 : l0)) / nb;
   const float d1 = (p1 - (y ? 1.f : 0.f)) / nb;  // dL/dl1; dL/dl0 = -d1
   const float d0 = -d1;
-  atomicAdd(&gb2[0], d0);
-  atomicAdd(&gb2[1], d1);
+  t[1] = d1;
   for (int o = 0; o < 16; o++) {
-    atomicAdd(&gw2[o], d0 * hn[o]);
-    atomicAdd(&gw2[16 + o], d1 * hn[o]);
     const float dh = d0 * w2[o] + d1 * w2[16 + o];
     const float dz = hn[o] > 0.f ? dh : 0.f;
     dz1[o * nb + n] = __float2bfloat16(dz);
-    atomicAdd(&gb1[o], dz);
+    t[2 + o] = dz;
   }
+}
+
+// loss (+= the per-sample terms), gb2, gw2 [2][16] and gb1 [16] from hs and
+// h, each a sum over the samples in order (thread per output)
+__global__ void k_head_reduce(const float* __restrict__ h, const float* __restrict__ hs, int nb,
+                              float* __restrict__ loss, float* __restrict__ gw2,
+                              float* __restrict__ gb2, float* __restrict__ gb1) {
+  const int k = threadIdx.x;  // 0: loss, 1-2: gb2, 3-34: gw2, 35-50: gb1
+  if (k > 50) return;
+  float acc = 0.f;
+  for (int n = 0; n < nb; n++) {
+    const float* t = hs + (size_t)n * kHeadTerms;
+    const float d1 = t[1], d0 = -d1;
+    float v;
+    if (k == 0) v = t[0];
+    else if (k == 1) v = d0;
+    else if (k == 2) v = d1;
+    else if (k < 19) v = d0 * h[n * 16 + (k - 3)];
+    else if (k < 35) v = d1 * h[n * 16 + (k - 19)];
+    else v = t[2 + (k - 35)];
+    acc = __fadd_rn(acc, v);
+  }
+  if (k == 0) loss[0] = __fadd_rn(loss[0], acc);
+  else if (k < 3) gb2[k - 1] = __fadd_rn(gb2[k - 1], acc);
+  else if (k < 35) gw2[k - 3] = __fadd_rn(gw2[k - 3], acc);
+  else gb1[k - 35] = __fadd_rn(gb1[k - 35], acc);
 }
 
 // per-sample batch gather: dataset [n][len] (BF16) rows idx -> [b][len]
@@ -846,7 +915,8 @@ struct hd_classifier_t {
   // per-batch work buffers
   int cap_batch = 0;
   DBuf in[2], col, z, act[2][3], arg[2][3], dz, dcol, dact_a[2], dact_b[2], x, z1, h, dz1,
-      dx, prob, loss, labels, idx;
+      dx, prob, loss, labels, idx, hs;
+  DBuf tc_ws, tc_err;               // tensor-core GEMM: split-K workspace, error word
   DBuf data_dm, data_ft, data_lab;  // resident training set
   DBuf stage_dm, stage_ft, sprob;    // scoring: host patches staged in FP32, scores
   int nsm = 0;
@@ -899,6 +969,7 @@ cudaError_t alloc_batch(hd_classifier c, int nb) {
   CK(c->h.ensure((size_t)nb * kHid * sizeof(float)));
   CK(c->dz1.ensure((size_t)nb * kHid * sizeof(bf16)));
   CK(c->prob.ensure((size_t)nb * sizeof(float)));
+  CK(c->hs.ensure((size_t)nb * kHeadTerms * sizeof(float)));
   CK(c->loss.ensure(sizeof(float)));
   CK(c->labels.ensure((size_t)nb * sizeof(int)));
   CK(c->idx.ensure((size_t)nb * sizeof(int)));
@@ -924,6 +995,19 @@ cudaError_t refresh_bf16(hd_classifier c) {
   return cudaGetLastError();
 }
 
+// C(m, n) (+)= sum_k A[m*lda + k] B[n*ldb + k] on the tcgen05 tensor cores
+// (umma_gemm): both operands K-major; split K over `splits` CTAs per tile
+// column, the splits added in order through c->tc_ws.
+cudaError_t tc_gemm(hd_classifier c, int M, int N, int K, const bf16* A, long long lda,
+                    const bf16* B, long long ldb, float* C, long long scm, long long scn,
+                    int accumulate, int splits) {
+  const size_t ws = hdb::umma_workspace_floats(M, N, K, splits);
+  CK(c->tc_ws.ensure(std::max<size_t>(ws, 1) * sizeof(float)));
+  CK(c->tc_err.ensure(sizeof(unsigned)));
+  return hdb::umma_gemm(M, N, K, A, lda, B, ldb, C, scm, scn, accumulate, splits,
+                        c->tc_ws.as<float>(), c->tc_err.as<unsigned>(), c->stream);
+}
+
 // Forward over the batch already in c->in[]; with backward, accumulates the
 // gradients of the mean cross-entropy into c->g (which the caller zeroes).
 cudaError_t run_batch(hd_classifier c, int nb, bool backward) {
@@ -937,11 +1021,13 @@ cudaError_t run_batch(hd_classifier c, int nb, bool backward) {
     for (int l = 0; l < 3; l++) {
       const ConvSpec& sp = kConv[br][l];
       const size_t P = (size_t)nb * sp.h * sp.w;
-      k_im2col3<<<nblk(P * sp.kp()), 256, 0, s>>>(cur, sp.ci, nb, sp.h, sp.w, sp.kp(),
-                                                   c->col.as<bf16>()); hdb::note_launch();
-      GemmArgs ga{sp.co, (int)P, sp.kp(), c->wb_conv[br][l].as<bf16>(), sp.kp(), 1,
-                  c->col.as<bf16>(), (long long)P, 1, c->z.as<float>(), (long long)P, 1, 0, 0};
-      CK(gemm(ga, 1, s));
+      // z [co][P] = W [co][kp] x col: on the tensor cores as z^T [P][co] =
+      // colT [P][kp] x W^T, M = P pixels, N = co, K = kp
+      k_im2col3_t<<<nblk(P * sp.kp()), 256, 0, s>>>(cur, sp.ci, nb, sp.h, sp.w, sp.kp(),
+                                                     c->col.as<bf16>()); hdb::note_launch();
+      CK(tc_gemm(c, (int)P, sp.co, sp.kp(), c->col.as<bf16>(), sp.kp(),
+                 c->wb_conv[br][l].as<bf16>(), sp.kp(), c->z.as<float>(), 1, (long long)P, 0,
+                 1));
       k_bias_relu_pool<<<nblk(P / 4 * sp.co), 256, 0, s>>>(
           c->z.as<float>(), w + c->off_b[br][l], sp.co, nb, sp.h, sp.w,
           c->act[br][l].as<bf16>(), c->arg[br][l].as<unsigned char>()); hdb::note_launch();
@@ -951,19 +1037,19 @@ cudaError_t run_batch(hd_classifier c, int nb, bool backward) {
   k_flatten<<<nblk((size_t)nb * kFeat), 256, 0, s>>>(c->act[0][2].as<bf16>(),
                                                      c->act[1][2].as<bf16>(), nb,
                                                      c->x.as<bf16>()); hdb::note_launch();
-  {
-    GemmArgs ga{kHid, nb, kFeat, c->wb1.as<bf16>(), kFeat, 1, c->x.as<bf16>(), 1, kFeat,
-                c->z1.as<float>(), nb, 1, 0, 0};
-    CK(gemm(ga, 1, s));
-  }
+  // z1 [16][b] = W1 x x: z1^T [b][16] = x [b][10240] x W1^T, K split over 64
+  CK(tc_gemm(c, nb, kHid, kFeat, c->x.as<bf16>(), kFeat, c->wb1.as<bf16>(), kFeat,
+             c->z1.as<float>(), 1, nb, 0, 64));
   k_fc1_act<<<nblk((size_t)nb * kHid), 256, 0, s>>>(c->z1.as<float>(), w + c->off_b1, nb,
                                                     c->h.as<float>()); hdb::note_launch();
   if (backward) CK(cudaMemsetAsync(c->loss.p, 0, sizeof(float), s));
   k_head<<<nblk(nb, 128), 128, 0, s>>>(c->h.as<float>(), w + c->off_w2, w + c->off_b2,
                                        c->labels.as<int>(), nb, backward ? 1 : 0,
-                                       c->prob.as<float>(), c->loss.as<float>(), g + c->off_w2,
-                                       g + c->off_b2, c->dz1.as<bf16>(), g + c->off_b1); hdb::note_launch();
+                                       c->prob.as<float>(), c->dz1.as<bf16>(),
+                                       c->hs.as<float>()); hdb::note_launch();
   if (!backward) return cudaGetLastError();
+  k_head_reduce<<<1, 64, 0, s>>>(c->h.as<float>(), c->hs.as<float>(), nb, c->loss.as<float>(),
+                                 g + c->off_w2, g + c->off_b2, g + c->off_b1); hdb::note_launch();
   // ---- backward ----
   {
     // dW1 [16][10240] += dz1 [16][b] x x [b][10240]
@@ -987,16 +1073,21 @@ cudaError_t run_batch(hd_classifier c, int nb, bool backward) {
       k_pool_relu_back<<<nblk(P * sp.co), 256, 0, s>>>(
           dcur, c->act[br][l].as<bf16>(), c->arg[br][l].as<unsigned char>(), sp.co, nb, sp.h,
           sp.w, c->dz.as<bf16>(), g + c->off_b[br][l]); hdb::note_launch();
+      k_bias_grad<<<sp.co, 256, 0, s>>>(dcur, c->act[br][l].as<bf16>(),
+                                        c->arg[br][l].as<unsigned char>(), nb, sp.h, sp.w,
+                                        g + c->off_b[br][l]); hdb::note_launch();
       // the layer's input again, as im2col (recomputed rather than stored)
       const bf16* lin = l == 0 ? c->in[br].as<bf16>() : c->act[br][l - 1].as<bf16>();
       k_im2col3<<<nblk(P * sp.kp()), 256, 0, s>>>(lin, sp.ci, nb, sp.h, sp.w, sp.kp(),
                                                    c->col.as<bf16>()); hdb::note_launch();
       // dW [co][kw] += dz [co][P] x col^T; the padded columns kw..kp are dropped
       // by writing into a [co][kp] scratch is avoided: N = kw with row stride kw
-      GemmArgs gw{sp.co, sp.kw(), (int)P, c->dz.as<bf16>(), (long long)P, 1, c->col.as<bf16>(),
-                  1, (long long)P, g + c->off_w[br][l], sp.kw(), 1, 0, 0};
-      const int splits = (int)std::min<size_t>(256, (P + 4095) / 4096);
-      CK(gemm(gw, splits, s));
+      // on the tensor cores as dW^T [kw][co] += col [kw][P] x dz^T: M = kw
+      // taps, N = co, K = P pixels split over the SMs; the splits are added
+      // in order (the same gradient every run)
+      const int splits = (int)std::min<size_t>(296, (P + 8191) / 8192);
+      CK(tc_gemm(c, sp.kw(), sp.co, (int)P, c->col.as<bf16>(), (long long)P, c->dz.as<bf16>(),
+                 (long long)P, g + c->off_w[br][l], 1, sp.kw(), 1, splits));
       if (l > 0) {
         // dcol [kp][P] = W^T x dz, then col2im into the previous layer's output gradient
         GemmArgs gd{sp.kp(), (int)P, sp.co, c->wb_conv[br][l].as<bf16>(), 1, sp.kp(),
@@ -1087,6 +1178,17 @@ cudaError_t score_batches(hd_classifier c, const float* dm, const float* ft, siz
   CK(cudaEventRecord(c->ev[1], s));
   CK(cudaStreamSynchronize(s));
   return cudaEventElapsedTime(&c->score_ms, c->ev[0], c->ev[1]);
+}
+
+// the tensor-core GEMM's error word: zeroed before a run, read after it
+cudaError_t tc_reset(hd_classifier c) {
+  CK(c->tc_err.ensure(sizeof(unsigned)));
+  return cudaMemsetAsync(c->tc_err.p, 0, sizeof(unsigned), c->stream);
+}
+cudaError_t tc_check(hd_classifier c) {
+  unsigned v = 0;
+  CK(cudaMemcpy(&v, c->tc_err.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return v ? cudaErrorLaunchTimeout : cudaSuccess;
 }
 
 hd_error to_hd(cudaError_t e) {
@@ -1191,6 +1293,7 @@ hd_error hd_classifier_gradients(hd_classifier c, const float* dm_time, const fl
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
   cudaError_t e = alloc_batch(c, (int)n);
+  if (e == cudaSuccess) e = tc_reset(c);
   if (e == cudaSuccess) e = upload_patches(c, dm_time, freq_time, (int)n);
   if (e == cudaSuccess) e = cudaMemcpyAsync(c->labels.p, labels, n * sizeof(int), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->g.p, 0, c->nparam * sizeof(float), s);
@@ -1199,6 +1302,7 @@ hd_error hd_classifier_gradients(hd_classifier c, const float* dm_time, const fl
     e = cudaMemcpyAsync(grads, c->g.p, c->nparam * sizeof(float), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && loss) e = cudaMemcpyAsync(loss, c->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = tc_check(c);
   return to_hd(e);
 }
 
@@ -1212,6 +1316,7 @@ hd_error hd_classifier_train(hd_classifier c, const float* dm_time, const float*
   cudaStream_t s = c->stream;
   const int nb = (int)std::min<size_t>(batch, n);
   cudaError_t e = alloc_batch(c, nb);
+  if (e == cudaSuccess) e = tc_reset(c);
   // the training set stays on the device in BF16
   if (e == cudaSuccess) e = c->data_dm.ensure(n * 4096 * sizeof(bf16));
   if (e == cudaSuccess) e = c->data_ft.ensure(n * 16384 * sizeof(bf16));
@@ -1271,6 +1376,7 @@ hd_error hd_classifier_train(hd_classifier c, const float* dm_time, const float*
     if (epoch_loss) epoch_loss[ep] = nbatches ? (float)(lsum / nbatches) : 0.f;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = tc_check(c);
   return to_hd(e);
 }
 
@@ -1297,6 +1403,33 @@ hd_error hd_classifier_get_timing(hd_classifier c, float* ms) {
   if (!ms) return HD_INVALID_POINTER;
   *ms = c->score_ms;
   return HD_NO_ERROR;
+}
+
+hd_error hd_bf16_gemm_tc(int m, int n, int k, const void* d_a, long long sam, long long sak,
+                         const void* d_b, long long sbk, long long sbn, float* d_c,
+                         long long scm, long long scn, int accumulate, int splits) {
+  if (!d_a || !d_b || !d_c) return HD_INVALID_POINTER;
+  if (sak != 1 || sbk != 1) return HD_INVALID_STRIDE;
+  float* ws = nullptr;
+  unsigned* err = nullptr;
+  const size_t nws = hdb::umma_workspace_floats(m, n, k, splits);
+  cudaError_t e = hdb::dev_malloc(&err, sizeof(unsigned));
+  if (e == cudaSuccess && nws) e = hdb::dev_malloc(&ws, nws * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(err, 0, sizeof(unsigned));
+  if (e == cudaSuccess)
+    e = hdb::umma_gemm(m, n, k, d_a, sam, d_b, sbn, d_c, scm, scn, accumulate, splits, ws, err, 0);
+  hd_error he = HD_NO_ERROR;
+  if (e == cudaErrorNotSupported) he = HD_INVALID_STRIDE;
+  else if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  unsigned v = 0;
+  if (he == HD_NO_ERROR && e == cudaSuccess) {
+    e = cudaMemcpy(&v, err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && v) he = HD_INTERNAL_GPU_ERROR;
+  }
+  if (he == HD_NO_ERROR) he = to_hd(e);
+  if (ws) cudaFree(ws);
+  if (err) cudaFree(err);
+  return he;
 }
 
 hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long long sak,

@@ -277,6 +277,16 @@ cudaError_t extract_patches(const float* scan, size_t scan_pitch, size_t len, co
                             size_t nsamps, int nchans, const PatchJob* jobs, int njobs,
                             float* dm_out, float* ft_out, cudaStream_t s);
 
+// BF16 GEMM on tcgen05 (umma.cu): C(m, n) (+)= sum_k A[m*lda + k] B[n*ldb + k]
+// with C(m, n) at C[m*scm + n*scn]; N <= 128, K, lda, ldb multiples of 8,
+// A and B 16-byte aligned (else cudaErrorNotSupported).  splits > 1 splits K
+// and needs a workspace of umma_workspace_floats() floats; the splits are
+// added in order.  *err records a bounded wait that gave up.
+size_t umma_workspace_floats(int M, int N, int K, int splits);
+cudaError_t umma_gemm(int M, int N, int K, const void* A, long long lda, const void* B,
+                      long long ldb, float* C, long long scm, long long scn, int accumulate,
+                      int splits, float* ws, unsigned* err, cudaStream_t s);
+
 // normalise_series_array (candidate_profiler.C:88-134) on nrows rows of n
 // floats: row r at data + (r / rows_per_group) * group_pitch + (r %
 // rows_per_group) * pitch.  zero_flat: a row with zero deviation becomes 0

@@ -379,6 +379,15 @@ hd_error hd_classifier_get_timing(hd_classifier classifier, hd_float* ms);
 hd_error hd_bf16_gemm(int m, int n, int k, const void* d_a, long long sam, long long sak,
                       const void* d_b, long long sbk, long long sbn, float* d_c,
                       long long scm, long long scn, int accumulate, int splits);
+/* The same product on the fifth-generation tensor cores, as the classifier's
+ * training runs its convolutions and fully connected layer (tcgen05.mma with
+ * FP32 accumulators in tensor memory, operands staged by TMA), for testing:
+ * A and B K-major (sak == 1, sbk == 1), n <= 128, k, sam and sbn multiples of
+ * 8 and 16-byte aligned operands (else HD_INVALID_STRIDE); splits > 1 sums K
+ * in parts through a workspace, added in order (deterministic). */
+hd_error hd_bf16_gemm_tc(int m, int n, int k, const void* d_a, long long sam, long long sak,
+                         const void* d_b, long long sbk, long long sbn, float* d_c,
+                         long long scm, long long scn, int accumulate, int splits);
 
 /* Dedispersion tile of the last gulp: DM trials and output samples per CTA
  * and channel rows staged per pipeline stage.  The first gulp of each shape

@@ -3,8 +3,10 @@ patches against the oracle (bit-exact), the network's forward pass and
 gradients against the CPU network (oracle/classifier.c), and training on
 candidates the pipeline itself produces.
 
-Tolerances: the GEMM accumulates BF16 products in FP32 (relative error
-~1e-6 of the operands' scale, asserted at 1e-4); the network's gradients
+Tolerances: the GEMMs accumulate BF16 products in FP32 (relative error
+~1e-6 of the operands' scale, asserted at 1e-4); the tensor-core GEMM
+(tcgen05, hd_bf16_gemm_tc) is also checked for the same bits on a second run;
+the network's gradients
 agree with the CPU network (double sums, same BF16 rounding points) to 3e-2
 relative L2 per parameter tensor and its probabilities to 2e-3, because a
 different FP32 summation order can move an activation across a BF16 rounding
@@ -49,6 +51,48 @@ def test_gemm_matches_numpy(hdb, case):
     got = Cd.cpu().numpy()
     scale = np.abs(a).max() * np.abs(b).max() * np.sqrt(K)
     assert np.abs(got - ref).max() <= 1e-4 * scale
+
+
+@pytest.mark.parametrize("M,N,K,splits,acc", [
+    (1000, 16, 80, 1, 0),        # conv layer 2 shape: M tail, K = 80 (one partial block)
+    (333, 32, 144, 1, 1),        # conv layer 3 shape, accumulate into C
+    (12305, 8, 16, 1, 0),        # conv layer 1 shape: N = 8 padded to 16, K = 16
+    (256, 16, 10240, 64, 0),     # fully connected layer: split K
+    (144, 32, 65536, 37, 1),     # weight gradient: K = pixels, 37 splits, accumulate
+    (200, 128, 512, 3, 0),       # widest N, splits that do not divide the K blocks
+])
+def test_gemm_tensor_cores_match_numpy(hdb, M, N, K, splits, acc):
+    """hd_bf16_gemm_tc (tcgen05.mma, TMEM accumulators, TMA-staged K-major
+    operands) against float64 products of the same BF16 values, and the same
+    bits on a second run (split K is reduced in a fixed order)."""
+    rng = np.random.default_rng(M + N + K)
+    A, B = _bf16((M, K), rng), _bf16((N, K), rng)
+    a, b = A.float().cpu().numpy(), B.float().cpu().numpy()
+    c0 = rng.standard_normal((N, M)).astype(np.float32)
+    ref = (a.astype(np.float64) @ b.astype(np.float64).T).T + (c0 if acc else 0.0)
+    outs = []
+    for _ in range(2):
+        Cd = torch.from_numpy(c0.copy()).cuda()  # C(m, n) at n * M + m
+        err = H.lib().hd_bf16_gemm_tc(M, N, K, A.data_ptr(), K, 1, B.data_ptr(), 1, K,
+                                      H.C.cast(Cd.data_ptr(), H.C.POINTER(H.C.c_float)), 1, M,
+                                      acc, splits)
+        assert err == H.HD_NO_ERROR, H.error_string(err)
+        outs.append(Cd.cpu().numpy())
+    scale = np.abs(a).max() * np.abs(b).max() * np.sqrt(K)
+    assert np.abs(outs[0] - ref).max() <= 1e-4 * scale
+    np.testing.assert_array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+
+
+def test_gemm_tensor_cores_reject_unsupported(hdb):
+    """Operands that are not K-major, or N above 128, are refused."""
+    rng = np.random.default_rng(3)
+    A, B = _bf16((64, 64), rng), _bf16((200, 64), rng)
+    Cd = torch.zeros((64, 200), dtype=torch.float32, device="cuda")
+    cp = H.C.cast(Cd.data_ptr(), H.C.POINTER(H.C.c_float))
+    assert H.lib().hd_bf16_gemm_tc(64, 200, 64, A.data_ptr(), 64, 1, B.data_ptr(), 1, 64, cp,
+                                   200, 1, 0, 1) == H.HD_INVALID_STRIDE
+    assert H.lib().hd_bf16_gemm_tc(64, 64, 64, A.data_ptr(), 1, 64, B.data_ptr(), 1, 64, cp,
+                                   64, 1, 0, 1) == H.HD_INVALID_STRIDE
 
 
 def test_patches_match_oracle(hdb, oracle_lib):
@@ -125,6 +169,27 @@ def test_forward_and_gradients_match_oracle(hdb, oracle_lib):
         assert _rel(g[o:o + s], g_cpu[o:o + s]) < 3e-2, (k, _rel(g[o:o + s], g_cpu[o:o + s]))
         o += s
     assert o == params.size
+
+
+def test_gradients_and_training_reproducible(hdb):
+    """Every reduction of the backward pass runs in a fixed order (split-K
+    weight gradients added split by split, bias and head gradients summed
+    sample by sample), so the same batch gives the same gradient bits, and
+    the same training run the same weights."""
+    rng = np.random.default_rng(8)
+    n = 64
+    dm = rng.standard_normal((n, 64, 64)).astype(np.float32)
+    ft = rng.standard_normal((n, 64, 256)).astype(np.float32)
+    lab = (rng.random(n) < 0.5).astype(np.int32)
+    runs = []
+    for _ in range(2):
+        with H.Classifier(seed=9) as clf:
+            g, loss = clf.gradients(dm, ft, lab)
+            clf.train(dm, ft, lab, epochs=2, batch=32, seed=4)
+            runs.append((g, np.float32(loss), clf.params()))
+    np.testing.assert_array_equal(runs[0][0].view(np.uint32), runs[1][0].view(np.uint32))
+    assert runs[0][1] == runs[1][1]
+    np.testing.assert_array_equal(runs[0][2].view(np.uint32), runs[1][2].view(np.uint32))
 
 
 def test_training_keeps_pulses_and_rejects_rfi(hdb):
