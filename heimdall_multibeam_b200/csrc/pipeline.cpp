@@ -48,6 +48,10 @@ struct DevBuf {
 
 }  // namespace
 
+// Merged candidate rows read back with the group count, before it is known
+// (the rest follow in a second copy when there are more).
+constexpr size_t kSpecRows = 2048;
+
 // Host filterbanks of a batched gulp are copied in up to kMaxChunks pieces so
 // that the transpose and dedispersion of one piece overlap the next copy.
 constexpr int kMaxChunks = 8;
@@ -124,8 +128,22 @@ struct hd_pipeline_t {
   size_t last_nsamps = 0, last_len = 0, last_scan_pitch = 0, last_units = 0;
   DevBuf patch_jobs, patch_dm, patch_ft;
   std::vector<unsigned> unit_first;                    // first giant of each unit
-  std::vector<float> g_peaks;
-  std::vector<hd_size> g_inds, g_begins, g_ends, g_filters, g_dms, g_labels;
+  // the last gulp's giant list stays on the device (main_giants); it is
+  // copied only when hd_get_giants asks for it
+  size_t last_giants = 0, last_gap = 1;
+  // merged candidate rows read back (pinned)
+  hdb::GroupRow* h_rows = nullptr;
+  size_t h_rows_cap = 0;
+  cudaError_t ensure_rows_host(size_t n) {
+    if (n <= h_rows_cap) return cudaSuccess;
+    if (h_rows) cudaFreeHost(h_rows);
+    h_rows = nullptr;
+    h_rows_cap = 0;
+    cudaError_t e = cudaMallocHost(&h_rows, n * sizeof(hdb::GroupRow));
+    if (e == cudaSuccess) h_rows_cap = n;
+    else cudaGetLastError();
+    return e;
+  }
 
   ~hd_pipeline_t() {
     if (plan) dedisp_destroy_plan(plan);
@@ -135,6 +153,7 @@ struct hd_pipeline_t {
     if (stream) cudaStreamDestroy(stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (h_small) cudaFreeHost(h_small);
+    if (h_rows) cudaFreeHost(h_rows);
   }
 };
 
@@ -367,7 +386,7 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   pl->unit_meta.assign(U, {});
   pl->searched = false;
   pl->unit_first.assign(U + 1, 0);
-  pl->g_peaks.clear();
+  pl->last_giants = 0;
   std::memset(pl->timing, 0, sizeof(pl->timing));
   if (statuses)
     for (size_t u = 0; u < U; u++) statuses[u] = HD_NO_ERROR;
@@ -747,9 +766,13 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(hdb::cluster_init(gb, (int)ngiants, s));
     hdb::ClusterArgs ca{(int)ngiants, P.cand_sep_time, P.cand_sep_filter, dm_tol,
                         (unsigned long long)(nsamps / nbeams)};
+    // sweeps until one changes nothing; the fixed point is idempotent, so the
+    // flag is read after every second sweep (one more sweep than needed at
+    // most, half the host round trips)
     unsigned* changed = pl->small.as<unsigned>() + 8;
-    for (unsigned it = 0; it <= ngiants; it++) {
+    for (unsigned it = 0; it <= ngiants; it += 2) {
       HD_TRY(cudaMemsetAsync(changed, 0, sizeof(unsigned), s));
+      HD_TRY(hdb::cluster_sweep(ca, gb, changed, s));
       HD_TRY(hdb::cluster_sweep(ca, gb, changed, s));
       HD_TRY(cudaMemcpyAsync(pl->h_small + 8, changed, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
       HD_TRY(cudaStreamSynchronize(s));
@@ -767,42 +790,36 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
                              pl->root_flag.as<unsigned>(), pl->root_off.as<unsigned>(), nroots,
                              pl->scan_tmp.as<unsigned>(), pl->mkey.as<unsigned long long>(),
                              pl->rows.as<hdb::GroupRow>(), s));
+    // the group count, the error word and the first rows in one round trip
+    // (the giants stay on the device until hd_get_giants asks for them)
+    const size_t spec = std::min<size_t>(G, kSpecRows);
+    HD_TRY(pl->ensure_rows_host(std::max<size_t>(spec, 1)));
     HD_TRY(cudaMemcpyAsync(pl->h_small + 16, nroots, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(pl->h_small + 17, pl->plan->d_err, sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaMemcpyAsync(pl->h_rows, pl->rows.p, spec * sizeof(hdb::GroupRow),
+                           cudaMemcpyDeviceToHost, s));
+    cudaEventRecord(pl->ev[7], s);
     HD_TRY(cudaStreamSynchronize(s));
     ngroups = pl->h_small[16];
-    rows.resize(ngroups);
-    if (ngroups)
-      HD_TRY(cudaMemcpyAsync(rows.data(), pl->rows.p, ngroups * sizeof(hdb::GroupRow),
-                             cudaMemcpyDeviceToHost, s));
-    // giants for hd_get_giants
-    pl->g_peaks.resize(G);
-    std::vector<unsigned long long> ind(G), beg(G), end(G);
-    std::vector<int> fil(G), dmi(G), lab(G);
-    HD_TRY(cudaMemcpyAsync(pl->g_peaks.data(), gb.peak, G * sizeof(float), cudaMemcpyDeviceToHost, s));
-    HD_TRY(cudaMemcpyAsync(ind.data(), gb.ind, G * 8, cudaMemcpyDeviceToHost, s));
-    HD_TRY(cudaMemcpyAsync(beg.data(), gb.begin, G * 8, cudaMemcpyDeviceToHost, s));
-    HD_TRY(cudaMemcpyAsync(end.data(), gb.end, G * 8, cudaMemcpyDeviceToHost, s));
-    HD_TRY(cudaMemcpyAsync(fil.data(), gb.filter, G * 4, cudaMemcpyDeviceToHost, s));
-    HD_TRY(cudaMemcpyAsync(dmi.data(), gb.dm, G * 4, cudaMemcpyDeviceToHost, s));
-    HD_TRY(cudaMemcpyAsync(lab.data(), gb.label, G * 4, cudaMemcpyDeviceToHost, s));
-    cudaEventRecord(pl->ev[7], s);
-    HD_TRY(cudaStreamSynchronize(s));
-    pl->g_inds.assign(ind.begin(), ind.end());
-    pl->g_begins.assign(beg.begin(), beg.end());
-    pl->g_ends.assign(end.begin(), end.end());
-    pl->g_filters.assign(fil.begin(), fil.end());
-    pl->g_dms.resize(G);
-    for (size_t g = 0; g < G; g++) pl->g_dms[g] = (hd_size)((unsigned)dmi[g] % gap);
-    pl->g_labels.assign(lab.begin(), lab.end());
+    if (ngroups > spec) {
+      std::vector<hdb::GroupRow> head(pl->h_rows, pl->h_rows + spec);
+      HD_TRY(pl->ensure_rows_host(ngroups));
+      std::copy(head.begin(), head.end(), pl->h_rows);
+      HD_TRY(cudaMemcpyAsync(pl->h_rows + spec, pl->rows.as<hdb::GroupRow>() + spec,
+                             (ngroups - spec) * sizeof(hdb::GroupRow), cudaMemcpyDeviceToHost, s));
+      HD_TRY(cudaStreamSynchronize(s));
+    }
+    rows.assign(pl->h_rows, pl->h_rows + ngroups);
+    pl->last_giants = G;
   } else {
+    HD_TRY(cudaMemcpyAsync(pl->h_small + 17, pl->plan->d_err, sizeof(unsigned),
+                           cudaMemcpyDeviceToHost, s));
     cudaEventRecord(pl->ev[7], s);
     HD_TRY(cudaStreamSynchronize(s));
-    pl->g_inds.clear(); pl->g_begins.clear(); pl->g_ends.clear();
-    pl->g_filters.clear(); pl->g_dms.clear(); pl->g_labels.clear();
   }
-  unsigned derr = 0;
-  cudaMemcpy(&derr, pl->plan->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
-  if (derr) return HD_INTERNAL_GPU_ERROR;
+  pl->last_gap = gap;
+  if (pl->h_small[17]) return HD_INTERNAL_GPU_ERROR;
 
   // ---- candidate rows (pipeline.cu:1012-1039), split by unit -------------------
   const unsigned nsamps_beam = (unsigned)(nsamps / nbeams);
@@ -1116,15 +1133,41 @@ hd_error hd_get_giants(hd_pipeline pl, hd_float* peaks, hd_size* inds, hd_size* 
                        hd_size* count) {
   if (!pl) return HD_INVALID_PIPELINE;
   if (!count) return HD_INVALID_POINTER;
-  size_t n = std::min(*count, pl->g_peaks.size());
-  if (peaks) std::memcpy(peaks, pl->g_peaks.data(), n * sizeof(float));
-  if (inds) std::memcpy(inds, pl->g_inds.data(), n * sizeof(hd_size));
-  if (begins) std::memcpy(begins, pl->g_begins.data(), n * sizeof(hd_size));
-  if (ends) std::memcpy(ends, pl->g_ends.data(), n * sizeof(hd_size));
-  if (filter_inds) std::memcpy(filter_inds, pl->g_filters.data(), n * sizeof(hd_size));
-  if (dm_inds) std::memcpy(dm_inds, pl->g_dms.data(), n * sizeof(hd_size));
-  if (labels) std::memcpy(labels, pl->g_labels.data(), n * sizeof(hd_size));
-  *count = pl->g_peaks.size();
+  const size_t G = pl->last_giants;
+  const size_t n = std::min(*count, G);
+  *count = G;
+  if (n == 0) return HD_NO_ERROR;
+  if (cudaSetDevice(pl->device) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
+  // the last gulp's giants, from the device
+  hdb::GiantBuffers gb{};
+  pl->main_giants.view(gb);
+  cudaStream_t s = pl->stream;
+  std::vector<unsigned long long> u64(n);
+  std::vector<int> i32(n);
+  auto widen64 = [&](const unsigned long long* src, hd_size* dst) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(u64.data(), src, n * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    for (size_t g = 0; e == cudaSuccess && g < n; g++) dst[g] = (hd_size)u64[g];
+    return e;
+  };
+  auto widen32 = [&](const int* src, hd_size* dst, size_t mod) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(i32.data(), src, n * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    for (size_t g = 0; e == cudaSuccess && g < n; g++)
+      dst[g] = mod ? (hd_size)((unsigned)i32[g] % mod) : (hd_size)i32[g];
+    return e;
+  };
+  if (peaks) {
+    HD_TRY(cudaMemcpyAsync(peaks, gb.peak, n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    HD_TRY(cudaStreamSynchronize(s));
+  }
+  if (inds) HD_TRY(widen64(gb.ind, inds));
+  if (begins) HD_TRY(widen64(gb.begin, begins));
+  if (ends) HD_TRY(widen64(gb.end, ends));
+  if (filter_inds) HD_TRY(widen32(gb.filter, filter_inds, 0));
+  // DM trial of the key unit * gap + trial
+  if (dm_inds) HD_TRY(widen32(gb.dm, dm_inds, pl->last_gap));
+  if (labels) HD_TRY(widen32(gb.label, labels, 0));
   return HD_NO_ERROR;
 }
 

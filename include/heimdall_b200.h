@@ -558,7 +558,9 @@ void     hd_destroy_beam_set(hd_beam_set set);
  * before clustering, with its cluster label (the index of the cluster's first
  * giant).  After hd_execute_beams: filterbank by filterbank, dm_inds local to
  * each filterbank, labels indexing the whole list.  Giants are reported only
- * when some filterbank did not bail out.  Any pointer may be NULL. */
+ * when some filterbank did not bail out.  Any pointer may be NULL.  The giants
+ * stay in device memory after the gulp and are copied by this call, so call
+ * it before the next execute on the pipeline. */
 hd_error hd_get_giants(hd_pipeline pipeline, hd_float* peaks, hd_size* inds, hd_size* begins,
                        hd_size* ends, hd_size* filter_inds, hd_size* dm_inds,
                        hd_size* labels, hd_size* count);
