@@ -290,6 +290,7 @@ def run_product(args):
     launches = H.launch_count() - l0
     cands = [pl.candidates(u) for u in range(U)] if U > 1 else [pl.candidates()]
     tile = pl.dedisp_tile()
+    tile_source = pl.dedisp_tile_source()
 
     # ---- plain per-beam form on the same data ---------------------------------
     ms_plain = None
@@ -420,8 +421,7 @@ def run_product(args):
             "config": config_for(wk, D, world),
             "dedisp_tile": {"dm_block": tile[0], "time_block": tile[1],
                             "rows_per_stage": tile[2],
-                            "chosen_by": "HDB_DEDISP_TILE"
-                            if os.environ.get("HDB_DEDISP_TILE") else "autotuner"},
+                            "chosen_by": tile_source},
             "stage_ms": {k: round(v / args.steps, 4) for k, v in stage.items()},
             "roofline": roof,
             "recall": {"snr_ge_8_found": hit, "snr_ge_8_injected": nstrong},

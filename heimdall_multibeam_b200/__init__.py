@@ -196,6 +196,7 @@ SYMBOLS = {
     "hd_get_timing": (C.c_int, [_P, _FP, C.c_int]),
     "hd_get_dedisp_tile": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
+    "hd_get_dedisp_tile_source": (C.c_int, [_P]),
     "hd_read_sigproc_header": (C.c_int, [C.c_char_p, C.POINTER(HdSigprocHeader)]),
     "hd_coincide": (C.c_int, [_P, _SZ, _SZ, C.c_uint, C.c_uint, C.c_int, _P]),
     "hd_profile_candidates": (C.c_int, [_P, _SZ, _SZ, C.c_int, C.c_double, C.c_double,
@@ -600,6 +601,14 @@ class Pipeline:
         v = [C.c_int(0) for _ in range(3)]
         lib().hd_get_dedisp_tile(self._p, *(C.byref(x) for x in v))
         return tuple(int(x.value) for x in v)
+
+    TILE_SOURCES = ("default", "HDB_DEDISP_TILE", "autotuner", "tile cache")
+
+    def dedisp_tile_source(self) -> str:
+        """hd_get_dedisp_tile_source as a name: where the last gulp's tile
+        came from (the default, HDB_DEDISP_TILE, the autotuner or the
+        persistent tile cache)."""
+        return self.TILE_SOURCES[lib().hd_get_dedisp_tile_source(self._p)]
 
     def timing(self) -> Dict[str, float]:
         t = (C.c_float * 8)()

@@ -1188,6 +1188,11 @@ hd_error hd_get_dedisp_tile(hd_pipeline pl, int* dm_block, int* time_block, int*
   return HD_NO_ERROR;
 }
 
+int hd_get_dedisp_tile_source(hd_pipeline pl) {
+  if (!pl) return -1;
+  return pl->plan->last_tile_source;
+}
+
 hd_error hd_get_timing(hd_pipeline pl, float* ms, int n) {
   if (!pl) return HD_INVALID_PIPELINE;
   if (!ms) return HD_INVALID_POINTER;

@@ -12,7 +12,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
+
+#include <sys/stat.h>
 
 #include "internal.h"
 
@@ -255,10 +258,121 @@ size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
   return ft_pitch_for(p->max_span, p->max_delay, nsamps, nout);
 }
 
-// One launch set over trials whose delays are d_delays (dm_count rows) on a
-// channel-major input of nsamps samples, nout output samples per trial; the
-// tile is tuned per (nsamps, units, tune_key).
-static dedisp_error dedisperse_tables(dedisp_plan p, const int* d_delays, int* const* d_blk_min,
+// ---------------------------------------------------------------------------
+// Persistent tile cache.  The autotuner's choice is kept across processes in
+// a text file, one line per tuned shape: "<key, 16 hex digits> <dm_block>
+// <time_block> <rows>".  The key is a 64-bit FNV-1a hash of everything the
+// kernel's speed depends on: the kernel generation, the device (name, SM
+// count), the input and output lengths, the unit count and the trial-by-
+// channel delay table of the launch (which fixes the DM list, the sampling
+// time, the band and the active channels).  The file is HDB_TUNE_CACHE, else
+// $XDG_CACHE_HOME/heimdall_b200/dedisp_tiles.txt, else
+// $HOME/.cache/heimdall_b200/dedisp_tiles.txt; HDB_TUNE_CACHE=0 (or empty)
+// turns the cache off.  Entries naming a tile that no longer fits are
+// ignored and the shape is timed again.
+// ---------------------------------------------------------------------------
+namespace {
+// bump when the dedispersion kernel changes, so stale choices are not reused
+constexpr uint64_t kDedispKernelGeneration = 3;
+
+struct TileCache {
+  std::mutex mu;
+  bool loaded = false;
+  std::string path;
+  std::map<uint64_t, std::array<int, 3>> entries;
+};
+TileCache& tile_cache() {
+  static TileCache c;
+  return c;
+}
+
+std::string tile_cache_path() {
+  if (const char* e = std::getenv("HDB_TUNE_CACHE"))
+    return (e[0] == 0 || std::strcmp(e, "0") == 0) ? std::string() : std::string(e);
+  std::string base;
+  if (const char* x = std::getenv("XDG_CACHE_HOME"); x && x[0]) base = x;
+  else if (const char* h = std::getenv("HOME"); h && h[0]) base = std::string(h) + "/.cache";
+  else return std::string();
+  return base + "/heimdall_b200/dedisp_tiles.txt";
+}
+
+struct Fnv {
+  uint64_t h = 1469598103934665603ull;
+  void bytes(const void* p, size_t n) {
+    const uint8_t* b = static_cast<const uint8_t*>(p);
+    for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+  }
+  template <class T> void val(const T& v) { bytes(&v, sizeof v); }
+};
+
+uint64_t tile_key(const std::vector<int>& delays, const std::vector<int>& active, size_t nsamps,
+                  size_t nout, size_t units) {
+  Fnv f;
+  f.val(kDedispKernelGeneration);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) f.bytes(prop.name, std::strlen(prop.name));
+  f.val(sms);
+  f.val(nsamps);
+  f.val(nout);
+  f.val(units);
+  const size_t n = delays.size();
+  f.val(n);
+  f.bytes(delays.data(), n * sizeof(int));
+  const size_t na = active.size();
+  f.val(na);
+  f.bytes(active.data(), na * sizeof(int));
+  return f.h;
+}
+
+// Looks the key up (loading the file on first use); false when absent or
+// the cache is off.
+bool tile_cache_get(uint64_t key, std::array<int, 3>* out) {
+  TileCache& c = tile_cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  if (!c.loaded) {
+    c.loaded = true;
+    c.path = tile_cache_path();
+    if (!c.path.empty())
+      if (FILE* fp = std::fopen(c.path.c_str(), "r")) {
+        unsigned long long k = 0;
+        int a = 0, b = 0, r = 0;
+        char line[128];
+        while (std::fgets(line, sizeof line, fp))
+          if (std::sscanf(line, "%llx %d %d %d", &k, &a, &b, &r) == 4) c.entries[k] = {a, b, r};
+        std::fclose(fp);
+      }
+  }
+  if (c.path.empty()) return false;
+  auto it = c.entries.find(key);
+  if (it == c.entries.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+void tile_cache_put(uint64_t key, const std::array<int, 3>& t) {
+  TileCache& c = tile_cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  if (c.path.empty()) return;
+  c.entries[key] = t;
+  // create the directory chain; a failure only means the choice is not kept
+  for (size_t pos = c.path.find('/', 1); pos != std::string::npos; pos = c.path.find('/', pos + 1))
+    mkdir(c.path.substr(0, pos).c_str(), 0755);
+  if (FILE* fp = std::fopen(c.path.c_str(), "a")) {
+    std::fprintf(fp, "%016llx %d %d %d\n", (unsigned long long)key, t[0], t[1], t[2]);
+    std::fclose(fp);
+  }
+}
+}  // namespace
+
+// One launch set over trials whose delays are d_delays (dm_count rows; host
+// copy h_delays) on a channel-major input of nsamps samples, nout output
+// samples per trial; the tile is tuned per (nsamps, units, tune_key) and kept
+// in the persistent tile cache.
+static dedisp_error dedisperse_tables(dedisp_plan p, const std::vector<int>& h_delays,
+                                      const int* d_delays, int* const* d_blk_min,
                                       const size_t* max_span, int dm_count, size_t nout,
                                       size_t tune_key, const uint8_t* d_ft, size_t pitch,
                                       size_t nsamps, float* d_out, size_t out_pitch,
@@ -316,14 +430,27 @@ static dedisp_error dedisperse_tables(dedisp_plan p, const int* d_delays, int* c
     // default: 16 DMs x 512 samples when it fits
     std::array<int, 3> best = cand[0];
     bool forced = false;
+    int source = 0;
     for (const auto& t : cand)
       if (t[0] == 16 && t[1] == 512) best = t;
     for (const auto& t : cand)
       if (t[0] == p->forced_dm_block && t[1] == p->forced_time_block) {
         best = t;
         forced = true;
+        source = 1;
       }
+    uint64_t ckey = 0;
+    bool cached = false;
     if (p->tune && !forced && cand.size() > 1) {
+      ckey = tile_key(h_delays, p->active, nsamps, nout, units);
+      std::array<int, 3> t;
+      if (tile_cache_get(ckey, &t) && std::find(cand.begin(), cand.end(), t) != cand.end()) {
+        best = t;
+        cached = true;
+        source = 3;
+      }
+    }
+    if (p->tune && !forced && !cached && cand.size() > 1) {
       // autotuner: each candidate once to warm up and once timed; all give the
       // same sums, so the output of the last run stands
       cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -349,11 +476,14 @@ static dedisp_error dedisperse_tables(dedisp_plan p, const int* d_delays, int* c
       }
       if (e0) cudaEventDestroy(e0);
       if (e1) cudaEventDestroy(e1);
+      source = 2;
+      tile_cache_put(ckey, best);
     }
-    it = p->tiles.emplace(key, best).first;
+    it = p->tiles.emplace(key, std::array<int, 4>{best[0], best[1], best[2], source}).first;
   }
-  p->last_tile = it->second;
-  if (launch_dedisp(a, with_tile(it->second), s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
+  p->last_tile = {it->second[0], it->second[1], it->second[2]};
+  p->last_tile_source = it->second[3];
+  if (launch_dedisp(a, with_tile(p->last_tile), s) != cudaSuccess) return DEDISP_INTERNAL_GPU_ERROR;
   return DEDISP_NO_ERROR;
 }
 
@@ -366,7 +496,7 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
   if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
   const size_t nout = nsamps - p->max_delay;
   if (p->groups.empty())
-    return dedisperse_tables(p, p->d_delays, p->d_blk_min, p->max_span,
+    return dedisperse_tables(p, p->delays, p->d_delays, p->d_blk_min, p->max_span,
                              (int)p->dm_list.size(), nout, 0, d_ft, pitch, nsamps, d_out,
                              out_pitch, s, units, in_unit, out_unit);
   // adaptive dt: group g's trials [d0, d1) of every unit are rows
@@ -378,7 +508,7 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
     const size_t nout_s = nout / g.s;
     float* out_g = d_out + units * g.d0 * out_pitch;
     if (g.s == 1) {
-      de = dedisperse_tables(p, g.d_delays, g.d_blk_min, g.max_span, (int)Dg, nout_s, gi + 1,
+      de = dedisperse_tables(p, g.delays, g.d_delays, g.d_blk_min, g.max_span, (int)Dg, nout_s, gi + 1,
                              d_ft, pitch, nsamps, out_g, out_pitch, s, units, in_unit,
                              Dg * out_pitch);
     } else {
@@ -395,7 +525,7 @@ dedisp_error plan_dedisperse_ft(dedisp_plan p, const uint8_t* d_ft, size_t pitch
       if (launch_scrunch_ft(d_ft, pitch, nsamps, (int)C, (int)g.s, p->d_scr, pitch_s, units,
                             in_unit, pitch_s * C, s) != cudaSuccess)
         return DEDISP_INTERNAL_GPU_ERROR;
-      de = dedisperse_tables(p, g.d_delays, g.d_blk_min, g.max_span, (int)Dg, nout_s, gi + 1,
+      de = dedisperse_tables(p, g.delays, g.d_delays, g.d_blk_min, g.max_span, (int)Dg, nout_s, gi + 1,
                              p->d_scr, pitch_s, ns, out_g, out_pitch, s, units, pitch_s * C,
                              Dg * out_pitch);
     }

@@ -34,11 +34,15 @@ struct dedisp_plan_struct {
   size_t max_span[3] = {0, 0, 0};  // max over blocks/chans of (max - min) delay
   int* d_delays = nullptr;
   int* d_blk_min[3] = {nullptr, nullptr, nullptr};
-  // dedispersion tile {dm_block, time_block, rows} per (nsamps, units,
-  // scrunch group): the fastest of the candidates, timed on first use
-  // (autotuner)
-  std::map<std::array<size_t, 3>, std::array<int, 3>> tiles;
+  // dedispersion tile {dm_block, time_block, rows, source} per (nsamps,
+  // units, scrunch group): the fastest of the candidates, timed on first use
+  // (autotuner) or read from the persistent tile cache
+  std::map<std::array<size_t, 3>, std::array<int, 4>> tiles;
   std::array<int, 3> last_tile = {16, 512, 8};
+  // where last_tile came from (hd_get_dedisp_tile_source): 0 default,
+  // 1 forced (HDB_DEDISP_TILE), 2 timed by the autotuner in this process,
+  // 3 the persistent tile cache (HDB_TUNE_CACHE)
+  int last_tile_source = 0;
   bool tune = true;
   int forced_dm_block = 0, forced_time_block = 0;  // HDB_DEDISP_TILE="DBxTB"
   int* d_active = nullptr;

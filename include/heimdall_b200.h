@@ -22,7 +22,7 @@
  * a .cand file or a socket): hd_set_cleaning, hd_set_narrow_band,
  * hd_execute_device, hd_execute_beams, hd_get_candidates,
  * hd_get_beam_candidates, hd_get_raw_candidates, hd_get_giants, hd_get_timing,
- * hd_get_dedisp_tile, hd_get_launch_count, hd_measure_int_add_rate,
+ * hd_get_dedisp_tile, hd_get_dedisp_tile_source, hd_get_launch_count, hd_measure_int_add_rate,
  * hd_clean_filterbank_rfi_noalloc;
  * beam sets (hd_*_beam_set*); sigproc input and the gulp loop
  * (hd_read_sigproc_header, hd_mjd_to_utc, hd_params_from_sigproc,
@@ -393,8 +393,17 @@ hd_error hd_bf16_gemm_tc(int m, int n, int k, const void* d_a, long long sam, lo
  * and channel rows staged per pipeline stage.  The first gulp of each shape
  * times every tile that fits shared memory and keeps the fastest (environment:
  * HDB_DEDISP_TUNE=0 keeps 16 x 512, HDB_DEDISP_TILE=DBxTB forces one); all
- * tiles give the same sums. */
+ * tiles give the same sums.  The choice is kept across processes in a tile
+ * cache file, keyed by the device, the gulp shape and the delay table:
+ * HDB_TUNE_CACHE=path, else $XDG_CACHE_HOME/heimdall_b200/dedisp_tiles.txt,
+ * else $HOME/.cache/heimdall_b200/dedisp_tiles.txt; HDB_TUNE_CACHE=0 turns it
+ * off. */
 hd_error hd_get_dedisp_tile(hd_pipeline pipeline, int* dm_block, int* time_block, int* rows);
+
+/* Where the last gulp's dedispersion tile came from: 0 the default tile,
+ * 1 forced by HDB_DEDISP_TILE, 2 timed by the autotuner in this process,
+ * 3 read from the tile cache; -1 for a null pipeline. */
+int hd_get_dedisp_tile_source(hd_pipeline pipeline);
 
 /* Number of kernels this library has launched in this process. */
 unsigned long long hd_get_launch_count(void);
