@@ -61,6 +61,10 @@ struct DedispArgs {
   // test of the error path: the producer issues no copy for the last stage,
   // so the consumers' wait on it runs out (HDB_TEST_WITHHOLD_STAGE=1)
   int withhold_last;
+  // always 1: the multiplier of the kernel's multiply-add accumulations.  A
+  // runtime value keeps them multiply-adds, which issue to the FMA pipe and
+  // leave the ALU pipe (shifts, byte permutes, adds) to the rest of the work
+  unsigned one;
 };
 
 // Dedispersion tile: DMs and output samples per CTA, channel rows staged per
@@ -126,16 +130,32 @@ struct TreeScratch {
   size_t cap;  // floats in each
 };
 
+// The baseline subtraction of remove_baseline (remove_baseline.cu:90-102),
+// applied where the series is read instead of written back: sample i < nsub
+// of series ser reads x - (stretched baseline at i).  base == nullptr: none.
+struct BaselineSub {
+  const float* base = nullptr;  // [ser][nbeams][sc] scrunched baseline samples
+  unsigned sc = 0, stride = 0, last_start = 0, nsub = 0;
+  int nbeams = 1;
+  float step2 = 0.f, step3 = 0.f;  // stretch steps: beams 0..n-2, last beam
+};
+
 // Samples per beam of the scrunched baseline (remove_baseline.cu:38) and the
 // tree scratch (floats per buffer) remove_baseline needs for nseg beams.
 size_t baseline_samples(size_t stride, size_t smooth_radius);
 size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg);
 // RemoveBaselinePlan::exec for every series (Pipeline/remove_baseline.cu:21-160).
+// With fused == nullptr the baseline is subtracted from the series in place;
+// otherwise the series are left as they are and *fused describes the
+// subtraction for rms_beams and normalise_scan to apply as they read (the
+// same float operations, so the same values), which saves writing and
+// re-reading every series.  base_out must stay untouched until then.
 cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                            TreeScratch& ws, cudaStream_t s);
+                            TreeScratch& ws, cudaStream_t s, BaselineSub* fused = nullptr);
 // GetRMSPlanMB::exec_multibeam, vector form (Pipeline/get_rms.cu:236-270):
 // rms[ser*nbeams + b].
-cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s);
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s,
+                      const BaselineSub& sub = BaselineSub());
 // normalise_multibeam (get_rms.cu:372-382) fused with the exclusive prefix sum
 // of MatchedFilterPlan::prep (matched_filter.cu:21-32), sequential association:
 // scan[ser][0..len] (len + 1 values, pitch scan_pitch).  norm_out (nullable,
@@ -143,7 +163,7 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // err (nullable): bit 1 is set if a staging wait timed out.
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
                            size_t scan_pitch, float* norm_out, cudaStream_t s,
-                           unsigned* err = nullptr);
+                           unsigned* err = nullptr, const BaselineSub& sub = BaselineSub());
 
 // Per-width constants of the boxcar loop (Pipeline/pipeline.cu:657-776).
 struct WidthInfo {
@@ -175,17 +195,32 @@ struct WidthCtx {
   int dm_offset;                // DM index of each unit's first series
   float* norm;        // [nser][nw]  1 / block_rms
   float thresh;
+  // Largest |boxcar value| of each block-RMS group (gsize consecutive
+  // filtered samples, ngroups complete groups per series) for the
+  // unscrunched widths [0, gmax_nw): [nser][gmax_nw][ngroups].  block_rms
+  // records it when gmax is set and the group geometry fits gmax_cap floats
+  // (else ngroups = 0); count_hits skips the tiles whose covering groups
+  // stay below every width's threshold.
+  float* gmax;
+  size_t gmax_cap;
+  unsigned gsize, ngroups;
+  int gmax_nw;
 };
 
 // Block RMS of width wi for every series (get_rms.cu:274-301 on the filtered
 // series) -> ctx.norm[ser][wi].  Widths in [w_begin, w_end) are handled
 // together; widths with ts > 1 must be passed one at a time after all earlier
 // widths (their RMS window reads the earlier widths' normalised output).
-cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* host_winfo, int w_begin, int w_end,
+cudaError_t block_rms(WidthCtx& ctx, const WidthInfo* host_winfo, int w_begin, int w_end,
                       TreeScratch& ws, cudaStream_t s);
 
 // Threshold + ordered compaction of every (series, width) into hit lists.
 struct HitBuffers {
+  // tiles (ser * ntiles + tile) with at least one hit of an unscrunched width,
+  // listed by count_hits for write_hits (list_valid when the list is complete)
+  unsigned* tile_list;  // capacity nser * ntiles
+  unsigned* tile_list_n;
+  bool list_valid;
   unsigned* tile_cnt;   // [nser][nw][ntiles]
   unsigned* sw_cnt;     // [nser*nw + 1]
   unsigned* sw_off;     // [nser*nw + 1]

@@ -371,7 +371,21 @@ __global__ void k_nb_zap(uint32_t* __restrict__ data, size_t nsamps, int units, 
 // are drained into 32-bit sums after at most 257 channels (255 * 257 =
 // 65535), so the sums are exact.  Every mbarrier wait is bounded; a wait that
 // gives up sets bit 0 of a.err and the warp leaves its loop.
+//
+// Pipe balance: the shifts, byte permutes and 3-input adds all issue to the
+// ALU pipe, which bounds the kernel, while the FMA pipe idles.  The odd-byte
+// sums are therefore accumulated with integer multiply-adds by a.one (= 1,
+// unknown to the compiler), which issue to the FMA pipe; and the producer
+// tabulates, per (DM, channel), the shared-memory word index of the row
+// segment and the realignment shift, so the consumers spend no ALU work on
+// addressing.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
 // CTAs per SM the register budget allows: per lane about 12 registers per
 // owned output word (two DMs x {2 packed, 4 drained} sums) plus ~48 others.
 constexpr int dd_min_blocks(int nw, int k, int g) {
@@ -391,8 +405,10 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
   constexpr int TB = 128 * K * G;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + NST;
-  int* s_off = reinterpret_cast<int*>(smem + 128);          // [NST][DB*CH]
-  uint8_t* rows = smem + 128 + NST * DB * CH * sizeof(int);  // [NST][CH][rowb]
+  // [NST][DB*CH] {word index of the (DM, channel) row segment in `rows`,
+  // realignment shift in bits}
+  int2* s_off = reinterpret_cast<int2*>(smem + 128);
+  uint8_t* rows = smem + 128 + NST * DB * CH * sizeof(int2);  // [NST][CH][rowb]
   const int dblk = blockIdx.x;
   const size_t t0 = (size_t)blockIdx.y * TB;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -428,14 +444,15 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
       if (a.withhold_last && st == nstage - 1) break;
       const int k0 = st * CH;
       const int nk = min(CH, a.nact - k0);
-      int* off = s_off + buf * DB * CH;
+      int2* off = s_off + buf * DB * CH;
       for (int e = lane; e < DB * CH; e += 32) {
         const int k = e % CH;
         if (k < nk) {
           const int c = a.chans[k0 + k];
           const int d = min(d_lo + e / CH, a.dm_count - 1);
           const size_t lo = (t0 + (size_t)bmin[c]) & ~(size_t)15;
-          off[e] = (int)(t0 + (size_t)a.delays[(size_t)d * C + c] - lo);
+          const int o = (int)(t0 + (size_t)a.delays[(size_t)d * C + c] - lo);
+          off[e] = make_int2(((buf * CH + k) * a.rowb + o) >> 2, (o & 3) * 8);
         }
       }
       __syncwarp();
@@ -498,19 +515,17 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
     }
     const int k0 = st * CH;
     const int nk = min(CH, a.nact - k0);
-    const int* off = s_off + buf * DB * CH + (2 * warp) * CH;
-    const uint8_t* stage_rows = rows + (size_t)(buf * CH) * a.rowb;
+    const int2* off = s_off + buf * DB * CH + (2 * warp) * CH;
+    const uint32_t* rows32 = reinterpret_cast<const uint32_t*>(rows);
+    const uint32_t one = a.one;
     int k = 0;
     for (; k + 1 < nk; k += 2) {
-      const uint32_t* ra = reinterpret_cast<const uint32_t*>(stage_rows + (size_t)k * a.rowb);
-      const uint32_t* rb = reinterpret_cast<const uint32_t*>(stage_rows + (size_t)(k + 1) * a.rowb);
 #pragma unroll
       for (int d = 0; d < 2; d++) {
-        const int oa = off[d * CH + k];
-        const int ob = off[d * CH + k + 1];
-        const int sa = (oa & 3) * 8, sb = (ob & 3) * 8;
-        const uint32_t* pa = ra + (oa >> 2) + lw;
-        const uint32_t* pb = rb + (ob >> 2) + lw;
+        const int2 oa = off[d * CH + k];
+        const int2 ob = off[d * CH + k + 1];
+        const uint32_t* pa = rows32 + (oa.x + lw);
+        const uint32_t* pb = rows32 + (ob.x + lw);
 #pragma unroll
         for (int g = 0; g < G; g++) {
           uint32_t wa[K + 1], wb[K + 1];
@@ -521,10 +536,12 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
           }
 #pragma unroll
           for (int j = 0; j < K; j++) {
-            const uint32_t xa = __funnelshift_r(wa[j], wa[j + 1], sa);
-            const uint32_t xb = __funnelshift_r(wb[j], wb[j + 1], sb);
+            const uint32_t xa = __funnelshift_r(wa[j], wa[j + 1], oa.y);
+            const uint32_t xb = __funnelshift_r(wb[j], wb[j + 1], ob.y);
             pk[d][K * g + j][0] += xa + xb;
-            pk[d][K * g + j][1] += __byte_perm(xa, 0u, 0x4341) + __byte_perm(xb, 0u, 0x4341);
+            pk[d][K * g + j][1] = mad_u32(__byte_perm(xb, 0u, 0x4341), one,
+                                          mad_u32(__byte_perm(xa, 0u, 0x4341), one,
+                                                  pk[d][K * g + j][1]));
           }
         }
       }
@@ -532,12 +549,10 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
       if (nsum >= 256) { drain(); nsum = 0; }
     }
     if (k < nk) {
-      const uint32_t* ra = reinterpret_cast<const uint32_t*>(stage_rows + (size_t)k * a.rowb);
 #pragma unroll
       for (int d = 0; d < 2; d++) {
-        const int oa = off[d * CH + k];
-        const int sa = (oa & 3) * 8;
-        const uint32_t* pa = ra + (oa >> 2) + lw;
+        const int2 oa = off[d * CH + k];
+        const uint32_t* pa = rows32 + (oa.x + lw);
 #pragma unroll
         for (int g = 0; g < G; g++) {
           uint32_t wa[K + 1];
@@ -545,9 +560,9 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
           for (int j = 0; j <= K; j++) wa[j] = pa[32 * K * g + j];
 #pragma unroll
           for (int j = 0; j < K; j++) {
-            const uint32_t xa = __funnelshift_r(wa[j], wa[j + 1], sa);
+            const uint32_t xa = __funnelshift_r(wa[j], wa[j + 1], oa.y);
             pk[d][K * g + j][0] += xa;
-            pk[d][K * g + j][1] += __byte_perm(xa, 0u, 0x4341);
+            pk[d][K * g + j][1] = mad_u32(__byte_perm(xa, 0u, 0x4341), one, pk[d][K * g + j][1]);
           }
         }
       }
@@ -746,7 +761,7 @@ namespace {
 constexpr int DD_NST = 3;
 // Shared memory of a variant: DB = dm_block DMs, `ch` channel rows per stage.
 size_t dd_smem(int dm_block, int ch, int rowb) {
-  return 128 + (size_t)DD_NST * dm_block * ch * sizeof(int) + (size_t)DD_NST * ch * rowb;
+  return 128 + (size_t)DD_NST * dm_block * ch * sizeof(int2) + (size_t)DD_NST * ch * rowb;
 }
 template <int NW, int K, int G, int CH>
 cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {

@@ -185,15 +185,59 @@ __global__ void k_baseline_stretch0(const float* __restrict__ data, size_t pitch
   out[(ser * nbeams + b) * cr + i] = v;
 }
 
+// Exact int <-> float conversions on the FMA pipe (the conversion unit runs
+// at a fraction of its rate), valid for 0 <= v < 2^23: 2^23 + u is the float
+// with exponent 23 and mantissa u, and adding 2^23 to x with rounding toward
+// zero leaves floor(x) in the mantissa (the binade [2^23, 2^24) has ulp 1).
+__device__ __forceinline__ float u2f_small(unsigned u) {
+  return __fsub_rn(__uint_as_float(0x4B000000u | u), 8388608.f);
+}
+__device__ __forceinline__ unsigned trunc_small(float x) {
+  return __float_as_uint(__fadd_rz(x, 8388608.f)) & 0x7FFFFFu;
+}
+
+// stretch_at / stretch_beam_at with those conversions (same float results;
+// arguments outside their range take the general functions)
+__device__ __forceinline__ float stretch_at_nc(const float* in, unsigned i, float step) {
+  if (i >= (1u << 23)) return stretch_at(in, i, step);
+  const float x = __fmul_rn(u2f_small(i), step);
+  if (!(x >= 0.f && x < 8388608.f)) return stretch_at(in, i, step);
+  const unsigned j = trunc_small(x);
+  const float fr = __fsub_rn(x, u2f_small(j));
+  const float add = (fr > kStretchEps) ? __fmul_rn(fr, __fsub_rn(in[j + 1], in[j])) : 0.f;
+  return __fadd_rn(in[j], add);
+}
+__device__ __forceinline__ float stretch_beam_at_nc(const float* in, unsigned i, float step,
+                                                    unsigned beam) {
+  if (i >= (1u << 23) || beam >= (1u << 23))
+    return stretch_beam_at(in, i, step, (unsigned long long)beam);
+  const float x = __fmul_rn(u2f_small(i), step);
+  const float fb = u2f_small(beam);
+  const float xs = __fadd_rn(x, fb);
+  if (!(x >= 0.f && xs < 8388608.f)) return stretch_beam_at(in, i, step, (unsigned long long)beam);
+  const unsigned k = trunc_small(xs);
+  const float o = __fadd_rn(__fsub_rn(x, u2f_small(k)), fb);
+  const float add = (o > kStretchEps) ? __fmul_rn(o, __fsub_rn(in[k + 1], in[k])) : 0.f;
+  return __fadd_rn(in[k], add);
+}
+
+// x - stretched baseline at sample i of series ser (i < nsub), else x
+__device__ __forceinline__ float sub_baseline(const BaselineSub& b, size_t ser, unsigned i,
+                                              float x) {
+  if (!b.base || i >= b.nsub) return x;
+  const float* bs = b.base + ser * (size_t)b.nbeams * b.sc;
+  const float v = (i < b.last_start)
+                      ? stretch_beam_at_nc(bs, i, b.step2, i / b.stride)
+                      : stretch_at_nc(bs + (size_t)(b.nbeams - 1) * b.sc, i - b.last_start,
+                                      b.step3);
+  return __fsub_rn(x, v);
+}
+
 // data[i] -= stretched baseline, i < nbeams*stride - dm_delay
-__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, int nbeams,
-                               unsigned stride, unsigned nsub, const float* __restrict__ base,
-                               size_t sc, float step2, float step3) {
+__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, BaselineSub b) {
   const size_t ser = blockIdx.y;
   float* d = data + ser * pitch;
-  const float* bs = base + ser * (size_t)nbeams * sc;
-  const float* last = bs + (size_t)(nbeams - 1) * sc;
-  const unsigned last_start = (unsigned)(nbeams - 1) * stride;
+  const unsigned nsub = b.nsub;
   // four consecutive samples per thread (rows are 16-byte aligned)
   for (unsigned i = 4u * (blockIdx.x * blockDim.x + threadIdx.x); i < nsub;
        i += 4u * gridDim.x * blockDim.x) {
@@ -205,13 +249,7 @@ __global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, int nbeam
     for (int j = 0; j < 4; j++) {
       const unsigned ij = i + j;
       if (!full) xs[j] = ij < nsub ? d[ij] : 0.f;
-      float v;
-      if (ij < last_start) {
-        v = stretch_beam_at(bs, ij, step2, (unsigned long long)(ij / stride));
-      } else {
-        v = stretch_at(last, ij - last_start, step3);
-      }
-      xs[j] = __fsub_rn(xs[j], v);
+      xs[j] = sub_baseline(b, ser, ij, xs[j]);
     }
     if (full) {
       *reinterpret_cast<float4*>(d + i) = x;
@@ -234,7 +272,8 @@ size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg) {
 }
 
 cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                            TreeScratch& ws, cudaStream_t s) {
+                            TreeScratch& ws, cudaStream_t s, BaselineSub* fused) {
+  if (fused) *fused = BaselineSub();
   BaselinePlan p = baseline_plan(sb.stride, smooth_radius);
   if (p.sample_count == 0) return cudaSuccess;
   const size_t sc = p.sample_count, cr = p.count_round;
@@ -282,10 +321,22 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   const size_t nsub = sb.stride * sb.nbeams - dm_delay;
   if (nsub >= 0xFFFFFF00u || sb.pitch % 4 || (reinterpret_cast<uintptr_t>(sb.data) & 15))
     return cudaErrorInvalidValue;
+  BaselineSub b;
+  b.base = base_out;
+  b.sc = (unsigned)sc;
+  b.stride = (unsigned)sb.stride;
+  b.last_start = (unsigned)((size_t)(sb.nbeams - 1) * sb.stride);
+  b.nsub = (unsigned)nsub;
+  b.nbeams = sb.nbeams;
+  b.step2 = step2;
+  b.step3 = step3;
+  if (fused) {
+    *fused = b;
+    return cudaSuccess;
+  }
   const size_t nq = (nsub + 3) / 4;
   dim3 grid((unsigned)((nq + 255) / 256 < 4096 ? (nq + 255) / 256 : 4096), sb.nser);
-  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, sb.nbeams, (unsigned)sb.stride,
-                                      (unsigned)nsub, base_out, sc, step2, step3); note_launch();
+  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, b); note_launch();
   return cudaGetLastError();
 }
 
@@ -298,7 +349,8 @@ __device__ __forceinline__ size_t reblock_index(size_t beam, float delta, unsign
 
 __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, int nbeams,
                                   size_t beam_count, float delta, int m,
-                                  float* __restrict__ out, size_t out_pitch_beam) {
+                                  float* __restrict__ out, size_t out_pitch_beam,
+                                  BaselineSub sub) {
   __shared__ float sm[625 + 125];
   const int b = blockIdx.y;
   const size_t ser = blockIdx.z;
@@ -307,7 +359,8 @@ __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, 
   const size_t o0 = (size_t)b * beam_count + g * pow5(m);
   float r = block_tree([&](int i) {
     unsigned o = (unsigned)(o0 + i);
-    return fabsf(d[reblock_index((size_t)b, delta, o)]);
+    const size_t k = reblock_index((size_t)b, delta, o);
+    return fabsf(sub_baseline(sub, ser, (unsigned)k, d[k]));
   }, m, sm);
   if (threadIdx.x == 0) out[(ser * nbeams + b) * out_pitch_beam + g] = r;
 }
@@ -315,15 +368,17 @@ __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, 
 __global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitch, size_t count,
                                   int nseg, const float* __restrict__ data, size_t pitch,
                                   int nbeams, size_t beam_count, float delta, int from_data,
-                                  float* __restrict__ rms) {
+                                  float* __restrict__ rms, BaselineSub sub) {
   int seg = blockIdx.x * blockDim.x + threadIdx.x;
   if (seg >= nseg) return;
   float v[4];
   if (from_data) {
     int ser = seg / nbeams, b = seg % nbeams;
     const float* d = data + (size_t)ser * pitch;
-    for (size_t i = 0; i < count && i < 4; i++)
-      v[i] = fabsf(d[reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i))]);
+    for (size_t i = 0; i < count && i < 4; i++) {
+      const size_t k = reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i));
+      v[i] = fabsf(sub_baseline(sub, (size_t)ser, (unsigned)k, d[k]));
+    }
   } else {
     for (size_t i = 0; i < count && i < 4; i++) v[i] = lev[(size_t)seg * lev_pitch + i];
   }
@@ -331,7 +386,8 @@ __global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitc
   rms[seg] = __fmul_rn(m, (float)1.4862);  // multiplies<hd_float>(x, 1.4862)
 }
 
-cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s) {
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s,
+                      const BaselineSub& sub) {
   int levels;
   size_t rem;
   tree_levels(sb.beam_count, &levels, &rem);
@@ -340,21 +396,23 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
   cudaError_t e;
   if (levels == 0) {
     k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms); note_launch();
+        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms,
+        sub); note_launch();
     return cudaGetLastError();
   }
   int m1 = levels < 5 ? levels : 5;
   size_t ng1 = sb.beam_count / pow5(m1);
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
   k_rms_beams_pass1<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
-      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1); note_launch();
+      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1, sub); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   float* fin;
   size_t fin_pitch, fin_count;
   e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
   if (e != cudaSuccess) return e;
   k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
+      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms,
+      sub); note_launch();
   return cudaGetLastError();
 }
 
@@ -412,7 +470,7 @@ template <int CH>
 __global__ void __launch_bounds__(256) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
-    float* norm_out, int ser_per_block, unsigned* err) {
+    float* norm_out, int ser_per_block, unsigned* err, BaselineSub sub) {
   constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
   constexpr int QN = CH / 128; // float4 per lane per row
   extern __shared__ __align__(128) float sc_smem[];
@@ -528,6 +586,17 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
             float4 x[QN];
 #pragma unroll
             for (int q = 0; q < QN; q++) x[q] = *reinterpret_cast<const float4*>(crow + 4 * lane + 128 * q);
+            if (sub.base) {
+#pragma unroll
+              for (int q = 0; q < QN; q++) {
+                const unsigned i = base + 4u * lane + 128u * q;
+                const size_t ser = (size_t)(s0 + sl);
+                x[q].x = sub_baseline(sub, ser, i, x[q].x);
+                x[q].y = sub_baseline(sub, ser, i + 1, x[q].y);
+                x[q].z = sub_baseline(sub, ser, i + 2, x[q].z);
+                x[q].w = sub_baseline(sub, ser, i + 3, x[q].w);
+              }
+            }
 #pragma unroll
             for (int q = 0; q < QN; q++) {
               x[q].x = div_rn_by(x[q].x, rb, y);
@@ -553,6 +622,7 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
               for (int j = 0; j < 4; j++) {
                 const unsigned ij = i + j;
                 if (ij >= len) { x[j] = 0.f; continue; }
+                x[j] = sub_baseline(sub, (size_t)(s0 + sl), ij, x[j]);
                 unsigned b;
                 if (stride >= (unsigned)CH) b = (ij >= bend && b0 + 1 < (unsigned)nbeams) ? b0 + 1 : b0;
                 else b = min(ij / stride, (unsigned)nbeams - 1);
@@ -590,19 +660,20 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
 template <int CH>
 static cudaError_t launch_scan(const SeriesBatch& sb, const float* rms, float* scan,
                                size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
-                               int ser) {
+                               int ser, const BaselineSub& sub) {
   const int np = ser < 7 ? ser : 7;
   const size_t smem = scan_smem_bytes(ser, sb.nbeams, CH);
   cudaError_t e = raise_smem_limit(k_normalise_scan<CH>, smem);
   if (e != cudaSuccess) return e;
   k_normalise_scan<CH><<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
       sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
-      scan_pitch, norm_out, ser, err); note_launch();
+      scan_pitch, norm_out, ser, err, sub); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
-                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err) {
+                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
+                           const BaselineSub& sub) {
   if (sb.len >= 0xFFFFFF00u || sb.pitch % 4 || scan_pitch % 4 || sb.stride == 0 ||
       sb.pitch < ((sb.len + 3) & ~(size_t)3) || scan_pitch < sb.len + 1 ||
       (reinterpret_cast<uintptr_t>(sb.data) & 15) || (reinterpret_cast<uintptr_t>(scan) & 15) ||
@@ -614,8 +685,8 @@ cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
   // multibeam gulp, and 4 with 512 beat 2 with 512 on the survey gulp)
   int ser = 8;
   while (ser > 1 && (sb.nser + ser - 1) / ser < 296) ser /= 2;
-  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
-  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
+  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser, sub);
+  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser, sub);
 }
 
 // ===========================================================================
@@ -717,6 +788,7 @@ __global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m, in
 // float4 (a thread stride of 80 bytes keeps the 8 lanes of each access phase
 // on distinct banks); widths 1, 2 and 4 read one 28-value window.
 constexpr int BRV_THREADS = 256;
+constexpr int VH_MAXW = 16;  // unscrunched widths the vector kernels handle at once
 
 template <int AH, int BH>
 __device__ __forceinline__ void brv_small(const float* win, float* v) {
@@ -729,10 +801,24 @@ __device__ __forceinline__ float brv_med5(float a, float b, float c, float d, fl
   return MM ? med5_mm(a, b, c, d, e) : med5(a, b, c, d, e);
 }
 
+__device__ __forceinline__ float max5(float a, float b, float c, float d, float e) {
+  return fmaxf(fmaxf(fmaxf(a, b), fmaxf(c, d)), e);
+}
+
+// Folds a thread's largest |boxcar| of width slot wl into smax[wl] (the
+// values are non-negative or NaN, so their bit patterns order as unsigned;
+// a NaN maximum only ever prevents a skip).  Lanes of one slot combine first.
+__device__ __forceinline__ void fold_gmax(unsigned* smax, int wl, float m) {
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, wl);
+  const unsigned key = __reduce_max_sync(same, __float_as_uint(m));
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicMax(&smax[wl], key);
+}
+
 template <bool MM>
 __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, int w0, int nwb,
                            int m, float* la, float* lb, float* __restrict__ out,
-                           size_t out_pitch, size_t ser, size_t g) {
+                           size_t out_pitch, size_t ser, size_t g, unsigned* smax, bool rec) {
   const int n1 = (int)pow5(m - 1);
   const int n1p = (n1 + 3) & ~3;
 
@@ -772,6 +858,11 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
     o.z = brv_med5<MM>(v[10], v[11], v[12], v[13], v[14]);
     o.w = brv_med5<MM>(v[15], v[16], v[17], v[18], v[19]);
     *reinterpret_cast<float4*>(la + wl * n1p + k0) = o;
+    if (rec)
+      fold_gmax(smax, wl,
+                fmaxf(fmaxf(max5(v[0], v[1], v[2], v[3], v[4]), max5(v[5], v[6], v[7], v[8], v[9])),
+                      fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
+                            max5(v[15], v[16], v[17], v[18], v[19]))));
   }
   for (int item = threadIdx.x; item < nwb * rem; item += blockDim.x) {
     const int wl = item / rem, k = 4 * nq + (item - wl * rem);
@@ -781,6 +872,7 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
 #pragma unroll
     for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
     la[wl * n1p + k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+    if (rec) fold_gmax(smax, wl, max5(v[0], v[1], v[2], v[3], v[4]));
   }
   __syncthreads();
 
@@ -801,8 +893,15 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
     pitch_cur = nn;
   }
   // n == 1: one value per width
-  for (int wl = threadIdx.x; wl < nwb; wl += blockDim.x)
+  for (int wl = threadIdx.x; wl < nwb; wl += blockDim.x) {
     out[(ser * nwb + wl) * out_pitch + g] = cur[wl * pitch_cur];
+    if (rec) {
+      // every fold of this group happened before the level-1 barrier; the
+      // next group's folds start after the loop's next barrier
+      ctx.gmax[(ser * nwb + wl) * ctx.ngroups + g] = __uint_as_float(smax[wl]);
+      smax[wl] = 0u;
+    }
+  }
 }
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
@@ -830,6 +929,7 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
                                                                      size_t out_pitch,
                                                                      int ngroups, int gpb) {
   extern __shared__ __align__(16) float dyn[];
+  __shared__ unsigned smax[VH_MAXW];     // this group's largest |boxcar| per width
   const int win4 = (win + 3) & ~3;
   float* tiles = dyn;                    // [2][win4]
   const int n1 = (int)pow5(m - 1);       // level-1 medians per width
@@ -861,6 +961,8 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
   const float last = sc[ctx.scan_len - 1];
   const bool finite = fabsf(last) <= 3.402823466e38f;
   if (g_begin >= g_end || span > (size_t)win) return;
+  const bool rec = ctx.gmax != nullptr && ctx.ngroups > 0;
+  if (threadIdx.x < VH_MAXW) smax[threadIdx.x] = 0u;  // ordered by the loop's first barrier
   prefetch(g_begin, tiles);
   for (int g = g_begin; g < g_end; g++) {
     float* tile = tiles + (size_t)((g - g_begin) & 1) * win4;
@@ -874,9 +976,9 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
     }
     __syncthreads();
     if (finite)
-      brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+      brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, smax, rec);
     else
-      brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g);
+      brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, smax, rec);
   }
 }
 
@@ -904,8 +1006,9 @@ __global__ void k_block_rms_final(WidthCtx ctx, int w0, int nwb, const float* __
   ctx.norm[(size_t)ser * ctx.nw + wi] = __fdiv_rn(1.0f, rms);  // get_rms.cu:365
 }
 
-cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end,
+cudaError_t block_rms(WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end,
                       TreeScratch& ws, cudaStream_t s) {
+  if (w_begin == 0) ctx.ngroups = 0;  // no group maxima unless recorded below
   const int nwb = w_end - w_begin;
   const size_t cnt = (size_t)ctx.nbeams * hw[w_begin].bn;
   for (int wi = w_begin; wi < w_end; wi++)
@@ -940,6 +1043,12 @@ cudaError_t block_rms(const WidthCtx& ctx, const WidthInfo* hw, int w_begin, int
         sizeof(float);
     if (smem <= 200 * 1024) {
       if ((e = raise_smem_limit(k_block_rms_pass1_vec, smem)) != cudaSuccess) return e;
+      // the group maxima of the widths [0, nwb) for count_hits
+      if (ctx.gmax && w_begin == 0 && nwb <= VH_MAXW && nseg * ng1 <= ctx.gmax_cap) {
+        ctx.gsize = (unsigned)pow5(m1);
+        ctx.ngroups = (unsigned)ng1;
+        ctx.gmax_nw = nwb;
+      }
       // about 8 consecutive groups per block, spread evenly
       const size_t nblk_x = (ng1 + 7) / 8;
       const size_t gpb = (ng1 + nblk_x - 1) / nblk_x;
@@ -1222,7 +1331,6 @@ __global__ void __launch_bounds__(HIT_THREADS) k_write_hits_multi(WidthCtx ctx, 
 // consecutive 16-byte words (no bank conflicts).  Per-width counts are kept
 // in 16-bit halves of registers and reduced once per tile.
 // ---------------------------------------------------------------------------
-constexpr int VH_MAXW = 16;
 
 struct VecTile {
   float* tile;
@@ -1397,22 +1505,32 @@ __device__ __forceinline__ void count_vec_body(const float* tile, int offset, in
   }
 }
 
-// Block (x, y): tiles [x * tpb, (x + 1) * tpb) of series y; the next tile's
-// window is copied (cp.async, double buffer) while the current one is counted.
+// Block (x, y): tiles [x * tpb, (x + 1) * tpb) of series y (tpb <= 8); the
+// next tile's window is copied (cp.async, double buffer) while the current one
+// is counted.  With group maxima (ctx.gmax, recorded by the block-RMS pass) a
+// tile whose covering groups all lie below a width's bound dmin cannot hold a
+// hit of that width (|d| <= group max < dmin for each of its samples, and
+// the test is d >= dmin); a tile that no width can hit gets zero counts
+// without being read.  Tiles with hits are appended to hb.tile_list.
 __global__ void __launch_bounds__(HIT_THREADS) k_count_hits_vec(WidthCtx ctx, HitBuffers hb,
                                                                 int nw1, size_t slen,
                                                                 size_t span4, int tpb) {
   extern __shared__ __align__(16) float tiles[];  // [2][span4]
   __shared__ int s_ahead[VH_MAXW], s_behind[VH_MAXW];
-  __shared__ float s_norm[VH_MAXW], s_dmin[VH_MAXW];
+  __shared__ float s_norm[VH_MAXW], s_dmin[VH_MAXW], s_skip[VH_MAXW];
   __shared__ int s_mul;
+  __shared__ unsigned s_need;
   __shared__ unsigned red[HIT_THREADS / 32][VH_MAXW / 2];
   const size_t ser = blockIdx.y;
   const unsigned t_begin = blockIdx.x * (unsigned)tpb;
   const unsigned t_end = min(t_begin + (unsigned)tpb, hb.ntiles);
   const float thresh = ctx.thresh;
   const float* sc = ctx.scan + ser * ctx.scan_pitch;
-  if (threadIdx.x == 0) s_mul = 0;
+  const bool use_gmax = ctx.gmax != nullptr && ctx.ngroups > 0 && ctx.gmax_nw >= nw1;
+  if (threadIdx.x == 0) {
+    s_mul = 0;
+    s_need = use_gmax ? 0u : 0xFFu;
+  }
   __syncthreads();
   if (threadIdx.x < (unsigned)nw1) {
     s_ahead[threadIdx.x] = ctx.winfo[threadIdx.x].ahead;
@@ -1420,20 +1538,56 @@ __global__ void __launch_bounds__(HIT_THREADS) k_count_hits_vec(WidthCtx ctx, Hi
     const float nrm = ctx.norm[ser * ctx.nw + threadIdx.x];
     s_norm[threadIdx.x] = nrm;
     float dm = 0.f;
-    if (!hit_bound(nrm, thresh, &dm)) atomicOr(&s_mul, 1);
+    const bool ok = hit_bound(nrm, thresh, &dm);
+    if (!ok) atomicOr(&s_mul, 1);
     s_dmin[threadIdx.x] = dm;
+    s_skip[threadIdx.x] = ok ? dm : -1.f;  // -1: never skipped (maxima are >= 0)
   }
   if (t_begin >= t_end) return;  // uniform
+  const unsigned ntb = t_end - t_begin;
+  if (use_gmax) {
+    __syncthreads();
+    for (unsigned idx = threadIdx.x; idx < ntb * (unsigned)nw1; idx += blockDim.x) {
+      const unsigned ti = idx / (unsigned)nw1, wi = idx - ti * (unsigned)nw1;
+      const size_t i0 = (size_t)(t_begin + ti) * HIT_TILE;
+      const size_t g_lo = i0 / ctx.gsize, g_hi = (i0 + HIT_TILE - 1) / ctx.gsize;
+      bool need = true;
+      if (g_hi < ctx.ngroups) {
+        // bit patterns of non-negative floats (or NaN, which wins and keeps
+        // the tile) order as unsigned
+        const float* gm = ctx.gmax + (ser * (size_t)ctx.gmax_nw + wi) * ctx.ngroups;
+        unsigned mk = 0;
+        for (size_t g = g_lo; g <= g_hi; g++) mk = max(mk, __float_as_uint(gm[g]));
+        need = !(__uint_as_float(mk) < s_skip[wi]);
+      }
+      if (need) atomicOr(&s_need, 1u << ti);
+    }
+    __syncthreads();
+    // skipped tiles: zero counts (read by the scans and the write pass)
+    for (unsigned idx = threadIdx.x; idx < ntb * (unsigned)nw1; idx += blockDim.x) {
+      const unsigned ti = idx / (unsigned)nw1, wi = idx - ti * (unsigned)nw1;
+      if (!((s_need >> ti) & 1u))
+        hb.tile_cnt[(ser * ctx.nw + wi) * hb.ntiles + t_begin + ti] = 0;
+    }
+  }
+  unsigned rest = s_need & ((1u << ntb) - 1u);
+  if (!rest) return;  // uniform
   const int offset = ctx.offset;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  vec_prefetch(sc, (size_t)t_begin * HIT_TILE, tiles, span4, slen);
-  for (unsigned t = t_begin; t < t_end; t++) {
-    float* tile = tiles + (size_t)((t - t_begin) & 1) * span4;
+  unsigned t = t_begin + (unsigned)(__ffs(rest) - 1);
+  rest &= rest - 1u;
+  int bi = 0;
+  vec_prefetch(sc, (size_t)t * HIT_TILE, tiles, span4, slen);
+  for (;;) {
+    float* tile = tiles + (size_t)bi * span4;
     // the previous tile is counted and its reduction slots are read
     __syncthreads();
-    if (t + 1 < t_end) {
-      vec_prefetch(sc, (size_t)(t + 1) * HIT_TILE, tiles + (size_t)((t + 1 - t_begin) & 1) * span4,
-                   span4, slen);
+    const bool more = rest != 0u;
+    unsigned tn = 0;
+    if (more) {
+      tn = t_begin + (unsigned)(__ffs(rest) - 1);
+      rest &= rest - 1u;
+      vec_prefetch(sc, (size_t)tn * HIT_TILE, tiles + (size_t)(bi ^ 1) * span4, span4, slen);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -1461,25 +1615,27 @@ __global__ void __launch_bounds__(HIT_THREADS) k_count_hits_vec(WidthCtx ctx, Hi
       if (lane == 0) red[warp][p] = c;
     }
     __syncthreads();
+    unsigned tot = 0;
     if (threadIdx.x < (unsigned)nw1) {
       const int wi = threadIdx.x;
-      unsigned tot = 0;
       for (int k = 0; k < HIT_THREADS / 32; k++) tot += (red[k][wi >> 1] >> (16 * (wi & 1))) & 0xFFFFu;
       const size_t sw = ser * ctx.nw + wi;
       hb.tile_cnt[sw * hb.ntiles + t] = tot;
       if (tot) atomicAdd(&hb.sw_cnt[sw], tot);
     }
+    if (__syncthreads_or(tot != 0u) && threadIdx.x == 0 && hb.tile_list)
+      hb.tile_list[atomicAdd(hb.tile_list_n, 1u)] = (unsigned)(ser * hb.ntiles + t);
+    if (!more) break;
+    t = tn;
+    bi ^= 1;
   }
 }
 
 
-__global__ void __launch_bounds__(HIT_THREADS) k_write_hits_vec(WidthCtx ctx, HitBuffers hb,
-                                                                int nw1, size_t slen,
-                                                                size_t span4) {
-  extern __shared__ __align__(16) float tile[];
-  __shared__ unsigned wsum[HIT_THREADS / 32];
-  const size_t ser = blockIdx.y;
-  const unsigned t = blockIdx.x;
+__device__ __forceinline__ void write_hits_vec_tile(const WidthCtx& ctx, const HitBuffers& hb,
+                                                    int nw1, size_t slen, size_t span4,
+                                                    float* tile, unsigned* wsum, size_t ser,
+                                                    unsigned t) {
   unsigned any = 0;
   for (int wi = 0; wi < nw1; wi++) any |= hb.tile_cnt[(ser * ctx.nw + wi) * hb.ntiles + t];
   if (!any) return;  // uniform across the block
@@ -1551,6 +1707,25 @@ __global__ void __launch_bounds__(HIT_THREADS) k_write_hits_vec(WidthCtx ctx, Hi
   }
 }
 
+// Block (x, y): tile x of series y; or, with hb.list_valid, the tiles listed
+// by the count pass (the only ones with hits), strided over the blocks.
+__global__ void __launch_bounds__(HIT_THREADS) k_write_hits_vec(WidthCtx ctx, HitBuffers hb,
+                                                                int nw1, size_t slen,
+                                                                size_t span4) {
+  extern __shared__ __align__(16) float tile[];
+  __shared__ unsigned wsum[HIT_THREADS / 32];
+  if (!hb.list_valid) {
+    write_hits_vec_tile(ctx, hb, nw1, slen, span4, tile, wsum, blockIdx.y, blockIdx.x);
+    return;
+  }
+  const unsigned n = *hb.tile_list_n;
+  for (unsigned idx = blockIdx.x; idx < n; idx += gridDim.x) {
+    const unsigned e = hb.tile_list[idx];
+    write_hits_vec_tile(ctx, hb, nw1, slen, span4, tile, wsum, e / hb.ntiles, e % hb.ntiles);
+    __syncthreads();  // the staged tile is reused by the next item
+  }
+}
+
 // Vector kernels apply when the offset is a multiple of 4 (>= 4), the widths
 // are 1, 2, 4, ... and at most VH_MAXW of them are unscrunched.
 static bool vec_hits_ok(const WidthCtx& ctx, int nw1) {
@@ -1568,6 +1743,7 @@ static bool vec_hits_ok(const WidthCtx& ctx, int nw1) {
 
 cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cudaStream_t s) {
   hb.ntiles = ntiles;
+  hb.list_valid = false;
   cudaError_t e = cudaMemsetAsync(hb.sw_cnt, 0, ((size_t)ctx.nser * ctx.nw + 1) * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   // unscrunched widths share one staged window per tile
@@ -1579,7 +1755,11 @@ cudaError_t count_hits(const WidthCtx& ctx, HitBuffers& hb, unsigned ntiles, cud
   if (vec_hits_ok(ctx, nw1) && 2 * span4 * sizeof(float) <= 200 * 1024) {
     if ((e = raise_smem_limit(k_count_hits_vec, 2 * span4 * sizeof(float))) != cudaSuccess)
       return e;
-    // about 8 consecutive tiles per block, spread evenly
+    if (hb.tile_list) {
+      if ((e = cudaMemsetAsync(hb.tile_list_n, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
+      hb.list_valid = true;
+    }
+    // about 8 consecutive tiles per block (at most 8), spread evenly
     const unsigned nbx = (ntiles + 7) / 8;
     const unsigned tpb = (ntiles + nbx - 1) / nbx;
     k_count_hits_vec<<<dim3((ntiles + tpb - 1) / tpb, ctx.nser), HIT_THREADS,
@@ -1612,8 +1792,13 @@ cudaError_t write_hits(const WidthCtx& ctx, HitBuffers& hb, cudaStream_t s) {
   if (vec_hits_ok(ctx, nw1) && span4 * sizeof(float) <= 200 * 1024) {
     if (cudaError_t e = raise_smem_limit(k_write_hits_vec, span4 * sizeof(float)))
       return e;
-    k_write_hits_vec<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, span4 * sizeof(float), s>>>(
-        ctx, hb, nw1, slen, span4); note_launch();
+    // the listed tiles (count pass), strided over a grid of 8 blocks per SM;
+    // else every tile once
+    const size_t ntile_all = (size_t)hb.ntiles * ctx.nser;
+    const dim3 grid = hb.list_valid ? dim3((unsigned)std::min<size_t>(ntile_all, 148 * 8))
+                                    : dim3(hb.ntiles, ctx.nser);
+    k_write_hits_vec<<<grid, HIT_THREADS, span4 * sizeof(float), s>>>(ctx, hb, nw1, slen,
+                                                                      span4); note_launch();
   } else if (nw1 > 0 && smem <= 200 * 1024) {
     if (cudaError_t e = raise_smem_limit(k_write_hits_multi, smem)) return e;
     k_write_hits_multi<<<dim3(hb.ntiles, ctx.nser), HIT_THREADS, smem, s>>>(ctx, hb, nw1, slen); note_launch();

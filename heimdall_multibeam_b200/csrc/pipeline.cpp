@@ -90,7 +90,7 @@ struct hd_pipeline_t {
   DevBuf dm0, dm0_scan, base, rms, mask, fmask, rms0, nb_scratch;
   DevBuf dd, scan;
   DevBuf ws_a, ws_b;
-  DevBuf winfo, norm;
+  DevBuf winfo, norm, gmax, tile_list;
   DevBuf tile_cnt, tile_off, sw_cnt, sw_off, hit_ind, hit_val, hit_sw;
   DevBuf head, gid;
   // a giant list's arrays
@@ -557,10 +557,12 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     const float cur_dt = P.dt * (float)scr;
     const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
     hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
-    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
-    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
+    // the baseline is subtracted as the RMS and scan kernels read the series
+    hdb::BaselineSub bsub;
+    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s, &bsub));
+    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s, bsub));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan_g, scan_pitch, nullptr, s,
-                               pl->plan->d_err));
+                               pl->plan->d_err, bsub));
     if (gi == 0) cudaEventRecord(pl->ev[4], s);
 
     // ---- widths (pipeline.cu:657-776 at this group's factor) ------------------
@@ -606,6 +608,12 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     wctx.dm_offset = (int)G.d0;
     wctx.norm = pl->norm.as<float>();
     wctx.thresh = P.detect_thresh;
+    // largest |boxcar| per block-RMS group (at most nbeams * stride / 5^5 + 4
+    // groups per series), read by the count pass to skip quiet tiles
+    const size_t gcap = NSg * (size_t)nw * (nbeams * stride_s / 3125 + 5);
+    HD_TRY(pl->gmax.ensure(gcap * sizeof(float)));
+    wctx.gmax = pl->gmax.as<float>();
+    wctx.gmax_cap = gcap;
     int n_ts1 = 0;
     while (n_ts1 < nw && wi[n_ts1].ts == 1) n_ts1++;
     if (n_ts1 > 0) HD_TRY(hdb::block_rms(wctx, wi.data(), 0, n_ts1, ws, s));
@@ -618,6 +626,9 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(pl->tile_off.ensure(nsw * ntiles * sizeof(unsigned)));
     HD_TRY(pl->sw_cnt.ensure((nsw + 1) * sizeof(unsigned)));
     HD_TRY(pl->sw_off.ensure((nsw + 1) * sizeof(unsigned)));
+    HD_TRY(pl->tile_list.ensure((NSg * ntiles + 1) * sizeof(unsigned)));
+    hb.tile_list = pl->tile_list.as<unsigned>();
+    hb.tile_list_n = hb.tile_list + NSg * ntiles;
     hb.tile_cnt = pl->tile_cnt.as<unsigned>();
     hb.tile_off = pl->tile_off.as<unsigned>();
     hb.sw_cnt = pl->sw_cnt.as<unsigned>();

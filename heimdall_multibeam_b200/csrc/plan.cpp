@@ -273,7 +273,7 @@ size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
 // ---------------------------------------------------------------------------
 namespace {
 // bump when the dedispersion kernel changes, so stale choices are not reused
-constexpr uint64_t kDedispKernelGeneration = 3;
+constexpr uint64_t kDedispKernelGeneration = 4;
 
 struct TileCache {
   std::mutex mu;
@@ -403,6 +403,7 @@ static dedisp_error dedisperse_tables(dedisp_plan p, const std::vector<int>& h_d
   a.out_unit = out_unit;
   a.wait_limit = kDedispWaitLimit;
   a.withhold_last = 0;
+  a.one = 1;
   // error-path test (read per call so a test can clear it between gulps):
   // the last channel stage is withheld and the waits give up quickly
   if (const char* e = std::getenv("HDB_TEST_WITHHOLD_STAGE"))

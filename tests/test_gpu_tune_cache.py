@@ -39,7 +39,9 @@ def _run(cache, nsamps=1 << 14, **extra):
     env = dict(os.environ)
     env.pop("HDB_DEDISP_TILE", None)
     env.pop("HDB_DEDISP_TUNE", None)
-    env["HDB_TUNE_CACHE"] = cache
+    env.pop("HDB_TUNE_CACHE", None)
+    if cache is not None:
+        env["HDB_TUNE_CACHE"] = cache
     env.update(extra)
     out = subprocess.run([sys.executable, "-c", SCRIPT, ROOT, str(nsamps)], env=env,
                          capture_output=True, text=True, timeout=300)
@@ -66,9 +68,14 @@ def test_tile_choice_persists_across_processes(hdb, tmp_path):
     assert len(open(cache).read().splitlines()) == 2
 
 
-def test_tile_cache_off(hdb, tmp_path):
+def test_tile_cache_off_and_default_location(hdb, tmp_path):
     """HDB_TUNE_CACHE=0: the default locations under the home and cache
-    directories stay untouched."""
+    directories stay untouched; unset: the XDG cache directory is used."""
     r = _run("0", HOME=str(tmp_path), XDG_CACHE_HOME=str(tmp_path / "xdg"))
     assert r["source"] == "autotuner"
-    assert not any(tmp_path.iterdir())
+    assert not (tmp_path / "xdg" / "heimdall_b200").exists()
+    assert not (tmp_path / ".cache" / "heimdall_b200").exists()
+    # unset: the choice lands in the XDG cache directory
+    unset = _run(None, HOME=str(tmp_path), XDG_CACHE_HOME=str(tmp_path / "xdg"))
+    assert unset["source"] == "autotuner"
+    assert len((tmp_path / "xdg" / "heimdall_b200" / "dedisp_tiles.txt").read_text().splitlines()) == 1
