@@ -130,9 +130,8 @@ struct TreeScratch {
   size_t cap;  // floats in each
 };
 
-// The baseline subtraction of remove_baseline (remove_baseline.cu:90-102),
-// applied where the series is read instead of written back: sample i < nsub
-// of series ser reads x - (stretched baseline at i).  base == nullptr: none.
+// The baseline subtraction of remove_baseline (remove_baseline.cu:90-102):
+// sample i < nsub of series ser becomes x - (stretched baseline at i).
 struct BaselineSub {
   const float* base = nullptr;  // [ser][nbeams][sc] scrunched baseline samples
   unsigned sc = 0, stride = 0, last_start = 0, nsub = 0;
@@ -144,18 +143,13 @@ struct BaselineSub {
 // tree scratch (floats per buffer) remove_baseline needs for nseg beams.
 size_t baseline_samples(size_t stride, size_t smooth_radius);
 size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg);
-// RemoveBaselinePlan::exec for every series (Pipeline/remove_baseline.cu:21-160).
-// With fused == nullptr the baseline is subtracted from the series in place;
-// otherwise the series are left as they are and *fused describes the
-// subtraction for rms_beams and normalise_scan to apply as they read (the
-// same float operations, so the same values), which saves writing and
-// re-reading every series.  base_out must stay untouched until then.
+// RemoveBaselinePlan::exec for every series (Pipeline/remove_baseline.cu:21-160):
+// the baseline is subtracted from the series in place.
 cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                            TreeScratch& ws, cudaStream_t s, BaselineSub* fused = nullptr);
+                            TreeScratch& ws, cudaStream_t s);
 // GetRMSPlanMB::exec_multibeam, vector form (Pipeline/get_rms.cu:236-270):
 // rms[ser*nbeams + b].
-cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s,
-                      const BaselineSub& sub = BaselineSub());
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s);
 // normalise_multibeam (get_rms.cu:372-382) fused with the exclusive prefix sum
 // of MatchedFilterPlan::prep (matched_filter.cu:21-32), sequential association:
 // scan[ser][0..len] (len + 1 values, pitch scan_pitch).  norm_out (nullable,
@@ -163,7 +157,7 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // err (nullable): bit 1 is set if a staging wait timed out.
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
                            size_t scan_pitch, float* norm_out, cudaStream_t s,
-                           unsigned* err = nullptr, const BaselineSub& sub = BaselineSub());
+                           unsigned* err = nullptr);
 
 // Per-width constants of the boxcar loop (Pipeline/pipeline.cu:657-776).
 struct WidthInfo {

@@ -387,17 +387,24 @@ __device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) 
 }
 
 // CTAs per SM the register budget allows: per lane about 12 registers per
-// owned output word (two DMs x {2 packed, 4 drained} sums) plus ~48 others.
-constexpr int dd_min_blocks(int nw, int k, int g) {
-  return (65536 / ((nw + 1) * 32 * (12 * k * g + 48))) < 1
+// owned output word (two DMs x {2 packed, 4 drained} sums; 8 with the
+// compact drain) plus ~48 others.
+constexpr int dd_regs(int k, int g, bool a16) { return (a16 ? 8 : 12) * k * g + 48; }
+constexpr int dd_min_blocks(int nw, int k, int g, bool a16) {
+  return (65536 / ((nw + 1) * 32 * dd_regs(k, g, a16))) < 1
              ? 1
-             : (65536 / ((nw + 1) * 32 * (12 * k * g + 48))) > 3
+             : (65536 / ((nw + 1) * 32 * dd_regs(k, g, a16))) > 3
                    ? 3
-                   : (65536 / ((nw + 1) * 32 * (12 * k * g + 48)));
+                   : (65536 / ((nw + 1) * 32 * dd_regs(k, g, a16)));
 }
 
-template <int NW, int K, int G, int CH, int NST>
-__global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
+// A16 (at most 511 active channels): the sums drained after the first 256 or
+// 257 channels stay packed as two 16-bit lane pairs (each <= 257 * 255 =
+// 65535), and the remaining < 257 channels are added to them in 32 bits when
+// the output is written; 8 rather than 12 registers per output word, so
+// more CTAs fit an SM.
+template <int NW, int K, int G, int CH, int NST, bool A16>
+__global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G, A16))
     k_dedisp(DedispArgs a) {
   static_assert(K % 2 == 1, "odd K keeps the strided shared loads conflict-free");
   extern __shared__ __align__(128) uint8_t smem[];
@@ -478,14 +485,17 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
   // channels between drains every byte-lane sum is <= 65535, so
   // raw - (odd << 8) = E0 + 2^16 E2 exactly: the even-byte sums.
   constexpr int W = K * G;  // output words per lane and DM
+  constexpr int NA = A16 ? 2 : 4;
   uint32_t pk[2][W][2];
-  int acc[2][W][4];
+  // drained sums: samples 0..3 in 32 bits, or (A16) {even, odd} lane pairs
+  uint32_t acc[2][W][NA];
 #pragma unroll
   for (int d = 0; d < 2; d++)
 #pragma unroll
     for (int w = 0; w < W; w++) {
       pk[d][w][0] = pk[d][w][1] = 0;
-      acc[d][w][0] = acc[d][w][1] = acc[d][w][2] = acc[d][w][3] = 0;
+#pragma unroll
+      for (int q = 0; q < NA; q++) acc[d][w][q] = 0;
     }
   auto drain = [&]() {
 #pragma unroll
@@ -494,10 +504,16 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
       for (int w = 0; w < W; w++) {
         const uint32_t odd = pk[d][w][1];
         const uint32_t even = pk[d][w][0] - (odd << 8);
-        acc[d][w][0] += (int)(even & 0xFFFFu);
-        acc[d][w][2] += (int)(even >> 16);
-        acc[d][w][1] += (int)(odd & 0xFFFFu);
-        acc[d][w][3] += (int)(odd >> 16);
+        if constexpr (A16) {
+          // only drain before the last: the accumulators are still zero
+          acc[d][w][0] = even;
+          acc[d][w][1] = odd;
+        } else {
+          acc[d][w][0] += even & 0xFFFFu;
+          acc[d][w][2] += even >> 16;
+          acc[d][w][1] += odd & 0xFFFFu;
+          acc[d][w][3] += odd >> 16;
+        }
         pk[d][w][0] = pk[d][w][1] = 0;
       }
   };
@@ -574,7 +590,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
                                 :: "r"(smem_addr(&empty[buf])) : "memory");
   }
   if (failed) return;
-  drain();
+  if constexpr (!A16) drain();
   float* __restrict__ out = a.out + (size_t)blockIdx.z * a.out_unit;
 #pragma unroll
   for (int d = 0; d < 2; d++) {
@@ -587,8 +603,21 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
       for (int j = 0; j < K; j++) {
         const int w = K * g + j;
         size_t t = t0 + 4 * (32 * K * g + lw + j);
-        float4 v = make_float4((float)acc[d][w][0], (float)acc[d][w][1], (float)acc[d][w][2],
-                               (float)acc[d][w][3]);
+        uint32_t s0, s1, s2, s3;
+        if constexpr (A16) {
+          const uint32_t odd = pk[d][w][1];
+          const uint32_t even = pk[d][w][0] - (odd << 8);
+          s0 = (even & 0xFFFFu) + (acc[d][w][0] & 0xFFFFu);
+          s2 = (even >> 16) + (acc[d][w][0] >> 16);
+          s1 = (odd & 0xFFFFu) + (acc[d][w][1] & 0xFFFFu);
+          s3 = (odd >> 16) + (acc[d][w][1] >> 16);
+        } else {
+          s0 = acc[d][w][0];
+          s1 = acc[d][w][1];
+          s2 = acc[d][w][2];
+          s3 = acc[d][w][3];
+        }
+        float4 v = make_float4((float)s0, (float)s1, (float)s2, (float)s3);
         if (t + 3 < a.nout) {
           *reinterpret_cast<float4*>(o + t) = v;
         } else {
@@ -765,7 +794,9 @@ size_t dd_smem(int dm_block, int ch, int rowb) {
 }
 template <int NW, int K, int G, int CH>
 cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
-  auto kern = k_dedisp<NW, K, G, CH, DD_NST>;
+  // the compact drain holds two 257-channel chunks at most
+  auto kern = a.nact <= 511 ? k_dedisp<NW, K, G, CH, DD_NST, true>
+                            : k_dedisp<NW, K, G, CH, DD_NST, false>;
   const size_t smem = dd_smem(2 * NW, CH, a.rowb);
   cudaError_t e = raise_smem_limit(kern, smem);
   if (e != cudaSuccess) return e;

@@ -224,7 +224,7 @@ __device__ __forceinline__ float stretch_beam_at_nc(const float* in, unsigned i,
 // x - stretched baseline at sample i of series ser (i < nsub), else x
 __device__ __forceinline__ float sub_baseline(const BaselineSub& b, size_t ser, unsigned i,
                                               float x) {
-  if (!b.base || i >= b.nsub) return x;
+  if (i >= b.nsub) return x;
   const float* bs = b.base + ser * (size_t)b.nbeams * b.sc;
   const float v = (i < b.last_start)
                       ? stretch_beam_at_nc(bs, i, b.step2, i / b.stride)
@@ -272,8 +272,7 @@ size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg) {
 }
 
 cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                            TreeScratch& ws, cudaStream_t s, BaselineSub* fused) {
-  if (fused) *fused = BaselineSub();
+                            TreeScratch& ws, cudaStream_t s) {
   BaselinePlan p = baseline_plan(sb.stride, smooth_radius);
   if (p.sample_count == 0) return cudaSuccess;
   const size_t sc = p.sample_count, cr = p.count_round;
@@ -330,10 +329,6 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   b.nbeams = sb.nbeams;
   b.step2 = step2;
   b.step3 = step3;
-  if (fused) {
-    *fused = b;
-    return cudaSuccess;
-  }
   const size_t nq = (nsub + 3) / 4;
   dim3 grid((unsigned)((nq + 255) / 256 < 4096 ? (nq + 255) / 256 : 4096), sb.nser);
   k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, b); note_launch();
@@ -349,8 +344,7 @@ __device__ __forceinline__ size_t reblock_index(size_t beam, float delta, unsign
 
 __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, int nbeams,
                                   size_t beam_count, float delta, int m,
-                                  float* __restrict__ out, size_t out_pitch_beam,
-                                  BaselineSub sub) {
+                                  float* __restrict__ out, size_t out_pitch_beam) {
   __shared__ float sm[625 + 125];
   const int b = blockIdx.y;
   const size_t ser = blockIdx.z;
@@ -359,8 +353,7 @@ __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, 
   const size_t o0 = (size_t)b * beam_count + g * pow5(m);
   float r = block_tree([&](int i) {
     unsigned o = (unsigned)(o0 + i);
-    const size_t k = reblock_index((size_t)b, delta, o);
-    return fabsf(sub_baseline(sub, ser, (unsigned)k, d[k]));
+    return fabsf(d[reblock_index((size_t)b, delta, o)]);
   }, m, sm);
   if (threadIdx.x == 0) out[(ser * nbeams + b) * out_pitch_beam + g] = r;
 }
@@ -368,17 +361,15 @@ __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, 
 __global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitch, size_t count,
                                   int nseg, const float* __restrict__ data, size_t pitch,
                                   int nbeams, size_t beam_count, float delta, int from_data,
-                                  float* __restrict__ rms, BaselineSub sub) {
+                                  float* __restrict__ rms) {
   int seg = blockIdx.x * blockDim.x + threadIdx.x;
   if (seg >= nseg) return;
   float v[4];
   if (from_data) {
     int ser = seg / nbeams, b = seg % nbeams;
     const float* d = data + (size_t)ser * pitch;
-    for (size_t i = 0; i < count && i < 4; i++) {
-      const size_t k = reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i));
-      v[i] = fabsf(sub_baseline(sub, (size_t)ser, (unsigned)k, d[k]));
-    }
+    for (size_t i = 0; i < count && i < 4; i++)
+      v[i] = fabsf(d[reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i))]);
   } else {
     for (size_t i = 0; i < count && i < 4; i++) v[i] = lev[(size_t)seg * lev_pitch + i];
   }
@@ -386,8 +377,7 @@ __global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitc
   rms[seg] = __fmul_rn(m, (float)1.4862);  // multiplies<hd_float>(x, 1.4862)
 }
 
-cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s,
-                      const BaselineSub& sub) {
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s) {
   int levels;
   size_t rem;
   tree_levels(sb.beam_count, &levels, &rem);
@@ -396,23 +386,21 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
   cudaError_t e;
   if (levels == 0) {
     k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms,
-        sub); note_launch();
+        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms); note_launch();
     return cudaGetLastError();
   }
   int m1 = levels < 5 ? levels : 5;
   size_t ng1 = sb.beam_count / pow5(m1);
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
   k_rms_beams_pass1<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
-      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1, sub); note_launch();
+      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   float* fin;
   size_t fin_pitch, fin_count;
   e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
   if (e != cudaSuccess) return e;
   k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms,
-      sub); note_launch();
+      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
   return cudaGetLastError();
 }
 
@@ -470,7 +458,7 @@ template <int CH>
 __global__ void __launch_bounds__(256) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
-    float* norm_out, int ser_per_block, unsigned* err, BaselineSub sub) {
+    float* norm_out, int ser_per_block, unsigned* err) {
   constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
   constexpr int QN = CH / 128; // float4 per lane per row
   extern __shared__ __align__(128) float sc_smem[];
@@ -586,17 +574,6 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
             float4 x[QN];
 #pragma unroll
             for (int q = 0; q < QN; q++) x[q] = *reinterpret_cast<const float4*>(crow + 4 * lane + 128 * q);
-            if (sub.base) {
-#pragma unroll
-              for (int q = 0; q < QN; q++) {
-                const unsigned i = base + 4u * lane + 128u * q;
-                const size_t ser = (size_t)(s0 + sl);
-                x[q].x = sub_baseline(sub, ser, i, x[q].x);
-                x[q].y = sub_baseline(sub, ser, i + 1, x[q].y);
-                x[q].z = sub_baseline(sub, ser, i + 2, x[q].z);
-                x[q].w = sub_baseline(sub, ser, i + 3, x[q].w);
-              }
-            }
 #pragma unroll
             for (int q = 0; q < QN; q++) {
               x[q].x = div_rn_by(x[q].x, rb, y);
@@ -622,7 +599,6 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
               for (int j = 0; j < 4; j++) {
                 const unsigned ij = i + j;
                 if (ij >= len) { x[j] = 0.f; continue; }
-                x[j] = sub_baseline(sub, (size_t)(s0 + sl), ij, x[j]);
                 unsigned b;
                 if (stride >= (unsigned)CH) b = (ij >= bend && b0 + 1 < (unsigned)nbeams) ? b0 + 1 : b0;
                 else b = min(ij / stride, (unsigned)nbeams - 1);
@@ -660,20 +636,19 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
 template <int CH>
 static cudaError_t launch_scan(const SeriesBatch& sb, const float* rms, float* scan,
                                size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
-                               int ser, const BaselineSub& sub) {
+                               int ser) {
   const int np = ser < 7 ? ser : 7;
   const size_t smem = scan_smem_bytes(ser, sb.nbeams, CH);
   cudaError_t e = raise_smem_limit(k_normalise_scan<CH>, smem);
   if (e != cudaSuccess) return e;
   k_normalise_scan<CH><<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
       sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
-      scan_pitch, norm_out, ser, err, sub); note_launch();
+      scan_pitch, norm_out, ser, err); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
-                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
-                           const BaselineSub& sub) {
+                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err) {
   if (sb.len >= 0xFFFFFF00u || sb.pitch % 4 || scan_pitch % 4 || sb.stride == 0 ||
       sb.pitch < ((sb.len + 3) & ~(size_t)3) || scan_pitch < sb.len + 1 ||
       (reinterpret_cast<uintptr_t>(sb.data) & 15) || (reinterpret_cast<uintptr_t>(scan) & 15) ||
@@ -685,8 +660,8 @@ cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
   // multibeam gulp, and 4 with 512 beat 2 with 512 on the survey gulp)
   int ser = 8;
   while (ser > 1 && (sb.nser + ser - 1) / ser < 296) ser /= 2;
-  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser, sub);
-  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser, sub);
+  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
+  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
 }
 
 // ===========================================================================
@@ -805,22 +780,15 @@ __device__ __forceinline__ float max5(float a, float b, float c, float d, float 
   return fmaxf(fmaxf(fmaxf(a, b), fmaxf(c, d)), e);
 }
 
-// Folds a thread's largest |boxcar| of width slot wl into smax[wl] (the
-// values are non-negative or NaN, so their bit patterns order as unsigned;
-// a NaN maximum only ever prevents a skip).  Lanes of one slot combine first.
-__device__ __forceinline__ void fold_gmax(unsigned* smax, int wl, float m) {
-  const unsigned act = __activemask();
-  const unsigned same = __match_any_sync(act, wl);
-  const unsigned key = __reduce_max_sync(same, __float_as_uint(m));
-  if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicMax(&smax[wl], key);
-}
-
 template <bool MM>
 __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, int w0, int nwb,
                            int m, float* la, float* lb, float* __restrict__ out,
-                           size_t out_pitch, size_t ser, size_t g, unsigned* smax, bool rec) {
+                           size_t out_pitch, size_t ser, size_t g, float* srun, bool rec) {
   const int n1 = (int)pow5(m - 1);
   const int n1p = (n1 + 3) & ~3;
+  // srun[wl][q]: largest |boxcar| of level-1 item q of width slot wl (runs of
+  // 20 samples, then the < 4 remaining single medians)
+  const int rp = n1 / 4 + 4;
 
   // ---- level 1 ----
   const int nq = n1 / 4, rem = n1 - 4 * nq;
@@ -859,10 +827,10 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
     o.w = brv_med5<MM>(v[15], v[16], v[17], v[18], v[19]);
     *reinterpret_cast<float4*>(la + wl * n1p + k0) = o;
     if (rec)
-      fold_gmax(smax, wl,
-                fmaxf(fmaxf(max5(v[0], v[1], v[2], v[3], v[4]), max5(v[5], v[6], v[7], v[8], v[9])),
-                      fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
-                            max5(v[15], v[16], v[17], v[18], v[19]))));
+      srun[wl * rp + k0 / 4] =
+          fmaxf(fmaxf(max5(v[0], v[1], v[2], v[3], v[4]), max5(v[5], v[6], v[7], v[8], v[9])),
+                fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
+                      max5(v[15], v[16], v[17], v[18], v[19])));
   }
   for (int item = threadIdx.x; item < nwb * rem; item += blockDim.x) {
     const int wl = item / rem, k = 4 * nq + (item - wl * rem);
@@ -872,9 +840,23 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
 #pragma unroll
     for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
     la[wl * n1p + k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
-    if (rec) fold_gmax(smax, wl, max5(v[0], v[1], v[2], v[3], v[4]));
+    if (rec) srun[wl * rp + nq + (k - 4 * nq)] = max5(v[0], v[1], v[2], v[3], v[4]);
   }
   __syncthreads();
+  if (rec) {
+    // one warp per width slot: the group's largest |boxcar|.  Values are
+    // non-negative or NaN, so their bit patterns order as unsigned (a NaN
+    // maximum only ever keeps a tile from being skipped); fmaxf above drops
+    // a NaN unless all its operands are NaN, and no sample is then left out
+    // of a maximum that decides a skip: a NaN boxcar never passes the test.
+    const int lane = threadIdx.x & 31;
+    for (int wl = threadIdx.x >> 5; wl < nwb; wl += blockDim.x >> 5) {
+      unsigned mk = 0;
+      for (int q = lane; q < nq + rem; q += 32) mk = max(mk, __float_as_uint(srun[wl * rp + q]));
+      mk = __reduce_max_sync(0xffffffffu, mk);
+      if (lane == 0) ctx.gmax[(ser * nwb + wl) * ctx.ngroups + g] = __uint_as_float(mk);
+    }
+  }
 
   // ---- levels 2..m, all widths per barrier ----
   float* cur = la;
@@ -893,15 +875,8 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
     pitch_cur = nn;
   }
   // n == 1: one value per width
-  for (int wl = threadIdx.x; wl < nwb; wl += blockDim.x) {
+  for (int wl = threadIdx.x; wl < nwb; wl += blockDim.x)
     out[(ser * nwb + wl) * out_pitch + g] = cur[wl * pitch_cur];
-    if (rec) {
-      // every fold of this group happened before the level-1 barrier; the
-      // next group's folds start after the loop's next barrier
-      ctx.gmax[(ser * nwb + wl) * ctx.ngroups + g] = __uint_as_float(smax[wl]);
-      smax[wl] = 0u;
-    }
-  }
 }
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
@@ -929,13 +904,13 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
                                                                      size_t out_pitch,
                                                                      int ngroups, int gpb) {
   extern __shared__ __align__(16) float dyn[];
-  __shared__ unsigned smax[VH_MAXW];     // this group's largest |boxcar| per width
   const int win4 = (win + 3) & ~3;
   float* tiles = dyn;                    // [2][win4]
   const int n1 = (int)pow5(m - 1);       // level-1 medians per width
   const int n1p = (n1 + 3) & ~3;         // row pitch: 16-byte aligned rows
   float* la = dyn + 2 * win4;            // [nwb][n1p]
-  float* lb = la + nwb * n1p;            // [nwb][n1 / 5]
+  float* lb = la + nwb * n1p;            // [nwb][n1 / 5 + 1]
+  float* srun = lb + nwb * (n1 / 5 + 1); // [nwb][n1 / 4 + 4] (group maxima)
   const size_t ser = blockIdx.y;
   const int g_begin = blockIdx.x * gpb;
   const int g_end = min(g_begin + gpb, ngroups);
@@ -962,7 +937,6 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
   const bool finite = fabsf(last) <= 3.402823466e38f;
   if (g_begin >= g_end || span > (size_t)win) return;
   const bool rec = ctx.gmax != nullptr && ctx.ngroups > 0;
-  if (threadIdx.x < VH_MAXW) smax[threadIdx.x] = 0u;  // ordered by the loop's first barrier
   prefetch(g_begin, tiles);
   for (int g = g_begin; g < g_end; g++) {
     float* tile = tiles + (size_t)((g - g_begin) & 1) * win4;
@@ -976,9 +950,9 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
     }
     __syncthreads();
     if (finite)
-      brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, smax, rec);
+      brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, srun, rec);
     else
-      brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, smax, rec);
+      brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, srun, rec);
   }
 }
 
@@ -1038,9 +1012,9 @@ cudaError_t block_rms(WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end
   if (vec && ctx.nbeams == 1) {
     const size_t win = pow5(m1) + 2 * (size_t)ctx.offset + 2;
     const size_t n1 = pow5(m1 - 1);
-    const size_t smem =
-        (2 * ((win + 3) & ~(size_t)3) + nwb * ((n1 + 3) & ~(size_t)3) + nwb * (n1 / 5 + 1)) *
-        sizeof(float);
+    const size_t smem = (2 * ((win + 3) & ~(size_t)3) + nwb * ((n1 + 3) & ~(size_t)3) +
+                         nwb * (n1 / 5 + 1) + nwb * (n1 / 4 + 4)) *
+                        sizeof(float);
     if (smem <= 200 * 1024) {
       if ((e = raise_smem_limit(k_block_rms_pass1_vec, smem)) != cudaSuccess) return e;
       // the group maxima of the widths [0, nwb) for count_hits

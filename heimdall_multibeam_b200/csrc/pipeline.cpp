@@ -557,12 +557,10 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     const float cur_dt = P.dt * (float)scr;
     const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
     hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
-    // the baseline is subtracted as the RMS and scan kernels read the series
-    hdb::BaselineSub bsub;
-    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s, &bsub));
-    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s, bsub));
+    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
+    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan_g, scan_pitch, nullptr, s,
-                               pl->plan->d_err, bsub));
+                               pl->plan->d_err));
     if (gi == 0) cudaEventRecord(pl->ev[4], s);
 
     // ---- widths (pipeline.cu:657-776 at this group's factor) ------------------
