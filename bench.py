@@ -528,7 +528,52 @@ def classifier_bench(args, H, torch, dev, pl):
             "note": "untrained weights (the work does not depend on their values); one "
                     "persistent fused kernel (k_clf_infer, one CTA per SM): mma.sync BF16 "
                     "convolutions with FP32 accumulation, FC layers in the same kernel"}
+    out["training_gemm"] = training_gemm_bench(args, H, torch, dev, peaks, peak_kind)
     return out
+
+
+def training_gemm_bench(args, H, torch, dev, peaks, peak_kind):
+    """The training GEMM kernel (hd_bf16_gemm_tc: tcgen05.mma, TMEM
+    accumulators, TMA-staged operands) on an im2col-shaped product: M =
+    131072 patch pixels, N = 128 output channels (the kernel's widest tile),
+    K = 1152 (3 x 3 taps x 128 input channels), FP32 out.  With N <= 128 the
+    arithmetic intensity stays below the B200's ridge point, so the bound is
+    HBM (A read once); both fractions are reported."""
+    import ctypes as C
+    M, N, K = 131072, 128, 1152
+    g = torch.Generator(device=dev).manual_seed(9)
+    A = torch.randn((M, K), generator=g, device=dev).to(torch.bfloat16)
+    B = torch.randn((N, K), generator=g, device=dev).to(torch.bfloat16)
+    Cm = torch.empty((M, N), device=dev, dtype=torch.float32)
+    L = H.lib()
+
+    def run():
+        err = L.hd_bf16_gemm_tc(M, N, K, A.data_ptr(), K, 1, B.data_ptr(), 1, K,
+                                C.cast(Cm.data_ptr(), C.POINTER(C.c_float)), N, 1, 0, 1)
+        assert err == H.HD_NO_ERROR, H.error_string(err)
+
+    for _ in range(3):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = max(args.steps, 5)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(n):
+        run()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / n
+    flops = 2.0 * M * N * K
+    nbytes = 2 * M * K + 2 * N * K + 4 * M * N
+    tf = flops / (ms / 1e3) / 1e12
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"api": "hd_bf16_gemm_tc", "m": M, "n": N, "k": K, "ms": round(ms, 4),
+            "tensor": {"achieved_tflops": round(tf, 2), "peak": peaks["bf16_tflops"],
+                       "frac": round(tf / peaks["bf16_tflops"], 4), "peak_kind": f"of {peak_kind}"},
+            "hbm": {"bytes": nbytes, "achieved_gbs": round(gbs, 1), "peak": peaks["hbm_gbs"],
+                    "frac": round(gbs / peaks["hbm_gbs"], 4), "peak_kind": f"of {peak_kind}"},
+            "bound": "hbm" if flops / nbytes < peaks["bf16_tflops"] * 1e3 / peaks["hbm_gbs"]
+            else "tensor"}
 
 
 def uneven_bench(args, H, torch, dev, barrier, dist, world):

@@ -775,17 +775,20 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(hdb::cluster_init(gb, (int)ngiants, s));
     hdb::ClusterArgs ca{(int)ngiants, P.cand_sep_time, P.cand_sep_filter, dm_tol,
                         (unsigned long long)(nsamps / nbeams)};
-    // sweeps until one changes nothing; the fixed point is idempotent, so the
-    // flag is read after every second sweep (one more sweep than needed at
-    // most, half the host round trips)
+    // sweeps until one changes nothing; the fixed point is idempotent, so
+    // the sweeps run in pairs, each with its own flag, and the host reads
+    // both flags once per pair: the loop ends when the pair's second sweep
+    // changed nothing (half the host round trips, no sweep beyond the one
+    // that confirms the fixed point)
     unsigned* changed = pl->small.as<unsigned>() + 8;
     for (unsigned it = 0; it <= ngiants; it += 2) {
-      HD_TRY(cudaMemsetAsync(changed, 0, sizeof(unsigned), s));
+      HD_TRY(cudaMemsetAsync(changed, 0, 2 * sizeof(unsigned), s));
       HD_TRY(hdb::cluster_sweep(ca, gb, changed, s));
-      HD_TRY(hdb::cluster_sweep(ca, gb, changed, s));
-      HD_TRY(cudaMemcpyAsync(pl->h_small + 8, changed, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+      HD_TRY(hdb::cluster_sweep(ca, gb, changed + 1, s));
+      HD_TRY(cudaMemcpyAsync(pl->h_small + 8, changed, 2 * sizeof(unsigned),
+                             cudaMemcpyDeviceToHost, s));
       HD_TRY(cudaStreamSynchronize(s));
-      if (pl->h_small[8] == 0) break;
+      if (pl->h_small[9] == 0) break;
     }
     // ---- merge -----------------------------------------------------------------
     size_t G = ngiants;
