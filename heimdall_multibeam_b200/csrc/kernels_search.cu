@@ -633,97 +633,6 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       mbar_wait(&full[st % SC_NB], (st / SC_NB) & 1u, SC_WAIT_LIMIT);
 }
 
-// Single-beam series without a normalised copy, many series: one series per
-// lane.  A warp owns 32 series; each lane copies its own series' next stage
-// (CH samples, one bulk copy) into the warp's ring of NB stages, all 32
-// copies completing one mbarrier, and runs the normalise + sequential prefix
-// sum of its series from shared memory into the scan row with plain stores.
-// No block-wide barrier: the chains of 32 series share each warp
-// instruction, and the ring keeps NB - 1 stages of every series in flight.
-constexpr int SL_CH = 128, SL_NB = 4;
-
-size_t scan_lanes_smem_bytes() { return 128 + (size_t)SL_NB * 32 * (SL_CH + 4) * sizeof(float); }
-
-__global__ void __launch_bounds__(32) k_scan_lanes(const float* __restrict__ data, size_t pitch,
-                                                   int nser, unsigned len,
-                                                   const float* __restrict__ rms,
-                                                   float* __restrict__ scan, size_t scan_pitch,
-                                                   unsigned* err) {
-  constexpr int CH = SL_CH, NB = SL_NB, ROW = CH + 4;  // row pitch: lane l's float4 on banks 4l..
-  extern __shared__ __align__(128) float sl_smem[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(sl_smem);  // [NB], first 128 bytes
-  float* rows = sl_smem + 32;                              // [NB][32][ROW]
-  const int lane = threadIdx.x;
-  const int s0 = blockIdx.x * 32;
-  const int nb = min(32, nser - s0);
-  const bool mine = lane < nb;
-  const size_t ser = (size_t)s0 + (size_t)lane;
-  const unsigned len4 = (len + 3u) & ~3u;
-  const unsigned nstage = (len + CH - 1) / CH;
-  if (lane == 0) {
-    for (int b = 0; b < NB; b++) mbar_init(&full[b], 1);
-    fence_mbar_init();
-  }
-  __syncwarp();
-  auto request = [&](unsigned st) {
-    uint64_t* bar = &full[st % NB];
-    const unsigned base = st * CH;
-    const unsigned bytes = (min(base + (unsigned)CH, len4) - base) * 4u;
-    if (lane == 0) mbar_expect_tx(bar, bytes * (unsigned)nb);
-    __syncwarp();
-    // the buffer was last read by this warp's lanes (generic proxy)
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (mine) bulk_g2s(rows + ((size_t)(st % NB) * 32 + lane) * ROW, data + ser * pitch + base,
-                       bytes, bar);
-  };
-  float rb = 1.f, y = 1.f;
-  if (mine) {
-    rb = rms[ser];
-    y = __frcp_rn(rb);
-  }
-  for (unsigned st = 0; st + 1 < (unsigned)NB && st < nstage; st++) request(st);
-  float* orow = scan + ser * scan_pitch;
-  float sum = 0.f;
-  unsigned st = 0;
-  for (; st < nstage; st++) {
-    if (!mbar_wait(&full[st % NB], (st / NB) & 1u, SC_WAIT_LIMIT)) {
-      if (lane == 0 && err) atomicOr(err, 2u);
-      break;
-    }
-    if (mine) {
-      const float* row = rows + ((size_t)(st % NB) * 32 + lane) * ROW;
-      const unsigned base = st * CH;
-      if (base + CH <= len) {
-#pragma unroll 4
-        for (int e = 0; e < CH; e += 4) {
-          const float4 v = *reinterpret_cast<const float4*>(row + e);
-          float4 o;
-          o.x = sum; sum = __fadd_rn(sum, div_rn_by(v.x, rb, y));
-          o.y = sum; sum = __fadd_rn(sum, div_rn_by(v.y, rb, y));
-          o.z = sum; sum = __fadd_rn(sum, div_rn_by(v.z, rb, y));
-          o.w = sum; sum = __fadd_rn(sum, div_rn_by(v.w, rb, y));
-          *reinterpret_cast<float4*>(orow + base + e) = o;
-        }
-      } else {
-        for (unsigned e = 0; base + e < len; e++) {
-          orow[base + e] = sum;
-          sum = __fadd_rn(sum, div_rn_by(row[e], rb, y));
-        }
-      }
-    }
-    __syncwarp();  // every lane is done with buffer st % NB
-    if (st + NB - 1 < nstage) request(st + NB - 1);
-  }
-  if (st < nstage) {
-    // a wait gave up: let the copies already issued (stages st .. st + NB - 2)
-    // land before leaving, again with bounded waits
-    for (unsigned k = st; k < nstage && k + 1 < st + NB; k++)
-      mbar_wait(&full[k % NB], (k / NB) & 1u, SC_WAIT_LIMIT);
-    return;
-  }
-  if (mine) orow[len] = sum;
-}
-
 template <int CH>
 static cudaError_t launch_scan(const SeriesBatch& sb, const float* rms, float* scan,
                                size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
@@ -746,16 +655,6 @@ cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
       (norm_out && (reinterpret_cast<uintptr_t>(norm_out) & 15)))
     return cudaErrorInvalidValue;
   if (sb.nser <= 0) return cudaSuccess;
-  // many single-beam series and no normalised copy: one series per lane,
-  // once there are at least as many warps as SMs
-  if (sb.nbeams == 1 && !norm_out && sb.nser >= 32 * 148) {
-    const size_t smem = scan_lanes_smem_bytes();
-    cudaError_t e = raise_smem_limit(k_scan_lanes, smem);
-    if (e != cudaSuccess) return e;
-    k_scan_lanes<<<(unsigned)((sb.nser + 31) / 32), 32, smem, s>>>(
-        sb.data, sb.pitch, sb.nser, (unsigned)sb.len, rms, scan, scan_pitch, err); note_launch();
-    return cudaGetLastError();
-  }
   // series per block: enough blocks to cover the SMs twice where possible, at
   // most 8 (measured: 8 series with 256-sample stages beat 16 with 128 on the
   // multibeam gulp, and 4 with 512 beat 2 with 512 on the survey gulp)
