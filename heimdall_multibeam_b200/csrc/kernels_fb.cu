@@ -368,10 +368,9 @@ __global__ void k_nb_zap(uint32_t* __restrict__ data, size_t nsamps, int units, 
 // 1.33 at K = 3, 1.2 at K = 5).  Each realigned word is split into two
 // 16-bit lane pairs (even/odd samples); two channels are summed per 3-input
 // add, so one add accumulates four sample-channel terms.  The 16-bit lanes
-// are drained after at most 257 channels (255 * 257 = 65535), so the sums
-// are exact (the drain is described above the kernel).  Every mbarrier wait
-// is bounded; a wait that gives up sets bit 0 of a.err and the warp leaves
-// its loop.
+// are drained into 32-bit sums after at most 257 channels (255 * 257 =
+// 65535), so the sums are exact.  Every mbarrier wait is bounded; a wait that
+// gives up sets bit 0 of a.err and the warp leaves its loop.
 //
 // Pipe balance: the shifts, byte permutes and 3-input adds all issue to the
 // ALU pipe, which bounds the kernel, while the FMA pipe idles.  The odd-byte
@@ -387,29 +386,25 @@ __device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) 
   return d;
 }
 
-// CTAs per SM the register budget allows: per lane about 8 registers per
-// owned output word (two DMs x {2 packed, 2 drained} sums) plus ~48 others.
-constexpr int dd_regs(int k, int g) { return 8 * k * g + 48; }
-constexpr int dd_min_blocks(int nw, int k, int g) {
-  return (65536 / ((nw + 1) * 32 * dd_regs(k, g))) < 1
+// CTAs per SM the register budget allows: per lane about 12 registers per
+// owned output word (two DMs x {2 packed, 4 drained} sums; 8 with the
+// compact drain) plus ~48 others.
+constexpr int dd_regs(int k, int g, bool a16) { return (a16 ? 8 : 12) * k * g + 48; }
+constexpr int dd_min_blocks(int nw, int k, int g, bool a16) {
+  return (65536 / ((nw + 1) * 32 * dd_regs(k, g, a16))) < 1
              ? 1
-             : (65536 / ((nw + 1) * 32 * dd_regs(k, g))) > 3
+             : (65536 / ((nw + 1) * 32 * dd_regs(k, g, a16))) > 3
                    ? 3
-                   : (65536 / ((nw + 1) * 32 * dd_regs(k, g)));
+                   : (65536 / ((nw + 1) * 32 * dd_regs(k, g, a16)));
 }
 
-// Drained sums stay packed: after the first chunk of at most 257 channels
-// the even- and odd-sample sums are kept as two 16-bit lane pairs (each lane
-// <= 257 * 255 = 65535); after the second chunk both chunks are added in 32
-// bits and flushed into the output row (the first flush stores, later ones
-// add the float row's values back in: every partial is an integer below
-// 2^24, so the float sums are exact).  Only the thread that owns an output
-// word ever reads or writes it.  A gulp of at most 511 active channels has
-// at most one drain before the end and writes its output once: the FL =
-// false instance, which leaves the flush out (and with it the registers it
-// needs), serves those gulps; FL = true the others.
-template <int NW, int K, int G, int CH, int NST, bool FL>
-__global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
+// A16 (at most 511 active channels): the sums drained after the first 256 or
+// 257 channels stay packed as two 16-bit lane pairs (each <= 257 * 255 =
+// 65535), and the remaining < 257 channels are added to them in 32 bits when
+// the output is written; 8 rather than 12 registers per output word, so
+// more CTAs fit an SM.
+template <int NW, int K, int G, int CH, int NST, bool A16>
+__global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G, A16))
     k_dedisp(DedispArgs a) {
   static_assert(K % 2 == 1, "odd K keeps the strided shared loads conflict-free");
   extern __shared__ __align__(128) uint8_t smem[];
@@ -490,37 +485,18 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
   // channels between drains every byte-lane sum is <= 65535, so
   // raw - (odd << 8) = E0 + 2^16 E2 exactly: the even-byte sums.
   constexpr int W = K * G;  // output words per lane and DM
+  constexpr int NA = A16 ? 2 : 4;
   uint32_t pk[2][W][2];
-  uint32_t acc[2][W][2];  // one drained chunk: {even, odd} 16-bit lane pairs
+  // drained sums: samples 0..3 in 32 bits, or (A16) {even, odd} lane pairs
+  uint32_t acc[2][W][NA];
 #pragma unroll
   for (int d = 0; d < 2; d++)
 #pragma unroll
-    for (int w = 0; w < W; w++) pk[d][w][0] = pk[d][w][1] = acc[d][w][0] = acc[d][w][1] = 0;
-  // first word of this lane in group 0; group g adds 32*K*g words
-  const int lw = K * lane;
-  float* __restrict__ out = a.out + (size_t)blockIdx.z * a.out_unit;
-  // samples 4w'..4w'+3 of the lane's word w of DM slot d, plus the row's
-  // earlier partial sums when `add`
-  auto emit = [&](int d, int w, uint32_t s0, uint32_t s1, uint32_t s2, uint32_t s3, bool add) {
-    const int dd = d_lo + 2 * warp + d;
-    if (dd >= a.dm_count) return;
-    float* o = out + (size_t)dd * a.out_pitch;
-    const size_t t = t0 + 4 * (32 * K * (w / K) + lw + (w % K));
-    float4 v = make_float4((float)s0, (float)s1, (float)s2, (float)s3);
-    if (t + 3 < a.nout) {
-      if (add) {
-        const float4 p = *reinterpret_cast<const float4*>(o + t);
-        v.x += p.x; v.y += p.y; v.z += p.z; v.w += p.w;
-      }
-      *reinterpret_cast<float4*>(o + t) = v;
-    } else {
-      if (t < a.nout) o[t] = add ? v.x + o[t] : v.x;
-      if (t + 1 < a.nout) o[t + 1] = add ? v.y + o[t + 1] : v.y;
-      if (t + 2 < a.nout) o[t + 2] = add ? v.z + o[t + 2] : v.z;
+    for (int w = 0; w < W; w++) {
+      pk[d][w][0] = pk[d][w][1] = 0;
+#pragma unroll
+      for (int q = 0; q < NA; q++) acc[d][w][q] = 0;
     }
-  };
-  bool held = false;     // acc holds a chunk
-  bool flushed = false;  // the output row holds earlier chunks
   auto drain = [&]() {
 #pragma unroll
     for (int d = 0; d < 2; d++)
@@ -528,28 +504,22 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
       for (int w = 0; w < W; w++) {
         const uint32_t odd = pk[d][w][1];
         const uint32_t even = pk[d][w][0] - (odd << 8);
-        if constexpr (FL) {
-          if (held) {
-            emit(d, w, (even & 0xFFFFu) + (acc[d][w][0] & 0xFFFFu),
-                 (odd & 0xFFFFu) + (acc[d][w][1] & 0xFFFFu), (even >> 16) + (acc[d][w][0] >> 16),
-                 (odd >> 16) + (acc[d][w][1] >> 16), flushed);
-            acc[d][w][0] = acc[d][w][1] = 0;
-          } else {
-            acc[d][w][0] = even;
-            acc[d][w][1] = odd;
-          }
-        } else {
-          // at most one drain before the end (<= 511 channels)
+        if constexpr (A16) {
+          // only drain before the last: the accumulators are still zero
           acc[d][w][0] = even;
           acc[d][w][1] = odd;
+        } else {
+          acc[d][w][0] += even & 0xFFFFu;
+          acc[d][w][2] += even >> 16;
+          acc[d][w][1] += odd & 0xFFFFu;
+          acc[d][w][3] += odd >> 16;
         }
         pk[d][w][0] = pk[d][w][1] = 0;
       }
-    if constexpr (FL) {
-      if (held) flushed = true;
-      held = !held;
-    }
   };
+  // first word of this lane in group 0; group g adds 32*K*g words
+  const int lw = K * lane;
+
   int nsum = 0;
   bool failed = false;
   for (int st = 0; st < nstage; st++) {
@@ -620,17 +590,43 @@ __global__ void __launch_bounds__((NW + 1) * 32, dd_min_blocks(NW, K, G))
                                 :: "r"(smem_addr(&empty[buf])) : "memory");
   }
   if (failed) return;
-  // the last chunk (and a held one) into the output row
+  if constexpr (!A16) drain();
+  float* __restrict__ out = a.out + (size_t)blockIdx.z * a.out_unit;
 #pragma unroll
-  for (int d = 0; d < 2; d++)
+  for (int d = 0; d < 2; d++) {
+    int dd = d_lo + 2 * warp + d;
+    if (dd >= a.dm_count) continue;
+    float* o = out + (size_t)dd * a.out_pitch;
 #pragma unroll
-    for (int w = 0; w < W; w++) {
-      const uint32_t odd = pk[d][w][1];
-      const uint32_t even = pk[d][w][0] - (odd << 8);
-      emit(d, w, (even & 0xFFFFu) + (acc[d][w][0] & 0xFFFFu),
-           (odd & 0xFFFFu) + (acc[d][w][1] & 0xFFFFu), (even >> 16) + (acc[d][w][0] >> 16),
-           (odd >> 16) + (acc[d][w][1] >> 16), flushed);
-    }
+    for (int g = 0; g < G; g++)
+#pragma unroll
+      for (int j = 0; j < K; j++) {
+        const int w = K * g + j;
+        size_t t = t0 + 4 * (32 * K * g + lw + j);
+        uint32_t s0, s1, s2, s3;
+        if constexpr (A16) {
+          const uint32_t odd = pk[d][w][1];
+          const uint32_t even = pk[d][w][0] - (odd << 8);
+          s0 = (even & 0xFFFFu) + (acc[d][w][0] & 0xFFFFu);
+          s2 = (even >> 16) + (acc[d][w][0] >> 16);
+          s1 = (odd & 0xFFFFu) + (acc[d][w][1] & 0xFFFFu);
+          s3 = (odd >> 16) + (acc[d][w][1] >> 16);
+        } else {
+          s0 = acc[d][w][0];
+          s1 = acc[d][w][1];
+          s2 = acc[d][w][2];
+          s3 = acc[d][w][3];
+        }
+        float4 v = make_float4((float)s0, (float)s1, (float)s2, (float)s3);
+        if (t + 3 < a.nout) {
+          *reinterpret_cast<float4*>(o + t) = v;
+        } else {
+          if (t < a.nout) o[t] = v.x;
+          if (t + 1 < a.nout) o[t + 1] = v.y;
+          if (t + 2 < a.nout) o[t + 2] = v.z;
+        }
+      }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -798,9 +794,9 @@ size_t dd_smem(int dm_block, int ch, int rowb) {
 }
 template <int NW, int K, int G, int CH>
 cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
-  // the flushing instance only where the channels need more than two chunks
-  auto kern = a.nact <= 511 ? k_dedisp<NW, K, G, CH, DD_NST, false>
-                            : k_dedisp<NW, K, G, CH, DD_NST, true>;
+  // the compact drain holds two 257-channel chunks at most
+  auto kern = a.nact <= 511 ? k_dedisp<NW, K, G, CH, DD_NST, true>
+                            : k_dedisp<NW, K, G, CH, DD_NST, false>;
   const size_t smem = dd_smem(2 * NW, CH, a.rowb);
   cudaError_t e = raise_smem_limit(kern, smem);
   if (e != cudaSuccess) return e;

@@ -273,7 +273,7 @@ size_t ft_pitch(const dedisp_plan p, size_t nsamps) {
 // ---------------------------------------------------------------------------
 namespace {
 // bump when the dedispersion kernel changes, so stale choices are not reused
-constexpr uint64_t kDedispKernelGeneration = 5;
+constexpr uint64_t kDedispKernelGeneration = 6;
 
 struct TileCache {
   std::mutex mu;
