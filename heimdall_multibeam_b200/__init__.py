@@ -422,12 +422,14 @@ class Pipeline:
         return lib().hd_get_max_overlap(self._p, nbeams)
 
     def execute(self, filterbank: np.ndarray, nbeams: int = 1, first_idx: int = 0,
-                raise_on_error: bool = True) -> Tuple[int, int]:
-        """One gulp; filterbank is (nsamps, nchans) uint8 (STF for nbeams > 1).
-        Returns (hd_error, nsamps_processed); HD_TOO_MANY_EVENTS is soft."""
-        fb = _u8(filterbank)
+                raise_on_error: bool = True, nbits: int = 8) -> Tuple[int, int]:
+        """One gulp; filterbank is (nsamps, nchans) uint8 (STF for nbeams > 1),
+        or with nbits = 1, 2, 4 or 16 one row of packed samples per spectrum
+        (synth.pack_filterbank).  Returns (hd_error, nsamps_processed);
+        HD_TOO_MANY_EVENTS is soft."""
+        fb = _u8(filterbank) if nbits == 8 else np.ascontiguousarray(filterbank)
         proc = C.c_size_t(0)
-        err = lib().hd_execute(self._p, fb.ctypes.data, fb.shape[0], 8, first_idx, nbeams,
+        err = lib().hd_execute(self._p, fb.ctypes.data, fb.shape[0], nbits, first_idx, nbeams,
                                C.byref(proc))
         if raise_on_error and err not in (HD_NO_ERROR, HD_TOO_MANY_EVENTS):
             raise HdError(err, "hd_execute")
@@ -441,11 +443,11 @@ class Pipeline:
         return err, proc.value
 
     def execute_device(self, dev_ptr: int, nsamps: int, nbeams: int = 1,
-                       first_idx: int = 0) -> Tuple[int, int]:
+                       first_idx: int = 0, nbits: int = 8) -> Tuple[int, int]:
         """hd_execute_device: the filterbank already sits in device memory."""
         proc = C.c_size_t(0)
-        err = lib().hd_execute_device(self._p, C.c_void_p(dev_ptr), nsamps, 8, first_idx, nbeams,
-                                      C.byref(proc))
+        err = lib().hd_execute_device(self._p, C.c_void_p(dev_ptr), nsamps, nbits, first_idx,
+                                      nbeams, C.byref(proc))
         return err, proc.value
 
     def execute_beams(self, filterbanks: Sequence, nsamps: Optional[int] = None,
@@ -715,14 +717,16 @@ class DedispPlan:
     def max_delay(self) -> int:
         return lib().dedisp_get_max_delay(self._p)
 
-    def execute(self, filterbank: np.ndarray) -> np.ndarray:
-        fb = _u8(filterbank)
+    def execute(self, filterbank: np.ndarray, nbits: int = 8) -> np.ndarray:
+        """dedisp_execute: (nsamps, nchans) uint8, or packed rows of nbits = 1,
+        2, 4 or 16-bit samples (synth.pack_filterbank)."""
+        fb = _u8(filterbank) if nbits == 8 else np.ascontiguousarray(filterbank)
         nsamps = fb.shape[0]
         nout = nsamps - self.max_delay
         D = lib().dedisp_get_dm_count(self._p)
         out = np.zeros((D, nout), np.float32)
-        self._check(lib().dedisp_execute(self._p, nsamps, fb.ctypes.data, 8, out.ctypes.data, 32,
-                                         0), "dedisp_execute")
+        self._check(lib().dedisp_execute(self._p, nsamps, fb.ctypes.data, nbits, out.ctypes.data,
+                                         32, 0), "dedisp_execute")
         return out
 
 

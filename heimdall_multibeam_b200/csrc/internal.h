@@ -90,6 +90,30 @@ cudaError_t launch_dedisp(const DedispArgs& a, const DedispTile& t, cudaStream_t
 cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans, uint8_t* out,
                                    size_t pitch, cudaStream_t s, size_t units = 1,
                                    size_t out_unit = 0);
+// The same from packed samples of nbits = 1, 2, 4 or 16 bits (nchans * nbits a
+// multiple of 32; `in` 4-byte aligned): byte rows of the sample values, or for
+// 16 bits the low bytes at `out` and the high bytes at `out + hi_off`.
+cudaError_t launch_unpack_tf_ft(const uint8_t* in, size_t nsamps, int nchans, int nbits,
+                                uint8_t* out, size_t pitch, cudaStream_t s, size_t units,
+                                size_t out_unit, size_t hi_off);
+// lo[r * pitch + k] = RN(lo + 256 hi) for k < n, r < rows (the two byte planes'
+// exact integer sums of 16-bit input).
+cudaError_t launch_combine_planes(float* lo, const float* hi, size_t pitch, size_t n, size_t rows,
+                                  cudaStream_t s);
+// Channel-major byte rows of `units` filterbanks of nbits-bit samples (8: a
+// transpose; 1, 2, 4: unpacked; 16: low and high byte planes, the high plane
+// `units * out_unit` bytes after the low one).
+inline cudaError_t input_to_ft(const uint8_t* in, size_t nsamps, int nchans, int nbits,
+                               uint8_t* out, size_t pitch, cudaStream_t s, size_t units,
+                               size_t out_unit) {
+  if (nbits == 8) return launch_transpose_tf_ft(in, nsamps, nchans, out, pitch, s, units, out_unit);
+  return launch_unpack_tf_ft(in, nsamps, nchans, nbits, out, pitch, s, units, out_unit,
+                             units * out_unit);
+}
+// Input sample widths the search and the dedisp_* calls accept.
+inline bool nbits_supported(size_t nbits) {
+  return nbits == 1 || nbits == 2 || nbits == 4 || nbits == 8 || nbits == 16;
+}
 // Scrunched channel-major copy of `units` inputs: out[c][u] = the mean of
 // in[c][s u .. s u + s), rounded half up, for u < nsamps / s, and 0 from
 // there to out_pitch.

@@ -75,6 +75,71 @@ __global__ void __launch_bounds__(256) k_transpose_tf_ft(const uint8_t* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Packed TF -> byte FT rows for NB = 1, 2, 4 and 16 bits per sample.  A
+// spectrum is C * NB / 32 little-endian 32-bit words; channel c is the NB-bit
+// field at bit (c mod (32 / NB)) * NB of word c / (32 / NB) (the order of the
+// reference's writer and cleaning functor: Formats/giant_maker.C:385-392,
+// Pipeline/clean_filterbank_rfi.cu:86-90).  NB < 8 unpacks into one byte
+// plane; NB = 16 splits each sample into its low byte (plane `out`) and high
+// byte (plane `out + hi_off`), dedispersed separately and combined as
+// lo + 256 hi (exact integer sums).  128 x 128 tiles through shared memory.
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(256) k_unpack_tf_ft(const uint32_t* __restrict__ in,
+                                                      size_t nsamps, int nchans,
+                                                      uint8_t* __restrict__ out, size_t pitch,
+                                                      size_t out_unit, size_t hi_off) {
+  constexpr int CPW = 32 / NB;                 // channels per word
+  constexpr int WPR = 128 / CPW;               // words per tile row
+  constexpr uint32_t MASK = (NB == 32) ? 0xFFFFFFFFu : ((1u << NB) - 1u);
+  __shared__ uint16_t vals[128][130];          // [t][channel]
+  const size_t row_words = (size_t)nchans * NB / 32;
+  in += (size_t)blockIdx.z * nsamps * row_words;
+  out += (size_t)blockIdx.z * out_unit;
+  const size_t t0 = (size_t)blockIdx.x * 128;
+  const int c0 = blockIdx.y * 128;
+  const size_t w0 = (size_t)c0 / CPW;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int r = warp; r < 128; r += 8) {
+    const size_t t = t0 + r;
+    for (int w = lane; w < WPR; w += 32) {
+      uint32_t v = 0;
+      if (t < nsamps && w0 + w < row_words) v = in[t * row_words + w0 + w];
+#pragma unroll
+      for (int k = 0; k < CPW; k++) vals[r][w * CPW + k] = (uint16_t)((v >> (k * NB)) & MASK);
+    }
+  }
+  __syncthreads();
+  for (int cr = warp; cr < 128; cr += 8) {
+    const int c = c0 + cr;
+    if (c >= nchans) break;
+    const size_t t = t0 + 4 * lane;
+    if (t >= nsamps) continue;
+    uint32_t lo = 0, hi = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t v = vals[4 * lane + j][cr];
+      lo |= (v & 0xFFu) << (8 * j);
+      hi |= (v >> 8) << (8 * j);
+    }
+    reinterpret_cast<uint32_t*>(out + (size_t)c * pitch + t)[0] = lo;
+    if (NB == 16) reinterpret_cast<uint32_t*>(out + hi_off + (size_t)c * pitch + t)[0] = hi;
+  }
+}
+
+// rows x n floats (pitch apart): lo = RN(lo + 256 hi), both exact integer sums
+__global__ void k_combine_planes(float* __restrict__ lo, const float* __restrict__ hi,
+                                 size_t pitch, size_t n, size_t rows) {
+  const size_t total = rows * n;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / n, k = i - r * n;
+    const size_t at = r * pitch + k;
+    lo[at] = __uint2float_rn(__float2uint_rn(lo[at]) + 256u * __float2uint_rn(hi[at]));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Zero-DM series: s[t] = (float) sum_c in[t][c]  (dedisp at DM 0, all channels;
 // Pipeline/clean_filterbank_rfi.cu:361-397).  One warp per spectrum.
 // ---------------------------------------------------------------------------
@@ -637,6 +702,37 @@ cudaError_t launch_transpose_tf_ft(const uint8_t* in, size_t nsamps, int nchans,
   if (units < 1 || units > 65535) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128), (unsigned)units);
   k_transpose_tf_ft<<<grid, 256, 0, s>>>(in, nsamps, nchans, out, pitch, out_unit); note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_tf_ft(const uint8_t* in, size_t nsamps, int nchans, int nbits,
+                                uint8_t* out, size_t pitch, cudaStream_t s, size_t units,
+                                size_t out_unit, size_t hi_off) {
+  if (units < 1 || units > 65535 || nchans < 1 || ((size_t)nchans * nbits) % 32 ||
+      (reinterpret_cast<uintptr_t>(in) & 3) || pitch % 4)
+    return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((nsamps + 127) / 128), (unsigned)((nchans + 127) / 128), (unsigned)units);
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(in);
+  switch (nbits) {
+    case 1: k_unpack_tf_ft<1><<<grid, 256, 0, s>>>(w, nsamps, nchans, out, pitch, out_unit, 0); break;
+    case 2: k_unpack_tf_ft<2><<<grid, 256, 0, s>>>(w, nsamps, nchans, out, pitch, out_unit, 0); break;
+    case 4: k_unpack_tf_ft<4><<<grid, 256, 0, s>>>(w, nsamps, nchans, out, pitch, out_unit, 0); break;
+    case 16:
+      k_unpack_tf_ft<16><<<grid, 256, 0, s>>>(w, nsamps, nchans, out, pitch, out_unit, hi_off);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine_planes(float* lo, const float* hi, size_t pitch, size_t n, size_t rows,
+                                  cudaStream_t s) {
+  if (rows == 0 || n == 0) return cudaSuccess;
+  const size_t total = rows * n;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+  k_combine_planes<<<blocks, 256, 0, s>>>(lo, hi, pitch, n, rows);
+  note_launch();
   return cudaGetLastError();
 }
 

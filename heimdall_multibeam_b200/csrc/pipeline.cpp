@@ -88,7 +88,7 @@ struct hd_pipeline_t {
 
   DevBuf fb_tf, fb_ft, fb_tf_clean;
   DevBuf dm0, dm0_scan, base, rms, mask, fmask, rms0, nb_scratch;
-  DevBuf dd, scan;
+  DevBuf dd, dd_hi, scan;
   DevBuf ws_a, ws_b;
   DevBuf winfo, norm, gmax, tile_list;
   DevBuf tile_cnt, tile_off, sw_cnt, sw_off, hit_ind, hit_val, hit_sw;
@@ -371,10 +371,19 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   if (!fbs || !nsamps_processed || U == 0) return HD_INVALID_POINTER;
   for (size_t u = 0; u < U; u++)
     if (!fbs[u]) return HD_INVALID_POINTER;
-  if (nbits != 8) return HD_INVALID_NBITS;
+  // 1, 2, 4, 8 or 16-bit samples (dedisp's widths; packed little-endian,
+  // channel-fastest).  Cleaning and the resident prefetched gulp work on
+  // bytes; adaptive dt averages byte values, so 16-bit input searches at
+  // native resolution.
+  if (!hdb::nbits_supported(nbits)) return HD_INVALID_NBITS;
+  if (nbits != 8 && (pl->cleaning || resident)) return HD_INVALID_NBITS;
+  if (nbits == 16 && pl->plan->adaptive) return HD_INVALID_NBITS;
   const hd_params& P = pl->params;
   const size_t C = P.nchans;
-  if (C % 4 != 0 || nbeams == 0) return HD_INVALID_STRIDE;
+  if (C % 4 != 0 || nbeams == 0 || (C * nbits) % 32 != 0) return HD_INVALID_STRIDE;
+  if (nbits != 8)
+    for (size_t u = 0; u < U; u++)
+      if (on_device && (reinterpret_cast<uintptr_t>(fbs[u]) & 3)) return HD_INVALID_POINTER;
   if (P.min_tscrunch_width < 2) return HD_INVALID_STRIDE;
   // sample, hit and giant indices are kept in 31/32 bits on the device
   if (nsamps >= 0x7FFFFFFFull) return HD_INVALID_STRIDE;
@@ -418,17 +427,18 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   cudaEventRecord(pl->ev[0], s);
   HD_TRY(cudaMemsetAsync(pl->plan->d_err, 0, sizeof(unsigned), s));
   // ---- H2D, clean or channel-major copy, dedispersion ------------------------
-  const size_t fb_bytes = nsamps * C;
+  const size_t fb_bytes = nsamps * C * nbits / 8;
   const size_t pitch = hdb::ft_pitch(pl->plan, nsamps);
   const size_t ft_unit = pitch * C;
   const size_t dd_pitch = round_up(nc + 1, 4);
   const size_t NS = U * D;  // series of the batch, unit-major
   HD_TRY(pl->fb_tf.ensure(U * fb_bytes));
-  HD_TRY(pl->fb_ft.ensure(U * ft_unit));
+  // 16-bit input: the low-byte planes, then the high-byte planes
+  HD_TRY(pl->fb_ft.ensure(U * ft_unit * (nbits == 16 ? 2 : 1)));
   HD_TRY(pl->dd.ensure(NS * dd_pitch * sizeof(float)));
   float* dd = pl->dd.as<float>();
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if (!on_device && !pl->cleaning && U > 1 && pl->plan->groups.empty()) {
+  if (!on_device && !pl->cleaning && U > 1 && pl->plan->groups.empty() && nbits == 8) {
     // pipelined: copy chunk k on the copy stream while chunk k - 1 is
     // transposed and dedispersed on the compute stream (the unit-major series
     // layout; adaptive dt lays series out by scrunch factor and dedisperses
@@ -468,13 +478,23 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
                                 pl->fb_ft.as<uint8_t>(), pitch, nullptr);
       if (he != HD_NO_ERROR) return he;
     } else {
-      HD_TRY(hdb::launch_transpose_tf_ft(pl->fb_tf.as<uint8_t>(), nsamps, (int)C,
-                                         pl->fb_ft.as<uint8_t>(), pitch, s, U, ft_unit));
+      HD_TRY(hdb::input_to_ft(pl->fb_tf.as<uint8_t>(), nsamps, (int)C, (int)nbits,
+                              pl->fb_ft.as<uint8_t>(), pitch, s, U, ft_unit));
     }
     cudaEventRecord(pl->ev[2], s);
+    if (nbits == 16) {
+      // the high-byte plane's sums, then the low plane's, then lo + 256 hi
+      HD_TRY(pl->dd_hi.ensure(NS * dd_pitch * sizeof(float)));
+      de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>() + U * ft_unit, pitch,
+                                   nsamps, pl->dd_hi.as<float>(), dd_pitch, s, U, ft_unit,
+                                   D * dd_pitch);
+      if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+    }
     de = hdb::plan_dedisperse_ft(pl->plan, pl->fb_ft.as<uint8_t>(), pitch, nsamps, dd, dd_pitch,
                                  s, U, ft_unit, D * dd_pitch);
     if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+    if (nbits == 16)
+      HD_TRY(hdb::launch_combine_planes(dd, pl->dd_hi.as<float>(), dd_pitch, nc, NS, s));
   }
   // the element after each series is read (never used) by the baseline stretch
   if (pl->plan->groups.empty()) {

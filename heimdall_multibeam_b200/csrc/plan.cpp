@@ -546,6 +546,7 @@ dedisp_plan_struct::~dedisp_plan_struct() {
   hdb::free_dev(d_in_tf);
   hdb::free_dev(d_in_ft);
   hdb::free_dev(d_out);
+  hdb::free_dev(d_out_hi);
   hdb::free_dev(d_scr);
   hdb::free_groups(this);
   if (stream) cudaStreamDestroy(stream);
@@ -687,10 +688,17 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
   if (!p) return DEDISP_INVALID_PLAN;
   if (!in || !out) return DEDISP_INVALID_POINTER;
   if (p->dm_list.empty()) return DEDISP_NO_DM_LIST_SET;
-  if (in_nbits != 8) return DEDISP_UNSUPPORTED_IN_NBITS;
+  // 1, 2, 4, 8 or 16-bit samples (packed little-endian, channel-fastest);
+  // adaptive dt averages byte values, so 16-bit input searches at native
+  // resolution only
+  if (!hdb::nbits_supported(in_nbits) || (in_nbits == 16 && p->adaptive))
+    return DEDISP_UNSUPPORTED_IN_NBITS;
   if (out_nbits != 32) return DEDISP_UNSUPPORTED_OUT_NBITS;
-  if (in_stride != p->nchans || (p->nchans % 4) != 0) return DEDISP_INVALID_STRIDE;
+  if ((p->nchans * in_nbits) % 32 != 0 || in_stride != p->nchans * in_nbits / 8 ||
+      (p->nchans % 4) != 0)
+    return DEDISP_INVALID_STRIDE;
   if (out_stride % 4) return DEDISP_INVALID_STRIDE;
+  if (in_nbits != 8 && (reinterpret_cast<uintptr_t>(in) & 3)) return DEDISP_INVALID_POINTER;
   dedisp_error de = hdb::plan_prepare(p);
   if (de != DEDISP_NO_ERROR) return de;
   if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;
@@ -704,7 +712,7 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
   const bool dev_ptrs = (flags & DEDISP_DEVICE_POINTERS) != 0;
   const uint8_t* d_tf = in;
   if (!dev_ptrs) {
-    size_t need = nsamps * p->nchans;
+    size_t need = nsamps * in_stride;
     if (p->d_in_tf_cap < need) {
       hdb::free_dev(p->d_in_tf);
       p->d_in_tf = nullptr;
@@ -715,7 +723,8 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
       return DEDISP_MEM_COPY_FAILED;
     d_tf = p->d_in_tf;
   }
-  size_t need_ft = pitch * p->nchans;
+  const size_t plane = pitch * p->nchans;
+  size_t need_ft = plane * (in_nbits == 16 ? 2 : 1);
   if (p->d_in_ft_cap < need_ft) {
     hdb::free_dev(p->d_in_ft);
     p->d_in_ft = nullptr;
@@ -724,8 +733,8 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
     p->d_in_ft_cap = need_ft;
   }
   if (cudaMemsetAsync(p->d_err, 0, sizeof(unsigned), s) != cudaSuccess ||
-      hdb::launch_transpose_tf_ft(d_tf, nsamps, (int)p->nchans, p->d_in_ft, pitch, s) !=
-          cudaSuccess)
+      hdb::input_to_ft(d_tf, nsamps, (int)p->nchans, (int)in_nbits, p->d_in_ft, pitch, s, 1,
+                       plane) != cudaSuccess)
     return DEDISP_INTERNAL_GPU_ERROR;
   float* d_o = reinterpret_cast<float*>(out);
   size_t opitch = out_stride / 4;
@@ -743,8 +752,24 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
   } else if (opitch % 4) {
     return DEDISP_INVALID_STRIDE;
   }
+  if (in_nbits == 16) {
+    // high-byte plane, low-byte plane, then lo + 256 hi
+    const size_t need = opitch * D;
+    if (p->d_out_hi_cap < need) {
+      hdb::free_dev(p->d_out_hi);
+      p->d_out_hi = nullptr;
+      if (hdb::dev_malloc(&p->d_out_hi, need * sizeof(float)) != cudaSuccess)
+        return DEDISP_MEM_ALLOC_FAILED;
+      p->d_out_hi_cap = need;
+    }
+    de = hdb::plan_dedisperse_ft(p, p->d_in_ft + plane, pitch, nsamps, p->d_out_hi, opitch, s);
+    if (de != DEDISP_NO_ERROR) return de;
+  }
   de = hdb::plan_dedisperse_ft(p, p->d_in_ft, pitch, nsamps, d_o, opitch, s);
   if (de != DEDISP_NO_ERROR) return de;
+  if (in_nbits == 16 &&
+      hdb::launch_combine_planes(d_o, p->d_out_hi, opitch, nout, D, s) != cudaSuccess)
+    return DEDISP_INTERNAL_GPU_ERROR;
   if (!dev_ptrs) {
     if (cudaMemcpy2DAsync(out, out_stride, d_o, opitch * sizeof(float), nout * sizeof(float), D,
                           cudaMemcpyDeviceToHost, s) != cudaSuccess)

@@ -73,6 +73,8 @@ struct dedisp_plan_struct {
   size_t d_in_ft_cap = 0;
   float* d_out = nullptr;
   size_t d_out_cap = 0;
+  float* d_out_hi = nullptr;  // high-byte plane sums of 16-bit input
+  size_t d_out_hi_cap = 0;
   cudaStream_t stream = nullptr;
 
   ~dedisp_plan_struct();

@@ -475,3 +475,24 @@ def write_sigproc(path: str, data: Optional[np.ndarray] = None, order: Sequence[
             f.write(np.ascontiguousarray(data, dtype=np.uint8).tobytes())
     return size
 
+
+
+def pack_filterbank(values: np.ndarray, nbits: int) -> np.ndarray:
+    """Packs an (nsamps, nchans) array of sample values (each < 2^nbits) into
+    one row of nbits-bit samples per spectrum, the layout hd_execute and
+    dedisp_execute take for nbits = 1, 2, 4 and 16: channel c is the
+    nbits-bit field at bit (c mod (32 / nbits)) * nbits of the little-endian
+    32-bit word c / (32 / nbits) (the order of the reference's writer,
+    Formats/giant_maker.C:385-392).  Returns uint8 rows of nchans * nbits / 8
+    bytes (nchans * nbits a multiple of 32)."""
+    v = np.asarray(values)
+    nsamps, nchans = v.shape
+    if nbits not in (1, 2, 4, 8, 16) or (nchans * nbits) % 32:
+        raise ValueError("nbits in {1, 2, 4, 8, 16} and nchans * nbits a multiple of 32")
+    if v.size and int(v.max()) >= (1 << nbits):
+        raise ValueError("sample values must be below 2^nbits")
+    cpw = 32 // nbits
+    fields = v.astype(np.uint64).reshape(nsamps, nchans // cpw, cpw)
+    shifts = (np.arange(cpw, dtype=np.uint64) * np.uint64(nbits))[None, None, :]
+    words = (fields << shifts).sum(axis=2).astype(np.uint32)
+    return np.ascontiguousarray(words.astype("<u4")).view(np.uint8).reshape(nsamps, -1)

@@ -126,9 +126,14 @@ dedisp_float        dedisp_get_dt(const dedisp_plan plan);
 dedisp_float        dedisp_get_f0(const dedisp_plan plan);
 dedisp_float        dedisp_get_df(const dedisp_plan plan);
 
-/* Brute-force dedispersion of nsamps spectra of `in` (in_stride bytes apart,
- * in_nbits per channel) into dm_count series of nsamps - max_delay samples
- * (out_stride bytes apart, out_nbits per sample; 32 = float).
+/* Brute-force dedispersion of nsamps spectra of `in` (in_stride = nchans *
+ * in_nbits / 8 bytes apart, in_nbits = 1, 2, 4, 8 or 16 per channel, packed as
+ * hd_execute documents) into dm_count series of nsamps - max_delay samples
+ * (out_stride bytes apart, out_nbits per sample; 32 = float, the only output
+ * width).  Sums are exact integers written as float (rounded once); 16-bit
+ * samples are summed as low and high bytes, lo + 256 hi, and take no adaptive
+ * dt (DEDISP_UNSUPPORTED_IN_NBITS).  Packed input from device memory must be
+ * 4-byte aligned.
  * pipeline.cu:459-462, clean_filterbank_rfi.cu:389-393 */
 dedisp_error dedisp_execute_adv(const dedisp_plan plan, dedisp_size nsamps,
                                 const dedisp_byte* in, dedisp_size in_nbits,

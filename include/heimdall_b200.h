@@ -157,9 +157,17 @@ hd_error hd_create_pipeline(hd_pipeline* pipeline, struct hd_params params);
 hd_error hd_preallocate(hd_pipeline pipeline, hd_size nsamps, hd_size nbeams);
 hd_size  hd_get_max_overlap(hd_pipeline pipeline, hd_size nbeams);
 /* One gulp: nsamps spectra (nbeams beams of nsamps/nbeams spectra each, time
- * concatenated) of nchans*nbits/8 bytes; nbits 8 and nchans a multiple of 4
- * (whole 32-bit words per spectrum, as Pipeline/clean_filterbank_rfi.cu:202-212
- * assumes), else HD_INVALID_NBITS / HD_INVALID_STRIDE.  Candidates go to
+ * concatenated) of nchans*nbits/8 bytes.  nbits is 1, 2, 4, 8 or 16 (the
+ * widths dedisp reads; samples packed little-endian, channel c the nbits-bit
+ * field at bit (c mod (32/nbits))*nbits of 32-bit word c/(32/nbits), as the
+ * reference's writer packs them, Formats/giant_maker.C:385-392); nchans a
+ * multiple of 4 and nchans*nbits a multiple of 32 (whole 32-bit words per
+ * spectrum, as Pipeline/clean_filterbank_rfi.cu:202-212 assumes), else
+ * HD_INVALID_NBITS / HD_INVALID_STRIDE.  Widths other than 8 are refused
+ * (HD_INVALID_NBITS) with cleaning on (hd_set_cleaning), with a prefetched
+ * gulp, and, for 16 bits, with adaptive dt; every width is searched through
+ * the same integer sums, so a gulp of values below 256 gives the same
+ * candidates at any width.  Candidates go to
  * <output_dir>/<UTC>_<beam+1>.cand as in Pipeline/pipeline.cu:1001-1044
  * (output_dir == NULL: no file).  Returns HD_TOO_MANY_EVENTS (soft) when the
  * giant rate exceeds max_giant_rate. */

@@ -359,18 +359,24 @@ def ref_set_dedisp_threads(n: int) -> None:
 
 
 def ref_execute(fb: np.ndarray, nbeams: int = 1, first_idx: int = 0, nthreads: int = 1,
-                **kw):
+                nbits: int = 8, nchans: Optional[int] = None, **kw):
     """Runs the reference's own pipeline (the CLEANING build when kw clean=1,
     the shipped build otherwise); returns (error, nsamps_processed, .cand
     lines, seconds).  nthreads=1 fixes the order of the reference's racy
-    clustering sweep (Pipeline/label_candidate_clusters.cu:179-195)."""
-    fb = np.ascontiguousarray(fb, dtype=np.uint8)
-    nsamps, nchans = fb.shape
+    clustering sweep (Pipeline/label_candidate_clusters.cu:179-195).  With
+    nbits != 8, fb holds one row of packed samples per spectrum and nchans
+    is given."""
+    if nbits == 8:
+        fb = np.ascontiguousarray(fb, dtype=np.uint8)
+        nsamps, nchans = fb.shape
+    else:
+        fb = np.ascontiguousarray(fb)
+        nsamps = fb.shape[0]
     p = make_params(nchans=nchans, **kw)
     with tempfile.TemporaryDirectory() as d:
         proc = C.c_size_t(0)
         secs = C.c_double(0)
-        err = ref_lib(bool(kw.get("clean", 0))).ref_execute(C.byref(p), fb.ctypes.data, nsamps, 8, first_idx, nbeams,
+        err = ref_lib(bool(kw.get("clean", 0))).ref_execute(C.byref(p), fb.ctypes.data, nsamps, nbits, first_idx, nbeams,
                                     d.encode(), C.byref(proc), C.byref(secs), nthreads)
         lines: List[str] = []
         for f in sorted(glob.glob(os.path.join(d, "*.cand"))):

@@ -12,6 +12,7 @@
 #include "dedisp.h"
 #include "oracle.h"
 
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -140,19 +141,65 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
   if (!p) return DEDISP_INVALID_PLAN;
   if (!in || !out) return DEDISP_INVALID_POINTER;
   if (!p->dm_count) return DEDISP_NO_DM_LIST_SET;
-  if (in_nbits != 8) return DEDISP_UNSUPPORTED_IN_NBITS;
+  if (in_nbits != 1 && in_nbits != 2 && in_nbits != 4 && in_nbits != 8 && in_nbits != 16)
+    return DEDISP_UNSUPPORTED_IN_NBITS;
+  if (in_nbits == 16 && p->adaptive) return DEDISP_UNSUPPORTED_IN_NBITS;
   if (out_nbits != 32) return DEDISP_UNSUPPORTED_OUT_NBITS;
   if (out_stride % 4) return DEDISP_INVALID_STRIDE;
+  if ((p->nchans * in_nbits) % 32) return DEDISP_INVALID_STRIDE;
   size_t md = dedisp_get_max_delay(p);
   if (nsamps < md) return DEDISP_TOO_FEW_NSAMPS;
   /* every host core unless dedisp_cpu_set_threads() says otherwise, whatever
    * thread count the caller set for the stage code: the integer sums do not
    * depend on it */
-  or_dedisperse_scrunched(in, nsamps, in_stride, p->nchans, p->killmask, p->dm_list,
-                          p->dm_count, p->table,
-                          p->adaptive ? (const size_t*)p->dt_factors : NULL, (float*)out,
-                          out_stride / 4,
-                          g_dedisp_threads > 0 ? g_dedisp_threads : omp_get_num_procs());
+  const int threads = g_dedisp_threads > 0 ? g_dedisp_threads : omp_get_num_procs();
+  const size_t* factors = p->adaptive ? (const size_t*)p->dt_factors : NULL;
+  if (in_nbits == 8) {
+    or_dedisperse_scrunched(in, nsamps, in_stride, p->nchans, p->killmask, p->dm_list,
+                            p->dm_count, p->table, factors, (float*)out, out_stride / 4, threads);
+    return DEDISP_NO_ERROR;
+  }
+  /* packed samples: channel c of spectrum t is the in_nbits-bit field at bit
+   * (c mod (32 / in_nbits)) * in_nbits of the little-endian 32-bit word
+   * c / (32 / in_nbits) (the reference's writer, Formats/giant_maker.C:385-392).
+   * Values below 256 are summed as bytes; 16-bit values as their low and high
+   * bytes, sum = sum(lo) + 256 sum(hi), exact in integers. */
+  const size_t C = p->nchans, cpw = 32 / in_nbits, mask = (in_nbits == 16) ? 0xFFFFu
+                                                        : ((1u << in_nbits) - 1u);
+  const int planes = in_nbits == 16 ? 2 : 1;
+  unsigned char* u = (unsigned char*)malloc((size_t)planes * nsamps * C);
+  if (!u) return DEDISP_MEM_ALLOC_FAILED;
+  for (size_t t = 0; t < nsamps; t++) {
+    const unsigned char* row = in + t * in_stride;
+    for (size_t c = 0; c < C; c++) {
+      const size_t w = c / cpw, k = c % cpw;
+      const uint32_t word = (uint32_t)row[4 * w] | ((uint32_t)row[4 * w + 1] << 8) |
+                            ((uint32_t)row[4 * w + 2] << 16) | ((uint32_t)row[4 * w + 3] << 24);
+      const uint32_t v = (word >> (k * in_nbits)) & mask;
+      u[t * C + c] = (unsigned char)(v & 0xFFu);
+      if (planes == 2) u[nsamps * C + t * C + c] = (unsigned char)(v >> 8);
+    }
+  }
+  float* o = (float*)out;
+  const size_t opitch = out_stride / 4, nout = nsamps - md;
+  or_dedisperse_scrunched(u, nsamps, C, C, p->killmask, p->dm_list, p->dm_count, p->table,
+                          factors, o, opitch, threads);
+  if (planes == 2) {
+    float* hi = (float*)malloc(opitch * p->dm_count * sizeof(float));
+    if (!hi) {
+      free(u);
+      return DEDISP_MEM_ALLOC_FAILED;
+    }
+    or_dedisperse_scrunched(u + nsamps * C, nsamps, C, C, p->killmask, p->dm_list,
+                            p->dm_count, p->table, NULL, hi, opitch, threads);
+    for (size_t d = 0; d < p->dm_count; d++)
+      for (size_t t = 0; t < nout; t++) {
+        const uint32_t v = (uint32_t)o[d * opitch + t] + 256u * (uint32_t)hi[d * opitch + t];
+        o[d * opitch + t] = (float)v;
+      }
+    free(hi);
+  }
+  free(u);
   return DEDISP_NO_ERROR;
 }
 
