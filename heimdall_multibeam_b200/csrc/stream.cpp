@@ -212,7 +212,10 @@ hd_error search_files(hd_pipeline pl, const char* const* paths, size_t nfiles,
     if (e != HD_NO_ERROR) return e;
   }
   const hd_sigproc_header& h = hs[0];
-  if (h.nbits != 8) return HD_INVALID_NBITS;
+  // the sample widths hd_execute takes (packed files: see hd_execute)
+  if (h.nbits != 1 && h.nbits != 2 && h.nbits != 4 && h.nbits != 8 && h.nbits != 16)
+    return HD_INVALID_NBITS;
+  if (((size_t)h.nchans * (size_t)h.nbits) % 32 != 0) return HD_INVALID_STRIDE;
   for (size_t u = 1; u < nfiles; u++) {
     const hd_sigproc_header& g = hs[u];
     if (g.nbits != h.nbits || g.nchans != h.nchans || g.tsamp != h.tsamp || g.fch1 != h.fch1 ||
@@ -220,7 +223,8 @@ hd_error search_files(hd_pipeline pl, const char* const* paths, size_t nfiles,
       return HD_INVALID_STRIDE;
   }
   const size_t nbeams = h.nbeams > 0 ? (size_t)h.nbeams : 1;
-  const size_t stride = (size_t)h.nchans;  // bytes per spectrum (8-bit)
+  const size_t nbits = (size_t)h.nbits;
+  const size_t stride = (size_t)h.nchans * nbits / 8;  // bytes per spectrum
   if (nsamps_gulp == 0 || nsamps_gulp % nbeams != 0) return HD_INVALID_STRIDE;
   if (cudaSetDevice(hdb::pipeline_device(pl)) != cudaSuccess) return HD_INVALID_DEVICE_INDEX;
   std::vector<FILE*> fs(nfiles, nullptr);
@@ -377,10 +381,10 @@ hd_error search_files(hd_pipeline pl, const char* const* paths, size_t nfiles,
     hd_size processed = 0;
     hd_error e;
     if (nfiles == 1) {
-      e = hd_execute_device(pl, d_buf[cur], to_process, 8, total, nbeams, &processed);
+      e = hd_execute_device(pl, d_buf[cur], to_process, nbits, total, nbeams, &processed);
     } else {
       for (size_t u = 0; u < nfiles; u++) units[u] = d_buf[cur] + u * cap;
-      e = hd_execute_beams(pl, units.data(), nfiles, to_process, 8, total, nbeams, nullptr, 1,
+      e = hd_execute_beams(pl, units.data(), nfiles, to_process, nbits, total, nbeams, nullptr, 1,
                            statuses.data(), &processed);
     }
     reader.join();

@@ -488,7 +488,9 @@ hd_error hd_params_from_sigproc(const hd_sigproc_header* header, struct hd_param
  * and the first sample index of the gulp. */
 typedef void (*hd_gulp_callback)(void* user, const hd_candidate* candidates, hd_size count,
                                  hd_size first_idx);
-/* Searches an 8-bit sigproc file gulp by gulp as heimdall.C's loop does: the
+/* Searches a sigproc file of 1, 2, 4, 8 or 16-bit samples (packed as
+ * hd_execute documents; the same width limits) gulp by gulp as heimdall.C's
+ * loop does: the
  * first gulp is nsamps_gulp spectra, each later one the previous gulp's
  * unprocessed overlap (boxcar_max + max_delay per beam) followed by
  * nsamps_gulp new spectra; a block shorter than nsamps_gulp ends the search

@@ -151,3 +151,27 @@ def test_sigproc_files_lockstep(hdb, tmp_path):
     with H.Pipeline(params(0), cleaning=True) as pl:
         err, _, gulps = pl.search_sigproc_files([paths[0], other], GULP)
     assert err == H.HD_INVALID_STRIDE and gulps == []
+
+
+@pytest.mark.parametrize("nbits", [2, 4])
+def test_sigproc_gulp_loop_packed_file(hdb, tmp_path, nbits):
+    """A packed sigproc file (the reference's writer order) searched by the
+    gulp loop gives, gulp by gulp, the candidates of the 8-bit file of the
+    same sample values."""
+    _, data = _file(tmp_path)
+    v = (data >> (8 - nbits)).astype(np.uint8)
+    hdr = dict(nchans=NCH, tsamp=DT, fch1=F0, foff=DF, tstart=60000.5, nifs=1,
+               source_name="stream_test")
+    packed_path, bytes_path = str(tmp_path / "packed.fil"), str(tmp_path / "bytes.fil")
+    synth.write_sigproc(packed_path, synth.pack_filterbank(v, nbits), nbits=nbits, **hdr)
+    synth.write_sigproc(bytes_path, v, nbits=8, **hdr)
+    kw = dict(dm_min=0.0, dm_max=300.0, boxcar_max=256)
+    out = []
+    for path in (packed_path, bytes_path):
+        params = H.params_from_sigproc(path, H.default_params(output_dir=None, **kw))
+        with H.Pipeline(params, cleaning=False) as pl:
+            err, total, gulps = pl.search_sigproc_file(path, GULP)
+        assert err == H.HD_NO_ERROR
+        out.append((total, [(first, H.cand_lines(c)) for first, c in gulps]))
+    assert out[0] == out[1]
+    assert len(out[0][1]) == 3 and sum(len(c) for _, c in out[0][1]) >= 3
