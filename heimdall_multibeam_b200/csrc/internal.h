@@ -290,6 +290,9 @@ cudaError_t giant_place(const GiantBuffers& src, unsigned n, int dm_key_gap,
 struct ClusterArgs {
   int ngiants;
   unsigned long long time_tol, filter_tol, dm_tol, nsamps_beam;
+  // giants per unit at most (a giant's DM window never leaves its unit):
+  // sizes the sweep grid's chunks of earlier giants (0: ngiants)
+  int max_unit_giants;
 };
 cudaError_t cluster_init(GiantBuffers& gb, int ngiants, cudaStream_t s);
 cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* changed,

@@ -905,6 +905,7 @@ cudaError_t launch_dd(const DedispArgs& a, cudaStream_t s) {
 template <int NW, int K, int G>
 cudaError_t launch_rows(const DedispArgs& a, int rows, cudaStream_t s) {
   switch (rows) {
+    case 16: return launch_dd<NW, K, G, 16>(a, s);
     case 8: return launch_dd<NW, K, G, 8>(a, s);
     case 4: return launch_dd<NW, K, G, 4>(a, s);
     case 2: return launch_dd<NW, K, G, 2>(a, s);
@@ -914,13 +915,14 @@ cudaError_t launch_rows(const DedispArgs& a, int rows, cudaStream_t s) {
 }
 }  // namespace
 
-// Channel rows per stage: the most that keep three CTAs on an SM (72 KB
-// each), else two (110 KB), else one (200 KB).  Rows are long when few
+// Channel rows per stage (16, 8, 4, 2 or 1): the most that keep three CTAs on
+// an SM (72 KB each), else two (110 KB), else one (200 KB).  More rows per
+// stage spread the per-stage waits and hand-offs over more channels.  Rows are long when few
 // channels cover a wide DM range (a DM block's delay span is long).  The
 // sums are exact integers, so the choice does not change the result.
 int dedisp_rows_per_stage(int dm_block, int rowb) {
   for (size_t cap : {(size_t)72 * 1024, (size_t)110 * 1024, (size_t)200 * 1024})
-    for (int ch = 8; ch >= 1; ch /= 2)
+    for (int ch = 16; ch >= 1; ch /= 2)
       if (dd_smem(dm_block, ch, rowb) <= cap) return ch;
   return 0;
 }

@@ -780,18 +780,27 @@ __device__ __forceinline__ float max5(float a, float b, float c, float d, float 
   return fmaxf(fmaxf(fmaxf(a, b), fmaxf(c, d)), e);
 }
 
-template <bool MM>
+__host__ __device__ constexpr int pow5c(int k) { return k <= 0 ? 1 : 5 * pow5c(k - 1); }
+
+// The median levels of one group for every width slot, M levels in the block
+// (compile-time: every index is divided by a constant).  Level 1 and level 2
+// run block-wide, one barrier each; levels 3..M of a width slot run inside
+// one warp (warp w takes slots w, w + 8, ...), with only warp
+// synchronisation, in the slot's own rows of la and lb.
+template <bool MM, int M>
 __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, int w0, int nwb,
-                           int m, float* la, float* lb, float* __restrict__ out,
-                           size_t out_pitch, size_t ser, size_t g, float* srun, bool rec) {
-  const int n1 = (int)pow5(m - 1);
-  const int n1p = (n1 + 3) & ~3;
+                           float* la, float* lb, float* __restrict__ out, size_t out_pitch,
+                           size_t ser, size_t g, float* srun, bool rec) {
+  constexpr int n1 = pow5c(M - 1);
+  constexpr int n1p = (n1 + 3) & ~3;
+  constexpr int lbp = n1 / 5 + 1;
   // srun[wl][q]: largest |boxcar| of level-1 item q of width slot wl (runs of
   // 20 samples, then the < 4 remaining single medians)
-  const int rp = n1 / 4 + 4;
+  constexpr int nq = n1 / 4, rem = n1 - 4 * nq;
+  constexpr int rp = nq + 4;
 
   // ---- level 1 ----
-  const int nq = n1 / 4, rem = n1 - 4 * nq;
+  if constexpr (nq > 0)
   for (int item = threadIdx.x; item < nwb * nq; item += blockDim.x) {
     const int wl = item / nq, k0 = 4 * (item - wl * nq);
     const int wi = w0 + wl;
@@ -808,7 +817,7 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
       else if (wi == 1) brv_small<1, 1>(wv, v);
       else brv_small<2, 2>(wv, v);
     } else {
-      const int h = ctx.winfo[wi].ahead;  // = behind = width / 2
+      const int h = 1 << (wi - 1);  // ahead = behind = width / 2 (the launcher checks)
       const float4* pa = reinterpret_cast<const float4*>(tile + 5 * k0 + offset + h);
       const float4* pb = reinterpret_cast<const float4*>(tile + 5 * k0 + offset - h);
 #pragma unroll
@@ -832,51 +841,63 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
                 fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
                       max5(v[15], v[16], v[17], v[18], v[19])));
   }
-  for (int item = threadIdx.x; item < nwb * rem; item += blockDim.x) {
-    const int wl = item / rem, k = 4 * nq + (item - wl * rem);
-    const WidthInfo& w = ctx.winfo[w0 + wl];
-    const int a = offset + w.ahead, b = offset - w.behind;
-    float v[5];
+  if constexpr (rem > 0)
+    for (int item = threadIdx.x; item < nwb * rem; item += blockDim.x) {
+      const int wl = item / rem, k = 4 * nq + (item - wl * rem);
+      const WidthInfo& w = ctx.winfo[w0 + wl];
+      const int a = offset + w.ahead, b = offset - w.behind;
+      float v[5];
 #pragma unroll
-    for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
-    la[wl * n1p + k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
-    if (rec) srun[wl * rp + nq + (k - 4 * nq)] = max5(v[0], v[1], v[2], v[3], v[4]);
-  }
+      for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
+      la[wl * n1p + k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+      if (rec) srun[wl * rp + nq + (k - 4 * nq)] = max5(v[0], v[1], v[2], v[3], v[4]);
+    }
   __syncthreads();
-  if (rec) {
-    // one warp per width slot: the group's largest |boxcar|.  Values are
-    // non-negative or NaN, so their bit patterns order as unsigned (a NaN
-    // maximum only ever keeps a tile from being skipped); fmaxf above drops
-    // a NaN unless all its operands are NaN, and no sample is then left out
-    // of a maximum that decides a skip: a NaN boxcar never passes the test.
-    const int lane = threadIdx.x & 31;
-    for (int wl = threadIdx.x >> 5; wl < nwb; wl += blockDim.x >> 5) {
+
+  // ---- level 2, block-wide: la -> lb ----
+  if constexpr (M >= 2) {
+    constexpr int n2 = n1 / 5;
+    for (int item = threadIdx.x; item < nwb * n2; item += blockDim.x) {
+      const int wl = item / n2, k = item - wl * n2;
+      const float* c = la + wl * n1p + 5 * k;
+      lb[wl * lbp + k] = brv_med5<MM>(c[0], c[1], c[2], c[3], c[4]);
+    }
+    __syncthreads();
+  }
+
+  // ---- the group maxima and levels 3..M: one warp per width slot ----
+  const int lane = threadIdx.x & 31;
+  for (int wl = threadIdx.x >> 5; wl < nwb; wl += blockDim.x >> 5) {
+    if (rec) {
+      // values are non-negative or NaN, so their bit patterns order as
+      // unsigned (a NaN maximum only ever keeps a tile from being skipped);
+      // fmaxf above drops a NaN unless all its operands are NaN, and no sample
+      // is then left out of a maximum that decides a skip: a NaN boxcar never
+      // passes the test
       unsigned mk = 0;
       for (int q = lane; q < nq + rem; q += 32) mk = max(mk, __float_as_uint(srun[wl * rp + q]));
       mk = __reduce_max_sync(0xffffffffu, mk);
       if (lane == 0) ctx.gmax[(ser * nwb + wl) * ctx.ngroups + g] = __uint_as_float(mk);
     }
-  }
-
-  // ---- levels 2..m, all widths per barrier ----
-  float* cur = la;
-  float* nxt = lb;
-  int n = n1, pitch_cur = n1p;
-  for (int lev = 2; lev <= m; lev++) {
-    const int nn = n / 5;
-    for (int item = threadIdx.x; item < nwb * nn; item += blockDim.x) {
-      const int wl = item / nn, k = item - wl * nn;
-      const float* c = cur + wl * pitch_cur + 5 * k;
-      nxt[wl * nn + k] = brv_med5<MM>(c[0], c[1], c[2], c[3], c[4]);
+    float* rows[2] = {lb + wl * lbp, la + wl * n1p};  // level 2's output is in lb
+    int n = M >= 2 ? n1 / 5 : n1;
+    const float* cur = M >= 2 ? rows[0] : la + wl * n1p;
+#pragma unroll
+    for (int lev = 3; lev <= M; lev++) {
+      float* nxt = rows[(lev - 2) & 1];
+      const int nn = n / 5;
+      // inputs and outputs alternate between the slot's lb and la rows
+      for (int k = lane; k < nn; k += 32) {
+        const float* c = cur + 5 * k;
+        nxt[k] = brv_med5<MM>(c[0], c[1], c[2], c[3], c[4]);
+      }
+      __syncwarp();  // every lane reaches it: the level is complete
+      cur = nxt;
+      n = nn;
     }
-    __syncthreads();
-    float* t = cur; cur = nxt; nxt = t;
-    n = nn;
-    pitch_cur = nn;
+    // n == 1: one value per width
+    if (lane == 0) out[(ser * nwb + wl) * out_pitch + g] = cur[0];
   }
-  // n == 1: one value per width
-  for (int wl = threadIdx.x; wl < nwb; wl += blockDim.x)
-    out[(ser * nwb + wl) * out_pitch + g] = cur[wl * pitch_cur];
 }
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
@@ -898,15 +919,16 @@ __device__ __forceinline__ void cp_async_wait() {
 // Block (x, y): groups [x * gpb, (x + 1) * gpb) of series y.  The next
 // group's window is copied into the other half of a double buffer (cp.async)
 // while the current group's medians are computed.
+template <int M>
 __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ctx, int w0,
-                                                                     int nwb, int m, int win,
+                                                                     int nwb, int win,
                                                                      float* __restrict__ out,
                                                                      size_t out_pitch,
                                                                      int ngroups, int gpb) {
   extern __shared__ __align__(16) float dyn[];
   const int win4 = (win + 3) & ~3;
   float* tiles = dyn;                    // [2][win4]
-  const int n1 = (int)pow5(m - 1);       // level-1 medians per width
+  constexpr int n1 = pow5c(M - 1);       // level-1 medians per width
   const int n1p = (n1 + 3) & ~3;         // row pitch: 16-byte aligned rows
   float* la = dyn + 2 * win4;            // [nwb][n1p]
   float* lb = la + nwb * n1p;            // [nwb][n1 / 5 + 1]
@@ -917,7 +939,7 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
   const WidthInfo& w_first = ctx.winfo[w0];
   const float* sc = ctx.scan + ser * ctx.scan_pitch;
   const float delta = (float)(ctx.stride - w_first.bn);
-  const size_t gsz = pow5(m);
+  constexpr size_t gsz = pow5c(M);
   const int offset = ctx.offset;
   // the launcher guarantees contiguous groups (one beam) whose window fits
   auto first_of = [&](int g) {
@@ -950,9 +972,9 @@ __global__ void __launch_bounds__(BRV_THREADS) k_block_rms_pass1_vec(WidthCtx ct
     }
     __syncthreads();
     if (finite)
-      brv_levels<true>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, srun, rec);
+      brv_levels<true, M>(ctx, tile, offset, w0, nwb, la, lb, out, out_pitch, ser, g, srun, rec);
     else
-      brv_levels<false>(ctx, tile, offset, w0, nwb, m, la, lb, out, out_pitch, ser, g, srun, rec);
+      brv_levels<false, M>(ctx, tile, offset, w0, nwb, la, lb, out, out_pitch, ser, g, srun, rec);
   }
 }
 
@@ -1016,7 +1038,12 @@ cudaError_t block_rms(WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end
                          nwb * (n1 / 5 + 1) + nwb * (n1 / 4 + 4)) *
                         sizeof(float);
     if (smem <= 200 * 1024) {
-      if ((e = raise_smem_limit(k_block_rms_pass1_vec, smem)) != cudaSuccess) return e;
+      auto kern = m1 == 5 ? k_block_rms_pass1_vec<5>
+                  : m1 == 4 ? k_block_rms_pass1_vec<4>
+                  : m1 == 3 ? k_block_rms_pass1_vec<3>
+                  : m1 == 2 ? k_block_rms_pass1_vec<2>
+                            : k_block_rms_pass1_vec<1>;
+      if ((e = raise_smem_limit(kern, smem)) != cudaSuccess) return e;
       // the group maxima of the widths [0, nwb) for count_hits
       if (ctx.gmax && w_begin == 0 && nwb <= VH_MAXW && nseg * ng1 <= ctx.gmax_cap) {
         ctx.gsize = (unsigned)pow5(m1);
@@ -1026,9 +1053,8 @@ cudaError_t block_rms(WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end
       // about 8 consecutive groups per block, spread evenly
       const size_t nblk_x = (ng1 + 7) / 8;
       const size_t gpb = (ng1 + nblk_x - 1) / nblk_x;
-      k_block_rms_pass1_vec<<<dim3((unsigned)((ng1 + gpb - 1) / gpb), ctx.nser), BRV_THREADS,
-                              smem, s>>>(ctx, w_begin, nwb, m1, (int)win, ws.a, ng1, (int)ng1,
-                                         (int)gpb); note_launch();
+      kern<<<dim3((unsigned)((ng1 + gpb - 1) / gpb), ctx.nser), BRV_THREADS, smem, s>>>(
+          ctx, w_begin, nwb, (int)win, ws.a, ng1, (int)ng1, (int)gpb); note_launch();
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       float* fin;
       size_t fin_pitch, fin_count;
@@ -1999,7 +2025,7 @@ cudaError_t giant_fill(const WidthCtx& ctx, const HitBuffers& hb, unsigned nhits
 // order; the final chain trace of the reference is then the identity.
 // ===========================================================================
 constexpr int CL_TILE = 128;
-constexpr int CL_JCHUNK = 1024;
+constexpr int CL_YBLOCKS = 8;  // chunks of earlier giants per window, about
 
 __global__ void k_cluster_init(int* label, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2007,14 +2033,18 @@ __global__ void k_cluster_init(int* label, int n) {
 }
 
 // Block (x, y): giants [x*CL_TILE, +CL_TILE) against the y-th chunk of
-// CL_JCHUNK earlier giants inside their DM window.
+// `jchunk` earlier giants inside their DM window.  The chunk is the window
+// bound over CL_YBLOCKS (at least 128), so every tile's window is spread over
+// about that many blocks: short scans for small windows, and a grid that
+// stays near tiles x CL_YBLOCKS for large ones.
 __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantBuffers gb,
-                                                           unsigned* changed) {
+                                                           unsigned* changed, int jchunk) {
   __shared__ unsigned s_samp[CL_TILE], s_beam[CL_TILE];
   __shared__ int s_f[CL_TILE], s_dm[CL_TILE], s_lab[CL_TILE];
   const int i_first = blockIdx.x * CL_TILE;
   const int i = i_first + threadIdx.x;
   const int i_last = min(i_first + CL_TILE, a.ngiants) - 1;
+  if ((long long)blockIdx.y * jchunk > (long long)i_last) return;  // uniform: past the tile
   // giants are in ascending DM order: the first candidate neighbour is the
   // first giant within dm_tol of the tile's smallest DM
   const int dm_first = gb.dm[i_first];
@@ -2024,9 +2054,10 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
     if ((long long)gb.dm[mid] + (long long)a.dm_tol < (long long)dm_first) lo = mid + 1;
     else hi = mid;
   }
-  const int j_begin = lo + (int)blockIdx.y * CL_JCHUNK;
-  if (j_begin > i_last) return;  // uniform: this chunk lies past the tile
-  const int j_end = min(j_begin + CL_JCHUNK, i_last + 1);
+  const long long jb = (long long)lo + (long long)blockIdx.y * jchunk;
+  if (jb > (long long)i_last) return;  // uniform: this chunk lies past the tile
+  const int j_begin = (int)jb;
+  const int j_end = (int)min((long long)j_begin + jchunk, (long long)i_last + 1);
   // sample indices fit 31 bits (checked by the host); the test below is
   // are_coincident_beam (are_coincident.cuh:47-68): same beam, time within
   // time_tol x the wider boxcar (a power of two), filter and DM within tolerance.
@@ -2097,8 +2128,14 @@ cudaError_t cluster_init(GiantBuffers& gb, int n, cudaStream_t s) {
 cudaError_t cluster_sweep(const ClusterArgs& a, GiantBuffers& gb, unsigned* changed,
                           cudaStream_t s) {
   if (a.ngiants == 0) return cudaSuccess;
-  dim3 grid((a.ngiants + CL_TILE - 1) / CL_TILE, (a.ngiants + CL_JCHUNK - 1) / CL_JCHUNK);
-  k_cluster_sweep<<<grid, CL_TILE, 0, s>>>(a, gb, changed); note_launch();
+  // a window holds at most the unit's giants (plus the tile's own)
+  const long long wmax = (long long)(a.max_unit_giants > 0 ? a.max_unit_giants : a.ngiants) +
+                         CL_TILE;
+  long long chunk = (wmax + CL_YBLOCKS - 1) / CL_YBLOCKS;
+  chunk = std::max<long long>(128, (chunk + 127) / 128 * 128);
+  const long long ny = (std::min<long long>(wmax, a.ngiants) + chunk - 1) / chunk;
+  dim3 grid((a.ngiants + CL_TILE - 1) / CL_TILE, (unsigned)std::max<long long>(ny, 1));
+  k_cluster_sweep<<<grid, CL_TILE, 0, s>>>(a, gb, changed, (int)chunk); note_launch();
   k_cluster_jump<<<(a.ngiants + 255) / 256, 256, 0, s>>>(gb.label, a.ngiants, changed); note_launch();
   return cudaGetLastError();
 }

@@ -793,8 +793,10 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   if (any_ok && ngiants > 0) {
     // ---- clustering ----------------------------------------------------------
     HD_TRY(hdb::cluster_init(gb, (int)ngiants, s));
+    unsigned max_unit = 0;
+    for (size_t u = 0; u < U; u++) max_unit = std::max(max_unit, first[u + 1] - first[u]);
     hdb::ClusterArgs ca{(int)ngiants, P.cand_sep_time, P.cand_sep_filter, dm_tol,
-                        (unsigned long long)(nsamps / nbeams)};
+                        (unsigned long long)(nsamps / nbeams), (int)max_unit};
     // sweeps until one changes nothing; the fixed point is idempotent, so
     // the sweeps run in pairs, each with its own flag, and the host reads
     // both flags once per pair: the loop ends when the pair's second sweep
