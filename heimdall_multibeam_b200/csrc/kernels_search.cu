@@ -233,31 +233,41 @@ __device__ __forceinline__ float sub_baseline(const BaselineSub& b, size_t ser, 
   return __fsub_rn(x, v);
 }
 
-// data[i] -= stretched baseline, i < nbeams*stride - dm_delay
-__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, BaselineSub b) {
+// data[i] -= stretched baseline, lo <= i < nbeams*stride - dm_delay
+__global__ void k_baseline_sub(float* __restrict__ data, size_t pitch, BaselineSub b,
+                               unsigned lo) {
   const size_t ser = blockIdx.y;
   float* d = data + ser * pitch;
   const unsigned nsub = b.nsub;
   // four consecutive samples per thread (rows are 16-byte aligned)
-  for (unsigned i = 4u * (blockIdx.x * blockDim.x + threadIdx.x); i < nsub;
+  for (unsigned i = (lo & ~3u) + 4u * (blockIdx.x * blockDim.x + threadIdx.x); i < nsub;
        i += 4u * gridDim.x * blockDim.x) {
     float4 x;
-    const bool full = i + 3 < nsub;
+    const bool full = i >= lo && i + 3 < nsub;
     if (full) x = *reinterpret_cast<const float4*>(d + i);
     float* xs = reinterpret_cast<float*>(&x);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const unsigned ij = i + j;
-      if (!full) xs[j] = ij < nsub ? d[ij] : 0.f;
+      if (!full) xs[j] = (ij >= lo && ij < nsub) ? d[ij] : 0.f;
       xs[j] = sub_baseline(b, ser, ij, xs[j]);
     }
     if (full) {
       *reinterpret_cast<float4*>(d + i) = x;
     } else {
       for (int j = 0; j < 4; j++)
-        if (i + j < nsub) d[i + j] = xs[j];
+        if (i + j >= lo && i + j < nsub) d[i + j] = xs[j];
     }
   }
+}
+
+static cudaError_t launch_baseline_sub(const SeriesBatch& sb, const BaselineSub& b, unsigned lo,
+                                       cudaStream_t s) {
+  if (lo >= b.nsub) return cudaSuccess;
+  const size_t nq = (b.nsub - (lo & ~3u) + 3) / 4;
+  dim3 grid((unsigned)((nq + 255) / 256 < 4096 ? (nq + 255) / 256 : 4096), sb.nser);
+  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, b, lo); note_launch();
+  return cudaGetLastError();
 }
 
 size_t baseline_samples(size_t stride, size_t smooth_radius) {
@@ -271,8 +281,12 @@ size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg) {
   return nseg * (ng1 + 8) + 64;
 }
 
-cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                            TreeScratch& ws, cudaStream_t s) {
+// The scrunched baseline of every series into base_out and the description
+// of its subtraction (b->base stays null when there is no baseline).
+static cudaError_t baseline_prepare(const SeriesBatch& sb, size_t smooth_radius,
+                                    float* base_out, TreeScratch& ws, cudaStream_t s,
+                                    BaselineSub* bp) {
+  *bp = BaselineSub();
   BaselinePlan p = baseline_plan(sb.stride, smooth_radius);
   if (p.sample_count == 0) return cudaSuccess;
   const size_t sc = p.sample_count, cr = p.count_round;
@@ -329,10 +343,16 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   b.nbeams = sb.nbeams;
   b.step2 = step2;
   b.step3 = step3;
-  const size_t nq = (nsub + 3) / 4;
-  dim3 grid((unsigned)((nq + 255) / 256 < 4096 ? (nq + 255) / 256 : 4096), sb.nser);
-  k_baseline_sub<<<grid, 256, 0, s>>>(sb.data, sb.pitch, b); note_launch();
-  return cudaGetLastError();
+  *bp = b;
+  return cudaSuccess;
+}
+
+cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
+                            TreeScratch& ws, cudaStream_t s) {
+  BaselineSub b;
+  cudaError_t e = baseline_prepare(sb, smooth_radius, base_out, ws, s, &b);
+  if (e != cudaSuccess || !b.base) return e;
+  return launch_baseline_sub(sb, b, 0, s);
 }
 
 // ===========================================================================
@@ -399,6 +419,63 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
   size_t fin_pitch, fin_count;
   e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
   if (e != cudaSuccess) return e;
+  k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
+      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
+  return cudaGetLastError();
+}
+
+// Single-beam series: the baseline subtraction fused with the first pass of
+// the RMS tree.  Group g of series ser (samples [g 5^m, (g + 1) 5^m), all
+// below nsub) is read raw; each sample has the stretched baseline subtracted
+// (the value k_baseline_sub would write) and is written back, and the
+// group's level-m median of |x| goes to out (what k_rms_beams_pass1 would
+// compute from the subtracted series).  block_tree reads each sample once.
+__global__ void k_sub_rms_pass1(float* __restrict__ data, size_t pitch, BaselineSub b, int m,
+                                float* __restrict__ out, size_t out_pitch) {
+  __shared__ float sm[625 + 125];
+  const size_t ser = blockIdx.y;
+  const size_t g = blockIdx.x;
+  float* d = data + ser * pitch;
+  const size_t q0 = g * pow5(m);
+  float r = block_tree([&](int k) {
+    const unsigned i = (unsigned)(q0 + k);
+    const float x = sub_baseline(b, ser, i, d[i]);
+    d[i] = x;
+    return fabsf(x);
+  }, m, sm);
+  if (threadIdx.x == 0) out[ser * out_pitch + g] = r;
+}
+
+cudaError_t remove_baseline_rms(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
+                                float* rms, TreeScratch& ws, cudaStream_t s) {
+  BaselineSub b;
+  cudaError_t e = baseline_prepare(sb, smooth_radius, base_out, ws, s, &b);
+  if (e != cudaSuccess) return e;
+  if (!b.base) return rms_beams(sb, rms, ws, s);
+  int levels;
+  size_t rem;
+  tree_levels(sb.beam_count, &levels, &rem);
+  // the reference reblocks through a float index, the identity only below
+  // 2^24 samples; longer beams take the separate passes
+  if (sb.nbeams != 1 || levels == 0 || sb.nser > 65535 || sb.beam_count > (1u << 24)) {
+    if ((e = launch_baseline_sub(sb, b, 0, s)) != cudaSuccess) return e;
+    return rms_beams(sb, rms, ws, s);
+  }
+  const int m1 = levels < 5 ? levels : 5;
+  const size_t gsz = pow5(m1);
+  const size_t ng1 = sb.beam_count / gsz;
+  const size_t nseg = (size_t)sb.nser;
+  if (nseg * ng1 > ws.cap || ng1 > 0x7FFFFFFFu) return cudaErrorMemoryAllocation;
+  k_sub_rms_pass1<<<dim3((unsigned)ng1, (unsigned)sb.nser), TREE_THREADS, 0, s>>>(
+      sb.data, sb.pitch, b, m1, ws.a, ng1); note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // the samples past the last whole group: subtraction only
+  if ((e = launch_baseline_sub(sb, b, (unsigned)(ng1 * gsz), s)) != cudaSuccess) return e;
+  float* fin;
+  size_t fin_pitch, fin_count;
+  e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
+  if (e != cudaSuccess) return e;
+  const float delta = (float)(sb.stride - sb.beam_count);
   k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
       fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
   return cudaGetLastError();
@@ -762,7 +839,7 @@ __global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m, in
 // width >= 8 boxcar are 16-byte aligned in the staged window and load as
 // float4 (a thread stride of 80 bytes keeps the 8 lanes of each access phase
 // on distinct banks); widths 1, 2 and 4 read one 28-value window.
-constexpr int BRV_THREADS = 256;
+constexpr int BRV_THREADS = 320;  // 10 warps: the widths of a 2^9 boxcar search, one per warp
 constexpr int VH_MAXW = 16;  // unscrunched widths the vector kernels handle at once
 
 template <int AH, int BH>
