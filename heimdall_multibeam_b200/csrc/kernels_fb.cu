@@ -36,41 +36,88 @@ cudaError_t raise_smem_limit(const void* func, size_t bytes) {
 }
 
 // ---------------------------------------------------------------------------
-// TF -> FT byte transpose, 128 x 128 tiles through shared memory.
+// TF -> FT byte transpose, 128 samples x 128 channels per block through
+// shared memory.  The tile holds 128 sample rows of 32 channel words; word w
+// of row t sits at column w ^ ((t >> 2) & 31), so the row-wise stores of the
+// load phase and the sample-wise loads of the store phase (lane l reads rows
+// 4l..4l+3 of one column) both hit 32 distinct banks.  A thread turns four
+// samples x four channels into four output words with byte permutes.  Rows
+// of whole 16-byte words are loaded 16 bytes at a time.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int tp_col(int t, int w) { return w ^ ((t >> 2) & 31); }
+
 __global__ void __launch_bounds__(256) k_transpose_tf_ft(const uint8_t* __restrict__ in,
                                                          size_t nsamps, int nchans,
                                                          uint8_t* __restrict__ out,
                                                          size_t pitch, size_t out_unit) {
-  __shared__ uint32_t tile[128][33];  // [t][channel word], +1 word against conflicts
+  __shared__ uint32_t tile[128 * 32];
   // blockIdx.z: unit (independent filterbank) of a batch
   in += (size_t)blockIdx.z * nsamps * (size_t)nchans;
   out += (size_t)blockIdx.z * out_unit;
   const size_t t0 = (size_t)blockIdx.x * 128;
   const int c0 = blockIdx.y * 128;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwords = nchans >> 2;
-  for (int r = warp; r < 128; r += 8) {
-    size_t t = t0 + r;
-    int w = (c0 >> 2) + lane;
-    uint32_t v = 0;
-    if (t < nsamps && w < nwords) v = reinterpret_cast<const uint32_t*>(in + t * nchans)[w];
-    tile[r][lane] = v;
+  const int w0 = c0 >> 2;
+  if ((nchans & 15) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0) {
+    // thread: 16-byte chunk q of rows r, r + 32, r + 64, r + 96
+    const int q = threadIdx.x & 7, r0 = threadIdx.x >> 3;
+    uint4 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int r = r0 + 32 * k;
+      const size_t t = t0 + r;
+      v[k] = make_uint4(0u, 0u, 0u, 0u);
+      if (t < nsamps && w0 + 4 * q < nwords)
+        v[k] = *reinterpret_cast<const uint4*>(in + t * nchans + (size_t)(w0 + 4 * q) * 4);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int r = r0 + 32 * k;
+      tile[r * 32 + tp_col(r, 4 * q)] = v[k].x;
+      tile[r * 32 + tp_col(r, 4 * q + 1)] = v[k].y;
+      tile[r * 32 + tp_col(r, 4 * q + 2)] = v[k].z;
+      tile[r * 32 + tp_col(r, 4 * q + 3)] = v[k].w;
+    }
+  } else {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t v[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const size_t t = t0 + warp + 8 * k;
+      v[k] = 0u;
+      if (t < nsamps && w0 + lane < nwords)
+        v[k] = reinterpret_cast<const uint32_t*>(in + t * nchans)[w0 + lane];
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const int r = warp + 8 * k;
+      tile[r * 32 + tp_col(r, lane)] = v[k];
+    }
   }
   __syncthreads();
-  // each warp writes 16 channel rows; lane l writes samples 4l..4l+3 as a word
-  for (int cr = warp; cr < 128; cr += 8) {
-    int c = c0 + cr;
-    if (c >= nchans) break;
-    int wsel = cr >> 2, bsel = cr & 3;
-    uint32_t o = 0;
+  // warp: channel words wsel = warp, warp + 8, ...; lane: samples 4l .. 4l+3
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t t = t0 + 4 * lane;
+  for (int ws = warp; ws < 32; ws += 8) {
+    if (4 * ws + c0 >= nchans) break;
+    uint32_t a[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      uint32_t v = tile[4 * lane + j][wsel];
-      o |= ((v >> (8 * bsel)) & 0xFFu) << (8 * j);
+      const int r = 4 * lane + j;
+      a[j] = tile[r * 32 + tp_col(r, ws)];
     }
-    size_t t = t0 + 4 * lane;
-    if (t < nsamps) reinterpret_cast<uint32_t*>(out + (size_t)c * pitch + t)[0] = o;
+    // 4 x 4 byte transpose: o[b] = byte b of a[0..3]
+    const uint32_t lo01 = __byte_perm(a[0], a[1], 0x5140), lo23 = __byte_perm(a[2], a[3], 0x5140);
+    const uint32_t hi01 = __byte_perm(a[0], a[1], 0x7362), hi23 = __byte_perm(a[2], a[3], 0x7362);
+    const uint32_t o[4] = {__byte_perm(lo01, lo23, 0x5410), __byte_perm(lo01, lo23, 0x7632),
+                           __byte_perm(hi01, hi23, 0x5410), __byte_perm(hi01, hi23, 0x7632)};
+    if (t < nsamps) {
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const int c = c0 + 4 * ws + b;
+        if (c < nchans) reinterpret_cast<uint32_t*>(out + (size_t)c * pitch + t)[0] = o[b];
+      }
+    }
   }
 }
 

@@ -698,7 +698,9 @@ dedisp_error dedisp_execute_adv(const dedisp_plan p, dedisp_size nsamps, const d
       (p->nchans % 4) != 0)
     return DEDISP_INVALID_STRIDE;
   if (out_stride % 4) return DEDISP_INVALID_STRIDE;
-  if (in_nbits != 8 && (reinterpret_cast<uintptr_t>(in) & 3)) return DEDISP_INVALID_POINTER;
+  // spectra are read as 32-bit words: device input must be 4-byte aligned
+  if ((flags & DEDISP_DEVICE_POINTERS) && (reinterpret_cast<uintptr_t>(in) & 3))
+    return DEDISP_INVALID_POINTER;
   dedisp_error de = hdb::plan_prepare(p);
   if (de != DEDISP_NO_ERROR) return de;
   if (nsamps < p->max_delay) return DEDISP_TOO_FEW_NSAMPS;

@@ -132,8 +132,8 @@ dedisp_float        dedisp_get_df(const dedisp_plan plan);
  * (out_stride bytes apart, out_nbits per sample; 32 = float, the only output
  * width).  Sums are exact integers written as float (rounded once); 16-bit
  * samples are summed as low and high bytes, lo + 256 hi, and take no adaptive
- * dt (DEDISP_UNSUPPORTED_IN_NBITS).  Packed input from device memory must be
- * 4-byte aligned.
+ * dt (DEDISP_UNSUPPORTED_IN_NBITS).  Input in device memory
+ * (DEDISP_DEVICE_POINTERS) must be 4-byte aligned (DEDISP_INVALID_POINTER).
  * pipeline.cu:459-462, clean_filterbank_rfi.cu:389-393 */
 dedisp_error dedisp_execute_adv(const dedisp_plan plan, dedisp_size nsamps,
                                 const dedisp_byte* in, dedisp_size in_nbits,
