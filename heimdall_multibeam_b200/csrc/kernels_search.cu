@@ -426,23 +426,28 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 
 // Single-beam series: the baseline subtraction fused with the first pass of
 // the RMS tree.  Group g of series ser (samples [g 5^m, (g + 1) 5^m), all
-// below nsub) is read raw; each sample has the stretched baseline subtracted
-// (the value k_baseline_sub would write) and is written back, and the
-// group's level-m median of |x| goes to out (what k_rms_beams_pass1 would
-// compute from the subtracted series).  block_tree reads each sample once.
+// below nsub) is read raw, coalesced; each sample has the stretched baseline
+// subtracted (the value k_baseline_sub would write) and is written back, and
+// |x| is staged in shared memory, from which the group's level-m median of
+// |x| goes to out (what k_rms_beams_pass1 would compute from the subtracted
+// series).
 __global__ void k_sub_rms_pass1(float* __restrict__ data, size_t pitch, BaselineSub b, int m,
                                 float* __restrict__ out, size_t out_pitch) {
+  __shared__ float stage[3125];
   __shared__ float sm[625 + 125];
   const size_t ser = blockIdx.y;
   const size_t g = blockIdx.x;
   float* d = data + ser * pitch;
-  const size_t q0 = g * pow5(m);
-  float r = block_tree([&](int k) {
+  const int gsz = (int)pow5(m);
+  const size_t q0 = g * (size_t)gsz;
+  for (int k = threadIdx.x; k < gsz; k += blockDim.x) {
     const unsigned i = (unsigned)(q0 + k);
     const float x = sub_baseline(b, ser, i, d[i]);
     d[i] = x;
-    return fabsf(x);
-  }, m, sm);
+    stage[k] = fabsf(x);
+  }
+  __syncthreads();
+  const float r = block_tree([&](int k) { return stage[k]; }, m, sm);
   if (threadIdx.x == 0) out[ser * out_pitch + g] = r;
 }
 
@@ -487,17 +492,22 @@ cudaError_t remove_baseline_rms(const SeriesBatch& sb, size_t smooth_radius, flo
 // out[k+1] = out[k] + in[k]), for up to 8 series per block.
 //
 // The left-to-right float sum of a series is one dependent chain (~4 cycles
-// per sample), so the block is split by role:
+// per sample), so the block is split by role, and the roles hand stages to
+// each other through mbarriers rather than block barriers:
 //   warp 0       the chains: lane l owns series l of the block and runs its
 //                chain over one stage of its row in shared memory;
-//   warps 1..np  a stage's rows arrive by TMA bulk copies requested SC_DEPTH
-//                stages ahead; these warps divide them in place by their
-//                beam's RMS, and write them out once the chain warp has
-//                replaced them with their prefix sums.
-// Stage k lives in buffer k % SC_NB.  At step k the producers normalise stage
-// k and store stage k - 2 while the chain warp scans stage k - 1, and stage
-// k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
-// step k - 1).  One block barrier ends each step.
+//   warps 1..np  a stage's rows arrive by TMA bulk copies (warp 1, lane 0);
+//                these warps divide them in place by their beam's RMS, and
+//                write them out once the chain warp has replaced them with
+//                their prefix sums.
+// Stage k lives in buffer k % SC_NB and passes four mbarriers of that buffer:
+// full (its copies landed), ready (every producer warp normalised its rows),
+// scanned (the chain warp is done) and freed (every producer warp stored its
+// rows), after which stage k + SC_NB is requested into the buffer.  At its
+// step k a producer warp normalises stage k and stores stage k - 2, so the
+// chain warp only waits when a stage is genuinely not ready.  Every wait is
+// bounded; one that gives up sets bit 1 of *err and the warp leaves its
+// loop, the copy warp letting its copies in flight land first.
 // ===========================================================================
 constexpr int SC_DEPTH = 5;          // stages in flight ahead of the one being normalised
 constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
@@ -522,7 +532,7 @@ __device__ __forceinline__ float div_rn_by(float a, float b, float y) {
 }
 
 size_t scan_smem_bytes(int ser, int nbeams, int ch) {
-  size_t b = 128 + (size_t)SC_NB * ser * (ch + 4) * sizeof(float);
+  size_t b = 256 + (size_t)SC_NB * ser * (ch + 4) * sizeof(float);
   if ((size_t)ser * nbeams <= SC_MAXRMS) b += 2 * (size_t)ser * nbeams * sizeof(float);
   return b;
 }
@@ -538,10 +548,14 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
     float* norm_out, int ser_per_block, unsigned* err) {
   constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
   constexpr int QN = CH / 128; // float4 per lane per row
+  constexpr int LAG = 2;       // a producer warp stores stage k - LAG at its step k
   extern __shared__ __align__(128) float sc_smem[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(sc_smem);  // [SC_NB], first 128 bytes
+  uint64_t* full = reinterpret_cast<uint64_t*>(sc_smem);  // [SC_NB] each, first 256 bytes
+  uint64_t* ready = full + SC_NB;
+  uint64_t* scanned = ready + SC_NB;
+  uint64_t* freed = scanned + SC_NB;
   const int S = ser_per_block;
-  float* rows = sc_smem + 32;                             // [SC_NB][S][ROW]
+  float* rows = sc_smem + 64;                             // [SC_NB][S][ROW]
   float* srms = rows + (size_t)SC_NB * S * ROW;           // [S][nbeams]
   float* sy = srms + S * nbeams;                          // reciprocals
   const int s0 = blockIdx.x * S;
@@ -553,7 +567,12 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
   const unsigned len4 = (len + 3u) & ~3u;   // copies round up to 16 bytes (inside the row pitch)
 
   if (threadIdx.x == 0) {
-    for (int b = 0; b < SC_NB; b++) mbar_init(&full[b], 1);
+    for (int b = 0; b < SC_NB; b++) {
+      mbar_init(&full[b], 1);
+      mbar_init(&ready[b], (uint32_t)np);
+      mbar_init(&scanned[b], 1);
+      mbar_init(&freed[b], (uint32_t)np);
+    }
     fence_mbar_init();
   }
   if (rms_smem)
@@ -562,10 +581,10 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       srms[k] = r;
       sy[k] = __frcp_rn(r);
     }
-  __syncthreads();
+  __syncthreads();  // the only block barrier: the barriers and RMS table are set up
 
-  // stage st -> its buffer; warp 1, one row per lane; a stage past the data
-  // completes its barrier phase with a plain arrival
+  // stage st -> its buffer (warp 1); a stage past the data completes its
+  // `full` phase with a plain arrival
   auto request = [&](unsigned st) {
     uint64_t* bar = &full[st % SC_NB];
     const unsigned base = st * CH;
@@ -577,22 +596,25 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
     }
     if (lane == 0) mbar_expect_tx(bar, bytes * (unsigned)nb);
     __syncwarp();
-    // the buffer was last written by this block's threads (generic proxy)
+    // the buffer was last written and read by this block's threads
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (lane < nb)
       bulk_g2s(rows + ((size_t)(st % SC_NB) * S + lane) * ROW,
                data + (size_t)(s0 + lane) * pitch + base, bytes, bar);
   };
-  if (warp == 1)
-    for (unsigned st = 0; st < (unsigned)SC_DEPTH && st < nstage; st++) request(st);
-
-  float sum = 0.f;     // chain of series s0 + lane (warp 0)
+  auto par = [](unsigned st) { return (st / SC_NB) & 1u; };
   bool failed = false;
-  for (unsigned k = 0; k < nstage + 2; k++) {
-    if (warp == 0) {
-      // ---- the chains: stage k - 1 ----
-      if (k >= 1 && k - 1 < nstage && lane < nb) {
-        float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * ROW;
+
+  if (warp == 0) {
+    // ---------------- the chains ----------------
+    float sum = 0.f;
+    for (unsigned k = 0; k < nstage; k++) {
+      if (!mbar_wait(&ready[k % SC_NB], par(k), SC_WAIT_LIMIT)) {
+        if (err && lane == 0) atomicOr(err, 2u);
+        break;
+      }
+      if (lane < nb) {
+        float* row = rows + ((size_t)(k % SC_NB) * S + lane) * ROW;
 #pragma unroll 8
         for (int e = 0; e < CH; e += 4) {
           const float4 v = *reinterpret_cast<const float4*>(row + e);
@@ -604,37 +626,26 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
           *reinterpret_cast<float4*>(row + e) = o;
         }
       }
-    } else {
-      const int p = warp - 1;
-      if (warp == 1 && k + SC_DEPTH < nstage) request(k + SC_DEPTH);
-      // ---- store stage k - 2 ----
-      if (k >= 2 && k - 2 < nstage) {
-        const unsigned st = k - 2;
-        for (int sl = p; sl < nb; sl += np) {
-          const float* rrow = rows + ((size_t)(st % SC_NB) * S + sl) * ROW;
-          float* orow = scan + (size_t)(s0 + sl) * scan_pitch;
-#pragma unroll
-          for (int q = 0; q < QN; q++) {
-            const unsigned e = 4u * lane + 128u * q;
-            const unsigned i = st * CH + e;
-            const float4 v = *reinterpret_cast<const float4*>(rrow + e);
-            float* o = orow + i;
-            if (i + 3 <= len) {
-              *reinterpret_cast<float4*>(o) = v;
-            } else {
-              if (i <= len) o[0] = v.x;
-              if (i + 1 <= len) o[1] = v.y;
-              if (i + 2 <= len) o[2] = v.z;
-            }
-          }
-        }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&scanned[k % SC_NB]);
+    }
+    return;
+  }
+
+  // ---------------- producers (warps 1..np) ----------------
+  const int p = warp - 1;
+  if (warp == 1)
+    for (unsigned st = 0; st < (unsigned)SC_NB && st < nstage; st++) request(st);
+  unsigned issued = warp == 1 ? min((unsigned)SC_NB, nstage) : 0u;
+  for (unsigned k = 0; k < nstage + LAG; k++) {
+    if (k < nstage) {
+      if (!mbar_wait(&full[k % SC_NB], par(k), SC_WAIT_LIMIT)) {
+        if (err && lane == 0) atomicOr(err, 2u);
+        failed = true;
+        break;
       }
       // ---- normalise stage k (get_rms.cu:344-356): x / rms[beam of sample] ----
-      if (k < nstage) {
-        if (!mbar_wait(&full[k % SC_NB], (k / SC_NB) & 1u, SC_WAIT_LIMIT)) {
-          if (!failed && err && lane == 0) atomicOr(err, 2u);
-          failed = true;
-        }
+      {
         const unsigned base = k * CH;
         unsigned b0 = base / stride;
         if (b0 > (unsigned)nbeams - 1) b0 = (unsigned)nbeams - 1;
@@ -700,14 +711,54 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
           }
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ready[k % SC_NB]);
     }
-    __syncthreads();
+    // ---- store stage k - LAG once the chain warp has scanned it ----
+    if (k >= LAG && k - LAG < nstage) {
+      const unsigned st = k - LAG;
+      if (!mbar_wait(&scanned[st % SC_NB], par(st), SC_WAIT_LIMIT)) {
+        if (err && lane == 0) atomicOr(err, 2u);
+        failed = true;
+        break;
+      }
+      for (int sl = p; sl < nb; sl += np) {
+        const float* rrow = rows + ((size_t)(st % SC_NB) * S + sl) * ROW;
+        float* orow = scan + (size_t)(s0 + sl) * scan_pitch;
+#pragma unroll
+        for (int q = 0; q < QN; q++) {
+          const unsigned e = 4u * lane + 128u * q;
+          const unsigned i = st * CH + e;
+          const float4 v = *reinterpret_cast<const float4*>(rrow + e);
+          float* o = orow + i;
+          if (i + 3 <= len) {
+            *reinterpret_cast<float4*>(o) = v;
+          } else {
+            if (i <= len) o[0] = v.x;
+            if (i + 1 <= len) o[1] = v.y;
+            if (i + 2 <= len) o[2] = v.z;
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&freed[st % SC_NB]);
+      // ---- refill the buffer with stage st + SC_NB (warp 1) ----
+      if (warp == 1 && st + SC_NB < nstage) {
+        if (!mbar_wait(&freed[st % SC_NB], par(st), SC_WAIT_LIMIT)) {
+          if (err && lane == 0) atomicOr(err, 2u);
+          failed = true;
+          break;
+        }
+        request(st + SC_NB);
+        issued = st + SC_NB + 1;
+      }
+    }
   }
-  // every copy has been waited for at its normalise step; after a timed-out
-  // wait, let the buffers' last copies land before the block exits
+  // after a timed-out wait, let the copies this block issued land before it
+  // exits (warp 1 issued them all)
   if (failed && warp == 1)
-    for (unsigned st = (nstage > SC_NB ? nstage - SC_NB : 0); st < nstage; st++)
-      mbar_wait(&full[st % SC_NB], (st / SC_NB) & 1u, SC_WAIT_LIMIT);
+    for (unsigned st = (issued > SC_NB ? issued - SC_NB : 0); st < issued; st++)
+      mbar_wait(&full[st % SC_NB], par(st), SC_WAIT_LIMIT);
 }
 
 template <int CH>
