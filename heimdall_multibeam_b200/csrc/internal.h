@@ -174,11 +174,6 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
 // GetRMSPlanMB::exec_multibeam, vector form (Pipeline/get_rms.cu:236-270):
 // rms[ser*nbeams + b].
 cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s);
-// remove_baseline followed by rms_beams, with the subtraction fused into the
-// RMS tree's first pass for single-beam series (one read and write of the
-// series instead of two reads and a write); the same values in data and rms.
-cudaError_t remove_baseline_rms(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                                float* rms, TreeScratch& ws, cudaStream_t s);
 // normalise_multibeam (get_rms.cu:372-382) fused with the exclusive prefix sum
 // of MatchedFilterPlan::prep (matched_filter.cu:21-32), sequential association:
 // scan[ser][0..len] (len + 1 values, pitch scan_pitch).  norm_out (nullable,

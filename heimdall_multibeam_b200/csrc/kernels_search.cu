@@ -424,90 +424,23 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
   return cudaGetLastError();
 }
 
-// Single-beam series: the baseline subtraction fused with the first pass of
-// the RMS tree.  Group g of series ser (samples [g 5^m, (g + 1) 5^m), all
-// below nsub) is read raw, coalesced; each sample has the stretched baseline
-// subtracted (the value k_baseline_sub would write) and is written back, and
-// |x| is staged in shared memory, from which the group's level-m median of
-// |x| goes to out (what k_rms_beams_pass1 would compute from the subtracted
-// series).
-__global__ void k_sub_rms_pass1(float* __restrict__ data, size_t pitch, BaselineSub b, int m,
-                                float* __restrict__ out, size_t out_pitch) {
-  __shared__ float stage[3125];
-  __shared__ float sm[625 + 125];
-  const size_t ser = blockIdx.y;
-  const size_t g = blockIdx.x;
-  float* d = data + ser * pitch;
-  const int gsz = (int)pow5(m);
-  const size_t q0 = g * (size_t)gsz;
-  for (int k = threadIdx.x; k < gsz; k += blockDim.x) {
-    const unsigned i = (unsigned)(q0 + k);
-    const float x = sub_baseline(b, ser, i, d[i]);
-    d[i] = x;
-    stage[k] = fabsf(x);
-  }
-  __syncthreads();
-  const float r = block_tree([&](int k) { return stage[k]; }, m, sm);
-  if (threadIdx.x == 0) out[ser * out_pitch + g] = r;
-}
-
-cudaError_t remove_baseline_rms(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                                float* rms, TreeScratch& ws, cudaStream_t s) {
-  BaselineSub b;
-  cudaError_t e = baseline_prepare(sb, smooth_radius, base_out, ws, s, &b);
-  if (e != cudaSuccess) return e;
-  if (!b.base) return rms_beams(sb, rms, ws, s);
-  int levels;
-  size_t rem;
-  tree_levels(sb.beam_count, &levels, &rem);
-  // the reference reblocks through a float index, the identity only below
-  // 2^24 samples; longer beams take the separate passes
-  if (sb.nbeams != 1 || levels == 0 || sb.nser > 65535 || sb.beam_count > (1u << 24)) {
-    if ((e = launch_baseline_sub(sb, b, 0, s)) != cudaSuccess) return e;
-    return rms_beams(sb, rms, ws, s);
-  }
-  const int m1 = levels < 5 ? levels : 5;
-  const size_t gsz = pow5(m1);
-  const size_t ng1 = sb.beam_count / gsz;
-  const size_t nseg = (size_t)sb.nser;
-  if (nseg * ng1 > ws.cap || ng1 > 0x7FFFFFFFu) return cudaErrorMemoryAllocation;
-  k_sub_rms_pass1<<<dim3((unsigned)ng1, (unsigned)sb.nser), TREE_THREADS, 0, s>>>(
-      sb.data, sb.pitch, b, m1, ws.a, ng1); note_launch();
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  // the samples past the last whole group: subtraction only
-  if ((e = launch_baseline_sub(sb, b, (unsigned)(ng1 * gsz), s)) != cudaSuccess) return e;
-  float* fin;
-  size_t fin_pitch, fin_count;
-  e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
-  if (e != cudaSuccess) return e;
-  const float delta = (float)(sb.stride - sb.beam_count);
-  k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
-  return cudaGetLastError();
-}
-
 // ===========================================================================
 // Normalise + exclusive prefix sum with the sequential association of the
 // reference's scan (Thrust's sequential exclusive_scan: out[0] = 0,
 // out[k+1] = out[k] + in[k]), for up to 8 series per block.
 //
 // The left-to-right float sum of a series is one dependent chain (~4 cycles
-// per sample), so the block is split by role, and the roles hand stages to
-// each other through mbarriers rather than block barriers:
+// per sample), so the block is split by role:
 //   warp 0       the chains: lane l owns series l of the block and runs its
 //                chain over one stage of its row in shared memory;
-//   warps 1..np  a stage's rows arrive by TMA bulk copies (warp 1, lane 0);
-//                these warps divide them in place by their beam's RMS, and
-//                write them out once the chain warp has replaced them with
-//                their prefix sums.
-// Stage k lives in buffer k % SC_NB and passes four mbarriers of that buffer:
-// full (its copies landed), ready (every producer warp normalised its rows),
-// scanned (the chain warp is done) and freed (every producer warp stored its
-// rows), after which stage k + SC_NB is requested into the buffer.  At its
-// step k a producer warp normalises stage k and stores stage k - 2, so the
-// chain warp only waits when a stage is genuinely not ready.  Every wait is
-// bounded; one that gives up sets bit 1 of *err and the warp leaves its
-// loop, the copy warp letting its copies in flight land first.
+//   warps 1..np  a stage's rows arrive by TMA bulk copies requested SC_DEPTH
+//                stages ahead; these warps divide them in place by their
+//                beam's RMS, and write them out once the chain warp has
+//                replaced them with their prefix sums.
+// Stage k lives in buffer k % SC_NB.  At step k the producers normalise stage
+// k and store stage k - 2 while the chain warp scans stage k - 1, and stage
+// k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
+// step k - 1).  One block barrier ends each step.
 // ===========================================================================
 constexpr int SC_DEPTH = 5;          // stages in flight ahead of the one being normalised
 constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
@@ -532,7 +465,7 @@ __device__ __forceinline__ float div_rn_by(float a, float b, float y) {
 }
 
 size_t scan_smem_bytes(int ser, int nbeams, int ch) {
-  size_t b = 256 + (size_t)SC_NB * ser * (ch + 4) * sizeof(float);
+  size_t b = 128 + (size_t)SC_NB * ser * (ch + 4) * sizeof(float);
   if ((size_t)ser * nbeams <= SC_MAXRMS) b += 2 * (size_t)ser * nbeams * sizeof(float);
   return b;
 }
@@ -548,14 +481,10 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
     float* norm_out, int ser_per_block, unsigned* err) {
   constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
   constexpr int QN = CH / 128; // float4 per lane per row
-  constexpr int LAG = 2;       // a producer warp stores stage k - LAG at its step k
   extern __shared__ __align__(128) float sc_smem[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(sc_smem);  // [SC_NB] each, first 256 bytes
-  uint64_t* ready = full + SC_NB;
-  uint64_t* scanned = ready + SC_NB;
-  uint64_t* freed = scanned + SC_NB;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sc_smem);  // [SC_NB], first 128 bytes
   const int S = ser_per_block;
-  float* rows = sc_smem + 64;                             // [SC_NB][S][ROW]
+  float* rows = sc_smem + 32;                             // [SC_NB][S][ROW]
   float* srms = rows + (size_t)SC_NB * S * ROW;           // [S][nbeams]
   float* sy = srms + S * nbeams;                          // reciprocals
   const int s0 = blockIdx.x * S;
@@ -567,12 +496,7 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
   const unsigned len4 = (len + 3u) & ~3u;   // copies round up to 16 bytes (inside the row pitch)
 
   if (threadIdx.x == 0) {
-    for (int b = 0; b < SC_NB; b++) {
-      mbar_init(&full[b], 1);
-      mbar_init(&ready[b], (uint32_t)np);
-      mbar_init(&scanned[b], 1);
-      mbar_init(&freed[b], (uint32_t)np);
-    }
+    for (int b = 0; b < SC_NB; b++) mbar_init(&full[b], 1);
     fence_mbar_init();
   }
   if (rms_smem)
@@ -581,10 +505,10 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       srms[k] = r;
       sy[k] = __frcp_rn(r);
     }
-  __syncthreads();  // the only block barrier: the barriers and RMS table are set up
+  __syncthreads();
 
-  // stage st -> its buffer (warp 1); a stage past the data completes its
-  // `full` phase with a plain arrival
+  // stage st -> its buffer; warp 1, one row per lane; a stage past the data
+  // completes its barrier phase with a plain arrival
   auto request = [&](unsigned st) {
     uint64_t* bar = &full[st % SC_NB];
     const unsigned base = st * CH;
@@ -596,25 +520,22 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
     }
     if (lane == 0) mbar_expect_tx(bar, bytes * (unsigned)nb);
     __syncwarp();
-    // the buffer was last written and read by this block's threads
+    // the buffer was last written by this block's threads (generic proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (lane < nb)
       bulk_g2s(rows + ((size_t)(st % SC_NB) * S + lane) * ROW,
                data + (size_t)(s0 + lane) * pitch + base, bytes, bar);
   };
-  auto par = [](unsigned st) { return (st / SC_NB) & 1u; };
-  bool failed = false;
+  if (warp == 1)
+    for (unsigned st = 0; st < (unsigned)SC_DEPTH && st < nstage; st++) request(st);
 
-  if (warp == 0) {
-    // ---------------- the chains ----------------
-    float sum = 0.f;
-    for (unsigned k = 0; k < nstage; k++) {
-      if (!mbar_wait(&ready[k % SC_NB], par(k), SC_WAIT_LIMIT)) {
-        if (err && lane == 0) atomicOr(err, 2u);
-        break;
-      }
-      if (lane < nb) {
-        float* row = rows + ((size_t)(k % SC_NB) * S + lane) * ROW;
+  float sum = 0.f;     // chain of series s0 + lane (warp 0)
+  bool failed = false;
+  for (unsigned k = 0; k < nstage + 2; k++) {
+    if (warp == 0) {
+      // ---- the chains: stage k - 1 ----
+      if (k >= 1 && k - 1 < nstage && lane < nb) {
+        float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * ROW;
 #pragma unroll 8
         for (int e = 0; e < CH; e += 4) {
           const float4 v = *reinterpret_cast<const float4*>(row + e);
@@ -626,26 +547,37 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
           *reinterpret_cast<float4*>(row + e) = o;
         }
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&scanned[k % SC_NB]);
-    }
-    return;
-  }
-
-  // ---------------- producers (warps 1..np) ----------------
-  const int p = warp - 1;
-  if (warp == 1)
-    for (unsigned st = 0; st < (unsigned)SC_NB && st < nstage; st++) request(st);
-  unsigned issued = warp == 1 ? min((unsigned)SC_NB, nstage) : 0u;
-  for (unsigned k = 0; k < nstage + LAG; k++) {
-    if (k < nstage) {
-      if (!mbar_wait(&full[k % SC_NB], par(k), SC_WAIT_LIMIT)) {
-        if (err && lane == 0) atomicOr(err, 2u);
-        failed = true;
-        break;
+    } else {
+      const int p = warp - 1;
+      if (warp == 1 && k + SC_DEPTH < nstage) request(k + SC_DEPTH);
+      // ---- store stage k - 2 ----
+      if (k >= 2 && k - 2 < nstage) {
+        const unsigned st = k - 2;
+        for (int sl = p; sl < nb; sl += np) {
+          const float* rrow = rows + ((size_t)(st % SC_NB) * S + sl) * ROW;
+          float* orow = scan + (size_t)(s0 + sl) * scan_pitch;
+#pragma unroll
+          for (int q = 0; q < QN; q++) {
+            const unsigned e = 4u * lane + 128u * q;
+            const unsigned i = st * CH + e;
+            const float4 v = *reinterpret_cast<const float4*>(rrow + e);
+            float* o = orow + i;
+            if (i + 3 <= len) {
+              *reinterpret_cast<float4*>(o) = v;
+            } else {
+              if (i <= len) o[0] = v.x;
+              if (i + 1 <= len) o[1] = v.y;
+              if (i + 2 <= len) o[2] = v.z;
+            }
+          }
+        }
       }
       // ---- normalise stage k (get_rms.cu:344-356): x / rms[beam of sample] ----
-      {
+      if (k < nstage) {
+        if (!mbar_wait(&full[k % SC_NB], (k / SC_NB) & 1u, SC_WAIT_LIMIT)) {
+          if (!failed && err && lane == 0) atomicOr(err, 2u);
+          failed = true;
+        }
         const unsigned base = k * CH;
         unsigned b0 = base / stride;
         if (b0 > (unsigned)nbeams - 1) b0 = (unsigned)nbeams - 1;
@@ -711,54 +643,14 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
           }
         }
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&ready[k % SC_NB]);
     }
-    // ---- store stage k - LAG once the chain warp has scanned it ----
-    if (k >= LAG && k - LAG < nstage) {
-      const unsigned st = k - LAG;
-      if (!mbar_wait(&scanned[st % SC_NB], par(st), SC_WAIT_LIMIT)) {
-        if (err && lane == 0) atomicOr(err, 2u);
-        failed = true;
-        break;
-      }
-      for (int sl = p; sl < nb; sl += np) {
-        const float* rrow = rows + ((size_t)(st % SC_NB) * S + sl) * ROW;
-        float* orow = scan + (size_t)(s0 + sl) * scan_pitch;
-#pragma unroll
-        for (int q = 0; q < QN; q++) {
-          const unsigned e = 4u * lane + 128u * q;
-          const unsigned i = st * CH + e;
-          const float4 v = *reinterpret_cast<const float4*>(rrow + e);
-          float* o = orow + i;
-          if (i + 3 <= len) {
-            *reinterpret_cast<float4*>(o) = v;
-          } else {
-            if (i <= len) o[0] = v.x;
-            if (i + 1 <= len) o[1] = v.y;
-            if (i + 2 <= len) o[2] = v.z;
-          }
-        }
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&freed[st % SC_NB]);
-      // ---- refill the buffer with stage st + SC_NB (warp 1) ----
-      if (warp == 1 && st + SC_NB < nstage) {
-        if (!mbar_wait(&freed[st % SC_NB], par(st), SC_WAIT_LIMIT)) {
-          if (err && lane == 0) atomicOr(err, 2u);
-          failed = true;
-          break;
-        }
-        request(st + SC_NB);
-        issued = st + SC_NB + 1;
-      }
-    }
+    __syncthreads();
   }
-  // after a timed-out wait, let the copies this block issued land before it
-  // exits (warp 1 issued them all)
+  // every copy has been waited for at its normalise step; after a timed-out
+  // wait, let the buffers' last copies land before the block exits
   if (failed && warp == 1)
-    for (unsigned st = (issued > SC_NB ? issued - SC_NB : 0); st < issued; st++)
-      mbar_wait(&full[st % SC_NB], par(st), SC_WAIT_LIMIT);
+    for (unsigned st = (nstage > SC_NB ? nstage - SC_NB : 0); st < nstage; st++)
+      mbar_wait(&full[st % SC_NB], (st / SC_NB) & 1u, SC_WAIT_LIMIT);
 }
 
 template <int CH>

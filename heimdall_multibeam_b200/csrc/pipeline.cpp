@@ -577,8 +577,8 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     const float cur_dt = P.dt * (float)scr;
     const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
     hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
-    HD_TRY(hdb::remove_baseline_rms(sb, nsmooth, pl->base.as<float>(), pl->rms.as<float>(), ws,
-                                    s));
+    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
+    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan_g, scan_pitch, nullptr, s,
                                pl->plan->d_err));
     if (gi == 0) cudaEventRecord(pl->ev[4], s);
