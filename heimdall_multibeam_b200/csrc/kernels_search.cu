@@ -782,7 +782,7 @@ __global__ void k_block_rms_pass1_multi(WidthCtx ctx, int w0, int nwb, int m, in
 // width >= 8 boxcar are 16-byte aligned in the staged window and load as
 // float4 (a thread stride of 80 bytes keeps the 8 lanes of each access phase
 // on distinct banks); widths 1, 2 and 4 read one 28-value window.
-constexpr int BRV_THREADS = 320;  // 10 warps: the widths of a 2^9 boxcar search, one per warp
+constexpr int BRV_THREADS = 512;  // at most 16 warps: one per boxcar width
 constexpr int VH_MAXW = 16;  // unscrunched widths the vector kernels handle at once
 
 template <int AH, int BH>
@@ -803,10 +803,11 @@ __device__ __forceinline__ float max5(float a, float b, float c, float d, float 
 __host__ __device__ constexpr int pow5c(int k) { return k <= 0 ? 1 : 5 * pow5c(k - 1); }
 
 // The median levels of one group for every width slot, M levels in the block
-// (compile-time: every index is divided by a constant).  Level 1 and level 2
-// run block-wide, one barrier each; levels 3..M of a width slot run inside
-// one warp (warp w takes slots w, w + 8, ...), with only warp
-// synchronisation, in the slot's own rows of la and lb.
+// (compile-time).  Warp w takes width slots w, w + nwarps, ... (the launcher
+// gives a block one warp per slot, up to 16), and each slot's work -- level
+// 1 over the staged window, levels 2..M in the slot's own rows of la and lb,
+// and the group maximum -- stays inside its warp: branches are uniform, and
+// no block barrier is needed until the next group's window.
 template <bool MM, int M>
 __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, int w0, int nwb,
                            float* la, float* lb, float* __restrict__ out, size_t out_pitch,
@@ -818,76 +819,79 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
   // 20 samples, then the < 4 remaining single medians)
   constexpr int nq = n1 / 4, rem = n1 - 4 * nq;
   constexpr int rp = nq + 4;
-
-  // ---- level 1 ----
-  if constexpr (nq > 0)
-  for (int item = threadIdx.x; item < nwb * nq; item += blockDim.x) {
-    const int wl = item / nq, k0 = 4 * (item - wl * nq);
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  for (int wl = threadIdx.x >> 5; wl < nwb; wl += nwarps) {
     const int wi = w0 + wl;
-    float v[20];
+    float* la_w = la + wl * n1p;
+    float* srun_w = srun + wl * rp;
+
+    // ---- level 1: runs of 4 medians (20 consecutive samples) per lane ----
     if (wi < 3) {
-      float wv[28];
-      const float4* p = reinterpret_cast<const float4*>(tile + 5 * k0 + offset - 4);
+      for (int q = lane; q < nq; q += 32) {
+        const int k0 = 4 * q;
+        float v[20], wv[28];
+        const float4* p = reinterpret_cast<const float4*>(tile + 5 * k0 + offset - 4);
 #pragma unroll
-      for (int r = 0; r < 7; r++) {
-        const float4 x = p[r];
-        wv[4 * r] = x.x; wv[4 * r + 1] = x.y; wv[4 * r + 2] = x.z; wv[4 * r + 3] = x.w;
+        for (int r = 0; r < 7; r++) {
+          const float4 x = p[r];
+          wv[4 * r] = x.x; wv[4 * r + 1] = x.y; wv[4 * r + 2] = x.z; wv[4 * r + 3] = x.w;
+        }
+        if (wi == 0) brv_small<1, 0>(wv, v);
+        else if (wi == 1) brv_small<1, 1>(wv, v);
+        else brv_small<2, 2>(wv, v);
+        float4 o;
+        o.x = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+        o.y = brv_med5<MM>(v[5], v[6], v[7], v[8], v[9]);
+        o.z = brv_med5<MM>(v[10], v[11], v[12], v[13], v[14]);
+        o.w = brv_med5<MM>(v[15], v[16], v[17], v[18], v[19]);
+        *reinterpret_cast<float4*>(la_w + k0) = o;
+        if (rec)
+          srun_w[q] = fmaxf(fmaxf(max5(v[0], v[1], v[2], v[3], v[4]), max5(v[5], v[6], v[7], v[8], v[9])),
+                            fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
+                                  max5(v[15], v[16], v[17], v[18], v[19])));
       }
-      if (wi == 0) brv_small<1, 0>(wv, v);
-      else if (wi == 1) brv_small<1, 1>(wv, v);
-      else brv_small<2, 2>(wv, v);
     } else {
       const int h = 1 << (wi - 1);  // ahead = behind = width / 2 (the launcher checks)
-      const float4* pa = reinterpret_cast<const float4*>(tile + 5 * k0 + offset + h);
-      const float4* pb = reinterpret_cast<const float4*>(tile + 5 * k0 + offset - h);
+      const float* ta = tile + offset + h;
+      const float* tb = tile + offset - h;
+      for (int q = lane; q < nq; q += 32) {
+        const float4* pa = reinterpret_cast<const float4*>(ta + 20 * q);
+        const float4* pb = reinterpret_cast<const float4*>(tb + 20 * q);
+        float v[20];
 #pragma unroll
-      for (int r = 0; r < 5; r++) {
-        const float4 a = pa[r], b = pb[r];
-        v[4 * r] = fabsf(__fsub_rn(a.x, b.x));
-        v[4 * r + 1] = fabsf(__fsub_rn(a.y, b.y));
-        v[4 * r + 2] = fabsf(__fsub_rn(a.z, b.z));
-        v[4 * r + 3] = fabsf(__fsub_rn(a.w, b.w));
+        for (int r = 0; r < 5; r++) {
+          const float4 a = pa[r], b = pb[r];
+          v[4 * r] = fabsf(__fsub_rn(a.x, b.x));
+          v[4 * r + 1] = fabsf(__fsub_rn(a.y, b.y));
+          v[4 * r + 2] = fabsf(__fsub_rn(a.z, b.z));
+          v[4 * r + 3] = fabsf(__fsub_rn(a.w, b.w));
+        }
+        float4 o;
+        o.x = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+        o.y = brv_med5<MM>(v[5], v[6], v[7], v[8], v[9]);
+        o.z = brv_med5<MM>(v[10], v[11], v[12], v[13], v[14]);
+        o.w = brv_med5<MM>(v[15], v[16], v[17], v[18], v[19]);
+        *reinterpret_cast<float4*>(la_w + 4 * q) = o;
+        if (rec)
+          srun_w[q] = fmaxf(fmaxf(max5(v[0], v[1], v[2], v[3], v[4]), max5(v[5], v[6], v[7], v[8], v[9])),
+                            fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
+                                  max5(v[15], v[16], v[17], v[18], v[19])));
       }
     }
-    float4 o;
-    o.x = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
-    o.y = brv_med5<MM>(v[5], v[6], v[7], v[8], v[9]);
-    o.z = brv_med5<MM>(v[10], v[11], v[12], v[13], v[14]);
-    o.w = brv_med5<MM>(v[15], v[16], v[17], v[18], v[19]);
-    *reinterpret_cast<float4*>(la + wl * n1p + k0) = o;
-    if (rec)
-      srun[wl * rp + k0 / 4] =
-          fmaxf(fmaxf(max5(v[0], v[1], v[2], v[3], v[4]), max5(v[5], v[6], v[7], v[8], v[9])),
-                fmaxf(max5(v[10], v[11], v[12], v[13], v[14]),
-                      max5(v[15], v[16], v[17], v[18], v[19])));
-  }
-  if constexpr (rem > 0)
-    for (int item = threadIdx.x; item < nwb * rem; item += blockDim.x) {
-      const int wl = item / rem, k = 4 * nq + (item - wl * rem);
-      const WidthInfo& w = ctx.winfo[w0 + wl];
-      const int a = offset + w.ahead, b = offset - w.behind;
-      float v[5];
+    if constexpr (rem > 0)
+      if (lane < rem) {
+        const int k = 4 * nq + lane;
+        const WidthInfo& w = ctx.winfo[wi];
+        const int a = offset + w.ahead, b = offset - w.behind;
+        float v[5];
 #pragma unroll
-      for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
-      la[wl * n1p + k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
-      if (rec) srun[wl * rp + nq + (k - 4 * nq)] = max5(v[0], v[1], v[2], v[3], v[4]);
-    }
-  __syncthreads();
+        for (int r = 0; r < 5; r++) v[r] = fabsf(__fsub_rn(tile[5 * k + r + a], tile[5 * k + r + b]));
+        la_w[k] = brv_med5<MM>(v[0], v[1], v[2], v[3], v[4]);
+        if (rec) srun_w[nq + lane] = max5(v[0], v[1], v[2], v[3], v[4]);
+      }
+    __syncwarp();  // the slot's level-1 row and run maxima are complete
 
-  // ---- level 2, block-wide: la -> lb ----
-  if constexpr (M >= 2) {
-    constexpr int n2 = n1 / 5;
-    for (int item = threadIdx.x; item < nwb * n2; item += blockDim.x) {
-      const int wl = item / n2, k = item - wl * n2;
-      const float* c = la + wl * n1p + 5 * k;
-      lb[wl * lbp + k] = brv_med5<MM>(c[0], c[1], c[2], c[3], c[4]);
-    }
-    __syncthreads();
-  }
-
-  // ---- the group maxima and levels 3..M: one warp per width slot ----
-  const int lane = threadIdx.x & 31;
-  for (int wl = threadIdx.x >> 5; wl < nwb; wl += blockDim.x >> 5) {
     if (rec) {
       // values are non-negative or NaN, so their bit patterns order as
       // unsigned (a NaN maximum only ever keeps a tile from being skipped);
@@ -895,18 +899,19 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
       // is then left out of a maximum that decides a skip: a NaN boxcar never
       // passes the test
       unsigned mk = 0;
-      for (int q = lane; q < nq + rem; q += 32) mk = max(mk, __float_as_uint(srun[wl * rp + q]));
+      for (int q = lane; q < nq + rem; q += 32) mk = max(mk, __float_as_uint(srun_w[q]));
       mk = __reduce_max_sync(0xffffffffu, mk);
       if (lane == 0) ctx.gmax[(ser * nwb + wl) * ctx.ngroups + g] = __uint_as_float(mk);
     }
-    float* rows[2] = {lb + wl * lbp, la + wl * n1p};  // level 2's output is in lb
-    int n = M >= 2 ? n1 / 5 : n1;
-    const float* cur = M >= 2 ? rows[0] : la + wl * n1p;
+
+    // ---- levels 2..M: rows alternate between the slot's lb and la rows ----
+    float* rows[2] = {lb + wl * lbp, la_w};
+    const float* cur = la_w;
+    int n = n1;
 #pragma unroll
-    for (int lev = 3; lev <= M; lev++) {
-      float* nxt = rows[(lev - 2) & 1];
+    for (int lev = 2; lev <= M; lev++) {
+      float* nxt = rows[lev & 1 ? 1 : 0];
       const int nn = n / 5;
-      // inputs and outputs alternate between the slot's lb and la rows
       for (int k = lane; k < nn; k += 32) {
         const float* c = cur + 5 * k;
         nxt[k] = brv_med5<MM>(c[0], c[1], c[2], c[3], c[4]);
@@ -917,6 +922,7 @@ __device__ void brv_levels(const WidthCtx& ctx, const float* tile, int offset, i
     }
     // n == 1: one value per width
     if (lane == 0) out[(ser * nwb + wl) * out_pitch + g] = cur[0];
+    __syncwarp();  // the rows are free for the slot's next use
   }
 }
 
@@ -1073,7 +1079,8 @@ cudaError_t block_rms(WidthCtx& ctx, const WidthInfo* hw, int w_begin, int w_end
       // about 8 consecutive groups per block, spread evenly
       const size_t nblk_x = (ng1 + 7) / 8;
       const size_t gpb = (ng1 + nblk_x - 1) / nblk_x;
-      kern<<<dim3((unsigned)((ng1 + gpb - 1) / gpb), ctx.nser), BRV_THREADS, smem, s>>>(
+      const unsigned nthreads = 32u * (unsigned)std::min(nwb, BRV_THREADS / 32);
+      kern<<<dim3((unsigned)((ng1 + gpb - 1) / gpb), ctx.nser), nthreads, smem, s>>>(
           ctx, w_begin, nwb, (int)win, ws.a, ng1, (int)ng1, (int)gpb); note_launch();
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       float* fin;
