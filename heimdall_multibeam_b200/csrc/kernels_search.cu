@@ -2101,15 +2101,6 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
   const int start_best = best;
   const unsigned ftol = (unsigned)min(a.filter_tol, 0x7FFFFFFFull);
   const unsigned dtol = (unsigned)min(a.dm_tol, 0x7FFFFFFFull);
-  // staged giant jj coincident with this thread's giant
-  auto coinc = [&](int jj) {
-    const unsigned sj = s_samp[jj];
-    const int fj = s_f[jj];
-    const unsigned dt = sj > si ? sj - si : si - sj;
-    const unsigned long long tt = a.time_tol << max(fi, fj);
-    return s_beam[jj] == bi && (unsigned long long)dt <= tt && (unsigned)abs(fj - fi) <= ftol &&
-           (unsigned)abs(s_dm[jj] - di) <= dtol;
-  };
   for (int j0 = j_begin; j0 < j_end; j0 += CL_TILE) {
     const int j = j0 + threadIdx.x;
     __syncthreads();
@@ -2124,40 +2115,17 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
     __syncthreads();
     if (i < a.ngiants) {
       const int jn = min(min(CL_TILE, j_end - j0), i - j0);  // only j < i
-      for (int jj = 0; jj < jn; jj++)
-        if (coinc(jj) && s_lab[jj] < best) best = s_lab[jj];
+      for (int jj = 0; jj < jn; jj++) {
+        const unsigned sj = s_samp[jj];
+        const int fj = s_f[jj];
+        const unsigned dt = sj > si ? sj - si : si - sj;
+        const unsigned long long tt = a.time_tol << max(fi, fj);
+        const bool coinc = s_beam[jj] == bi && (unsigned long long)dt <= tt &&
+                           (unsigned)abs(fj - fi) <= ftol &&
+                           (unsigned)abs(s_dm[jj] - di) <= dtol;
+        if (coinc && s_lab[jj] < best) best = s_lab[jj];
+      }
     }
-  }
-  // The block whose chunk holds the tile's first giant also relaxes the
-  // tile's own chains to a fixed point in shared memory (each giant takes the
-  // smallest label among its coincident earlier giants of the tile, round
-  // after round), so chains inside a tile settle in one sweep.  Every label
-  // taken is still that of a giant reachable through coincident giants of
-  // decreasing index, so the sweeps' fixed point does not change.
-  if (j_begin <= i_first && i_first < j_end) {  // uniform
-    __syncthreads();
-    const int t = threadIdx.x;
-    s_samp[t] = si;
-    s_beam[t] = bi;
-    s_f[t] = fi;
-    s_dm[t] = di;
-    s_lab[t] = best;  // 0x7FFFFFFF past the last giant
-    __syncthreads();
-    uint32_t m[CL_TILE / 32] = {};
-    if (i < a.ngiants)
-      for (int jj = 0; jj < t; jj++)
-        if (coinc(jj)) m[jj >> 5] |= 1u << (jj & 31);
-    for (int round = 0; round < CL_TILE; round++) {  // a chain is at most CL_TILE long
-      int nb = s_lab[t];
-#pragma unroll
-      for (int w = 0; w < CL_TILE / 32; w++)
-        for (uint32_t x = m[w]; x; x &= x - 1) nb = min(nb, s_lab[32 * w + __ffs(x) - 1]);
-      const bool ch = nb < s_lab[t];
-      __syncthreads();
-      if (ch) s_lab[t] = nb;
-      if (!__syncthreads_or(ch)) break;
-    }
-    best = s_lab[t];
   }
   if (i < a.ngiants && best < start_best) {
     int old = atomicMin(&gb.label[i], best);
