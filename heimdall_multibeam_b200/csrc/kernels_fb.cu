@@ -38,13 +38,14 @@ cudaError_t raise_smem_limit(const void* func, size_t bytes) {
 // ---------------------------------------------------------------------------
 // TF -> FT byte transpose, 128 samples x 128 channels per block through
 // shared memory.  The tile holds 128 sample rows of 32 channel words; word w
-// of row t sits at column w ^ ((t >> 2) & 31), so the row-wise stores of the
-// load phase and the sample-wise loads of the store phase (lane l reads rows
-// 4l..4l+3 of one column) both hit 32 distinct banks.  A thread turns four
+// of row t sits at column w ^ (((t >> 2) ^ (t & 3)) & 31), so the row-wise
+// stores of the load phase (a warp stores four consecutive rows at once in
+// the 16-byte form) and the sample-wise loads of the store phase (lane l
+// reads rows 4l..4l+3 of one column) all hit 32 distinct banks.  A thread turns four
 // samples x four channels into four output words with byte permutes.  Rows
 // of whole 16-byte words are loaded 16 bytes at a time.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int tp_col(int t, int w) { return w ^ ((t >> 2) & 31); }
+__device__ __forceinline__ int tp_col(int t, int w) { return w ^ (((t >> 2) ^ (t & 3)) & 31); }
 
 __global__ void __launch_bounds__(256) k_transpose_tf_ft(const uint8_t* __restrict__ in,
                                                          size_t nsamps, int nchans,
