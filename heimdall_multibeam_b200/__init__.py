@@ -188,6 +188,8 @@ SYMBOLS = {
     "hd_get_beam_set_candidates": (C.c_int, [_P, _SZ, _P, _SZP]),
     "hd_destroy_beam_set": (None, [_P]),
     "hd_get_launch_count": (C.c_ulonglong, []),
+    "hd_set_graphs": (C.c_int, [_P, C.c_int]),
+    "hd_get_graph_replays": (C.c_ulonglong, [_P]),
     "hd_measure_int_add_rate": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "hd_clean_filterbank_rfi_noalloc": (C.c_int, [_P, _SZ, _SZ, _SZ, _P, _P, C.c_float,
                                                   C.c_float, C.c_float, _SZ, _SZ, _P, _P]),
@@ -420,6 +422,17 @@ class Pipeline:
 
     def max_overlap(self, nbeams: int = 1) -> int:
         return lib().hd_get_max_overlap(self._p, nbeams)
+
+    def set_graphs(self, enable: bool) -> None:
+        """hd_set_graphs: the batched device-resident calls replay each gulp
+        of a shape seen before as one CUDA graph (on by default)."""
+        err = lib().hd_set_graphs(self._p, 1 if enable else 0)
+        if err != HD_NO_ERROR:
+            raise HdError(err, "hd_set_graphs")
+
+    def graph_replays(self) -> int:
+        """hd_get_graph_replays: gulps this pipeline served by a graph replay."""
+        return int(lib().hd_get_graph_replays(self._p))
 
     def execute(self, filterbank: np.ndarray, nbeams: int = 1, first_idx: int = 0,
                 raise_on_error: bool = True, nbits: int = 8) -> Tuple[int, int]:

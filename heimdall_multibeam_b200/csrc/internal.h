@@ -27,6 +27,9 @@ inline cudaError_t dev_malloc(T** p, size_t bytes) {
 // read through hd_get_launch_count).
 void note_launch();
 unsigned long long launch_count();
+// Adds n (may be negative) to the counter: a CUDA graph's kernel nodes are
+// counted when the graph is launched, not when they are captured.
+void add_launches(long long n);
 
 // Raises the dynamic shared-memory limit of kernel `func` on the current
 // device to at least `bytes`.  The limit is a process-wide attribute of the
@@ -311,6 +314,27 @@ cudaError_t merge_groups(const GiantBuffers& gb, int ngiants, int dm_key_gap, co
                          unsigned* root_flag, unsigned* root_off, unsigned* nroots,
                          unsigned* scan_tmp, unsigned long long* gkey, GroupRow* rows,
                          cudaStream_t s);
+
+// Device-count forms of the stages after thresholding, for a gulp captured as
+// a CUDA graph: the totals are device words (*nhits from the hit scan,
+// *ngiants written here), the grids are sized by the capacities hcap and
+// gcap, and every kernel clamps to them.
+// giants_dev: heads over hcap hit slots, their scan (-> *ngiants), giant
+// maxima, begin/end, filter, DM key, peak and index.  scan_tmp needs
+// scan_tmp_words(max(hcap, gcap)) words.
+cudaError_t giants_dev(const WidthCtx& ctx, const HitBuffers& hb, const unsigned* nhits,
+                       unsigned hcap, GiantBuffers& gb, unsigned gcap, unsigned* ngiants,
+                       unsigned* scan_tmp, cudaStream_t s);
+// cluster_merge_dev: unit offsets (unit_off[0..units]), `pairs` pairs of
+// clustering sweeps (flags[2 pairs]: flag 2p + 1 stays 0 when pair p reached
+// the fixed point; later pairs do nothing), then the merge into rows with the
+// group count in *nroots.  geo: 2 device ints.  gkey: 2 gcap words.
+cudaError_t cluster_merge_dev(const ClusterArgs& a, GiantBuffers& gb, unsigned gcap,
+                              const unsigned* ngiants, int units, int dm_key_gap,
+                              unsigned* unit_off, int* geo, unsigned* flags, int pairs,
+                              const float* dm_list, unsigned* root_flag, unsigned* root_off,
+                              unsigned* nroots, unsigned* scan_tmp, unsigned long long* gkey,
+                              GroupRow* rows, cudaStream_t s);
 
 // RFI mask of clean_filterbank_rfi (clean_filterbank_rfi.cu:447-506) from the
 // normalised zero-DM series and its prefix sum.

@@ -20,6 +20,9 @@ namespace hdb {
 static unsigned long long g_launches = 0;
 void note_launch() { __atomic_add_fetch(&g_launches, 1ull, __ATOMIC_RELAXED); }
 unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+void add_launches(long long n) {
+  __atomic_add_fetch(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED);
+}
 
 cudaError_t raise_smem_limit(const void* func, size_t bytes) {
   static std::mutex m;

@@ -1933,28 +1933,38 @@ cudaError_t scan_u32(const unsigned* in, unsigned* out, size_t n, unsigned* tota
 // ===========================================================================
 // Giants (find_giants.cu:194-316, pipeline.cu:755-775)
 // ===========================================================================
-__global__ void k_giant_heads(WidthCtx ctx, HitBuffers hb, unsigned nhits, unsigned* head) {
-  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nhits) return;
-  unsigned sw = hb.sw[k];
+// 1 when hit k (of nhits) starts a giant: the first hit of its (series,
+// width), or one farther than the width's merge distance from the previous.
+__device__ __forceinline__ unsigned giant_head_of(const WidthCtx& ctx, const HitBuffers& hb,
+                                                  size_t k) {
+  const unsigned sw = hb.sw[k];
   unsigned h = 1;
   if (k > 0 && hb.sw[k - 1] == sw) {
     const WidthInfo& w = ctx.winfo[sw % ctx.nw];
     // not_nearby: b > a + max_dist  (find_giants.cu:79-87)
     h = ((unsigned long long)hb.ind[k] > (unsigned long long)hb.ind[k - 1] + w.merge_dist) ? 1u : 0u;
   }
-  head[k] = h;
+  return h;
 }
 
-__global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, GiantBuffers gb) {
-  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_giant_heads(WidthCtx ctx, HitBuffers hb, unsigned nhits, unsigned* head) {
+  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nhits) return;
+  head[k] = giant_head_of(ctx, hb, k);
+}
+
+// Hit k's share of its giant: the first maximum (larger value wins, ties to
+// the smaller hit position), begin, end, filter and DM key.  Giants at or
+// beyond gcap are not written (the device-count form's capacity).
+__device__ __forceinline__ void giant_reduce_at(const WidthCtx& ctx, const HitBuffers& hb,
+                                                size_t k, unsigned nhits, const GiantBuffers& gb,
+                                                unsigned gcap) {
   const bool live = k < nhits;
   const int lane = threadIdx.x & 31;
   unsigned g = 0xFFFFFFFFu;
   unsigned long long key = 0;
   if (live) {
     g = gb.gid[k] + gb.head[k] - 1u;  // inclusive count of heads - 1
-    // first maximum: larger value wins, ties to the smaller hit position
     key = ((unsigned long long)float_key(hb.val[k]) << 32) |
           (unsigned long long)(0xFFFFFFFFu - (unsigned)k);
   }
@@ -1967,7 +1977,7 @@ __global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, Gian
     if (lane + off < 32 && og == g && ok > key) key = ok;
   }
   const unsigned gp = __shfl_up_sync(0xffffffffu, g, 1);
-  if (!live) return;
+  if (!live || g >= gcap) return;
   if (lane == 0 || gp != g) atomicMax(&gb.key[g], key);
   unsigned sw = hb.sw[k];
   const WidthInfo& w = ctx.winfo[sw % ctx.nw];
@@ -1986,15 +1996,26 @@ __global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, Gian
   }
 }
 
-__global__ void k_giant_finish(HitBuffers hb, unsigned ngiants, GiantBuffers gb,
-                               const WidthInfo* winfo, int nw) {
-  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ngiants) return;
+__global__ void k_giant_reduce(WidthCtx ctx, HitBuffers hb, unsigned nhits, GiantBuffers gb) {
+  giant_reduce_at(ctx, hb, (size_t)blockIdx.x * blockDim.x + threadIdx.x, nhits, gb,
+                  0xFFFFFFFFu);
+}
+
+__device__ __forceinline__ void giant_finish_at(const HitBuffers& hb, size_t g,
+                                                const GiantBuffers& gb, const WidthInfo* winfo,
+                                                int nw) {
   unsigned long long key = gb.key[g];
   unsigned k = 0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull);
   const WidthInfo& w = winfo[hb.sw[k] % nw];
   gb.peak[g] = hb.val[k];
   gb.ind[g] = ((unsigned long long)hb.ind[k] + w.rel_off) * (unsigned long long)w.scr;
+}
+
+__global__ void k_giant_finish(HitBuffers hb, unsigned ngiants, GiantBuffers gb,
+                               const WidthInfo* winfo, int nw) {
+  size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngiants) return;
+  giant_finish_at(hb, g, gb, winfo, nw);
 }
 
 __global__ void k_giant_place(GiantBuffers src, unsigned n, int dm_key_gap,
@@ -2064,13 +2085,15 @@ __global__ void k_cluster_init(int* label, int n) {
 // bound over CL_YBLOCKS (at least 128), so every tile's window is spread over
 // about that many blocks: short scans for small windows, and a grid that
 // stays near tiles x CL_YBLOCKS for large ones.
-__global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantBuffers gb,
-                                                           unsigned* changed, int jchunk) {
+// The sweep of block (blockIdx.x, blockIdx.y) over the first n giants.
+__device__ __forceinline__ void cluster_sweep_block(const ClusterArgs& a, const GiantBuffers& gb,
+                                                    const int n, unsigned* changed,
+                                                    const int jchunk) {
   __shared__ unsigned s_samp[CL_TILE], s_beam[CL_TILE];
   __shared__ int s_f[CL_TILE], s_dm[CL_TILE], s_lab[CL_TILE];
   const int i_first = blockIdx.x * CL_TILE;
   const int i = i_first + threadIdx.x;
-  const int i_last = min(i_first + CL_TILE, a.ngiants) - 1;
+  const int i_last = min(i_first + CL_TILE, n) - 1;
   if ((long long)blockIdx.y * jchunk > (long long)i_last) return;  // uniform: past the tile
   // giants are in ascending DM order: the first candidate neighbour is the
   // first giant within dm_tol of the tile's smallest DM
@@ -2091,7 +2114,7 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
   // A giant's beam is computed once, when it is staged.
   unsigned si = 0, bi = 0;
   int fi = 0, di = 0, best = 0x7FFFFFFF;
-  if (i < a.ngiants) {
+  if (i < n) {
     si = (unsigned)gb.ind[i];
     bi = (unsigned)(gb.ind[i] / a.nsamps_beam);
     fi = gb.filter[i];
@@ -2113,7 +2136,7 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
       s_lab[threadIdx.x] = *((volatile int*)&gb.label[j]);
     }
     __syncthreads();
-    if (i < a.ngiants) {
+    if (i < n) {
       const int jn = min(min(CL_TILE, j_end - j0), i - j0);  // only j < i
       for (int jj = 0; jj < jn; jj++) {
         const unsigned sj = s_samp[jj];
@@ -2127,10 +2150,15 @@ __global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantB
       }
     }
   }
-  if (i < a.ngiants && best < start_best) {
+  if (i < n && best < start_best) {
     int old = atomicMin(&gb.label[i], best);
     if (best < old) *changed = 1u;
   }
+}
+
+__global__ void __launch_bounds__(CL_TILE) k_cluster_sweep(ClusterArgs a, GiantBuffers gb,
+                                                           unsigned* changed, int jchunk) {
+  cluster_sweep_block(a, gb, a.ngiants, changed, jchunk);
 }
 
 // Path jumping: lab[i] is reachable from i, so anything reachable from lab[i]
@@ -2247,6 +2275,195 @@ cudaError_t merge_groups(const GiantBuffers& gb, int n, int dm_key_gap, const fl
   // emit for every possible group index; rows beyond nroots are never read
   k_merge_emit<<<(n + 255) / 256, 256, 0, s>>>(gb, dm_key_gap, nroots, gkey, members, dm_list,
                                                rows); note_launch();
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Device-count forms of the giant, clustering and merge stages, for a gulp
+// captured as a CUDA graph.  The hit and giant totals stay in device words
+// that the kernels read; grids are sized by capacities fixed when the graph
+// is captured and every kernel clamps to them.  A total above its capacity
+// is seen by the host after the gulp, which then searches the gulp again on
+// the host-sized path, so a clamped result is never reported.
+// ===========================================================================
+__device__ __forceinline__ unsigned clamp_count(const unsigned* n, unsigned cap) {
+  const unsigned v = *n;
+  return v < cap ? v : cap;
+}
+
+// head[k] for every k < hcap (0 past the hit count, so that a scan over the
+// capacity counts the giants)
+__global__ void k_giant_heads_dev(WidthCtx ctx, HitBuffers hb, const unsigned* nhits,
+                                  unsigned hcap, unsigned* head) {
+  const unsigned n = clamp_count(nhits, hcap);
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < hcap;
+       k += (size_t)gridDim.x * blockDim.x)
+    head[k] = k < n ? giant_head_of(ctx, hb, k) : 0u;
+}
+
+__global__ void k_giant_reduce_dev(WidthCtx ctx, HitBuffers hb, const unsigned* nhits,
+                                   unsigned hcap, GiantBuffers gb, unsigned gcap) {
+  giant_reduce_at(ctx, hb, (size_t)blockIdx.x * blockDim.x + threadIdx.x,
+                  clamp_count(nhits, hcap), gb, gcap);
+}
+
+__global__ void k_giant_finish_dev(HitBuffers hb, const unsigned* ngiants, unsigned gcap,
+                                   GiantBuffers gb, const WidthInfo* winfo, int nw) {
+  const unsigned n = clamp_count(ngiants, gcap);
+  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+       g += (size_t)gridDim.x * blockDim.x)
+    giant_finish_at(hb, g, gb, winfo, nw);
+}
+
+__global__ void k_unit_offsets_dev(const int* __restrict__ dm, const unsigned* ngiants,
+                                   unsigned gcap, int dm_key_gap, int units, unsigned* offs) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u > units) return;
+  const int n = (int)clamp_count(ngiants, gcap);
+  const long long target = (long long)u * dm_key_gap;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = lo + (hi - lo) / 2;
+    if ((long long)dm[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  offs[u] = (unsigned)lo;
+}
+
+// geo[0] = giant count (clamped), geo[1] = the sweep's chunk of earlier
+// giants per block (the host form's rule in cluster_sweep, from the largest
+// unit's giant count)
+__global__ void k_cluster_geom(const unsigned* __restrict__ offs, int units,
+                               const unsigned* ngiants, unsigned gcap, int* geo) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const unsigned n = clamp_count(ngiants, gcap);
+  unsigned max_unit = 0;
+  for (int u = 0; u < units; u++) max_unit = max(max_unit, offs[u + 1] - offs[u]);
+  const long long wmax = (long long)(max_unit > 0 ? max_unit : n) + CL_TILE;
+  long long chunk = (wmax + CL_YBLOCKS - 1) / CL_YBLOCKS;
+  chunk = max(128ll, (chunk + 127) / 128 * 128);
+  geo[0] = (int)n;
+  geo[1] = (int)chunk;
+}
+
+__global__ void k_cluster_init_dev(int* label, const int* geo) {
+  const int n = geo[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    label[i] = i;
+}
+
+// Sweep `which` (0, 1) of pair `pair`: nothing to do once the previous
+// pair's second sweep changed no label (the fixed point is reached).
+__global__ void __launch_bounds__(CL_TILE) k_cluster_sweep_dev(ClusterArgs a, GiantBuffers gb,
+                                                               const int* geo, unsigned* flags,
+                                                               int pair, int which) {
+  if (pair > 0 && *((volatile unsigned*)&flags[2 * pair - 1]) == 0u) return;
+  const int n = geo[0];
+  if ((long long)blockIdx.x * CL_TILE >= (long long)n) return;
+  cluster_sweep_block(a, gb, n, &flags[2 * pair + which], geo[1]);
+}
+
+__global__ void k_cluster_jump_dev(int* label, const int* geo, unsigned* flags, int pair,
+                                   int which) {
+  if (pair > 0 && *((volatile unsigned*)&flags[2 * pair - 1]) == 0u) return;
+  const int n = geo[0];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int l = label[i];
+  const int ll = *((volatile int*)&label[l]);
+  if (ll < l) {
+    atomicMin(&label[i], ll);
+    flags[2 * pair + which] = 1u;
+  }
+}
+
+__global__ void k_root_flags_dev(const int* label, const int* geo, unsigned gcap,
+                                 unsigned* flag) {
+  const int n = geo[0];
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < gcap; i += gridDim.x * blockDim.x)
+    flag[i] = ((int)i < n && label[i] == (int)i) ? 1u : 0u;
+}
+
+__global__ void k_merge_reduce_dev(GiantBuffers gb, const int* geo, const unsigned* root_off,
+                                   unsigned long long* gkey, unsigned long long* members) {
+  const int n = geo[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned g = root_off[gb.label[i]];
+    const unsigned long long key = ((unsigned long long)float_key(gb.peak[i]) << 32) |
+                                   (unsigned long long)(0xFFFFFFFFu - (unsigned)i);
+    atomicMax(&gkey[g], key);
+    atomicAdd(&members[g], 1ull);
+  }
+}
+
+static unsigned grid_for(size_t n, unsigned threads) {
+  return (unsigned)std::max<size_t>(1, std::min<size_t>((n + threads - 1) / threads, 148 * 32));
+}
+
+cudaError_t giants_dev(const WidthCtx& ctx, const HitBuffers& hb, const unsigned* nhits,
+                       unsigned hcap, GiantBuffers& gb, unsigned gcap, unsigned* ngiants,
+                       unsigned* scan_tmp, cudaStream_t s) {
+  k_giant_heads_dev<<<grid_for(hcap, 256), 256, 0, s>>>(ctx, hb, nhits, hcap, gb.head);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = scan_u32(gb.head, gb.gid, hcap, ngiants, scan_tmp, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(gb.key, 0, (size_t)gcap * sizeof(unsigned long long), s)) !=
+      cudaSuccess)
+    return e;
+  // one thread per hit slot: the warp reduction needs whole runs in a warp
+  k_giant_reduce_dev<<<(unsigned)((hcap + 255) / 256), 256, 0, s>>>(ctx, hb, nhits, hcap, gb,
+                                                                     gcap);
+  note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_giant_finish_dev<<<grid_for(gcap, 256), 256, 0, s>>>(hb, ngiants, gcap, gb, ctx.winfo,
+                                                         ctx.nw);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t cluster_merge_dev(const ClusterArgs& a, GiantBuffers& gb, unsigned gcap,
+                              const unsigned* ngiants, int units, int dm_key_gap,
+                              unsigned* unit_off, int* geo, unsigned* flags, int pairs,
+                              const float* dm_list, unsigned* root_flag, unsigned* root_off,
+                              unsigned* nroots, unsigned* scan_tmp, unsigned long long* gkey,
+                              GroupRow* rows, cudaStream_t s) {
+  k_unit_offsets_dev<<<(units + 1 + 127) / 128, 128, 0, s>>>(gb.dm, ngiants, gcap, dm_key_gap,
+                                                             units, unit_off);
+  note_launch();
+  k_cluster_geom<<<1, 32, 0, s>>>(unit_off, units, ngiants, gcap, geo);
+  note_launch();
+  k_cluster_init_dev<<<grid_for(gcap, 256), 256, 0, s>>>(gb.label, geo);
+  note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(flags, 0, 2 * (size_t)pairs * sizeof(unsigned), s)) != cudaSuccess)
+    return e;
+  // the sweep grid of the host form at the capacity: tiles x CL_YBLOCKS
+  // (chunks past a tile's window return at once)
+  const dim3 sgrid((gcap + CL_TILE - 1) / CL_TILE, CL_YBLOCKS);
+  for (int p = 0; p < pairs; p++)
+    for (int w = 0; w < 2; w++) {
+      k_cluster_sweep_dev<<<sgrid, CL_TILE, 0, s>>>(a, gb, geo, flags, p, w);
+      note_launch();
+      k_cluster_jump_dev<<<(gcap + 255) / 256, 256, 0, s>>>(gb.label, geo, flags, p, w);
+      note_launch();
+    }
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_root_flags_dev<<<grid_for(gcap, 256), 256, 0, s>>>(gb.label, geo, gcap, root_flag);
+  note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = scan_u32(root_flag, root_off, gcap, nroots, scan_tmp, s)) != cudaSuccess) return e;
+  unsigned long long* members = gkey + gcap;
+  if ((e = cudaMemsetAsync(gkey, 0, 2 * (size_t)gcap * sizeof(unsigned long long), s)) !=
+      cudaSuccess)
+    return e;
+  k_merge_reduce_dev<<<grid_for(gcap, 256), 256, 0, s>>>(gb, geo, root_off, gkey, members);
+  note_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_merge_emit<<<(gcap + 255) / 256, 256, 0, s>>>(gb, dm_key_gap, nroots, gkey, members,
+                                                    dm_list, rows);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -16,6 +16,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <new>
@@ -114,6 +115,45 @@ struct hd_pipeline_t {
   DevBuf root_flag, root_off, mkey, rows, unit_off;
   DevBuf h_small_dev;
 
+  // Gulps captured as CUDA graphs (hd_execute_beams with device input and
+  // hd_execute_prefetched).  The first gulp of a shape runs on the
+  // host-sized path and fixes the shape's hit and giant capacities and its
+  // number of clustering sweep pairs; later gulps of the shape replay one
+  // graph per set of device buffers.
+  struct GraphShape {
+    std::vector<size_t> key;
+    unsigned hcap = 0, gcap = 0, pairs = 0;
+    bool broken = false;  // capture failed: this shape stays on the host-sized path
+  };
+  struct GraphGulp {
+    std::vector<size_t> key;   // shape key followed by the buffers' addresses and sizes
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;    // kernel nodes per replay
+    bool events = false;       // the stage events are graph nodes
+    unsigned long long used = 0;
+  };
+  std::vector<GraphShape> graph_shapes;
+  std::vector<GraphGulp> graphs;
+  unsigned long long graph_clock = 0;
+  bool use_graphs = true;
+  bool last_graph = false;     // the last gulp ran as a graph replay
+  unsigned long long graph_replays = 0;
+  std::vector<size_t> pending_shape;  // registered once its host-sized gulp succeeds
+  DevBuf geo, gflags;
+  // what the last host-sized gulp saw (sizes a new shape's capacities)
+  unsigned obs_hits = 0, obs_giants = 0, obs_pairs = 0;
+  void drop_graphs(const std::vector<size_t>& shape) {
+    for (size_t i = 0; i < graphs.size();) {
+      const auto& k = graphs[i].key;
+      if (k.size() >= shape.size() && std::equal(shape.begin(), shape.end(), k.begin())) {
+        if (graphs[i].exec) cudaGraphExecDestroy(graphs[i].exec);
+        graphs.erase(graphs.begin() + i);
+      } else {
+        i++;
+      }
+    }
+  }
+
   unsigned* h_small = nullptr;  // pinned host words
 
   std::vector<hd_candidate> cands;                     // all units, unit by unit
@@ -146,6 +186,8 @@ struct hd_pipeline_t {
   }
 
   ~hd_pipeline_t() {
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
     if (plan) dedisp_destroy_plan(plan);
     for (auto& e : ev) if (e) cudaEventDestroy(e);
     for (auto& e : chunk_ev) if (e) cudaEventDestroy(e);
@@ -305,6 +347,8 @@ hd_error hd_create_pipeline(hd_pipeline* pipeline_, hd_params params) {
   cudaError_t ce = cudaSetDevice(params.gpu_id);
   if (ce != cudaSuccess) { delete pl; return cuda_err(ce); }
   pl->device = params.gpu_id;
+  if (const char* g = std::getenv("HDB_NO_GRAPH"))
+    if (g[0] == '1') pl->use_graphs = false;
   if (cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&pl->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete pl;
@@ -361,10 +405,499 @@ hd_error hd_set_cleaning(hd_pipeline pl, int enable) {
 // every stage runs over all units' DM series at once; giants carry a DM key
 // that keeps units more than dm_tol apart, so clustering never links units
 // and each unit's result equals a separate hd_execute of it.
+// Per-width constants of the boxcar loop (pipeline.cu:657-776) for trials
+// searched at scrunch factor scr: nc_s filtered-input samples, stride_s
+// samples per beam, cur_delay the scrunched largest delay.
+static std::vector<hdb::WidthInfo> widths_for(const hd_params& P, size_t scr, size_t nc_s,
+                                              size_t stride_s, size_t cur_delay) {
+  std::vector<hdb::WidthInfo> wi;
+  const size_t Bmax = P.boxcar_max;
+  const size_t rel_bmax = Bmax / scr;
+  const size_t max_nf = nc_s + 1 - rel_bmax;
+  const size_t cur_off = rel_bmax / 2;
+  for (size_t fw = scr; fw <= Bmax; fw *= 2) {
+    hdb::WidthInfo w{};
+    const size_t rel_fw = fw / scr;
+    size_t rel_min_ts = std::max<size_t>(P.min_tscrunch_width / scr, 1);
+    size_t ts = std::max<size_t>(2 * rel_fw / rel_min_ts, 1);
+    w.width = (int)rel_fw;
+    w.ts = (int)ts;
+    w.ahead = (int)((rel_fw - 1) / 2 + 1);
+    w.behind = (int)(rel_fw / 2);
+    w.filter_idx = (int)log2u(fw);
+    w.n = (unsigned)((max_nf - 1) / ts + 1);
+    w.bn = (unsigned)(stride_s - (cur_delay + rel_bmax));
+    w.merge_dist = (unsigned)(P.cand_sep_time * (rel_fw / ts));
+    w.rel_off = (unsigned)(cur_off / ts);
+    w.prev_cover = (int)wi.size() - 1;
+    w.scr = (int)(scr * ts);
+    wi.push_back(w);
+  }
+  return wi;
+}
+
+// Giant-rate bail-out per unit (pipeline.cu:779-787) from each unit's first
+// giant (first[u] .. first[u + 1]): the running count only grows, so it
+// trips exactly when the final count does.
+static void giant_rate_bail_out(hd_pipeline pl, size_t U, size_t nsamps,
+                                const std::vector<unsigned>& first, hd_error* statuses,
+                                std::vector<char>& too_many, bool& any_ok, bool& any_too_many) {
+  const hd_params& P = pl->params;
+  too_many.assign(U, 0);
+  any_ok = any_too_many = false;
+  float mins = (float)((double)((float)nsamps * P.dt) / 60.0);
+  for (size_t u = 0; u < U; u++) {
+    unsigned gu = first[u + 1] - first[u];
+    if (P.max_giant_rate != 0.0f && ((float)gu / mins > P.max_giant_rate)) too_many[u] = 1;
+    if (too_many[u]) any_too_many = true;
+    else any_ok = true;
+    if (statuses && too_many[u]) statuses[u] = HD_TOO_MANY_EVENTS;
+  }
+}
+
+// Merged candidate rows -> each unit's candidates and .cand file
+// (pipeline.cu:1012-1039).
+static void emit_candidates(hd_pipeline pl, size_t U, const hdb::GroupRow* rows,
+                            unsigned ngroups, const std::vector<char>& too_many, size_t nsamps,
+                            size_t nbeams, size_t first_idx, const hd_size* beams,
+                            size_t nsamps_processed) {
+  const hd_params& P = pl->params;
+  const unsigned nsamps_beam = (unsigned)(nsamps / nbeams);
+  const unsigned nsamps_valid = (unsigned)(nsamps_processed / nbeams);
+  for (unsigned i = 0; i < ngroups; i++) {
+    const hdb::GroupRow& r = rows[i];
+    const size_t u = (size_t)r.unit;
+    if (u >= U || too_many[u]) continue;
+    const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
+    size_t ind = (size_t)r.ind;
+    size_t beam_idx = (size_t)std::floor((float)ind / (float)nsamps_beam);
+    size_t beam_start = beam_idx * nsamps_beam + (P.boxcar_max / 2);
+    size_t beam_end = beam_start + nsamps_valid;
+    if (!(beam_start <= ind && ind < beam_end)) continue;
+    hd_candidate c;
+    size_t samp_off = ind - (size_t)nsamps_beam * beam_idx;
+    c.samp_idx = first_idx + samp_off;
+    c.snr = std::isinf(r.peak) ? 0.0f : r.peak;
+    c.time = P.dt * (float)c.samp_idx;
+    c.filter = (hd_size)r.filter;
+    c.dm_trial = (hd_size)r.dm_ind;
+    c.dm = r.dm;
+    c.members = (hd_size)r.members;
+    c.begin = first_idx + ((size_t)r.begin % nsamps_beam);
+    c.end = first_idx + ((size_t)r.end % nsamps_beam);
+    c.beam = beam_base + beam_idx + 1;
+    pl->unit_cands[u].push_back(c);
+    pl->unit_meta[u].push_back({(unsigned)u, (unsigned)ind, (int)r.dm_ind, (int)r.filter});
+  }
+  for (size_t u = 0; u < U; u++) {
+    const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
+    write_cand_file(pl, pl->unit_cands[u], beam_base, first_idx);
+    pl->cands.insert(pl->cands.end(), pl->unit_cands[u].begin(), pl->unit_cands[u].end());
+    pl->meta.insert(pl->meta.end(), pl->unit_meta[u].begin(), pl->unit_meta[u].end());
+  }
+}
+
+// ---- the gulp as a CUDA graph -------------------------------------------------
+// Capture-safe enqueue of one gulp of U device-resident 8-bit filterbanks at
+// native resolution: no host synchronisation, no allocation (every buffer was
+// sized by graph_gulp), hits and giants at the shape's capacities, clustering
+// as `pairs` sweep pairs that stop themselves at the fixed point.
+struct GulpGeom {
+  size_t U, nsamps, nbeams, C, D, max_delay, dm_tol, gap, nc, fb_bytes, pitch, ft_unit,
+      dd_pitch, NS, stride, bcount, scan_pitch, nsmooth, nsw, gcap_groups;
+  unsigned ntiles;
+};
+
+// With `events`, the stage boundaries of hd_get_timing are recorded by event
+// nodes of the graph (the events of the host-sized path, at the same points).
+static hd_error enqueue_gulp(hd_pipeline pl, const hd_byte* const* fbs, bool resident,
+                             const GulpGeom& g, const std::vector<hdb::WidthInfo>& wi,
+                             unsigned hcap, unsigned gcap, unsigned pairs, bool events) {
+  const hd_params& P = pl->params;
+  dedisp_plan plan = pl->plan;
+  cudaStream_t s = pl->stream;
+  auto mark = [&](int k) {
+    return events ? cudaEventRecordWithFlags(pl->ev[k], s, cudaEventRecordExternal)
+                  : cudaSuccess;
+  };
+  HD_TRY(cudaMemsetAsync(plan->d_err, 0, sizeof(unsigned), s));
+  if (!resident)
+    for (size_t u = 0; u < g.U; u++)
+      HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * g.fb_bytes, fbs[u], g.fb_bytes,
+                             cudaMemcpyDeviceToDevice, s));
+  HD_TRY(mark(1));
+  if (pl->cleaning) {
+    hd_error he = clean_units(pl, g.U, pl->fb_tf.as<uint8_t>(), g.nsamps, g.C, P.dt,
+                              P.baseline_length, P.rfi_tol, 64, g.nbeams,
+                              pl->fb_ft.as<uint8_t>(), g.pitch, nullptr);
+    if (he != HD_NO_ERROR) return he;
+  } else {
+    HD_TRY(hdb::input_to_ft(pl->fb_tf.as<uint8_t>(), g.nsamps, (int)g.C, 8,
+                            pl->fb_ft.as<uint8_t>(), g.pitch, s, g.U, g.ft_unit));
+  }
+  HD_TRY(mark(2));
+  float* dd = pl->dd.as<float>();
+  dedisp_error de = hdb::plan_dedisperse_ft(plan, pl->fb_ft.as<uint8_t>(), g.pitch, g.nsamps, dd,
+                                            g.dd_pitch, s, g.U, g.ft_unit, g.D * g.dd_pitch);
+  if (de != DEDISP_NO_ERROR) return dedisp_err(de);
+  HD_TRY(cudaMemset2DAsync(dd + g.nc, g.dd_pitch * sizeof(float), 0, sizeof(float), g.NS, s));
+  HD_TRY(mark(3));
+
+  hdb::SeriesBatch sb{dd, g.dd_pitch, (int)g.NS, g.nc, g.stride, g.bcount, (int)g.nbeams};
+  hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
+  float* scan = pl->scan.as<float>();
+  HD_TRY(hdb::remove_baseline(sb, g.nsmooth, pl->base.as<float>(), ws, s));
+  HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
+  HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan, g.scan_pitch, nullptr, s, plan->d_err));
+  HD_TRY(mark(4));
+
+  const int nw = (int)wi.size();
+  hdb::WidthCtx wctx{};
+  wctx.scan = scan;
+  wctx.scan_pitch = g.scan_pitch;
+  wctx.nser = (int)g.NS;
+  wctx.stride = g.stride;
+  wctx.nbeams = (int)g.nbeams;
+  wctx.offset = (int)(P.boxcar_max / 2);
+  wctx.nw = nw;
+  wctx.winfo = pl->winfo.as<hdb::WidthInfo>();
+  wctx.host_winfo = wi.data();
+  wctx.scan_len = g.nc + 1;
+  wctx.dms_per_unit = (int)g.D;
+  wctx.dm_key_gap = (int)g.gap;
+  wctx.dm_offset = 0;
+  wctx.norm = pl->norm.as<float>();
+  wctx.thresh = P.detect_thresh;
+  wctx.gmax = pl->gmax.as<float>();
+  wctx.gmax_cap = g.gcap_groups;
+  int n_ts1 = 0;
+  while (n_ts1 < nw && wi[n_ts1].ts == 1) n_ts1++;
+  if (n_ts1 > 0) HD_TRY(hdb::block_rms(wctx, wi.data(), 0, n_ts1, ws, s));
+  for (int w = n_ts1; w < nw; w++) HD_TRY(hdb::block_rms(wctx, wi.data(), w, w + 1, ws, s));
+
+  hdb::HitBuffers hb{};
+  hb.tile_list = pl->tile_list.as<unsigned>();
+  hb.tile_list_n = hb.tile_list + g.NS * g.ntiles;
+  hb.tile_cnt = pl->tile_cnt.as<unsigned>();
+  hb.tile_off = pl->tile_off.as<unsigned>();
+  hb.sw_cnt = pl->sw_cnt.as<unsigned>();
+  hb.sw_off = pl->sw_off.as<unsigned>();
+  HD_TRY(hdb::count_hits(wctx, hb, g.ntiles, s));
+  HD_TRY(hdb::scan_hit_counts(wctx, hb, s));
+  unsigned* small = pl->small.as<unsigned>();
+  unsigned* scan_tmp = pl->scan_tmp.as<unsigned>();
+  HD_TRY(hdb::scan_u32(hb.sw_cnt, hb.sw_off, g.nsw, small, scan_tmp, s));
+  hb.ind = pl->hit_ind.as<unsigned>();
+  hb.val = pl->hit_val.as<float>();
+  hb.sw = pl->hit_sw.as<unsigned>();
+  hb.cap = hcap;
+  HD_TRY(hdb::write_hits(wctx, hb, s));
+  HD_TRY(mark(5));
+
+  hdb::GiantBuffers gb{};
+  pl->main_giants.view(gb);
+  gb.head = pl->head.as<unsigned>();
+  gb.gid = pl->gid.as<unsigned>();
+  gb.cap = gcap;
+  HD_TRY(hdb::giants_dev(wctx, hb, small, hcap, gb, gcap, small + 1, scan_tmp, s));
+  HD_TRY(mark(6));
+  hdb::ClusterArgs ca{0, P.cand_sep_time, P.cand_sep_filter, g.dm_tol,
+                      (unsigned long long)(g.nsamps / g.nbeams), 0};
+  HD_TRY(hdb::cluster_merge_dev(ca, gb, gcap, small + 1, (int)g.U, (int)g.gap,
+                                pl->unit_off.as<unsigned>(), pl->geo.as<int>(), small + 32,
+                                (int)pairs, plan->d_dm_list, pl->root_flag.as<unsigned>(),
+                                pl->root_off.as<unsigned>(), small + 16, scan_tmp,
+                                pl->mkey.as<unsigned long long>(), pl->rows.as<hdb::GroupRow>(),
+                                s));
+  return HD_NO_ERROR;
+}
+
+// Capacity for a total first seen as n: room for 4x as many, at least `floor`.
+static unsigned graph_capacity(unsigned n, unsigned floor) {
+  const unsigned long long c = std::max<unsigned long long>(4ull * n + 1024, floor);
+  return (unsigned)std::min<unsigned long long>((c + 1023) / 1024 * 1024, 0x7FFFF000ull);
+}
+
+// One gulp as a CUDA graph replay.  Returns false when the host-sized path is
+// to search this gulp instead: a shape seen for the first time (that search
+// sizes the shape's capacities), a gulp with nothing to search, a failed
+// capture, or a replay whose totals overflowed the capacities or whose
+// clustering needed more sweeps than were captured (the capacities grow for
+// the next gulp of the shape, and no clamped result is reported).  Returns
+// true with *result set when the graph's results stand or a CUDA call failed.
+static bool graph_gulp(hd_pipeline pl, const hd_byte* const* fbs, size_t U, bool resident,
+                       size_t nsamps, size_t nbeams, size_t first_idx, const hd_size* beams,
+                       hd_error* statuses, size_t nsamps_processed, hd_error* result) {
+  const hd_params& P = pl->params;
+  dedisp_plan plan = pl->plan;
+  GulpGeom g{};
+  g.U = U;
+  g.nsamps = nsamps;
+  g.nbeams = nbeams;
+  g.C = P.nchans;
+  g.D = plan->dm_list.size();
+  g.max_delay = plan->max_delay;
+  g.stride = nsamps / nbeams;
+  const size_t Bmax = P.boxcar_max;
+  if (g.max_delay >= g.stride || g.max_delay + Bmax > g.stride) return false;
+  bool withhold = false;
+  if (const char* e = std::getenv("HDB_TEST_WITHHOLD_STAGE")) withhold = e[0] == '1';
+  const std::vector<size_t> shape = {U, nsamps, nbeams, g.C, g.D, g.max_delay,
+                                     (size_t)pl->cleaning, (size_t)resident,
+                                     (size_t)plan->forced_dm_block,
+                                     (size_t)plan->forced_time_block, (size_t)plan->tune,
+                                     (size_t)withhold, (size_t)plan->gen};
+  hd_pipeline_t::GraphShape* gs = nullptr;
+  for (auto& x : pl->graph_shapes)
+    if (x.key == shape) gs = &x;
+  if (!gs) {
+    pl->pending_shape = shape;
+    return false;
+  }
+  if (gs->broken) return false;
+  const unsigned hcap = gs->hcap, gcap = gs->gcap, pairs = gs->pairs;
+
+  g.dm_tol = std::min<size_t>(P.cand_sep_dm, g.D);
+  g.gap = g.D + g.dm_tol + 2;
+  g.nc = nsamps - g.max_delay;
+  g.fb_bytes = nsamps * g.C;
+  g.pitch = hdb::ft_pitch(plan, nsamps);
+  g.ft_unit = g.pitch * g.C;
+  g.dd_pitch = round_up(g.nc + 1, 4);
+  g.NS = U * g.D;
+  g.bcount = g.stride - g.max_delay;
+  g.scan_pitch = round_up(g.nc + 1, 4);
+  g.nsmooth = (size_t)(P.baseline_length / (2 * P.dt));
+  const std::vector<hdb::WidthInfo> wi = widths_for(P, 1, g.nc, g.stride, g.max_delay);
+  if (wi.empty()) return false;
+  const size_t nw = wi.size();
+  g.ntiles = (unsigned)((wi[0].n + 2047) / 2048);
+  g.nsw = g.NS * nw;
+  g.gcap_groups = g.NS * nw * (nbeams * g.stride / 3125 + 5);
+
+  // every buffer at the size the host-sized path gives this shape, with the
+  // hit and giant lists at the capacities
+  cudaError_t ae = cudaSuccess;
+  auto need = [&](DevBuf& b, size_t bytes) {
+    if (ae == cudaSuccess) ae = b.ensure(bytes);
+  };
+  if (!resident) need(pl->fb_tf, U * g.fb_bytes);
+  need(pl->fb_ft, U * g.ft_unit);
+  need(pl->dd, g.NS * g.dd_pitch * sizeof(float));
+  const size_t tcap = std::max({tree_cap(g.NS * nbeams, g.stride),
+                                tree_cap(g.NS * (log2u(Bmax) + 1), nbeams * g.stride),
+                                hdb::baseline_scratch(g.stride, g.nsmooth, g.NS * nbeams)});
+  need(pl->ws_a, tcap * sizeof(float));
+  need(pl->ws_b, tcap * sizeof(float));
+  need(pl->base, (g.NS * nbeams * hdb::baseline_samples(g.stride, g.nsmooth) + 64) *
+                     sizeof(float));
+  need(pl->rms, g.NS * nbeams * sizeof(float) + 64);
+  need(pl->scan, g.NS * g.scan_pitch * sizeof(float));
+  need(pl->small, 64 * sizeof(unsigned));
+  need(pl->winfo, nw * sizeof(hdb::WidthInfo));
+  need(pl->norm, g.NS * nw * sizeof(float));
+  need(pl->gmax, g.gcap_groups * sizeof(float));
+  need(pl->tile_cnt, g.nsw * g.ntiles * sizeof(unsigned));
+  need(pl->tile_off, g.nsw * g.ntiles * sizeof(unsigned));
+  need(pl->sw_cnt, (g.nsw + 1) * sizeof(unsigned));
+  need(pl->sw_off, (g.nsw + 1) * sizeof(unsigned));
+  need(pl->tile_list, (g.NS * g.ntiles + 1) * sizeof(unsigned));
+  const size_t H = (size_t)hcap + 1, G = (size_t)gcap + 1;
+  need(pl->hit_ind, H * sizeof(unsigned));
+  need(pl->hit_val, H * sizeof(float));
+  need(pl->hit_sw, H * sizeof(unsigned));
+  need(pl->head, H * sizeof(unsigned));
+  need(pl->gid, H * sizeof(unsigned));
+  hd_pipeline_t::GiantSet& m = pl->main_giants;
+  need(m.key, G * sizeof(unsigned long long));
+  need(m.peak, G * sizeof(float));
+  need(m.ind, G * sizeof(unsigned long long));
+  need(m.begin, G * sizeof(unsigned long long));
+  need(m.end, G * sizeof(unsigned long long));
+  need(m.filter, G * sizeof(int));
+  need(m.dm, G * sizeof(int));
+  need(m.label, G * sizeof(int));
+  need(pl->scan_tmp,
+       hdb::scan_tmp_words(std::max({g.nsw, (size_t)hcap, (size_t)gcap})) * sizeof(unsigned));
+  need(pl->root_flag, G * sizeof(unsigned));
+  need(pl->root_off, G * sizeof(unsigned));
+  need(pl->mkey, 2 * G * sizeof(unsigned long long));
+  need(pl->rows, G * sizeof(hdb::GroupRow));
+  need(pl->unit_off, (U + 1) * sizeof(unsigned));
+  need(pl->geo, 4 * sizeof(int));
+  if (ae != cudaSuccess) return false;  // the host-sized path reports it
+  const size_t spec = std::min<size_t>(gcap, kSpecRows);
+  if (pl->ensure_rows_host(std::max<size_t>(spec, 1)) != cudaSuccess) return false;
+
+  // the graph's key: the shape, then every device address it uses
+  std::vector<size_t> key = shape;
+  key.push_back(hcap);
+  key.push_back(gcap);
+  key.push_back(pairs);
+  for (size_t u = 0; u < U; u++) key.push_back(resident ? 0 : (size_t)fbs[u]);
+  for (const DevBuf* b : {&pl->fb_tf, &pl->fb_ft, &pl->dm0, &pl->dm0_scan, &pl->base, &pl->rms,
+                          &pl->mask, &pl->fmask, &pl->rms0, &pl->dd, &pl->scan, &pl->ws_a,
+                          &pl->ws_b, &pl->winfo, &pl->norm, &pl->gmax, &pl->tile_list,
+                          &pl->tile_cnt, &pl->tile_off, &pl->sw_cnt, &pl->sw_off, &pl->hit_ind,
+                          &pl->hit_val, &pl->hit_sw, &pl->head, &pl->gid, &m.key, &m.peak,
+                          &m.ind, &m.begin, &m.end, &m.filter, &m.dm, &m.label, &pl->scan_tmp,
+                          &pl->small, &pl->root_flag, &pl->root_off, &pl->mkey, &pl->rows,
+                          &pl->unit_off, &pl->geo}) {
+    key.push_back((size_t)b->p);
+    key.push_back(b->cap);
+  }
+  for (const void* q : {(const void*)plan->d_delays, (const void*)plan->d_blk_min[0],
+                        (const void*)plan->d_blk_min[1], (const void*)plan->d_blk_min[2],
+                        (const void*)plan->d_active, (const void*)plan->d_dm_list,
+                        (const void*)plan->d_err})
+    key.push_back((size_t)q);
+
+  cudaStream_t s = pl->stream;
+  hd_pipeline_t::GraphGulp* gg = nullptr;
+  for (auto& x : pl->graphs)
+    if (x.key == key) gg = &x;
+  if (!gg) {
+    hd_pipeline_t::GraphGulp ng;
+    ng.key = key;
+    cudaError_t ce = cudaErrorUnknown;
+    hd_error he = HD_NO_ERROR;
+    // with the stage events first; without them if that capture fails
+    for (int events = 1; events >= 0 && !ng.exec; events--) {
+      const unsigned long long l0 = hdb::launch_count();
+      ce = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      if (ce == cudaSuccess) {
+        he = enqueue_gulp(pl, fbs, resident, g, wi, hcap, gcap, pairs, events != 0);
+        cudaGraph_t graph = nullptr;
+        ce = cudaStreamEndCapture(s, &graph);
+        if (he == HD_NO_ERROR && ce == cudaSuccess && graph)
+          ce = cudaGraphInstantiate(&ng.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+      }
+      ng.launches = (long long)(hdb::launch_count() - l0);
+      hdb::add_launches(-ng.launches);
+      if (!ng.exec) cudaGetLastError();
+      ng.events = events != 0;
+    }
+    if (ce != cudaSuccess || he != HD_NO_ERROR || !ng.exec) {
+      // not capturable here: this shape stays on the host-sized path
+      if (ng.exec) cudaGraphExecDestroy(ng.exec);
+      cudaGetLastError();
+      gs->broken = true;
+      return false;
+    }
+    // a few graphs per pipeline (the prefetched form rotates three input
+    // buffers); the least recently used goes
+    if (pl->graphs.size() >= 6) {
+      size_t old = 0;
+      for (size_t i = 1; i < pl->graphs.size(); i++)
+        if (pl->graphs[i].used < pl->graphs[old].used) old = i;
+      cudaGraphExecDestroy(pl->graphs[old].exec);
+      pl->graphs.erase(pl->graphs.begin() + old);
+    }
+    pl->graphs.push_back(ng);
+    gg = &pl->graphs.back();
+  }
+  gg->used = ++pl->graph_clock;
+
+#define GG_TRY(x)                         \
+  do {                                    \
+    cudaError_t e_ = (x);                 \
+    if (e_ != cudaSuccess) {              \
+      *result = cuda_err(e_);             \
+      return true;                        \
+    }                                     \
+  } while (0)
+  // the width table is the pipeline's (another shape's gulp may have
+  // replaced it since the capture)
+  GG_TRY(cudaMemcpyAsync(pl->winfo.p, wi.data(), nw * sizeof(hdb::WidthInfo),
+                         cudaMemcpyHostToDevice, s));
+  cudaEventRecord(pl->ev[0], s);
+  GG_TRY(cudaGraphLaunch(gg->exec, s));
+  hdb::add_launches(gg->launches);
+  std::vector<unsigned>& first = pl->unit_first;
+  first.assign(U + 1, 0);
+  GG_TRY(cudaMemcpyAsync(pl->h_small, pl->small.p, 64 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                         s));
+  GG_TRY(cudaMemcpyAsync(pl->h_small + 20, plan->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                         s));
+  GG_TRY(cudaMemcpyAsync(first.data(), pl->unit_off.p, (U + 1) * sizeof(unsigned),
+                         cudaMemcpyDeviceToHost, s));
+  GG_TRY(cudaMemcpyAsync(pl->h_rows, pl->rows.p, spec * sizeof(hdb::GroupRow),
+                         cudaMemcpyDeviceToHost, s));
+  cudaEventRecord(pl->ev[7], s);
+  GG_TRY(cudaStreamSynchronize(s));
+  const unsigned nh = pl->h_small[0], ngi = pl->h_small[1];
+  if (nh > hcap || ngi > gcap) {
+    gs->hcap = std::max(hcap, graph_capacity(nh, hcap));
+    gs->gcap = std::max(gcap, graph_capacity(ngi, gcap));
+    pl->drop_graphs(shape);
+    return false;
+  }
+  int conv = -1;
+  for (unsigned p = 0; p < pairs && conv < 0; p++)
+    if (pl->h_small[32 + 2 * p + 1] == 0) conv = (int)p;
+  if (conv < 0) {
+    gs->pairs = std::min(pairs + 2, 16u);
+    if (gs->pairs == pairs) gs->broken = true;
+    pl->drop_graphs(shape);
+    return false;
+  }
+  if (pl->h_small[20]) {
+    *result = HD_INTERNAL_GPU_ERROR;
+    return true;
+  }
+  unsigned ngroups = pl->h_small[16];
+  if (ngroups > spec) {
+    std::vector<hdb::GroupRow> head(pl->h_rows, pl->h_rows + spec);
+    GG_TRY(pl->ensure_rows_host(ngroups));
+    std::copy(head.begin(), head.end(), pl->h_rows);
+    GG_TRY(cudaMemcpyAsync(pl->h_rows + spec, pl->rows.as<hdb::GroupRow>() + spec,
+                           (ngroups - spec) * sizeof(hdb::GroupRow), cudaMemcpyDeviceToHost, s));
+    GG_TRY(cudaStreamSynchronize(s));
+  }
+#undef GG_TRY
+  std::vector<char> too_many;
+  bool any_ok = false, any_too_many = false;
+  giant_rate_bail_out(pl, U, nsamps, first, statuses, too_many, any_ok, any_too_many);
+  if (!any_ok) ngroups = 0;
+  pl->searched = true;
+  pl->last_nsamps = nsamps;
+  pl->last_len = g.nc;
+  pl->last_scan_pitch = g.scan_pitch;
+  pl->last_units = U;
+  pl->last_giants = (any_ok && ngi > 0) ? ngi : 0;
+  pl->last_gap = g.gap;
+  pl->obs_hits = nh;
+  pl->obs_giants = ngi;
+  pl->obs_pairs = (unsigned)conv + 1;
+  emit_candidates(pl, U, pl->h_rows, ngroups, too_many, nsamps, nbeams, first_idx, beams,
+                  nsamps_processed);
+  auto el = [&](int a, int b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pl->ev[a], pl->ev[b]) != cudaSuccess) ms = 0.f;
+    return ms;
+  };
+  pl->timing[0] = el(0, 7);
+  if (gg->events) {
+    pl->timing[7] = el(0, 1);
+    pl->timing[1] = el(1, 2);
+    pl->timing[2] = el(2, 3);
+    pl->timing[3] = el(3, 4);
+    pl->timing[4] = el(4, 5);
+    pl->timing[5] = el(5, 6);
+    pl->timing[6] = el(6, 7);
+  }
+  cudaGetLastError();
+  pl->last_graph = true;
+  pl->graph_replays++;
+  *result = any_too_many ? HD_TOO_MANY_EVENTS : HD_NO_ERROR;
+  return true;
+}
+
 static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t U, bool on_device,
                               hd_size nsamps, hd_size nbits, hd_size first_idx, hd_size nbeams,
                               const hd_size* beams, hd_error* statuses,
-                              hd_size* nsamps_processed) {
+                              hd_size* nsamps_processed, bool graph = false) {
   if (!pl) return HD_INVALID_PIPELINE;
   const bool resident = pl->fb_resident;
   pl->fb_resident = false;
@@ -423,6 +956,18 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   const size_t nc = nsamps - max_delay;  // nsamps_computed
   *nsamps_processed = nsamps - nbeams * (P.boxcar_max + max_delay);
   if (nsamps < nbeams * (P.boxcar_max + max_delay)) *nsamps_processed = 0;
+
+  // the batched forms with device-resident input: a shape seen before runs as
+  // one CUDA graph replay
+  pl->last_graph = false;
+  pl->pending_shape.clear();
+  if (graph && on_device && nbits == 8 && pl->use_graphs && pl->plan->groups.empty() &&
+      !pl->narrow_band) {
+    hd_error ge = HD_NO_ERROR;
+    if (graph_gulp(pl, fbs, U, resident, nsamps, nbeams, first_idx, beams, statuses,
+                   *nsamps_processed, &ge))
+      return ge;
+  }
 
   cudaEventRecord(pl->ev[0], s);
   HD_TRY(cudaMemsetAsync(pl->plan->d_err, 0, sizeof(unsigned), s));
@@ -584,27 +1129,8 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     if (gi == 0) cudaEventRecord(pl->ev[4], s);
 
     // ---- widths (pipeline.cu:657-776 at this group's factor) ------------------
-    wi.clear();
-    const size_t max_nf = nc_s + 1 - rel_bmax;
+    wi = widths_for(P, scr, nc_s, stride_s, cur_delay);
     const size_t cur_off = rel_bmax / 2;
-    for (size_t fw = scr; fw <= Bmax; fw *= 2) {
-      hdb::WidthInfo w{};
-      const size_t rel_fw = fw / scr;
-      size_t rel_min_ts = std::max<size_t>(P.min_tscrunch_width / scr, 1);
-      size_t ts = std::max<size_t>(2 * rel_fw / rel_min_ts, 1);
-      w.width = (int)rel_fw;
-      w.ts = (int)ts;
-      w.ahead = (int)((rel_fw - 1) / 2 + 1);
-      w.behind = (int)(rel_fw / 2);
-      w.filter_idx = (int)log2u(fw);
-      w.n = (unsigned)((max_nf - 1) / ts + 1);
-      w.bn = (unsigned)(stride_s - (cur_delay + rel_bmax));
-      w.merge_dist = (unsigned)(P.cand_sep_time * (rel_fw / ts));
-      w.rel_off = (unsigned)(cur_off / ts);
-      w.prev_cover = (int)wi.size() - 1;
-      w.scr = (int)(scr * ts);
-      wi.push_back(w);
-    }
     const int nw = (int)wi.size();
     if (nw == 0) continue;  // the trials' factor exceeds the widest boxcar
     HD_TRY(pl->winfo.ensure(nw * sizeof(hdb::WidthInfo)));
@@ -773,23 +1299,15 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(cudaStreamSynchronize(s));
   }
 
-  // giant-rate bail-out per unit (pipeline.cu:779-787): the running count
-  // only grows, so it trips exactly when the final count does
-  std::vector<char> too_many(U, 0);
+  std::vector<char> too_many;
   bool any_ok = false, any_too_many = false;
-  {
-    float mins = (float)((double)((float)nsamps * P.dt) / 60.0);
-    for (size_t u = 0; u < U; u++) {
-      unsigned gu = first[u + 1] - first[u];
-      if (P.max_giant_rate != 0.0f && ((float)gu / mins > P.max_giant_rate)) too_many[u] = 1;
-      if (too_many[u]) any_too_many = true;
-      else any_ok = true;
-      if (statuses && too_many[u]) statuses[u] = HD_TOO_MANY_EVENTS;
-    }
-  }
+  giant_rate_bail_out(pl, U, nsamps, first, statuses, too_many, any_ok, any_too_many);
 
   unsigned ngroups = 0;
   std::vector<hdb::GroupRow> rows;
+  pl->obs_hits = nhits;
+  pl->obs_giants = ngiants;
+  pl->obs_pairs = 0;
   if (any_ok && ngiants > 0) {
     // ---- clustering ----------------------------------------------------------
     HD_TRY(hdb::cluster_init(gb, (int)ngiants, s));
@@ -804,6 +1322,7 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     // that confirms the fixed point)
     unsigned* changed = pl->small.as<unsigned>() + 8;
     for (unsigned it = 0; it <= ngiants; it += 2) {
+      pl->obs_pairs++;
       HD_TRY(cudaMemsetAsync(changed, 0, 2 * sizeof(unsigned), s));
       HD_TRY(hdb::cluster_sweep(ca, gb, changed, s));
       HD_TRY(hdb::cluster_sweep(ca, gb, changed + 1, s));
@@ -855,40 +1374,8 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
   pl->last_gap = gap;
   if (pl->h_small[17]) return HD_INTERNAL_GPU_ERROR;
 
-  // ---- candidate rows (pipeline.cu:1012-1039), split by unit -------------------
-  const unsigned nsamps_beam = (unsigned)(nsamps / nbeams);
-  const unsigned nsamps_valid = (unsigned)(*nsamps_processed / nbeams);
-  for (unsigned i = 0; i < ngroups; i++) {
-    const hdb::GroupRow& r = rows[i];
-    const size_t u = (size_t)r.unit;
-    if (u >= U || too_many[u]) continue;
-    const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
-    size_t ind = (size_t)r.ind;
-    size_t beam_idx = (size_t)std::floor((float)ind / (float)nsamps_beam);
-    size_t beam_start = beam_idx * nsamps_beam + (P.boxcar_max / 2);
-    size_t beam_end = beam_start + nsamps_valid;
-    if (!(beam_start <= ind && ind < beam_end)) continue;
-    hd_candidate c;
-    size_t samp_off = ind - (size_t)nsamps_beam * beam_idx;
-    c.samp_idx = first_idx + samp_off;
-    c.snr = std::isinf(r.peak) ? 0.0f : r.peak;
-    c.time = P.dt * (float)c.samp_idx;
-    c.filter = (hd_size)r.filter;
-    c.dm_trial = (hd_size)r.dm_ind;
-    c.dm = r.dm;
-    c.members = (hd_size)r.members;
-    c.begin = first_idx + ((size_t)r.begin % nsamps_beam);
-    c.end = first_idx + ((size_t)r.end % nsamps_beam);
-    c.beam = beam_base + beam_idx + 1;
-    pl->unit_cands[u].push_back(c);
-    pl->unit_meta[u].push_back({(unsigned)u, (unsigned)ind, (int)r.dm_ind, (int)r.filter});
-  }
-  for (size_t u = 0; u < U; u++) {
-    const size_t beam_base = beams ? (size_t)beams[u] : (size_t)P.beam + u * nbeams;
-    write_cand_file(pl, pl->unit_cands[u], beam_base, first_idx);
-    pl->cands.insert(pl->cands.end(), pl->unit_cands[u].begin(), pl->unit_cands[u].end());
-    pl->meta.insert(pl->meta.end(), pl->unit_meta[u].begin(), pl->unit_meta[u].end());
-  }
+  emit_candidates(pl, U, rows.data(), ngroups, too_many, nsamps, nbeams, first_idx, beams,
+                  *nsamps_processed);
 
   // stage timings
   auto el = [&](int a, int b) {
@@ -906,6 +1393,27 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     pl->timing[5] = el(5, 6);
   }
   pl->timing[6] = el(6, 7);
+  if (!pl->pending_shape.empty()) {
+    // a new shape for the graph form: capacities from what this gulp saw
+    if (pl->graph_shapes.size() >= 64) pl->graph_shapes.erase(pl->graph_shapes.begin());
+    hd_pipeline_t::GraphShape gsh;
+    gsh.key = pl->pending_shape;
+    gsh.hcap = graph_capacity(pl->obs_hits, 1u << 16);
+    gsh.gcap = graph_capacity(pl->obs_giants, 1u << 14);
+    gsh.pairs = std::min(std::max(pl->obs_pairs + 1, 2u), 16u);
+    // HDB_GRAPH_CAPS="hits,giants,pairs" sets a new shape's starting
+    // capacities instead (tests of the overflow and extra-sweep paths)
+    if (const char* c = std::getenv("HDB_GRAPH_CAPS")) {
+      unsigned h = 0, g = 0, q = 0;
+      if (std::sscanf(c, "%u,%u,%u", &h, &g, &q) == 3 && h && g && q && q <= 16) {
+        gsh.hcap = h;
+        gsh.gcap = g;
+        gsh.pairs = q;
+      }
+    }
+    pl->graph_shapes.push_back(gsh);
+    pl->pending_shape.clear();
+  }
   return any_too_many ? HD_TOO_MANY_EVENTS : HD_NO_ERROR;
 }
 
@@ -929,7 +1437,7 @@ hd_error hd_execute_beams(hd_pipeline pl, const hd_byte* const* filterbanks,
                           hd_size first_idx, hd_size nbeams, const hd_size* beams,
                           int on_device, hd_error* statuses, hd_size* nsamps_processed) {
   return execute_units(pl, filterbanks, nfilterbanks, on_device != 0, nsamps, nbits, first_idx,
-                       nbeams, beams, statuses, nsamps_processed);
+                       nbeams, beams, statuses, nsamps_processed, true);
 }
 
 hd_error hd_prefetch_beams(hd_pipeline pl, const hd_byte* const* filterbanks,
@@ -985,12 +1493,26 @@ hd_error hd_execute_prefetched(hd_pipeline pl, hd_size first_idx, hd_size nbeams
   for (size_t u = 0; u < q.units; u++) fbs[u] = pl->fb_tf.as<uint8_t>() + u * fb_bytes;
   pl->fb_resident = true;
   const hd_error e = execute_units(pl, fbs.data(), q.units, true, q.nsamps, 8, first_idx,
-                                   nbeams, beams, statuses, nsamps_processed);
+                                   nbeams, beams, statuses, nsamps_processed, true);
   q.pending = false;
   return e;
 }
 
 unsigned long long hd_get_launch_count(void) { return hdb::launch_count(); }
+
+hd_error hd_set_graphs(hd_pipeline pl, int enable) {
+  if (!pl) return HD_INVALID_PIPELINE;
+  pl->use_graphs = enable != 0;
+  if (!pl->use_graphs) {
+    cudaSetDevice(pl->device);
+    for (auto& g : pl->graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    pl->graphs.clear();
+  }
+  return HD_NO_ERROR;
+}
+
+unsigned long long hd_get_graph_replays(hd_pipeline pl) { return pl ? pl->graph_replays : 0; }
 
 void hd_destroy_pipeline(hd_pipeline pl) {
   if (!pl) return;

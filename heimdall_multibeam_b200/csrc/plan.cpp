@@ -222,6 +222,7 @@ dedisp_error plan_prepare(dedisp_plan p) {
   if (ge != DEDISP_NO_ERROR) return ge;
   p->device = dev;
   p->dirty = false;
+  p->gen++;
   return DEDISP_NO_ERROR;
 }
 

@@ -26,6 +26,7 @@ struct dedisp_plan_struct {
 
   // derived / device state (rebuilt lazily when the list or killmask change)
   bool dirty = true;
+  unsigned long long gen = 0;      // counts the rebuilds of the device tables
   std::vector<int> delays;         // [dm][chan]
   // per DM-block size (8, 16, 32 trials): [dm block][chan] minimum delay
   std::vector<int> blk_min[3];

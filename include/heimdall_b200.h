@@ -23,7 +23,7 @@
  * hd_execute_device, hd_execute_beams, hd_get_candidates,
  * hd_get_beam_candidates, hd_get_raw_candidates, hd_get_giants, hd_get_timing,
  * hd_get_dedisp_tile, hd_get_dedisp_tile_source, hd_get_launch_count, hd_measure_int_add_rate,
- * hd_clean_filterbank_rfi_noalloc;
+ * hd_clean_filterbank_rfi_noalloc, hd_set_graphs, hd_get_graph_replays;
  * beam sets (hd_*_beam_set*); sigproc input and the gulp loop
  * (hd_read_sigproc_header, hd_mjd_to_utc, hd_params_from_sigproc,
  * hd_search_sigproc_file, hd_search_sigproc_files); the coincidencer (hd_coincide,
@@ -413,8 +413,27 @@ hd_error hd_get_dedisp_tile(hd_pipeline pipeline, int* dm_block, int* time_block
  * 3 read from the tile cache; -1 for a null pipeline. */
 int hd_get_dedisp_tile_source(hd_pipeline pipeline);
 
-/* Number of kernels this library has launched in this process. */
+/* Number of kernels this library has launched in this process (a CUDA
+ * graph's kernels counted at each replay). */
 unsigned long long hd_get_launch_count(void);
+
+/* The batched calls with device-resident input (hd_execute_beams with
+ * on_device != 0, hd_execute_prefetched) run each gulp as one CUDA graph
+ * replay once its shape (filterbank count, spectra, beams, cleaning, DM
+ * trials) has been searched once: the first gulp of a shape runs on the
+ * host-sized path and fixes the shape's hit and giant capacities and its
+ * number of clustering sweeps; later gulps of the shape launch one captured
+ * graph (one per set of input buffers) with every total kept on the device,
+ * and the host reads the results once.  A gulp whose totals exceed the
+ * capacities, or whose clustering needs more sweeps, is searched again on
+ * the host-sized path and the shape's capacities grow: results never depend
+ * on the form.  Adaptive dt, narrow-band zapping and input other than 8-bit
+ * stay on the host-sized path.  hd_set_graphs(p, 0) turns the graph form off
+ * (the environment variable HDB_NO_GRAPH=1 does so for new pipelines);
+ * hd_get_graph_replays counts the gulps it served.  No reference
+ * counterpart (the reference synchronises after every stage). */
+hd_error hd_set_graphs(hd_pipeline pipeline, int enable);
+unsigned long long hd_get_graph_replays(hd_pipeline pipeline);
 
 /* Measured throughput of 32-bit integer adds on `device` (adds per second):
  * independent add chains on every SM, timed with CUDA events (best of three
