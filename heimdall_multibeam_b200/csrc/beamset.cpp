@@ -273,6 +273,11 @@ hd_error hd_execute_beam_set(hd_beam_set s, const hd_byte* const* filterbanks,
           continue;
         }
         hd_set_cleaning(pl, s->cleaning);
+        // one pipeline serves beams of many gulp lengths: each length is a
+        // shape of its own whose graph would be captured, and its buffers
+        // regrown, for every new length, so the set stays on the
+        // host-sized path
+        hd_set_graphs(pl, 0);
         mine.emplace(cfg, pl);
       }
       const size_t U = i1 - i0;
