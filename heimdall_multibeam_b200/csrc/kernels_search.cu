@@ -475,7 +475,7 @@ size_t scan_smem_bytes(int ser, int nbeams, int ch) {
 // spread over more samples and each producer lane has CH / 128 independent
 // float4 values in flight.
 template <int CH>
-__global__ void __launch_bounds__(256, 3) k_normalise_scan(
+__global__ void __launch_bounds__(256) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
     float* norm_out, int ser_per_block, unsigned* err) {
@@ -536,31 +536,15 @@ __global__ void __launch_bounds__(256, 3) k_normalise_scan(
       // ---- the chains: stage k - 1 ----
       if (k >= 1 && k - 1 < nstage && lane < nb) {
         float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * ROW;
-        // batches of 16 samples: the next batch's loads are issued before
-        // this batch's dependent adds, so the chain never waits on shared
-        // memory (the adds stay in sample order)
-        constexpr int BQ = 4;  // float4 per batch
-        float4 v[BQ], nv[BQ];
-#pragma unroll
-        for (int q = 0; q < BQ; q++) v[q] = *reinterpret_cast<const float4*>(row + 4 * q);
-#pragma unroll 2
-        for (int e = 0; e < CH; e += 4 * BQ) {
-          if (e + 4 * BQ < CH) {
-#pragma unroll
-            for (int q = 0; q < BQ; q++)
-              nv[q] = *reinterpret_cast<const float4*>(row + e + 4 * BQ + 4 * q);
-          }
-#pragma unroll
-          for (int q = 0; q < BQ; q++) {
-            float4 o;
-            o.x = sum; sum = __fadd_rn(sum, v[q].x);
-            o.y = sum; sum = __fadd_rn(sum, v[q].y);
-            o.z = sum; sum = __fadd_rn(sum, v[q].z);
-            o.w = sum; sum = __fadd_rn(sum, v[q].w);
-            *reinterpret_cast<float4*>(row + e + 4 * q) = o;
-          }
-#pragma unroll
-          for (int q = 0; q < BQ; q++) v[q] = nv[q];
+#pragma unroll 8
+        for (int e = 0; e < CH; e += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(row + e);
+          float4 o;
+          o.x = sum; sum = __fadd_rn(sum, v.x);
+          o.y = sum; sum = __fadd_rn(sum, v.y);
+          o.z = sum; sum = __fadd_rn(sum, v.z);
+          o.w = sum; sum = __fadd_rn(sum, v.w);
+          *reinterpret_cast<float4*>(row + e) = o;
         }
       }
     } else {
