@@ -174,16 +174,9 @@ size_t baseline_scratch(size_t stride, size_t smooth_radius, size_t nseg);
 // the baseline is subtracted from the series in place.
 cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
                             TreeScratch& ws, cudaStream_t s);
-// The same baseline, fitted but not subtracted: *sub describes it (sub->base
-// stays null when there is none).  rms_beams and normalise_scan given *sub
-// read every sample as x - (stretched baseline), the value remove_baseline
-// would have stored, so the series need not be rewritten.
-cudaError_t fit_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                         TreeScratch& ws, cudaStream_t s, BaselineSub* sub);
 // GetRMSPlanMB::exec_multibeam, vector form (Pipeline/get_rms.cu:236-270):
 // rms[ser*nbeams + b].
-cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s,
-                      const BaselineSub* sub = nullptr);
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s);
 // normalise_multibeam (get_rms.cu:372-382) fused with the exclusive prefix sum
 // of MatchedFilterPlan::prep (matched_filter.cu:21-32), sequential association:
 // scan[ser][0..len] (len + 1 values, pitch scan_pitch).  norm_out (nullable,
@@ -191,7 +184,7 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // err (nullable): bit 1 is set if a staging wait timed out.
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
                            size_t scan_pitch, float* norm_out, cudaStream_t s,
-                           unsigned* err = nullptr, const BaselineSub* sub = nullptr);
+                           unsigned* err = nullptr);
 
 // Per-width constants of the boxcar loop (Pipeline/pipeline.cu:657-776).
 struct WidthInfo {

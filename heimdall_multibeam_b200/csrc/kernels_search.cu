@@ -355,11 +355,6 @@ cudaError_t remove_baseline(const SeriesBatch& sb, size_t smooth_radius, float* 
   return launch_baseline_sub(sb, b, 0, s);
 }
 
-cudaError_t fit_baseline(const SeriesBatch& sb, size_t smooth_radius, float* base_out,
-                         TreeScratch& ws, cudaStream_t s, BaselineSub* sub) {
-  return baseline_prepare(sb, smooth_radius, base_out, ws, s, sub);
-}
-
 // ===========================================================================
 // Robust RMS per beam (Pipeline/get_rms.cu:236-270, reblock_abs_beam 384-418)
 // ===========================================================================
@@ -367,12 +362,9 @@ __device__ __forceinline__ size_t reblock_index(size_t beam, float delta, unsign
   return (size_t)__fadd_rn(__fmul_rn(__ull2float_rn(beam), delta), __uint2float_rn(o));
 }
 
-// With has_sub, a sample is read as x - (stretched baseline), the value
-// k_baseline_sub would have stored (the series themselves stay unsubtracted).
 __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, int nbeams,
                                   size_t beam_count, float delta, int m,
-                                  float* __restrict__ out, size_t out_pitch_beam,
-                                  BaselineSub bsub, int has_sub) {
+                                  float* __restrict__ out, size_t out_pitch_beam) {
   __shared__ float sm[625 + 125];
   const int b = blockIdx.y;
   const size_t ser = blockIdx.z;
@@ -381,9 +373,7 @@ __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, 
   const size_t o0 = (size_t)b * beam_count + g * pow5(m);
   float r = block_tree([&](int i) {
     unsigned o = (unsigned)(o0 + i);
-    const size_t k = reblock_index((size_t)b, delta, o);
-    const float x = d[k];
-    return fabsf(has_sub ? sub_baseline(bsub, ser, (unsigned)k, x) : x);
+    return fabsf(d[reblock_index((size_t)b, delta, o)]);
   }, m, sm);
   if (threadIdx.x == 0) out[(ser * nbeams + b) * out_pitch_beam + g] = r;
 }
@@ -391,18 +381,15 @@ __global__ void k_rms_beams_pass1(const float* __restrict__ data, size_t pitch, 
 __global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitch, size_t count,
                                   int nseg, const float* __restrict__ data, size_t pitch,
                                   int nbeams, size_t beam_count, float delta, int from_data,
-                                  float* __restrict__ rms, BaselineSub bsub, int has_sub) {
+                                  float* __restrict__ rms) {
   int seg = blockIdx.x * blockDim.x + threadIdx.x;
   if (seg >= nseg) return;
   float v[4];
   if (from_data) {
     int ser = seg / nbeams, b = seg % nbeams;
     const float* d = data + (size_t)ser * pitch;
-    for (size_t i = 0; i < count && i < 4; i++) {
-      const size_t k = reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i));
-      const float x = d[k];
-      v[i] = fabsf(has_sub ? sub_baseline(bsub, (size_t)ser, (unsigned)k, x) : x);
-    }
+    for (size_t i = 0; i < count && i < 4; i++)
+      v[i] = fabsf(d[reblock_index((size_t)b, delta, (unsigned)((size_t)b * beam_count + i))]);
   } else {
     for (size_t i = 0; i < count && i < 4; i++) v[i] = lev[(size_t)seg * lev_pitch + i];
   }
@@ -410,10 +397,7 @@ __global__ void k_rms_beams_final(const float* __restrict__ lev, size_t lev_pitc
   rms[seg] = __fmul_rn(m, (float)1.4862);  // multiplies<hd_float>(x, 1.4862)
 }
 
-cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s,
-                      const BaselineSub* sub) {
-  const BaselineSub bsub = (sub && sub->base) ? *sub : BaselineSub();
-  const int has_sub = (sub && sub->base) ? 1 : 0;
+cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaStream_t s) {
   int levels;
   size_t rem;
   tree_levels(sb.beam_count, &levels, &rem);
@@ -422,23 +406,21 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
   cudaError_t e;
   if (levels == 0) {
     k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms,
-        bsub, has_sub); note_launch();
+        nullptr, 0, rem, (int)nseg, sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, 1, rms); note_launch();
     return cudaGetLastError();
   }
   int m1 = levels < 5 ? levels : 5;
   size_t ng1 = sb.beam_count / pow5(m1);
   if (nseg * ng1 > ws.cap) return cudaErrorMemoryAllocation;
   k_rms_beams_pass1<<<seg_grid(ng1, sb.nbeams, sb.nser), TREE_THREADS, 0, s>>>(
-      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1, bsub, has_sub); note_launch();
+      sb.data, sb.pitch, sb.nbeams, sb.beam_count, delta, m1, ws.a, ng1); note_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   float* fin;
   size_t fin_pitch, fin_count;
   e = tree_reduce_array(ws.a, ng1, ng1, nseg, ws, s, &fin, &fin_pitch, &fin_count);
   if (e != cudaSuccess) return e;
   k_rms_beams_final<<<(unsigned)((nseg + 127) / 128), 128, 0, s>>>(
-      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms,
-      bsub, 0); note_launch();
+      fin, fin_pitch, fin_count, (int)nseg, nullptr, 0, sb.nbeams, sb.beam_count, delta, 0, rms); note_launch();
   return cudaGetLastError();
 }
 
@@ -493,10 +475,10 @@ size_t scan_smem_bytes(int ser, int nbeams, int ch) {
 // spread over more samples and each producer lane has CH / 128 independent
 // float4 values in flight.
 template <int CH>
-__global__ void __launch_bounds__(256, 3) k_normalise_scan(
+__global__ void __launch_bounds__(256) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
-    float* norm_out, int ser_per_block, unsigned* err, BaselineSub bsub, int has_sub) {
+    float* norm_out, int ser_per_block, unsigned* err) {
   constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
   constexpr int QN = CH / 128; // float4 per lane per row
   extern __shared__ __align__(128) float sc_smem[];
@@ -614,16 +596,6 @@ __global__ void __launch_bounds__(256, 3) k_normalise_scan(
             for (int q = 0; q < QN; q++) x[q] = *reinterpret_cast<const float4*>(crow + 4 * lane + 128 * q);
 #pragma unroll
             for (int q = 0; q < QN; q++) {
-              if (has_sub) {
-                // the baseline subtraction of remove_baseline, applied as the
-                // sample is read (the same float operations)
-                const size_t ser = (size_t)(s0 + sl);
-                const unsigned i = base + 4u * lane + 128u * q;
-                x[q].x = sub_baseline(bsub, ser, i, x[q].x);
-                x[q].y = sub_baseline(bsub, ser, i + 1, x[q].y);
-                x[q].z = sub_baseline(bsub, ser, i + 2, x[q].z);
-                x[q].w = sub_baseline(bsub, ser, i + 3, x[q].w);
-              }
               x[q].x = div_rn_by(x[q].x, rb, y);
               x[q].y = div_rn_by(x[q].y, rb, y);
               x[q].z = div_rn_by(x[q].z, rb, y);
@@ -647,7 +619,6 @@ __global__ void __launch_bounds__(256, 3) k_normalise_scan(
               for (int j = 0; j < 4; j++) {
                 const unsigned ij = i + j;
                 if (ij >= len) { x[j] = 0.f; continue; }
-                if (has_sub) x[j] = sub_baseline(bsub, (size_t)(s0 + sl), ij, x[j]);
                 unsigned b;
                 if (stride >= (unsigned)CH) b = (ij >= bend && b0 + 1 < (unsigned)nbeams) ? b0 + 1 : b0;
                 else b = min(ij / stride, (unsigned)nbeams - 1);
@@ -685,22 +656,19 @@ __global__ void __launch_bounds__(256, 3) k_normalise_scan(
 template <int CH>
 static cudaError_t launch_scan(const SeriesBatch& sb, const float* rms, float* scan,
                                size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
-                               int ser, const BaselineSub* sub) {
-  const BaselineSub bsub = (sub && sub->base) ? *sub : BaselineSub();
-  const int has_sub = (sub && sub->base) ? 1 : 0;
+                               int ser) {
   const int np = ser < 7 ? ser : 7;
   const size_t smem = scan_smem_bytes(ser, sb.nbeams, CH);
   cudaError_t e = raise_smem_limit(k_normalise_scan<CH>, smem);
   if (e != cudaSuccess) return e;
   k_normalise_scan<CH><<<(unsigned)((sb.nser + ser - 1) / ser), 32 * (np + 1), smem, s>>>(
       sb.data, sb.pitch, sb.nser, (unsigned)sb.len, (unsigned)sb.stride, sb.nbeams, rms, scan,
-      scan_pitch, norm_out, ser, err, bsub, has_sub); note_launch();
+      scan_pitch, norm_out, ser, err); note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
-                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err,
-                           const BaselineSub* sub) {
+                           size_t scan_pitch, float* norm_out, cudaStream_t s, unsigned* err) {
   if (sb.len >= 0xFFFFFF00u || sb.pitch % 4 || scan_pitch % 4 || sb.stride == 0 ||
       sb.pitch < ((sb.len + 3) & ~(size_t)3) || scan_pitch < sb.len + 1 ||
       (reinterpret_cast<uintptr_t>(sb.data) & 15) || (reinterpret_cast<uintptr_t>(scan) & 15) ||
@@ -712,8 +680,8 @@ cudaError_t normalise_scan(const SeriesBatch& sb, const float* rms, float* scan,
   // multibeam gulp, and 4 with 512 beat 2 with 512 on the survey gulp)
   int ser = 8;
   while (ser > 1 && (sb.nser + ser - 1) / ser < 296) ser /= 2;
-  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser, sub);
-  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser, sub);
+  if (ser <= 4) return launch_scan<512>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
+  return launch_scan<256>(sb, rms, scan, scan_pitch, norm_out, s, err, ser);
 }
 
 // ===========================================================================

@@ -546,11 +546,9 @@ static hd_error enqueue_gulp(hd_pipeline pl, const hd_byte* const* fbs, bool res
   hdb::SeriesBatch sb{dd, g.dd_pitch, (int)g.NS, g.nc, g.stride, g.bcount, (int)g.nbeams};
   hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
   float* scan = pl->scan.as<float>();
-  hdb::BaselineSub bsub;
-  HD_TRY(hdb::fit_baseline(sb, g.nsmooth, pl->base.as<float>(), ws, s, &bsub));
-  HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s, &bsub));
-  HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan, g.scan_pitch, nullptr, s, plan->d_err,
-                             &bsub));
+  HD_TRY(hdb::remove_baseline(sb, g.nsmooth, pl->base.as<float>(), ws, s));
+  HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
+  HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan, g.scan_pitch, nullptr, s, plan->d_err));
   HD_TRY(mark(4));
 
   const int nw = (int)wi.size();
@@ -1124,13 +1122,10 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     const float cur_dt = P.dt * (float)scr;
     const size_t nsmooth = (size_t)(P.baseline_length / (2 * cur_dt));
     hdb::TreeScratch ws{pl->ws_a.as<float>(), pl->ws_b.as<float>(), pl->ws_a.cap / sizeof(float)};
-    // the per-DM baseline is fitted, then subtracted as the RMS and the
-    // normalise + scan passes read each sample (the series are not rewritten)
-    hdb::BaselineSub bsub;
-    HD_TRY(hdb::fit_baseline(sb, nsmooth, pl->base.as<float>(), ws, s, &bsub));
-    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s, &bsub));
+    HD_TRY(hdb::remove_baseline(sb, nsmooth, pl->base.as<float>(), ws, s));
+    HD_TRY(hdb::rms_beams(sb, pl->rms.as<float>(), ws, s));
     HD_TRY(hdb::normalise_scan(sb, pl->rms.as<float>(), scan_g, scan_pitch, nullptr, s,
-                               pl->plan->d_err, &bsub));
+                               pl->plan->d_err));
     if (gi == 0) cudaEventRecord(pl->ev[4], s);
 
     // ---- widths (pipeline.cu:657-776 at this group's factor) ------------------
