@@ -4,7 +4,9 @@
   channels x 2^15 samples at 655.36 us, 851 MHz top, DM 0-2000 = 234 trials,
   boxcars to 512, seed 2026), through the batched call: every beam's giants
   (peak bits, index, begin, end, width, DM trial), cluster labels and .cand
-  lines equal the oracle's run of that beam.
+  lines equal the oracle's run of that beam, from host input and from device
+  input in both of the benchmark's forms (host-sized, and the CUDA graph
+  replay of a shape seen before).
 * Beams shaped like the uneven-beam workload, where the dedispersion runs
   long staged rows and many drains: a 4096-channel beam of 2^16 samples, a
   2048-channel beam at DM 4800-5000 (delays near 59 000 samples) and a
@@ -35,11 +37,30 @@ def test_headline_gulp_every_beam_equals_oracle(hdb, oracle_lib):
     beams = synth.make_multibeam(w, seed=2026)
     assert len(beams) == 36
     p = H.default_params(nchans=w.nchans, output_dir=None, **_okw(w))
+    torch = pytest.importorskip("torch")
     with H.Pipeline(p, cleaning=w.clean) as pl:
         err, proc, st = pl.execute_beams([b.data for b in beams])
         assert err == H.HD_NO_ERROR
         g = pl.giants()
         cands = [pl.candidates(u) for u in range(len(beams))]
+        # the benchmark's own call: the 36 filterbanks resident on the device,
+        # the first gulp host-sized, the second a CUDA graph replay; both
+        # equal the host-input call (which the oracle checks below)
+        d = torch.from_numpy(np.stack([b.data for b in beams])).cuda()
+        fb_bytes = w.nsamps * w.nchans
+        ptrs = [d.data_ptr() + u * fb_bytes for u in range(len(beams))]
+        for _ in range(2):
+            err_d, proc_d, st_d = pl.execute_beams(ptrs, nsamps=w.nsamps, on_device=True)
+            assert (err_d, proc_d, st_d) == (err, proc, st)
+            g_d = pl.giants()
+            for k in g:
+                np.testing.assert_array_equal(g_d[k].view(np.uint8), g[k].view(np.uint8),
+                                              err_msg=k)
+            for u in range(len(beams)):
+                assert H.cand_lines(pl.candidates(u)) == H.cand_lines(cands[u]), u
+                np.testing.assert_array_equal(pl.candidates(u)["snr"].view(np.uint32),
+                                              cands[u]["snr"].view(np.uint32))
+        assert pl.graph_replays() == 1
     off = 0
     total = 0
     for u, b in enumerate(beams):
