@@ -431,14 +431,12 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 //
 // The left-to-right float sum of a series is one dependent chain (~4 cycles
 // per sample), so the block is split by role:
-//   one warp     the chains: lane l owns series l of the block and runs its
-//                chain over one stage of its row in shared memory (which
-//                warp is drawn per block so that the chains of the blocks on
-//                one SM run on different schedulers);
-//   the others   the producers: a stage's rows arrive by TMA bulk copies
-//                requested SC_DEPTH stages ahead; these warps divide them in
-//                place by their beam's RMS, and write them out once the chain
-//                warp has replaced them with their prefix sums.
+//   warp 0       the chains: lane l owns series l of the block and runs its
+//                chain over one stage of its row in shared memory;
+//   warps 1..np  a stage's rows arrive by TMA bulk copies requested SC_DEPTH
+//                stages ahead; these warps divide them in place by their
+//                beam's RMS, and write them out once the chain warp has
+//                replaced them with their prefix sums.
 // Stage k lives in buffer k % SC_NB.  At step k the producers normalise stage
 // k and store stage k - 2 while the chain warp scans stage k - 1, and stage
 // k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
@@ -476,9 +474,6 @@ size_t scan_smem_bytes(int ser, int nbeams, int ch) {
 // long stages, so the per-stage fixed cost (barrier, copy issue, waits) is
 // spread over more samples and each producer lane has CH / 128 independent
 // float4 values in flight.
-// Blocks of k_normalise_scan started on each SM (ids below 256), modulo 2^32.
-__device__ unsigned g_scan_ticket[256];
-
 template <int CH>
 __global__ void __launch_bounds__(256) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
@@ -500,16 +495,9 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
   const unsigned nstage = len / CH + 1;     // outputs 0..len
   const unsigned len4 = (len + 3u) & ~3u;   // copies round up to 16 bytes (inside the row pitch)
 
-  // The chain warp of this block: the blocks resident on one SM take tickets
-  // in turn, so their chain warps (a warp's index modulo 4 selects its
-  // scheduler) sit on different schedulers rather than all on the first.
-  __shared__ int s_chain;
   if (threadIdx.x == 0) {
     for (int b = 0; b < SC_NB; b++) mbar_init(&full[b], 1);
     fence_mbar_init();
-    unsigned smid;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-    s_chain = (int)(atomicAdd(&g_scan_ticket[smid & 255u], 1u) % (unsigned)(np + 1));
   }
   if (rms_smem)
     for (int k = threadIdx.x; k < nb * nbeams; k += blockDim.x) {
@@ -518,10 +506,8 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       sy[k] = __frcp_rn(r);
     }
   __syncthreads();
-  const int chain = s_chain;
-  const int p = warp == chain ? -1 : (warp < chain ? warp : warp - 1);  // producer index
 
-  // stage st -> its buffer; producer 0, one row per lane; a stage past the data
+  // stage st -> its buffer; warp 1, one row per lane; a stage past the data
   // completes its barrier phase with a plain arrival
   auto request = [&](unsigned st) {
     uint64_t* bar = &full[st % SC_NB];
@@ -540,13 +526,13 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
       bulk_g2s(rows + ((size_t)(st % SC_NB) * S + lane) * ROW,
                data + (size_t)(s0 + lane) * pitch + base, bytes, bar);
   };
-  if (p == 0)
+  if (warp == 1)
     for (unsigned st = 0; st < (unsigned)SC_DEPTH && st < nstage; st++) request(st);
 
-  float sum = 0.f;     // chain of series s0 + lane (the chain warp)
+  float sum = 0.f;     // chain of series s0 + lane (warp 0)
   bool failed = false;
   for (unsigned k = 0; k < nstage + 2; k++) {
-    if (warp == chain) {
+    if (warp == 0) {
       // ---- the chains: stage k - 1 ----
       if (k >= 1 && k - 1 < nstage && lane < nb) {
         float* row = rows + ((size_t)((k - 1) % SC_NB) * S + lane) * ROW;
@@ -562,7 +548,8 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
         }
       }
     } else {
-      if (p == 0 && k + SC_DEPTH < nstage) request(k + SC_DEPTH);
+      const int p = warp - 1;
+      if (warp == 1 && k + SC_DEPTH < nstage) request(k + SC_DEPTH);
       // ---- store stage k - 2 ----
       if (k >= 2 && k - 2 < nstage) {
         const unsigned st = k - 2;
@@ -661,7 +648,7 @@ __global__ void __launch_bounds__(256) k_normalise_scan(
   }
   // every copy has been waited for at its normalise step; after a timed-out
   // wait, let the buffers' last copies land before the block exits
-  if (failed && p == 0)
+  if (failed && warp == 1)
     for (unsigned st = (nstage > SC_NB ? nstage - SC_NB : 0); st < nstage; st++)
       mbar_wait(&full[st % SC_NB], (st / SC_NB) & 1u, SC_WAIT_LIMIT);
 }
