@@ -240,6 +240,23 @@ unsigned log2u(size_t v) {
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Copies filterbanks u0 .. u1-1 of `bytes` each, from srcs[u] to dst + u *
+// bytes, with one cudaMemcpyAsync per run of sources that lie back to back in
+// memory (one call for a caller's contiguous block of filterbanks).
+cudaError_t copy_units(uint8_t* dst, const hd_byte* const* srcs, size_t u0, size_t u1,
+                       size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+  size_t u = u0;
+  while (u < u1) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(srcs[u]);
+    size_t v = u + 1;
+    while (v < u1 && reinterpret_cast<uintptr_t>(srcs[v]) == a + (v - u) * bytes) v++;
+    const cudaError_t e = cudaMemcpyAsync(dst + u * bytes, srcs[u], (v - u) * bytes, kind, s);
+    if (e != cudaSuccess) return e;
+    u = v;
+  }
+  return cudaSuccess;
+}
+
 // Scratch needed by the median trees of `nseg` segments of `count` values.
 size_t tree_cap(size_t nseg, size_t count) { return nseg * (count / 3125 + 8) + 64; }
 
@@ -522,9 +539,8 @@ static hd_error enqueue_gulp(hd_pipeline pl, const hd_byte* const* fbs, bool res
   };
   HD_TRY(cudaMemsetAsync(plan->d_err, 0, sizeof(unsigned), s));
   if (!resident)
-    for (size_t u = 0; u < g.U; u++)
-      HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * g.fb_bytes, fbs[u], g.fb_bytes,
-                             cudaMemcpyDeviceToDevice, s));
+    HD_TRY(copy_units(pl->fb_tf.as<uint8_t>(), fbs, 0, g.U, g.fb_bytes, cudaMemcpyDeviceToDevice,
+                      s));
   HD_TRY(mark(1));
   if (pl->cleaning) {
     hd_error he = clean_units(pl, g.U, pl->fb_tf.as<uint8_t>(), g.nsamps, g.C, P.dt,
@@ -993,9 +1009,8 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
     HD_TRY(cudaStreamWaitEvent(pl->copy_stream, pl->ev[9], 0));
     for (size_t k = 0; k < nch; k++) {
       const size_t u0 = U * k / nch, u1 = U * (k + 1) / nch;
-      for (size_t u = u0; u < u1; u++)
-        HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes, kind,
-                               pl->copy_stream));
+      HD_TRY(copy_units(pl->fb_tf.as<uint8_t>(), fbs, u0, u1, fb_bytes, kind,
+                        pl->copy_stream));
       HD_TRY(cudaEventRecord(pl->chunk_ev[k], pl->copy_stream));
     }
     HD_TRY(cudaEventRecord(pl->ev[1], pl->copy_stream));
@@ -1012,10 +1027,7 @@ static hd_error execute_units(hd_pipeline pl, const hd_byte* const* fbs, size_t 
       if (de != DEDISP_NO_ERROR) return dedisp_err(de);
     }
   } else {
-    if (!resident)
-      for (size_t u = 0; u < U; u++)
-        HD_TRY(cudaMemcpyAsync(pl->fb_tf.as<uint8_t>() + u * fb_bytes, fbs[u], fb_bytes, kind,
-                               s));
+    if (!resident) HD_TRY(copy_units(pl->fb_tf.as<uint8_t>(), fbs, 0, U, fb_bytes, kind, s));
     cudaEventRecord(pl->ev[1], s);
     if (pl->cleaning) {
       hd_error he = clean_units(pl, U, pl->fb_tf.as<uint8_t>(), nsamps, C, P.dt,
@@ -1461,9 +1473,8 @@ hd_error hd_prefetch_beams(hd_pipeline pl, const hd_byte* const* filterbanks,
   // the slot may still be read by a search queued earlier on the compute stream
   HD_TRY(cudaEventRecord(q.done, pl->stream));
   HD_TRY(cudaStreamWaitEvent(pl->copy_stream, q.done, 0));
-  for (size_t u = 0; u < nfilterbanks; u++)
-    HD_TRY(cudaMemcpyAsync(q.buf.as<uint8_t>() + u * fb_bytes, filterbanks[u], fb_bytes,
-                           cudaMemcpyHostToDevice, pl->copy_stream));
+  HD_TRY(copy_units(q.buf.as<uint8_t>(), filterbanks, 0, nfilterbanks, fb_bytes,
+                    cudaMemcpyHostToDevice, pl->copy_stream));
   HD_TRY(cudaEventRecord(q.done, pl->copy_stream));
   q.pending = true;
   q.tag = ++pl->pf_seq;
