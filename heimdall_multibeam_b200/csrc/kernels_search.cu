@@ -442,7 +442,10 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
 // step k - 1).  One block barrier ends each step.
 // ===========================================================================
-constexpr int SC_DEPTH = 5;          // stages in flight ahead of the one being normalised
+// stages in flight ahead of the one being normalised: 3 (a ring of 6 stage
+// buffers, 50 KB for 8 series of 256 samples) keeps four blocks on an SM; the
+// copies are still requested about 5 us before they are read
+constexpr int SC_DEPTH = 3;
 constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
 constexpr int SC_MAXRMS = 2048;      // series x beams whose RMS stays in shared memory
 constexpr uint32_t SC_WAIT_LIMIT = 1u << 22;
@@ -475,7 +478,7 @@ size_t scan_smem_bytes(int ser, int nbeams, int ch) {
 // spread over more samples and each producer lane has CH / 128 independent
 // float4 values in flight.
 template <int CH>
-__global__ void __launch_bounds__(256) k_normalise_scan(
+__global__ void __launch_bounds__(256, 4) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
     float* norm_out, int ser_per_block, unsigned* err) {
