@@ -442,11 +442,12 @@ cudaError_t rms_beams(const SeriesBatch& sb, float* rms, TreeScratch& ws, cudaSt
 // k + SC_DEPTH is requested into the buffer that held stage k - 3 (stored at
 // step k - 1).  One block barrier ends each step.
 // ===========================================================================
-// stages in flight ahead of the one being normalised: 3 (a ring of 6 stage
-// buffers, 50 KB for 8 series of 256 samples) keeps four blocks on an SM; the
-// copies are still requested about 5 us before they are read
-constexpr int SC_DEPTH = 3;
-constexpr int SC_NB = SC_DEPTH + 3;  // ring of stage buffers
+// Stages in flight ahead of the one being normalised, and the ring of stage
+// buffers (depth + 3).  Stages of 256 samples: depth 3 (a ring of 6, 50 KB for
+// 8 series) keeps four blocks on an SM, with each copy still requested about
+// 5 us before it is read; stages of 512 samples (blocks of few series): 5.
+__host__ __device__ constexpr int sc_depth(int ch) { return ch >= 512 ? 5 : 3; }
+__host__ __device__ constexpr int sc_nb(int ch) { return sc_depth(ch) + 3; }
 constexpr int SC_MAXRMS = 2048;      // series x beams whose RMS stays in shared memory
 constexpr uint32_t SC_WAIT_LIMIT = 1u << 22;
 
@@ -468,7 +469,7 @@ __device__ __forceinline__ float div_rn_by(float a, float b, float y) {
 }
 
 size_t scan_smem_bytes(int ser, int nbeams, int ch) {
-  size_t b = 128 + (size_t)SC_NB * ser * (ch + 4) * sizeof(float);
+  size_t b = 128 + (size_t)sc_nb(ch) * ser * (ch + 4) * sizeof(float);
   if ((size_t)ser * nbeams <= SC_MAXRMS) b += 2 * (size_t)ser * nbeams * sizeof(float);
   return b;
 }
@@ -482,6 +483,8 @@ __global__ void __launch_bounds__(256, 4) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
     float* norm_out, int ser_per_block, unsigned* err) {
+  constexpr int SC_DEPTH = sc_depth(CH);
+  constexpr int SC_NB = sc_nb(CH);
   constexpr int ROW = CH + 4;  // row pitch in floats: lane l's 16 bytes hit banks 4l..4l+3
   constexpr int QN = CH / 128; // float4 per lane per row
   extern __shared__ __align__(128) float sc_smem[];

@@ -23,6 +23,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "heimdall_b200.h"
 #include "internal.h"
 #include "plan.h"
@@ -240,16 +242,51 @@ unsigned log2u(size_t v) {
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// The allocation that contains p (CUDA device or page-locked host memory):
+// false for memory CUDA does not know (pageable host memory), or when the
+// driver's pointer-range query is unavailable.
+bool allocation_range(const void* p, uintptr_t* base, size_t* size) {
+  using Fn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+  static Fn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    cudaGetLastError();
+    return reinterpret_cast<Fn>(f);
+  }();
+  if (!fn) return false;
+  CUdeviceptr b = 0;
+  size_t n = 0;
+  const CUdeviceptr d = (CUdeviceptr) reinterpret_cast<uintptr_t>(p);
+  if (fn(&b, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS ||
+      fn(&n, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS)
+    return false;
+  *base = (uintptr_t)b;
+  *size = n;
+  return true;
+}
+
 // Copies filterbanks u0 .. u1-1 of `bytes` each, from srcs[u] to dst + u *
-// bytes, with one cudaMemcpyAsync per run of sources that lie back to back in
-// memory (one call for a caller's contiguous block of filterbanks).
+// bytes, with one cudaMemcpyAsync per run of sources that lie back to back
+// inside one allocation (one call for a caller's contiguous block of
+// filterbanks).  Page-locked or device buffers that merely sit next to each
+// other are separate allocations, which one copy may not span; pageable host
+// buffers that do are read as plain host memory.
 cudaError_t copy_units(uint8_t* dst, const hd_byte* const* srcs, size_t u0, size_t u1,
                        size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
   size_t u = u0;
   while (u < u1) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(srcs[u]);
+    uintptr_t rb = 0;
+    size_t rn = 0;
+    const bool known = u + 1 < u1 && allocation_range(srcs[u], &rb, &rn);
     size_t v = u + 1;
-    while (v < u1 && reinterpret_cast<uintptr_t>(srcs[v]) == a + (v - u) * bytes) v++;
+    while (v < u1 && reinterpret_cast<uintptr_t>(srcs[v]) == a + (v - u) * bytes &&
+           (!known || a + (v - u + 1) * bytes <= rb + rn))
+      v++;
     const cudaError_t e = cudaMemcpyAsync(dst + u * bytes, srcs[u], (v - u) * bytes, kind, s);
     if (e != cudaSuccess) return e;
     u = v;
