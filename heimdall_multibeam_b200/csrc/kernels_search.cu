@@ -479,7 +479,7 @@ size_t scan_smem_bytes(int ser, int nbeams, int ch) {
 // spread over more samples and each producer lane has CH / 128 independent
 // float4 values in flight.
 template <int CH>
-__global__ void __launch_bounds__(256, 4) k_normalise_scan(
+__global__ void __launch_bounds__(256, CH >= 512 ? 3 : 4) k_normalise_scan(
     const float* __restrict__ data, size_t pitch, int nser, unsigned len, unsigned stride,
     int nbeams, const float* __restrict__ rms, float* __restrict__ scan, size_t scan_pitch,
     float* norm_out, int ser_per_block, unsigned* err) {
