@@ -283,11 +283,13 @@ def run_product(args):
     for _ in range(args.warmup):
         batched()
     l0 = H.launch_count()
+    r0 = pl.graph_replays()
     stage = {k: 0.0 for k in pl.timing()}
     clk = ClockSampler(dev.index)
     clk.start()
     ms = _timed(torch, dev, barrier, args.steps, batched, stage, pl.timing)
     launches = H.launch_count() - l0
+    replays = pl.graph_replays() - r0
     cands = [pl.candidates(u) for u in range(U)] if U > 1 else [pl.candidates()]
     tile = pl.dedisp_tile()
     tile_source = pl.dedisp_tile_source()
@@ -427,6 +429,8 @@ def run_product(args):
             "roofline": roof,
             "recall": {"snr_ge_8_found": hit, "snr_ge_8_injected": nstrong},
             "gpu_launches": int(launches),
+            # timed gulps served by one CUDA graph replay each (hd_get_graph_replays)
+            "graph_replays": int(replays),
             "clocks": clocks,
         }
         if ms_plain is not None:
